@@ -1,0 +1,176 @@
+/*
+ * sdot.h -- C ABI of libsdot_cuda.so, the B200 (sm_100a) implementation of
+ * SemiDiscreteOT's entropic semi-discrete dual evaluation and its solver.
+ *
+ * Plain C: pointers, sizes and status codes; no exceptions, no C++ or torch
+ * types cross this boundary.  Host pointers passed in are caller-owned and
+ * copied; device state is library-owned.  One context per host thread (a
+ * context owns its CUDA stream).  Unless stated otherwise every array uses the
+ * caller's ordering (the library reorders internally and maps back).
+ *
+ * Each entry point cites the reference interface it replaces
+ * (paths relative to the SemiDiscreteOT source tree).
+ */
+#ifndef SDOT_H
+#define SDOT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SDOT_ABI_VERSION 1
+
+typedef enum {
+    SDOT_OK = 0,
+    SDOT_EINVAL = 1,       /* bad argument / inconsistent sizes */
+    SDOT_ENOMEM = 2,       /* device allocation failed */
+    SDOT_ENONFINITE = 3,   /* NaN/Inf in inputs or in the evaluated functional */
+    SDOT_ELINESEARCH = 4,  /* line search could not satisfy the Wolfe conditions */
+    SDOT_EMAXITER = 5,     /* solver stopped at max_iterations without converging */
+    SDOT_EBUDGET = 6,      /* request exceeds the context's device-memory budget */
+    SDOT_ETIMEOUT = 7,     /* a bounded device wait expired */
+    SDOT_ECUDA = 8,        /* CUDA runtime error (message in sdot_last_error) */
+    SDOT_ESTATE = 9        /* call made in the wrong state (e.g. no source set) */
+} sdot_status;
+
+/* Arithmetic of the two exponential sweeps.
+ *   SDOT_PREC_FP64  : both sweeps in FP64 (value 1e-10 rel., gradient ~1e-14).
+ *   SDOT_PREC_HYBRID: value sweep FP64, gradient sweep FP32 exp2 with FP64
+ *                     accumulation (gradient error <= ~3e-6 * max nu_j).
+ *   SDOT_PREC_MIXED : both sweeps FP32 exp2, FP64 accumulation.            */
+typedef enum { SDOT_PREC_FP64 = 0, SDOT_PREC_HYBRID = 1, SDOT_PREC_MIXED = 2 } sdot_precision;
+
+typedef enum { SDOT_THRESH_POINTWISE = 0, SDOT_THRESH_INTEGRAL = 1, SDOT_THRESH_GEOMETRIC = 2 } sdot_threshold_type;
+typedef enum { SDOT_CONTROL_L1NORM = 0, SDOT_CONTROL_COMPONENTWISE = 1, SDOT_CONTROL_LINF = 2 } sdot_control_type;
+typedef enum { SDOT_LS_UPSTREAM = 0, SDOT_LS_VENDORED = 1 } sdot_line_search;
+
+typedef struct {
+    int device;                 /* CUDA device ordinal */
+    int precision;              /* sdot_precision */
+    size_t memory_budget;       /* bytes of device memory the context may hold (0 = unlimited) */
+    int verbose;                /* print per-iteration lines like VerboseSolverControl */
+} sdot_options;
+
+/* Mirrors SotParameterManager::SolverParameters
+ * (include/SemiDiscreteOT/utils/ParameterManager.h:56-72) plus the line
+ * search variant. */
+typedef struct {
+    unsigned max_iterations;    /* max_iterations (default 1000) */
+    double tolerance;           /* tolerance (default 1) */
+    int control_type;           /* solver_control_type: l1norm | componentwise | linf */
+    double epsilon;             /* epsilon (default 1e-3) */
+    double tau;                 /* tau (default 1e-8); <= 0 disables truncation */
+    int threshold_type;         /* distance_threshold_type */
+    int use_log_sum_exp;        /* use_log_sum_exp_trick (default false) */
+    int line_search;            /* sdot_line_search: deal.II SolverBFGS (default) or the vendored copy */
+} sdot_solver_params;
+
+typedef struct {
+    double value;               /* J(psi) */
+    double C_global;            /* sum_q rho_q JxW_q / S_q */
+    double threshold;           /* distance threshold used */
+    int64_t n_pairs;            /* sum over q of |candidates(cell(q))| */
+    double device_ms;           /* device time of the evaluation (CUDA events) */
+} sdot_eval_info;
+
+typedef struct {
+    unsigned iterations;        /* like get_last_iteration_count() */
+    int converged;              /* like get_convergence_status() */
+    int64_t n_evaluations;
+    double last_value;
+    double last_check_value;
+    int64_t total_pairs;
+    double device_ms;
+} sdot_solve_info;
+
+typedef struct sdot_ctx sdot_ctx;
+
+/* Library identity: ABI version and the sm architecture it was built for. */
+int sdot_abi_version(void);
+const char *sdot_build_info(void);
+
+/* Human-readable text of the last error on this context (never NULL). */
+const char *sdot_last_error(const sdot_ctx *ctx);
+
+/* Replaces SotSolver::SotSolver(const MPI_Comm&)
+ * (include/SemiDiscreteOT/solvers/SotSolver.h:176; src/solvers/SotSolver.cc:3-20). */
+sdot_status sdot_create(sdot_ctx **ctx, const sdot_options *opts);
+void sdot_destroy(sdot_ctx *ctx);
+
+/* Replaces SotSolver::setup_source(dof_handler, mapping, fe, density,
+ * quadrature_order) (SotSolver.h:186-190; SotSolver.cc:43-51).  deal.II objects
+ * cannot cross a C ABI, so the source arrives flattened exactly as
+ * SemiDiscreteOT::save_discrete_measures writes it (src/core/SemiDiscreteOT.cc
+ * :2489-2558): quadrature points x (n_q*dim, row-major), JxW and the density
+ * value at each point, grouped by cell: cell c owns points
+ * [cell_offsets[c], cell_offsets[c+1]) and has centre cell_centers[c*dim..]
+ * (TriaAccessor::center(), used by the truncation query at SotSolver.cc:801). */
+sdot_status sdot_set_source(sdot_ctx *ctx, int dim, int64_t n_q, const double *x,
+                            const double *jxw, const double *density, int64_t n_cells,
+                            const int64_t *cell_offsets, const double *cell_centers);
+
+/* Replaces SotSolver::setup_target(points, density) (SotSolver.h:197-198;
+ * SotSolver.cc:53-60).  Like the reference, the weights are NOT normalised. */
+sdot_status sdot_set_target(sdot_ctx *ctx, int64_t n, const double *y, const double *nu);
+
+/* Replaces SotSolver::configure(params) (SotSolver.h:204; SotSolver.cc:62-69). */
+sdot_status sdot_configure(sdot_ctx *ctx, const sdot_solver_params *params);
+/* Defaults of SolverParameters (ParameterManager.h:56-72). */
+void sdot_default_params(sdot_solver_params *params);
+
+/* Replaces SotSolver::evaluate_functional(psi, gradient_out) (SotSolver.h:336-337;
+ * SotSolver.cc:217-377): returns J(psi) in *value and grad_j =
+ * sum_q w_q pi_qj - nu_j in grad (host arrays of n_targets doubles).  Updates
+ * the persistent state read by the integral/geometric thresholds, like the
+ * reference's members global_functional and C_global. */
+sdot_status sdot_evaluate(sdot_ctx *ctx, const double *psi, double *grad, double *value,
+                          sdot_eval_info *info);
+
+/* Same evaluation on device pointers (internal ordering is NOT applied: psi
+ * and grad are in the caller's ordering, resident on the context's device);
+ * no host synchronisation beyond reading the scalar value. */
+sdot_status sdot_evaluate_device(sdot_ctx *ctx, const double *psi_dev, double *grad_dev,
+                                 double *value, sdot_eval_info *info);
+
+/* Replaces SotSolver::solve(potential, params) (SotSolver.h:211-212;
+ * SotSolver.cc:105-215): L-BFGS (history 5) with the strong-Wolfe line search
+ * of deal.II SolverBFGS, driven on the device.  psi is read as the initial
+ * potential and overwritten with the result.  Like the reference,
+ * non-convergence is not an error: it returns SDOT_OK with converged = 0
+ * (query sdot_get_convergence_status); SDOT_ELINESEARCH corresponds to the
+ * exception the upstream line search throws. */
+sdot_status sdot_solve(sdot_ctx *ctx, double *psi, const sdot_solver_params *params,
+                       sdot_solve_info *info);
+
+/* Replaces the declared-only SotSolver::compute_hessian(potential, hessian_out)
+ * (SotSolver.h:343-344): dense row-major n_targets x n_targets matrix
+ * H = (1/eps) sum_q w_q (diag(pi_q) - pi_q pi_q^T) into host memory H. */
+sdot_status sdot_hessian(sdot_ctx *ctx, const double *psi, double *H);
+
+/* Getters replacing SotSolver::get_last_functional_value, get_last_iteration_count,
+ * get_convergence_status, get_last_distance_threshold, get_C_global
+ * (SotSolver.h:233-255) and the setter set_distance_threshold (:261). */
+double sdot_get_last_functional_value(const sdot_ctx *ctx);
+unsigned sdot_get_last_iteration_count(const sdot_ctx *ctx);
+int sdot_get_convergence_status(const sdot_ctx *ctx);
+double sdot_get_last_distance_threshold(const sdot_ctx *ctx);
+double sdot_get_C_global(const sdot_ctx *ctx);
+sdot_status sdot_set_distance_threshold(sdot_ctx *ctx, double threshold);
+
+/* Replaces SotSolver::compute_covering_radius (SotSolver.h:275; SotSolver.cc:431-473). */
+sdot_status sdot_compute_covering_radius(sdot_ctx *ctx, double *radius);
+/* Replaces SotSolver::compute_geometric_radius_bound (SotSolver.h:296-299;
+ * SotSolver.cc:509-551). */
+sdot_status sdot_compute_geometric_radius_bound(sdot_ctx *ctx, const double *psi, double epsilon,
+                                                double tolerance, double *radius);
+/* Replaces SotSolver::set_distance_function (SotSolver.h:305; SotSolver.cc:22-41):
+ * only "euclidean" is on the accelerated path; anything else is SDOT_EINVAL. */
+sdot_status sdot_set_distance_function(sdot_ctx *ctx, const char *name);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SDOT_H */

@@ -1,0 +1,15 @@
+"""semidiscreteot_b200 -- B200-native entropic semi-discrete OT dual evaluation.
+
+A drop-in for the hot path of SemiDiscreteOT's ``SotSolver`` (functional,
+gradient, Hessian and the L-BFGS solve), implemented as hand-written sm_100a
+CUDA kernels behind the C ABI in ``include/sdot.h`` (``libsdot_cuda.so``).
+"""
+from .parameters import (MultilevelParameters, SolverParameters, distribute_epsilon_values, epsilon_sequence,
+                         read_prm, solver_parameters_from_prm, multilevel_parameters_from_prm)
+from .solver import SotSolver
+from .source import structured_source
+
+__all__ = [
+    "SotSolver", "SolverParameters", "MultilevelParameters", "read_prm", "solver_parameters_from_prm",
+    "multilevel_parameters_from_prm", "epsilon_sequence", "distribute_epsilon_values", "structured_source",
+]

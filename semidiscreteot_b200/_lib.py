@@ -1,0 +1,111 @@
+"""ctypes binding of ``libsdot_cuda.so`` (declared in ``include/sdot.h``).
+
+The shared library is built in-tree (``python -m semidiscreteot_b200.build``)
+and is required: there is no CPU fallback.  Loading it needs no GPU (CUDA is
+linked statically); creating a context does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libsdot_cuda.so")
+
+SDOT_OK = 0
+STATUS_NAMES = {
+    0: "SDOT_OK", 1: "SDOT_EINVAL", 2: "SDOT_ENOMEM", 3: "SDOT_ENONFINITE", 4: "SDOT_ELINESEARCH",
+    5: "SDOT_EMAXITER", 6: "SDOT_EBUDGET", 7: "SDOT_ETIMEOUT", 8: "SDOT_ECUDA", 9: "SDOT_ESTATE",
+}
+PRECISION = {"fp64": 0, "hybrid": 1, "mixed": 2}
+THRESHOLD = {"pointwise": 0, "integral": 1, "geometric": 2}
+CONTROL = {"l1norm": 0, "componentwise": 1, "linf": 2}
+LINE_SEARCH = {"upstream": 0, "vendored": 1}
+
+# Every symbol include/sdot.h declares (checked by tests).
+EXPORTED = [
+    "sdot_abi_version", "sdot_build_info", "sdot_last_error", "sdot_create", "sdot_destroy",
+    "sdot_set_source", "sdot_set_target", "sdot_configure", "sdot_default_params", "sdot_evaluate",
+    "sdot_evaluate_device", "sdot_solve", "sdot_hessian", "sdot_get_last_functional_value",
+    "sdot_get_last_iteration_count", "sdot_get_convergence_status", "sdot_get_last_distance_threshold",
+    "sdot_get_C_global", "sdot_set_distance_threshold", "sdot_compute_covering_radius",
+    "sdot_compute_geometric_radius_bound", "sdot_set_distance_function",
+]
+
+
+class Options(C.Structure):
+    _fields_ = [("device", C.c_int), ("precision", C.c_int), ("memory_budget", C.c_size_t),
+                ("verbose", C.c_int)]
+
+
+class SolverParams(C.Structure):
+    _fields_ = [("max_iterations", C.c_uint), ("tolerance", C.c_double), ("control_type", C.c_int),
+                ("epsilon", C.c_double), ("tau", C.c_double), ("threshold_type", C.c_int),
+                ("use_log_sum_exp", C.c_int), ("line_search", C.c_int)]
+
+
+class EvalInfo(C.Structure):
+    _fields_ = [("value", C.c_double), ("C_global", C.c_double), ("threshold", C.c_double),
+                ("n_pairs", C.c_int64), ("device_ms", C.c_double)]
+
+
+class SolveInfo(C.Structure):
+    _fields_ = [("iterations", C.c_uint), ("converged", C.c_int), ("n_evaluations", C.c_int64),
+                ("last_value", C.c_double), ("last_check_value", C.c_double), ("total_pairs", C.c_int64),
+                ("device_ms", C.c_double)]
+
+
+_lib = None
+
+
+def load():
+    """Load the library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build the CUDA library first "
+            "(python -m semidiscreteot_b200.build); there is no CPU fallback")
+    lib = C.CDLL(LIB_PATH)
+    vp, i64, d, ip = C.c_void_p, C.c_int64, C.c_double, C.c_int
+    lib.sdot_abi_version.restype = ip
+    lib.sdot_build_info.restype = C.c_char_p
+    lib.sdot_last_error.argtypes = [vp]
+    lib.sdot_last_error.restype = C.c_char_p
+    lib.sdot_create.argtypes = [C.POINTER(vp), C.POINTER(Options)]
+    lib.sdot_destroy.argtypes = [vp]
+    lib.sdot_destroy.restype = None
+    lib.sdot_set_source.argtypes = [vp, ip, i64, vp, vp, vp, i64, vp, vp]
+    lib.sdot_set_target.argtypes = [vp, i64, vp, vp]
+    lib.sdot_configure.argtypes = [vp, C.POINTER(SolverParams)]
+    lib.sdot_default_params.argtypes = [C.POINTER(SolverParams)]
+    lib.sdot_default_params.restype = None
+    lib.sdot_evaluate.argtypes = [vp, vp, vp, C.POINTER(d), C.POINTER(EvalInfo)]
+    lib.sdot_evaluate_device.argtypes = [vp, vp, vp, C.POINTER(d), C.POINTER(EvalInfo)]
+    lib.sdot_solve.argtypes = [vp, vp, C.POINTER(SolverParams), C.POINTER(SolveInfo)]
+    lib.sdot_hessian.argtypes = [vp, vp, vp]
+    for name in ("sdot_get_last_functional_value", "sdot_get_last_distance_threshold", "sdot_get_C_global"):
+        getattr(lib, name).argtypes = [vp]
+        getattr(lib, name).restype = d
+    lib.sdot_get_last_iteration_count.argtypes = [vp]
+    lib.sdot_get_last_iteration_count.restype = C.c_uint
+    lib.sdot_get_convergence_status.argtypes = [vp]
+    lib.sdot_get_convergence_status.restype = ip
+    lib.sdot_set_distance_threshold.argtypes = [vp, d]
+    lib.sdot_compute_covering_radius.argtypes = [vp, C.POINTER(d)]
+    lib.sdot_compute_geometric_radius_bound.argtypes = [vp, vp, d, d, C.POINTER(d)]
+    lib.sdot_set_distance_function.argtypes = [vp, C.c_char_p]
+    for fn in ("sdot_create", "sdot_set_source", "sdot_set_target", "sdot_configure", "sdot_evaluate",
+               "sdot_evaluate_device", "sdot_solve", "sdot_hessian", "sdot_set_distance_threshold",
+               "sdot_compute_covering_radius", "sdot_compute_geometric_radius_bound",
+               "sdot_set_distance_function"):
+        getattr(lib, fn).restype = ip
+    _lib = lib
+    return lib
+
+
+class SdotError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status

@@ -1,0 +1,953 @@
+// sdot_capi.cu -- C ABI of libsdot_cuda: context, measures, evaluation,
+// solver and queries.  Host logic in C++; all per-pair work on the device.
+#include <float.h>
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "sdot_device.cuh"
+#include "sdot_internal.h"
+
+using namespace sdot;
+
+namespace sdot {
+
+sdot_status set_error(sdot_ctx *c, sdot_status s, const std::string &msg)
+{
+    if (c) c->err = msg;
+    return s;
+}
+
+sdot_status cuda_error(sdot_ctx *c, cudaError_t e, const char *where)
+{
+    if (e == cudaSuccess) return SDOT_OK;
+    if (e == cudaErrorMemoryAllocation)
+        return set_error(c, SDOT_ENOMEM, std::string(where) + ": " + cudaGetErrorString(e));
+    return set_error(c, SDOT_ECUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+}  // namespace sdot
+
+#define CK(call, where)                                        \
+    do {                                                       \
+        cudaError_t e_ = (call);                               \
+        if (e_ != cudaSuccess) return cuda_error(c, e_, where); \
+    } while (0)
+
+namespace {
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+// Interleave the low 21 bits of three coordinates (2D: two coordinates, 31 bits).
+uint64_t morton(const double *p, int dim, const double *lo, const double *hi)
+{
+    uint64_t code = 0;
+    const int bits = dim == 3 ? 21 : 31;
+    const double scale = (double)((1u << (bits < 31 ? bits : 31)) - 1);
+    uint64_t q[3] = {0, 0, 0};
+    for (int d = 0; d < dim; ++d) {
+        const double ext = hi[d] - lo[d];
+        double t = ext > 0 ? (p[d] - lo[d]) / ext : 0.0;
+        t = std::min(std::max(t, 0.0), 1.0);
+        q[d] = (uint64_t)(t * scale);
+    }
+    for (int b = bits - 1; b >= 0; --b)
+        for (int d = dim - 1; d >= 0; --d) code = (code << 1) | ((q[d] >> b) & 1u);
+    return code;
+}
+
+std::vector<int64_t> morton_order(const std::vector<double> &pts, int dim, int64_t n)
+{
+    double lo[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, hi[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+    for (int64_t i = 0; i < n; ++i)
+        for (int d = 0; d < dim; ++d) {
+            lo[d] = std::min(lo[d], pts[i * dim + d]);
+            hi[d] = std::max(hi[d], pts[i * dim + d]);
+        }
+    std::vector<uint64_t> code(n);
+    for (int64_t i = 0; i < n; ++i) code[i] = morton(&pts[i * dim], dim, lo, hi);
+    std::vector<int64_t> ord(n);
+    std::iota(ord.begin(), ord.end(), 0);
+    std::stable_sort(ord.begin(), ord.end(), [&](int64_t a, int64_t b) { return code[a] < code[b]; });
+    return ord;
+}
+
+// Bounding sphere (bbox centre, max distance, enlarged by 1e-12 relative).
+void sphere_of(const double *pts, const std::vector<int64_t> &idx, int dim, double *out)
+{
+    double lo[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, hi[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+    for (int64_t i : idx)
+        for (int d = 0; d < dim; ++d) {
+            lo[d] = std::min(lo[d], pts[i * dim + d]);
+            hi[d] = std::max(hi[d], pts[i * dim + d]);
+        }
+    double c[3] = {0, 0, 0};
+    for (int d = 0; d < dim; ++d) c[d] = 0.5 * (lo[d] + hi[d]);
+    double R = 0.0;
+    for (int64_t i : idx) {
+        double s = 0.0;
+        for (int d = 0; d < dim; ++d) {
+            const double t = pts[i * dim + d] - c[d];
+            s += t * t;
+        }
+        R = std::max(R, std::sqrt(s));
+    }
+    out[0] = c[0];
+    out[1] = c[1];
+    out[2] = c[2];
+    out[3] = R * (1.0 + 1e-12) + 1e-300;
+}
+
+bool all_finite(const double *v, int64_t n)
+{
+    for (int64_t i = 0; i < n; ++i)
+        if (!std::isfinite(v[i])) return false;
+    return true;
+}
+
+void update_geometry(sdot_ctx *c)
+{
+    if (c->nq == 0 || c->nt == 0) return;
+    double lo[3], hi[3], s = 0.0;
+    for (int d = 0; d < 3; ++d) {
+        lo[d] = std::min(c->src_lo[d], c->tgt_lo[d]);
+        hi[d] = std::max(c->src_hi[d], c->tgt_hi[d]);
+        c->origin[d] = d < c->dim ? 0.5 * (lo[d] + hi[d]) : 0.0;
+        if (d < c->dim) s += (hi[d] - lo[d]) * (hi[d] - lo[d]);
+    }
+    c->diam = std::sqrt(s) * (1.0 + 1e-12);
+}
+
+size_t device_bytes(const sdot_ctx *c)
+{
+    return c->x.bytes() + c->rho.bytes() + c->jxw.bytes() + c->w.bytes() + c->lw.bytes() + c->cell_ctr.bytes() +
+           c->sblk_sph.bytes() + c->cblk_sph.bytes() + c->y.bytes() + c->nu.bytes() + c->perm.bytes() +
+           c->tblk_sph.bytes() + c->psi.bytes() + c->grad.bytes() + c->tpack.bytes() + c->Lq.bytes() +
+           c->gpart.bytes() + c->blkpart.bytes() + c->scal.bytes() + c->redpart.bytes() + c->io_a.bytes() +
+           c->io_b.bytes() + c->x0.bytes() + c->pdir.bytes() + c->sk.bytes() + c->yk.bytes() + c->hist_s.bytes() +
+           c->hist_y.bytes() + c->gtmp.bytes();
+}
+
+sdot_status ensure_eval_buffers(sdot_ctx *c)
+{
+    const int64_t nt = c->nt, nq = c->nq;
+    const int64_t dense_blocks = (nq + DENSE_A_THREADS * DENSE_A_QT - 1) / (DENSE_A_THREADS * DENSE_A_QT);
+    const int64_t nval = std::max<int64_t>(dense_blocks, c->nsblk);
+    const size_t need = (size_t)(nt * (2 + TPACK + 64 + 2) + nq + 4 * nval + 148 * 8 + 64) * sizeof(double);
+    if (c->budget && device_bytes(c) + need > c->budget && c->tpack.n < (size_t)(nt * TPACK))
+        return set_error(c, SDOT_EBUDGET, "evaluation buffers exceed the context memory budget");
+    CK(c->psi.alloc(nt), "alloc psi");
+    CK(c->grad.alloc(nt), "alloc grad");
+    CK(c->tpack.alloc(nt * TPACK), "alloc tpack");
+    CK(c->Lq.alloc(nq), "alloc Lq");
+    CK(c->gpart.alloc(nt * 64), "alloc gpart");
+    CK(c->blkpart.alloc(4 * nval), "alloc blkpart");
+    CK(c->redpart.alloc(148 * 8), "alloc redpart");
+    CK(c->scal.alloc(SC_COUNT), "alloc scal");
+    CK(c->io_a.alloc(nt), "alloc io");
+    CK(c->io_b.alloc(nt), "alloc io");
+    return SDOT_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// covering radius: max over cells of min over targets of |y_j - c_K|
+// (SotSolver.cc:431-473; the R-tree nearest query returns the same distance)
+// ---------------------------------------------------------------------------
+
+template <int DIM>
+__global__ void k_covering(const double *__restrict__ cell_ctr, int64_t ncells, const double *__restrict__ y,
+                           int64_t nt, double *__restrict__ blockmax)
+{
+    __shared__ double sy[1024 * DIM];
+    __shared__ double red[32];
+    const int64_t cidx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    double cc[3] = {0, 0, 0};
+    if (cidx < ncells)
+        for (int d = 0; d < DIM; ++d) cc[d] = cell_ctr[cidx * DIM + d];
+    double best = DBL_MAX;
+    for (int64_t t0 = 0; t0 < nt; t0 += 1024) {
+        const int tn = (int)min((int64_t)1024, nt - t0);
+        __syncthreads();
+        for (int i = threadIdx.x; i < tn * DIM; i += blockDim.x) sy[i] = y[t0 * DIM + i];
+        __syncthreads();
+        for (int t = 0; t < tn; ++t) best = fmin(best, dist2_exact<DIM>(sy + t * DIM, cc));
+    }
+    double v = cidx < ncells ? __dsqrt_rn(best) : 0.0;
+    v = warp_max(v);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = 0.0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) m = fmax(m, red[i]);
+        blockmax[blockIdx.x] = m;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// L-BFGS device kernels
+// ---------------------------------------------------------------------------
+
+// History of the L-BFGS two-loop recursion: m logical entries, newest first,
+// mapped onto physical slots of the S/Y arrays (one spare slot receives the
+// next s_k, y_k before the curvature test decides whether it is kept).
+struct Hist {
+    int m;
+    int slot[6];
+};
+
+// Two-loop recursion (deal.II SolverBFGS::solve, wasserstein_solver_bfgs.h
+// :420-441), H0 = I; one CTA, order-fixed reductions.  Also writes g.p.
+__global__ void __launch_bounds__(1024)
+k_two_loop(int64_t n, Hist h, const double *__restrict__ S, const double *__restrict__ Y,
+           const double *__restrict__ rho, const double *__restrict__ g, double *__restrict__ p,
+           double *__restrict__ gp_out)
+{
+    __shared__ double red[32];
+    __shared__ double bc;
+    __shared__ double c1[8];
+    const int tid = threadIdx.x;
+    auto block_dot = [&](const double *a, const double *b) -> double {
+        double s = 0.0;
+        for (int64_t i = tid; i < n; i += blockDim.x) s += a[i] * b[i];
+        s = warp_sum(s);
+        __syncthreads();
+        if ((tid & 31) == 0) red[tid >> 5] = s;
+        __syncthreads();
+        if (tid == 0) {
+            double t = 0.0;
+            for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
+            bc = t;
+        }
+        __syncthreads();
+        return bc;
+    };
+    for (int64_t i = tid; i < n; i += blockDim.x) p[i] = g[i];
+    __syncthreads();
+    for (int i = 0; i < h.m; ++i) {
+        const int slot = h.slot[i];
+        const double ci = rho[slot] * block_dot(S + (int64_t)slot * n, p);
+        if (tid == 0) c1[i] = ci;
+        const double a = -ci;
+        const double *yv = Y + (int64_t)slot * n;
+        for (int64_t t = tid; t < n; t += blockDim.x) p[t] += a * yv[t];
+        __syncthreads();
+    }
+    for (int i = h.m - 1; i >= 0; --i) {
+        const int slot = h.slot[i];
+        const double c2 = rho[slot] * block_dot(Y + (int64_t)slot * n, p);
+        const double a = c1[i] - c2;
+        const double *sv = S + (int64_t)slot * n;
+        for (int64_t t = tid; t < n; t += blockDim.x) p[t] += a * sv[t];
+        __syncthreads();
+    }
+    for (int64_t i = tid; i < n; i += blockDim.x) p[i] *= -1.;
+    __syncthreads();
+    const double gp = block_dot(g, p);
+    if (tid == 0) gp_out[0] = gp;
+}
+
+// s_k = x - x_old, y_k = g - g_old into a history slot; out = s_k . y_k
+__global__ void __launch_bounds__(1024)
+k_sy(int64_t n, const double *__restrict__ x, const double *__restrict__ xold, const double *__restrict__ g,
+     const double *__restrict__ gold, double *__restrict__ s, double *__restrict__ yv, double *__restrict__ out)
+{
+    __shared__ double red[32];
+    double acc = 0.0;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const double a = x[i] - xold[i];
+        const double b = g[i] - gold[i];
+        s[i] = a;
+        yv[i] = b;
+        acc += a * b;
+    }
+    acc = warp_sum(acc);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
+        out[0] = t;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+
+extern "C" {
+
+int sdot_abi_version(void) { return SDOT_ABI_VERSION; }
+
+const char *sdot_build_info(void)
+{
+    return "libsdot_cuda sm_100a (B200): FP64 exp2 value sweep, FP32/FP64 gradient sweep, exact cell-centre "
+           "truncation, device L-BFGS";
+}
+
+const char *sdot_last_error(const sdot_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+void sdot_default_params(sdot_solver_params *p)
+{
+    if (!p) return;
+    p->max_iterations = 1000;
+    p->tolerance = 1;
+    p->control_type = SDOT_CONTROL_L1NORM;
+    p->epsilon = 1e-3;
+    p->tau = 1e-8;
+    p->threshold_type = SDOT_THRESH_POINTWISE;
+    p->use_log_sum_exp = 0;
+    p->line_search = SDOT_LS_UPSTREAM;
+}
+
+sdot_status sdot_create(sdot_ctx **out, const sdot_options *opts)
+{
+    if (!out) return SDOT_EINVAL;
+    *out = nullptr;
+    sdot_ctx *c = new sdot_ctx();
+    if (opts) {
+        c->device = opts->device;
+        c->precision = opts->precision;
+        c->budget = opts->memory_budget;
+        c->verbose = opts->verbose;
+    }
+    if (c->precision < SDOT_PREC_FP64 || c->precision > SDOT_PREC_MIXED) {
+        delete c;
+        return SDOT_EINVAL;
+    }
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || c->device < 0 || c->device >= ndev) {
+        delete c;
+        return e != cudaSuccess ? SDOT_ECUDA : SDOT_EINVAL;
+    }
+    DeviceGuard g(c->device);
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
+        cudaMallocHost(&c->scal_host, SC_COUNT * sizeof(double)) != cudaSuccess) {
+        sdot_destroy(c);
+        return SDOT_ECUDA;
+    }
+    memset(c->scal_host, 0, SC_COUNT * sizeof(double));
+    sdot_default_params(&c->prm);
+    *out = c;
+    return SDOT_OK;
+}
+
+void sdot_destroy(sdot_ctx *c)
+{
+    if (!c) return;
+    {
+        DeviceGuard g(c->device);
+        if (c->stream) cudaStreamSynchronize(c->stream);
+        c->x.release(); c->rho.release(); c->jxw.release(); c->w.release(); c->lw.release();
+        c->cell_ctr.release(); c->sblk_sph.release(); c->cblk_sph.release(); c->y.release(); c->nu.release();
+        c->perm.release(); c->tblk_sph.release(); c->psi.release(); c->grad.release(); c->tpack.release();
+        c->Lq.release(); c->gpart.release(); c->blkpart.release(); c->scal.release(); c->redpart.release();
+        c->io_a.release(); c->io_b.release(); c->x0.release(); c->pdir.release(); c->sk.release(); c->yk.release();
+        c->hist_s.release(); c->hist_y.release(); c->gtmp.release();
+        if (c->scal_host) cudaFreeHost(c->scal_host);
+        if (c->ev0) cudaEventDestroy(c->ev0);
+        if (c->ev1) cudaEventDestroy(c->ev1);
+        if (c->stream) cudaStreamDestroy(c->stream);
+    }
+    delete c;
+}
+
+sdot_status sdot_set_source(sdot_ctx *c, int dim, int64_t n_q, const double *x, const double *jxw,
+                            const double *density, int64_t n_cells, const int64_t *cell_offsets,
+                            const double *cell_centers)
+{
+    if (!c) return SDOT_EINVAL;
+    if ((dim != 2 && dim != 3) || n_q <= 0 || n_cells <= 0 || !x || !jxw || !density || !cell_offsets ||
+        !cell_centers)
+        return set_error(c, SDOT_EINVAL, "set_source: bad arguments");
+    if (c->nt > 0 && c->dim != dim) return set_error(c, SDOT_EINVAL, "set_source: dimension differs from targets");
+    if (cell_offsets[0] != 0 || cell_offsets[n_cells] != n_q)
+        return set_error(c, SDOT_EINVAL, "set_source: cell_offsets must start at 0 and end at n_q");
+    const int64_t qpc = cell_offsets[1] - cell_offsets[0];
+    if (qpc <= 0 || qpc > MAX_QPC) return set_error(c, SDOT_EINVAL, "set_source: 1..64 quadrature points per cell");
+    for (int64_t k = 0; k < n_cells; ++k)
+        if (cell_offsets[k + 1] - cell_offsets[k] != qpc)
+            return set_error(c, SDOT_EINVAL, "set_source: every cell must have the same number of quadrature points");
+    if (!all_finite(x, n_q * dim) || !all_finite(jxw, n_q) || !all_finite(density, n_q) ||
+        !all_finite(cell_centers, n_cells * dim))
+        return set_error(c, SDOT_ENONFINITE, "set_source: non-finite input");
+    DeviceGuard g(c->device);
+    std::vector<double> ctr(cell_centers, cell_centers + n_cells * dim);
+    const std::vector<int64_t> ord = morton_order(ctr, dim, n_cells);
+    std::vector<double> hx(n_q * dim), hr(n_q), hj(n_q), hw(n_q), hc(n_cells * dim);
+    bool nonneg = true;
+    for (int64_t k = 0; k < n_cells; ++k) {
+        const int64_t src = ord[k];
+        for (int d = 0; d < dim; ++d) hc[k * dim + d] = cell_centers[src * dim + d];
+        for (int64_t i = 0; i < qpc; ++i) {
+            const int64_t qs = src * qpc + i, qd = k * qpc + i;
+            for (int d = 0; d < dim; ++d) hx[qd * dim + d] = x[qs * dim + d];
+            hr[qd] = density[qs];
+            hj[qd] = jxw[qs];
+            hw[qd] = density[qs] * jxw[qs];
+            if (hw[qd] < 0) nonneg = false;
+        }
+    }
+    // value-sweep units and blocks
+    int ql;
+    if (qpc <= 4) ql = (int)qpc;
+    else if (qpc <= 9) ql = (int)qpc;
+    else ql = (qpc % 9 == 0) ? 9 : 8;
+    const int ngroups = (int)((qpc + ql - 1) / ql);
+    const int64_t nunits = n_cells * ngroups;
+    const int64_t nsblk = (nunits + SBLK_CELLS - 1) / SBLK_CELLS;
+    std::vector<double> ssph(nsblk * 4);
+    for (int64_t b = 0; b < nsblk; ++b) {
+        std::vector<int64_t> cells;
+        for (int64_t u = b * SBLK_CELLS; u < std::min(nunits, (b + 1) * SBLK_CELLS); ++u) {
+            const int64_t cl = u / ngroups;
+            if (cells.empty() || cells.back() != cl) cells.push_back(cl);
+        }
+        sphere_of(hc.data(), cells, dim, &ssph[b * 4]);
+    }
+    const int64_t ncblk = (n_cells + SBLK_CELLS - 1) / SBLK_CELLS;
+    std::vector<double> csph(ncblk * 4);
+    for (int64_t b = 0; b < ncblk; ++b) {
+        std::vector<int64_t> cells;
+        for (int64_t k = b * SBLK_CELLS; k < std::min(n_cells, (b + 1) * SBLK_CELLS); ++k) cells.push_back(k);
+        sphere_of(hc.data(), cells, dim, &csph[b * 4]);
+    }
+    c->dim = dim;
+    c->nq = n_q;
+    c->ncells = n_cells;
+    c->qpc = (int)qpc;
+    c->ql = ql;
+    c->ngroups = ngroups;
+    c->nsblk = nsblk;
+    c->ncblk = ncblk;
+    c->w_nonneg = nonneg;
+    for (int d = 0; d < 3; ++d) {
+        c->src_lo[d] = DBL_MAX;
+        c->src_hi[d] = -DBL_MAX;
+    }
+    for (int64_t k = 0; k < n_cells; ++k)
+        for (int d = 0; d < dim; ++d) {
+            c->src_lo[d] = std::min(c->src_lo[d], hc[k * dim + d]);
+            c->src_hi[d] = std::max(c->src_hi[d], hc[k * dim + d]);
+        }
+    for (int d = dim; d < 3; ++d) c->src_lo[d] = c->src_hi[d] = 0.0;
+    c->cell_ctr_host = hc;
+    const size_t need = (size_t)(n_q * (dim + 4) + n_cells * dim + (nsblk + ncblk) * 4) * sizeof(double);
+    if (c->budget && need > c->budget) return set_error(c, SDOT_EBUDGET, "set_source: exceeds the memory budget");
+    CK(c->x.alloc(n_q * dim), "alloc x");
+    CK(c->rho.alloc(n_q), "alloc rho");
+    CK(c->jxw.alloc(n_q), "alloc jxw");
+    CK(c->w.alloc(n_q), "alloc w");
+    CK(c->cell_ctr.alloc(n_cells * dim), "alloc cells");
+    CK(c->sblk_sph.alloc(nsblk * 4), "alloc spheres");
+    CK(c->cblk_sph.alloc(ncblk * 4), "alloc spheres");
+    CK(cudaMemcpy(c->x.p, hx.data(), hx.size() * 8, cudaMemcpyHostToDevice), "copy x");
+    CK(cudaMemcpy(c->rho.p, hr.data(), hr.size() * 8, cudaMemcpyHostToDevice), "copy rho");
+    CK(cudaMemcpy(c->jxw.p, hj.data(), hj.size() * 8, cudaMemcpyHostToDevice), "copy jxw");
+    CK(cudaMemcpy(c->w.p, hw.data(), hw.size() * 8, cudaMemcpyHostToDevice), "copy w");
+    CK(cudaMemcpy(c->cell_ctr.p, hc.data(), hc.size() * 8, cudaMemcpyHostToDevice), "copy cells");
+    CK(cudaMemcpy(c->sblk_sph.p, ssph.data(), ssph.size() * 8, cudaMemcpyHostToDevice), "copy spheres");
+    CK(cudaMemcpy(c->cblk_sph.p, csph.data(), csph.size() * 8, cudaMemcpyHostToDevice), "copy spheres");
+    c->covering_radius = 0.0;  // reference: recomputed by the next solve
+    update_geometry(c);
+    return SDOT_OK;
+}
+
+sdot_status sdot_set_target(sdot_ctx *c, int64_t n, const double *y, const double *nu)
+{
+    if (!c) return SDOT_EINVAL;
+    if (n <= 0 || !y || !nu) return set_error(c, SDOT_EINVAL, "set_target: bad arguments");
+    if (c->dim == 0) return set_error(c, SDOT_ESTATE, "set_target: set the source first (it fixes the dimension)");
+    const int dim = c->dim;
+    if (!all_finite(y, n * dim) || !all_finite(nu, n)) return set_error(c, SDOT_ENONFINITE, "set_target: non-finite input");
+    for (int64_t i = 0; i < n; ++i)
+        if (nu[i] < 0) return set_error(c, SDOT_EINVAL, "set_target: negative target weight");
+    DeviceGuard g(c->device);
+    std::vector<double> yy(y, y + n * dim);
+    const std::vector<int64_t> ord = morton_order(yy, dim, n);
+    std::vector<double> hy(n * dim), hn(n);
+    for (int64_t k = 0; k < n; ++k) {
+        for (int d = 0; d < dim; ++d) hy[k * dim + d] = y[ord[k] * dim + d];
+        hn[k] = nu[ord[k]];
+    }
+    const int64_t ntblk = (n + TBLK - 1) / TBLK;
+    std::vector<double> tsph(ntblk * 4);
+    for (int64_t b = 0; b < ntblk; ++b) {
+        std::vector<int64_t> idx;
+        for (int64_t k = b * TBLK; k < std::min(n, (b + 1) * TBLK); ++k) idx.push_back(k);
+        sphere_of(hy.data(), idx, dim, &tsph[b * 4]);
+    }
+    CK(c->y.alloc(n * dim), "alloc y");
+    CK(c->nu.alloc(n), "alloc nu");
+    CK(c->perm.alloc(n), "alloc perm");
+    CK(c->tblk_sph.alloc(ntblk * 4), "alloc spheres");
+    CK(cudaMemcpy(c->y.p, hy.data(), hy.size() * 8, cudaMemcpyHostToDevice), "copy y");
+    CK(cudaMemcpy(c->nu.p, hn.data(), hn.size() * 8, cudaMemcpyHostToDevice), "copy nu");
+    CK(cudaMemcpy(c->perm.p, ord.data(), ord.size() * 8, cudaMemcpyHostToDevice), "copy perm");
+    CK(cudaMemcpy(c->tblk_sph.p, tsph.data(), tsph.size() * 8, cudaMemcpyHostToDevice), "copy spheres");
+    c->nt = n;
+    c->ntblk = ntblk;
+    c->nu_host.assign(nu, nu + n);
+    c->y_host.assign(y, y + n * dim);
+    for (int d = 0; d < 3; ++d) {
+        c->tgt_lo[d] = 0.0;
+        c->tgt_hi[d] = 0.0;
+    }
+    for (int d = 0; d < dim; ++d) {
+        c->tgt_lo[d] = DBL_MAX;
+        c->tgt_hi[d] = -DBL_MAX;
+        for (int64_t k = 0; k < n; ++k) {
+            c->tgt_lo[d] = std::min(c->tgt_lo[d], hy[k * dim + d]);
+            c->tgt_hi[d] = std::max(c->tgt_hi[d], hy[k * dim + d]);
+        }
+    }
+    update_geometry(c);
+    return SDOT_OK;
+}
+
+sdot_status sdot_configure(sdot_ctx *c, const sdot_solver_params *p)
+{
+    if (!c || !p) return SDOT_EINVAL;
+    if (!(p->epsilon > 0) || !std::isfinite(p->epsilon)) return set_error(c, SDOT_EINVAL, "configure: epsilon must be > 0");
+    if (p->control_type < 0 || p->control_type > 2 || p->threshold_type < 0 || p->threshold_type > 2 ||
+        p->line_search < 0 || p->line_search > 1)
+        return set_error(c, SDOT_EINVAL, "configure: unknown enum value");
+    c->prm = *p;
+    return SDOT_OK;
+}
+
+sdot_status sdot_set_distance_function(sdot_ctx *c, const char *name)
+{
+    if (!c || !name) return SDOT_EINVAL;
+    if (strcmp(name, "euclidean") != 0)
+        return set_error(c, SDOT_EINVAL, std::string("Unknown distance function: ") + name);
+    return SDOT_OK;
+}
+
+static sdot_status prepare_eval(sdot_ctx *c)
+{
+    if (c->nq == 0) return set_error(c, SDOT_ESTATE, "source measure not set");
+    if (c->nt == 0) return set_error(c, SDOT_ESTATE, "target measure not set");
+    return ensure_eval_buffers(c);
+}
+
+static void fill_eval_info(sdot_ctx *c, sdot_eval_info *info, double ms)
+{
+    const double dense_pairs = (double)c->nq * (double)c->nt;
+    double pairs = c->scal_host[SC_PAIRS];
+    if (pairs == 0.0 && c->current_distance_threshold >= c->diam) pairs = dense_pairs;
+    c->last_pairs = (int64_t)pairs;
+    if (!info) return;
+    info->value = c->scal_host[SC_VALUE];
+    info->C_global = c->scal_host[SC_C];
+    info->threshold = c->current_distance_threshold;
+    info->n_pairs = (int64_t)pairs;
+    info->device_ms = ms;
+}
+
+sdot_status sdot_evaluate(sdot_ctx *c, const double *psi, double *grad, double *value, sdot_eval_info *info)
+{
+    if (!c || !psi || !grad) return SDOT_EINVAL;
+    DeviceGuard g(c->device);
+    sdot_status s = prepare_eval(c);
+    if (s != SDOT_OK) return s;
+    CK(cudaMemcpyAsync(c->io_a.p, psi, c->nt * 8, cudaMemcpyHostToDevice, c->stream), "copy psi");
+    if ((s = launch_gather(c, c->psi.p, c->io_a.p, c->nt)) != SDOT_OK) return s;
+    double ms = 0;
+    s = evaluate_internal(c, nullptr, c->prm.tolerance, &ms);
+    if (s != SDOT_OK && s != SDOT_ENONFINITE) return s;
+    sdot_status s2 = launch_scatter(c, c->io_b.p, c->grad.p, c->nt);
+    if (s2 != SDOT_OK) return s2;
+    CK(cudaMemcpyAsync(grad, c->io_b.p, c->nt * 8, cudaMemcpyDeviceToHost, c->stream), "copy grad");
+    CK(cudaStreamSynchronize(c->stream), "evaluate sync");
+    if (value) *value = c->scal_host[SC_VALUE];
+    fill_eval_info(c, info, ms);
+    return s;
+}
+
+sdot_status sdot_evaluate_device(sdot_ctx *c, const double *psi_dev, double *grad_dev, double *value,
+                                 sdot_eval_info *info)
+{
+    if (!c || !psi_dev || !grad_dev) return SDOT_EINVAL;
+    DeviceGuard g(c->device);
+    sdot_status s = prepare_eval(c);
+    if (s != SDOT_OK) return s;
+    if ((s = launch_gather(c, c->psi.p, psi_dev, c->nt)) != SDOT_OK) return s;
+    double ms = 0;
+    s = evaluate_internal(c, nullptr, c->prm.tolerance, &ms);
+    if (s != SDOT_OK && s != SDOT_ENONFINITE) return s;
+    sdot_status s2 = launch_scatter(c, grad_dev, c->grad.p, c->nt);
+    if (s2 != SDOT_OK) return s2;
+    CK(cudaStreamSynchronize(c->stream), "evaluate sync");
+    if (value) *value = c->scal_host[SC_VALUE];
+    fill_eval_info(c, info, ms);
+    return s;
+}
+
+sdot_status sdot_compute_covering_radius(sdot_ctx *c, double *radius)
+{
+    if (!c || !radius) return SDOT_EINVAL;
+    if (c->nq == 0 || c->nt == 0) return set_error(c, SDOT_ESTATE, "Invalid measures configuration for computing covering radius");
+    DeviceGuard g(c->device);
+    const int threads = 256;
+    const int64_t nb = (c->ncells + threads - 1) / threads;
+    sdot::DevBuf<double> bm;
+    CK(bm.alloc(nb), "alloc covering");
+    if (c->dim == 2)
+        k_covering<2><<<(unsigned)nb, threads, 0, c->stream>>>(c->cell_ctr.p, c->ncells, c->y.p, c->nt, bm.p);
+    else
+        k_covering<3><<<(unsigned)nb, threads, 0, c->stream>>>(c->cell_ctr.p, c->ncells, c->y.p, c->nt, bm.p);
+    CK(cudaGetLastError(), "covering launch");
+    std::vector<double> h(nb);
+    CK(cudaMemcpyAsync(h.data(), bm.p, nb * 8, cudaMemcpyDeviceToHost, c->stream), "covering copy");
+    CK(cudaStreamSynchronize(c->stream), "covering sync");
+    double m = 0.0;
+    for (double v : h) m = std::max(m, v);
+    *radius = m;
+    return SDOT_OK;
+}
+
+sdot_status sdot_compute_geometric_radius_bound(sdot_ctx *c, const double *psi, double epsilon, double tolerance,
+                                                double *radius)
+{
+    if (!c || !psi || !radius) return SDOT_EINVAL;
+    if (c->nq == 0 || c->nt == 0)
+        return set_error(c, SDOT_ESTATE, "Invalid configuration for computing geometric radius bound");
+    double r0 = c->covering_radius;
+    if (!(r0 > 0.0)) {
+        sdot_status s = sdot_compute_covering_radius(c, &r0);
+        if (s != SDOT_OK) return s;
+    }
+    double mx = psi[0], mn = psi[0];
+    for (int64_t i = 1; i < c->nt; ++i) {
+        mx = std::max(mx, psi[i]);
+        mn = std::min(mn, psi[i]);
+    }
+    const double range = mx - mn;
+    const double mind = c->min_target_density > 0.0 ? c->min_target_density
+                                                     : *std::min_element(c->nu_host.begin(), c->nu_host.end());
+    double fv = std::fabs(c->global_functional);
+    if (fv < 1e-10) fv = 1e-10;
+    const double log_term = std::log(epsilon / (mind * tolerance * fv));
+    double r2 = r0 * r0 + 2.0 * range + 2.0 * epsilon * log_term;
+    if (r2 < r0 * r0) r2 = r0 * r0;
+    *radius = std::sqrt(r2);
+    return SDOT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// solver: SotSolver::solve (SotSolver.cc:105-215) with deal.II SolverBFGS and
+// LineMinimization::line_search (third-party; algorithm restated from the
+// readable copies core/wasserstein_solver_bfgs.h:302-492 and
+// core/line_minimization.h:423-749).  Vectors live on the device; the scalar
+// control flow of the line search runs on the host with one readback per
+// trial evaluation.
+// ---------------------------------------------------------------------------
+
+namespace {
+
+struct Solver {
+    sdot_ctx *c;
+    int64_t n;
+    int64_t evals = 0;
+    double total_ms = 0.0;
+    int64_t pairs = 0;
+    double tol_comp = 0.0;
+
+    sdot_status eval_at(double *f, double *gp)
+    {
+        double ms = 0;
+        sdot_status s = evaluate_internal(c, c->pdir.p, tol_comp, &ms);
+        ++evals;
+        total_ms += ms;
+        pairs += (int64_t)c->scal_host[SC_PAIRS];
+        if (s != SDOT_OK && s != SDOT_ENONFINITE) return s;
+        *f = c->scal_host[SC_VALUE];
+        *gp = c->scal_host[SC_DOT_GP];
+        return SDOT_OK;
+    }
+
+    // x = x0 + a p; evaluate
+    sdot_status line_func(double a, double *f, double *gp)
+    {
+        k_axpy_launch(c->stream, c->psi.p, c->x0.p, a, c->pdir.p, n);
+        return eval_at(f, gp);
+    }
+};
+
+bool cubic_fit(double x1, double f1, double g1, double x2, double f2, double g2, double *res)
+{
+    const double beta1 = g1 + g2 - 3. * (f1 - f2) / (x1 - x2);
+    const double s = beta1 * beta1 - g1 * g2;
+    if (s < 0) return false;
+    const double beta2 = std::sqrt(s);
+    const double denom = x1 < x2 ? g2 - g1 + 2. * beta2 : g1 - g2 + 2. * beta2;
+    if (denom == 0.) return false;
+    *res = x1 < x2 ? x2 - (x2 - x1) * (g2 + beta2 - beta1) / denom : x1 - (x1 - x2) * (g1 + beta2 - beta1) / denom;
+    return true;
+}
+
+bool quadratic_fit(double x1, double f1, double g1, double x2, double f2, double *res)
+{
+    const double denom = (2. * g1 * x2 - 2. * g1 * x1 - 2. * f2 + 2. * f1);
+    if (denom == 0) return false;
+    *res = (g1 * (x2 * x2 - x1 * x1) + 2. * (f1 - f2) * x1) / denom;
+    return true;
+}
+
+double poly_fit(double x1, double f1, double g1, double x2, double f2, double g2, double b0, double b1)
+{
+    double r;
+    if (cubic_fit(x1, f1, g1, x2, f2, g2, &r) && r >= b0 && r <= b1) return r;
+    if (quadratic_fit(x1, f1, g1, x2, f2, &r) && r >= b0 && r <= b1) return r;
+    return (b0 + b1) * 0.5;
+}
+
+// 0: ok; 1: no bracket; 2: sectioning exhausted; <0: evaluation error (-status)
+int line_search(Solver &S, double f0, double g0, double a1, double eta, double mu, double a_max, unsigned max_evals,
+                double *alpha, sdot_status *err)
+{
+    const double tau1 = 9., tau2 = 0.1, tau3 = 0.5;
+    const double g0_abs = std::fabs(g0);
+    const double f_min = f0 + a_max * mu * g0;
+    auto w1 = [&](double a, double f) { return f <= f0 + a * mu * g0; };
+    auto w2 = [&](double g) { return std::fabs(g) <= eta * g0_abs; };
+    double a_lo = NAN, f_lo = NAN, g_lo = NAN, a_hi = NAN, f_hi = NAN, g_hi = NAN, ai, fi = 0, gi = 0;
+    unsigned i = 0;
+    {
+        double f_prev = f0, g_prev = g0, a_prev = 0;
+        ai = a1;
+        while (i < max_evals) {
+            if ((*err = S.line_func(ai, &fi, &gi)) != SDOT_OK) return -1;
+            ++i;
+            if (fi <= f_min || ai == a_max) { *alpha = ai; return 0; }
+            if (!w1(ai, fi) || (fi >= f_prev && i > 1)) {
+                a_lo = a_prev; f_lo = f_prev; g_lo = g_prev;
+                a_hi = ai; f_hi = fi; g_hi = gi;
+                break;
+            }
+            if (w2(gi)) { *alpha = ai; return 0; }
+            if (gi >= 0) {
+                a_lo = ai; f_lo = fi; g_lo = gi;
+                a_hi = a_prev; f_hi = f_prev; g_hi = g_prev;
+                break;
+            }
+            const double ub = ai + tau1 * (ai - a_prev);
+            a_prev = ai; f_prev = fi; g_prev = gi;
+            ai = std::min(a_max, ub);
+        }
+    }
+    if (!(i < max_evals)) return 1;
+    while (i < max_evals) {
+        const double lo_safe = a_lo + tau2 * (a_hi - a_lo);
+        const double hi_safe = a_hi - tau3 * (a_hi - a_lo);
+        const double b0 = std::min(lo_safe, hi_safe), b1 = std::max(lo_safe, hi_safe);
+        ai = poly_fit(a_lo, f_lo, g_lo, a_hi, f_hi, g_hi, b0, b1);
+        if ((*err = S.line_func(ai, &fi, &gi)) != SDOT_OK) return -1;
+        ++i;
+        if (!w1(ai, fi) || fi >= f_lo) {
+            a_hi = ai; f_hi = fi; g_hi = gi;
+        } else {
+            if (w2(gi)) { *alpha = ai; return 0; }
+            if (gi * (a_hi - a_lo) >= 0) { a_hi = a_lo; f_hi = f_lo; g_hi = g_lo; }
+            a_lo = ai; f_lo = fi; g_lo = gi;
+        }
+    }
+    *alpha = NAN;
+    return 2;
+}
+
+// VerboseSolverControl::check + SolverControl::check: 1 success, 0 iterate, -1 failure
+int control_check(sdot_ctx *c, unsigned step, double *value)
+{
+    const sdot_solver_params &p = c->prm;
+    double v, tol = p.tolerance;
+    if (p.control_type == SDOT_CONTROL_COMPONENTWISE) {
+        v = c->scal_host[SC_COMP];
+        tol = DBL_MIN;
+    } else if (p.control_type == SDOT_CONTROL_LINF) {
+        v = c->scal_host[SC_LINF];
+    } else {
+        v = c->scal_host[SC_L1];
+    }
+    *value = v;
+    if (c->verbose)
+        printf("Iteration %u - L-2 gradient norm: %.6e - check value: %.6e\n", step, std::sqrt(c->scal_host[SC_L2SQ]), v);
+    if (v <= tol) return 1;
+    if (step >= p.max_iterations || std::isnan(v)) return -1;
+    return 0;
+}
+
+}  // namespace
+
+sdot_status sdot_solve(sdot_ctx *c, double *psi, const sdot_solver_params *params, sdot_solve_info *info)
+{
+    if (!c || !psi) return SDOT_EINVAL;
+    if (params) {
+        sdot_status s = sdot_configure(c, params);
+        if (s != SDOT_OK) return s;
+    }
+    DeviceGuard guard(c->device);
+    sdot_status s = prepare_eval(c);
+    if (s != SDOT_OK) return set_error(c, SDOT_ESTATE, "Invalid measures configuration");
+    const int64_t n = c->nt;
+    const int M = 5;  // SolverBFGS::AdditionalData::max_history_size
+    CK(c->x0.alloc(n), "alloc solver");
+    CK(c->pdir.alloc(n), "alloc solver");
+    CK(c->gtmp.alloc(n), "alloc solver");           // g at the start of the line search
+    CK(c->hist_s.alloc((M + 1) * n), "alloc solver");
+    CK(c->hist_y.alloc((M + 1) * n), "alloc solver");
+    CK(c->sk.alloc(8), "alloc solver");             // rho per physical slot (6) + scratch (2)
+    CK(cudaMemsetAsync(c->pdir.p, 0, n * 8, c->stream), "memset");
+
+    // solve() prologue (SotSolver.cc:131-133)
+    double cov = 0.0;
+    if ((s = sdot_compute_covering_radius(c, &cov)) != SDOT_OK) return s;
+    c->covering_radius = cov * 1.1;
+    c->min_target_density = *std::min_element(c->nu_host.begin(), c->nu_host.end());
+    c->have_solve = true;
+
+    Solver S{c, n};
+    S.tol_comp = c->prm.tolerance;
+    CK(cudaMemcpyAsync(c->io_a.p, psi, n * 8, cudaMemcpyHostToDevice, c->stream), "copy psi");
+    if ((s = launch_gather(c, c->psi.p, c->io_a.p, n)) != SDOT_OK) return s;
+
+    double f = 0, gp = 0, check_value = 0;
+    unsigned k = 0;
+    int first_step = 1;
+    double f_prev = 0.;
+    Hist hist{};
+    hist.m = 0;
+    std::vector<int> order;  // physical slots, newest first
+    int spare = 0;
+    std::vector<int> free_slots = {1, 2, 3, 4, 5};
+    double *rho_dev = c->sk.p;
+    double *scratch = c->sk.p + 6;
+    sdot_status result = SDOT_OK;
+    int conv;
+    if ((s = S.eval_at(&f, &gp)) != SDOT_OK) return s;
+    conv = control_check(c, k, &check_value);
+    double host2[2];
+    while (conv == 0) {
+        hist.m = (int)order.size();
+        for (int i = 0; i < hist.m; ++i) hist.slot[i] = order[i];
+        k_two_loop<<<1, 1024, 0, c->stream>>>(n, hist, c->hist_s.p, c->hist_y.p, rho_dev, c->grad.p, c->pdir.p,
+                                               scratch);
+        CK(cudaGetLastError(), "two-loop");
+        CK(cudaMemcpyAsync(c->x0.p, c->psi.p, n * 8, cudaMemcpyDeviceToDevice, c->stream), "copy x0");
+        CK(cudaMemcpyAsync(c->gtmp.p, c->grad.p, n * 8, cudaMemcpyDeviceToDevice, c->stream), "copy g");
+        CK(cudaMemcpyAsync(host2, scratch, 8, cudaMemcpyDeviceToHost, c->stream), "g0 copy");
+        CK(cudaStreamSynchronize(c->stream), "g0 sync");
+        const double g0 = host2[0];
+        // default line search lambda (wasserstein_solver_bfgs.h:316-389)
+        const double f0 = f;
+        double df = f_prev - f;
+        df = std::max(df, 100. * DBL_EPSILON);
+        const double a1 = first_step ? 1. : std::min(1., -1.01 * 2. * df / g0);
+        f_prev = f;
+        double alpha = 0;
+        sdot_status err = SDOT_OK;
+        const int rc = line_search(S, f0, g0, a1, 0.9, 0.001, DBL_MAX, 20, &alpha, &err);
+        f = c->scal_host[SC_VALUE];
+        if (rc < 0) { result = err; break; }
+        if (rc == 1) {
+            result = set_error(c, SDOT_ELINESEARCH, "Could not find the initial bracket within the given number of iterations.");
+            break;
+        }
+        if (rc == 2) {
+            if (c->prm.line_search != SDOT_LS_VENDORED) {
+                result = set_error(c, SDOT_ELINESEARCH, "Could not complete the sectioning phase within the given number of iterations.");
+                break;
+            }
+            alpha = 0.5;  // vendored NaN fallback (wasserstein_solver_bfgs.h:371-386)
+            for (int it = 0; it < 5; ++it) {
+                double ff, gg;
+                if ((s = S.line_func(alpha, &ff, &gg)) != SDOT_OK) { result = s; break; }
+                f = ff;
+                if (f < f_prev) break;
+                alpha *= 0.5;
+            }
+            if (result != SDOT_OK) break;
+        } else if (first_step) {
+            first_step = 0;
+        }
+        ++k;
+        conv = control_check(c, k, &check_value);
+        if (conv != 0) break;
+        // s_k = x - x0, y_k = g - g0 into the spare slot; keep it iff curvature > 0
+        k_sy<<<1, 1024, 0, c->stream>>>(n, c->psi.p, c->x0.p, c->grad.p, c->gtmp.p, c->hist_s.p + (int64_t)spare * n,
+                                        c->hist_y.p + (int64_t)spare * n, scratch);
+        CK(cudaGetLastError(), "sy");
+        CK(cudaMemcpyAsync(host2, scratch, 8, cudaMemcpyDeviceToHost, c->stream), "curv copy");
+        CK(cudaStreamSynchronize(c->stream), "curv sync");
+        const double curvature = host2[0];
+        if (curvature > 0.) {
+            const double r = 1. / curvature;
+            CK(cudaMemcpyAsync(rho_dev + spare, &r, 8, cudaMemcpyHostToDevice, c->stream), "rho");
+            CK(cudaStreamSynchronize(c->stream), "rho sync");
+            order.insert(order.begin(), spare);
+            if ((int)order.size() > M) {
+                spare = order.back();
+                order.pop_back();
+            } else {
+                spare = free_slots.back();
+                free_slots.pop_back();
+            }
+        }
+    }
+    c->last_iterations = k;
+    c->last_converged = (conv == 1);
+    // psi back to the caller (also after a failure: the reference updates in place)
+    sdot_status s2 = launch_scatter(c, c->io_b.p, c->psi.p, n);
+    if (s2 == SDOT_OK) {
+        cudaError_t e = cudaMemcpyAsync(psi, c->io_b.p, n * 8, cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) s2 = cuda_error(c, e, "copy psi");
+    }
+    if (info) {
+        info->iterations = k;
+        info->converged = (conv == 1);
+        info->n_evaluations = S.evals;
+        info->last_value = f;
+        info->last_check_value = check_value;
+        info->total_pairs = S.pairs;
+        info->device_ms = S.total_ms;
+    }
+    if (result != SDOT_OK) return result;
+    return s2;
+}
+
+double sdot_get_last_functional_value(const sdot_ctx *c) { return c ? c->global_functional : NAN; }
+unsigned sdot_get_last_iteration_count(const sdot_ctx *c) { return c ? c->last_iterations : 0; }
+int sdot_get_convergence_status(const sdot_ctx *c) { return c ? c->last_converged : 0; }
+double sdot_get_last_distance_threshold(const sdot_ctx *c) { return c ? c->current_distance_threshold : NAN; }
+double sdot_get_C_global(const sdot_ctx *c) { return c ? c->C_global : NAN; }
+
+sdot_status sdot_set_distance_threshold(sdot_ctx *c, double threshold)
+{
+    if (!c) return SDOT_EINVAL;
+    c->current_distance_threshold = threshold;
+    return SDOT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,1103 @@
+// sdot_eval.cu -- evaluation of the entropic semi-discrete dual functional
+// and its gradient on B200 (sm_100a).
+//
+// Replaces SotSolver::evaluate_functional / local_assemble / the value-grad
+// lambda / find_nearest_target_points (src/solvers/SotSolver.cc:217-377,
+// 769-869, 267-296, 553-570).  One evaluation is two sweeps over the
+// (quadrature point, target) pairs plus two small reductions:
+//
+//   value sweep  (source-centric): per q the reference's max exponent m_q and
+//     shifted sum S_q, accumulated online in FP64 with a hand-written exp2
+//     (sdot_device.cuh) -> L_q = m_q + log S_q, value and C_global partials.
+//   gradient sweep (target-centric, pull): g_j = sum_q w_q nu_j e^{t_qj - L_q}
+//     accumulated per target without atomics; exponentials in FP32 ex2 with
+//     FP64 accumulation (HYBRID/MIXED) or FP64 (FP64 precision).
+//
+// Truncation: a (cell, target) pair is a candidate iff
+// sqrt_rn(d2(y_j, c_K)) <= r, evaluated as d2 <= s* where s* is the largest
+// double with sqrt_rn(s*) <= r (sqrt_rn is monotone, so the two tests are
+// identical); d2 is rounded exactly like the reference.  Both sweeps apply
+// the same test, after a conservative bounding-sphere cull of whole blocks.
+#include <float.h>
+#include <math.h>
+#include <stdio.h>
+
+#include <algorithm>
+#include <cmath>
+
+#include "sdot_device.cuh"
+#include "sdot_internal.h"
+
+namespace sdot {
+
+// ---------------------------------------------------------------------------
+// small kernels
+// ---------------------------------------------------------------------------
+
+__global__ void k_gather(double *dst, const double *src, const int64_t *perm, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        dst[i] = src[perm[i]];
+}
+
+__global__ void k_scatter(double *dst, const double *src, const int64_t *perm, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        dst[perm[i]] = src[i];
+}
+
+__global__ void k_axpy(double *x, const double *x0, double a, const double *p, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        x[i] = x0[i] + a * p[i];
+}
+
+// max/min/non-finite flag of a vector: out[0]=max, out[1]=min, out[2]=1 if non-finite.
+__global__ void k_minmax(const double *v, int64_t n, double *out)
+{
+    __shared__ double smx[32], smn[32];
+    __shared__ int sbad[32];
+    double mx = -DBL_MAX, mn = DBL_MAX;
+    int bad = 0;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const double a = v[i];
+        if (!isfinite(a)) bad = 1;
+        mx = a > mx ? a : mx;
+        mn = a < mn ? a : mn;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+        bad |= __shfl_xor_sync(0xffffffffu, bad, o);
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) { smx[w] = mx; smn[w] = mn; sbad[w] = bad; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int i = 1; i < (int)(blockDim.x >> 5); ++i) {
+            mx = fmax(mx, smx[i]);
+            mn = fmin(mn, smn[i]);
+            bad |= sbad[i];
+        }
+        out[0] = mx;
+        out[1] = mn;
+        out[2] = bad;
+    }
+}
+
+// tpack[j] = {A_j, B_j(DIM), nu_j, y_j(DIM)}: scaled exponent coefficients.
+template <int DIM>
+__global__ void k_target_prep(int64_t nt, const double *__restrict__ y, const double *__restrict__ nu,
+                              const double *__restrict__ psi, EvalArgs a, double *__restrict__ tpack)
+{
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nt; j += (int64_t)gridDim.x * blockDim.x) {
+        double yt[3], ysq = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            yt[d] = y[j * DIM + d] - a.o[d];
+            ysq += yt[d] * yt[d];
+        }
+        double *t = tpack + j * TPACK;
+        t[0] = a.s * psi[j] - a.halfs * ysq;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) t[1 + d] = a.s * yt[d];
+        t[1 + DIM] = nu[j];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) t[2 + DIM + d] = y[j * DIM + d];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// per-q epilogue of the value sweep (SotSolver.cc:843-866 + lambda :274-286)
+// ---------------------------------------------------------------------------
+
+// mx: max scaled exponent (without C_q); S: sum relative to mx.
+__device__ __forceinline__ void value_epilogue(const EvalArgs &a, double mx, double S, double Cq,
+                                               double rho, double jxw, double &val, double &cval,
+                                               double &L, int &skipped)
+{
+    val = 0.0;
+    cval = 0.0;
+    L = CUDART_INF;
+    skipped = 1;
+    if (mx == -CUDART_INF) return;           // no candidates: cell skipped (:802)
+    const double m_ref = (mx + Cq) * (1.0 / KAPPA);
+    if (a.lse) {
+        if (!(S > 0.0)) return;              // total_sum_exp <= 0 (:846)
+        const double lt = m_ref + log(S);
+        val = rho * a.eps * lt * jxw;
+        cval = rho * jxw / S;
+        L = lt;
+    } else {
+        const double total = S * exp(m_ref);  // sum of unshifted terms
+        if (!(total > 0.0)) return;
+        const double lt = log(total);
+        val = rho * a.eps * lt * jxw;
+        cval = rho * jxw / total;
+        L = lt;
+    }
+    skipped = 0;
+}
+
+// One online-LSE update in scaled units (b relative to the unit's C_q).
+__device__ __forceinline__ void lse_update(double b, double nu, double &M, double &S, double &mx,
+                                           const double *tab)
+{
+    mx = fmax(mx, b);
+    double u = b - M;
+    if (u > LSE_THR) {
+        S = S * exp2_16(M - b, tab);
+        M = b;
+        u = 0.0;
+    }
+    S = fma(nu, exp2_16(u, tab), S);
+}
+
+// Block-level ordered sum of (value, C, skipped, pairs) -> part[blockIdx.x*4..].
+__device__ __forceinline__ void block_partials(double v, double c, double sk, double np, double *part)
+{
+    __shared__ double sv[32], sc[32], ss[32], sp[32];
+    v = warp_sum(v);
+    c = warp_sum(c);
+    sk = warp_sum(sk);
+    np = warp_sum(np);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) { sv[w] = v; sc[w] = c; ss[w] = sk; sp[w] = np; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tv = 0.0, tc = 0.0, ts = 0.0, tp = 0.0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) { tv += sv[i]; tc += sc[i]; ts += ss[i]; tp += sp[i]; }
+        part[blockIdx.x * 4 + 0] = tv;
+        part[blockIdx.x * 4 + 1] = tc;
+        part[blockIdx.x * 4 + 2] = ts;
+        part[blockIdx.x * 4 + 3] = tp;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// value sweep, dense: thread <-> DENSE_A_QT quadrature points, all targets
+// streamed through shared memory (broadcast reads).
+// ---------------------------------------------------------------------------
+
+constexpr int DA_CHUNK = 256;
+
+template <int DIM>
+__global__ void __launch_bounds__(DENSE_A_THREADS)
+k_value_dense(const double *__restrict__ x, const double *__restrict__ rho, const double *__restrict__ jxw,
+              const double *__restrict__ tpack, EvalArgs a, double *__restrict__ Lq, double *__restrict__ part)
+{
+    constexpr int QT = DENSE_A_QT;
+    constexpr int TS = DIM + 2;  // A, B(DIM), nu
+    __shared__ double tab[16];
+    __shared__ double stg[DA_CHUNK * TS];
+    if (threadIdx.x < 16) tab[threadIdx.x] = c_exp2_tab[threadIdx.x];
+
+    const int64_t qbase = (int64_t)blockIdx.x * (DENSE_A_THREADS * QT) + threadIdx.x;
+    double xt[QT][DIM], M[QT], S[QT], mx[QT];
+#pragma unroll
+    for (int k = 0; k < QT; ++k) {
+        const int64_t q = qbase + (int64_t)k * DENSE_A_THREADS;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) xt[k][d] = (q < a.nq) ? x[q * DIM + d] - a.o[d] : 0.0;
+        M[k] = -CUDART_INF;
+        S[k] = 0.0;
+        mx[k] = -CUDART_INF;
+    }
+    for (int64_t c0 = 0; c0 < a.nt; c0 += DA_CHUNK) {
+        const int cn = (int)min((int64_t)DA_CHUNK, a.nt - c0);
+        __syncthreads();
+        for (int i = threadIdx.x; i < cn * TS; i += DENSE_A_THREADS) {
+            const int t = i / TS, f = i - t * TS;
+            stg[i] = tpack[(c0 + t) * TPACK + f];
+        }
+        __syncthreads();
+#pragma unroll 2
+        for (int t = 0; t < cn; ++t) {
+            const double *tp = stg + t * TS;
+            const double A = tp[0];
+            double B[DIM];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) B[d] = tp[1 + d];
+            const double nuj = tp[1 + DIM];
+#pragma unroll
+            for (int k = 0; k < QT; ++k) {
+                double b = fma(B[0], xt[k][0], A);
+#pragma unroll
+                for (int d = 1; d < DIM; ++d) b = fma(B[d], xt[k][d], b);
+                lse_update(b, nuj, M[k], S[k], mx[k], tab);
+            }
+        }
+    }
+    double tv = 0.0, tc = 0.0, ts = 0.0;
+#pragma unroll
+    for (int k = 0; k < QT; ++k) {
+        const int64_t q = qbase + (int64_t)k * DENSE_A_THREADS;
+        if (q < a.nq) {
+            double xsq = 0.0;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) xsq += xt[k][d] * xt[k][d];
+            const double Cq = -a.halfs * xsq;
+            const double Sref = (mx[k] == -CUDART_INF) ? 0.0 : S[k] * exp2_16(M[k] - mx[k], tab);
+            double v, cv, L;
+            int sk;
+            value_epilogue(a, mx[k], Sref, Cq, rho[q], jxw[q], v, cv, L, sk);
+            Lq[q] = L;
+            tv += v;
+            tc += cv;
+            ts += sk;
+        }
+    }
+    block_partials(tv, tc, ts, 0.0, part);
+}
+
+// ---------------------------------------------------------------------------
+// value sweep, truncated: CTA <-> 8 warp units (cell, q-group); candidate
+// target blocks culled by bounding spheres and staged in shared memory; each
+// warp applies the exact per-cell test, compacts its candidates in order and
+// walks them with lane <-> target, every lane holding all q of its unit.
+// ---------------------------------------------------------------------------
+
+constexpr int VT_WARPS = 8;
+constexpr int VT_MAXTB = 16;                 // target blocks staged per round
+constexpr int VT_STG = VT_MAXTB * TBLK;      // staged targets per round (1024)
+
+struct VTSmem {
+    double tab[16];
+    double stg[VT_STG * TPACK];
+    double xw[VT_WARPS][9][4];
+    unsigned short cand[VT_WARPS][VT_STG];
+    int tblist[VT_MAXTB];
+    int wcount[VT_WARPS];
+    int ctl[4];
+};
+
+// Deterministic block-wide compaction of the blocks that pass the sphere
+// cull, continuing from *next; at most cap entries.  Returns the count.
+__device__ __forceinline__ int cull_blocks(const double *sph, int64_t nblk, const double *c, double R,
+                                           double cullr, int *list, int cap, int64_t &next, int *wcount,
+                                           int *ctl)
+{
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int nw = blockDim.x >> 5;
+    int cnt = 0;
+    while (next < nblk && cnt < cap) {
+        const int64_t idx = next + tid;
+        bool flag = false;
+        if (idx < nblk) {
+            const double *s = sph + idx * 4;
+            const double d0 = s[0] - c[0], d1 = s[1] - c[1], d2 = s[2] - c[2];
+            const double d = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+            const double lim = (cullr + R + s[3]) * (1.0 + 1e-12) + 1e-300;
+            flag = (d <= lim) || !(d == d);
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, flag);
+        if (lane == 0) wcount[w] = __popc(bal);
+        __syncthreads();
+        int off = cnt, tot = 0;
+        for (int i = 0; i < nw; ++i) {
+            if (i < w) off += wcount[i];
+            tot += wcount[i];
+        }
+        const int pos = off + __popc(bal & ((1u << lane) - 1u));
+        if (flag && pos < cap) list[pos] = (int)idx;
+        if (flag && pos == cap) ctl[0] = (int)(idx);
+        __syncthreads();
+        if (cnt + tot > cap) {
+            next = ctl[0];
+            cnt = cap;
+        } else {
+            cnt += tot;
+            next += blockDim.x;
+        }
+        __syncthreads();
+    }
+    return cnt;
+}
+
+template <int DIM, int QL>
+__global__ void __launch_bounds__(VT_WARPS * 32)
+k_value_trunc(const double *__restrict__ x, const double *__restrict__ rho, const double *__restrict__ jxw,
+              const double *__restrict__ cell_ctr, const double *__restrict__ sblk_sph,
+              const double *__restrict__ tpack, const double *__restrict__ tblk_sph, int64_t ntblk,
+              EvalArgs a, double *__restrict__ Lq, double *__restrict__ part)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    VTSmem &sm = *reinterpret_cast<VTSmem *>(smem_raw);
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    if (tid < 16) sm.tab[tid] = c_exp2_tab[tid];
+
+    const int64_t unit = (int64_t)blockIdx.x * VT_WARPS + w;
+    const bool valid = unit < a.nunits;
+    const int64_t cell = valid ? unit / a.ngroups : 0;
+    const int grp = valid ? (int)(unit - cell * a.ngroups) : 0;
+    const int64_t q0 = cell * a.qpc + (int64_t)grp * a.ql;
+    const int nql = valid ? min(a.ql, a.qpc - grp * a.ql) : 0;
+    double cc[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) cc[d] = cell_ctr[cell * DIM + d];
+    if (lane < QL) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            sm.xw[w][lane][d] = (lane < nql && d < DIM) ? x[(q0 + lane) * DIM + d] - a.o[d] : 0.0;
+    }
+    const double *bs = sblk_sph + (int64_t)blockIdx.x * 4;
+    const double bc[3] = {bs[0], bs[1], bs[2]};
+    const double bR = bs[3];
+
+    double M[QL], S[QL], mx[QL];
+#pragma unroll
+    for (int k = 0; k < QL; ++k) { M[k] = -CUDART_INF; S[k] = 0.0; mx[k] = -CUDART_INF; }
+
+    int64_t next = 0;
+    double npairs = 0.0;
+    while (true) {
+        const int ntb = cull_blocks(tblk_sph, ntblk, bc, bR, a.cull, sm.tblist, VT_MAXTB, next, sm.wcount,
+                                    sm.ctl);
+        if (ntb == 0) break;
+        // stage the targets of the listed blocks
+        int nstg = 0;
+        for (int b = 0; b < ntb; ++b) {
+            const int64_t t0 = (int64_t)sm.tblist[b] * TBLK;
+            const int tn = (int)min((int64_t)TBLK, a.nt - t0);
+            const double *src = tpack + t0 * TPACK;
+            double *dst = sm.stg + (int64_t)nstg * TPACK;
+            for (int i = tid; i < tn * TPACK; i += blockDim.x) dst[i] = src[i];
+            nstg += tn;
+        }
+        __syncthreads();
+        // exact per-cell candidate test + in-order compaction (one warp per unit)
+        int ncand = 0;
+        if (valid) {
+            for (int b0 = 0; b0 < nstg; b0 += 32) {
+                const int t = b0 + lane;
+                bool in = false;
+                if (t < nstg) in = dist2_exact<DIM>(sm.stg + t * TPACK + 2 + DIM, cc) <= a.sstar;
+                const unsigned bal = __ballot_sync(0xffffffffu, in);
+                if (in) sm.cand[w][ncand + __popc(bal & ((1u << lane) - 1u))] = (unsigned short)t;
+                ncand += __popc(bal);
+            }
+            __syncwarp();
+            npairs += (double)ncand * nql;
+            for (int p = lane; p < ncand; p += 32) {
+                const double *tp = sm.stg + sm.cand[w][p] * TPACK;
+                const double A = tp[0];
+                double B[DIM];
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) B[d] = tp[1 + d];
+                const double nuj = tp[1 + DIM];
+#pragma unroll
+                for (int k = 0; k < QL; ++k) {
+                    if (k < nql) {
+                        double b = fma(B[0], sm.xw[w][k][0], A);
+#pragma unroll
+                        for (int d = 1; d < DIM; ++d) b = fma(B[d], sm.xw[w][k][d], b);
+                        lse_update(b, nuj, M[k], S[k], mx[k], sm.tab);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+    // merge the lanes of each unit, then per-q epilogue on lane k
+    double tv = 0.0, tc = 0.0, ts = 0.0;
+#pragma unroll
+    for (int k = 0; k < QL; ++k) {
+        const double mxw = warp_max(mx[k]);
+        const double sl = (M[k] == -CUDART_INF || mxw == -CUDART_INF) ? 0.0 : S[k] * exp2_16(M[k] - mxw, sm.tab);
+        const double Sw = warp_sum(sl);
+        if (valid && k < nql && lane == 0) {
+            const int64_t q = q0 + k;
+            double xsq = 0.0;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) xsq += sm.xw[w][k][d] * sm.xw[w][k][d];
+            const double Cq = -a.halfs * xsq;
+            double v, cv, L;
+            int sk;
+            value_epilogue(a, mxw, Sw, Cq, rho[q], jxw[q], v, cv, L, sk);
+            Lq[q] = L;
+            tv += v;
+            tc += cv;
+            ts += sk;
+        }
+    }
+    block_partials(tv, tc, ts, lane == 0 ? npairs : 0.0, part);
+}
+
+// ---------------------------------------------------------------------------
+// gradient sweep, dense: thread <-> DENSE_B_TT targets, q-slices streamed
+// through shared memory (broadcast reads); FP64 partial per (slice, target).
+// ---------------------------------------------------------------------------
+
+constexpr int DB_CHUNK = 256;
+
+template <int DIM, bool FP32>
+__global__ void __launch_bounds__(DENSE_B_THREADS)
+k_grad_dense(const double *__restrict__ x, const double *__restrict__ w, const double *__restrict__ Lq,
+             const double *__restrict__ tpack, const double *__restrict__ psi, EvalArgs a, int64_t qslice,
+             double *__restrict__ gpart)
+{
+    constexpr int TT = DENSE_B_TT;
+    constexpr int TB = DENSE_B_THREADS * TT;
+    __shared__ double tab[16];
+    __shared__ double red[2][32];
+    __shared__ __align__(16) double stgd[FP32 ? 1 : DB_CHUNK * (DIM + 2)];
+    __shared__ __align__(16) float stgf[FP32 ? DB_CHUNK * 4 : 1];
+    __shared__ float stgw[FP32 ? DB_CHUNK : 1];
+    if (threadIdx.x < 16) tab[threadIdx.x] = c_exp2_tab[threadIdx.x];
+    const int tid = threadIdx.x;
+    const int64_t j0 = (int64_t)blockIdx.x * TB;
+    const int64_t qa = (int64_t)blockIdx.y * qslice;
+    const int64_t qb = min(a.nq, qa + qslice);
+
+    // per-target data and the block centring (FP32 path)
+    double ob[3] = {0.0, 0.0, 0.0};
+    double aref = 0.0;
+    float yt[TT][3], alpha[TT];
+    double A[TT], B[TT][3], acc64[TT];
+    bool has[TT];
+    if (FP32) {
+        double lo[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, hi[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+        double amax = -DBL_MAX;
+#pragma unroll
+        for (int k = 0; k < TT; ++k) {
+            const int64_t j = j0 + tid + k * DENSE_B_THREADS;
+            if (j < a.nt) {
+                const double *tp = tpack + j * TPACK;
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) {
+                    lo[d] = fmin(lo[d], tp[2 + DIM + d]);
+                    hi[d] = fmax(hi[d], tp[2 + DIM + d]);
+                }
+                const double al = log2(tp[1 + DIM]) + a.l2e_eps * psi[j];
+                if (al > amax) amax = al;
+            }
+        }
+        // block reductions (lo/hi/amax) through shared memory
+        __shared__ double sred[7][DENSE_B_THREADS / 32];
+        for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                lo[d] = fmin(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
+                hi[d] = fmax(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+            }
+            amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+        }
+        if ((tid & 31) == 0) {
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) { sred[d][tid >> 5] = lo[d]; sred[3 + d][tid >> 5] = hi[d]; }
+            sred[6][tid >> 5] = amax;
+        }
+        __syncthreads();
+        for (int i = 0; i < DENSE_B_THREADS / 32; ++i) {
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) { lo[d] = fmin(lo[d], sred[d][i]); hi[d] = fmax(hi[d], sred[3 + d][i]); }
+            amax = fmax(amax, sred[6][i]);
+        }
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) ob[d] = 0.5 * (lo[d] + hi[d]);
+        aref = (amax > -DBL_MAX && isfinite(amax)) ? amax : 0.0;
+    }
+#pragma unroll
+    for (int k = 0; k < TT; ++k) {
+        const int64_t j = j0 + tid + k * DENSE_B_THREADS;
+        has[k] = j < a.nt;
+        acc64[k] = 0.0;
+        const double *tp = tpack + (has[k] ? j : 0) * TPACK;
+        if (FP32) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) yt[k][d] = (d < DIM && has[k]) ? (float)(tp[2 + DIM + d] - ob[d]) : 0.f;
+            alpha[k] = has[k] ? (float)(log2(tp[1 + DIM]) + a.l2e_eps * psi[j] - aref) : -INFINITY;
+        } else {
+            A[k] = tp[0];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) B[k][d] = tp[1 + d];
+        }
+    }
+    const float c32 = (float)a.c32;
+    for (int64_t c0 = qa; c0 < qb; c0 += DB_CHUNK) {
+        const int cn = (int)min((int64_t)DB_CHUNK, qb - c0);
+        __syncthreads();
+        for (int i = tid; i < cn; i += DENSE_B_THREADS) {
+            const int64_t q = c0 + i;
+            double xt[3];
+            double xsq = 0.0;
+            if (FP32) {
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) xt[d] = x[q * DIM + d] - ob[d];
+                const double beta = -LOG2E * Lq[q] + aref;
+                float4 v;
+                v.x = (float)xt[0];
+                v.y = (float)xt[1];
+                v.z = DIM == 3 ? (float)xt[2] : (float)beta;
+                v.w = DIM == 3 ? (float)beta : 0.f;
+                reinterpret_cast<float4 *>(stgf)[i] = v;
+                stgw[i] = (float)w[q];
+            } else {
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) {
+                    xt[d] = x[q * DIM + d] - a.o[d];
+                    xsq += xt[d] * xt[d];
+                    stgd[i * (DIM + 2) + d] = xt[d];
+                }
+                stgd[i * (DIM + 2) + DIM] = -a.halfs * xsq - KAPPA * Lq[q];
+                stgd[i * (DIM + 2) + DIM + 1] = w[q];
+            }
+        }
+        __syncthreads();
+        if (FP32) {
+            float acc[TT];
+#pragma unroll
+            for (int k = 0; k < TT; ++k) acc[k] = 0.f;
+            int t = 0;
+            for (; t < cn; ++t) {
+                const float4 v = reinterpret_cast<const float4 *>(stgf)[t];
+                const float beta = DIM == 3 ? v.w : v.z;
+                const float wq = stgw[t];
+#pragma unroll
+                for (int k = 0; k < TT; ++k) {
+                    const float d0 = v.x - yt[k][0], d1 = v.y - yt[k][1];
+                    float d2 = d0 * d0;
+                    d2 = fmaf(d1, d1, d2);
+                    if (DIM == 3) {
+                        const float dz = v.z - yt[k][2];
+                        d2 = fmaf(dz, dz, d2);
+                    }
+                    const float e = fmaf(-c32, d2, alpha[k] + beta);
+                    acc[k] = fmaf(wq, ex2_approx(e), acc[k]);
+                }
+                if ((t & 7) == 7) {
+#pragma unroll
+                    for (int k = 0; k < TT; ++k) { acc64[k] += (double)acc[k]; acc[k] = 0.f; }
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < TT; ++k) acc64[k] += (double)acc[k];
+        } else {
+            for (int t = 0; t < cn; ++t) {
+                const double *v = stgd + t * (DIM + 2);
+                const double D = v[DIM], wq = v[DIM + 1];
+#pragma unroll
+                for (int k = 0; k < TT; ++k) {
+                    double u = fma(B[k][0], v[0], A[k] + D);
+#pragma unroll
+                    for (int d = 1; d < DIM; ++d) u = fma(B[k][d], v[d], u);
+                    acc64[k] = fma(wq, exp2_16(u, tab), acc64[k]);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < TT; ++k) {
+        const int64_t j = j0 + tid + k * DENSE_B_THREADS;
+        if (j < a.nt) {
+            double g = acc64[k];
+            if (!FP32) g *= tpack[j * TPACK + 1 + DIM];  // nu_j (FP32 path folds it into alpha)
+            gpart[(int64_t)blockIdx.y * a.nt + j] = g;
+        }
+    }
+    (void)red;
+}
+
+// ---------------------------------------------------------------------------
+// gradient sweep, truncated: CTA <-> target block (TBLK targets, 8 warps x 8
+// targets); candidate cell blocks culled by spheres and staged; each warp
+// compacts the exact candidate cells of its target and walks the flattened
+// (cell, q) pairs with all 32 lanes.
+// ---------------------------------------------------------------------------
+
+constexpr int GT_WARPS = 8;
+constexpr int GT_TPW = TBLK / GT_WARPS;   // targets per warp
+constexpr int GT_MAXQ = 4096;             // staged quadrature points per round (FP32 data)
+constexpr int GT_MAXQ64 = 2048;           // staged quadrature points per round (FP64 data)
+constexpr int GT_MAXCELL = 512;           // staged cells per round
+
+struct GTSmem {
+    double tab[16];
+    double cctr[GT_MAXCELL * 3];
+    double acc[GT_WARPS][GT_TPW][32];     // per-lane FP64 accumulators, persist across rounds
+    int cblist[GT_MAXCELL / SBLK_CELLS];
+    unsigned short cand[GT_WARPS][GT_MAXCELL];
+    int wcount[GT_WARPS];
+    int ctl[4];
+    double red[GT_WARPS];
+    // followed by the staged quadrature data (float4 + float, or 5 doubles)
+};
+
+template <int DIM, bool FP32>
+__global__ void __launch_bounds__(GT_WARPS * 32)
+k_grad_trunc(const double *__restrict__ x, const double *__restrict__ w, const double *__restrict__ Lq,
+             const double *__restrict__ cell_ctr, const double *__restrict__ cblk_sph, int64_t ncblk,
+             const double *__restrict__ tpack, const double *__restrict__ psi, const double *__restrict__ tblk_sph,
+             EvalArgs a, int maxcb, double *__restrict__ gacc)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    GTSmem &sm = *reinterpret_cast<GTSmem *>(smem_raw);
+    unsigned char *qraw = smem_raw + ((sizeof(GTSmem) + 15) & ~size_t(15));
+    float4 *qf = reinterpret_cast<float4 *>(qraw);
+    float *qw = reinterpret_cast<float *>(qraw + sizeof(float4) * GT_MAXQ);
+    double *qd = reinterpret_cast<double *>(qraw);
+
+    const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
+    if (tid < 16) sm.tab[tid] = c_exp2_tab[tid];
+    for (int i = tid; i < GT_WARPS * GT_TPW * 32; i += blockDim.x) (&sm.acc[0][0][0])[i] = 0.0;
+    const int64_t j0 = (int64_t)blockIdx.x * TBLK;
+    const double *bs = tblk_sph + (int64_t)blockIdx.x * 4;
+    const double bc[3] = {bs[0], bs[1], bs[2]};
+    const double bR = bs[3];
+    const int qpc = a.qpc;
+    const unsigned qmagic = (unsigned)((0x100000000ull + qpc - 1) / qpc);
+
+    // alpha reference of the block (FP32 path): max over the block
+    double aref = 0.0;
+    if (FP32) {
+        double am = -DBL_MAX;
+        for (int i = tid; i < TBLK; i += blockDim.x) {
+            const int64_t j = j0 + i;
+            if (j < a.nt) {
+                const double al = log2(tpack[j * TPACK + 1 + DIM]) + a.l2e_eps * psi[j];
+                if (al > am) am = al;
+            }
+        }
+        am = warp_max(am);
+        if (lane == 0) sm.red[wp] = am;
+        __syncthreads();
+        for (int i = 0; i < GT_WARPS; ++i) am = fmax(am, sm.red[i]);
+        aref = (am > -DBL_MAX && isfinite(am)) ? am : 0.0;
+    }
+    const float c32 = (float)a.c32;
+    int64_t next = 0;
+    while (true) {
+        const int ncb = cull_blocks(cblk_sph, ncblk, bc, bR, a.cull, sm.cblist, maxcb, next, sm.wcount, sm.ctl);
+        if (ncb == 0) break;
+        // stage cells (centres) and their quadrature data
+        int nst = 0;
+        for (int b = 0; b < ncb; ++b) {
+            const int64_t cb0 = (int64_t)sm.cblist[b] * SBLK_CELLS;
+            const int cn = (int)min((int64_t)SBLK_CELLS, a.ncells - cb0);
+            for (int i = tid; i < cn * DIM; i += blockDim.x) {
+                const int ci = i / DIM, d = i - ci * DIM;
+                sm.cctr[(nst + ci) * 3 + d] = cell_ctr[(cb0 + ci) * DIM + d];
+            }
+            for (int i = tid; i < cn * qpc; i += blockDim.x) {
+                const int64_t q = cb0 * qpc + i;
+                const int slot = nst * qpc + i;
+                if (FP32) {
+                    double xt[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) xt[d] = x[q * DIM + d] - bc[d];
+                    const double beta = -LOG2E * Lq[q] + aref;
+                    float4 v;
+                    v.x = (float)xt[0];
+                    v.y = (float)xt[1];
+                    v.z = DIM == 3 ? (float)xt[2] : (float)beta;
+                    v.w = DIM == 3 ? (float)beta : 0.f;
+                    qf[slot] = v;
+                    qw[slot] = (float)w[q];
+                } else {
+                    double xsq = 0.0;
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) {
+                        const double xt = x[q * DIM + d] - a.o[d];
+                        qd[slot * 5 + d] = xt;
+                        xsq += xt * xt;
+                    }
+                    qd[slot * 5 + 3] = -a.halfs * xsq - KAPPA * Lq[q];
+                    qd[slot * 5 + 4] = w[q];
+                }
+            }
+            nst += cn;
+        }
+        __syncthreads();
+        for (int i = 0; i < GT_TPW; ++i) {
+            const int64_t j = j0 + wp * GT_TPW + i;
+            if (j >= a.nt) break;
+            const double *tp = tpack + j * TPACK;
+            double yj[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) yj[d] = tp[2 + DIM + d];
+            // exact candidate test of every staged cell for target j, in order
+            int ncand = 0;
+            for (int c0 = 0; c0 < nst; c0 += 32) {
+                const int c = c0 + lane;
+                bool in = false;
+                if (c < nst) in = dist2_exact<DIM>(yj, sm.cctr + c * 3) <= a.sstar;
+                const unsigned bal = __ballot_sync(0xffffffffu, in);
+                if (in) sm.cand[wp][ncand + __popc(bal & ((1u << lane) - 1u))] = (unsigned short)c;
+                ncand += __popc(bal);
+            }
+            __syncwarp();
+            const int npair = ncand * qpc;
+            double a64 = 0.0;
+            if (FP32) {
+                const float ty0 = (float)(yj[0] - bc[0]), ty1 = (float)(yj[1] - bc[1]);
+                const float ty2 = DIM == 3 ? (float)(yj[2] - bc[2]) : 0.f;
+                const float al = (float)(log2(tp[1 + DIM]) + a.l2e_eps * psi[j] - aref);
+                float acc = 0.f;
+                int it = 0;
+                for (int p = lane; p < npair; p += 32, ++it) {
+                    const unsigned ci = fast_div((unsigned)p, qmagic);
+                    const int slot = sm.cand[wp][ci] * qpc + (p - (int)ci * qpc);
+                    const float4 v = qf[slot];
+                    const float beta = DIM == 3 ? v.w : v.z;
+                    const float d0 = v.x - ty0, d1 = v.y - ty1;
+                    float d2 = d0 * d0;
+                    d2 = fmaf(d1, d1, d2);
+                    if (DIM == 3) {
+                        const float dz = v.z - ty2;
+                        d2 = fmaf(dz, dz, d2);
+                    }
+                    const float e = fmaf(-c32, d2, al + beta);
+                    acc = fmaf(qw[slot], ex2_approx(e), acc);
+                    if ((it & 7) == 7) { a64 += (double)acc; acc = 0.f; }
+                }
+                a64 += (double)acc;
+            } else {
+                const double A = tp[0], B0 = tp[1], B1 = tp[2], B2 = DIM == 3 ? tp[3] : 0.0;
+                for (int p = lane; p < npair; p += 32) {
+                    const unsigned ci = fast_div((unsigned)p, qmagic);
+                    const int slot = sm.cand[wp][ci] * qpc + (p - (int)ci * qpc);
+                    const double *v = qd + slot * 5;
+                    double u = fma(B0, v[0], A + v[3]);
+                    u = fma(B1, v[1], u);
+                    if (DIM == 3) u = fma(B2, v[2], u);
+                    a64 = fma(v[4], exp2_16(u, sm.tab), a64);
+                }
+            }
+            sm.acc[wp][i][lane] += a64;
+            __syncwarp();
+        }
+        __syncthreads();
+    }
+    for (int i = 0; i < GT_TPW; ++i) {
+        const int64_t j = j0 + wp * GT_TPW + i;
+        const double g = warp_sum(sm.acc[wp][i][lane]);
+        if (lane == 0 && j < a.nt) gacc[j] = FP32 ? g : g * tpack[j * TPACK + 1 + DIM];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// finalize: g_j = sum of partials - nu_j, plus the reductions the solver and
+// the solver control need (SotSolver.cc:322-327, SotSolver.h:391-442).
+// ---------------------------------------------------------------------------
+
+constexpr int FIN_THREADS = 256;
+constexpr int FIN_BLOCKS = 148;
+constexpr int NRED = 8;  // psinu, l1, linf, comp, l2sq, gp, nonfinite, unused
+
+__global__ void __launch_bounds__(FIN_THREADS)
+k_finalize_grad(int64_t nt, int nks, const double *__restrict__ gpart, const double *__restrict__ nu,
+                const double *__restrict__ psi, const double *__restrict__ pdir, double tol,
+                double *__restrict__ grad, double *__restrict__ redpart)
+{
+    double psinu = 0.0, l1 = 0.0, linf = 0.0, comp = -CUDART_INF, l2 = 0.0, gp = 0.0, bad = 0.0;
+    for (int64_t j = blockIdx.x * (int64_t)FIN_THREADS + threadIdx.x; j < nt; j += (int64_t)gridDim.x * FIN_THREADS) {
+        double s = 0.0;
+        for (int k = 0; k < nks; ++k) s += gpart[(int64_t)k * nt + j];
+        const double g = s - nu[j];
+        grad[j] = g;
+        psinu += psi[j] * nu[j];
+        const double ag = fabs(g);
+        l1 += ag;
+        linf = fmax(linf, ag);
+        comp = fmax(comp, ag - nu[j] * tol);
+        l2 += g * g;
+        if (pdir) gp += g * pdir[j];
+        if (!isfinite(g) || !isfinite(psi[j])) bad = 1.0;
+    }
+    __shared__ double sh[NRED][FIN_THREADS / 32];
+    psinu = warp_sum(psinu);
+    l1 = warp_sum(l1);
+    linf = warp_max(linf);
+    comp = warp_max(comp);
+    l2 = warp_sum(l2);
+    gp = warp_sum(gp);
+    bad = warp_max(bad);
+    const int wi = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        sh[0][wi] = psinu; sh[1][wi] = l1; sh[2][wi] = linf; sh[3][wi] = comp;
+        sh[4][wi] = l2; sh[5][wi] = gp; sh[6][wi] = bad;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r[7] = {0, 0, 0, -CUDART_INF, 0, 0, 0};
+        for (int i = 0; i < FIN_THREADS / 32; ++i) {
+            r[0] += sh[0][i]; r[1] += sh[1][i]; r[2] = fmax(r[2], sh[2][i]); r[3] = fmax(r[3], sh[3][i]);
+            r[4] += sh[4][i]; r[5] += sh[5][i]; r[6] = fmax(r[6], sh[6][i]);
+        }
+        for (int k = 0; k < 7; ++k) redpart[blockIdx.x * NRED + k] = r[k];
+    }
+}
+
+__global__ void __launch_bounds__(256)
+k_finalize_scalars(int nred, const double *__restrict__ redpart, int64_t nval, const double *__restrict__ valpart,
+                   double *__restrict__ scal)
+{
+    __shared__ double sh[11][8];
+    double v = 0.0, c = 0.0, sk = 0.0, np = 0.0;
+    for (int64_t b = threadIdx.x; b < nval; b += blockDim.x) {
+        v += valpart[b * 4 + 0];
+        c += valpart[b * 4 + 1];
+        sk += valpart[b * 4 + 2];
+        np += valpart[b * 4 + 3];
+    }
+    double r[7] = {0, 0, 0, -CUDART_INF, 0, 0, 0};
+    for (int b = threadIdx.x; b < nred; b += blockDim.x) {
+        const double *p = redpart + b * NRED;
+        r[0] += p[0]; r[1] += p[1]; r[2] = fmax(r[2], p[2]); r[3] = fmax(r[3], p[3]);
+        r[4] += p[4]; r[5] += p[5]; r[6] = fmax(r[6], p[6]);
+    }
+    v = warp_sum(v); c = warp_sum(c); sk = warp_sum(sk); np = warp_sum(np);
+    r[0] = warp_sum(r[0]); r[1] = warp_sum(r[1]); r[2] = warp_max(r[2]); r[3] = warp_max(r[3]);
+    r[4] = warp_sum(r[4]); r[5] = warp_sum(r[5]); r[6] = warp_max(r[6]);
+    const int wi = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        sh[0][wi] = v; sh[1][wi] = c; sh[2][wi] = sk; sh[10][wi] = np;
+        for (int k = 0; k < 7; ++k) sh[3 + k][wi] = r[k];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t[10] = {0, 0, 0, 0, 0, 0, -CUDART_INF, 0, 0, 0};
+        double tnp = 0.0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) {
+            tnp += sh[10][i];
+            t[0] += sh[0][i]; t[1] += sh[1][i]; t[2] += sh[2][i];
+            t[3] += sh[3][i]; t[4] += sh[4][i]; t[5] = fmax(t[5], sh[5][i]); t[6] = fmax(t[6], sh[6][i]);
+            t[7] += sh[7][i]; t[8] += sh[8][i]; t[9] = fmax(t[9], sh[9][i]);
+        }
+        const double psinu = t[3];
+        scal[SC_VALUE] = t[0] - psinu;
+        scal[SC_C] = t[1];
+        scal[SC_SKIPPED] = t[2];
+        scal[SC_PSINU] = psinu;
+        scal[SC_L1] = t[4];
+        scal[SC_LINF] = t[5];
+        scal[SC_COMP] = t[6];
+        scal[SC_L2SQ] = t[7];
+        scal[SC_DOT_GP] = t[8];
+        scal[SC_NONFINITE] = (t[9] != 0.0 || !isfinite(scal[SC_VALUE])) ? 1.0 : 0.0;
+        scal[SC_PAIRS] = tnp;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+
+static int grid_for(int64_t n, int threads, int cap = 148 * 8)
+{
+    int64_t g = (n + threads - 1) / threads;
+    if (g < 1) g = 1;
+    if (g > cap) g = cap;
+    return (int)g;
+}
+
+void k_axpy_launch(cudaStream_t s, double *x, const double *x0, double a, const double *p, int64_t n)
+{
+    k_axpy<<<grid_for(n, 256), 256, 0, s>>>(x, x0, a, p, n);
+}
+
+sdot_status launch_gather(sdot_ctx *c, double *dst, const double *src, int64_t n)
+{
+    k_gather<<<grid_for(n, 256), 256, 0, c->stream>>>(dst, src, c->perm.p, n);
+    return cuda_error(c, cudaGetLastError(), "gather");
+}
+
+sdot_status launch_scatter(sdot_ctx *c, double *dst, const double *src, int64_t n)
+{
+    k_scatter<<<grid_for(n, 256), 256, 0, c->stream>>>(dst, src, c->perm.p, n);
+    return cuda_error(c, cudaGetLastError(), "scatter");
+}
+
+// largest double s with sqrt_rn(s) <= r (s* = NaN if r is NaN)
+double sstar_of(double r)
+{
+    if (std::isnan(r)) return NAN;
+    if (r < 0) return -1.0;
+    if (r >= 1.3407807929942596e154) return DBL_MAX;
+    double s = r * r;
+    while (s > 0 && std::sqrt(s) > r) s = std::nextafter(s, 0.0);
+    while (std::sqrt(std::nextafter(s, INFINITY)) <= r) s = std::nextafter(s, INFINITY);
+    return s;
+}
+
+static double vmin_host(const std::vector<double> &v)
+{
+    return *std::min_element(v.begin(), v.end());
+}
+
+// SotSolver::compute_distance_threshold (SotSolver.cc:379-429), on the host
+// with the same libm calls and operation order as the reference.
+double host_threshold(sdot_ctx *c, double maxpsi, double minpsi)
+{
+    const sdot_solver_params &p = c->prm;
+    if (p.threshold_type == SDOT_THRESH_INTEGRAL) {
+        double absJ = std::fabs(c->global_functional);
+        if (absJ < 1e-10) absJ = 1e-10;
+        const double num = p.epsilon * c->C_global;
+        const double den = p.tau * absJ;
+        const double arg = num / den;
+        const double r2 = 2.0 * maxpsi + 2.0 * p.epsilon * std::log(arg);
+        const double r = std::sqrt(std::max(0.0, r2));
+        return std::max(r, c->covering_radius);
+    }
+    if (p.threshold_type == SDOT_THRESH_GEOMETRIC) {
+        double r0 = c->covering_radius;
+        if (!(r0 > 0.0)) {
+            double rr = 0.0;
+            sdot_compute_covering_radius(c, &rr);
+            r0 = rr;
+        }
+        const double range = maxpsi - minpsi;
+        const double mind = c->min_target_density > 0.0 ? c->min_target_density : vmin_host(c->nu_host);
+        double fv = std::fabs(c->global_functional);
+        if (fv < 1e-10) fv = 1e-10;
+        const double log_term = std::log(p.epsilon / (mind * p.tau * fv));
+        double r2 = r0 * r0 + 2.0 * range + 2.0 * p.epsilon * log_term;
+        if (r2 < r0 * r0) r2 = r0 * r0;
+        return std::sqrt(r2);
+    }
+    const double numin = c->min_target_density > 0.0 ? c->min_target_density : vmin_host(c->nu_host);
+    if (numin <= 0 || p.tau <= 0) return DBL_MAX;
+    const double r2 = -2.0 * p.epsilon * std::log(p.tau / numin) + 2.0 * maxpsi;
+    return std::sqrt(std::max(0.0, r2));
+}
+
+template <int DIM>
+static sdot_status run_eval(sdot_ctx *c, const EvalArgs &a, bool dense, const double *pdir, double tol)
+{
+    cudaStream_t st = c->stream;
+    const int prec = c->precision;
+    k_target_prep<DIM><<<grid_for(a.nt, 256), 256, 0, st>>>(a.nt, c->y.p, c->nu.p, c->psi.p, a, c->tpack.p);
+    int64_t nval = 0;
+    int nks = 1;
+    if (dense) {
+        const int64_t per = (int64_t)DENSE_A_THREADS * DENSE_A_QT;
+        nval = (a.nq + per - 1) / per;
+        k_value_dense<DIM><<<(unsigned)nval, DENSE_A_THREADS, 0, st>>>(c->x.p, c->rho.p, c->jxw.p, c->tpack.p, a,
+                                                                       c->Lq.p, c->blkpart.p);
+        // gradient: target blocks x q-slices, ~4 waves of CTAs
+        const int64_t tb = (a.nt + DENSE_B_THREADS * DENSE_B_TT - 1) / (DENSE_B_THREADS * DENSE_B_TT);
+        int64_t want = (148 * 8 + tb - 1) / tb;
+        int64_t maxks = (a.nq + 255) / 256;
+        nks = (int)std::max<int64_t>(1, std::min<int64_t>(want, maxks));
+        if (nks > 64) nks = 64;
+        const int64_t qslice = (a.nq + nks - 1) / nks;
+        dim3 g((unsigned)tb, (unsigned)nks);
+        if (prec == SDOT_PREC_FP64)
+            k_grad_dense<DIM, false><<<g, DENSE_B_THREADS, 0, st>>>(c->x.p, c->w.p, c->Lq.p, c->tpack.p, c->psi.p, a,
+                                                                    qslice, c->gpart.p);
+        else
+            k_grad_dense<DIM, true><<<g, DENSE_B_THREADS, 0, st>>>(c->x.p, c->w.p, c->Lq.p, c->tpack.p, c->psi.p, a,
+                                                                   qslice, c->gpart.p);
+    } else {
+        nval = c->nsblk;
+        const size_t smA = sizeof(VTSmem);
+        if (a.ql <= 4) {
+            cudaFuncSetAttribute(k_value_trunc<DIM, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smA);
+            k_value_trunc<DIM, 4><<<(unsigned)c->nsblk, VT_WARPS * 32, smA, st>>>(
+                c->x.p, c->rho.p, c->jxw.p, c->cell_ctr.p, c->sblk_sph.p, c->tpack.p, c->tblk_sph.p, c->ntblk, a,
+                c->Lq.p, c->blkpart.p);
+        } else if (a.ql <= 8) {
+            cudaFuncSetAttribute(k_value_trunc<DIM, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smA);
+            k_value_trunc<DIM, 8><<<(unsigned)c->nsblk, VT_WARPS * 32, smA, st>>>(
+                c->x.p, c->rho.p, c->jxw.p, c->cell_ctr.p, c->sblk_sph.p, c->tpack.p, c->tblk_sph.p, c->ntblk, a,
+                c->Lq.p, c->blkpart.p);
+        } else {
+            cudaFuncSetAttribute(k_value_trunc<DIM, 9>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smA);
+            k_value_trunc<DIM, 9><<<(unsigned)c->nsblk, VT_WARPS * 32, smA, st>>>(
+                c->x.p, c->rho.p, c->jxw.p, c->cell_ctr.p, c->sblk_sph.p, c->tpack.p, c->tblk_sph.p, c->ntblk, a,
+                c->Lq.p, c->blkpart.p);
+        }
+        const int64_t ncblk = c->ncblk;
+        const bool fp32 = prec != SDOT_PREC_FP64;
+        const int qbytes = fp32 ? (int)(sizeof(float4) + sizeof(float)) : 5 * (int)sizeof(double);
+        const int maxq = fp32 ? GT_MAXQ : GT_MAXQ64;
+        int maxcb = std::min(GT_MAXCELL / SBLK_CELLS, maxq / (SBLK_CELLS * a.qpc));
+        if (maxcb < 1) maxcb = 1;
+        const size_t smB = ((sizeof(GTSmem) + 15) & ~size_t(15)) + (size_t)maxq * qbytes;
+        if (fp32) {
+            cudaFuncSetAttribute(k_grad_trunc<DIM, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smB);
+            k_grad_trunc<DIM, true><<<(unsigned)c->ntblk, GT_WARPS * 32, smB, st>>>(
+                c->x.p, c->w.p, c->Lq.p, c->cell_ctr.p, c->cblk_sph.p, ncblk, c->tpack.p, c->psi.p, c->tblk_sph.p, a,
+                maxcb, c->gpart.p);
+        } else {
+            cudaFuncSetAttribute(k_grad_trunc<DIM, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smB);
+            k_grad_trunc<DIM, false><<<(unsigned)c->ntblk, GT_WARPS * 32, smB, st>>>(
+                c->x.p, c->w.p, c->Lq.p, c->cell_ctr.p, c->cblk_sph.p, ncblk, c->tpack.p, c->psi.p, c->tblk_sph.p,
+                a, maxcb, c->gpart.p);
+        }
+    }
+    k_finalize_grad<<<FIN_BLOCKS, FIN_THREADS, 0, st>>>(a.nt, nks, c->gpart.p, c->nu.p, c->psi.p, pdir, tol, c->grad.p,
+                                                       c->redpart.p);
+    k_finalize_scalars<<<1, 256, 0, st>>>(FIN_BLOCKS, c->redpart.p, nval, c->blkpart.p, c->scal.p);
+    return cuda_error(c, cudaGetLastError(), "evaluate launch");
+}
+
+sdot_status evaluate_internal(sdot_ctx *c, const double *p_dir, double comp_tol, double *ms_out)
+{
+    if (c->dim == 0 || c->nq == 0) return set_error(c, SDOT_ESTATE, "source measure not set");
+    if (c->nt == 0) return set_error(c, SDOT_ESTATE, "target measure not set");
+    const sdot_solver_params &p = c->prm;
+    // threshold (host, exact libm), from device max/min of psi
+    double r = DBL_MAX;
+    const bool may_truncate = (p.threshold_type != SDOT_THRESH_POINTWISE) ||
+                              (p.tau > 0 && (c->min_target_density > 0.0 ? c->min_target_density
+                                                                          : vmin_host(c->nu_host)) > 0);
+    cudaEventRecord(c->ev0, c->stream);
+    double mm[3] = {0, 0, 0};
+    k_minmax<<<1, 1024, 0, c->stream>>>(c->psi.p, c->nt, c->scal.p + SC_MAXPSI);
+    if (may_truncate) {
+        cudaError_t e = cudaMemcpyAsync(mm, c->scal.p + SC_MAXPSI, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) return cuda_error(c, e, "threshold readback");
+        if (mm[2] != 0.0) return set_error(c, SDOT_ENONFINITE, "non-finite potential");
+        r = host_threshold(c, mm[0], mm[1]);
+    }
+    c->current_distance_threshold = r;
+    const double sstar = sstar_of(r);
+    const bool dense = !(r < c->diam * (1.0 + 1e-12)) || std::isinf(r) ? true : false;
+    const bool dense_ok = dense && !std::isnan(r);
+
+    EvalArgs a{};
+    a.qpc = c->qpc;
+    a.ql = c->ql;
+    a.ngroups = c->ngroups;
+    a.lse = p.use_log_sum_exp;
+    a.nq = c->nq;
+    a.ncells = c->ncells;
+    a.nunits = c->ncells * a.ngroups;
+    a.nt = c->nt;
+    a.eps = p.epsilon;
+    a.s = KAPPA / p.epsilon;
+    a.halfs = 0.5 * a.s;
+    for (int d = 0; d < 3; ++d) a.o[d] = c->origin[d];
+    a.sstar = sstar;
+    a.cull = std::isnan(r) ? 0.0 : std::min(r, 1e300);
+    a.c32 = LOG2E / (2.0 * p.epsilon);
+    a.l2e_eps = LOG2E / p.epsilon;
+
+    if (!dense_ok && std::isnan(r)) {
+        // NaN threshold: the reference's predicate d <= NaN rejects everything
+        a.sstar = NAN;
+    }
+    sdot_status s = (c->dim == 2) ? run_eval<2>(c, a, dense_ok, p_dir, comp_tol)
+                                  : run_eval<3>(c, a, dense_ok, p_dir, comp_tol);
+    if (s != SDOT_OK) return s;
+    cudaEventRecord(c->ev1, c->stream);
+    cudaError_t e = cudaMemcpyAsync(c->scal_host, c->scal.p, SC_COUNT * sizeof(double), cudaMemcpyDeviceToHost,
+                                    c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_error(c, e, "evaluate");
+    if (ms_out) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        *ms_out = ms;
+    }
+    c->scal_host[SC_R] = r;
+    c->global_functional = c->scal_host[SC_VALUE];
+    c->C_global = c->scal_host[SC_C];
+    if (c->scal_host[SC_NONFINITE] != 0.0) return set_error(c, SDOT_ENONFINITE, "non-finite value or gradient");
+    return SDOT_OK;
+}
+
+}  // namespace sdot

@@ -1,0 +1,189 @@
+// sdot_hessian.cu -- dense Hessian of the entropic dual functional.
+//
+// SotSolver declares compute_hessian(potential, LAPACKFullMatrix&) but never
+// defines it (include/SemiDiscreteOT/solvers/SotSolver.h:343-344).  This file
+// provides it:
+//     H = (1/eps) [ diag(sum_q w_q pi_q) - sum_q w_q pi_q pi_q^T ],
+//     pi_qj = nu_j exp(t_qj - L_q)   (0 outside the candidate set of cell(q)),
+// which is d(grad)/d(psi) of the evaluation in sdot_eval.cu.  The diagonal
+// term equals (g_j + nu_j)/eps and is taken from the evaluation; the
+// contraction P_w^T P (P_w = diag(w) P) is accumulated here in FP64 on
+// 64x64 output tiles (upper triangle, mirrored), P regenerated on the fly
+// from the L_q of the value sweep and never stored.
+#include <float.h>
+#include <math.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "sdot_device.cuh"
+#include "sdot_internal.h"
+
+namespace sdot {
+
+constexpr int HT = 64;        // output tile edge
+constexpr int HQ = 16;        // quadrature points per smem chunk
+
+template <int DIM, bool TRUNC>
+__global__ void __launch_bounds__(256)
+k_hessian_simt(const double *__restrict__ x, const double *__restrict__ w, const double *__restrict__ Lq,
+               const double *__restrict__ cell_ctr, const double *__restrict__ tpack, const double *__restrict__ grad,
+               const double *__restrict__ nu, EvalArgs a, double *__restrict__ H)
+{
+    const int tb = blockIdx.x, ta = blockIdx.y;
+    if (tb < ta) return;  // upper triangle of tiles
+    __shared__ double tab[16];
+    __shared__ double PA[HQ][HT + 1];   // w_q pi_qa
+    __shared__ double PB[HQ][HT + 1];   // pi_qb
+    __shared__ double tgt[2][HT][8];
+    const int tid = threadIdx.x;
+    if (tid < 16) tab[tid] = c_exp2_tab[tid];
+    for (int i = tid; i < 2 * HT * 8; i += 256) {
+        const int side = i / (HT * 8), r = (i / 8) % HT, f = i % 8;
+        const int64_t j = (int64_t)(side == 0 ? ta : tb) * HT + r;
+        tgt[side][r][f] = j < a.nt ? tpack[j * TPACK + f] : 0.0;
+    }
+    const int tr = tid / 16, tc = tid % 16;  // thread owns rows tr*4.., cols tc*4..
+    double acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) acc[i][k] = 0.0;
+    __syncthreads();
+    for (int64_t q0 = 0; q0 < a.nq; q0 += HQ) {
+        // fill PA/PB: HQ x 2*HT entries, 256 threads -> 8 each
+        for (int i = tid; i < HQ * 2 * HT; i += 256) {
+            const int qi = i / (2 * HT), col = i % (2 * HT);
+            const int side = col / HT, r = col % HT;
+            const int64_t q = q0 + qi;
+            const int64_t j = (int64_t)(side == 0 ? ta : tb) * HT + r;
+            double val = 0.0;
+            if (q < a.nq && j < a.nt) {
+                const double Lv = Lq[q];
+                bool in = isfinite(Lv);
+                const double *tp = tgt[side][r];
+                if (TRUNC && in) {
+                    const int64_t cell = q / a.qpc;
+                    in = dist2_exact<DIM>(tp + 2 + DIM, cell_ctr + cell * DIM) <= a.sstar;
+                }
+                if (in) {
+                    double xt[3], xsq = 0.0;
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) {
+                        xt[d] = x[q * DIM + d] - a.o[d];
+                        xsq += xt[d] * xt[d];
+                    }
+                    double u = fma(tp[1], xt[0], tp[0] + (-a.halfs * xsq - KAPPA * Lv));
+#pragma unroll
+                    for (int d = 1; d < DIM; ++d) u = fma(tp[1 + d], xt[d], u);
+                    val = tp[1 + DIM] * exp2_16(u, tab);
+                    if (side == 0) val *= w[q];
+                }
+            }
+            if (side == 0) PA[qi][r] = val;
+            else PB[qi][r] = val;
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int qi = 0; qi < HQ; ++qi) {
+            double av[4], bv[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) av[i] = PA[qi][tr * 4 + i];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) bv[k] = PB[qi][tc * 4 + k];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int k = 0; k < 4; ++k) acc[i][k] = fma(av[i], bv[k], acc[i][k]);
+        }
+        __syncthreads();
+    }
+    const double einv = 1.0 / a.eps;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int64_t ja = (int64_t)ta * HT + tr * 4 + i;
+        if (ja >= a.nt) continue;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int64_t jb = (int64_t)tb * HT + tc * 4 + k;
+            if (jb >= a.nt) continue;
+            double h = -acc[i][k];
+            if (ja == jb) h += grad[ja] + nu[ja];
+            h *= einv;
+            H[ja * a.nt + jb] = h;
+            if (tb != ta) H[jb * a.nt + ja] = h;
+        }
+    }
+}
+
+// Hu[perm[a], perm[b]] = Hi[a, b]
+__global__ void k_permute_matrix(const double *__restrict__ Hi, double *__restrict__ Hu, const int64_t *__restrict__ perm,
+                                 int64_t n)
+{
+    for (int64_t a = blockIdx.y; a < n; a += gridDim.y) {
+        const int64_t pa = perm[a];
+        for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < n; b += (int64_t)gridDim.x * blockDim.x)
+            Hu[pa * n + perm[b]] = Hi[a * n + b];
+    }
+}
+
+sdot_status hessian_internal(sdot_ctx *c, double *H_host)
+{
+    // an evaluation at c->psi provides L_q, the gradient and the threshold
+    double ms = 0;
+    sdot_status s = evaluate_internal(c, nullptr, c->prm.tolerance, &ms);
+    if (s != SDOT_OK) return s;
+    const int64_t n = c->nt;
+    if (n > 46340) return set_error(c, SDOT_EBUDGET, "dense Hessian limited to n_targets <= 46340");
+    const double r = c->current_distance_threshold;
+    EvalArgs a{};
+    a.qpc = c->qpc;
+    a.nq = c->nq;
+    a.ncells = c->ncells;
+    a.nt = n;
+    a.eps = c->prm.epsilon;
+    a.s = KAPPA / c->prm.epsilon;
+    a.halfs = 0.5 * a.s;
+    for (int d = 0; d < 3; ++d) a.o[d] = c->origin[d];
+    a.sstar = sstar_of(r);
+    const bool trunc = std::isnan(r) || r < c->diam;
+    DevBuf<double> Hi, Hu;
+    cudaError_t e = Hi.alloc((size_t)n * n);
+    if (e == cudaSuccess) e = Hu.alloc((size_t)n * n);
+    if (e != cudaSuccess) return cuda_error(c, e, "hessian alloc");
+    const unsigned nb = (unsigned)((n + HT - 1) / HT);
+    dim3 g(nb, nb);
+    if (c->dim == 2) {
+        if (trunc) k_hessian_simt<2, true><<<g, 256, 0, c->stream>>>(c->x.p, c->w.p, c->Lq.p, c->cell_ctr.p, c->tpack.p, c->grad.p, c->nu.p, a, Hi.p);
+        else k_hessian_simt<2, false><<<g, 256, 0, c->stream>>>(c->x.p, c->w.p, c->Lq.p, c->cell_ctr.p, c->tpack.p, c->grad.p, c->nu.p, a, Hi.p);
+    } else {
+        if (trunc) k_hessian_simt<3, true><<<g, 256, 0, c->stream>>>(c->x.p, c->w.p, c->Lq.p, c->cell_ctr.p, c->tpack.p, c->grad.p, c->nu.p, a, Hi.p);
+        else k_hessian_simt<3, false><<<g, 256, 0, c->stream>>>(c->x.p, c->w.p, c->Lq.p, c->cell_ctr.p, c->tpack.p, c->grad.p, c->nu.p, a, Hi.p);
+    }
+    k_permute_matrix<<<dim3(std::max<unsigned>(1, (unsigned)std::min<int64_t>((n + 255) / 256, 64)),
+                            (unsigned)std::min<int64_t>(n, 65535)), 256, 0,
+                       c->stream>>>(Hi.p, Hu.p, c->perm.p, n);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(H_host, Hu.p, (size_t)n * n * 8, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    return cuda_error(c, e, "hessian");
+}
+
+}  // namespace sdot
+
+extern "C" sdot_status sdot_hessian(sdot_ctx *c, const double *psi, double *H)
+{
+    if (!c || !psi || !H) return SDOT_EINVAL;
+    if (c->nq == 0 || c->nt == 0) return sdot::set_error(c, SDOT_ESTATE, "measures not set");
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != c->device) cudaSetDevice(c->device);
+    double dummy = 0;
+    // reuse the public evaluation to stage psi and the per-evaluation buffers
+    std::vector<double> g((size_t)c->nt);
+    sdot_status s = sdot_evaluate(c, psi, g.data(), &dummy, nullptr);
+    if (s == SDOT_OK) s = sdot::hessian_internal(c, H);
+    if (prev >= 0 && prev != c->device) cudaSetDevice(prev);
+    return s;
+}

@@ -1,0 +1,210 @@
+"""``SotSolver``: the reference's solver interface on top of ``libsdot_cuda``.
+
+Mirrors ``SotSolver<dim, spacedim>`` (include/SemiDiscreteOT/solvers/SotSolver.h
+:54-525): the same method names, argument meaning and error behaviour, with
+numpy arrays in place of deal.II types.  deal.II ``DoFHandler``/``Mapping``
+objects cannot cross the C ABI, so ``setup_source`` takes the flattened
+quadrature data that ``SemiDiscreteOT::save_discrete_measures`` writes
+(src/core/SemiDiscreteOT.cc:2489-2558); ``source.structured_source`` builds it
+for structured Q1 meshes.
+
+Errors raise ``RuntimeError`` (``SdotError``) like the reference's exceptions,
+except non-convergence of ``solve``, which the reference swallows
+(SotSolver.cc:207-211) and reports through ``get_convergence_status()``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from .parameters import SolverParameters
+
+
+def _f64(a, shape=None) -> np.ndarray:
+    out = np.ascontiguousarray(a, dtype=np.float64)
+    if shape is not None:
+        out = out.reshape(shape)
+    return out
+
+
+class SotSolver:
+    """Entropic semi-discrete OT dual solver on one GPU (one CUDA stream)."""
+
+    def __init__(self, dim: int = 3, device: int = 0, precision: str = "hybrid",
+                 memory_budget: int = 0, verbose: bool = False):
+        self.dim = int(dim)
+        self._L = _lib.load()
+        opts = _lib.Options(int(device), _lib.PRECISION[precision], int(memory_budget), int(verbose))
+        h = C.c_void_p()
+        st = self._L.sdot_create(C.byref(h), C.byref(opts))
+        if st != _lib.SDOT_OK:
+            raise _lib.SdotError(st, "sdot_create failed (no CUDA device?)")
+        self._h = h
+        self.precision = precision
+        self.current_params = SolverParameters()
+        self._n_targets = 0
+        self.last_eval_info: dict = {}
+        self.last_solve_info: dict = {}
+
+    # ------------------------------------------------------------------ utils
+    def _check(self, st: int):
+        if st != _lib.SDOT_OK:
+            msg = self._L.sdot_last_error(self._h).decode()
+            raise _lib.SdotError(st, msg)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.sdot_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @staticmethod
+    def _cparams(p: SolverParameters) -> _lib.SolverParams:
+        return _lib.SolverParams(int(p.max_iterations), float(p.tolerance),
+                                 _lib.CONTROL[p.solver_control_type], float(p.epsilon), float(p.tau),
+                                 _lib.THRESHOLD[p.distance_threshold_type], int(bool(p.use_log_sum_exp_trick)),
+                                 _lib.LINE_SEARCH[p.line_search])
+
+    # ------------------------------------------------------------- measures
+    def setup_source(self, x, jxw, density, cell_offsets, cell_centers):
+        """SotSolver::setup_source (SotSolver.cc:43-51) on flattened quadrature data."""
+        x = _f64(x).reshape(-1, self.dim)
+        jxw = _f64(jxw)
+        density = _f64(density)
+        off = np.ascontiguousarray(cell_offsets, dtype=np.int64)
+        ctr = _f64(cell_centers).reshape(-1, self.dim)
+        if not (x.shape[0] == jxw.size == density.size):
+            raise ValueError("x, jxw and density must have one entry per quadrature point")
+        if off.size != ctr.shape[0] + 1:
+            raise ValueError("cell_offsets must have n_cells + 1 entries")
+        self._check(self._L.sdot_set_source(self._h, self.dim, x.shape[0], x.ctypes.data, jxw.ctypes.data,
+                                            density.ctypes.data, ctr.shape[0], off.ctypes.data, ctr.ctypes.data))
+        self._src = (x, jxw, density, off, ctr)
+
+    def setup_source_measure(self, src: dict):
+        self.setup_source(src["x"], src["jxw"], src["density"], src["cell_offsets"], src["cell_centers"])
+
+    def setup_target(self, target_points, target_density):
+        """SotSolver::setup_target (SotSolver.cc:53-60); weights are not normalised."""
+        y = _f64(target_points).reshape(-1, self.dim)
+        nu = _f64(target_density)
+        if y.shape[0] != nu.size:
+            raise ValueError(f"Dimension mismatch: {y.shape[0]} != {nu.size}")
+        self._check(self._L.sdot_set_target(self._h, y.shape[0], y.ctypes.data, nu.ctypes.data))
+        self._n_targets = y.shape[0]
+
+    def configure(self, params: SolverParameters):
+        """SotSolver::configure (SotSolver.cc:62-69)."""
+        self.current_params = params
+        cp = self._cparams(params)
+        self._check(self._L.sdot_configure(self._h, C.byref(cp)))
+
+    def set_distance_function(self, name: str):
+        self._check(self._L.sdot_set_distance_function(self._h, name.encode()))
+
+    # ------------------------------------------------------------- hot path
+    def evaluate_functional(self, potential, gradient_out: Optional[np.ndarray] = None) -> float:
+        """SotSolver::evaluate_functional (SotSolver.cc:217-377): returns J(psi);
+        the gradient sum_q w_q pi_qj - nu_j is written into gradient_out."""
+        psi = _f64(potential)
+        if psi.size != self._n_targets:
+            raise ValueError("potential size differs from the number of targets")
+        g = gradient_out if (gradient_out is not None and gradient_out.dtype == np.float64
+                             and gradient_out.flags.c_contiguous) else np.empty(self._n_targets)
+        val = C.c_double(0.0)
+        info = _lib.EvalInfo()
+        self._check(self._L.sdot_evaluate(self._h, psi.ctypes.data, g.ctypes.data, C.byref(val), C.byref(info)))
+        if gradient_out is not None and g is not gradient_out:
+            gradient_out[...] = g
+        self.last_eval_info = {"value": info.value, "C_global": info.C_global, "threshold": info.threshold,
+                               "n_pairs": info.n_pairs, "device_ms": info.device_ms}
+        self._last_grad = g
+        return val.value
+
+    def evaluate_functional_device(self, psi_ptr: int, grad_ptr: int) -> float:
+        """Evaluation on device pointers (caller ordering, context's device)."""
+        val = C.c_double(0.0)
+        info = _lib.EvalInfo()
+        self._check(self._L.sdot_evaluate_device(self._h, C.c_void_p(psi_ptr), C.c_void_p(grad_ptr),
+                                                 C.byref(val), C.byref(info)))
+        self.last_eval_info = {"value": info.value, "C_global": info.C_global, "threshold": info.threshold,
+                               "n_pairs": info.n_pairs, "device_ms": info.device_ms}
+        return val.value
+
+    def solve(self, potential: np.ndarray, params: Optional[SolverParameters] = None) -> np.ndarray:
+        """SotSolver::solve (SotSolver.cc:105-215): L-BFGS on the device.
+        ``potential`` is updated in place when it is a float64 C-contiguous array."""
+        if params is not None:
+            self.current_params = params
+        if potential is None or np.asarray(potential).size != self._n_targets:
+            psi = np.zeros(self._n_targets)   # potentials.reinit(n) (SotSolver.cc:151-153)
+        else:
+            psi = potential if (isinstance(potential, np.ndarray) and potential.dtype == np.float64
+                                and potential.flags.c_contiguous) else _f64(potential).copy()
+        cp = self._cparams(self.current_params)
+        info = _lib.SolveInfo()
+        st = self._L.sdot_solve(self._h, psi.ctypes.data, C.byref(cp), C.byref(info))
+        self.last_solve_info = {"iterations": info.iterations, "converged": bool(info.converged),
+                                "n_evaluations": info.n_evaluations, "last_value": info.last_value,
+                                "last_check_value": info.last_check_value, "total_pairs": info.total_pairs,
+                                "device_ms": info.device_ms}
+        self._check(st)
+        if isinstance(potential, np.ndarray) and potential is not psi and potential.size == psi.size:
+            potential[...] = psi
+        return psi
+
+    def compute_hessian(self, potential, hessian_out: Optional[np.ndarray] = None) -> np.ndarray:
+        """Dense Hessian H = (1/eps) sum_q w_q (diag(pi_q) - pi_q pi_q^T) (declared at SotSolver.h:343-344)."""
+        psi = _f64(potential)
+        n = self._n_targets
+        H = hessian_out if (hessian_out is not None and hessian_out.shape == (n, n) and
+                            hessian_out.dtype == np.float64 and hessian_out.flags.c_contiguous) else np.empty((n, n))
+        self._check(self._L.sdot_hessian(self._h, psi.ctypes.data, H.ctypes.data))
+        if hessian_out is not None and H is not hessian_out:
+            hessian_out[...] = H
+        return H
+
+    # ---------------------------------------------------------------- getters
+    def get_last_functional_value(self) -> float:
+        return self._L.sdot_get_last_functional_value(self._h)
+
+    def get_last_iteration_count(self) -> int:
+        return self._L.sdot_get_last_iteration_count(self._h)
+
+    def get_convergence_status(self) -> bool:
+        return bool(self._L.sdot_get_convergence_status(self._h))
+
+    def get_last_distance_threshold(self) -> float:
+        return self._L.sdot_get_last_distance_threshold(self._h)
+
+    def get_C_global(self) -> float:
+        return self._L.sdot_get_C_global(self._h)
+
+    def set_distance_threshold(self, threshold: float):
+        self._check(self._L.sdot_set_distance_threshold(self._h, float(threshold)))
+
+    def compute_covering_radius(self) -> float:
+        r = C.c_double(0.0)
+        self._check(self._L.sdot_compute_covering_radius(self._h, C.byref(r)))
+        return r.value
+
+    def compute_geometric_radius_bound(self, potentials, epsilon: float, tolerance: float) -> float:
+        psi = _f64(potentials)
+        r = C.c_double(0.0)
+        self._check(self._L.sdot_compute_geometric_radius_bound(self._h, psi.ctypes.data, float(epsilon),
+                                                                float(tolerance), C.byref(r)))
+        return r.value
