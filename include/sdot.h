@@ -170,6 +170,36 @@ sdot_status sdot_compute_geometric_radius_bound(sdot_ctx *ctx, const double *psi
  * only "euclidean" is on the accelerated path; anything else is SDOT_EINVAL. */
 sdot_status sdot_set_distance_function(sdot_ctx *ctx, const char *name);
 
+/* ---- multi-GPU sharding (no reference counterpart as one call: it replaces
+ * the MPI sums of SotSolver.cc:316-319 by letting the caller all-reduce). ----
+ * Evaluation of this context's source shard only: writes n_targets + 3
+ * doubles to out_dev (device memory): [0, n) the source part of the gradient
+ * sum_q w_q pi_qj (caller ordering, nu NOT subtracted), [n] the source part
+ * of the functional (linear term NOT subtracted), [n+1] C_global part,
+ * [n+2] candidate pairs.  Summing out_dev over the shards and then
+ * subtracting nu_j and sum_j psi_j nu_j gives sdot_evaluate's results. */
+sdot_status sdot_evaluate_partial_device(sdot_ctx *ctx, const double *psi_dev, double *out_dev,
+                                         sdot_eval_info *info);
+/* Sets the state the integral/geometric thresholds read (the reference's
+ * members global_functional and C_global, SotSolver.cc:316-331) after a
+ * sharded evaluation has been reduced. */
+sdot_status sdot_set_state(sdot_ctx *ctx, double global_functional, double C_global);
+
+/* ---- measurement ---- */
+/* The CUDA stream (cudaStream_t) every kernel of this context is launched on. */
+void *sdot_get_stream(const sdot_ctx *ctx);
+/* Enable CUDA-event timing of each evaluation phase (0 = off). */
+sdot_status sdot_set_profiling(sdot_ctx *ctx, int enable);
+/* Cumulative device milliseconds and launch counts per phase since the last
+ * reset: phases 0 threshold, 1 target prep, 2 value sweep, 3 gradient sweep,
+ * 4 finalize.  ms and launches hold n entries; reset != 0 zeroes them after
+ * reading. */
+sdot_status sdot_get_kernel_times(sdot_ctx *ctx, double *ms, int64_t *launches, int n, int reset);
+/* Microbenchmarks of the pipes the kernels are bound by, on device `device`:
+ * out[0] FP64 FMA TFLOP/s, out[1] FP32 FMA TFLOP/s, out[2] MUFU ex2.approx.f32
+ * Gop/s, out[3] SM clock (MHz) reported by the device. */
+sdot_status sdot_measure_peaks(int device, double *out);
+
 #ifdef __cplusplus
 }
 #endif

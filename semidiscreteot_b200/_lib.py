@@ -29,7 +29,8 @@ EXPORTED = [
     "sdot_evaluate_device", "sdot_solve", "sdot_hessian", "sdot_get_last_functional_value",
     "sdot_get_last_iteration_count", "sdot_get_convergence_status", "sdot_get_last_distance_threshold",
     "sdot_get_C_global", "sdot_set_distance_threshold", "sdot_compute_covering_radius",
-    "sdot_compute_geometric_radius_bound", "sdot_set_distance_function",
+    "sdot_compute_geometric_radius_bound", "sdot_set_distance_function", "sdot_evaluate_partial_device",
+    "sdot_set_state", "sdot_get_stream", "sdot_set_profiling", "sdot_get_kernel_times", "sdot_measure_peaks",
 ]
 
 
@@ -96,6 +97,16 @@ def load():
     lib.sdot_compute_covering_radius.argtypes = [vp, C.POINTER(d)]
     lib.sdot_compute_geometric_radius_bound.argtypes = [vp, vp, d, d, C.POINTER(d)]
     lib.sdot_set_distance_function.argtypes = [vp, C.c_char_p]
+    lib.sdot_evaluate_partial_device.argtypes = [vp, vp, vp, C.POINTER(EvalInfo)]
+    lib.sdot_set_state.argtypes = [vp, d, d]
+    lib.sdot_get_stream.argtypes = [vp]
+    lib.sdot_get_stream.restype = vp
+    lib.sdot_set_profiling.argtypes = [vp, ip]
+    lib.sdot_get_kernel_times.argtypes = [vp, vp, vp, ip, ip]
+    lib.sdot_measure_peaks.argtypes = [ip, vp]
+    for fn in ("sdot_evaluate_partial_device", "sdot_set_state", "sdot_set_profiling", "sdot_get_kernel_times",
+               "sdot_measure_peaks"):
+        getattr(lib, fn).restype = ip
     for fn in ("sdot_create", "sdot_set_source", "sdot_set_target", "sdot_configure", "sdot_evaluate",
                "sdot_evaluate_device", "sdot_solve", "sdot_hessian", "sdot_set_distance_threshold",
                "sdot_compute_covering_radius", "sdot_compute_geometric_radius_bound",

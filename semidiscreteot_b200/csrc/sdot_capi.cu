@@ -365,6 +365,8 @@ void sdot_destroy(sdot_ctx *c)
         c->io_a.release(); c->io_b.release(); c->x0.release(); c->pdir.release(); c->sk.release(); c->yk.release();
         c->hist_s.release(); c->hist_y.release(); c->gtmp.release();
         if (c->scal_host) cudaFreeHost(c->scal_host);
+        for (int i = 0; i < 8; ++i)
+            if (c->pev[i]) cudaEventDestroy(c->pev[i]);
         if (c->ev0) cudaEventDestroy(c->ev0);
         if (c->ev1) cudaEventDestroy(c->ev1);
         if (c->stream) cudaStreamDestroy(c->stream);
@@ -935,6 +937,161 @@ sdot_status sdot_solve(sdot_ctx *c, double *psi, const sdot_solver_params *param
     }
     if (result != SDOT_OK) return result;
     return s2;
+}
+
+__global__ void k_partial_tail(const double *scal, double *out)
+{
+    out[0] = scal[SC_VALSRC];
+    out[1] = scal[SC_C];
+    out[2] = scal[SC_PAIRS];
+}
+
+sdot_status sdot_evaluate_partial_device(sdot_ctx *c, const double *psi_dev, double *out_dev, sdot_eval_info *info)
+{
+    if (!c || !psi_dev || !out_dev) return SDOT_EINVAL;
+    DeviceGuard g(c->device);
+    sdot_status s = prepare_eval(c);
+    if (s != SDOT_OK) return s;
+    if ((s = launch_gather(c, c->psi.p, psi_dev, c->nt)) != SDOT_OK) return s;
+    double ms = 0;
+    s = evaluate_internal(c, nullptr, c->prm.tolerance, &ms, true);
+    if (s != SDOT_OK && s != SDOT_ENONFINITE) return s;
+    sdot_status s2 = launch_scatter(c, out_dev, c->grad.p, c->nt);
+    if (s2 != SDOT_OK) return s2;
+    k_partial_tail<<<1, 1, 0, c->stream>>>(c->scal.p, out_dev + c->nt);
+    CK(cudaGetLastError(), "partial tail");
+    CK(cudaStreamSynchronize(c->stream), "partial sync");
+    fill_eval_info(c, info, ms);
+    if (info) info->value = c->scal_host[SC_VALSRC];
+    return s;
+}
+
+sdot_status sdot_set_state(sdot_ctx *c, double global_functional, double C_global)
+{
+    if (!c) return SDOT_EINVAL;
+    c->global_functional = global_functional;
+    c->C_global = C_global;
+    return SDOT_OK;
+}
+
+void *sdot_get_stream(const sdot_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+sdot_status sdot_set_profiling(sdot_ctx *c, int enable)
+{
+    if (!c) return SDOT_EINVAL;
+    DeviceGuard g(c->device);
+    if (enable && !c->pev[0])
+        for (int i = 0; i < 8; ++i) CK(cudaEventCreate(&c->pev[i]), "profiling events");
+    c->profiling = enable != 0;
+    return SDOT_OK;
+}
+
+sdot_status sdot_get_kernel_times(sdot_ctx *c, double *ms, int64_t *launches, int n, int reset)
+{
+    if (!c) return SDOT_EINVAL;
+    for (int i = 0; i < n && i < 6; ++i) {
+        if (ms) ms[i] = c->kms[i];
+        if (launches) launches[i] = c->klaunch[i];
+    }
+    if (reset)
+        for (int i = 0; i < 6; ++i) {
+            c->kms[i] = 0.0;
+            c->klaunch[i] = 0;
+        }
+    return SDOT_OK;
+}
+
+// Pipe microbenchmarks: independent FMA / ex2 chains, enough warps to fill
+// every SM; results are consumed so nothing is optimised away.
+__global__ void k_peak_fp64(double *out, int iters, double seed)
+{
+    double a0 = seed + threadIdx.x, a1 = a0 + 1, a2 = a0 + 2, a3 = a0 + 3, a4 = a0 + 4, a5 = a0 + 5, a6 = a0 + 6,
+           a7 = a0 + 7;
+    const double b = 0.999999, cc = 1e-7;
+    for (int i = 0; i < iters; ++i) {
+        a0 = fma(a0, b, cc); a1 = fma(a1, b, cc); a2 = fma(a2, b, cc); a3 = fma(a3, b, cc);
+        a4 = fma(a4, b, cc); a5 = fma(a5, b, cc); a6 = fma(a6, b, cc); a7 = fma(a7, b, cc);
+    }
+    const double r = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+    if (r == 1.2345) out[0] = r;
+}
+
+__global__ void k_peak_fp32(float *out, int iters, float seed)
+{
+    float a[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) a[k] = seed + threadIdx.x + k;
+    const float b = 0.9999f, cc = 1e-6f;
+    for (int i = 0; i < iters; ++i)
+#pragma unroll
+        for (int k = 0; k < 16; ++k) a[k] = fmaf(a[k], b, cc);
+    float r = 0.f;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) r += a[k];
+    if (r == 1.2345f) out[0] = r;
+}
+
+__global__ void k_peak_ex2(float *out, int iters, float seed)
+{
+    float a[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a[k] = -seed * (threadIdx.x % 7 + k) * 1e-3f;
+    for (int i = 0; i < iters; ++i)
+#pragma unroll
+        for (int k = 0; k < 8; ++k) a[k] = -ex2_approx(a[k]);
+    float r = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) r += a[k];
+    if (r == 1.2345f) out[0] = r;
+}
+
+sdot_status sdot_measure_peaks(int device, double *out)
+{
+    if (!out) return SDOT_EINVAL;
+    DeviceGuard g(device);
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return SDOT_ECUDA;
+    const int blocks = prop.multiProcessorCount * 8, threads = 256;
+    void *buf = nullptr;
+    if (cudaMalloc(&buf, 64) != cudaSuccess) return SDOT_ENOMEM;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float ms = 0;
+    const int it64 = 4000, it32 = 8000, itx = 8000;
+    // warm-up then timed
+    for (int rep = 0; rep < 2; ++rep) {
+        cudaEventRecord(e0);
+        k_peak_fp64<<<blocks, threads>>>((double *)buf, it64, 0.5);
+        cudaEventRecord(e1);
+        cudaEventSynchronize(e1);
+    }
+    cudaEventElapsedTime(&ms, e0, e1);
+    out[0] = 2.0 * 8.0 * it64 * (double)blocks * threads / (ms * 1e-3) / 1e12;
+    for (int rep = 0; rep < 2; ++rep) {
+        cudaEventRecord(e0);
+        k_peak_fp32<<<blocks, threads>>>((float *)buf, it32, 0.5f);
+        cudaEventRecord(e1);
+        cudaEventSynchronize(e1);
+    }
+    cudaEventElapsedTime(&ms, e0, e1);
+    out[1] = 2.0 * 16.0 * it32 * (double)blocks * threads / (ms * 1e-3) / 1e12;
+    for (int rep = 0; rep < 2; ++rep) {
+        cudaEventRecord(e0);
+        k_peak_ex2<<<blocks, threads>>>((float *)buf, itx, 0.5f);
+        cudaEventRecord(e1);
+        cudaEventSynchronize(e1);
+    }
+    cudaEventElapsedTime(&ms, e0, e1);
+    out[2] = 8.0 * itx * (double)blocks * threads / (ms * 1e-3) / 1e9;
+    int clk = 0;
+    cudaDeviceGetAttribute(&clk, cudaDevAttrClockRate, device);
+    out[3] = clk / 1000.0;
+    cudaError_t e = cudaGetLastError();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(buf);
+    return e == cudaSuccess ? SDOT_OK : SDOT_ECUDA;
 }
 
 double sdot_get_last_functional_value(const sdot_ctx *c) { return c ? c->global_functional : NAN; }

@@ -786,7 +786,7 @@ constexpr int NRED = 8;  // psinu, l1, linf, comp, l2sq, gp, nonfinite, unused
 
 __global__ void __launch_bounds__(FIN_THREADS)
 k_finalize_grad(int64_t nt, int nks, const double *__restrict__ gpart, const double *__restrict__ nu,
-                const double *__restrict__ psi, const double *__restrict__ pdir, double tol,
+                const double *__restrict__ psi, const double *__restrict__ pdir, double tol, int sub_nu,
                 double *__restrict__ grad, double *__restrict__ redpart)
 {
     double psinu = 0.0, l1 = 0.0, linf = 0.0, comp = -CUDART_INF, l2 = 0.0, gp = 0.0, bad = 0.0;
@@ -794,7 +794,7 @@ k_finalize_grad(int64_t nt, int nks, const double *__restrict__ gpart, const dou
         double s = 0.0;
         for (int k = 0; k < nks; ++k) s += gpart[(int64_t)k * nt + j];
         const double g = s - nu[j];
-        grad[j] = g;
+        grad[j] = sub_nu ? g : s;
         psinu += psi[j] * nu[j];
         const double ag = fabs(g);
         l1 += ag;
@@ -866,6 +866,7 @@ k_finalize_scalars(int nred, const double *__restrict__ redpart, int64_t nval, c
         }
         const double psinu = t[3];
         scal[SC_VALUE] = t[0] - psinu;
+        scal[SC_VALSRC] = t[0];
         scal[SC_C] = t[1];
         scal[SC_SKIPPED] = t[2];
         scal[SC_PSINU] = psinu;
@@ -899,12 +900,14 @@ void k_axpy_launch(cudaStream_t s, double *x, const double *x0, double a, const 
 sdot_status launch_gather(sdot_ctx *c, double *dst, const double *src, int64_t n)
 {
     k_gather<<<grid_for(n, 256), 256, 0, c->stream>>>(dst, src, c->perm.p, n);
+    c->klaunch[5] += 1;
     return cuda_error(c, cudaGetLastError(), "gather");
 }
 
 sdot_status launch_scatter(sdot_ctx *c, double *dst, const double *src, int64_t n)
 {
     k_scatter<<<grid_for(n, 256), 256, 0, c->stream>>>(dst, src, c->perm.p, n);
+    c->klaunch[5] += 1;
     return cuda_error(c, cudaGetLastError(), "scatter");
 }
 
@@ -963,11 +966,16 @@ double host_threshold(sdot_ctx *c, double maxpsi, double minpsi)
 }
 
 template <int DIM>
-static sdot_status run_eval(sdot_ctx *c, const EvalArgs &a, bool dense, const double *pdir, double tol)
+static sdot_status run_eval(sdot_ctx *c, const EvalArgs &a, bool dense, const double *pdir, double tol, bool partial)
 {
     cudaStream_t st = c->stream;
     const int prec = c->precision;
+    auto mark = [&](int i) {
+        if (c->profiling) cudaEventRecord(c->pev[i], st);
+    };
+    mark(0);
     k_target_prep<DIM><<<grid_for(a.nt, 256), 256, 0, st>>>(a.nt, c->y.p, c->nu.p, c->psi.p, a, c->tpack.p);
+    mark(1);
     int64_t nval = 0;
     int nks = 1;
     if (dense) {
@@ -975,6 +983,7 @@ static sdot_status run_eval(sdot_ctx *c, const EvalArgs &a, bool dense, const do
         nval = (a.nq + per - 1) / per;
         k_value_dense<DIM><<<(unsigned)nval, DENSE_A_THREADS, 0, st>>>(c->x.p, c->rho.p, c->jxw.p, c->tpack.p, a,
                                                                        c->Lq.p, c->blkpart.p);
+        mark(2);
         // gradient: target blocks x q-slices, ~4 waves of CTAs
         const int64_t tb = (a.nt + DENSE_B_THREADS * DENSE_B_TT - 1) / (DENSE_B_THREADS * DENSE_B_TT);
         int64_t want = (148 * 8 + tb - 1) / tb;
@@ -1008,6 +1017,7 @@ static sdot_status run_eval(sdot_ctx *c, const EvalArgs &a, bool dense, const do
                 c->x.p, c->rho.p, c->jxw.p, c->cell_ctr.p, c->sblk_sph.p, c->tpack.p, c->tblk_sph.p, c->ntblk, a,
                 c->Lq.p, c->blkpart.p);
         }
+        mark(2);
         const int64_t ncblk = c->ncblk;
         const bool fp32 = prec != SDOT_PREC_FP64;
         const int qbytes = fp32 ? (int)(sizeof(float4) + sizeof(float)) : 5 * (int)sizeof(double);
@@ -1027,13 +1037,19 @@ static sdot_status run_eval(sdot_ctx *c, const EvalArgs &a, bool dense, const do
                 a, maxcb, c->gpart.p);
         }
     }
-    k_finalize_grad<<<FIN_BLOCKS, FIN_THREADS, 0, st>>>(a.nt, nks, c->gpart.p, c->nu.p, c->psi.p, pdir, tol, c->grad.p,
-                                                       c->redpart.p);
+    mark(3);
+    k_finalize_grad<<<FIN_BLOCKS, FIN_THREADS, 0, st>>>(a.nt, nks, c->gpart.p, c->nu.p, c->psi.p, pdir, tol,
+                                                       partial ? 0 : 1, c->grad.p, c->redpart.p);
     k_finalize_scalars<<<1, 256, 0, st>>>(FIN_BLOCKS, c->redpart.p, nval, c->blkpart.p, c->scal.p);
+    mark(4);
+    c->klaunch[1] += 1;
+    c->klaunch[2] += 1;
+    c->klaunch[3] += 1;
+    c->klaunch[4] += 2;
     return cuda_error(c, cudaGetLastError(), "evaluate launch");
 }
 
-sdot_status evaluate_internal(sdot_ctx *c, const double *p_dir, double comp_tol, double *ms_out)
+sdot_status evaluate_internal(sdot_ctx *c, const double *p_dir, double comp_tol, double *ms_out, bool partial)
 {
     if (c->dim == 0 || c->nq == 0) return set_error(c, SDOT_ESTATE, "source measure not set");
     if (c->nt == 0) return set_error(c, SDOT_ESTATE, "target measure not set");
@@ -1045,7 +1061,10 @@ sdot_status evaluate_internal(sdot_ctx *c, const double *p_dir, double comp_tol,
                                                                           : vmin_host(c->nu_host)) > 0);
     cudaEventRecord(c->ev0, c->stream);
     double mm[3] = {0, 0, 0};
+    if (c->profiling) cudaEventRecord(c->pev[5], c->stream);
     k_minmax<<<1, 1024, 0, c->stream>>>(c->psi.p, c->nt, c->scal.p + SC_MAXPSI);
+    if (c->profiling) cudaEventRecord(c->pev[6], c->stream);
+    c->klaunch[0] += 1;
     if (may_truncate) {
         cudaError_t e = cudaMemcpyAsync(mm, c->scal.p + SC_MAXPSI, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
@@ -1080,8 +1099,8 @@ sdot_status evaluate_internal(sdot_ctx *c, const double *p_dir, double comp_tol,
         // NaN threshold: the reference's predicate d <= NaN rejects everything
         a.sstar = NAN;
     }
-    sdot_status s = (c->dim == 2) ? run_eval<2>(c, a, dense_ok, p_dir, comp_tol)
-                                  : run_eval<3>(c, a, dense_ok, p_dir, comp_tol);
+    sdot_status s = (c->dim == 2) ? run_eval<2>(c, a, dense_ok, p_dir, comp_tol, partial)
+                                  : run_eval<3>(c, a, dense_ok, p_dir, comp_tol, partial);
     if (s != SDOT_OK) return s;
     cudaEventRecord(c->ev1, c->stream);
     cudaError_t e = cudaMemcpyAsync(c->scal_host, c->scal.p, SC_COUNT * sizeof(double), cudaMemcpyDeviceToHost,
@@ -1092,6 +1111,15 @@ sdot_status evaluate_internal(sdot_ctx *c, const double *p_dir, double comp_tol,
         float ms = 0.f;
         cudaEventElapsedTime(&ms, c->ev0, c->ev1);
         *ms_out = ms;
+    }
+    if (c->profiling) {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, c->pev[5], c->pev[6]);
+        c->kms[0] += t;
+        for (int i = 0; i < 4; ++i) {
+            cudaEventElapsedTime(&t, c->pev[i], c->pev[i + 1]);
+            c->kms[1 + i] += t;
+        }
     }
     c->scal_host[SC_R] = r;
     c->global_functional = c->scal_host[SC_VALUE];

@@ -54,7 +54,8 @@ enum ScalarSlot {
     SC_SSTAR = 13,     // squared-distance bound equivalent to sqrt_rn(d2) <= r
     SC_NONFINITE = 14, // 1 if value or gradient not finite
     SC_PAIRS = 15,     // candidate pairs of the evaluation
-    SC_COUNT = 16
+    SC_VALSRC = 16,    // source part of J (before the linear term)
+    SC_COUNT = 20
 };
 
 template <class T>
@@ -147,6 +148,12 @@ struct sdot_ctx {
     sdot::DevBuf<double> x0, pdir, sk, yk, hist_s, hist_y, gtmp;
 
     int64_t last_pairs = 0;
+
+    // ---- measurement ----
+    bool profiling = false;
+    cudaEvent_t pev[8] = {};
+    double kms[6] = {0, 0, 0, 0, 0, 0};
+    int64_t klaunch[6] = {0, 0, 0, 0, 0, 0};
 };
 
 namespace sdot {
@@ -161,7 +168,7 @@ sdot_status cuda_error(sdot_ctx *c, cudaError_t e, const char *where);
 // on the host (integral/geometric) or NaN to let the device compute the
 // pointwise threshold.
 sdot_status evaluate_internal(sdot_ctx *c, const double *p_dir, double comp_tol,
-                              double *ms_out);
+                              double *ms_out, bool partial = false);
 
 // Threshold for the current psi (host computation mirroring
 // SotSolver::compute_distance_threshold), using device reductions for max/min.

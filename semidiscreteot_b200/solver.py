@@ -178,6 +178,35 @@ class SotSolver:
             hessian_out[...] = H
         return H
 
+    def evaluate_partial_device(self, psi_ptr: int, out_ptr: int) -> dict:
+        """Source-shard evaluation into out[n_targets + 3] on the device (see
+        sdot_evaluate_partial_device); the caller all-reduces and finishes."""
+        info = _lib.EvalInfo()
+        self._check(self._L.sdot_evaluate_partial_device(self._h, C.c_void_p(psi_ptr), C.c_void_p(out_ptr),
+                                                         C.byref(info)))
+        self.last_eval_info = {"value": info.value, "C_global": info.C_global, "threshold": info.threshold,
+                               "n_pairs": info.n_pairs, "device_ms": info.device_ms}
+        return self.last_eval_info
+
+    def set_state(self, global_functional: float, C_global: float):
+        self._check(self._L.sdot_set_state(self._h, float(global_functional), float(C_global)))
+
+    # ------------------------------------------------------------ measurement
+    @property
+    def stream_handle(self) -> int:
+        return int(self._L.sdot_get_stream(self._h) or 0)
+
+    def set_profiling(self, enable: bool = True):
+        self._check(self._L.sdot_set_profiling(self._h, int(enable)))
+
+    PHASES = ("threshold", "target_prep", "value_sweep", "gradient_sweep", "finalize", "layout")
+
+    def kernel_times(self, reset: bool = False) -> dict:
+        ms = np.zeros(6)
+        ln = np.zeros(6, dtype=np.int64)
+        self._check(self._L.sdot_get_kernel_times(self._h, ms.ctypes.data, ln.ctypes.data, 6, int(reset)))
+        return {k: {"ms": float(ms[i]), "launches": int(ln[i])} for i, k in enumerate(self.PHASES)}
+
     # ---------------------------------------------------------------- getters
     def get_last_functional_value(self) -> float:
         return self._L.sdot_get_last_functional_value(self._h)
@@ -201,6 +230,17 @@ class SotSolver:
         r = C.c_double(0.0)
         self._check(self._L.sdot_compute_covering_radius(self._h, C.byref(r)))
         return r.value
+
+    @staticmethod
+    def measure_peaks(device: int = 0) -> dict:
+        """Own microbenchmarks: FP64/FP32 FMA TFLOP/s, MUFU ex2 Gop/s, SM clock."""
+        L = _lib.load()
+        out = np.zeros(4)
+        st = L.sdot_measure_peaks(int(device), out.ctypes.data)
+        if st != _lib.SDOT_OK:
+            raise _lib.SdotError(st, "sdot_measure_peaks failed")
+        return {"fp64_tflops": float(out[0]), "fp32_tflops": float(out[1]), "ex2_gops": float(out[2]),
+                "sm_clock_mhz": float(out[3])}
 
     def compute_geometric_radius_bound(self, potentials, epsilon: float, tolerance: float) -> float:
         psi = _f64(potentials)
