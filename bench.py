@@ -339,7 +339,9 @@ def run_ours(args):
     local_pairs = lib.last_eval_info["n_pairs"]
     if tv >= tg:
         ach = VALUE_FLOPS_PER_PAIR[dim] * local_pairs / (tv * 1e-3) / 1e12
-        roof = {"kernel": "value sweep (k_value_%s, FP64 exp2)" % ("dense" if prm.tau <= 0 else "trunc"),
+        kname = ("k_value_dense (FP64 exp2 value sweep)" if prm.tau <= 0 else
+                 "k_fused (FP64 exp2 value sweep + FP32 ex2 gradient sweep, one kernel)")
+        roof = {"kernel": kname,
                 "bound": "fp64", "achieved": ach, "peak": peaks["fp64_tflops"], "unit": "TFLOP/s",
                 "frac": ach / peaks["fp64_tflops"],
                 "traffic": read_traffic("value_sweep", wl["name"]),

@@ -55,38 +55,56 @@ struct DeviceGuard {
     }
 };
 
-// Interleave the low 21 bits of three coordinates (2D: two coordinates, 31 bits).
-uint64_t morton(const double *p, int dim, const double *lo, const double *hi)
+// k-d tree order of n points: recursive split at the balanced position along
+// the widest axis until a node holds at most `leaf` points.  Returns the
+// point order and the leaf boundaries (DFS order, spatially coherent).
+void kd_split(const std::vector<double> &pts, int dim, std::vector<int64_t> &idx, int64_t a, int64_t b, int64_t leaf,
+              std::vector<int64_t> &bounds)
 {
-    uint64_t code = 0;
-    const int bits = dim == 3 ? 21 : 31;
-    const double scale = (double)((1u << (bits < 31 ? bits : 31)) - 1);
-    uint64_t q[3] = {0, 0, 0};
-    for (int d = 0; d < dim; ++d) {
-        const double ext = hi[d] - lo[d];
-        double t = ext > 0 ? (p[d] - lo[d]) / ext : 0.0;
-        t = std::min(std::max(t, 0.0), 1.0);
-        q[d] = (uint64_t)(t * scale);
+    const int64_t count = b - a;
+    if (count <= leaf) {
+        bounds.push_back(a);
+        return;
     }
-    for (int b = bits - 1; b >= 0; --b)
-        for (int d = dim - 1; d >= 0; --d) code = (code << 1) | ((q[d] >> b) & 1u);
-    return code;
+    double lo[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, hi[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+    for (int64_t i = a; i < b; ++i)
+        for (int d = 0; d < dim; ++d) {
+            lo[d] = std::min(lo[d], pts[idx[i] * dim + d]);
+            hi[d] = std::max(hi[d], pts[idx[i] * dim + d]);
+        }
+    int ax = 0;
+    for (int d = 1; d < dim; ++d)
+        if (hi[d] - lo[d] > hi[ax] - lo[ax]) ax = d;
+    const int64_t nleaves = (count + leaf - 1) / leaf;
+    const int64_t m = a + (nleaves / 2) * leaf;
+    std::nth_element(idx.begin() + a, idx.begin() + m, idx.begin() + b, [&](int64_t u, int64_t v) {
+        const double pu = pts[u * dim + ax], pv = pts[v * dim + ax];
+        return pu < pv || (pu == pv && u < v);
+    });
+    kd_split(pts, dim, idx, a, m, leaf, bounds);
+    kd_split(pts, dim, idx, m, b, leaf, bounds);
 }
 
-std::vector<int64_t> morton_order(const std::vector<double> &pts, int dim, int64_t n)
+std::vector<int64_t> kd_order(const std::vector<double> &pts, int dim, int64_t n, int64_t leaf,
+                              std::vector<int64_t> &bounds)
 {
-    double lo[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, hi[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
-    for (int64_t i = 0; i < n; ++i)
-        for (int d = 0; d < dim; ++d) {
-            lo[d] = std::min(lo[d], pts[i * dim + d]);
-            hi[d] = std::max(hi[d], pts[i * dim + d]);
-        }
-    std::vector<uint64_t> code(n);
-    for (int64_t i = 0; i < n; ++i) code[i] = morton(&pts[i * dim], dim, lo, hi);
-    std::vector<int64_t> ord(n);
-    std::iota(ord.begin(), ord.end(), 0);
-    std::stable_sort(ord.begin(), ord.end(), [&](int64_t a, int64_t b) { return code[a] < code[b]; });
-    return ord;
+    std::vector<int64_t> idx(n);
+    std::iota(idx.begin(), idx.end(), 0);
+    bounds.clear();
+    kd_split(pts, dim, idx, 0, n, leaf, bounds);
+    bounds.push_back(n);
+    return idx;
+}
+
+float4 sphere32(const double *s, double scale)
+{
+    // FP32 copy enlarged by the rounding of the centre and a relative margin
+    float4 r;
+    r.x = (float)s[0];
+    r.y = (float)s[1];
+    r.z = (float)s[2];
+    r.w = (float)(s[3] * (1.0 + 1e-5) + 1e-5 * scale);
+    return r;
 }
 
 // Bounding sphere (bbox centre, max distance, enlarged by 1e-12 relative).
@@ -133,12 +151,23 @@ void update_geometry(sdot_ctx *c)
         if (d < c->dim) s += (hi[d] - lo[d]) * (hi[d] - lo[d]);
     }
     c->diam = std::sqrt(s) * (1.0 + 1e-12);
+    double sc = 1e-30;
+    for (int d = 0; d < c->dim; ++d) sc = std::max(sc, std::max(std::fabs(lo[d]), std::fabs(hi[d])));
+    c->coord_scale = sc;
+    // conservative FP32 spheres depend on the common coordinate scale
+    std::vector<float4> s32(c->nsblk), t32(c->ntblk);
+    for (int64_t b = 0; b < c->nsblk; ++b) s32[b] = sphere32(&c->src_sph_host[b * 4], sc);
+    for (int64_t b = 0; b < c->ntblk; ++b) t32[b] = sphere32(&c->tgt_sph_host[b * 4], sc);
+    cudaMemcpy(c->sblk_sph32.p, s32.data(), s32.size() * sizeof(float4), cudaMemcpyHostToDevice);
+    cudaMemcpy(c->tblk_sph32.p, t32.data(), t32.size() * sizeof(float4), cudaMemcpyHostToDevice);
 }
 
 size_t device_bytes(const sdot_ctx *c)
 {
-    return c->x.bytes() + c->rho.bytes() + c->jxw.bytes() + c->w.bytes() + c->lw.bytes() + c->cell_ctr.bytes() +
-           c->sblk_sph.bytes() + c->cblk_sph.bytes() + c->y.bytes() + c->nu.bytes() + c->perm.bytes() +
+    return c->x.bytes() + c->rho.bytes() + c->jxw.bytes() + c->w.bytes() + c->cell_ctr.bytes() +
+           c->sblk_sph.bytes() + c->sblk_sph32.bytes() + c->sblk_cell.bytes() + c->tblk_off.bytes() +
+           c->tblk_sph32.bytes() + c->part.bytes() + c->fwd_t.bytes() + c->inv_b.bytes() +
+           c->y.bytes() + c->nu.bytes() + c->perm.bytes() +
            c->tblk_sph.bytes() + c->psi.bytes() + c->grad.bytes() + c->tpack.bytes() + c->Lq.bytes() +
            c->gpart.bytes() + c->blkpart.bytes() + c->scal.bytes() + c->redpart.bytes() + c->io_a.bytes() +
            c->io_b.bytes() + c->x0.bytes() + c->pdir.bytes() + c->sk.bytes() + c->yk.bytes() + c->hist_s.bytes() +
@@ -358,8 +387,11 @@ void sdot_destroy(sdot_ctx *c)
     {
         DeviceGuard g(c->device);
         if (c->stream) cudaStreamSynchronize(c->stream);
-        c->x.release(); c->rho.release(); c->jxw.release(); c->w.release(); c->lw.release();
-        c->cell_ctr.release(); c->sblk_sph.release(); c->cblk_sph.release(); c->y.release(); c->nu.release();
+        c->x.release(); c->rho.release(); c->jxw.release(); c->w.release();
+        c->cell_ctr.release(); c->sblk_sph.release(); c->sblk_sph32.release(); c->sblk_cell.release();
+        c->tblk_off.release(); c->tblk_sph32.release(); c->part.release(); c->fwd_t.release(); c->inv_b.release();
+        c->fwd_cnt.release(); c->inv_cnt.release(); c->fwd_off.release(); c->inv_off.release();
+        c->y.release(); c->nu.release();
         c->perm.release(); c->tblk_sph.release(); c->psi.release(); c->grad.release(); c->tpack.release();
         c->Lq.release(); c->gpart.release(); c->blkpart.release(); c->scal.release(); c->redpart.release();
         c->io_a.release(); c->io_b.release(); c->x0.release(); c->pdir.release(); c->sk.release(); c->yk.release();
@@ -394,8 +426,15 @@ sdot_status sdot_set_source(sdot_ctx *c, int dim, int64_t n_q, const double *x, 
         !all_finite(cell_centers, n_cells * dim))
         return set_error(c, SDOT_ENONFINITE, "set_source: non-finite input");
     DeviceGuard g(c->device);
+    // value-sweep warp units: <= 9 quadrature points each
+    int ql;
+    if (qpc <= 9) ql = (int)qpc;
+    else ql = (qpc % 9 == 0) ? 9 : 8;
+    const int ngroups = (int)((qpc + ql - 1) / ql);
+    const int64_t leaf_cells = std::max<int64_t>(1, SBLK_UNITS / ngroups);
     std::vector<double> ctr(cell_centers, cell_centers + n_cells * dim);
-    const std::vector<int64_t> ord = morton_order(ctr, dim, n_cells);
+    std::vector<int64_t> bounds;
+    const std::vector<int64_t> ord = kd_order(ctr, dim, n_cells, leaf_cells, bounds);
     std::vector<double> hx(n_q * dim), hr(n_q), hj(n_q), hw(n_q), hc(n_cells * dim);
     bool nonneg = true;
     for (int64_t k = 0; k < n_cells; ++k) {
@@ -410,29 +449,12 @@ sdot_status sdot_set_source(sdot_ctx *c, int dim, int64_t n_q, const double *x, 
             if (hw[qd] < 0) nonneg = false;
         }
     }
-    // value-sweep units and blocks
-    int ql;
-    if (qpc <= 4) ql = (int)qpc;
-    else if (qpc <= 9) ql = (int)qpc;
-    else ql = (qpc % 9 == 0) ? 9 : 8;
-    const int ngroups = (int)((qpc + ql - 1) / ql);
-    const int64_t nunits = n_cells * ngroups;
-    const int64_t nsblk = (nunits + SBLK_CELLS - 1) / SBLK_CELLS;
+    const int64_t nsblk = (int64_t)bounds.size() - 1;
     std::vector<double> ssph(nsblk * 4);
     for (int64_t b = 0; b < nsblk; ++b) {
         std::vector<int64_t> cells;
-        for (int64_t u = b * SBLK_CELLS; u < std::min(nunits, (b + 1) * SBLK_CELLS); ++u) {
-            const int64_t cl = u / ngroups;
-            if (cells.empty() || cells.back() != cl) cells.push_back(cl);
-        }
+        for (int64_t k = bounds[b]; k < bounds[b + 1]; ++k) cells.push_back(k);
         sphere_of(hc.data(), cells, dim, &ssph[b * 4]);
-    }
-    const int64_t ncblk = (n_cells + SBLK_CELLS - 1) / SBLK_CELLS;
-    std::vector<double> csph(ncblk * 4);
-    for (int64_t b = 0; b < ncblk; ++b) {
-        std::vector<int64_t> cells;
-        for (int64_t k = b * SBLK_CELLS; k < std::min(n_cells, (b + 1) * SBLK_CELLS); ++k) cells.push_back(k);
-        sphere_of(hc.data(), cells, dim, &csph[b * 4]);
     }
     c->dim = dim;
     c->nq = n_q;
@@ -441,7 +463,6 @@ sdot_status sdot_set_source(sdot_ctx *c, int dim, int64_t n_q, const double *x, 
     c->ql = ql;
     c->ngroups = ngroups;
     c->nsblk = nsblk;
-    c->ncblk = ncblk;
     c->w_nonneg = nonneg;
     for (int d = 0; d < 3; ++d) {
         c->src_lo[d] = DBL_MAX;
@@ -454,7 +475,7 @@ sdot_status sdot_set_source(sdot_ctx *c, int dim, int64_t n_q, const double *x, 
         }
     for (int d = dim; d < 3; ++d) c->src_lo[d] = c->src_hi[d] = 0.0;
     c->cell_ctr_host = hc;
-    const size_t need = (size_t)(n_q * (dim + 4) + n_cells * dim + (nsblk + ncblk) * 4) * sizeof(double);
+    const size_t need = (size_t)(n_q * (dim + 4) + n_cells * dim + nsblk * 7) * sizeof(double);
     if (c->budget && need > c->budget) return set_error(c, SDOT_EBUDGET, "set_source: exceeds the memory budget");
     CK(c->x.alloc(n_q * dim), "alloc x");
     CK(c->rho.alloc(n_q), "alloc rho");
@@ -462,14 +483,16 @@ sdot_status sdot_set_source(sdot_ctx *c, int dim, int64_t n_q, const double *x, 
     CK(c->w.alloc(n_q), "alloc w");
     CK(c->cell_ctr.alloc(n_cells * dim), "alloc cells");
     CK(c->sblk_sph.alloc(nsblk * 4), "alloc spheres");
-    CK(c->cblk_sph.alloc(ncblk * 4), "alloc spheres");
+    CK(c->sblk_sph32.alloc(nsblk), "alloc spheres");
+    CK(c->sblk_cell.alloc(nsblk + 1), "alloc blocks");
     CK(cudaMemcpy(c->x.p, hx.data(), hx.size() * 8, cudaMemcpyHostToDevice), "copy x");
     CK(cudaMemcpy(c->rho.p, hr.data(), hr.size() * 8, cudaMemcpyHostToDevice), "copy rho");
     CK(cudaMemcpy(c->jxw.p, hj.data(), hj.size() * 8, cudaMemcpyHostToDevice), "copy jxw");
     CK(cudaMemcpy(c->w.p, hw.data(), hw.size() * 8, cudaMemcpyHostToDevice), "copy w");
     CK(cudaMemcpy(c->cell_ctr.p, hc.data(), hc.size() * 8, cudaMemcpyHostToDevice), "copy cells");
     CK(cudaMemcpy(c->sblk_sph.p, ssph.data(), ssph.size() * 8, cudaMemcpyHostToDevice), "copy spheres");
-    CK(cudaMemcpy(c->cblk_sph.p, csph.data(), csph.size() * 8, cudaMemcpyHostToDevice), "copy spheres");
+    CK(cudaMemcpy(c->sblk_cell.p, bounds.data(), bounds.size() * 8, cudaMemcpyHostToDevice), "copy blocks");
+    c->src_sph_host = ssph;
     c->covering_radius = 0.0;  // reference: recomputed by the next solve
     update_geometry(c);
     return SDOT_OK;
@@ -486,27 +509,32 @@ sdot_status sdot_set_target(sdot_ctx *c, int64_t n, const double *y, const doubl
         if (nu[i] < 0) return set_error(c, SDOT_EINVAL, "set_target: negative target weight");
     DeviceGuard g(c->device);
     std::vector<double> yy(y, y + n * dim);
-    const std::vector<int64_t> ord = morton_order(yy, dim, n);
+    std::vector<int64_t> bounds;
+    const std::vector<int64_t> ord = kd_order(yy, dim, n, TBLK_KD, bounds);
     std::vector<double> hy(n * dim), hn(n);
     for (int64_t k = 0; k < n; ++k) {
         for (int d = 0; d < dim; ++d) hy[k * dim + d] = y[ord[k] * dim + d];
         hn[k] = nu[ord[k]];
     }
-    const int64_t ntblk = (n + TBLK - 1) / TBLK;
+    const int64_t ntblk = (int64_t)bounds.size() - 1;
     std::vector<double> tsph(ntblk * 4);
     for (int64_t b = 0; b < ntblk; ++b) {
         std::vector<int64_t> idx;
-        for (int64_t k = b * TBLK; k < std::min(n, (b + 1) * TBLK); ++k) idx.push_back(k);
+        for (int64_t k = bounds[b]; k < bounds[b + 1]; ++k) idx.push_back(k);
         sphere_of(hy.data(), idx, dim, &tsph[b * 4]);
     }
     CK(c->y.alloc(n * dim), "alloc y");
     CK(c->nu.alloc(n), "alloc nu");
     CK(c->perm.alloc(n), "alloc perm");
     CK(c->tblk_sph.alloc(ntblk * 4), "alloc spheres");
+    CK(c->tblk_sph32.alloc(ntblk), "alloc spheres");
+    CK(c->tblk_off.alloc(ntblk + 1), "alloc blocks");
     CK(cudaMemcpy(c->y.p, hy.data(), hy.size() * 8, cudaMemcpyHostToDevice), "copy y");
     CK(cudaMemcpy(c->nu.p, hn.data(), hn.size() * 8, cudaMemcpyHostToDevice), "copy nu");
     CK(cudaMemcpy(c->perm.p, ord.data(), ord.size() * 8, cudaMemcpyHostToDevice), "copy perm");
     CK(cudaMemcpy(c->tblk_sph.p, tsph.data(), tsph.size() * 8, cudaMemcpyHostToDevice), "copy spheres");
+    CK(cudaMemcpy(c->tblk_off.p, bounds.data(), bounds.size() * 8, cudaMemcpyHostToDevice), "copy blocks");
+    c->tgt_sph_host = tsph;
     c->nt = n;
     c->ntblk = ntblk;
     c->nu_host.assign(nu, nu + n);
@@ -989,12 +1017,12 @@ sdot_status sdot_set_profiling(sdot_ctx *c, int enable)
 sdot_status sdot_get_kernel_times(sdot_ctx *c, double *ms, int64_t *launches, int n, int reset)
 {
     if (!c) return SDOT_EINVAL;
-    for (int i = 0; i < n && i < 6; ++i) {
+    for (int i = 0; i < n && i < 8; ++i) {
         if (ms) ms[i] = c->kms[i];
         if (launches) launches[i] = c->klaunch[i];
     }
     if (reset)
-        for (int i = 0; i < 6; ++i) {
+        for (int i = 0; i < 8; ++i) {
             c->kms[i] = 0.0;
             c->klaunch[i] = 0;
         }

@@ -6,6 +6,8 @@
 #include <math_constants.h>
 #include <stdint.h>
 
+#include "sdot_internal.h"
+
 namespace sdot {
 
 // 2^(k/16), k = 0..15, correctly rounded.  Kept in shared memory by every
@@ -113,5 +115,72 @@ struct EvalArgs {
     double c32;       // log2(e) / (2 eps) (FP32 gradient sweep)
     double l2e_eps;   // log2(e) / eps
 };
+
+// ---------------------------------------------------------------------------
+// per-q epilogue of the value sweep (SotSolver.cc:843-866 + lambda :274-286)
+// ---------------------------------------------------------------------------
+
+// mx: max scaled exponent (without C_q); S: sum relative to mx.
+__device__ __forceinline__ void value_epilogue(const EvalArgs &a, double mx, double S, double Cq,
+                                               double rho, double jxw, double &val, double &cval,
+                                               double &L, int &skipped)
+{
+    val = 0.0;
+    cval = 0.0;
+    L = CUDART_INF;
+    skipped = 1;
+    if (mx == -CUDART_INF) return;           // no candidates: cell skipped (:802)
+    const double m_ref = (mx + Cq) * (1.0 / KAPPA);
+    if (a.lse) {
+        if (!(S > 0.0)) return;              // total_sum_exp <= 0 (:846)
+        const double lt = m_ref + log(S);
+        val = rho * a.eps * lt * jxw;
+        cval = rho * jxw / S;
+        L = lt;
+    } else {
+        const double total = S * exp(m_ref);  // sum of unshifted terms
+        if (!(total > 0.0)) return;
+        const double lt = log(total);
+        val = rho * a.eps * lt * jxw;
+        cval = rho * jxw / total;
+        L = lt;
+    }
+    skipped = 0;
+}
+
+// One online-LSE update in scaled units (b relative to the unit's C_q).
+__device__ __forceinline__ void lse_update(double b, double nu, double &M, double &S, double &mx,
+                                           const double *tab)
+{
+    mx = fmax(mx, b);
+    double u = b - M;
+    if (u > LSE_THR) {
+        S = S * exp2_16(M - b, tab);
+        M = b;
+        u = 0.0;
+    }
+    S = fma(nu, exp2_16(u, tab), S);
+}
+
+// Block-level ordered sum of (value, C, skipped, pairs) -> part[blockIdx.x*4..].
+__device__ __forceinline__ void block_partials(double v, double c, double sk, double np, double *part)
+{
+    __shared__ double sv[32], sc[32], ss[32], sp[32];
+    v = warp_sum(v);
+    c = warp_sum(c);
+    sk = warp_sum(sk);
+    np = warp_sum(np);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) { sv[w] = v; sc[w] = c; ss[w] = sk; sp[w] = np; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tv = 0.0, tc = 0.0, ts = 0.0, tp = 0.0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) { tv += sv[i]; tc += sc[i]; ts += ss[i]; tp += sp[i]; }
+        part[blockIdx.x * 4 + 0] = tv;
+        part[blockIdx.x * 4 + 1] = tc;
+        part[blockIdx.x * 4 + 2] = ts;
+        part[blockIdx.x * 4 + 3] = tp;
+    }
+}
 
 }  // namespace sdot

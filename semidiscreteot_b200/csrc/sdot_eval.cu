@@ -107,70 +107,18 @@ __global__ void k_target_prep(int64_t nt, const double *__restrict__ y, const do
     }
 }
 
-// ---------------------------------------------------------------------------
-// per-q epilogue of the value sweep (SotSolver.cc:843-866 + lambda :274-286)
-// ---------------------------------------------------------------------------
-
-// mx: max scaled exponent (without C_q); S: sum relative to mx.
-__device__ __forceinline__ void value_epilogue(const EvalArgs &a, double mx, double S, double Cq,
-                                               double rho, double jxw, double &val, double &cval,
-                                               double &L, int &skipped)
+// truncated-path layout: {y(3), nu, log2 nu, kappa psi / eps}
+template <int DIM>
+__global__ void k_target_prep_kd(int64_t nt, const double *__restrict__ y, const double *__restrict__ nu,
+                                 const double *__restrict__ psi, EvalArgs a, double *__restrict__ tpack)
 {
-    val = 0.0;
-    cval = 0.0;
-    L = CUDART_INF;
-    skipped = 1;
-    if (mx == -CUDART_INF) return;           // no candidates: cell skipped (:802)
-    const double m_ref = (mx + Cq) * (1.0 / KAPPA);
-    if (a.lse) {
-        if (!(S > 0.0)) return;              // total_sum_exp <= 0 (:846)
-        const double lt = m_ref + log(S);
-        val = rho * a.eps * lt * jxw;
-        cval = rho * jxw / S;
-        L = lt;
-    } else {
-        const double total = S * exp(m_ref);  // sum of unshifted terms
-        if (!(total > 0.0)) return;
-        const double lt = log(total);
-        val = rho * a.eps * lt * jxw;
-        cval = rho * jxw / total;
-        L = lt;
-    }
-    skipped = 0;
-}
-
-// One online-LSE update in scaled units (b relative to the unit's C_q).
-__device__ __forceinline__ void lse_update(double b, double nu, double &M, double &S, double &mx,
-                                           const double *tab)
-{
-    mx = fmax(mx, b);
-    double u = b - M;
-    if (u > LSE_THR) {
-        S = S * exp2_16(M - b, tab);
-        M = b;
-        u = 0.0;
-    }
-    S = fma(nu, exp2_16(u, tab), S);
-}
-
-// Block-level ordered sum of (value, C, skipped, pairs) -> part[blockIdx.x*4..].
-__device__ __forceinline__ void block_partials(double v, double c, double sk, double np, double *part)
-{
-    __shared__ double sv[32], sc[32], ss[32], sp[32];
-    v = warp_sum(v);
-    c = warp_sum(c);
-    sk = warp_sum(sk);
-    np = warp_sum(np);
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    if (l == 0) { sv[w] = v; sc[w] = c; ss[w] = sk; sp[w] = np; }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double tv = 0.0, tc = 0.0, ts = 0.0, tp = 0.0;
-        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) { tv += sv[i]; tc += sc[i]; ts += ss[i]; tp += sp[i]; }
-        part[blockIdx.x * 4 + 0] = tv;
-        part[blockIdx.x * 4 + 1] = tc;
-        part[blockIdx.x * 4 + 2] = ts;
-        part[blockIdx.x * 4 + 3] = tp;
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nt; j += (int64_t)gridDim.x * blockDim.x) {
+        double *t = tpack + j * TPACK;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) t[d] = d < DIM ? y[j * DIM + d] : 0.0;
+        t[3] = nu[j];
+        t[4] = log2(nu[j]);
+        t[5] = a.s * psi[j];
     }
 }
 
@@ -248,179 +196,6 @@ k_value_dense(const double *__restrict__ x, const double *__restrict__ rho, cons
         }
     }
     block_partials(tv, tc, ts, 0.0, part);
-}
-
-// ---------------------------------------------------------------------------
-// value sweep, truncated: CTA <-> 8 warp units (cell, q-group); candidate
-// target blocks culled by bounding spheres and staged in shared memory; each
-// warp applies the exact per-cell test, compacts its candidates in order and
-// walks them with lane <-> target, every lane holding all q of its unit.
-// ---------------------------------------------------------------------------
-
-constexpr int VT_WARPS = 8;
-constexpr int VT_MAXTB = 16;                 // target blocks staged per round
-constexpr int VT_STG = VT_MAXTB * TBLK;      // staged targets per round (1024)
-
-struct VTSmem {
-    double tab[16];
-    double stg[VT_STG * TPACK];
-    double xw[VT_WARPS][9][4];
-    unsigned short cand[VT_WARPS][VT_STG];
-    int tblist[VT_MAXTB];
-    int wcount[VT_WARPS];
-    int ctl[4];
-};
-
-// Deterministic block-wide compaction of the blocks that pass the sphere
-// cull, continuing from *next; at most cap entries.  Returns the count.
-__device__ __forceinline__ int cull_blocks(const double *sph, int64_t nblk, const double *c, double R,
-                                           double cullr, int *list, int cap, int64_t &next, int *wcount,
-                                           int *ctl)
-{
-    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    const int nw = blockDim.x >> 5;
-    int cnt = 0;
-    while (next < nblk && cnt < cap) {
-        const int64_t idx = next + tid;
-        bool flag = false;
-        if (idx < nblk) {
-            const double *s = sph + idx * 4;
-            const double d0 = s[0] - c[0], d1 = s[1] - c[1], d2 = s[2] - c[2];
-            const double d = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
-            const double lim = (cullr + R + s[3]) * (1.0 + 1e-12) + 1e-300;
-            flag = (d <= lim) || !(d == d);
-        }
-        const unsigned bal = __ballot_sync(0xffffffffu, flag);
-        if (lane == 0) wcount[w] = __popc(bal);
-        __syncthreads();
-        int off = cnt, tot = 0;
-        for (int i = 0; i < nw; ++i) {
-            if (i < w) off += wcount[i];
-            tot += wcount[i];
-        }
-        const int pos = off + __popc(bal & ((1u << lane) - 1u));
-        if (flag && pos < cap) list[pos] = (int)idx;
-        if (flag && pos == cap) ctl[0] = (int)(idx);
-        __syncthreads();
-        if (cnt + tot > cap) {
-            next = ctl[0];
-            cnt = cap;
-        } else {
-            cnt += tot;
-            next += blockDim.x;
-        }
-        __syncthreads();
-    }
-    return cnt;
-}
-
-template <int DIM, int QL>
-__global__ void __launch_bounds__(VT_WARPS * 32)
-k_value_trunc(const double *__restrict__ x, const double *__restrict__ rho, const double *__restrict__ jxw,
-              const double *__restrict__ cell_ctr, const double *__restrict__ sblk_sph,
-              const double *__restrict__ tpack, const double *__restrict__ tblk_sph, int64_t ntblk,
-              EvalArgs a, double *__restrict__ Lq, double *__restrict__ part)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    VTSmem &sm = *reinterpret_cast<VTSmem *>(smem_raw);
-    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    if (tid < 16) sm.tab[tid] = c_exp2_tab[tid];
-
-    const int64_t unit = (int64_t)blockIdx.x * VT_WARPS + w;
-    const bool valid = unit < a.nunits;
-    const int64_t cell = valid ? unit / a.ngroups : 0;
-    const int grp = valid ? (int)(unit - cell * a.ngroups) : 0;
-    const int64_t q0 = cell * a.qpc + (int64_t)grp * a.ql;
-    const int nql = valid ? min(a.ql, a.qpc - grp * a.ql) : 0;
-    double cc[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) cc[d] = cell_ctr[cell * DIM + d];
-    if (lane < QL) {
-#pragma unroll
-        for (int d = 0; d < 3; ++d)
-            sm.xw[w][lane][d] = (lane < nql && d < DIM) ? x[(q0 + lane) * DIM + d] - a.o[d] : 0.0;
-    }
-    const double *bs = sblk_sph + (int64_t)blockIdx.x * 4;
-    const double bc[3] = {bs[0], bs[1], bs[2]};
-    const double bR = bs[3];
-
-    double M[QL], S[QL], mx[QL];
-#pragma unroll
-    for (int k = 0; k < QL; ++k) { M[k] = -CUDART_INF; S[k] = 0.0; mx[k] = -CUDART_INF; }
-
-    int64_t next = 0;
-    double npairs = 0.0;
-    while (true) {
-        const int ntb = cull_blocks(tblk_sph, ntblk, bc, bR, a.cull, sm.tblist, VT_MAXTB, next, sm.wcount,
-                                    sm.ctl);
-        if (ntb == 0) break;
-        // stage the targets of the listed blocks
-        int nstg = 0;
-        for (int b = 0; b < ntb; ++b) {
-            const int64_t t0 = (int64_t)sm.tblist[b] * TBLK;
-            const int tn = (int)min((int64_t)TBLK, a.nt - t0);
-            const double *src = tpack + t0 * TPACK;
-            double *dst = sm.stg + (int64_t)nstg * TPACK;
-            for (int i = tid; i < tn * TPACK; i += blockDim.x) dst[i] = src[i];
-            nstg += tn;
-        }
-        __syncthreads();
-        // exact per-cell candidate test + in-order compaction (one warp per unit)
-        int ncand = 0;
-        if (valid) {
-            for (int b0 = 0; b0 < nstg; b0 += 32) {
-                const int t = b0 + lane;
-                bool in = false;
-                if (t < nstg) in = dist2_exact<DIM>(sm.stg + t * TPACK + 2 + DIM, cc) <= a.sstar;
-                const unsigned bal = __ballot_sync(0xffffffffu, in);
-                if (in) sm.cand[w][ncand + __popc(bal & ((1u << lane) - 1u))] = (unsigned short)t;
-                ncand += __popc(bal);
-            }
-            __syncwarp();
-            npairs += (double)ncand * nql;
-            for (int p = lane; p < ncand; p += 32) {
-                const double *tp = sm.stg + sm.cand[w][p] * TPACK;
-                const double A = tp[0];
-                double B[DIM];
-#pragma unroll
-                for (int d = 0; d < DIM; ++d) B[d] = tp[1 + d];
-                const double nuj = tp[1 + DIM];
-#pragma unroll
-                for (int k = 0; k < QL; ++k) {
-                    if (k < nql) {
-                        double b = fma(B[0], sm.xw[w][k][0], A);
-#pragma unroll
-                        for (int d = 1; d < DIM; ++d) b = fma(B[d], sm.xw[w][k][d], b);
-                        lse_update(b, nuj, M[k], S[k], mx[k], sm.tab);
-                    }
-                }
-            }
-        }
-        __syncthreads();
-    }
-    // merge the lanes of each unit, then per-q epilogue on lane k
-    double tv = 0.0, tc = 0.0, ts = 0.0;
-#pragma unroll
-    for (int k = 0; k < QL; ++k) {
-        const double mxw = warp_max(mx[k]);
-        const double sl = (M[k] == -CUDART_INF || mxw == -CUDART_INF) ? 0.0 : S[k] * exp2_16(M[k] - mxw, sm.tab);
-        const double Sw = warp_sum(sl);
-        if (valid && k < nql && lane == 0) {
-            const int64_t q = q0 + k;
-            double xsq = 0.0;
-#pragma unroll
-            for (int d = 0; d < DIM; ++d) xsq += sm.xw[w][k][d] * sm.xw[w][k][d];
-            const double Cq = -a.halfs * xsq;
-            double v, cv, L;
-            int sk;
-            value_epilogue(a, mxw, Sw, Cq, rho[q], jxw[q], v, cv, L, sk);
-            Lq[q] = L;
-            tv += v;
-            tc += cv;
-            ts += sk;
-        }
-    }
-    block_partials(tv, tc, ts, lane == 0 ? npairs : 0.0, part);
 }
 
 // ---------------------------------------------------------------------------
@@ -599,183 +374,6 @@ k_grad_dense(const double *__restrict__ x, const double *__restrict__ w, const d
 }
 
 // ---------------------------------------------------------------------------
-// gradient sweep, truncated: CTA <-> target block (TBLK targets, 8 warps x 8
-// targets); candidate cell blocks culled by spheres and staged; each warp
-// compacts the exact candidate cells of its target and walks the flattened
-// (cell, q) pairs with all 32 lanes.
-// ---------------------------------------------------------------------------
-
-constexpr int GT_WARPS = 8;
-constexpr int GT_TPW = TBLK / GT_WARPS;   // targets per warp
-constexpr int GT_MAXQ = 4096;             // staged quadrature points per round (FP32 data)
-constexpr int GT_MAXQ64 = 2048;           // staged quadrature points per round (FP64 data)
-constexpr int GT_MAXCELL = 512;           // staged cells per round
-
-struct GTSmem {
-    double tab[16];
-    double cctr[GT_MAXCELL * 3];
-    double acc[GT_WARPS][GT_TPW][32];     // per-lane FP64 accumulators, persist across rounds
-    int cblist[GT_MAXCELL / SBLK_CELLS];
-    unsigned short cand[GT_WARPS][GT_MAXCELL];
-    int wcount[GT_WARPS];
-    int ctl[4];
-    double red[GT_WARPS];
-    // followed by the staged quadrature data (float4 + float, or 5 doubles)
-};
-
-template <int DIM, bool FP32>
-__global__ void __launch_bounds__(GT_WARPS * 32)
-k_grad_trunc(const double *__restrict__ x, const double *__restrict__ w, const double *__restrict__ Lq,
-             const double *__restrict__ cell_ctr, const double *__restrict__ cblk_sph, int64_t ncblk,
-             const double *__restrict__ tpack, const double *__restrict__ psi, const double *__restrict__ tblk_sph,
-             EvalArgs a, int maxcb, double *__restrict__ gacc)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    GTSmem &sm = *reinterpret_cast<GTSmem *>(smem_raw);
-    unsigned char *qraw = smem_raw + ((sizeof(GTSmem) + 15) & ~size_t(15));
-    float4 *qf = reinterpret_cast<float4 *>(qraw);
-    float *qw = reinterpret_cast<float *>(qraw + sizeof(float4) * GT_MAXQ);
-    double *qd = reinterpret_cast<double *>(qraw);
-
-    const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
-    if (tid < 16) sm.tab[tid] = c_exp2_tab[tid];
-    for (int i = tid; i < GT_WARPS * GT_TPW * 32; i += blockDim.x) (&sm.acc[0][0][0])[i] = 0.0;
-    const int64_t j0 = (int64_t)blockIdx.x * TBLK;
-    const double *bs = tblk_sph + (int64_t)blockIdx.x * 4;
-    const double bc[3] = {bs[0], bs[1], bs[2]};
-    const double bR = bs[3];
-    const int qpc = a.qpc;
-    const unsigned qmagic = (unsigned)((0x100000000ull + qpc - 1) / qpc);
-
-    // alpha reference of the block (FP32 path): max over the block
-    double aref = 0.0;
-    if (FP32) {
-        double am = -DBL_MAX;
-        for (int i = tid; i < TBLK; i += blockDim.x) {
-            const int64_t j = j0 + i;
-            if (j < a.nt) {
-                const double al = log2(tpack[j * TPACK + 1 + DIM]) + a.l2e_eps * psi[j];
-                if (al > am) am = al;
-            }
-        }
-        am = warp_max(am);
-        if (lane == 0) sm.red[wp] = am;
-        __syncthreads();
-        for (int i = 0; i < GT_WARPS; ++i) am = fmax(am, sm.red[i]);
-        aref = (am > -DBL_MAX && isfinite(am)) ? am : 0.0;
-    }
-    const float c32 = (float)a.c32;
-    int64_t next = 0;
-    while (true) {
-        const int ncb = cull_blocks(cblk_sph, ncblk, bc, bR, a.cull, sm.cblist, maxcb, next, sm.wcount, sm.ctl);
-        if (ncb == 0) break;
-        // stage cells (centres) and their quadrature data
-        int nst = 0;
-        for (int b = 0; b < ncb; ++b) {
-            const int64_t cb0 = (int64_t)sm.cblist[b] * SBLK_CELLS;
-            const int cn = (int)min((int64_t)SBLK_CELLS, a.ncells - cb0);
-            for (int i = tid; i < cn * DIM; i += blockDim.x) {
-                const int ci = i / DIM, d = i - ci * DIM;
-                sm.cctr[(nst + ci) * 3 + d] = cell_ctr[(cb0 + ci) * DIM + d];
-            }
-            for (int i = tid; i < cn * qpc; i += blockDim.x) {
-                const int64_t q = cb0 * qpc + i;
-                const int slot = nst * qpc + i;
-                if (FP32) {
-                    double xt[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-                    for (int d = 0; d < DIM; ++d) xt[d] = x[q * DIM + d] - bc[d];
-                    const double beta = -LOG2E * Lq[q] + aref;
-                    float4 v;
-                    v.x = (float)xt[0];
-                    v.y = (float)xt[1];
-                    v.z = DIM == 3 ? (float)xt[2] : (float)beta;
-                    v.w = DIM == 3 ? (float)beta : 0.f;
-                    qf[slot] = v;
-                    qw[slot] = (float)w[q];
-                } else {
-                    double xsq = 0.0;
-#pragma unroll
-                    for (int d = 0; d < DIM; ++d) {
-                        const double xt = x[q * DIM + d] - a.o[d];
-                        qd[slot * 5 + d] = xt;
-                        xsq += xt * xt;
-                    }
-                    qd[slot * 5 + 3] = -a.halfs * xsq - KAPPA * Lq[q];
-                    qd[slot * 5 + 4] = w[q];
-                }
-            }
-            nst += cn;
-        }
-        __syncthreads();
-        for (int i = 0; i < GT_TPW; ++i) {
-            const int64_t j = j0 + wp * GT_TPW + i;
-            if (j >= a.nt) break;
-            const double *tp = tpack + j * TPACK;
-            double yj[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-            for (int d = 0; d < DIM; ++d) yj[d] = tp[2 + DIM + d];
-            // exact candidate test of every staged cell for target j, in order
-            int ncand = 0;
-            for (int c0 = 0; c0 < nst; c0 += 32) {
-                const int c = c0 + lane;
-                bool in = false;
-                if (c < nst) in = dist2_exact<DIM>(yj, sm.cctr + c * 3) <= a.sstar;
-                const unsigned bal = __ballot_sync(0xffffffffu, in);
-                if (in) sm.cand[wp][ncand + __popc(bal & ((1u << lane) - 1u))] = (unsigned short)c;
-                ncand += __popc(bal);
-            }
-            __syncwarp();
-            const int npair = ncand * qpc;
-            double a64 = 0.0;
-            if (FP32) {
-                const float ty0 = (float)(yj[0] - bc[0]), ty1 = (float)(yj[1] - bc[1]);
-                const float ty2 = DIM == 3 ? (float)(yj[2] - bc[2]) : 0.f;
-                const float al = (float)(log2(tp[1 + DIM]) + a.l2e_eps * psi[j] - aref);
-                float acc = 0.f;
-                int it = 0;
-                for (int p = lane; p < npair; p += 32, ++it) {
-                    const unsigned ci = fast_div((unsigned)p, qmagic);
-                    const int slot = sm.cand[wp][ci] * qpc + (p - (int)ci * qpc);
-                    const float4 v = qf[slot];
-                    const float beta = DIM == 3 ? v.w : v.z;
-                    const float d0 = v.x - ty0, d1 = v.y - ty1;
-                    float d2 = d0 * d0;
-                    d2 = fmaf(d1, d1, d2);
-                    if (DIM == 3) {
-                        const float dz = v.z - ty2;
-                        d2 = fmaf(dz, dz, d2);
-                    }
-                    const float e = fmaf(-c32, d2, al + beta);
-                    acc = fmaf(qw[slot], ex2_approx(e), acc);
-                    if ((it & 7) == 7) { a64 += (double)acc; acc = 0.f; }
-                }
-                a64 += (double)acc;
-            } else {
-                const double A = tp[0], B0 = tp[1], B1 = tp[2], B2 = DIM == 3 ? tp[3] : 0.0;
-                for (int p = lane; p < npair; p += 32) {
-                    const unsigned ci = fast_div((unsigned)p, qmagic);
-                    const int slot = sm.cand[wp][ci] * qpc + (p - (int)ci * qpc);
-                    const double *v = qd + slot * 5;
-                    double u = fma(B0, v[0], A + v[3]);
-                    u = fma(B1, v[1], u);
-                    if (DIM == 3) u = fma(B2, v[2], u);
-                    a64 = fma(v[4], exp2_16(u, sm.tab), a64);
-                }
-            }
-            sm.acc[wp][i][lane] += a64;
-            __syncwarp();
-        }
-        __syncthreads();
-    }
-    for (int i = 0; i < GT_TPW; ++i) {
-        const int64_t j = j0 + wp * GT_TPW + i;
-        const double g = warp_sum(sm.acc[wp][i][lane]);
-        if (lane == 0 && j < a.nt) gacc[j] = FP32 ? g : g * tpack[j * TPACK + 1 + DIM];
-    }
-}
-
-// ---------------------------------------------------------------------------
 // finalize: g_j = sum of partials - nu_j, plus the reductions the solver and
 // the solver control need (SotSolver.cc:322-327, SotSolver.h:391-442).
 // ---------------------------------------------------------------------------
@@ -892,6 +490,14 @@ static int grid_for(int64_t n, int threads, int cap = 148 * 8)
     return (int)g;
 }
 
+void launch_target_prep_dense(sdot_ctx *c, const EvalArgs &a)
+{
+    if (c->dim == 2)
+        k_target_prep<2><<<grid_for(a.nt, 256), 256, 0, c->stream>>>(a.nt, c->y.p, c->nu.p, c->psi.p, a, c->tpack.p);
+    else
+        k_target_prep<3><<<grid_for(a.nt, 256), 256, 0, c->stream>>>(a.nt, c->y.p, c->nu.p, c->psi.p, a, c->tpack.p);
+}
+
 void k_axpy_launch(cudaStream_t s, double *x, const double *x0, double a, const double *p, int64_t n)
 {
     k_axpy<<<grid_for(n, 256), 256, 0, s>>>(x, x0, a, p, n);
@@ -974,7 +580,7 @@ static sdot_status run_eval(sdot_ctx *c, const EvalArgs &a, bool dense, const do
         if (c->profiling) cudaEventRecord(c->pev[i], st);
     };
     mark(0);
-    k_target_prep<DIM><<<grid_for(a.nt, 256), 256, 0, st>>>(a.nt, c->y.p, c->nu.p, c->psi.p, a, c->tpack.p);
+    if (dense) k_target_prep<DIM><<<grid_for(a.nt, 256), 256, 0, st>>>(a.nt, c->y.p, c->nu.p, c->psi.p, a, c->tpack.p);
     mark(1);
     int64_t nval = 0;
     int nks = 1;
@@ -1000,51 +606,20 @@ static sdot_status run_eval(sdot_ctx *c, const EvalArgs &a, bool dense, const do
                                                                    qslice, c->gpart.p);
     } else {
         nval = c->nsblk;
-        const size_t smA = sizeof(VTSmem);
-        if (a.ql <= 4) {
-            cudaFuncSetAttribute(k_value_trunc<DIM, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smA);
-            k_value_trunc<DIM, 4><<<(unsigned)c->nsblk, VT_WARPS * 32, smA, st>>>(
-                c->x.p, c->rho.p, c->jxw.p, c->cell_ctr.p, c->sblk_sph.p, c->tpack.p, c->tblk_sph.p, c->ntblk, a,
-                c->Lq.p, c->blkpart.p);
-        } else if (a.ql <= 8) {
-            cudaFuncSetAttribute(k_value_trunc<DIM, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smA);
-            k_value_trunc<DIM, 8><<<(unsigned)c->nsblk, VT_WARPS * 32, smA, st>>>(
-                c->x.p, c->rho.p, c->jxw.p, c->cell_ctr.p, c->sblk_sph.p, c->tpack.p, c->tblk_sph.p, c->ntblk, a,
-                c->Lq.p, c->blkpart.p);
-        } else {
-            cudaFuncSetAttribute(k_value_trunc<DIM, 9>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smA);
-            k_value_trunc<DIM, 9><<<(unsigned)c->nsblk, VT_WARPS * 32, smA, st>>>(
-                c->x.p, c->rho.p, c->jxw.p, c->cell_ctr.p, c->sblk_sph.p, c->tpack.p, c->tblk_sph.p, c->ntblk, a,
-                c->Lq.p, c->blkpart.p);
-        }
-        mark(2);
-        const int64_t ncblk = c->ncblk;
-        const bool fp32 = prec != SDOT_PREC_FP64;
-        const int qbytes = fp32 ? (int)(sizeof(float4) + sizeof(float)) : 5 * (int)sizeof(double);
-        const int maxq = fp32 ? GT_MAXQ : GT_MAXQ64;
-        int maxcb = std::min(GT_MAXCELL / SBLK_CELLS, maxq / (SBLK_CELLS * a.qpc));
-        if (maxcb < 1) maxcb = 1;
-        const size_t smB = ((sizeof(GTSmem) + 15) & ~size_t(15)) + (size_t)maxq * qbytes;
-        if (fp32) {
-            cudaFuncSetAttribute(k_grad_trunc<DIM, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smB);
-            k_grad_trunc<DIM, true><<<(unsigned)c->ntblk, GT_WARPS * 32, smB, st>>>(
-                c->x.p, c->w.p, c->Lq.p, c->cell_ctr.p, c->cblk_sph.p, ncblk, c->tpack.p, c->psi.p, c->tblk_sph.p, a,
-                maxcb, c->gpart.p);
-        } else {
-            cudaFuncSetAttribute(k_grad_trunc<DIM, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smB);
-            k_grad_trunc<DIM, false><<<(unsigned)c->ntblk, GT_WARPS * 32, smB, st>>>(
-                c->x.p, c->w.p, c->Lq.p, c->cell_ctr.p, c->cblk_sph.p, ncblk, c->tpack.p, c->psi.p, c->tblk_sph.p,
-                a, maxcb, c->gpart.p);
-        }
+        k_target_prep_kd<DIM><<<grid_for(a.nt, 256), 256, 0, st>>>(a.nt, c->y.p, c->nu.p, c->psi.p, a, c->tpack.p);
+        sdot_status s = run_trunc(c, a, c->current_distance_threshold);  // records pev 7, 2, 3
+        if (s != SDOT_OK) return s;
     }
-    mark(3);
+    if (dense) mark(3);
     k_finalize_grad<<<FIN_BLOCKS, FIN_THREADS, 0, st>>>(a.nt, nks, c->gpart.p, c->nu.p, c->psi.p, pdir, tol,
                                                        partial ? 0 : 1, c->grad.p, c->redpart.p);
     k_finalize_scalars<<<1, 256, 0, st>>>(FIN_BLOCKS, c->redpart.p, nval, c->blkpart.p, c->scal.p);
     mark(4);
     c->klaunch[1] += 1;
-    c->klaunch[2] += 1;
-    c->klaunch[3] += 1;
+    if (dense) {
+        c->klaunch[2] += 1;
+        c->klaunch[3] += 1;
+    }
     c->klaunch[4] += 2;
     return cuda_error(c, cudaGetLastError(), "evaluate launch");
 }
@@ -1116,10 +691,21 @@ sdot_status evaluate_internal(sdot_ctx *c, const double *p_dir, double comp_tol,
         float t = 0.f;
         cudaEventElapsedTime(&t, c->pev[5], c->pev[6]);
         c->kms[0] += t;
-        for (int i = 0; i < 4; ++i) {
-            cudaEventElapsedTime(&t, c->pev[i], c->pev[i + 1]);
-            c->kms[1 + i] += t;
+        cudaEventElapsedTime(&t, c->pev[0], c->pev[1]);
+        c->kms[1] += t;
+        if (dense_ok) {
+            cudaEventElapsedTime(&t, c->pev[1], c->pev[2]);
+            c->kms[2] += t;
+        } else {
+            cudaEventElapsedTime(&t, c->pev[1], c->pev[7]);
+            c->kms[6] += t;
+            cudaEventElapsedTime(&t, c->pev[7], c->pev[2]);
+            c->kms[2] += t;
         }
+        cudaEventElapsedTime(&t, c->pev[2], c->pev[3]);
+        c->kms[3] += t;
+        cudaEventElapsedTime(&t, c->pev[3], c->pev[4]);
+        c->kms[4] += t;
     }
     c->scal_host[SC_R] = r;
     c->global_functional = c->scal_host[SC_VALUE];

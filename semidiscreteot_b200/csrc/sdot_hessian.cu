@@ -148,6 +148,7 @@ sdot_status hessian_internal(sdot_ctx *c, double *H_host)
     for (int d = 0; d < 3; ++d) a.o[d] = c->origin[d];
     a.sstar = sstar_of(r);
     const bool trunc = std::isnan(r) || r < c->diam;
+    launch_target_prep_dense(c, a);  // the truncated evaluation leaves another layout in tpack
     DevBuf<double> Hi, Hu;
     cudaError_t e = Hi.alloc((size_t)n * n);
     if (e == cudaSuccess) e = Hu.alloc((size_t)n * n);

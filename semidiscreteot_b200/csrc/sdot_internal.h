@@ -1,15 +1,16 @@
 // sdot_internal.h -- context layout and shared device helpers of libsdot_cuda.
 //
 // Data layout in HBM (all FP64 unless noted, internal orderings):
-//   source cells are sorted by the Morton code of their centres; quadrature
-//   points follow their cell (cell-major, uniform points per cell).  Source
-//   blocks = SBLK_CELLS consecutive cells, each with a bounding sphere.
-//   targets are sorted by Morton code of their position; target blocks =
-//   TBLK consecutive targets with a bounding sphere.
+//   source cells are ordered by a k-d tree over their centres (leaves of at
+//   most SBLK_UNITS warp units = source blocks); quadrature points follow
+//   their cell (cell-major, uniform points per cell).  Targets are ordered by
+//   a k-d tree over their positions (leaves of at most TBLK_KD = target
+//   blocks).  Every block has a bounding sphere (FP64 and conservative FP32).
 // Per evaluation:
-//   tpack[j] = {A_j, B_j(dim), nu_j, y_j(dim)} padded to 8 doubles, where the
+//   tpack[j], 8 doubles: dense path {A_j, B_j(dim), nu_j, y_j(dim)} where the
 //     scaled exponent is b_qj = A_j + B_j.xt_q + C_q = kappa*(psi_j-|x_q-y_j|^2/2)/eps,
-//     kappa = 16/ln 2 (units of 2^(1/16)), xt = x - origin;
+//     kappa = 16/ln 2 (units of 2^(1/16)), xt = x - origin; truncated path
+//     {y_j(3), nu_j, log2 nu_j, kappa psi_j / eps};
 //   Lq[q] = log of the reference's total_sum_exp at q (natural units, +inf if
 //     the point is skipped), written by the value sweep and read by the
 //     gradient sweep.
@@ -25,8 +26,8 @@
 
 namespace sdot {
 
-constexpr int SBLK_CELLS = 8;        // cells per source block (value sweep, one warp per cell)
-constexpr int TBLK = 64;             // targets per target block (gradient sweep CTA)
+constexpr int SBLK_UNITS = 8;        // warp units (cell, q-group) per source block
+constexpr int TBLK_KD = 32;          // max targets per target block (k-d tree leaf)
 constexpr int DENSE_A_THREADS = 128; // dense value sweep: threads per CTA
 constexpr int DENSE_A_QT = 4;        // dense value sweep: quadrature points per thread
 constexpr int DENSE_B_THREADS = 128; // dense gradient sweep: threads per CTA
@@ -105,28 +106,38 @@ struct sdot_ctx {
     int64_t nq = 0, ncells = 0;
     int qpc = 0;                       // quadrature points per cell (uniform)
     bool w_nonneg = true;              // all rho*JxW >= 0
-    sdot::DevBuf<double> x, rho, jxw, w, lw;  // x: nq*dim
+    sdot::DevBuf<double> x, rho, jxw, w;  // x: nq*dim
     sdot::DevBuf<double> cell_ctr;     // ncells*dim
-    int64_t nsblk = 0;                 // value-sweep blocks (8 warp units each)
-    sdot::DevBuf<double> sblk_sph;     // 4 per block: centre(3), radius
-    int64_t ncblk = 0;                 // gradient-sweep cell blocks (SBLK_CELLS cells)
-    sdot::DevBuf<double> cblk_sph;
+    int64_t nsblk = 0;                 // source blocks (k-d leaves)
+    sdot::DevBuf<int64_t> sblk_cell;   // first cell of each block (nsblk + 1)
+    sdot::DevBuf<double> sblk_sph;     // 4 per block: centre(3), radius (FP64)
+    sdot::DevBuf<float4> sblk_sph32;   // conservative FP32 spheres
     int ql = 0, ngroups = 1;           // quadrature points per warp unit, units per cell
     std::vector<double> cell_ctr_host; // internal order, for the covering radius
+    std::vector<double> src_sph_host, tgt_sph_host;  // FP64 block spheres (4 per block)
     double src_lo[3] = {0, 0, 0}, src_hi[3] = {0, 0, 0};
 
     // ---- target (internal order) ----
     int64_t nt = 0;
     sdot::DevBuf<double> y, nu;        // y: nt*dim
     sdot::DevBuf<int64_t> perm;        // internal index -> caller index
-    int64_t ntblk = 0;
+    int64_t ntblk = 0;                 // target blocks (k-d leaves)
+    sdot::DevBuf<int64_t> tblk_off;    // first target of each block (ntblk + 1)
     sdot::DevBuf<double> tblk_sph;     // 4 per block
+    sdot::DevBuf<float4> tblk_sph32;
     std::vector<double> nu_host;       // caller order
     std::vector<double> y_host;        // caller order
     double tgt_lo[3] = {0, 0, 0}, tgt_hi[3] = {0, 0, 0};
 
-    double origin[3] = {0, 0, 0};      // centring point of the value sweep
+    double origin[3] = {0, 0, 0};      // centring point of the dense value sweep
     double diam = 0;                   // diameter bound of cells U targets
+    double coord_scale = 1.0;          // max |coordinate|, for FP32 cull margins
+
+    // ---- truncated path: block-pair lists and gradient partials ----
+    sdot::DevBuf<int64_t> fwd_cnt, inv_cnt, fwd_off, inv_off;
+    sdot::DevBuf<int> fwd_t, inv_b;
+    sdot::DevBuf<double> part;
+    size_t part_cap_bytes = (size_t)4 << 30;
 
     // ---- per-evaluation buffers ----
     sdot::DevBuf<double> psi, grad, tpack, Lq, gpart, blkpart, scal, redpart;
@@ -152,8 +163,10 @@ struct sdot_ctx {
     // ---- measurement ----
     bool profiling = false;
     cudaEvent_t pev[8] = {};
-    double kms[6] = {0, 0, 0, 0, 0, 0};
-    int64_t klaunch[6] = {0, 0, 0, 0, 0, 0};
+    // phases: threshold, target prep, value sweep, gradient sweep, finalize,
+    // layout (gather/scatter), block-pair lists
+    double kms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int64_t klaunch[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 };
 
 namespace sdot {
@@ -180,6 +193,12 @@ double sstar_of(double r);
 sdot_status launch_gather(sdot_ctx *c, double *dst, const double *src, int64_t n);
 sdot_status launch_scatter(sdot_ctx *c, double *dst, const double *src, int64_t n);
 sdot_status launch_minmax(sdot_ctx *c, const double *v, int64_t n, double *mx, double *mn);
+
+struct EvalArgs;
+// truncated evaluation (block-pair lists, fused sweeps, partial reduction)
+sdot_status run_trunc(sdot_ctx *c, const EvalArgs &a, double r);
+// dense-layout tpack for the current psi (used by the Hessian)
+void launch_target_prep_dense(sdot_ctx *c, const EvalArgs &a);
 
 // L-BFGS helpers (device vector kernels)
 void k_axpy_launch(cudaStream_t s, double *x, const double *x0, double a, const double *p, int64_t n);

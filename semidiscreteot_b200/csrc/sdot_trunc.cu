@@ -1,0 +1,613 @@
+// sdot_trunc.cu -- truncated evaluation (tau > 0): exact cell-centre candidate
+// sets, one fused source-block kernel for both exponential sweeps, and an
+// atomic-free reduction of the per-block gradient partials.
+//
+// Replaces find_nearest_target_points + local_assemble + the WorkStream
+// copier (src/solvers/SotSolver.cc:553-570, 769-869, 307-311).
+//
+// Blocks.  Source cells and targets are ordered by k-d trees built at
+// set_source / set_target; a source block is a leaf of <= 8 warp units
+// (cell, q-group), a target block a leaf of <= 32 targets.  Each block has a
+// bounding sphere (FP64 and a conservative FP32 copy).
+//
+// Per evaluation:
+//   1. block-pair lists.  (b, t) is a pair iff dist(c_b, c_t) <= r + R_b + R_t
+//      (FP32, conservatively enlarged).  The forward list (per b, t ascending)
+//      and the inverse list (per t, b ascending) are built by count / scan /
+//      fill kernels that evaluate the identical expression, so they hold the
+//      same pairs.
+//   2. k_fused (CTA <-> source block, warp <-> unit):
+//      staging: the targets of the block's pairs, culled per target against
+//        the block sphere (|y - c_b| <= r + R_b), compacted in order;
+//      exact test: warp of cell K keeps j iff d2(y_j, c_K) <= s*, rounded like
+//        the reference (this is the candidate set, bit-exact);
+//      value sweep: lane <-> candidate, all q of the unit in registers, FP64
+//        online log-sum-exp of b_qj = B0_Kj + G_Kj.delta_q + C'_q, where
+//        B0_Kj = kappa (psi_j - d2/2)/eps, G_Kj = kappa (y_j - c_K)/eps,
+//        delta_q = x_q - c_K, C'_q = -kappa |delta_q|^2 / (2 eps)
+//        (kappa = 16/ln 2; the same expansion as |x_q - y_j|^2 about c_K);
+//      gradient sweep: thread <-> staged target, loop over the block's cells
+//        whose candidate set contains it, sum over q of
+//        w_q nu_j 2^(E0_Kj + G'_Kj.delta_q + D_q) in FP32 ex2 (or FP64 exp2),
+//        E0 and G' formed in FP64 per (cell, target) so every FP32 operand is
+//        small; FP64 accumulation across cells.  The block's partial for each
+//        target of each pair is written to a slot of the pair in the inverse
+//        list order.
+//   3. k_grad_reduce (warp <-> target block): sum of the partials over the
+//      pairs in ascending source-block order, lane <-> target.  No atomics;
+//      the summation order is fixed, results are bitwise reproducible.
+#include <float.h>
+#include <math.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "sdot_device.cuh"
+#include "sdot_internal.h"
+
+namespace sdot {
+
+constexpr int FT_WARPS = 8;
+constexpr int FT_MAXS = 1024;               // staged targets per chunk
+constexpr int FT_TS = 6;                    // doubles per staged target: y(3), nu, log2 nu, s*psi
+constexpr int FT_MAXT = FT_MAXS / TBLK_KD;  // target blocks per chunk
+constexpr int FT_MAXQ = 80;                 // quadrature points of one source block
+
+struct FusedArgs {
+    const double *x, *rho, *jxw, *w, *cell_ctr;
+    const double *tpk;           // per target: y(3), nu, log2 nu, s*psi, -, -
+    const int64_t *sblk_cell;    // source block -> first cell (nsblk + 1)
+    const double *sblk_sph;      // FP64 centre(3), radius
+    const int64_t *tblk_off;     // target block -> first target (ntblk + 1)
+    const int64_t *fwd_off, *inv_off;
+    const int *fwd_t, *inv_b;
+    double *part;                // partials, 32 per pair in inverse order
+    double *Lq;                  // per q (written by the value sweep)
+    double *valpart;             // per source block: value, C, skipped, pairs
+    int do_a, do_b;
+    int tlo, thi;                // gradient sweep restricted to target blocks [tlo, thi)
+    int64_t part_base;           // inverse position of the first pair of tlo
+    double cullt;                // per-target cull radius addend (r, enlarged)
+};
+
+struct FTSmem {
+    double tab[16];
+    double stg[FT_MAXS * FT_TS];
+    double qd[FT_MAXQ][4];        // delta_q (FP64) and C'_q
+    double qL[FT_MAXQ];           // L_q of the block
+    float qb[FT_MAXQ][4];         // pass B: delta (3) as float, D_q
+    float qw[FT_MAXQ];            // pass B: w_q
+    double cellc[FT_WARPS][3];    // centre of each cell of the block
+    double cellC[FT_WARPS];       // -kappa L_Kref for each cell (pass B), -inf if the cell is skipped
+    double pv[FT_MAXS];           // pass B partial per staged target
+    unsigned mask[FT_WARPS][FT_MAXS / 32];
+    unsigned short cand[FT_WARPS][FT_MAXS];
+    short smap[FT_MAXT][TBLK_KD]; // (chunk target block, slot) -> staged position or -1
+    int ctb[FT_MAXT];             // target blocks of the chunk
+    int64_t cpos[FT_MAXT];        // their partial base index (or -1 when outside [tlo, thi))
+    int ccnt[FT_MAXT + 1];        // prefix of their sizes
+    int wcount[FT_WARPS];
+    int nstg;
+};
+
+// ---------------------------------------------------------------------------
+// block-pair lists
+// ---------------------------------------------------------------------------
+
+// Rounded operation by operation (no contraction): the forward and inverse
+// list kernels must reach bitwise identical decisions.
+__device__ __forceinline__ bool pair_test(float4 s, float4 t, float cr)
+{
+    const float dx = __fsub_rn(s.x, t.x), dy = __fsub_rn(s.y, t.y), dz = __fsub_rn(s.z, t.z);
+    const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+    const float lim = __fadd_rn(__fadd_rn(cr, s.w), t.w);
+    return d2 <= __fmul_rn(lim, lim);
+}
+
+// mode 0: count, 1: fill.  rows <-> A, columns <-> B (A/B = source/target
+// spheres for the forward list, target/source for the inverse list).
+template <bool ROWS_ARE_SOURCE>
+__global__ void __launch_bounds__(256)
+k_pairs(const float4 *__restrict__ rowsph, int nrow, const float4 *__restrict__ colsph, int ncol, float cr,
+        const int64_t *__restrict__ off, int64_t *__restrict__ cnt, int *__restrict__ out)
+{
+    __shared__ float4 sc[1024];
+    const int row = blockIdx.x * blockDim.x + threadIdx.x;
+    const float4 me = row < nrow ? rowsph[row] : make_float4(0.f, 0.f, 0.f, -1e30f);
+    int64_t k = 0;
+    const int64_t base = (out && row < nrow) ? off[row] : 0;
+    for (int c0 = 0; c0 < ncol; c0 += 1024) {
+        const int cn = min(1024, ncol - c0);
+        __syncthreads();
+        for (int i = threadIdx.x; i < cn; i += blockDim.x) sc[i] = colsph[c0 + i];
+        __syncthreads();
+        if (row < nrow) {
+            for (int i = 0; i < cn; ++i) {
+                const bool hit = ROWS_ARE_SOURCE ? pair_test(me, sc[i], cr) : pair_test(sc[i], me, cr);
+                if (hit) {
+                    if (out) out[base + k] = c0 + i;
+                    ++k;
+                }
+            }
+        }
+    }
+    if (!out && row < nrow) cnt[row] = k;
+}
+
+// exclusive scan of n counts into off[0..n] (single CTA, order-fixed)
+__global__ void __launch_bounds__(1024) k_scan(const int64_t *__restrict__ cnt, int64_t n, int64_t *__restrict__ off)
+{
+    __shared__ int64_t part[1024];
+    const int tid = threadIdx.x;
+    const int64_t per = (n + 1023) / 1024;
+    const int64_t a = tid * per, b = min(n, a + per);
+    int64_t s = 0;
+    for (int64_t i = a; i < b; ++i) s += cnt[i];
+    part[tid] = s;
+    __syncthreads();
+    if (tid == 0) {
+        int64_t acc = 0;
+        for (int i = 0; i < 1024; ++i) {
+            const int64_t v = part[i];
+            part[i] = acc;
+            acc += v;
+        }
+        off[n] = acc;
+    }
+    __syncthreads();
+    s = part[tid];
+    for (int64_t i = a; i < b; ++i) {
+        off[i] = s;
+        s += cnt[i];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// fused value + gradient sweeps
+// ---------------------------------------------------------------------------
+
+// stage the targets of fwd pairs [k0, k1) of block b; returns the number of pairs taken
+template <int DIM>
+__device__ int stage_chunk(FTSmem &sm, const FusedArgs &f, const EvalArgs &a, int64_t k0, int64_t k1,
+                           const double *bc, double rcull2, bool for_b)
+{
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    // choose target blocks while the worst case fits
+    if (tid == 0) {
+        int n = 0, acc = 0;
+        for (int64_t k = k0; k < k1 && n < FT_MAXT; ++k) {
+            const int t = f.fwd_t[k];
+            const int sz = (int)(f.tblk_off[t + 1] - f.tblk_off[t]);
+            if (acc + sz > FT_MAXS) break;
+            sm.ctb[n] = t;
+            sm.ccnt[n] = acc;
+            acc += sz;
+            ++n;
+        }
+        sm.ccnt[n] = acc;
+        sm.wcount[0] = n;
+    }
+    __syncthreads();
+    const int nt = sm.wcount[0];
+    const int total = sm.ccnt[nt];
+    // partial base of each pair (inverse position), -1 outside [tlo, thi)
+    if (for_b && tid < nt) {
+        const int t = sm.ctb[tid];
+        int64_t pos = -1;
+        if (t >= f.tlo && t < f.thi) {
+            int64_t lo = f.inv_off[t], hi = f.inv_off[t + 1];
+            const int b = blockIdx.x;
+            while (lo < hi) {
+                const int64_t mid = (lo + hi) >> 1;
+                if (f.inv_b[mid] < b) lo = mid + 1;
+                else hi = mid;
+            }
+            if (lo < f.inv_off[t + 1] && f.inv_b[lo] == b) pos = (lo - f.part_base) * TBLK_KD;
+        }
+        sm.cpos[tid] = pos;
+    }
+    for (int i = tid; i < FT_MAXT * TBLK_KD; i += blockDim.x) (&sm.smap[0][0])[i] = -1;
+    __syncthreads();
+    // per-target cull against the block sphere, in-order compaction
+    int base = 0;
+    for (int e0 = 0; e0 < total; e0 += blockDim.x) {
+        const int e = e0 + tid;
+        bool keep = false;
+        int ti = 0;
+        int64_t j = 0;
+        if (e < total) {
+            while (ti + 1 < nt && sm.ccnt[ti + 1] <= e) ++ti;
+            j = f.tblk_off[sm.ctb[ti]] + (e - sm.ccnt[ti]);
+            const double *tp = f.tpk + j * TPACK;
+            double d2 = 0.0;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                const double t = tp[d] - bc[d];
+                d2 += t * t;
+            }
+            keep = d2 <= rcull2;
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, keep);
+        if (lane == 0) sm.wcount[w] = __popc(bal);
+        __syncthreads();
+        int off = base, tot = 0;
+        for (int i = 0; i < FT_WARPS; ++i) {
+            if (i < w) off += sm.wcount[i];
+            tot += sm.wcount[i];
+        }
+        if (keep) {
+            const int pos = off + __popc(bal & ((1u << lane) - 1u));
+            const double *tp = f.tpk + j * TPACK;
+            double *dst = sm.stg + pos * FT_TS;
+#pragma unroll
+            for (int d = 0; d < FT_TS; ++d) dst[d] = tp[d];
+            sm.smap[ti][e - sm.ccnt[ti]] = (short)pos;
+        }
+        __syncthreads();
+        base += tot;
+    }
+    if (tid == 0) sm.nstg = base;
+    __syncthreads();
+    return nt;
+}
+
+template <int DIM, int QL, bool FP32B>
+__global__ void __launch_bounds__(FT_WARPS * 32, 2)
+k_fused(FusedArgs f, EvalArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    FTSmem &sm = *reinterpret_cast<FTSmem *>(smem_raw);
+    const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
+    const int b = blockIdx.x;
+    if (tid < 16) sm.tab[tid] = c_exp2_tab[tid];
+    const int64_t cb0 = f.sblk_cell[b], cb1 = f.sblk_cell[b + 1];
+    const int ncell = (int)(cb1 - cb0);
+    const int nunit = ncell * a.ngroups;
+    const bool valid = wp < nunit;
+    const int cl = valid ? wp / a.ngroups : 0;          // cell of this warp (block-local)
+    const int grp = valid ? wp - cl * a.ngroups : 0;
+    const int qoff = cl * a.qpc + grp * a.ql;           // block-local index of the unit's first q
+    const int nql = valid ? min(a.ql, a.qpc - grp * a.ql) : 0;
+    const int64_t qblk0 = cb0 * a.qpc;                  // first q of the block
+    const int nqb = ncell * a.qpc;
+    const double *bs = f.sblk_sph + (int64_t)b * 4;
+    const double bc[3] = {bs[0], bs[1], bs[2]};
+    const double rc = (f.cullt + bs[3]) * (1.0 + 1e-12) + 1e-300;
+    const double rcull2 = rc * rc;
+    // cell centres and per-q geometry of the block
+    for (int i = tid; i < ncell * 3; i += blockDim.x) {
+        const int c = i / 3, d = i - c * 3;
+        sm.cellc[c][d] = d < DIM ? f.cell_ctr[(cb0 + c) * DIM + d] : 0.0;
+    }
+    __syncthreads();
+    for (int i = tid; i < nqb; i += blockDim.x) {
+        const int c = i / a.qpc;
+        double dsq = 0.0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const double dl = d < DIM ? f.x[(qblk0 + i) * DIM + d] - sm.cellc[c][d] : 0.0;
+            sm.qd[i][d] = dl;
+            dsq += dl * dl;
+        }
+        sm.qd[i][3] = -a.halfs * dsq;
+    }
+    __syncthreads();
+    const double cc0 = sm.cellc[cl][0], cc1 = sm.cellc[cl][1], cc2 = sm.cellc[cl][2];
+    const int64_t k0 = f.fwd_off[b], k1 = f.fwd_off[b + 1];
+    int chunks = 0;
+    int64_t single_end = -1;  // end of the only chunk, when everything fit in one
+
+    if (f.do_a) {
+        double M[QL], S[QL], mx[QL];
+#pragma unroll
+        for (int k = 0; k < QL; ++k) { M[k] = -CUDART_INF; S[k] = 0.0; mx[k] = -CUDART_INF; }
+        double npairs = 0.0;
+        for (int64_t k = k0; k < k1;) {
+            const int nt = stage_chunk<DIM>(sm, f, a, k, k1, bc, rcull2, f.do_b != 0);
+            const int nstg = sm.nstg;
+            ++chunks;
+            // exact candidate test for this unit's cell, in-order compaction + mask
+            int ncand = 0;
+            if (valid) {
+                for (int b0 = 0; b0 < nstg; b0 += 32) {
+                    const int t = b0 + lane;
+                    bool in = false;
+                    if (t < nstg) in = dist2_exact<DIM>(sm.stg + t * FT_TS, sm.cellc[cl]) <= a.sstar;
+                    const unsigned bal = __ballot_sync(0xffffffffu, in);
+                    if (in) sm.cand[wp][ncand + __popc(bal & ((1u << lane) - 1u))] = (unsigned short)t;
+                    if (lane == 0) sm.mask[wp][b0 >> 5] = bal;
+                    ncand += __popc(bal);
+                }
+                __syncwarp();
+                npairs += (double)ncand * nql;
+                for (int p = lane; p < ncand; p += 32) {
+                    const double *tp = sm.stg + sm.cand[wp][p] * FT_TS;
+                    const double g0 = tp[0] - cc0, g1 = tp[1] - cc1, g2 = DIM == 3 ? tp[2] - cc2 : 0.0;
+                    const double d2 = DIM == 3 ? g0 * g0 + g1 * g1 + g2 * g2 : g0 * g0 + g1 * g1;
+                    const double B0 = fma(-a.halfs, d2, tp[5]);
+                    const double G0 = a.s * g0, G1 = a.s * g1, G2 = a.s * g2;
+                    const double nuj = tp[3];
+#pragma unroll
+                    for (int q = 0; q < QL; ++q) {
+                        if (q < nql) {
+                            const double *dq = sm.qd[qoff + q];
+                            double bb = fma(G0, dq[0], B0);
+                            bb = fma(G1, dq[1], bb);
+                            if (DIM == 3) bb = fma(G2, dq[2], bb);
+                            lse_update(bb, nuj, M[q], S[q], mx[q], sm.tab);
+                        }
+                    }
+                }
+            }
+            k += nt;
+            if (k >= k1 && chunks == 1) single_end = k;
+            __syncthreads();
+        }
+        // merge lanes; epilogue per q on lane 0
+        double tv = 0.0, tcv = 0.0, tsk = 0.0;
+#pragma unroll
+        for (int q = 0; q < QL; ++q) {
+            const double mxw = warp_max(mx[q]);
+            const double sl = (M[q] == -CUDART_INF || mxw == -CUDART_INF) ? 0.0 : S[q] * exp2_16(M[q] - mxw, sm.tab);
+            const double Sw = warp_sum(sl);
+            if (valid && q < nql && lane == 0) {
+                const int qi = qoff + q;
+                const int64_t qg = qblk0 + qi;
+                double v, cv, L;
+                int sk;
+                value_epilogue(a, mxw, Sw, sm.qd[qi][3], f.rho[qg], f.jxw[qg], v, cv, L, sk);
+                f.Lq[qg] = L;
+                sm.qL[qi] = L;
+                tv += v;
+                tcv += cv;
+                tsk += sk;
+            }
+        }
+        block_partials(tv, tcv, tsk, lane == 0 ? npairs : 0.0, f.valpart);
+    } else {
+        for (int i = tid; i < nqb; i += blockDim.x) sm.qL[i] = f.Lq[qblk0 + i];
+    }
+    if (!f.do_b) return;
+    __syncthreads();
+    // pass B per-q data: D_q relative to a per-cell reference L_Kref
+    if (tid < ncell) {
+        double Lref = CUDART_INF;
+        for (int i = 0; i < a.qpc; ++i) Lref = fmin(Lref, sm.qL[tid * a.qpc + i]);
+        sm.cellC[tid] = isfinite(Lref) ? Lref : CUDART_INF;
+    }
+    __syncthreads();
+    for (int i = tid; i < nqb; i += blockDim.x) {
+        const int c = i / a.qpc;
+        const double Lref = sm.cellC[c];
+        const double L = sm.qL[i];
+        double D;
+        if (!isfinite(Lref) || !isfinite(L)) D = -CUDART_INF;
+        else D = (sm.qd[i][3] - KAPPA * (L - Lref)) * (1.0 / 16.0);
+        sm.qb[i][0] = (float)sm.qd[i][0];
+        sm.qb[i][1] = (float)sm.qd[i][1];
+        sm.qb[i][2] = (float)sm.qd[i][2];
+        sm.qb[i][3] = (float)D;
+        sm.qw[i] = (float)f.w[qblk0 + i];
+    }
+    __syncthreads();
+    const float sf = (float)(a.s * (1.0 / 16.0));
+    for (int64_t k = k0; k < k1;) {
+        int nt;
+        if (single_end >= 0) {
+            nt = (int)(single_end - k0);   // staged data and masks of the single chunk are still in smem
+            if (tid < nt) {
+                const int t = sm.ctb[tid];
+                int64_t pos = -1;
+                if (t >= f.tlo && t < f.thi) {
+                    int64_t lo = f.inv_off[t], hi = f.inv_off[t + 1];
+                    while (lo < hi) {
+                        const int64_t mid = (lo + hi) >> 1;
+                        if (f.inv_b[mid] < b) lo = mid + 1;
+                        else hi = mid;
+                    }
+                    if (lo < f.inv_off[t + 1] && f.inv_b[lo] == b) pos = (lo - f.part_base) * TBLK_KD;
+                }
+                sm.cpos[tid] = pos;
+            }
+            __syncthreads();
+        } else {
+            nt = stage_chunk<DIM>(sm, f, a, k, k1, bc, rcull2, true);
+            // masks for this chunk (one warp per cell; units of group 0)
+            if (valid && grp == 0) {
+                for (int b0 = 0; b0 < sm.nstg; b0 += 32) {
+                    const int t = b0 + lane;
+                    bool in = false;
+                    if (t < sm.nstg) in = dist2_exact<DIM>(sm.stg + t * FT_TS, sm.cellc[cl]) <= a.sstar;
+                    const unsigned bal = __ballot_sync(0xffffffffu, in);
+                    if (lane == 0) sm.mask[wp][b0 >> 5] = bal;
+                }
+            }
+            __syncthreads();
+        }
+        const int nstg = sm.nstg;
+        for (int t = tid; t < nstg; t += blockDim.x) {
+            const double *tp = sm.stg + t * FT_TS;
+            double acc64 = 0.0;
+            for (int c = 0; c < ncell; ++c) {
+                const int mw = c * a.ngroups;
+                if (!((sm.mask[mw][t >> 5] >> (t & 31)) & 1u)) continue;
+                const double Lref = sm.cellC[c];
+                if (!isfinite(Lref)) continue;
+                const double g0 = tp[0] - sm.cellc[c][0], g1 = tp[1] - sm.cellc[c][1];
+                const double g2 = DIM == 3 ? tp[2] - sm.cellc[c][2] : 0.0;
+                const double d2 = DIM == 3 ? g0 * g0 + g1 * g1 + g2 * g2 : g0 * g0 + g1 * g1;
+                const int qa = c * a.qpc;
+                if (FP32B) {
+                    const double E0 = tp[4] + (fma(-a.halfs, d2, tp[5]) - KAPPA * Lref) * (1.0 / 16.0);
+                    const float e0 = (float)E0;
+                    const float G0 = sf * (float)g0, G1 = sf * (float)g1, G2 = sf * (float)g2;
+                    float acc = 0.f;
+                    for (int q = 0; q < a.qpc; ++q) {
+                        const float *qb = sm.qb[qa + q];
+                        float e = fmaf(G0, qb[0], e0 + qb[3]);
+                        e = fmaf(G1, qb[1], e);
+                        if (DIM == 3) e = fmaf(G2, qb[2], e);
+                        acc = fmaf(sm.qw[qa + q], ex2_approx(e), acc);
+                    }
+                    acc64 += (double)acc;
+                } else {
+                    const double U0 = 16.0 * tp[4] + fma(-a.halfs, d2, tp[5]) - KAPPA * Lref;
+                    const double G0 = a.s * g0, G1 = a.s * g1, G2 = a.s * g2;
+                    for (int q = 0; q < a.qpc; ++q) {
+                        const double *dq = sm.qd[qa + q];
+                        const double L = sm.qL[qa + q];
+                        if (!isfinite(L)) continue;
+                        double u = fma(G0, dq[0], U0 + dq[3] - KAPPA * (L - Lref));
+                        u = fma(G1, dq[1], u);
+                        if (DIM == 3) u = fma(G2, dq[2], u);
+                        acc64 = fma(f.w[qblk0 + qa + q], exp2_16(u, sm.tab), acc64);
+                    }
+                }
+            }
+            sm.pv[t] = acc64;
+        }
+        __syncthreads();
+        // write every slot of every pair of the chunk (zeros where not staged)
+        for (int i = tid; i < nt * TBLK_KD; i += blockDim.x) {
+            const int ti = i / TBLK_KD, sl = i - ti * TBLK_KD;
+            const int64_t base = sm.cpos[ti];
+            if (base < 0) continue;
+            const short p = sm.smap[ti][sl];
+            f.part[base + sl] = p >= 0 ? sm.pv[p] : 0.0;
+        }
+        k += nt;
+        __syncthreads();
+    }
+}
+
+// gradient of target block t = sum over its pairs (ascending source block)
+__global__ void __launch_bounds__(256)
+k_grad_reduce(const int64_t *__restrict__ tblk_off, const int64_t *__restrict__ inv_off, int tlo, int thi,
+              int64_t part_base, const double *__restrict__ part, int fp32_nu_folded, const double *__restrict__ nu,
+              double *__restrict__ gacc)
+{
+    const int t = tlo + (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (t >= thi) return;
+    const int64_t p0 = inv_off[t], p1 = inv_off[t + 1];
+    double acc = 0.0;
+    for (int64_t p = p0; p < p1; ++p) acc += part[(p - part_base) * TBLK_KD + lane];
+    const int64_t j = tblk_off[t] + lane;
+    if (j < tblk_off[t + 1]) gacc[j] = acc * (fp32_nu_folded ? 1.0 : 1.0);
+    (void)nu;
+}
+
+// ---------------------------------------------------------------------------
+// host orchestration
+// ---------------------------------------------------------------------------
+
+template <int DIM, int QL, bool FP32B>
+static void launch_fused(sdot_ctx *c, const FusedArgs &f, const EvalArgs &a, size_t smem)
+{
+    cudaFuncSetAttribute(k_fused<DIM, QL, FP32B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_fused<DIM, QL, FP32B><<<(unsigned)c->nsblk, FT_WARPS * 32, smem, c->stream>>>(f, a);
+}
+
+template <int DIM>
+static void dispatch_fused(sdot_ctx *c, const FusedArgs &f, const EvalArgs &a, bool fp32b)
+{
+    const size_t smem = sizeof(FTSmem);
+    if (a.ql <= 4) {
+        if (fp32b) launch_fused<DIM, 4, true>(c, f, a, smem);
+        else launch_fused<DIM, 4, false>(c, f, a, smem);
+    } else if (a.ql <= 8) {
+        if (fp32b) launch_fused<DIM, 8, true>(c, f, a, smem);
+        else launch_fused<DIM, 8, false>(c, f, a, smem);
+    } else {
+        if (fp32b) launch_fused<DIM, 9, true>(c, f, a, smem);
+        else launch_fused<DIM, 9, false>(c, f, a, smem);
+    }
+}
+
+sdot_status run_trunc(sdot_ctx *c, const EvalArgs &a, double r)
+{
+    cudaStream_t st = c->stream;
+    // 1. block-pair lists (conservative FP32 test, identical in both directions)
+    const float cr = (float)(std::min(r, 1e30) * (1.0 + 1e-6) + 1e-6 * c->coord_scale);
+    const int nsb = (int)c->nsblk, ntb = (int)c->ntblk;
+    cudaError_t e = c->fwd_cnt.alloc(nsb + 1);
+    if (e == cudaSuccess) e = c->inv_cnt.alloc(ntb + 1);
+    if (e == cudaSuccess) e = c->fwd_off.alloc(nsb + 1);
+    if (e == cudaSuccess) e = c->inv_off.alloc(ntb + 1);
+    if (e != cudaSuccess) return cuda_error(c, e, "pair list alloc");
+    k_pairs<true><<<(nsb + 255) / 256, 256, 0, st>>>(c->sblk_sph32.p, nsb, c->tblk_sph32.p, ntb, cr, nullptr,
+                                                    c->fwd_cnt.p, nullptr);
+    k_pairs<false><<<(ntb + 255) / 256, 256, 0, st>>>(c->tblk_sph32.p, ntb, c->sblk_sph32.p, nsb, cr, nullptr,
+                                                     c->inv_cnt.p, nullptr);
+    k_scan<<<1, 1024, 0, st>>>(c->fwd_cnt.p, nsb, c->fwd_off.p);
+    k_scan<<<1, 1024, 0, st>>>(c->inv_cnt.p, ntb, c->inv_off.p);
+    int64_t tot[2] = {0, 0};
+    e = cudaMemcpyAsync(&tot[0], c->fwd_off.p + nsb, 8, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&tot[1], c->inv_off.p + ntb, 8, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_error(c, e, "pair list count");
+    if (tot[0] != tot[1]) return set_error(c, SDOT_ECUDA, "block-pair lists disagree");
+    const int64_t npairs = tot[0];
+    e = c->fwd_t.alloc(npairs + 1);
+    if (e == cudaSuccess) e = c->inv_b.alloc(npairs + 1);
+    if (e != cudaSuccess) return cuda_error(c, e, "pair list alloc");
+    k_pairs<true><<<(nsb + 255) / 256, 256, 0, st>>>(c->sblk_sph32.p, nsb, c->tblk_sph32.p, ntb, cr, c->fwd_off.p,
+                                                    nullptr, c->fwd_t.p);
+    k_pairs<false><<<(ntb + 255) / 256, 256, 0, st>>>(c->tblk_sph32.p, ntb, c->sblk_sph32.p, nsb, cr, c->inv_off.p,
+                                                     nullptr, c->inv_b.p);
+    c->klaunch[6] += 6;
+    if (c->profiling) cudaEventRecord(c->pev[7], st);
+    // 2. partial buffer: all pairs at once when it fits the cap, else target-block groups
+    const int64_t cap_pairs = std::max<int64_t>(1, (int64_t)(c->part_cap_bytes / (TBLK_KD * sizeof(double))));
+    std::vector<int64_t> inv_host;
+    std::vector<std::pair<int, int>> groups;
+    if (npairs <= cap_pairs) {
+        groups.push_back({0, ntb});
+    } else {
+        inv_host.resize(ntb + 1);
+        e = cudaMemcpyAsync(inv_host.data(), c->inv_off.p, (ntb + 1) * 8, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return cuda_error(c, e, "pair list copy");
+        int t0 = 0;
+        while (t0 < ntb) {
+            int t1 = t0 + 1;
+            while (t1 < ntb && inv_host[t1 + 1] - inv_host[t0] <= cap_pairs) ++t1;
+            groups.push_back({t0, t1});
+            t0 = t1;
+        }
+    }
+    int64_t part_pairs = npairs;
+    if (groups.size() > 1) {
+        part_pairs = 0;
+        for (auto &g : groups) part_pairs = std::max(part_pairs, inv_host[g.second] - inv_host[g.first]);
+    }
+    e = c->part.alloc((size_t)std::max<int64_t>(1, part_pairs) * TBLK_KD);
+    if (e != cudaSuccess) return cuda_error(c, e, "partial buffer alloc");
+    FusedArgs f{};
+    f.x = c->x.p; f.rho = c->rho.p; f.jxw = c->jxw.p; f.w = c->w.p; f.cell_ctr = c->cell_ctr.p;
+    f.tpk = c->tpack.p; f.sblk_cell = c->sblk_cell.p; f.sblk_sph = c->sblk_sph.p; f.tblk_off = c->tblk_off.p;
+    f.fwd_off = c->fwd_off.p; f.inv_off = c->inv_off.p; f.fwd_t = c->fwd_t.p; f.inv_b = c->inv_b.p;
+    f.part = c->part.p; f.Lq = c->Lq.p; f.valpart = c->blkpart.p;
+    f.cullt = std::isnan(r) ? 0.0 : std::min(r, 1e300);
+    const bool fp32b = c->precision != SDOT_PREC_FP64;
+    for (size_t gi = 0; gi < groups.size(); ++gi) {
+        f.do_a = gi == 0;
+        f.do_b = 1;
+        f.tlo = groups[gi].first;
+        f.thi = groups[gi].second;
+        f.part_base = groups.size() == 1 ? 0 : inv_host[f.tlo];
+        if (c->dim == 2) dispatch_fused<2>(c, f, a, fp32b);
+        else dispatch_fused<3>(c, f, a, fp32b);
+        if (c->profiling && gi + 1 == groups.size()) cudaEventRecord(c->pev[2], st);
+        const int nw = f.thi - f.tlo;
+        k_grad_reduce<<<(unsigned)((nw * 32 + 255) / 256), 256, 0, st>>>(c->tblk_off.p, c->inv_off.p, f.tlo, f.thi,
+                                                                         f.part_base, c->part.p, 1, c->nu.p, c->gpart.p);
+        c->klaunch[2] += 1;
+        c->klaunch[3] += 1;
+    }
+    if (c->profiling) cudaEventRecord(c->pev[3], st);
+    return cuda_error(c, cudaGetLastError(), "truncated evaluation");
+}
+
+}  // namespace sdot

@@ -199,12 +199,15 @@ class SotSolver:
     def set_profiling(self, enable: bool = True):
         self._check(self._L.sdot_set_profiling(self._h, int(enable)))
 
-    PHASES = ("threshold", "target_prep", "value_sweep", "gradient_sweep", "finalize", "layout")
+    PHASES = ("threshold", "target_prep", "value_sweep", "gradient_sweep", "finalize", "layout", "pair_lists")
 
     def kernel_times(self, reset: bool = False) -> dict:
-        ms = np.zeros(6)
-        ln = np.zeros(6, dtype=np.int64)
-        self._check(self._L.sdot_get_kernel_times(self._h, ms.ctypes.data, ln.ctypes.data, 6, int(reset)))
+        """Device ms and launches per phase.  Truncated path: value_sweep is the
+        fused kernel (both exponential sweeps), gradient_sweep the partial
+        reduction, pair_lists the block-pair list build."""
+        ms = np.zeros(7)
+        ln = np.zeros(7, dtype=np.int64)
+        self._check(self._L.sdot_get_kernel_times(self._h, ms.ctypes.data, ln.ctypes.data, 7, int(reset)))
         return {k: {"ms": float(ms[i]), "launches": int(ln[i])} for i, k in enumerate(self.PHASES)}
 
     # ---------------------------------------------------------------- getters
