@@ -3,6 +3,7 @@
 #include <float.h>
 #include <math.h>
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -160,13 +161,44 @@ void update_geometry(sdot_ctx *c)
     for (int64_t b = 0; b < c->ntblk; ++b) t32[b] = sphere32(&c->tgt_sph_host[b * 4], sc);
     cudaMemcpy(c->sblk_sph32.p, s32.data(), s32.size() * sizeof(float4), cudaMemcpyHostToDevice);
     cudaMemcpy(c->tblk_sph32.p, t32.data(), t32.size() * sizeof(float4), cudaMemcpyHostToDevice);
+    // super-blocks of 32 consecutive blocks: sphere containing the member spheres
+    auto supers = [&](const std::vector<double> &sph, int64_t nb, std::vector<float4> &out) {
+        const int64_t ns = (nb + 31) / 32;
+        out.resize(ns);
+        for (int64_t si = 0; si < ns; ++si) {
+            double lo[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, hi[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+            const int64_t b0 = si * 32, b1 = std::min(nb, b0 + 32);
+            for (int64_t b = b0; b < b1; ++b)
+                for (int d = 0; d < 3; ++d) {
+                    lo[d] = std::min(lo[d], sph[b * 4 + d]);
+                    hi[d] = std::max(hi[d], sph[b * 4 + d]);
+                }
+            double cc[4];
+            for (int d = 0; d < 3; ++d) cc[d] = 0.5 * (lo[d] + hi[d]);
+            double R = 0.0;
+            for (int64_t b = b0; b < b1; ++b) {
+                double s2 = 0.0;
+                for (int d = 0; d < 3; ++d) s2 += (sph[b * 4 + d] - cc[d]) * (sph[b * 4 + d] - cc[d]);
+                R = std::max(R, std::sqrt(s2) + sph[b * 4 + 3]);
+            }
+            cc[3] = R * (1.0 + 1e-12);
+            out[si] = sphere32(cc, sc);
+        }
+    };
+    std::vector<float4> ss, ts;
+    supers(c->src_sph_host, c->nsblk, ss);
+    supers(c->tgt_sph_host, c->ntblk, ts);
+    c->ssup_sph32.alloc(ss.size());
+    c->tsup_sph32.alloc(ts.size());
+    cudaMemcpy(c->ssup_sph32.p, ss.data(), ss.size() * sizeof(float4), cudaMemcpyHostToDevice);
+    cudaMemcpy(c->tsup_sph32.p, ts.data(), ts.size() * sizeof(float4), cudaMemcpyHostToDevice);
 }
 
 size_t device_bytes(const sdot_ctx *c)
 {
     return c->x.bytes() + c->rho.bytes() + c->jxw.bytes() + c->w.bytes() + c->cell_ctr.bytes() +
            c->sblk_sph.bytes() + c->sblk_sph32.bytes() + c->sblk_cell.bytes() + c->tblk_off.bytes() +
-           c->tblk_sph32.bytes() + c->part.bytes() + c->fwd_t.bytes() + c->inv_b.bytes() +
+           c->tblk_sph32.bytes() + c->part.bytes() + c->fwd_t.bytes() + c->pmask.bytes() + c->pmpre.bytes() +
            c->y.bytes() + c->nu.bytes() + c->perm.bytes() +
            c->tblk_sph.bytes() + c->psi.bytes() + c->grad.bytes() + c->tpack.bytes() + c->Lq.bytes() +
            c->gpart.bytes() + c->blkpart.bytes() + c->scal.bytes() + c->redpart.bytes() + c->io_a.bytes() +
@@ -377,6 +409,12 @@ sdot_status sdot_create(sdot_ctx **out, const sdot_options *opts)
     }
     memset(c->scal_host, 0, SC_COUNT * sizeof(double));
     sdot_default_params(&c->prm);
+    // cap on the gradient-partial buffer of the truncated path (bytes); above
+    // it the source blocks are processed in groups
+    if (const char *cap = getenv("SDOT_PART_CAP_BYTES")) {
+        const long long v = atoll(cap);
+        if (v > 0) c->part_cap_bytes = (size_t)v;
+    }
     *out = c;
     return SDOT_OK;
 }
@@ -389,8 +427,10 @@ void sdot_destroy(sdot_ctx *c)
         if (c->stream) cudaStreamSynchronize(c->stream);
         c->x.release(); c->rho.release(); c->jxw.release(); c->w.release();
         c->cell_ctr.release(); c->sblk_sph.release(); c->sblk_sph32.release(); c->sblk_cell.release();
-        c->tblk_off.release(); c->tblk_sph32.release(); c->part.release(); c->fwd_t.release(); c->inv_b.release();
-        c->fwd_cnt.release(); c->inv_cnt.release(); c->fwd_off.release(); c->inv_off.release();
+        c->tblk_off.release(); c->tblk_sph32.release(); c->part.release(); c->fwd_t.release();
+        c->fwd_cnt.release(); c->fwd_off.release(); c->shit.release(); c->spidx.release(); c->scount.release();
+        c->inv_cnt.release(); c->inv_off.release(); c->inv_b.release(); c->fwd2inv.release();
+        c->pmask.release(); c->pmpre.release(); c->superpair.release(); c->ssup_sph32.release(); c->tsup_sph32.release();
         c->y.release(); c->nu.release();
         c->perm.release(); c->tblk_sph.release(); c->psi.release(); c->grad.release(); c->tpack.release();
         c->Lq.release(); c->gpart.release(); c->blkpart.release(); c->scal.release(); c->redpart.release();

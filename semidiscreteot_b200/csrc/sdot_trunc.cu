@@ -53,6 +53,7 @@ constexpr int FT_MAXS = 1024;               // staged targets per chunk
 constexpr int FT_TS = 6;                    // doubles per staged target: y(3), nu, log2 nu, s*psi
 constexpr int FT_MAXT = FT_MAXS / TBLK_KD;  // target blocks per chunk
 constexpr int FT_MAXQ = 80;                 // quadrature points of one source block
+constexpr int SUPER = 32;                   // blocks per super-block of the pair-list hierarchy
 
 struct FusedArgs {
     const double *x, *rho, *jxw, *w, *cell_ctr;
@@ -60,13 +61,14 @@ struct FusedArgs {
     const int64_t *sblk_cell;    // source block -> first cell (nsblk + 1)
     const double *sblk_sph;      // FP64 centre(3), radius
     const int64_t *tblk_off;     // target block -> first target (ntblk + 1)
-    const int64_t *fwd_off, *inv_off;
-    const int *fwd_t, *inv_b;
-    double *part;                // partials, 32 per pair in inverse order
+    const int64_t *fwd_off;
+    const int *fwd_t;
+    const int64_t *fwd2inv;      // inverse position of each forward pair
+    double *part;                // partials, 32 per pair, at inverse positions minus part_base
     double *Lq;                  // per q (written by the value sweep)
     double *valpart;             // per source block: value, C, skipped, pairs
     int do_a, do_b;
-    int tlo, thi;                // gradient sweep restricted to target blocks [tlo, thi)
+    int tlo, thi;                // gradient partials only for target blocks [tlo, thi)
     int64_t part_base;           // inverse position of the first pair of tlo
     double cullt;                // per-target cull radius addend (r, enlarged)
 };
@@ -85,8 +87,8 @@ struct FTSmem {
     unsigned short cand[FT_WARPS][FT_MAXS];
     short smap[FT_MAXT][TBLK_KD]; // (chunk target block, slot) -> staged position or -1
     int ctb[FT_MAXT];             // target blocks of the chunk
-    int64_t cpos[FT_MAXT];        // their partial base index (or -1 when outside [tlo, thi))
-    int ccnt[FT_MAXT + 1];        // prefix of their sizes
+    int64_t cpos[FT_MAXT];        // their partial base index
+    int ecnt[FT_MAXT];            // survivors per examined forward entry (-1: none)
     int wcount[FT_WARPS];
     int nstg;
 };
@@ -105,34 +107,140 @@ __device__ __forceinline__ bool pair_test(float4 s, float4 t, float cr)
     return d2 <= __fmul_rn(lim, lim);
 }
 
-// mode 0: count, 1: fill.  rows <-> A, columns <-> B (A/B = source/target
-// spheres for the forward list, target/source for the inverse list).
-template <bool ROWS_ARE_SOURCE>
+// Super-block pairs: sp[si * nts + ti] = 1 iff source super-block si and
+// target super-block ti may hold a pair (the same conservative test; a
+// super-sphere contains its member spheres, so no block pair is lost).
 __global__ void __launch_bounds__(256)
-k_pairs(const float4 *__restrict__ rowsph, int nrow, const float4 *__restrict__ colsph, int ncol, float cr,
-        const int64_t *__restrict__ off, int64_t *__restrict__ cnt, int *__restrict__ out)
+k_super_pairs(const float4 *__restrict__ ssph, int nss, const float4 *__restrict__ tsph, int nts, float cr,
+              unsigned char *__restrict__ sp)
 {
-    __shared__ float4 sc[1024];
-    const int row = blockIdx.x * blockDim.x + threadIdx.x;
-    const float4 me = row < nrow ? rowsph[row] : make_float4(0.f, 0.f, 0.f, -1e30f);
-    int64_t k = 0;
-    const int64_t base = (out && row < nrow) ? off[row] : 0;
-    for (int c0 = 0; c0 < ncol; c0 += 1024) {
-        const int cn = min(1024, ncol - c0);
-        __syncthreads();
-        for (int i = threadIdx.x; i < cn; i += blockDim.x) sc[i] = colsph[c0 + i];
-        __syncthreads();
-        if (row < nrow) {
-            for (int i = 0; i < cn; ++i) {
-                const bool hit = ROWS_ARE_SOURCE ? pair_test(me, sc[i], cr) : pair_test(sc[i], me, cr);
-                if (hit) {
-                    if (out) out[base + k] = c0 + i;
-                    ++k;
-                }
-            }
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= (int64_t)nss * nts) return;
+    const int si = (int)(i / nts), ti = (int)(i - (int64_t)si * nts);
+    sp[i] = pair_test(ssph[si], tsph[ti], cr) ? 1 : 0;
+}
+
+// Warp <-> source super-block: its paired target super-blocks in ascending
+// order (shit[si * nts + h]), their count, and the inverse map
+// spidx[si * nts + ti] = h (or -1).
+__global__ void __launch_bounds__(256)
+k_super_compact(const unsigned char *__restrict__ sp, int nss, int nts, int *__restrict__ shit,
+                int *__restrict__ scount, int *__restrict__ spidx)
+{
+    const int si = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (si >= nss) return;
+    int h = 0;
+    for (int t0 = 0; t0 < nts; t0 += 32) {
+        const int ti = t0 + lane;
+        const bool on = ti < nts && sp[(int64_t)si * nts + ti];
+        const unsigned bal = __ballot_sync(0xffffffffu, on);
+        const int pos = h + __popc(bal & ((1u << lane) - 1u));
+        if (ti < nts) spidx[(int64_t)si * nts + ti] = on ? pos : -1;
+        if (on) shit[(int64_t)si * nts + pos] = ti;
+        h += __popc(bal);
+    }
+    if (lane == 0) scount[si] = h;
+}
+
+// Warp <-> source block b: for each paired target super-block h, the 32-bit
+// mask of its target blocks t with pair_test(b, t), and the number of b's
+// pairs before it; cnt[b] = total.  Pairs are ordered by t, so the forward
+// position of (b, t) is fwd_off[b] + mpre[b, h] + popc(mask[b, h] below t).
+__global__ void __launch_bounds__(256)
+k_fwd_masks(const float4 *__restrict__ sph, int nsb, const float4 *__restrict__ tph, int ntb, int nts, int hmax,
+            float cr, const int *__restrict__ shit, const int *__restrict__ scount, unsigned *__restrict__ mask,
+            int *__restrict__ mpre, int64_t *__restrict__ cnt)
+{
+    const int b = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (b >= nsb) return;
+    const float4 me = sph[b];
+    const int si = b / SUPER;
+    const int nh = scount[si];
+    int k = 0;
+    for (int h = 0; h < nh; ++h) {
+        const int t = shit[(int64_t)si * nts + h] * SUPER + lane;
+        const bool hit = t < ntb && pair_test(me, tph[t], cr);
+        const unsigned bal = __ballot_sync(0xffffffffu, hit);
+        if (lane == 0) {
+            mask[(int64_t)b * hmax + h] = bal;
+            mpre[(int64_t)b * hmax + h] = k;
+        }
+        k += __popc(bal);
+    }
+    if (lane == 0) cnt[b] = k;
+}
+
+// Forward lists from the masks: fwd_t[fwd_off[b] ..] = paired t, ascending.
+__global__ void __launch_bounds__(256)
+k_fwd_fill(int nsb, int nts, int hmax, const int *__restrict__ shit, const int *__restrict__ scount,
+           const unsigned *__restrict__ mask, const int64_t *__restrict__ fwd_off, int *__restrict__ fwd_t)
+{
+    const int b = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (b >= nsb) return;
+    const int si = b / SUPER;
+    const int nh = scount[si];
+    int64_t k = fwd_off[b];
+    for (int h = 0; h < nh; ++h) {
+        const unsigned bal = mask[(int64_t)b * hmax + h];
+        if ((bal >> lane) & 1u) fwd_t[k + __popc(bal & ((1u << lane) - 1u))] = shit[(int64_t)si * nts + h] * SUPER + lane;
+        k += __popc(bal);
+    }
+}
+
+// Inverse list (warp <-> target block t): source blocks b paired with t,
+// ascending b, visiting the source super-blocks paired with t's super-block.
+// Evaluates pair_test(b, t) with the same operands as k_fwd_masks.
+template <bool FILL>
+__global__ void __launch_bounds__(256)
+k_inv_list(const float4 *__restrict__ sph, int nsb, int nss, const float4 *__restrict__ tph, int ntb, int nts,
+           float cr, const unsigned char *__restrict__ sp, const int64_t *__restrict__ off, int64_t *__restrict__ cnt,
+           int *__restrict__ out)
+{
+    const int t = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (t >= ntb) return;
+    const float4 me = tph[t];
+    const int ti = t / SUPER;
+    int64_t k = FILL ? off[t] : 0;
+    for (int s0 = 0; s0 < nss; s0 += 32) {
+        const int sl = s0 + lane;
+        unsigned sbal = __ballot_sync(0xffffffffu, sl < nss && sp[(int64_t)sl * nts + ti]);
+        while (sbal) {
+            const int si = s0 + __ffs(sbal) - 1;
+            sbal &= sbal - 1;
+            const int b = si * SUPER + lane;
+            const bool hit = b < nsb && pair_test(sph[b], me, cr);
+            const unsigned bal = __ballot_sync(0xffffffffu, hit);
+            if (FILL && hit) out[k + __popc(bal & ((1u << lane) - 1u))] = b;
+            k += __popc(bal);
         }
     }
-    if (!out && row < nrow) cnt[row] = k;
+    if (!FILL && lane == 0) cnt[t] = k;
+}
+
+// fwd2inv[k] = inverse position of forward pair k (warp <-> source block b,
+// lane <-> its pairs; binary search of b in the inverse list of t; -1 if absent).
+__global__ void __launch_bounds__(256)
+k_fwd2inv(int nsb, const int64_t *__restrict__ fwd_off, const int *__restrict__ fwd_t,
+          const int64_t *__restrict__ inv_off, const int *__restrict__ inv_b, int64_t *__restrict__ fwd2inv)
+{
+    const int b = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (b >= nsb) return;
+    for (int64_t k = fwd_off[b] + lane; k < fwd_off[b + 1]; k += 32) {
+        const int t = fwd_t[k];
+        int64_t lo = inv_off[t], hi = inv_off[t + 1];
+        const int64_t end = hi;
+        while (lo < hi) {
+            const int64_t mid = (lo + hi) >> 1;
+            if (inv_b[mid] < b) lo = mid + 1;
+            else hi = mid;
+        }
+        fwd2inv[k] = (lo < end && inv_b[lo] == b) ? lo : -1;
+    }
 }
 
 // exclusive scan of n counts into off[0..n] (single CTA, order-fixed)
@@ -167,89 +275,98 @@ __global__ void __launch_bounds__(1024) k_scan(const int64_t *__restrict__ cnt, 
 // fused value + gradient sweeps
 // ---------------------------------------------------------------------------
 
-// stage the targets of fwd pairs [k0, k1) of block b; returns the number of pairs taken
+// Stage the targets of the forward pairs [k0, k1) of block b, culled per
+// target against the block sphere: each warp takes target blocks (lane <->
+// target), counts its survivors with a ballot, and whole target blocks are
+// accepted in list order while the staged total fits FT_MAXS.  Returns the
+// number of forward entries consumed; staged order = (target block, slot).
 template <int DIM>
-__device__ int stage_chunk(FTSmem &sm, const FusedArgs &f, const EvalArgs &a, int64_t k0, int64_t k1,
-                           const double *bc, double rcull2, bool for_b)
+__device__ int stage_chunk(FTSmem &sm, const FusedArgs &f, int64_t k0, int64_t k1, const double *bc, double rcull2,
+                           bool for_b)
 {
-    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    // choose target blocks while the worst case fits
-    if (tid == 0) {
-        int n = 0, acc = 0;
-        for (int64_t k = k0; k < k1 && n < FT_MAXT; ++k) {
-            const int t = f.fwd_t[k];
-            const int sz = (int)(f.tblk_off[t + 1] - f.tblk_off[t]);
-            if (acc + sz > FT_MAXS) break;
-            sm.ctb[n] = t;
-            sm.ccnt[n] = acc;
-            acc += sz;
-            ++n;
-        }
-        sm.ccnt[n] = acc;
-        sm.wcount[0] = n;
-    }
-    __syncthreads();
-    const int nt = sm.wcount[0];
-    const int total = sm.ccnt[nt];
-    // partial base of each pair (inverse position), -1 outside [tlo, thi)
-    if (for_b && tid < nt) {
-        const int t = sm.ctb[tid];
-        int64_t pos = -1;
-        if (t >= f.tlo && t < f.thi) {
-            int64_t lo = f.inv_off[t], hi = f.inv_off[t + 1];
-            const int b = blockIdx.x;
-            while (lo < hi) {
-                const int64_t mid = (lo + hi) >> 1;
-                if (f.inv_b[mid] < b) lo = mid + 1;
-                else hi = mid;
-            }
-            if (lo < f.inv_off[t + 1] && f.inv_b[lo] == b) pos = (lo - f.part_base) * TBLK_KD;
-        }
-        sm.cpos[tid] = pos;
-    }
-    for (int i = tid; i < FT_MAXT * TBLK_KD; i += blockDim.x) (&sm.smap[0][0])[i] = -1;
-    __syncthreads();
-    // per-target cull against the block sphere, in-order compaction
-    int base = 0;
-    for (int e0 = 0; e0 < total; e0 += blockDim.x) {
-        const int e = e0 + tid;
-        bool keep = false;
-        int ti = 0;
-        int64_t j = 0;
-        if (e < total) {
-            while (ti + 1 < nt && sm.ccnt[ti + 1] <= e) ++ti;
-            j = f.tblk_off[sm.ctb[ti]] + (e - sm.ccnt[ti]);
-            const double *tp = f.tpk + j * TPACK;
-            double d2 = 0.0;
+    constexpr int SUB = 4;                       // target blocks per warp per iteration
+    constexpr int PER = FT_WARPS * SUB;          // entries examined per iteration
+    const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
+    int total = 0, nb = 0;
+    int64_t k = k0;
+    while (k < k1 && nb < FT_MAXT) {
+        unsigned bal[SUB];
+        int tt[SUB];
 #pragma unroll
-            for (int d = 0; d < DIM; ++d) {
-                const double t = tp[d] - bc[d];
-                d2 += t * t;
-            }
-            keep = d2 <= rcull2;
-        }
-        const unsigned bal = __ballot_sync(0xffffffffu, keep);
-        if (lane == 0) sm.wcount[w] = __popc(bal);
-        __syncthreads();
-        int off = base, tot = 0;
-        for (int i = 0; i < FT_WARPS; ++i) {
-            if (i < w) off += sm.wcount[i];
-            tot += sm.wcount[i];
-        }
-        if (keep) {
-            const int pos = off + __popc(bal & ((1u << lane) - 1u));
-            const double *tp = f.tpk + j * TPACK;
-            double *dst = sm.stg + pos * FT_TS;
+        for (int s = 0; s < SUB; ++s) {
+            const int idx = s * FT_WARPS + wp;
+            const int64_t e = k + idx;
+            bal[s] = 0u;
+            tt[s] = -1;
+            int cntv = -1;
+            if (e < k1 && nb + idx < FT_MAXT) {
+                const int t = f.fwd_t[e];
+                tt[s] = t;
+                const int64_t j0 = f.tblk_off[t];
+                const int sz = (int)(f.tblk_off[t + 1] - j0);
+                bool keep = false;
+                if (lane < sz) {
+                    const double *tp = f.tpk + (j0 + lane) * TPACK;
+                    double d2 = 0.0;
 #pragma unroll
-            for (int d = 0; d < FT_TS; ++d) dst[d] = tp[d];
-            sm.smap[ti][e - sm.ccnt[ti]] = (short)pos;
+                    for (int d = 0; d < DIM; ++d) {
+                        const double q = tp[d] - bc[d];
+                        d2 += q * q;
+                    }
+                    keep = d2 <= rcull2;
+                }
+                bal[s] = __ballot_sync(0xffffffffu, keep);
+                cntv = __popc(bal[s]);
+            }
+            if (lane == 0) sm.ecnt[idx] = cntv;
         }
         __syncthreads();
-        base += tot;
+        // accept entries in list order while they fit (every thread computes the same prefix)
+        int nacc = 0, run = total;
+        int mypre[SUB] = {0, 0, 0, 0};
+        for (int i = 0; i < PER; ++i) {
+            const int c = sm.ecnt[i];
+            if (c < 0 || run + c > FT_MAXS) break;
+#pragma unroll
+            for (int s = 0; s < SUB; ++s)
+                if (i == s * FT_WARPS + wp) mypre[s] = run;
+            run += c;
+            ++nacc;
+        }
+#pragma unroll
+        for (int s = 0; s < SUB; ++s) {
+            const int idx = s * FT_WARPS + wp;
+            if (idx < nacc) {
+                const int slot = nb + idx;
+                const int64_t j0 = f.tblk_off[tt[s]];
+                const bool keep = (bal[s] >> lane) & 1u;
+                short pos = -1;
+                if (keep) {
+                    pos = (short)(mypre[s] + __popc(bal[s] & ((1u << lane) - 1u)));
+                    const double *tp = f.tpk + (j0 + lane) * TPACK;
+                    double *dst = sm.stg + pos * FT_TS;
+#pragma unroll
+                    for (int d = 0; d < FT_TS; ++d) dst[d] = tp[d];
+                }
+                sm.smap[slot][lane] = pos;
+                if (lane == 0) {
+                    const int tb = tt[s];
+                    sm.ctb[slot] = tb;
+                    const int64_t ip = f.fwd2inv[k + idx];
+                    sm.cpos[slot] = (for_b && ip >= 0 && tb >= f.tlo && tb < f.thi) ? (ip - f.part_base) * TBLK_KD
+                                                                                    : (int64_t)-1;
+                }
+            }
+        }
+        total = run;
+        nb += nacc;
+        k += nacc;
+        __syncthreads();
+        if (nacc < PER) break;  // capacity reached, list exhausted or block limit
     }
-    if (tid == 0) sm.nstg = base;
+    if (tid == 0) sm.nstg = total;
     __syncthreads();
-    return nt;
+    return nb;
 }
 
 template <int DIM, int QL, bool FP32B>
@@ -304,7 +421,7 @@ k_fused(FusedArgs f, EvalArgs a)
         for (int k = 0; k < QL; ++k) { M[k] = -CUDART_INF; S[k] = 0.0; mx[k] = -CUDART_INF; }
         double npairs = 0.0;
         for (int64_t k = k0; k < k1;) {
-            const int nt = stage_chunk<DIM>(sm, f, a, k, k1, bc, rcull2, f.do_b != 0);
+            const int nt = stage_chunk<DIM>(sm, f, k, k1, bc, rcull2, f.do_b != 0);
             const int nstg = sm.nstg;
             ++chunks;
             // exact candidate test for this unit's cell, in-order compaction + mask
@@ -397,22 +514,13 @@ k_fused(FusedArgs f, EvalArgs a)
         if (single_end >= 0) {
             nt = (int)(single_end - k0);   // staged data and masks of the single chunk are still in smem
             if (tid < nt) {
-                const int t = sm.ctb[tid];
-                int64_t pos = -1;
-                if (t >= f.tlo && t < f.thi) {
-                    int64_t lo = f.inv_off[t], hi = f.inv_off[t + 1];
-                    while (lo < hi) {
-                        const int64_t mid = (lo + hi) >> 1;
-                        if (f.inv_b[mid] < b) lo = mid + 1;
-                        else hi = mid;
-                    }
-                    if (lo < f.inv_off[t + 1] && f.inv_b[lo] == b) pos = (lo - f.part_base) * TBLK_KD;
-                }
-                sm.cpos[tid] = pos;
+                const int tb = sm.ctb[tid];
+                const int64_t ip = f.fwd2inv[k0 + tid];
+                sm.cpos[tid] = (ip >= 0 && tb >= f.tlo && tb < f.thi) ? (ip - f.part_base) * TBLK_KD : (int64_t)-1;
             }
             __syncthreads();
         } else {
-            nt = stage_chunk<DIM>(sm, f, a, k, k1, bc, rcull2, true);
+            nt = stage_chunk<DIM>(sm, f, k, k1, bc, rcull2, true);
             // masks for this chunk (one warp per cell; units of group 0)
             if (valid && grp == 0) {
                 for (int b0 = 0; b0 < sm.nstg; b0 += 32) {
@@ -481,21 +589,25 @@ k_fused(FusedArgs f, EvalArgs a)
     }
 }
 
-// gradient of target block t = sum over its pairs (ascending source block)
+// gradient of target block t = sum of its pair partials in inverse order
+// (ascending source block), lane <-> target; contiguous rows of 32 doubles.
 __global__ void __launch_bounds__(256)
 k_grad_reduce(const int64_t *__restrict__ tblk_off, const int64_t *__restrict__ inv_off, int tlo, int thi,
-              int64_t part_base, const double *__restrict__ part, int fp32_nu_folded, const double *__restrict__ nu,
-              double *__restrict__ gacc)
+              int64_t part_base, const double *__restrict__ part, double *__restrict__ gacc)
 {
     const int t = tlo + (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
     if (t >= thi) return;
     const int64_t p0 = inv_off[t], p1 = inv_off[t + 1];
-    double acc = 0.0;
-    for (int64_t p = p0; p < p1; ++p) acc += part[(p - part_base) * TBLK_KD + lane];
+    double a0 = 0.0, a1 = 0.0;
+    int64_t p = p0;
+    for (; p + 1 < p1; p += 2) {  // two independent chains, combined in a fixed order
+        a0 += part[(p - part_base) * TBLK_KD + lane];
+        a1 += part[(p + 1 - part_base) * TBLK_KD + lane];
+    }
+    if (p < p1) a0 += part[(p - part_base) * TBLK_KD + lane];
     const int64_t j = tblk_off[t] + lane;
-    if (j < tblk_off[t + 1]) gacc[j] = acc * (fp32_nu_folded ? 1.0 : 1.0);
-    (void)nu;
+    if (j < tblk_off[t + 1]) gacc[j] = a0 + a1;
 }
 
 // ---------------------------------------------------------------------------
@@ -503,44 +615,65 @@ k_grad_reduce(const int64_t *__restrict__ tblk_off, const int64_t *__restrict__ 
 // ---------------------------------------------------------------------------
 
 template <int DIM, int QL, bool FP32B>
-static void launch_fused(sdot_ctx *c, const FusedArgs &f, const EvalArgs &a, size_t smem)
+static void launch_fused(sdot_ctx *c, const FusedArgs &f, const EvalArgs &a, size_t smem, int nb)
 {
     cudaFuncSetAttribute(k_fused<DIM, QL, FP32B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_fused<DIM, QL, FP32B><<<(unsigned)c->nsblk, FT_WARPS * 32, smem, c->stream>>>(f, a);
+    k_fused<DIM, QL, FP32B><<<(unsigned)nb, FT_WARPS * 32, smem, c->stream>>>(f, a);
 }
 
 template <int DIM>
-static void dispatch_fused(sdot_ctx *c, const FusedArgs &f, const EvalArgs &a, bool fp32b)
+static void dispatch_fused(sdot_ctx *c, const FusedArgs &f, const EvalArgs &a, bool fp32b, int nb)
 {
     const size_t smem = sizeof(FTSmem);
     if (a.ql <= 4) {
-        if (fp32b) launch_fused<DIM, 4, true>(c, f, a, smem);
-        else launch_fused<DIM, 4, false>(c, f, a, smem);
+        if (fp32b) launch_fused<DIM, 4, true>(c, f, a, smem, nb);
+        else launch_fused<DIM, 4, false>(c, f, a, smem, nb);
     } else if (a.ql <= 8) {
-        if (fp32b) launch_fused<DIM, 8, true>(c, f, a, smem);
-        else launch_fused<DIM, 8, false>(c, f, a, smem);
+        if (fp32b) launch_fused<DIM, 8, true>(c, f, a, smem, nb);
+        else launch_fused<DIM, 8, false>(c, f, a, smem, nb);
     } else {
-        if (fp32b) launch_fused<DIM, 9, true>(c, f, a, smem);
-        else launch_fused<DIM, 9, false>(c, f, a, smem);
+        if (fp32b) launch_fused<DIM, 9, true>(c, f, a, smem, nb);
+        else launch_fused<DIM, 9, false>(c, f, a, smem, nb);
     }
 }
 
 sdot_status run_trunc(sdot_ctx *c, const EvalArgs &a, double r)
 {
     cudaStream_t st = c->stream;
-    // 1. block-pair lists (conservative FP32 test, identical in both directions)
+    // 1. block-pair structure (conservative FP32 test)
     const float cr = (float)(std::min(r, 1e30) * (1.0 + 1e-6) + 1e-6 * c->coord_scale);
     const int nsb = (int)c->nsblk, ntb = (int)c->ntblk;
+    const int nss = (nsb + SUPER - 1) / SUPER, nts = (ntb + SUPER - 1) / SUPER;
     cudaError_t e = c->fwd_cnt.alloc(nsb + 1);
-    if (e == cudaSuccess) e = c->inv_cnt.alloc(ntb + 1);
     if (e == cudaSuccess) e = c->fwd_off.alloc(nsb + 1);
+    if (e == cudaSuccess) e = c->superpair.alloc((size_t)nss * nts);
+    if (e == cudaSuccess) e = c->shit.alloc((size_t)nss * nts);
+    if (e == cudaSuccess) e = c->spidx.alloc((size_t)nss * nts);
+    if (e == cudaSuccess) e = c->scount.alloc(nss + 1);
+    if (e != cudaSuccess) return cuda_error(c, e, "pair list alloc");
+    k_super_pairs<<<(unsigned)(((int64_t)nss * nts + 255) / 256), 256, 0, st>>>(c->ssup_sph32.p, nss, c->tsup_sph32.p,
+                                                                             nts, cr, c->superpair.p);
+    k_super_compact<<<(unsigned)(((int64_t)nss * 32 + 255) / 256), 256, 0, st>>>(c->superpair.p, nss, nts, c->shit.p,
+                                                                              c->scount.p, c->spidx.p);
+    std::vector<int> sc((size_t)nss);
+    e = cudaMemcpyAsync(sc.data(), c->scount.p, nss * sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_error(c, e, "pair list count");
+    int hmax = 1;
+    for (int v : sc) hmax = std::max(hmax, v);
+    e = c->pmask.alloc((size_t)nsb * hmax);
+    if (e == cudaSuccess) e = c->pmpre.alloc((size_t)nsb * hmax);
+    if (e != cudaSuccess) return cuda_error(c, e, "pair mask alloc");
+    const unsigned gw = (unsigned)(((int64_t)nsb * 32 + 255) / 256);
+    k_fwd_masks<<<gw, 256, 0, st>>>(c->sblk_sph32.p, nsb, c->tblk_sph32.p, ntb, nts, hmax, cr, c->shit.p, c->scount.p,
+                                    c->pmask.p, c->pmpre.p, c->fwd_cnt.p);
+    k_scan<<<1, 1024, 0, st>>>(c->fwd_cnt.p, nsb, c->fwd_off.p);
+    e = c->inv_cnt.alloc(ntb + 1);
     if (e == cudaSuccess) e = c->inv_off.alloc(ntb + 1);
     if (e != cudaSuccess) return cuda_error(c, e, "pair list alloc");
-    k_pairs<true><<<(nsb + 255) / 256, 256, 0, st>>>(c->sblk_sph32.p, nsb, c->tblk_sph32.p, ntb, cr, nullptr,
-                                                    c->fwd_cnt.p, nullptr);
-    k_pairs<false><<<(ntb + 255) / 256, 256, 0, st>>>(c->tblk_sph32.p, ntb, c->sblk_sph32.p, nsb, cr, nullptr,
-                                                     c->inv_cnt.p, nullptr);
-    k_scan<<<1, 1024, 0, st>>>(c->fwd_cnt.p, nsb, c->fwd_off.p);
+    const unsigned gt = (unsigned)(((int64_t)ntb * 32 + 255) / 256);
+    k_inv_list<false><<<gt, 256, 0, st>>>(c->sblk_sph32.p, nsb, nss, c->tblk_sph32.p, ntb, nts, cr, c->superpair.p,
+                                          nullptr, c->inv_cnt.p, nullptr);
     k_scan<<<1, 1024, 0, st>>>(c->inv_cnt.p, ntb, c->inv_off.p);
     int64_t tot[2] = {0, 0};
     e = cudaMemcpyAsync(&tot[0], c->fwd_off.p + nsb, 8, cudaMemcpyDeviceToHost, st);
@@ -551,43 +684,42 @@ sdot_status run_trunc(sdot_ctx *c, const EvalArgs &a, double r)
     const int64_t npairs = tot[0];
     e = c->fwd_t.alloc(npairs + 1);
     if (e == cudaSuccess) e = c->inv_b.alloc(npairs + 1);
+    if (e == cudaSuccess) e = c->fwd2inv.alloc(npairs + 1);
     if (e != cudaSuccess) return cuda_error(c, e, "pair list alloc");
-    k_pairs<true><<<(nsb + 255) / 256, 256, 0, st>>>(c->sblk_sph32.p, nsb, c->tblk_sph32.p, ntb, cr, c->fwd_off.p,
-                                                    nullptr, c->fwd_t.p);
-    k_pairs<false><<<(ntb + 255) / 256, 256, 0, st>>>(c->tblk_sph32.p, ntb, c->sblk_sph32.p, nsb, cr, c->inv_off.p,
-                                                     nullptr, c->inv_b.p);
-    c->klaunch[6] += 6;
+    k_fwd_fill<<<gw, 256, 0, st>>>(nsb, nts, hmax, c->shit.p, c->scount.p, c->pmask.p, c->fwd_off.p, c->fwd_t.p);
+    k_inv_list<true><<<gt, 256, 0, st>>>(c->sblk_sph32.p, nsb, nss, c->tblk_sph32.p, ntb, nts, cr, c->superpair.p,
+                                         c->inv_off.p, nullptr, c->inv_b.p);
+    k_fwd2inv<<<gw, 256, 0, st>>>(nsb, c->fwd_off.p, c->fwd_t.p, c->inv_off.p, c->inv_b.p, c->fwd2inv.p);
+    c->klaunch[6] += 9;
     if (c->profiling) cudaEventRecord(c->pev[7], st);
-    // 2. partial buffer: all pairs at once when it fits the cap, else target-block groups
+    // 2. partial buffer (inverse order): all pairs at once under the cap, else target-block groups
     const int64_t cap_pairs = std::max<int64_t>(1, (int64_t)(c->part_cap_bytes / (TBLK_KD * sizeof(double))));
-    std::vector<int64_t> inv_host;
     std::vector<std::pair<int, int>> groups;
+    std::vector<int64_t> inv_host;
+    int64_t part_pairs = npairs;
     if (npairs <= cap_pairs) {
         groups.push_back({0, ntb});
     } else {
-        inv_host.resize(ntb + 1);
-        e = cudaMemcpyAsync(inv_host.data(), c->inv_off.p, (ntb + 1) * 8, cudaMemcpyDeviceToHost, st);
+        inv_host.resize((size_t)ntb + 1);
+        e = cudaMemcpyAsync(inv_host.data(), c->inv_off.p, (ntb + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) return cuda_error(c, e, "pair list copy");
+        part_pairs = 0;
         int t0 = 0;
         while (t0 < ntb) {
             int t1 = t0 + 1;
             while (t1 < ntb && inv_host[t1 + 1] - inv_host[t0] <= cap_pairs) ++t1;
             groups.push_back({t0, t1});
+            part_pairs = std::max(part_pairs, inv_host[t1] - inv_host[t0]);
             t0 = t1;
         }
-    }
-    int64_t part_pairs = npairs;
-    if (groups.size() > 1) {
-        part_pairs = 0;
-        for (auto &g : groups) part_pairs = std::max(part_pairs, inv_host[g.second] - inv_host[g.first]);
     }
     e = c->part.alloc((size_t)std::max<int64_t>(1, part_pairs) * TBLK_KD);
     if (e != cudaSuccess) return cuda_error(c, e, "partial buffer alloc");
     FusedArgs f{};
     f.x = c->x.p; f.rho = c->rho.p; f.jxw = c->jxw.p; f.w = c->w.p; f.cell_ctr = c->cell_ctr.p;
     f.tpk = c->tpack.p; f.sblk_cell = c->sblk_cell.p; f.sblk_sph = c->sblk_sph.p; f.tblk_off = c->tblk_off.p;
-    f.fwd_off = c->fwd_off.p; f.inv_off = c->inv_off.p; f.fwd_t = c->fwd_t.p; f.inv_b = c->inv_b.p;
+    f.fwd_off = c->fwd_off.p; f.fwd_t = c->fwd_t.p; f.fwd2inv = c->fwd2inv.p;
     f.part = c->part.p; f.Lq = c->Lq.p; f.valpart = c->blkpart.p;
     f.cullt = std::isnan(r) ? 0.0 : std::min(r, 1e300);
     const bool fp32b = c->precision != SDOT_PREC_FP64;
@@ -597,12 +729,13 @@ sdot_status run_trunc(sdot_ctx *c, const EvalArgs &a, double r)
         f.tlo = groups[gi].first;
         f.thi = groups[gi].second;
         f.part_base = groups.size() == 1 ? 0 : inv_host[f.tlo];
-        if (c->dim == 2) dispatch_fused<2>(c, f, a, fp32b);
-        else dispatch_fused<3>(c, f, a, fp32b);
+        if (c->dim == 2) dispatch_fused<2>(c, f, a, fp32b, nsb);
+        else dispatch_fused<3>(c, f, a, fp32b, nsb);
         if (c->profiling && gi + 1 == groups.size()) cudaEventRecord(c->pev[2], st);
         const int nw = f.thi - f.tlo;
-        k_grad_reduce<<<(unsigned)((nw * 32 + 255) / 256), 256, 0, st>>>(c->tblk_off.p, c->inv_off.p, f.tlo, f.thi,
-                                                                         f.part_base, c->part.p, 1, c->nu.p, c->gpart.p);
+        k_grad_reduce<<<(unsigned)(((int64_t)nw * 32 + 255) / 256), 256, 0, st>>>(c->tblk_off.p, c->inv_off.p, f.tlo,
+                                                                                 f.thi, f.part_base, c->part.p,
+                                                                                 c->gpart.p);
         c->klaunch[2] += 1;
         c->klaunch[3] += 1;
     }
