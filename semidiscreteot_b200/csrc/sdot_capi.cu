@@ -489,6 +489,17 @@ sdot_status sdot_set_source(sdot_ctx *c, int dim, int64_t n_q, const double *x, 
             if (hw[qd] < 0) nonneg = false;
         }
     }
+    double dmax = 0.0;
+    for (int64_t k = 0; k < n_cells; ++k)
+        for (int64_t i = 0; i < qpc; ++i) {
+            double s2 = 0.0;
+            for (int d = 0; d < dim; ++d) {
+                const double t = hx[(k * qpc + i) * dim + d] - hc[k * dim + d];
+                s2 += t * t;
+            }
+            dmax = std::max(dmax, std::sqrt(s2));
+        }
+    c->delta_max = dmax;
     const int64_t nsblk = (int64_t)bounds.size() - 1;
     std::vector<double> ssph(nsblk * 4);
     for (int64_t b = 0; b < nsblk; ++b) {

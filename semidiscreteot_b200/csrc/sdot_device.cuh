@@ -49,6 +49,23 @@ __device__ __forceinline__ double exp2_16(double u, const double *tab)
     return __hiloint2double(hi, __double2loint(r));
 }
 
+// exp2_16 without the lower clamp, for arguments proven >= -16000 by the caller.
+__device__ __forceinline__ double exp2_16_nc(double u, const double *tab)
+{
+    const double magic = 6755399441055744.0;  // 1.5 * 2^52
+    const double v = __dadd_rn(u, magic);
+    const int n = __double2loint(v);
+    const double f = __dsub_rn(u, __dsub_rn(v, magic));
+    double p = fma(f, 0x1.5d87fe78a6731p-30, 0x1.3b2ab6fba4e77p-23);
+    p = fma(f, p, 0x1.c6b08d704a0c0p-17);
+    p = fma(f, p, 0x1.ebfbdff82c58fp-11);
+    p = fma(f, p, 0x1.62e42fefa39efp-5);
+    p = fma(f, p, 1.0);
+    const double r = tab[n & 15] * p;
+    const int hi = __double2hiint(r) + ((n >> 4) << 20);
+    return __hiloint2double(hi, __double2loint(r));
+}
+
 // Squared distance rounded exactly like the reference's
 // (a-b).norm_square(): ((d0*d0) + d1*d1) + d2*d2, no contraction.
 template <int DIM>

@@ -645,6 +645,8 @@ sdot_status evaluate_internal(sdot_ctx *c, const double *p_dir, double comp_tol,
         if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
         if (e != cudaSuccess) return cuda_error(c, e, "threshold readback");
         if (mm[2] != 0.0) return set_error(c, SDOT_ENONFINITE, "non-finite potential");
+        c->scal_host[SC_MAXPSI] = mm[0];
+        c->scal_host[SC_MINPSI] = mm[1];
         r = host_threshold(c, mm[0], mm[1]);
     }
     c->current_distance_threshold = r;

@@ -132,6 +132,7 @@ struct sdot_ctx {
     double origin[3] = {0, 0, 0};      // centring point of the dense value sweep
     double diam = 0;                   // diameter bound of cells U targets
     double coord_scale = 1.0;          // max |coordinate|, for FP32 cull margins
+    double delta_max = 0.0;            // max distance of a quadrature point to its cell centre
 
     // ---- truncated path: block-pair lists and gradient partials ----
     sdot::DevBuf<int64_t> fwd_cnt, fwd_off, inv_cnt, inv_off, fwd2inv;

@@ -51,7 +51,7 @@ namespace sdot {
 constexpr int FT_WARPS = 8;
 constexpr int FT_MAXS = 1024;               // staged targets per chunk
 constexpr int FT_TS = 6;                    // doubles per staged target: y(3), nu, log2 nu, s*psi
-constexpr int FT_MAXT = FT_MAXS / TBLK_KD;  // target blocks per chunk
+constexpr int FT_MAXT = 96;                 // target blocks per chunk
 constexpr int FT_MAXQ = 80;                 // quadrature points of one source block
 constexpr int SUPER = 32;                   // blocks per super-block of the pair-list hierarchy
 
@@ -68,6 +68,7 @@ struct FusedArgs {
     double *Lq;                  // per q (written by the value sweep)
     double *valpart;             // per source block: value, C, skipped, pairs
     int do_a, do_b;
+    int w_nonneg;                // all w_q >= 0: log2 w_q folded into the FP32 exponent
     int tlo, thi;                // gradient partials only for target blocks [tlo, thi)
     int64_t part_base;           // inverse position of the first pair of tlo
     double cullt;                // per-target cull radius addend (r, enlarged)
@@ -75,10 +76,11 @@ struct FusedArgs {
 
 struct FTSmem {
     double tab[16];
-    double stg[FT_MAXS * FT_TS];
+    double stg[FT_TS][FT_MAXS];    // staged targets, structure of arrays (conflict-free lane access)
     double qd[FT_MAXQ][4];        // delta_q (FP64) and C'_q
+    double qn[FT_MAXQ];           // |delta_q|
     double qL[FT_MAXQ];           // L_q of the block
-    float qb[FT_MAXQ][4];         // pass B: delta (3) as float, D_q
+    __align__(16) float qb[FT_MAXQ][4];  // pass B: delta (3) as float, D_q (+ log2 w_q)
     float qw[FT_MAXQ];            // pass B: w_q
     double cellc[FT_WARPS][3];    // centre of each cell of the block
     double cellC[FT_WARPS];       // -kappa L_Kref for each cell (pass B), -inf if the cell is skipped
@@ -88,7 +90,9 @@ struct FTSmem {
     short smap[FT_MAXT][TBLK_KD]; // (chunk target block, slot) -> staged position or -1
     int ctb[FT_MAXT];             // target blocks of the chunk
     int64_t cpos[FT_MAXT];        // their partial base index
-    int ecnt[FT_MAXT];            // survivors per examined forward entry (-1: none)
+    int ecnt[32];                 // survivors per examined forward entry (-1: none)
+    int epre[32];                 // staged position of the first survivor of each accepted entry
+    int eacc, etot;
     int wcount[FT_WARPS];
     int nstg;
 };
@@ -321,18 +325,29 @@ __device__ int stage_chunk(FTSmem &sm, const FusedArgs &f, int64_t k0, int64_t k
             if (lane == 0) sm.ecnt[idx] = cntv;
         }
         __syncthreads();
-        // accept entries in list order while they fit (every thread computes the same prefix)
-        int nacc = 0, run = total;
-        int mypre[SUB] = {0, 0, 0, 0};
-        for (int i = 0; i < PER; ++i) {
-            const int c = sm.ecnt[i];
-            if (c < 0 || run + c > FT_MAXS) break;
+        // accept entries in list order while they fit: warp 0 scans the PER
+        // survivor counts (lane <-> entry), the prefix goes through smem
+        if (wp == 0) {
+            const int cv = sm.ecnt[lane];
+            int incl = cv < 0 ? 0 : cv;
 #pragma unroll
-            for (int s = 0; s < SUB; ++s)
-                if (i == s * FT_WARPS + wp) mypre[s] = run;
-            run += c;
-            ++nacc;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += v;
+            }
+            const int excl = incl - (cv < 0 ? 0 : cv);
+            const unsigned bad = __ballot_sync(0xffffffffu, cv < 0 || total + incl > FT_MAXS);
+            const int na = bad ? __ffs(bad) - 1 : 32;
+            sm.epre[lane] = total + excl;
+            const int accsum = __shfl_sync(0xffffffffu, incl, na > 0 ? na - 1 : 0);
+            if (lane == 0) {
+                sm.eacc = na;
+                sm.etot = total + (na > 0 ? accsum : 0);
+            }
         }
+        __syncthreads();
+        const int nacc = sm.eacc;
+        const int run = nacc > 0 ? sm.etot : total;
 #pragma unroll
         for (int s = 0; s < SUB; ++s) {
             const int idx = s * FT_WARPS + wp;
@@ -342,11 +357,10 @@ __device__ int stage_chunk(FTSmem &sm, const FusedArgs &f, int64_t k0, int64_t k
                 const bool keep = (bal[s] >> lane) & 1u;
                 short pos = -1;
                 if (keep) {
-                    pos = (short)(mypre[s] + __popc(bal[s] & ((1u << lane) - 1u)));
+                    pos = (short)(sm.epre[idx] + __popc(bal[s] & ((1u << lane) - 1u)));
                     const double *tp = f.tpk + (j0 + lane) * TPACK;
-                    double *dst = sm.stg + pos * FT_TS;
 #pragma unroll
-                    for (int d = 0; d < FT_TS; ++d) dst[d] = tp[d];
+                    for (int d = 0; d < FT_TS; ++d) sm.stg[d][pos] = tp[d];
                 }
                 sm.smap[slot][lane] = pos;
                 if (lane == 0) {
@@ -369,7 +383,82 @@ __device__ int stage_chunk(FTSmem &sm, const FusedArgs &f, int64_t k0, int64_t k
     return nb;
 }
 
-template <int DIM, int QL, bool FP32B>
+// Exact squared distance from a staged target (SoA) to a cell centre.
+template <int DIM>
+__device__ __forceinline__ double stg_dist2(const FTSmem &sm, int t, const double *c)
+{
+    const double y[3] = {sm.stg[0][t], sm.stg[1][t], DIM == 3 ? sm.stg[2][t] : 0.0};
+    return dist2_exact<DIM>(y, c);
+}
+
+// Value-sweep pair loop of one unit over its compacted candidates.
+// MODE 0: shift M = per-unit upper bound, exponents provably >= -16000 (no
+//         clamp); MODE 1: same with the clamp; MODE 2: per-pair lazy rescale
+//         (when the bound could sit more than 2^500 above the true maximum).
+// NQ: quadrature points handled (== QL for full units: straight-line code
+//     whose NQ exponential chains interleave).
+template <int DIM, int QL, int NQ, int MODE>
+__device__ __forceinline__ void value_pairs(const FTSmem &sm, int wp, int lane, int ncand, int qoff, double cc0,
+                                            double cc1, double cc2, const EvalArgs &a, double Munit, double *M,
+                                            double *S, double *mx)
+{
+    for (int p = lane; p < ncand; p += 32) {
+        const int ti = sm.cand[wp][p];
+        const double g0 = sm.stg[0][ti] - cc0, g1 = sm.stg[1][ti] - cc1;
+        const double g2 = DIM == 3 ? sm.stg[2][ti] - cc2 : 0.0;
+        const double d2 = DIM == 3 ? g0 * g0 + g1 * g1 + g2 * g2 : g0 * g0 + g1 * g1;
+        const double B0 = fma(-a.halfs, d2, sm.stg[5][ti]) - (MODE == 2 ? 0.0 : Munit);
+        const double G0 = a.s * g0, G1 = a.s * g1, G2 = a.s * g2;
+        const double nuj = sm.stg[3][ti];
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            const double *dq = sm.qd[qoff + q];
+            double bb = fma(G0, dq[0], B0);
+            bb = fma(G1, dq[1], bb);
+            if (DIM == 3) bb = fma(G2, dq[2], bb);
+            if (MODE == 2) {
+                lse_update(bb, nuj, M[q], S[q], mx[q], sm.tab);
+            } else {
+                mx[q] = fmax(mx[q], bb);
+                S[q] = fma(nuj, MODE == 0 ? exp2_16_nc(bb, sm.tab) : exp2_16(bb, sm.tab), S[q]);
+            }
+        }
+    }
+}
+
+// Units with fewer than QL quadrature points (the last q-group of a cell).
+template <int DIM, int QL, int MODE>
+__device__ __noinline__ void value_pairs_partial(const FTSmem &sm, int wp, int lane, int ncand, int qoff, int nql,
+                                                 double cc0, double cc1, double cc2, const EvalArgs &a, double Munit,
+                                                 double *M, double *S, double *mx)
+{
+    for (int p = lane; p < ncand; p += 32) {
+        const int ti = sm.cand[wp][p];
+        const double g0 = sm.stg[0][ti] - cc0, g1 = sm.stg[1][ti] - cc1;
+        const double g2 = DIM == 3 ? sm.stg[2][ti] - cc2 : 0.0;
+        const double d2 = DIM == 3 ? g0 * g0 + g1 * g1 + g2 * g2 : g0 * g0 + g1 * g1;
+        const double B0 = fma(-a.halfs, d2, sm.stg[5][ti]) - (MODE == 2 ? 0.0 : Munit);
+        const double G0 = a.s * g0, G1 = a.s * g1, G2 = a.s * g2;
+        const double nuj = sm.stg[3][ti];
+#pragma unroll
+        for (int q = 0; q < QL; ++q) {
+            if (q < nql) {
+                const double *dq = sm.qd[qoff + q];
+                double bb = fma(G0, dq[0], B0);
+                bb = fma(G1, dq[1], bb);
+                if (DIM == 3) bb = fma(G2, dq[2], bb);
+                if (MODE == 2) {
+                    lse_update(bb, nuj, M[q], S[q], mx[q], sm.tab);
+                } else {
+                    mx[q] = fmax(mx[q], bb);
+                    S[q] = fma(nuj, exp2_16(bb, sm.tab), S[q]);
+                }
+            }
+        }
+    }
+}
+
+template <int DIM, int QL, bool FP32B, int MODE>
 __global__ void __launch_bounds__(FT_WARPS * 32, 2)
 k_fused(FusedArgs f, EvalArgs a)
 {
@@ -408,6 +497,7 @@ k_fused(FusedArgs f, EvalArgs a)
             dsq += dl * dl;
         }
         sm.qd[i][3] = -a.halfs * dsq;
+        sm.qn[i] = sqrt(dsq);
     }
     __syncthreads();
     const double cc0 = sm.cellc[cl][0], cc1 = sm.cellc[cl][1], cc2 = sm.cellc[cl][2];
@@ -416,10 +506,21 @@ k_fused(FusedArgs f, EvalArgs a)
     int64_t single_end = -1;  // end of the only chunk, when everything fit in one
 
     if (f.do_a) {
-        double M[QL], S[QL], mx[QL];
+        // Shift of the online sums.  MODE 0/1: Munit = max_j B0_Kj + s r
+        // max_q |delta_q| bounds every exponent of the unit from above
+        // (|G_Kj| <= s r for a candidate), so no per-pair rescale is needed;
+        // exponents are kept relative to Munit (mx too) and a chunk that raises
+        // the bound rescales S once.  MODE 2 keeps a per-q lazy shift M[q].
+        double M[MODE == 2 ? QL : 1], S[QL], mx[QL];
 #pragma unroll
-        for (int k = 0; k < QL; ++k) { M[k] = -CUDART_INF; S[k] = 0.0; mx[k] = -CUDART_INF; }
+        for (int k = 0; k < QL; ++k) { S[k] = 0.0; mx[k] = -CUDART_INF; }
+#pragma unroll
+        for (int k = 0; k < (MODE == 2 ? QL : 1); ++k) M[k] = -CUDART_INF;
+        double Munit = -CUDART_INF;
+        double dqmax = 0.0;
+        for (int q = 0; q < nql; ++q) dqmax = fmax(dqmax, sm.qn[qoff + q]);
         double npairs = 0.0;
+        const double sr = a.s * a.cull;
         for (int64_t k = k0; k < k1;) {
             const int nt = stage_chunk<DIM>(sm, f, k, k1, bc, rcull2, f.do_b != 0);
             const int nstg = sm.nstg;
@@ -427,61 +528,76 @@ k_fused(FusedArgs f, EvalArgs a)
             // exact candidate test for this unit's cell, in-order compaction + mask
             int ncand = 0;
             if (valid) {
+                double bmax = -CUDART_INF;
                 for (int b0 = 0; b0 < nstg; b0 += 32) {
                     const int t = b0 + lane;
                     bool in = false;
-                    if (t < nstg) in = dist2_exact<DIM>(sm.stg + t * FT_TS, sm.cellc[cl]) <= a.sstar;
+                    if (t < nstg) {
+                        const double d2 = stg_dist2<DIM>(sm, t, sm.cellc[cl]);
+                        in = d2 <= a.sstar;
+                        if (in) bmax = fmax(bmax, fma(-a.halfs, d2, sm.stg[5][t]));
+                    }
                     const unsigned bal = __ballot_sync(0xffffffffu, in);
                     if (in) sm.cand[wp][ncand + __popc(bal & ((1u << lane) - 1u))] = (unsigned short)t;
                     if (lane == 0) sm.mask[wp][b0 >> 5] = bal;
                     ncand += __popc(bal);
                 }
+                bmax = warp_max(bmax);
                 __syncwarp();
                 npairs += (double)ncand * nql;
-                for (int p = lane; p < ncand; p += 32) {
-                    const double *tp = sm.stg + sm.cand[wp][p] * FT_TS;
-                    const double g0 = tp[0] - cc0, g1 = tp[1] - cc1, g2 = DIM == 3 ? tp[2] - cc2 : 0.0;
-                    const double d2 = DIM == 3 ? g0 * g0 + g1 * g1 + g2 * g2 : g0 * g0 + g1 * g1;
-                    const double B0 = fma(-a.halfs, d2, tp[5]);
-                    const double G0 = a.s * g0, G1 = a.s * g1, G2 = a.s * g2;
-                    const double nuj = tp[3];
+                if (MODE != 2 && bmax > -CUDART_INF) {
+                    const double mnew = bmax + sr * dqmax;
+                    if (mnew > Munit) {
+                        if (Munit > -CUDART_INF) {
+                            const double sc = exp2_16(Munit - mnew, sm.tab);
 #pragma unroll
-                    for (int q = 0; q < QL; ++q) {
-                        if (q < nql) {
-                            const double *dq = sm.qd[qoff + q];
-                            double bb = fma(G0, dq[0], B0);
-                            bb = fma(G1, dq[1], bb);
-                            if (DIM == 3) bb = fma(G2, dq[2], bb);
-                            lse_update(bb, nuj, M[q], S[q], mx[q], sm.tab);
+                            for (int q = 0; q < QL; ++q) {
+                                S[q] *= sc;
+                                mx[q] += Munit - mnew;
+                            }
                         }
+                        Munit = mnew;
                     }
                 }
+                if (nql == QL)
+                    value_pairs<DIM, QL, QL, MODE>(sm, wp, lane, ncand, qoff, cc0, cc1, cc2, a, Munit, M, S, mx);
+                else
+                    value_pairs_partial<DIM, QL, MODE>(sm, wp, lane, ncand, qoff, nql, cc0, cc1, cc2, a, Munit, M, S,
+                                                       mx);
             }
             k += nt;
             if (k >= k1 && chunks == 1) single_end = k;
             __syncthreads();
         }
-        // merge lanes; epilogue per q on lane 0
-        double tv = 0.0, tcv = 0.0, tsk = 0.0;
+        // merge the lanes of each q (warp max / sum); lane q keeps q's totals
+        // and runs q's epilogue, so the QL epilogues proceed in parallel
+        double my_mx = -CUDART_INF, my_S = 0.0;
 #pragma unroll
         for (int q = 0; q < QL; ++q) {
             const double mxw = warp_max(mx[q]);
-            const double sl = (M[q] == -CUDART_INF || mxw == -CUDART_INF) ? 0.0 : S[q] * exp2_16(M[q] - mxw, sm.tab);
+            // shift of this lane's sum: Munit (exponents relative to it: 0) or the lazy M[q]
+            const double Ml = MODE == 2 ? M[MODE == 2 ? q : 0] : (Munit > -CUDART_INF ? 0.0 : -CUDART_INF);
+            const double sl = (Ml == -CUDART_INF || mxw == -CUDART_INF) ? 0.0 : S[q] * exp2_16(Ml - mxw, sm.tab);
             const double Sw = warp_sum(sl);
-            if (valid && q < nql && lane == 0) {
-                const int qi = qoff + q;
-                const int64_t qg = qblk0 + qi;
-                double v, cv, L;
-                int sk;
-                value_epilogue(a, mxw, Sw, sm.qd[qi][3], f.rho[qg], f.jxw[qg], v, cv, L, sk);
-                f.Lq[qg] = L;
-                sm.qL[qi] = L;
-                tv += v;
-                tcv += cv;
-                tsk += sk;
+            if (lane == q) {
+                my_mx = mxw;
+                my_S = Sw;
             }
         }
-        block_partials(tv, tcv, tsk, lane == 0 ? npairs : 0.0, f.valpart);
+        double tv = 0.0, tcv = 0.0, tsk = 0.0;
+        if (valid && lane < nql) {
+            const int qi = qoff + lane;
+            const int64_t qg = qblk0 + qi;
+            double v, cv, L;
+            int sk;
+            value_epilogue(a, MODE == 2 ? my_mx : my_mx + Munit, my_S, sm.qd[qi][3], f.rho[qg], f.jxw[qg], v, cv, L, sk);
+            f.Lq[qg] = L;
+            sm.qL[qi] = L;
+            tv = v;
+            tcv = cv;
+            tsk = sk;
+        }
+        block_partials(tv, tcv, tsk, lane == 0 ? npairs : 0.0, f.valpart);  // (valid warps only add)
     } else {
         for (int i = tid; i < nqb; i += blockDim.x) sm.qL[i] = f.Lq[qblk0 + i];
     }
@@ -504,8 +620,9 @@ k_fused(FusedArgs f, EvalArgs a)
         sm.qb[i][0] = (float)sm.qd[i][0];
         sm.qb[i][1] = (float)sm.qd[i][1];
         sm.qb[i][2] = (float)sm.qd[i][2];
-        sm.qb[i][3] = (float)D;
-        sm.qw[i] = (float)f.w[qblk0 + i];
+        const double wq = f.w[qblk0 + i];
+        sm.qb[i][3] = (float)(f.w_nonneg ? D + log2(wq) : D);  // w_q folded in: p = 2^e directly
+        sm.qw[i] = (float)wq;
     }
     __syncthreads();
     const float sf = (float)(a.s * (1.0 / 16.0));
@@ -526,7 +643,7 @@ k_fused(FusedArgs f, EvalArgs a)
                 for (int b0 = 0; b0 < sm.nstg; b0 += 32) {
                     const int t = b0 + lane;
                     bool in = false;
-                    if (t < sm.nstg) in = dist2_exact<DIM>(sm.stg + t * FT_TS, sm.cellc[cl]) <= a.sstar;
+                    if (t < sm.nstg) in = stg_dist2<DIM>(sm, t, sm.cellc[cl]) <= a.sstar;
                     const unsigned bal = __ballot_sync(0xffffffffu, in);
                     if (lane == 0) sm.mask[wp][b0 >> 5] = bal;
                 }
@@ -535,7 +652,8 @@ k_fused(FusedArgs f, EvalArgs a)
         }
         const int nstg = sm.nstg;
         for (int t = tid; t < nstg; t += blockDim.x) {
-            const double *tp = sm.stg + t * FT_TS;
+            const double tp[FT_TS] = {sm.stg[0][t], sm.stg[1][t], sm.stg[2][t], sm.stg[3][t], sm.stg[4][t],
+                                      sm.stg[5][t]};
             double acc64 = 0.0;
             for (int c = 0; c < ncell; ++c) {
                 const int mw = c * a.ngroups;
@@ -550,15 +668,39 @@ k_fused(FusedArgs f, EvalArgs a)
                     const double E0 = tp[4] + (fma(-a.halfs, d2, tp[5]) - KAPPA * Lref) * (1.0 / 16.0);
                     const float e0 = (float)E0;
                     const float G0 = sf * (float)g0, G1 = sf * (float)g1, G2 = sf * (float)g2;
-                    float acc = 0.f;
-                    for (int q = 0; q < a.qpc; ++q) {
-                        const float *qb = sm.qb[qa + q];
-                        float e = fmaf(G0, qb[0], e0 + qb[3]);
-                        e = fmaf(G1, qb[1], e);
-                        if (DIM == 3) e = fmaf(G2, qb[2], e);
-                        acc = fmaf(sm.qw[qa + q], ex2_approx(e), acc);
+                    float acc0 = 0.f, acc1 = 0.f;
+                    if (f.w_nonneg) {
+                        int q = 0;
+                        for (; q + 1 < a.qpc; q += 2) {
+                            const float4 v0 = *reinterpret_cast<const float4 *>(sm.qb[qa + q]);
+                            const float4 v1 = *reinterpret_cast<const float4 *>(sm.qb[qa + q + 1]);
+                            float e0v = fmaf(G0, v0.x, e0 + v0.w), e1v = fmaf(G0, v1.x, e0 + v1.w);
+                            e0v = fmaf(G1, v0.y, e0v);
+                            e1v = fmaf(G1, v1.y, e1v);
+                            if (DIM == 3) {
+                                e0v = fmaf(G2, v0.z, e0v);
+                                e1v = fmaf(G2, v1.z, e1v);
+                            }
+                            acc0 += ex2_approx(e0v);
+                            acc1 += ex2_approx(e1v);
+                        }
+                        if (q < a.qpc) {
+                            const float4 v0 = *reinterpret_cast<const float4 *>(sm.qb[qa + q]);
+                            float ev = fmaf(G0, v0.x, e0 + v0.w);
+                            ev = fmaf(G1, v0.y, ev);
+                            if (DIM == 3) ev = fmaf(G2, v0.z, ev);
+                            acc0 += ex2_approx(ev);
+                        }
+                    } else {
+                        for (int q = 0; q < a.qpc; ++q) {
+                            const float *qb = sm.qb[qa + q];
+                            float e = fmaf(G0, qb[0], e0 + qb[3]);
+                            e = fmaf(G1, qb[1], e);
+                            if (DIM == 3) e = fmaf(G2, qb[2], e);
+                            acc0 = fmaf(sm.qw[qa + q], ex2_approx(e), acc0);
+                        }
                     }
-                    acc64 += (double)acc;
+                    acc64 += (double)(acc0 + acc1);
                 } else {
                     const double U0 = 16.0 * tp[4] + fma(-a.halfs, d2, tp[5]) - KAPPA * Lref;
                     const double G0 = a.s * g0, G1 = a.s * g1, G2 = a.s * g2;
@@ -590,51 +732,70 @@ k_fused(FusedArgs f, EvalArgs a)
 }
 
 // gradient of target block t = sum of its pair partials in inverse order
-// (ascending source block), lane <-> target; contiguous rows of 32 doubles.
+// (ascending source block), lane <-> target.  CTA <-> target block: warp w
+// sums rows w, w+8, ...; the 8 warp sums are added in warp order.
 __global__ void __launch_bounds__(256)
 k_grad_reduce(const int64_t *__restrict__ tblk_off, const int64_t *__restrict__ inv_off, int tlo, int thi,
               int64_t part_base, const double *__restrict__ part, double *__restrict__ gacc)
 {
-    const int t = tlo + (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
-    const int lane = threadIdx.x & 31;
-    if (t >= thi) return;
+    __shared__ double ws[8][32];
+    const int t = tlo + blockIdx.x;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int64_t p0 = inv_off[t], p1 = inv_off[t + 1];
-    double a0 = 0.0, a1 = 0.0;
-    int64_t p = p0;
-    for (; p + 1 < p1; p += 2) {  // two independent chains, combined in a fixed order
-        a0 += part[(p - part_base) * TBLK_KD + lane];
-        a1 += part[(p + 1 - part_base) * TBLK_KD + lane];
+    double acc = 0.0;
+    for (int64_t p = p0 + w; p < p1; p += 8) acc += part[(p - part_base) * TBLK_KD + lane];
+    ws[w][lane] = acc;
+    __syncthreads();
+    if (w == 0) {
+        double s = 0.0;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) s += ws[i][lane];
+        const int64_t j = tblk_off[t] + lane;
+        if (j < tblk_off[t + 1]) gacc[j] = s;
     }
-    if (p < p1) a0 += part[(p - part_base) * TBLK_KD + lane];
-    const int64_t j = tblk_off[t] + lane;
-    if (j < tblk_off[t + 1]) gacc[j] = a0 + a1;
 }
 
-// ---------------------------------------------------------------------------
-// host orchestration
-// ---------------------------------------------------------------------------
-
-template <int DIM, int QL, bool FP32B>
+template <int DIM, int QL, bool FP32B, int MODE>
 static void launch_fused(sdot_ctx *c, const FusedArgs &f, const EvalArgs &a, size_t smem, int nb)
 {
-    cudaFuncSetAttribute(k_fused<DIM, QL, FP32B>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_fused<DIM, QL, FP32B><<<(unsigned)nb, FT_WARPS * 32, smem, c->stream>>>(f, a);
+    cudaFuncSetAttribute(k_fused<DIM, QL, FP32B, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_fused<DIM, QL, FP32B, MODE><<<(unsigned)nb, FT_WARPS * 32, smem, c->stream>>>(f, a);
 }
 
-template <int DIM>
-static void dispatch_fused(sdot_ctx *c, const FusedArgs &f, const EvalArgs &a, bool fp32b, int nb)
+template <int DIM, int QL, int MODE>
+static void dispatch_fused_b(sdot_ctx *c, const FusedArgs &f, const EvalArgs &a, bool fp32b, int nb)
 {
     const size_t smem = sizeof(FTSmem);
-    if (a.ql <= 4) {
-        if (fp32b) launch_fused<DIM, 4, true>(c, f, a, smem, nb);
-        else launch_fused<DIM, 4, false>(c, f, a, smem, nb);
-    } else if (a.ql <= 8) {
-        if (fp32b) launch_fused<DIM, 8, true>(c, f, a, smem, nb);
-        else launch_fused<DIM, 8, false>(c, f, a, smem, nb);
+    if (fp32b) launch_fused<DIM, QL, true, MODE>(c, f, a, smem, nb);
+    else launch_fused<DIM, QL, false, MODE>(c, f, a, smem, nb);
+}
+
+template <int DIM, int MODE>
+static void dispatch_fused_q(sdot_ctx *c, const FusedArgs &f, const EvalArgs &a, bool fp32b, int nb)
+{
+    // 2D: units of 4 (order 2) or 9 (order 3 and groups of 9); 3D: 8 or 9.
+    if constexpr (DIM == 2) {
+        if (a.ql <= 4) dispatch_fused_b<DIM, 4, MODE>(c, f, a, fp32b, nb);
+        else dispatch_fused_b<DIM, 9, MODE>(c, f, a, fp32b, nb);
     } else {
-        if (fp32b) launch_fused<DIM, 9, true>(c, f, a, smem, nb);
-        else launch_fused<DIM, 9, false>(c, f, a, smem, nb);
+        if (a.ql <= 8) dispatch_fused_b<DIM, 8, MODE>(c, f, a, fp32b, nb);
+        else dispatch_fused_b<DIM, 9, MODE>(c, f, a, fp32b, nb);
     }
+}
+
+// MODE selection.  The shift Munit may exceed the true maximum exponent of a
+// q by up to 2 s r |delta|max (units of 2^(1/16)); beyond 2^500 the lazy form
+// is used.  Exponents u relative to Munit satisfy
+// u >= -s (psi_max - psi_min + r^2/2 + 2 r |delta|max); when that is above
+// -16000 the clamp of exp2 is provably inactive and dropped.
+template <int DIM>
+static void dispatch_fused(sdot_ctx *c, const FusedArgs &f, const EvalArgs &a, bool fp32b, int nb, double psi_range)
+{
+    const double gap = 2.0 * a.s * a.cull * c->delta_max;
+    const double umin = -a.s * (psi_range + 0.5 * a.cull * a.cull + 2.0 * a.cull * c->delta_max);
+    if (gap >= 16.0 * 500.0) dispatch_fused_q<DIM, 2>(c, f, a, fp32b, nb);
+    else if (umin > -15000.0) dispatch_fused_q<DIM, 0>(c, f, a, fp32b, nb);
+    else dispatch_fused_q<DIM, 1>(c, f, a, fp32b, nb);
 }
 
 sdot_status run_trunc(sdot_ctx *c, const EvalArgs &a, double r)
@@ -722,6 +883,7 @@ sdot_status run_trunc(sdot_ctx *c, const EvalArgs &a, double r)
     f.fwd_off = c->fwd_off.p; f.fwd_t = c->fwd_t.p; f.fwd2inv = c->fwd2inv.p;
     f.part = c->part.p; f.Lq = c->Lq.p; f.valpart = c->blkpart.p;
     f.cullt = std::isnan(r) ? 0.0 : std::min(r, 1e300);
+    f.w_nonneg = c->w_nonneg ? 1 : 0;
     const bool fp32b = c->precision != SDOT_PREC_FP64;
     for (size_t gi = 0; gi < groups.size(); ++gi) {
         f.do_a = gi == 0;
@@ -729,11 +891,12 @@ sdot_status run_trunc(sdot_ctx *c, const EvalArgs &a, double r)
         f.tlo = groups[gi].first;
         f.thi = groups[gi].second;
         f.part_base = groups.size() == 1 ? 0 : inv_host[f.tlo];
-        if (c->dim == 2) dispatch_fused<2>(c, f, a, fp32b, nsb);
-        else dispatch_fused<3>(c, f, a, fp32b, nsb);
+        const double prange = c->scal_host[SC_MAXPSI] - c->scal_host[SC_MINPSI];
+        if (c->dim == 2) dispatch_fused<2>(c, f, a, fp32b, nsb, std::isfinite(prange) ? prange : 1e300);
+        else dispatch_fused<3>(c, f, a, fp32b, nsb, std::isfinite(prange) ? prange : 1e300);
         if (c->profiling && gi + 1 == groups.size()) cudaEventRecord(c->pev[2], st);
         const int nw = f.thi - f.tlo;
-        k_grad_reduce<<<(unsigned)(((int64_t)nw * 32 + 255) / 256), 256, 0, st>>>(c->tblk_off.p, c->inv_off.p, f.tlo,
+        k_grad_reduce<<<(unsigned)nw, 256, 0, st>>>(c->tblk_off.p, c->inv_off.p, f.tlo,
                                                                                  f.thi, f.part_base, c->part.p,
                                                                                  c->gpart.p);
         c->klaunch[2] += 1;
