@@ -83,9 +83,7 @@ struct FTSmem {
     __align__(16) float qb[FT_MAXQ][4];  // pass B: delta (3) as float, D_q (+ log2 w_q)
     float qw[FT_MAXQ];            // pass B: w_q
     double cellc[FT_WARPS][3];    // centre of each cell of the block
-    double cellC[FT_WARPS];       // -kappa L_Kref for each cell (pass B), -inf if the cell is skipped
-    double pv[FT_MAXS];           // pass B partial per staged target
-    unsigned mask[FT_WARPS][FT_MAXS / 32];
+    float pvw[FT_WARPS][FT_MAXS]; // gradient partial of each unit (warp) per staged target (FP32 mode)
     unsigned short cand[FT_WARPS][FT_MAXS];
     short smap[FT_MAXT][TBLK_KD]; // (chunk target block, slot) -> staged position or -1
     int ctb[FT_MAXT];             // target blocks of the chunk
@@ -96,6 +94,21 @@ struct FTSmem {
     int wcount[FT_WARPS];
     int nstg;
 };
+
+// Partial rows of the gradient sweep: FP32 in the hybrid mode (inside
+// FTSmem), FP64 in the FP64 mode (appended after FTSmem in dynamic shared
+// memory, so that the FP64 gradient keeps its precision through the sum of
+// the warps' rows).
+template <bool FP32B> struct PRow { using T = double; };
+template <> struct PRow<true> { using T = float; };
+constexpr size_t FT_ROWS64_BYTES = sizeof(double) * FT_WARPS * FT_MAXS;
+
+template <bool FP32B>
+__device__ __forceinline__ typename PRow<FP32B>::T *partial_rows(FTSmem &sm)
+{
+    if constexpr (FP32B) return &sm.pvw[0][0];
+    else return reinterpret_cast<double *>(reinterpret_cast<unsigned char *>(&sm) + sizeof(FTSmem));
+}
 
 // ---------------------------------------------------------------------------
 // block-pair lists
@@ -458,6 +471,121 @@ __device__ __noinline__ void value_pairs_partial(const FTSmem &sm, int wp, int l
     }
 }
 
+// Exact candidate test of the staged targets for the warp's cell, in-order
+// compaction into sm.cand[wp]; returns the count and (through bmax) the
+// largest B0_Kj = kappa (psi_j - d2/2)/eps over the candidates.
+template <int DIM>
+__device__ __forceinline__ int compact_candidates(FTSmem &sm, int wp, int lane, int nstg, const double *cc,
+                                                  const EvalArgs &a, double &bmax)
+{
+    int ncand = 0;
+    bmax = -CUDART_INF;
+    for (int b0 = 0; b0 < nstg; b0 += 32) {
+        const int t = b0 + lane;
+        bool in = false;
+        if (t < nstg) {
+            const double d2 = stg_dist2<DIM>(sm, t, cc);
+            in = d2 <= a.sstar;
+            if (in) bmax = fmax(bmax, fma(-a.halfs, d2, sm.stg[5][t]));
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, in);
+        if (in) sm.cand[wp][ncand + __popc(bal & ((1u << lane) - 1u))] = (unsigned short)t;
+        ncand += __popc(bal);
+    }
+    bmax = warp_max(bmax);
+    __syncwarp();
+    return ncand;
+}
+
+// Gradient sweep of one unit over its compacted candidates: for each
+// candidate target j (lane-strided) the unit's part of sum_q w_q nu_j
+// e^{t_qj - L_q}, written to the warp's partial row (FP32).  E0 and G' are
+// formed in FP64 per (cell, target) so that every FP32 operand is small.
+template <int DIM, bool FP32B>
+__device__ __forceinline__ void grad_pairs(FTSmem &sm, const FusedArgs &f, int wp, int lane, int ncand, int qoff,
+                                           int nql, const double *cc, double Lref, int64_t qblk0, const EvalArgs &a)
+{
+    const float sf = (float)(a.s * (1.0 / 16.0));
+    for (int p = lane; p < ncand; p += 32) {
+        const int ti = sm.cand[wp][p];
+        const double g0 = sm.stg[0][ti] - cc[0], g1 = sm.stg[1][ti] - cc[1];
+        const double g2 = DIM == 3 ? sm.stg[2][ti] - cc[2] : 0.0;
+        const double d2 = DIM == 3 ? g0 * g0 + g1 * g1 + g2 * g2 : g0 * g0 + g1 * g1;
+        double val;
+        if (FP32B) {
+            const float e0 = (float)(sm.stg[4][ti] + (fma(-a.halfs, d2, sm.stg[5][ti]) - KAPPA * Lref) * (1.0 / 16.0));
+            const float G0 = sf * (float)g0, G1 = sf * (float)g1, G2 = sf * (float)g2;
+            float acc0 = 0.f, acc1 = 0.f;
+            if (f.w_nonneg) {
+                int q = 0;
+                for (; q + 1 < nql; q += 2) {
+                    const float4 v0 = *reinterpret_cast<const float4 *>(sm.qb[qoff + q]);
+                    const float4 v1 = *reinterpret_cast<const float4 *>(sm.qb[qoff + q + 1]);
+                    float ea = fmaf(G0, v0.x, e0 + v0.w), eb = fmaf(G0, v1.x, e0 + v1.w);
+                    ea = fmaf(G1, v0.y, ea);
+                    eb = fmaf(G1, v1.y, eb);
+                    if (DIM == 3) {
+                        ea = fmaf(G2, v0.z, ea);
+                        eb = fmaf(G2, v1.z, eb);
+                    }
+                    acc0 += ex2_approx(ea);
+                    acc1 += ex2_approx(eb);
+                }
+                if (q < nql) {
+                    const float4 v0 = *reinterpret_cast<const float4 *>(sm.qb[qoff + q]);
+                    float ea = fmaf(G0, v0.x, e0 + v0.w);
+                    ea = fmaf(G1, v0.y, ea);
+                    if (DIM == 3) ea = fmaf(G2, v0.z, ea);
+                    acc0 += ex2_approx(ea);
+                }
+            } else {
+                for (int q = 0; q < nql; ++q) {
+                    const float *qb = sm.qb[qoff + q];
+                    float e = fmaf(G0, qb[0], e0 + qb[3]);
+                    e = fmaf(G1, qb[1], e);
+                    if (DIM == 3) e = fmaf(G2, qb[2], e);
+                    acc0 = fmaf(sm.qw[qoff + q], ex2_approx(e), acc0);
+                }
+            }
+            val = (double)(acc0 + acc1);
+        } else {
+            const double U0 = 16.0 * sm.stg[4][ti] + fma(-a.halfs, d2, sm.stg[5][ti]) - KAPPA * Lref;
+            const double G0 = a.s * g0, G1 = a.s * g1, G2 = a.s * g2;
+            double acc = 0.0;
+            for (int q = 0; q < nql; ++q) {
+                const double *dq = sm.qd[qoff + q];
+                const double L = sm.qL[qoff + q];
+                if (!isfinite(L)) continue;
+                double u = fma(G0, dq[0], U0 + dq[3] - KAPPA * (L - Lref));
+                u = fma(G1, dq[1], u);
+                if (DIM == 3) u = fma(G2, dq[2], u);
+                acc = fma(f.w[qblk0 + qoff + q], exp2_16(u, sm.tab), acc);
+            }
+            val = acc;
+        }
+        partial_rows<FP32B>(sm)[wp * FT_MAXS + ti] = (typename PRow<FP32B>::T)val;
+    }
+}
+
+// CTA sum of the warp partial rows (warp order) and the write of every slot
+// of every pair of the chunk (zeros where a target was not staged).
+template <bool FP32B>
+__device__ __forceinline__ void write_partials(FTSmem &sm, const FusedArgs &f, int nt, int nunit)
+{
+    const typename PRow<FP32B>::T *rows = partial_rows<FP32B>(sm);
+    const int tid = threadIdx.x;
+    for (int i = tid; i < nt * TBLK_KD; i += blockDim.x) {
+        const int ti = i / TBLK_KD, sl = i - ti * TBLK_KD;
+        const int64_t base = sm.cpos[ti];
+        if (base < 0) continue;
+        const short p = sm.smap[ti][sl];
+        double v = 0.0;
+        if (p >= 0)
+            for (int w = 0; w < nunit; ++w) v += (double)rows[w * FT_MAXS + p];
+        f.part[base + sl] = v;
+    }
+}
+
 template <int DIM, int QL, bool FP32B, int MODE>
 __global__ void __launch_bounds__(FT_WARPS * 32, 2)
 k_fused(FusedArgs f, EvalArgs a)
@@ -481,7 +609,6 @@ k_fused(FusedArgs f, EvalArgs a)
     const double bc[3] = {bs[0], bs[1], bs[2]};
     const double rc = (f.cullt + bs[3]) * (1.0 + 1e-12) + 1e-300;
     const double rcull2 = rc * rc;
-    // cell centres and per-q geometry of the block
     for (int i = tid; i < ncell * 3; i += blockDim.x) {
         const int c = i / 3, d = i - c * 3;
         sm.cellc[c][d] = d < DIM ? f.cell_ctr[(cb0 + c) * DIM + d] : 0.0;
@@ -500,11 +627,13 @@ k_fused(FusedArgs f, EvalArgs a)
         sm.qn[i] = sqrt(dsq);
     }
     __syncthreads();
-    const double cc0 = sm.cellc[cl][0], cc1 = sm.cellc[cl][1], cc2 = sm.cellc[cl][2];
+    const double cc[3] = {sm.cellc[cl][0], sm.cellc[cl][1], sm.cellc[cl][2]};
     const int64_t k0 = f.fwd_off[b], k1 = f.fwd_off[b + 1];
     int chunks = 0;
     int64_t single_end = -1;  // end of the only chunk, when everything fit in one
+    int ncand_single = 0;
 
+    // ---------------- value sweep ----------------
     if (f.do_a) {
         // Shift of the online sums.  MODE 0/1: Munit = max_j B0_Kj + s r
         // max_q |delta_q| bounds every exponent of the unit from above
@@ -525,25 +654,10 @@ k_fused(FusedArgs f, EvalArgs a)
             const int nt = stage_chunk<DIM>(sm, f, k, k1, bc, rcull2, f.do_b != 0);
             const int nstg = sm.nstg;
             ++chunks;
-            // exact candidate test for this unit's cell, in-order compaction + mask
-            int ncand = 0;
             if (valid) {
-                double bmax = -CUDART_INF;
-                for (int b0 = 0; b0 < nstg; b0 += 32) {
-                    const int t = b0 + lane;
-                    bool in = false;
-                    if (t < nstg) {
-                        const double d2 = stg_dist2<DIM>(sm, t, sm.cellc[cl]);
-                        in = d2 <= a.sstar;
-                        if (in) bmax = fmax(bmax, fma(-a.halfs, d2, sm.stg[5][t]));
-                    }
-                    const unsigned bal = __ballot_sync(0xffffffffu, in);
-                    if (in) sm.cand[wp][ncand + __popc(bal & ((1u << lane) - 1u))] = (unsigned short)t;
-                    if (lane == 0) sm.mask[wp][b0 >> 5] = bal;
-                    ncand += __popc(bal);
-                }
-                bmax = warp_max(bmax);
-                __syncwarp();
+                double bmax;
+                const int ncand = compact_candidates<DIM>(sm, wp, lane, nstg, cc, a, bmax);
+                ncand_single = ncand;
                 npairs += (double)ncand * nql;
                 if (MODE != 2 && bmax > -CUDART_INF) {
                     const double mnew = bmax + sr * dqmax;
@@ -560,14 +674,17 @@ k_fused(FusedArgs f, EvalArgs a)
                     }
                 }
                 if (nql == QL)
-                    value_pairs<DIM, QL, QL, MODE>(sm, wp, lane, ncand, qoff, cc0, cc1, cc2, a, Munit, M, S, mx);
+                    value_pairs<DIM, QL, QL, MODE>(sm, wp, lane, ncand, qoff, cc[0], cc[1], cc[2], a, Munit, M, S, mx);
                 else
-                    value_pairs_partial<DIM, QL, MODE>(sm, wp, lane, ncand, qoff, nql, cc0, cc1, cc2, a, Munit, M, S,
-                                                       mx);
+                    value_pairs_partial<DIM, QL, MODE>(sm, wp, lane, ncand, qoff, nql, cc[0], cc[1], cc[2], a, Munit,
+                                                       M, S, mx);
             }
             k += nt;
-            if (k >= k1 && chunks == 1) single_end = k;
-            __syncthreads();
+            if (k >= k1 && chunks == 1) {
+                single_end = k;
+            } else {
+                __syncthreads();  // the next chunk overwrites the staged targets
+            }
         }
         // merge the lanes of each q (warp max / sum); lane q keeps q's totals
         // and runs q's epilogue, so the QL epilogues proceed in parallel
@@ -590,142 +707,71 @@ k_fused(FusedArgs f, EvalArgs a)
             const int64_t qg = qblk0 + qi;
             double v, cv, L;
             int sk;
-            value_epilogue(a, MODE == 2 ? my_mx : my_mx + Munit, my_S, sm.qd[qi][3], f.rho[qg], f.jxw[qg], v, cv, L, sk);
+            value_epilogue(a, MODE == 2 ? my_mx : my_mx + Munit, my_S, sm.qd[qi][3], f.rho[qg], f.jxw[qg], v, cv, L,
+                           sk);
             f.Lq[qg] = L;
             sm.qL[qi] = L;
             tv = v;
             tcv = cv;
             tsk = sk;
         }
-        block_partials(tv, tcv, tsk, lane == 0 ? npairs : 0.0, f.valpart);  // (valid warps only add)
+        block_partials(tv, tcv, tsk, lane == 0 ? npairs : 0.0, f.valpart);  // contains __syncthreads
     } else {
         for (int i = tid; i < nqb; i += blockDim.x) sm.qL[i] = f.Lq[qblk0 + i];
+        __syncthreads();
     }
     if (!f.do_b) return;
-    __syncthreads();
-    // pass B per-q data: D_q relative to a per-cell reference L_Kref
-    if (tid < ncell) {
-        double Lref = CUDART_INF;
-        for (int i = 0; i < a.qpc; ++i) Lref = fmin(Lref, sm.qL[tid * a.qpc + i]);
-        sm.cellC[tid] = isfinite(Lref) ? Lref : CUDART_INF;
-    }
-    __syncthreads();
-    for (int i = tid; i < nqb; i += blockDim.x) {
-        const int c = i / a.qpc;
-        const double Lref = sm.cellC[c];
-        const double L = sm.qL[i];
-        double D;
-        if (!isfinite(Lref) || !isfinite(L)) D = -CUDART_INF;
-        else D = (sm.qd[i][3] - KAPPA * (L - Lref)) * (1.0 / 16.0);
-        sm.qb[i][0] = (float)sm.qd[i][0];
-        sm.qb[i][1] = (float)sm.qd[i][1];
-        sm.qb[i][2] = (float)sm.qd[i][2];
-        const double wq = f.w[qblk0 + i];
-        sm.qb[i][3] = (float)(f.w_nonneg ? D + log2(wq) : D);  // w_q folded in: p = 2^e directly
-        sm.qw[i] = (float)wq;
-    }
-    __syncthreads();
-    const float sf = (float)(a.s * (1.0 / 16.0));
-    for (int64_t k = k0; k < k1;) {
-        int nt;
-        if (single_end >= 0) {
-            nt = (int)(single_end - k0);   // staged data and masks of the single chunk are still in smem
-            if (tid < nt) {
-                const int tb = sm.ctb[tid];
-                const int64_t ip = f.fwd2inv[k0 + tid];
-                sm.cpos[tid] = (ip >= 0 && tb >= f.tlo && tb < f.thi) ? (ip - f.part_base) * TBLK_KD : (int64_t)-1;
-            }
-            __syncthreads();
-        } else {
-            nt = stage_chunk<DIM>(sm, f, k, k1, bc, rcull2, true);
-            // masks for this chunk (one warp per cell; units of group 0)
-            if (valid && grp == 0) {
-                for (int b0 = 0; b0 < sm.nstg; b0 += 32) {
-                    const int t = b0 + lane;
-                    bool in = false;
-                    if (t < sm.nstg) in = stg_dist2<DIM>(sm, t, sm.cellc[cl]) <= a.sstar;
-                    const unsigned bal = __ballot_sync(0xffffffffu, in);
-                    if (lane == 0) sm.mask[wp][b0 >> 5] = bal;
-                }
-            }
-            __syncthreads();
+
+    // ---------------- gradient sweep ----------------
+    // per-unit reference L_Kref = min L over the unit's q; per-q FP32 data
+    double Lref = CUDART_INF;
+    if (valid) {
+        double lv = lane < nql ? sm.qL[qoff + lane] : CUDART_INF;
+        Lref = -warp_max(-lv);
+        if (lane < nql) {
+            const int i = qoff + lane;
+            const double L = sm.qL[i];
+            const double D = (!isfinite(Lref) || !isfinite(L)) ? -CUDART_INF
+                                                                : (sm.qd[i][3] - KAPPA * (L - Lref)) * (1.0 / 16.0);
+            const double wq = f.w[qblk0 + i];
+            sm.qb[i][0] = (float)sm.qd[i][0];
+            sm.qb[i][1] = (float)sm.qd[i][1];
+            sm.qb[i][2] = (float)sm.qd[i][2];
+            sm.qb[i][3] = (float)(f.w_nonneg ? D + log2(wq) : D);  // w_q folded in: p = 2^e directly
+            sm.qw[i] = (float)wq;
         }
+        __syncwarp();
+    }
+    if (single_end >= 0) {
+        // the single chunk's staged targets and this warp's candidates are still in smem
+        const int nt = (int)(single_end - k0);
         const int nstg = sm.nstg;
-        for (int t = tid; t < nstg; t += blockDim.x) {
-            const double tp[FT_TS] = {sm.stg[0][t], sm.stg[1][t], sm.stg[2][t], sm.stg[3][t], sm.stg[4][t],
-                                      sm.stg[5][t]};
-            double acc64 = 0.0;
-            for (int c = 0; c < ncell; ++c) {
-                const int mw = c * a.ngroups;
-                if (!((sm.mask[mw][t >> 5] >> (t & 31)) & 1u)) continue;
-                const double Lref = sm.cellC[c];
-                if (!isfinite(Lref)) continue;
-                const double g0 = tp[0] - sm.cellc[c][0], g1 = tp[1] - sm.cellc[c][1];
-                const double g2 = DIM == 3 ? tp[2] - sm.cellc[c][2] : 0.0;
-                const double d2 = DIM == 3 ? g0 * g0 + g1 * g1 + g2 * g2 : g0 * g0 + g1 * g1;
-                const int qa = c * a.qpc;
-                if (FP32B) {
-                    const double E0 = tp[4] + (fma(-a.halfs, d2, tp[5]) - KAPPA * Lref) * (1.0 / 16.0);
-                    const float e0 = (float)E0;
-                    const float G0 = sf * (float)g0, G1 = sf * (float)g1, G2 = sf * (float)g2;
-                    float acc0 = 0.f, acc1 = 0.f;
-                    if (f.w_nonneg) {
-                        int q = 0;
-                        for (; q + 1 < a.qpc; q += 2) {
-                            const float4 v0 = *reinterpret_cast<const float4 *>(sm.qb[qa + q]);
-                            const float4 v1 = *reinterpret_cast<const float4 *>(sm.qb[qa + q + 1]);
-                            float e0v = fmaf(G0, v0.x, e0 + v0.w), e1v = fmaf(G0, v1.x, e0 + v1.w);
-                            e0v = fmaf(G1, v0.y, e0v);
-                            e1v = fmaf(G1, v1.y, e1v);
-                            if (DIM == 3) {
-                                e0v = fmaf(G2, v0.z, e0v);
-                                e1v = fmaf(G2, v1.z, e1v);
-                            }
-                            acc0 += ex2_approx(e0v);
-                            acc1 += ex2_approx(e1v);
-                        }
-                        if (q < a.qpc) {
-                            const float4 v0 = *reinterpret_cast<const float4 *>(sm.qb[qa + q]);
-                            float ev = fmaf(G0, v0.x, e0 + v0.w);
-                            ev = fmaf(G1, v0.y, ev);
-                            if (DIM == 3) ev = fmaf(G2, v0.z, ev);
-                            acc0 += ex2_approx(ev);
-                        }
-                    } else {
-                        for (int q = 0; q < a.qpc; ++q) {
-                            const float *qb = sm.qb[qa + q];
-                            float e = fmaf(G0, qb[0], e0 + qb[3]);
-                            e = fmaf(G1, qb[1], e);
-                            if (DIM == 3) e = fmaf(G2, qb[2], e);
-                            acc0 = fmaf(sm.qw[qa + q], ex2_approx(e), acc0);
-                        }
-                    }
-                    acc64 += (double)(acc0 + acc1);
-                } else {
-                    const double U0 = 16.0 * tp[4] + fma(-a.halfs, d2, tp[5]) - KAPPA * Lref;
-                    const double G0 = a.s * g0, G1 = a.s * g1, G2 = a.s * g2;
-                    for (int q = 0; q < a.qpc; ++q) {
-                        const double *dq = sm.qd[qa + q];
-                        const double L = sm.qL[qa + q];
-                        if (!isfinite(L)) continue;
-                        double u = fma(G0, dq[0], U0 + dq[3] - KAPPA * (L - Lref));
-                        u = fma(G1, dq[1], u);
-                        if (DIM == 3) u = fma(G2, dq[2], u);
-                        acc64 = fma(f.w[qblk0 + qa + q], exp2_16(u, sm.tab), acc64);
-                    }
-                }
-            }
-            sm.pv[t] = acc64;
+        if (valid) {
+            for (int t = lane; t < nstg; t += 32) partial_rows<FP32B>(sm)[wp * FT_MAXS + t] = 0;
+            __syncwarp();
+            if (isfinite(Lref)) grad_pairs<DIM, FP32B>(sm, f, wp, lane, ncand_single, qoff, nql, cc, Lref, qblk0, a);
+        }
+        if (tid < nt) {
+            const int tb = sm.ctb[tid];
+            const int64_t ip = f.fwd2inv[k0 + tid];
+            sm.cpos[tid] = (ip >= 0 && tb >= f.tlo && tb < f.thi) ? (ip - f.part_base) * TBLK_KD : (int64_t)-1;
         }
         __syncthreads();
-        // write every slot of every pair of the chunk (zeros where not staged)
-        for (int i = tid; i < nt * TBLK_KD; i += blockDim.x) {
-            const int ti = i / TBLK_KD, sl = i - ti * TBLK_KD;
-            const int64_t base = sm.cpos[ti];
-            if (base < 0) continue;
-            const short p = sm.smap[ti][sl];
-            f.part[base + sl] = p >= 0 ? sm.pv[p] : 0.0;
+        write_partials<FP32B>(sm, f, nt, nunit);
+        return;
+    }
+    for (int64_t k = k0; k < k1;) {
+        const int nt = stage_chunk<DIM>(sm, f, k, k1, bc, rcull2, true);
+        const int nstg = sm.nstg;
+        if (valid) {
+            double bmax;
+            const int ncand = compact_candidates<DIM>(sm, wp, lane, nstg, cc, a, bmax);
+            for (int t = lane; t < nstg; t += 32) partial_rows<FP32B>(sm)[wp * FT_MAXS + t] = 0;
+            __syncwarp();
+            if (isfinite(Lref)) grad_pairs<DIM, FP32B>(sm, f, wp, lane, ncand, qoff, nql, cc, Lref, qblk0, a);
         }
+        __syncthreads();
+        write_partials<FP32B>(sm, f, nt, nunit);
         k += nt;
         __syncthreads();
     }
@@ -765,9 +811,8 @@ static void launch_fused(sdot_ctx *c, const FusedArgs &f, const EvalArgs &a, siz
 template <int DIM, int QL, int MODE>
 static void dispatch_fused_b(sdot_ctx *c, const FusedArgs &f, const EvalArgs &a, bool fp32b, int nb)
 {
-    const size_t smem = sizeof(FTSmem);
-    if (fp32b) launch_fused<DIM, QL, true, MODE>(c, f, a, smem, nb);
-    else launch_fused<DIM, QL, false, MODE>(c, f, a, smem, nb);
+    if (fp32b) launch_fused<DIM, QL, true, MODE>(c, f, a, sizeof(FTSmem), nb);
+    else launch_fused<DIM, QL, false, MODE>(c, f, a, sizeof(FTSmem) + FT_ROWS64_BYTES, nb);
 }
 
 template <int DIM, int MODE>
