@@ -40,7 +40,9 @@ typedef enum {
  *   SDOT_PREC_FP64  : both sweeps in FP64 (value 1e-10 rel., gradient ~1e-14).
  *   SDOT_PREC_HYBRID: value sweep FP64, gradient sweep FP32 exp2 with FP64
  *                     accumulation (gradient error <= ~3e-6 * max nu_j).
- *   SDOT_PREC_MIXED : both sweeps FP32 exp2, FP64 accumulation.            */
+ *   SDOT_PREC_MIXED : accepted and currently run as SDOT_PREC_HYBRID (an FP32
+ *                     value sweep cannot meet the 1e-10 relative value bound,
+ *                     so the value sweep stays FP64).                       */
 typedef enum { SDOT_PREC_FP64 = 0, SDOT_PREC_HYBRID = 1, SDOT_PREC_MIXED = 2 } sdot_precision;
 
 typedef enum { SDOT_THRESH_POINTWISE = 0, SDOT_THRESH_INTEGRAL = 1, SDOT_THRESH_GEOMETRIC = 2 } sdot_threshold_type;

@@ -26,13 +26,14 @@
 //        B0_Kj = kappa (psi_j - d2/2)/eps, G_Kj = kappa (y_j - c_K)/eps,
 //        delta_q = x_q - c_K, C'_q = -kappa |delta_q|^2 / (2 eps)
 //        (kappa = 16/ln 2; the same expansion as |x_q - y_j|^2 about c_K);
-//      gradient sweep: thread <-> staged target, loop over the block's cells
-//        whose candidate set contains it, sum over q of
+//      gradient sweep: each warp over the same compacted candidates, lane <->
+//        candidate, sum over the unit's q of
 //        w_q nu_j 2^(E0_Kj + G'_Kj.delta_q + D_q) in FP32 ex2 (or FP64 exp2),
 //        E0 and G' formed in FP64 per (cell, target) so every FP32 operand is
-//        small; FP64 accumulation across cells.  The block's partial for each
-//        target of each pair is written to a slot of the pair in the inverse
-//        list order.
+//        small, into the warp's partial row (FP32 rows in the hybrid mode,
+//        FP64 rows in the FP64 mode); the rows are added in warp order in
+//        FP64.  The block's partial for each target of each pair is written
+//        to a slot of the pair in the inverse list order.
 //   3. k_grad_reduce (warp <-> target block): sum of the partials over the
 //      pairs in ascending source-block order, lane <-> target.  No atomics;
 //      the summation order is fixed, results are bitwise reproducible.
