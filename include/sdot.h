@@ -202,6 +202,34 @@ sdot_status sdot_get_kernel_times(sdot_ctx *ctx, double *ms, int64_t *launches, 
  * Gop/s, out[3] SM clock (MHz) reported by the device. */
 sdot_status sdot_measure_peaks(int device, double *out);
 
+/* ---- no-allocation evaluation (no counterpart in the reference) ----
+ * Same results as sdot_evaluate_device (same kernels, same launch shapes) for
+ * an untruncated problem (pointwise threshold with tau <= 0), but the call
+ * allocates no device memory: its scratch is one file-scope static device
+ * array of SDOT_NOALLOC_SCRATCH_BYTES (8 MiB) per device, not the context's
+ * evaluation buffers.  For callers that must not allocate while they run:
+ * a loop whose device memory is already fully committed to a pool or an
+ * admission budget, where a cudaMalloc could fail mid-request, or a
+ * latency-bound loop that cannot absorb cudaMalloc / cudaFree and the
+ * synchronisation they imply.  The set-up calls (sdot_create,
+ * sdot_set_source, sdot_set_target) still allocate, as before.
+ *   - Requests whose scratch exceeds the limit (about 8 * n_q + (10 + slices)
+ *     * 8 * n_targets bytes, slices <= 64) are rejected with SDOT_EINVAL and
+ *     a message giving the need and the limit; truncated problems likewise.
+ *   - Nothing in the scratch has to start at zero: every word a call reads is
+ *     written earlier by the same call on the context's stream.
+ *   - The scratch is shared by all contexts of the process on a device: calls
+ *     whose executions overlap (other threads, streams or contexts on the same
+ *     device) race and corrupt each other's results.  Serialise them.
+ *   - The first call on a device does one-time set-up (it looks up the
+ *     scratch address with cudaGetSymbolAddress, which may load the module);
+ *     make it before any stream capture.
+ * psi_dev, grad_dev: device arrays of n_targets doubles in caller order;
+ * *value receives J.  Updates the same state as sdot_evaluate_device. */
+#define SDOT_NOALLOC_SCRATCH_BYTES (8u << 20)
+sdot_status sdot_evaluate_device_noalloc(sdot_ctx *ctx, const double *psi_dev, double *grad_dev,
+                                         double *value);
+
 #ifdef __cplusplus
 }
 #endif

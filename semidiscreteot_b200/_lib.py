@@ -31,7 +31,10 @@ EXPORTED = [
     "sdot_get_C_global", "sdot_set_distance_threshold", "sdot_compute_covering_radius",
     "sdot_compute_geometric_radius_bound", "sdot_set_distance_function", "sdot_evaluate_partial_device",
     "sdot_set_state", "sdot_get_stream", "sdot_set_profiling", "sdot_get_kernel_times", "sdot_measure_peaks",
+    "sdot_evaluate_device_noalloc",
 ]
+
+NOALLOC_SCRATCH_BYTES = 8 << 20  # SDOT_NOALLOC_SCRATCH_BYTES
 
 
 class Options(C.Structure):
@@ -104,6 +107,8 @@ def load():
     lib.sdot_set_profiling.argtypes = [vp, ip]
     lib.sdot_get_kernel_times.argtypes = [vp, vp, vp, ip, ip]
     lib.sdot_measure_peaks.argtypes = [ip, vp]
+    lib.sdot_evaluate_device_noalloc.argtypes = [vp, vp, vp, C.POINTER(d)]
+    lib.sdot_evaluate_device_noalloc.restype = ip
     for fn in ("sdot_evaluate_partial_device", "sdot_set_state", "sdot_set_profiling", "sdot_get_kernel_times",
                "sdot_measure_peaks"):
         getattr(lib, fn).restype = ip

@@ -24,6 +24,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
+#include <string>
 
 #include "sdot_device.cuh"
 #include "sdot_internal.h"
@@ -717,3 +719,171 @@ sdot_status evaluate_internal(sdot_ctx *c, const double *p_dir, double comp_tol,
 }
 
 }  // namespace sdot
+
+// ---------------------------------------------------------------------------
+// No-allocation dense evaluation (sdot_evaluate_device_noalloc).
+//
+// The scratch of one untruncated evaluation (gathered psi, gradient, packed
+// targets, L_q, gradient partials per q-slice, value / reduction partials,
+// scalars) lives in one file-scope device array of NOALLOC_BYTES instead of
+// the context's lazily allocated evaluation buffers.  Its device address is
+// looked up once per device with cudaGetSymbolAddress and cached.  Every
+// scratch word the evaluation reads is written earlier by the same
+// evaluation on the same stream: nothing has to start at zero, and nothing
+// carries over between calls.  The array is shared by every context of the
+// process on a device, so calls whose executions overlap corrupt each other.
+// ---------------------------------------------------------------------------
+
+namespace sdot {
+
+constexpr size_t NOALLOC_BYTES = size_t(8) << 20;  // == SDOT_NOALLOC_SCRATCH_BYTES
+constexpr int NOALLOC_MAX_DEVICES = 64;
+
+static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_BYTES / sizeof(double)];
+
+static double *g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
+static std::mutex g_noalloc_mu;
+
+// Scratch segments of an evaluation, each rounded up to 256 bytes.
+struct NoallocLayout {
+    int64_t psi, grad, tpack, Lq, gpart, blkpart, redpart, scal, total;  // offsets in doubles
+    int64_t nval;
+    int nks;
+};
+
+static NoallocLayout noalloc_layout(int64_t nq, int64_t nt)
+{
+    auto up = [](int64_t n) { return (n + 31) / 32 * 32; };
+    NoallocLayout L{};
+    const int64_t per = (int64_t)DENSE_A_THREADS * DENSE_A_QT;
+    L.nval = (nq + per - 1) / per;
+    // q-slices of the gradient sweep: the same rule as the dense branch of run_eval
+    const int64_t tb = (nt + DENSE_B_THREADS * DENSE_B_TT - 1) / (DENSE_B_THREADS * DENSE_B_TT);
+    const int64_t want = (148 * 8 + tb - 1) / tb;
+    const int64_t maxks = (nq + 255) / 256;
+    L.nks = (int)std::max<int64_t>(1, std::min<int64_t>(want, maxks));
+    if (L.nks > 64) L.nks = 64;
+    int64_t o = 0;
+    L.psi = o;     o += up(nt);
+    L.grad = o;    o += up(nt);
+    L.tpack = o;   o += up(nt * TPACK);
+    L.Lq = o;      o += up(nq);
+    L.gpart = o;   o += up((int64_t)L.nks * nt);
+    L.blkpart = o; o += up(4 * L.nval);
+    L.redpart = o; o += up((int64_t)FIN_BLOCKS * NRED);
+    L.scal = o;    o += up(SC_COUNT);
+    L.total = o;
+    return L;
+}
+
+static sdot_status noalloc_scratch(sdot_ctx *c, double **out)
+{
+    if (c->device < 0 || c->device >= NOALLOC_MAX_DEVICES)
+        return set_error(c, SDOT_EINVAL, "no-alloc evaluation: device ordinal out of range");
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[c->device]) {
+        double *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress((void **)&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_error(c, e, "no-alloc evaluation: cudaGetSymbolAddress of the scratch array");
+        g_noalloc_ptr[c->device] = p;
+    }
+    *out = g_noalloc_ptr[c->device];
+    return SDOT_OK;
+}
+
+template <int DIM>
+static void noalloc_launch(sdot_ctx *c, const EvalArgs &a, double *S, const NoallocLayout &L)
+{
+    cudaStream_t st = c->stream;
+    double *psi = S + L.psi, *grad = S + L.grad, *tpack = S + L.tpack, *Lq = S + L.Lq, *gpart = S + L.gpart;
+    double *blkpart = S + L.blkpart, *redpart = S + L.redpart, *scal = S + L.scal;
+    k_target_prep<DIM><<<grid_for(a.nt, 256), 256, 0, st>>>(a.nt, c->y.p, c->nu.p, psi, a, tpack);
+    k_value_dense<DIM><<<(unsigned)L.nval, DENSE_A_THREADS, 0, st>>>(c->x.p, c->rho.p, c->jxw.p, tpack, a, Lq,
+                                                                      blkpart);
+    const int64_t tb = (a.nt + DENSE_B_THREADS * DENSE_B_TT - 1) / (DENSE_B_THREADS * DENSE_B_TT);
+    const int64_t qslice = (a.nq + L.nks - 1) / L.nks;
+    dim3 g((unsigned)tb, (unsigned)L.nks);
+    if (c->precision == SDOT_PREC_FP64)
+        k_grad_dense<DIM, false><<<g, DENSE_B_THREADS, 0, st>>>(c->x.p, c->w.p, Lq, tpack, psi, a, qslice, gpart);
+    else
+        k_grad_dense<DIM, true><<<g, DENSE_B_THREADS, 0, st>>>(c->x.p, c->w.p, Lq, tpack, psi, a, qslice, gpart);
+    k_finalize_grad<<<FIN_BLOCKS, FIN_THREADS, 0, st>>>(a.nt, L.nks, gpart, c->nu.p, psi, nullptr,
+                                                       c->prm.tolerance, 1, grad, redpart);
+    k_finalize_scalars<<<1, 256, 0, st>>>(FIN_BLOCKS, redpart, L.nval, blkpart, scal);
+}
+
+}  // namespace sdot
+
+extern "C" sdot_status sdot_evaluate_device_noalloc(sdot_ctx *c, const double *psi_dev, double *grad_dev,
+                                                    double *value)
+{
+    using namespace sdot;
+    if (!c || !psi_dev || !grad_dev) return SDOT_EINVAL;
+    if (c->dim == 0 || c->nq == 0) return set_error(c, SDOT_ESTATE, "source measure not set");
+    if (c->nt == 0) return set_error(c, SDOT_ESTATE, "target measure not set");
+    const sdot_solver_params &p = c->prm;
+    if (p.threshold_type != SDOT_THRESH_POINTWISE || p.tau > 0)
+        return set_error(c, SDOT_EINVAL,
+                         "no-alloc evaluation covers untruncated problems only (pointwise threshold, tau <= 0)");
+    const NoallocLayout L = noalloc_layout(c->nq, c->nt);
+    const size_t need = (size_t)L.total * sizeof(double);
+    if (need > NOALLOC_BYTES)
+        return set_error(c, SDOT_EINVAL,
+                         "no-alloc evaluation needs " + std::to_string(need) + " bytes of scratch; the static limit is " +
+                             std::to_string(NOALLOC_BYTES) + " bytes (use sdot_evaluate_device)");
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != c->device) {
+        const cudaError_t e = cudaSetDevice(c->device);
+        if (e != cudaSuccess) return cuda_error(c, e, "no-alloc evaluation: set device");
+    }
+    struct Restore {
+        int dev;
+        ~Restore() {
+            if (dev >= 0) cudaSetDevice(dev);
+        }
+    } restore{prev != c->device ? prev : -1};
+    double *S = nullptr;
+    sdot_status s = noalloc_scratch(c, &S);
+    if (s != SDOT_OK) return s;
+
+    EvalArgs a{};
+    a.qpc = c->qpc;
+    a.ql = c->ql;
+    a.ngroups = c->ngroups;
+    a.lse = p.use_log_sum_exp;
+    a.nq = c->nq;
+    a.ncells = c->ncells;
+    a.nunits = c->ncells * a.ngroups;
+    a.nt = c->nt;
+    a.eps = p.epsilon;
+    a.s = KAPPA / p.epsilon;
+    a.halfs = 0.5 * a.s;
+    for (int d = 0; d < 3; ++d) a.o[d] = c->origin[d];
+    a.sstar = sstar_of(DBL_MAX);
+    a.cull = 1e300;
+    a.c32 = LOG2E / (2.0 * p.epsilon);
+    a.l2e_eps = LOG2E / p.epsilon;
+
+    if ((s = launch_gather(c, S + L.psi, psi_dev, c->nt)) != SDOT_OK) return s;
+    if (c->dim == 2) noalloc_launch<2>(c, a, S, L);
+    else noalloc_launch<3>(c, a, S, L);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_error(c, e, "no-alloc evaluation launch");
+    if ((s = launch_scatter(c, grad_dev, S + L.grad, c->nt)) != SDOT_OK) return s;
+    e = cudaMemcpyAsync(c->scal_host, S + L.scal, SC_COUNT * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_error(c, e, "no-alloc evaluation");
+    c->klaunch[1] += 1;
+    c->klaunch[2] += 1;
+    c->klaunch[3] += 1;
+    c->klaunch[4] += 2;
+    c->current_distance_threshold = DBL_MAX;
+    c->scal_host[SC_R] = DBL_MAX;
+    c->global_functional = c->scal_host[SC_VALUE];
+    c->C_global = c->scal_host[SC_C];
+    c->last_pairs = (int64_t)((double)c->nq * (double)c->nt);
+    if (value) *value = c->scal_host[SC_VALUE];
+    if (c->scal_host[SC_NONFINITE] != 0.0) return set_error(c, SDOT_ENONFINITE, "non-finite value or gradient");
+    return SDOT_OK;
+}

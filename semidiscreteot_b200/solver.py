@@ -145,6 +145,16 @@ class SotSolver:
                                "n_pairs": info.n_pairs, "device_ms": info.device_ms}
         return val.value
 
+    def evaluate_functional_device_noalloc(self, psi_ptr: int, grad_ptr: int) -> float:
+        """Untruncated evaluation on device pointers that allocates no device
+        memory (scratch in a static device array of NOALLOC_SCRATCH_BYTES per
+        device; overlapping calls on one device race).  Same results as
+        evaluate_functional_device."""
+        val = C.c_double(0.0)
+        self._check(self._L.sdot_evaluate_device_noalloc(self._h, C.c_void_p(psi_ptr), C.c_void_p(grad_ptr),
+                                                         C.byref(val)))
+        return val.value
+
     def solve(self, potential: np.ndarray, params: Optional[SolverParameters] = None) -> np.ndarray:
         """SotSolver::solve (SotSolver.cc:105-215): L-BFGS on the device.
         ``potential`` is updated in place when it is a float64 C-contiguous array."""
