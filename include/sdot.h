@@ -152,6 +152,35 @@ sdot_status sdot_solve(sdot_ctx *ctx, double *psi, const sdot_solver_params *par
  * H = (1/eps) sum_q w_q (diag(pi_q) - pi_q pi_q^T) into host memory H. */
 sdot_status sdot_hessian(sdot_ctx *ctx, const double *psi, double *H);
 
+/* Hessian on device memory, by method:
+ *   SDOT_HESS_FP64  : the FP64 kernel of sdot_hessian (any threshold);
+ *   SDOT_HESS_TENSOR: tcgen05 tensor cores, H = (diag(sum w pi) - P_w^T P)/eps
+ *                     with P regenerated tile by tile (never stored), BF16
+ *                     hi+lo operands (three products), FP32 accumulation in
+ *                     tensor memory drained into FP64 every few thousand
+ *                     points; relative Frobenius error ~1e-5 against FP64.
+ *                     Needs an untruncated evaluation (tau <= 0, or a
+ *                     threshold above the domain diameter) and rho*JxW >= 0;
+ *   SDOT_HESS_AUTO  : SDOT_HESS_TENSOR when it applies, else SDOT_HESS_FP64.
+ * Same matrix as sdot_hessian (the declared-only SotSolver::compute_hessian,
+ * SotSolver.h:343-344), evaluated at psi_dev (device, caller order, n_targets
+ * doubles).  H_dev: device, n_targets^2 entries row-major in the caller's
+ * order, double (out_f32 = 0) or float (out_f32 = 1, tensor method only).
+ * Like an evaluation, it updates the state read by the thresholds. */
+typedef enum { SDOT_HESS_AUTO = 0, SDOT_HESS_FP64 = 1, SDOT_HESS_TENSOR = 2 } sdot_hessian_method;
+typedef struct {
+    int method;                 /* method used */
+    double eval_ms;             /* device time of the evaluation at psi */
+    double hessian_ms;          /* device time of the Hessian (set-up kernels included) */
+    double kernel_ms;           /* main Hessian kernel alone (tensor method: needs sdot_set_profiling) */
+    int64_t tiles;              /* tensor method: 128 x 256 output tiles computed */
+} sdot_hessian_info;
+sdot_status sdot_hessian_device(sdot_ctx *ctx, const double *psi_dev, void *H_dev, int method, int out_f32,
+                                sdot_hessian_info *info);
+/* Tuning of the tensor method: stages of 64 points accumulated in FP32 before
+ * each FP64 drain (default 16). */
+sdot_status sdot_set_hessian_chunk(sdot_ctx *ctx, int stages);
+
 /* Getters replacing SotSolver::get_last_functional_value, get_last_iteration_count,
  * get_convergence_status, get_last_distance_threshold, get_C_global
  * (SotSolver.h:233-255) and the setter set_distance_threshold (:261). */

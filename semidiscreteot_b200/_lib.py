@@ -21,6 +21,7 @@ PRECISION = {"fp64": 0, "hybrid": 1, "mixed": 2}
 THRESHOLD = {"pointwise": 0, "integral": 1, "geometric": 2}
 CONTROL = {"l1norm": 0, "componentwise": 1, "linf": 2}
 LINE_SEARCH = {"upstream": 0, "vendored": 1}
+HESSIAN_METHOD = {"auto": 0, "fp64": 1, "tensor": 2}
 
 # Every symbol include/sdot.h declares (checked by tests).
 EXPORTED = [
@@ -31,7 +32,7 @@ EXPORTED = [
     "sdot_get_C_global", "sdot_set_distance_threshold", "sdot_compute_covering_radius",
     "sdot_compute_geometric_radius_bound", "sdot_set_distance_function", "sdot_evaluate_partial_device",
     "sdot_set_state", "sdot_get_stream", "sdot_set_profiling", "sdot_get_kernel_times", "sdot_measure_peaks",
-    "sdot_evaluate_device_noalloc",
+    "sdot_evaluate_device_noalloc", "sdot_hessian_device", "sdot_set_hessian_chunk",
 ]
 
 NOALLOC_SCRATCH_BYTES = 8 << 20  # SDOT_NOALLOC_SCRATCH_BYTES
@@ -57,6 +58,11 @@ class SolveInfo(C.Structure):
     _fields_ = [("iterations", C.c_uint), ("converged", C.c_int), ("n_evaluations", C.c_int64),
                 ("last_value", C.c_double), ("last_check_value", C.c_double), ("total_pairs", C.c_int64),
                 ("device_ms", C.c_double)]
+
+
+class HessianInfo(C.Structure):
+    _fields_ = [("method", C.c_int), ("eval_ms", C.c_double), ("hessian_ms", C.c_double),
+                ("kernel_ms", C.c_double), ("tiles", C.c_int64)]
 
 
 _lib = None
@@ -109,6 +115,10 @@ def load():
     lib.sdot_measure_peaks.argtypes = [ip, vp]
     lib.sdot_evaluate_device_noalloc.argtypes = [vp, vp, vp, C.POINTER(d)]
     lib.sdot_evaluate_device_noalloc.restype = ip
+    lib.sdot_hessian_device.argtypes = [vp, vp, vp, ip, ip, C.POINTER(HessianInfo)]
+    lib.sdot_hessian_device.restype = ip
+    lib.sdot_set_hessian_chunk.argtypes = [vp, ip]
+    lib.sdot_set_hessian_chunk.restype = ip
     for fn in ("sdot_evaluate_partial_device", "sdot_set_state", "sdot_set_profiling", "sdot_get_kernel_times",
                "sdot_measure_peaks"):
         getattr(lib, fn).restype = ip

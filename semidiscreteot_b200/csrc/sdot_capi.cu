@@ -203,8 +203,13 @@ size_t device_bytes(const sdot_ctx *c)
            c->tblk_sph.bytes() + c->psi.bytes() + c->grad.bytes() + c->tpack.bytes() + c->Lq.bytes() +
            c->gpart.bytes() + c->blkpart.bytes() + c->scal.bytes() + c->redpart.bytes() + c->io_a.bytes() +
            c->io_b.bytes() + c->x0.bytes() + c->pdir.bytes() + c->sk.bytes() + c->yk.bytes() + c->hist_s.bytes() +
-           c->hist_y.bytes() + c->gtmp.bytes();
+           c->hist_y.bytes() + c->gtmp.bytes() + c->htc_tdat.bytes() + c->htc_diag.bytes() + c->htc_blk.bytes() +
+           c->htc_scr.bytes() + c->htc_qa.bytes() + c->htc_qb.bytes() + c->htc_tiles.bytes() + c->htc_err.bytes();
 }
+
+}  // namespace
+
+namespace sdot {
 
 sdot_status ensure_eval_buffers(sdot_ctx *c)
 {
@@ -227,7 +232,7 @@ sdot_status ensure_eval_buffers(sdot_ctx *c)
     return SDOT_OK;
 }
 
-}  // namespace
+}  // namespace sdot
 
 // ---------------------------------------------------------------------------
 // covering radius: max over cells of min over targets of |y_j - c_K|

@@ -128,12 +128,10 @@ __global__ void k_permute_matrix(const double *__restrict__ Hi, double *__restri
     }
 }
 
-sdot_status hessian_internal(sdot_ctx *c, double *H_host)
+// FP64 Hessian at the potential of the last evaluation into H_dev (device,
+// n x n row-major, caller order).
+static sdot_status hessian_fp64_to(sdot_ctx *c, double *H_dev)
 {
-    // an evaluation at c->psi provides L_q, the gradient and the threshold
-    double ms = 0;
-    sdot_status s = evaluate_internal(c, nullptr, c->prm.tolerance, &ms);
-    if (s != SDOT_OK) return s;
     const int64_t n = c->nt;
     if (n > 46340) return set_error(c, SDOT_EBUDGET, "dense Hessian limited to n_targets <= 46340");
     const double r = c->current_distance_threshold;
@@ -149,9 +147,8 @@ sdot_status hessian_internal(sdot_ctx *c, double *H_host)
     a.sstar = sstar_of(r);
     const bool trunc = std::isnan(r) || r < c->diam;
     launch_target_prep_dense(c, a);  // the truncated evaluation leaves another layout in tpack
-    DevBuf<double> Hi, Hu;
+    DevBuf<double> Hi;
     cudaError_t e = Hi.alloc((size_t)n * n);
-    if (e == cudaSuccess) e = Hu.alloc((size_t)n * n);
     if (e != cudaSuccess) return cuda_error(c, e, "hessian alloc");
     const unsigned nb = (unsigned)((n + HT - 1) / HT);
     dim3 g(nb, nb);
@@ -164,14 +161,103 @@ sdot_status hessian_internal(sdot_ctx *c, double *H_host)
     }
     k_permute_matrix<<<dim3(std::max<unsigned>(1, (unsigned)std::min<int64_t>((n + 255) / 256, 64)),
                             (unsigned)std::min<int64_t>(n, 65535)), 256, 0,
-                       c->stream>>>(Hi.p, Hu.p, c->perm.p, n);
+                       c->stream>>>(Hi.p, H_dev, c->perm.p, n);
     e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaMemcpyAsync(H_host, Hu.p, (size_t)n * n * 8, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);  // Hi is released on return
+    return cuda_error(c, e, "hessian");
+}
+
+sdot_status hessian_internal(sdot_ctx *c, double *H_host)
+{
+    // an evaluation at c->psi provides L_q, the gradient and the threshold
+    double ms = 0;
+    sdot_status s = evaluate_internal(c, nullptr, c->prm.tolerance, &ms);
+    if (s != SDOT_OK) return s;
+    const int64_t n = c->nt;
+    if (n > 46340) return set_error(c, SDOT_EBUDGET, "dense Hessian limited to n_targets <= 46340");
+    DevBuf<double> Hu;
+    cudaError_t e = Hu.alloc((size_t)n * n);
+    if (e != cudaSuccess) return cuda_error(c, e, "hessian alloc");
+    if ((s = hessian_fp64_to(c, Hu.p)) != SDOT_OK) return s;
+    e = cudaMemcpyAsync(H_host, Hu.p, (size_t)n * n * 8, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     return cuda_error(c, e, "hessian");
 }
 
+// The tensor-core path needs every (q, j) pair in the sum (no truncation) and
+// w_q >= 0 (its log2 w_q is folded into the exponent).
+static bool tensor_ok(const sdot_ctx *c)
+{
+    const double r = c->current_distance_threshold;
+    const bool dense = std::isinf(r) || !(r < c->diam * (1.0 + 1e-12));
+    return dense && !std::isnan(r) && c->w_nonneg;
+}
+
+sdot_status hessian_device(sdot_ctx *c, const double *psi_dev, void *H_dev, int method, int out_f32,
+                           sdot_hessian_info *info)
+{
+    if (method != SDOT_HESS_AUTO && method != SDOT_HESS_FP64 && method != SDOT_HESS_TENSOR)
+        return set_error(c, SDOT_EINVAL, "unknown Hessian method");
+    sdot_status s = launch_gather(c, c->psi.p, psi_dev, c->nt);
+    if (s != SDOT_OK) return s;
+    double ems = 0, hms = 0;
+    s = evaluate_internal(c, nullptr, c->prm.tolerance, &ems);
+    if (s != SDOT_OK) return s;
+    int used = method;
+    if (method == SDOT_HESS_AUTO) used = tensor_ok(c) ? SDOT_HESS_TENSOR : SDOT_HESS_FP64;
+    if (used == SDOT_HESS_TENSOR) {
+        if (!tensor_ok(c))
+            return set_error(c, SDOT_EINVAL,
+                             "tensor-core Hessian needs an untruncated evaluation (tau <= 0 or a threshold above the "
+                             "domain diameter) and rho*JxW >= 0");
+        s = hessian_tc(c, H_dev, out_f32 != 0, c->hess_chunk, &hms);
+    } else {
+        if (out_f32) return set_error(c, SDOT_EINVAL, "the FP64 Hessian writes doubles (out_f32 must be 0)");
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, c->stream);
+        s = hessian_fp64_to(c, static_cast<double *>(H_dev));
+        cudaEventRecord(e1, c->stream);
+        cudaEventSynchronize(e1);
+        float f = 0.f;
+        cudaEventElapsedTime(&f, e0, e1);
+        hms = f;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
+    if (info) {
+        info->method = used;
+        info->eval_ms = ems;
+        info->hessian_ms = hms;
+        info->tiles = used == SDOT_HESS_TENSOR ? c->hess_tiles : 0;
+        info->kernel_ms = used == SDOT_HESS_TENSOR ? c->hess_kernel_ms : hms;
+    }
+    return s;
+}
+
 }  // namespace sdot
+
+extern "C" sdot_status sdot_hessian_device(sdot_ctx *c, const double *psi_dev, void *H_dev, int method, int out_f32,
+                                           sdot_hessian_info *info)
+{
+    if (!c || !psi_dev || !H_dev) return SDOT_EINVAL;
+    if (c->nq == 0 || c->nt == 0) return sdot::set_error(c, SDOT_ESTATE, "measures not set");
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != c->device) cudaSetDevice(c->device);
+    sdot_status s = sdot::ensure_eval_buffers(c);
+    if (s == SDOT_OK) s = sdot::hessian_device(c, psi_dev, H_dev, method, out_f32, info);
+    if (prev >= 0 && prev != c->device) cudaSetDevice(prev);
+    return s;
+}
+
+extern "C" sdot_status sdot_set_hessian_chunk(sdot_ctx *c, int stages)
+{
+    if (!c || stages < 1) return SDOT_EINVAL;
+    c->hess_chunk = stages;
+    return SDOT_OK;
+}
 
 extern "C" sdot_status sdot_hessian(sdot_ctx *c, const double *psi, double *H)
 {

@@ -1,0 +1,585 @@
+// sdot_hessian_tc.cu -- Hessian of the entropic dual on the tcgen05 tensor cores.
+//
+//     H = (1/eps) [ diag(sum_q w_q pi_q) - P_w^T P ],   P_w = diag(w) P,
+//     pi_qj = nu_j exp(t_qj - L_q),  t_qj = (psi_j - |x_q - y_j|^2 / 2) / eps,
+// the same matrix as the FP64 path in sdot_hessian.cu (SotSolver::compute_hessian,
+// declared at include/SemiDiscreteOT/solvers/SotSolver.h:343-344).  Here the
+// contraction S = P_w^T P runs on tcgen05.mma (kind::f16, BF16 operands, FP32
+// accumulators in tensor memory):
+//
+//  * P is never stored.  A CTA owns a 128 x 256 tile of S (rows a, columns b)
+//    and, for every stage of 64 quadrature points, regenerates the 128 rows
+//    w_q pi_qa and the 256 rows pi_qb straight into 128B-swizzled K-major
+//    shared memory, where one elected thread hands them to tcgen05.mma.
+//  * BF16 hi+lo split: v = hi + lo with hi = bf16_rn(v), lo = bf16_rz(v - hi);
+//    S ~ Ahi.Bhi + Ahi.Blo + Alo.Bhi (the lo.lo term, ~2^-18 relative, dropped).
+//  * Exponents in FP32 with FP64-formed offsets: log2(w_q pi_qj) =
+//    E_bj + G_bj . d_q + F_q, where b is the 64-point block of q, c_b its
+//    bounding-box centre, d_q = x_q - c_b, and
+//       E_bj = log2 nu_j + (log2 e / eps)(psi_j - |y_j - c_b|^2 / 2) - log2 e L_b,
+//       G_bj = (log2 e / eps)(y_j - c_b),
+//       F_q  = -(log2 e / eps)|d_q|^2 / 2 - log2 e (L_q - L_b) [+ log2 w_q],
+//    L_b = min of L_q over the block.  E and G are computed in FP64 per
+//    (stage, target) and rounded once, so every FP32 operand is O(1)-O(100)
+//    and the exponent error stays ~1e-5 (relative error of pi ~ 1e-5).
+//  * Tensor-core FP32 accumulation over all Q points would lose accuracy, so
+//    the accumulator is double-buffered in TMEM (2 x 256 columns) and drained
+//    into FP64 every `ch` stages; the drain of one chunk overlaps the MMAs of
+//    the next.
+//  * Upper triangle only: tile (ta, tb) exists iff it holds some b >= a;
+//    entries with b > a are written to H[a][b] and mirrored to H[b][a], so H is
+//    exactly symmetric.
+//
+// Targets are in the caller's order (no permutation pass); quadrature points in
+// the library's internal order (the sum over q is order-free).  Every mbarrier
+// wait is bounded (~1 s of SM clocks); a timeout sets an error flag, the CTA
+// waits (bounded) for its MMAs in flight, frees its tensor memory and returns.
+// No TMA and no cluster multicast are used.
+#include <float.h>
+#include <math.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "sdot_device.cuh"
+#include "sdot_internal.h"
+
+namespace sdot {
+
+namespace htc {
+
+constexpr int M = 128;               // rows a per tile (MMA M)
+constexpr int N = 256;               // columns b per tile (MMA N)
+constexpr int KQ = 64;               // quadrature points per stage (one 128-byte swizzle row of BF16)
+constexpr int WARPS = 16;
+constexpr int THREADS = WARPS * 32;
+constexpr int ROWS = M + N;          // generated operand rows per stage
+constexpr int RG = WARPS * 4;        // row groups (4 per warp, 8 lanes = 8 K-chunks each)
+constexpr int RPT = ROWS / RG;       // rows per thread per stage
+constexpr int ARPT = M / RG;         // of which A rows
+static_assert(ROWS % RG == 0 && M % RG == 0, "row split");
+static_assert(THREADS == ROWS + 2 * KQ, "one staging item per thread");
+
+constexpr uint32_t A_BYTES = M * KQ * 2;                 // 16 KB
+constexpr uint32_t B_BYTES = N * KQ * 2;                 // 32 KB
+constexpr uint32_t STAGE_BYTES = 2 * (A_BYTES + B_BYTES); // Ahi, Alo, Bhi, Blo
+constexpr uint32_t OFF_EG = 2 * STAGE_BYTES;             // float4 [2][ROWS]
+constexpr uint32_t OFF_QA = OFF_EG + 2 * ROWS * 16;      // float4 [2][KQ]
+constexpr uint32_t OFF_QB = OFF_QA + 2 * KQ * 16;        // float  [2][KQ]
+constexpr uint32_t OFF_BAR = OFF_QB + 2 * KQ * 4;        // 4 mbarriers + TMEM address
+constexpr uint32_t SMEM_BYTES = OFF_BAR + 64 + 1024;     // + alignment slack
+constexpr int TMEM_COLS = 2 * N;                          // two FP32 accumulators
+constexpr int SCR_PER_CTA = M * N;                        // FP64 drain scratch per CTA
+
+// kind::f16 instruction descriptor: D F32 (bits 4-5 = 1), A BF16 (7-9 = 1),
+// B BF16 (10-12 = 1), both K-major, N >> 3 at bits 17-22, M >> 4 at bits 24-28.
+constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
+                           ((uint32_t)(M >> 4) << 24);
+
+constexpr long long WAIT_LIMIT = 2000000000ll;  // SM clocks (~1 s)
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for the completion of the phase with the given parity.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
+{
+    if (mbar_test(bar, parity)) return true;
+    const long long t0 = clock64();
+    while (!mbar_test(bar, parity))
+        if (clock64() - t0 > WAIT_LIMIT) return false;
+    return true;
+}
+
+// Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row atoms of
+// 1024 bytes (SBO = 1024), descriptor version 1 (bits 46-47), layout type 2
+// (SWIZZLE_128B, bits 61-63).  LBO is unused for this layout (set to 16 B).
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr)
+{
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+           ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t dtmem, uint64_t ad, uint64_t bd, uint32_t accum)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(dtmem),
+        "l"(ad), "l"(bd), "r"(IDESC), "r"(accum));
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// 32 lanes x 16 consecutive 32-bit columns; the wait is in the same asm so the
+// registers are never read before the load has landed.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
+{
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n\t"
+        "tcgen05.wait::ld.sync.aligned;\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr)
+        : "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+struct Args {
+    const float4 *qa;       // per q: {dx, dy, dz, F^B}
+    const float *qb;        // per q: F^A = F^B + log2 w_q
+    const double4 *blk;     // per 64-point block: {c_b (3), log2 e * L_b}
+    const double4 *tdat;    // per target (caller order, padded): {y - o (3), log2 nu + l2e_eps psi}
+    const double *diag;     // per target: sum_q w_q pi_qj = g_j + nu_j
+    const int2 *tiles;      // (ta, tb)
+    int ntiles;
+    int nst;                // stages per tile
+    int ch;                 // stages per FP32 accumulation chunk
+    int64_t n;
+    double l2e_eps;         // log2(e) / eps
+    double inv_eps;
+    double *scratch;        // SCR_PER_CTA doubles per CTA
+    void *H;
+    int *err;
+};
+
+template <int DIM, typename OutT>
+__global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
+{
+    extern __shared__ uint8_t smem_raw[];
+    const uint32_t raw_s = smem_u32(smem_raw);
+    uint8_t *sm = smem_raw + ((1024u - (raw_s & 1023u)) & 1023u);  // 1024-aligned shared address
+    const uint32_t sm_s = smem_u32(sm);
+    float4 *Eg = reinterpret_cast<float4 *>(sm + OFF_EG);
+    float4 *qA = reinterpret_cast<float4 *>(sm + OFF_QA);
+    float *qB = reinterpret_cast<float *>(sm + OFF_QB);
+    const uint32_t bar0 = sm_s + OFF_BAR;  // [0,1] stage buffers, [2,3] accumulators (8 bytes each)
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + OFF_BAR + 32);
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid == 0) {
+        for (int i = 0; i < 4; ++i) mbar_init(bar0 + 8 * i, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+
+    // ---- staging of one stage's per-target and per-point data (one item per thread) ----
+    double4 pt = make_double4(0, 0, 0, 0), pb = make_double4(0, 0, 0, 0);
+    float4 pq = make_float4(0, 0, 0, 0);
+    float pqb = 0.f;
+    auto stage_load = [&](int t, int st) {
+        const int2 tl = a.tiles[t];
+        if (tid < ROWS) {
+            const int64_t j = tid < M ? (int64_t)tl.x * M + tid : (int64_t)tl.y * N + (tid - M);
+            pt = a.tdat[j];
+            pb = a.blk[st];
+        } else if (tid < ROWS + KQ) {
+            pq = a.qa[(int64_t)st * KQ + (tid - ROWS)];
+        } else {
+            pqb = a.qb[(int64_t)st * KQ + (tid - ROWS - KQ)];
+        }
+    };
+    auto stage_store = [&](int buf) {
+        if (tid < ROWS) {
+            const double dx = pt.x - pb.x, dy = pt.y - pb.y, dz = DIM == 3 ? pt.z - pb.z : 0.0;
+            const double e = pt.w - 0.5 * a.l2e_eps * (dx * dx + dy * dy + dz * dz) - pb.w;
+            Eg[buf * ROWS + tid] = make_float4((float)e, (float)(a.l2e_eps * dx), (float)(a.l2e_eps * dy),
+                                               (float)(a.l2e_eps * dz));
+        } else if (tid < ROWS + KQ) {
+            const int p = tid - ROWS;
+            qA[buf * KQ + (p & 7) * 8 + (p >> 3)] = pq;   // transposed: [i][kc] for q = kc * 8 + i
+        } else {
+            const int p = tid - ROWS - KQ;
+            qB[buf * KQ + (p & 7) * 8 + (p >> 3)] = pqb;
+        }
+    };
+
+    // ---- generation of one stage's operands into shared memory ----
+    const int kc = lane & 7;                 // 16-byte chunk (8 points) of the 64-point stage
+    const int rg = warp * 4 + (lane >> 3);   // row group
+    auto generate = [&](int buf) {
+        float dx[8], dy[8], dz[8], fa[8], fb[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const float4 t = qA[buf * KQ + i * 8 + kc];
+            dx[i] = t.x;
+            dy[i] = t.y;
+            dz[i] = t.z;
+            fb[i] = t.w;
+            fa[i] = qB[buf * KQ + i * 8 + kc];
+        }
+        uint8_t *stage = sm + buf * STAGE_BYTES;
+#pragma unroll
+        for (int it = 0; it < RPT; ++it) {
+            const bool isA = it < ARPT;
+            const int r = rg + RG * it;
+            const float4 e = Eg[buf * ROWS + r];
+            uint32_t hw[4], lw[4];
+#pragma unroll
+            for (int k = 0; k < 8; k += 2) {
+                float u0 = e.x + (isA ? fa[k] : fb[k]);
+                float u1 = e.x + (isA ? fa[k + 1] : fb[k + 1]);
+                u0 = fmaf(e.y, dx[k], u0);
+                u1 = fmaf(e.y, dx[k + 1], u1);
+                u0 = fmaf(e.z, dy[k], u0);
+                u1 = fmaf(e.z, dy[k + 1], u1);
+                if (DIM == 3) {
+                    u0 = fmaf(e.w, dz[k], u0);
+                    u1 = fmaf(e.w, dz[k + 1], u1);
+                }
+                const float v0 = ex2_approx(u0), v1 = ex2_approx(u1);
+                const uint32_t h0 = (__float_as_uint(v0) + 0x8000u) & 0xffff0000u;
+                const uint32_t h1 = (__float_as_uint(v1) + 0x8000u) & 0xffff0000u;
+                const float l0 = v0 - __uint_as_float(h0), l1 = v1 - __uint_as_float(h1);
+                hw[k >> 1] = __byte_perm(h0, h1, 0x7632);
+                lw[k >> 1] = __byte_perm(__float_as_uint(l0), __float_as_uint(l1), 0x7632);
+            }
+            const int rr = isA ? r : r - M;
+            const uint32_t off = (uint32_t)(rr >> 3) * 1024u + (uint32_t)(rr & 7) * 128u + ((uint32_t)(kc ^ (rr & 7)) << 4);
+            uint8_t *hi = stage + (isA ? 0u : 2u * A_BYTES);
+            uint8_t *lo = hi + (isA ? A_BYTES : B_BYTES);
+            *reinterpret_cast<uint4 *>(hi + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+            *reinterpret_cast<uint4 *>(lo + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+        }
+    };
+
+    // ---- drain of one accumulation chunk into FP64 (and the epilogue on a tile's last chunk) ----
+    const int quad = warp & 3, cq = warp >> 2;   // TMEM lane quadrant, 64-column quarter
+    const int row = quad * 32 + lane;
+    double *scr = a.scratch + (size_t)blockIdx.x * SCR_PER_CTA;
+    auto drain = [&](unsigned pc, int tile, bool first, bool last) -> bool {
+        const bool ok = mbar_wait(bar0 + 8 * (2 + (pc & 1)), (pc >> 1) & 1);
+        tc_fence_after();
+        const int2 tl = a.tiles[tile];
+        const int64_t ga = (int64_t)tl.x * M + row;
+        const uint32_t taddr = tmem + (pc & 1) * N + cq * 64 + ((uint32_t)(quad * 32) << 16);
+#pragma unroll 1
+        for (int c16 = 0; c16 < 4; ++c16) {
+            float v[16];
+            tmem_ld16(taddr + c16 * 16, v);
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                const int col = cq * 64 + c16 * 16 + i;
+                const size_t idx = (size_t)col * M + row;
+                double s = (double)v[i];
+                if (!first) s += scr[idx];
+                if (!last) {
+                    scr[idx] = s;
+                } else {
+                    const int64_t gb = (int64_t)tl.y * N + col;
+                    if (ga < a.n && gb < a.n && gb >= ga) {
+                        const double h = ((gb == ga ? a.diag[ga] : 0.0) - s) * a.inv_eps;
+                        OutT *H = reinterpret_cast<OutT *>(a.H);
+                        H[ga * a.n + gb] = (OutT)h;
+                        if (gb != ga) H[gb * a.n + ga] = (OutT)h;
+                    }
+                }
+            }
+        }
+        tc_fence_before();
+        return ok;
+    };
+
+    int g = 0;               // global stage counter (stage-buffer phases)
+    unsigned chunk = 0;      // global chunk counter (accumulator phases)
+    int pend = -1, pend_tile = 0;
+    bool pend_first = false, pend_last = false;
+    bool bad = false;        // this thread saw a wait expire
+    bool aborted = false;
+    int last_g = -1;
+
+    if ((int)blockIdx.x < a.ntiles) {
+        stage_load(blockIdx.x, 0);
+        stage_store(0);
+    }
+    __syncthreads();
+
+    // One block-wide barrier per stage: it publishes the stage's operands to
+    // the MMA thread and orders the previous drain's TMEM reads before any MMA
+    // that reuses that accumulator.
+    for (int t = blockIdx.x; t < a.ntiles && !aborted; t += gridDim.x) {
+        for (int st = 0; st < a.nst; ++st, ++g) {
+            const int sb = g & 1;
+            int tn = t, sn = st + 1;
+            if (sn == a.nst) { tn = t + gridDim.x; sn = 0; }
+            const bool has_next = tn < a.ntiles;
+            if (has_next) stage_load(tn, sn);
+            // the MMAs that read this buffer two stages ago must be complete
+            if (g >= 2 && !mbar_wait(bar0 + 8 * sb, ((g >> 1) - 1) & 1)) bad = true;
+            generate(sb);
+            if (has_next) stage_store(sb ^ 1);
+            fence_async_smem();
+            if (__syncthreads_or(bad)) { aborted = true; break; }
+            const bool first_in_chunk = (st % a.ch) == 0;
+            const bool last_in_chunk = (st % a.ch) == a.ch - 1 || st == a.nst - 1;
+            const unsigned cb = chunk & 1;
+            if (tid == 0) {
+                tc_fence_after();
+                const uint32_t sbase = sm_s + sb * STAGE_BYTES;
+                const uint32_t dcol = tmem + cb * N;
+#pragma unroll
+                for (int kk = 0; kk < KQ / 16; ++kk) {
+                    const uint64_t ah = sdesc(sbase + kk * 32), al = sdesc(sbase + A_BYTES + kk * 32);
+                    const uint64_t bh = sdesc(sbase + 2 * A_BYTES + kk * 32);
+                    const uint64_t bl = sdesc(sbase + 2 * A_BYTES + B_BYTES + kk * 32);
+                    umma_bf16(dcol, ah, bh, (first_in_chunk && kk == 0) ? 0u : 1u);
+                    umma_bf16(dcol, ah, bl, 1u);
+                    umma_bf16(dcol, al, bh, 1u);
+                }
+                umma_commit(bar0 + 8 * sb);
+                if (last_in_chunk) umma_commit(bar0 + 8 * (2 + cb));
+            }
+            last_g = g;
+            // drain the previous chunk while the tensor core works on this one
+            if (first_in_chunk && pend >= 0) {
+                if (!drain((unsigned)pend, pend_tile, pend_first, pend_last)) bad = true;
+                pend = -1;
+            }
+            if (last_in_chunk) {
+                pend = (int)chunk;
+                pend_tile = t;
+                pend_first = st < a.ch;
+                pend_last = st == a.nst - 1;
+                ++chunk;
+            }
+        }
+    }
+    if (!aborted && pend >= 0) {
+        if (!drain((unsigned)pend, pend_tile, pend_first, pend_last)) bad = true;
+    }
+    if (__syncthreads_or(bad)) aborted = true;
+    if (aborted && tid == 0) {
+        atomicExch(a.err, 1);
+        // let the MMAs in flight finish before the tensor memory is released
+        if (last_g >= 0) mbar_wait(bar0 + 8 * (last_g & 1), (last_g >> 1) & 1);
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+    }
+}
+
+// Per-target data in the caller's order: tdat[perm[i]] = {y_i - o, log2 nu_i + l2e_eps psi_i},
+// diag[perm[i]] = g_i + nu_i.  Padding rows (>= n) get log2 weight -inf (pi = 0).
+template <int DIM>
+__global__ void k_htc_targets(int64_t n, int64_t npad, const double *__restrict__ y, const double *__restrict__ nu,
+                              const double *__restrict__ psi, const double *__restrict__ grad,
+                              const int64_t *__restrict__ perm, double ox, double oy, double oz, double l2e_eps,
+                              double4 *__restrict__ tdat, double *__restrict__ diag)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < npad; i += (int64_t)gridDim.x * blockDim.x) {
+        if (i < n) {
+            const int64_t j = perm[i];
+            const double lw = nu[i] > 0.0 ? log2(nu[i]) + l2e_eps * psi[i] : -CUDART_INF;
+            tdat[j] = make_double4(y[i * DIM] - ox, y[i * DIM + 1] - oy, DIM == 3 ? y[i * DIM + 2] - oz : 0.0, lw);
+            diag[j] = grad[i] + nu[i];
+        } else {
+            tdat[i] = make_double4(0.0, 0.0, 0.0, -CUDART_INF);
+            diag[i] = 0.0;
+        }
+    }
+}
+
+// One warp per 64-point block: block centre, reference L_b, per-point offsets
+// and the per-point exponent terms F^B, F^A.
+template <int DIM>
+__global__ void k_htc_points(int64_t nq, int nst, const double *__restrict__ x, const double *__restrict__ Lq,
+                             const double *__restrict__ w, double ox, double oy, double oz, double l2e_eps,
+                             float4 *__restrict__ qa, float *__restrict__ qb, double4 *__restrict__ blk)
+{
+    const int lane = threadIdx.x & 31;
+    const int b = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+    if (b >= nst) return;
+    const double o[3] = {ox, oy, oz};
+    double xt[2][3];
+    bool valid[2], fin[2];
+    double Lv[2];
+    double lo[3] = {CUDART_INF, CUDART_INF, CUDART_INF}, hi[3] = {-CUDART_INF, -CUDART_INF, -CUDART_INF};
+    double lmin = CUDART_INF;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int64_t q = (int64_t)b * KQ + lane + 32 * h;
+        valid[h] = q < nq;
+        Lv[h] = valid[h] ? Lq[q] : CUDART_INF;
+        fin[h] = valid[h] && isfinite(Lv[h]);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            xt[h][d] = (valid[h] && d < DIM) ? x[q * DIM + d] - o[d] : 0.0;
+            if (valid[h]) {
+                lo[d] = fmin(lo[d], xt[h][d]);
+                hi[d] = fmax(hi[d], xt[h][d]);
+            }
+        }
+        if (fin[h]) lmin = fmin(lmin, Lv[h]);
+    }
+#pragma unroll
+    for (int o2 = 16; o2 > 0; o2 >>= 1) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = fmin(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o2));
+            hi[d] = fmax(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o2));
+        }
+        lmin = fmin(lmin, __shfl_xor_sync(0xffffffffu, lmin, o2));
+    }
+    double cb[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) cb[d] = (d < DIM && lo[d] <= hi[d]) ? 0.5 * (lo[d] + hi[d]) : 0.0;
+    const double lref = isfinite(lmin) ? LOG2E * lmin : 0.0;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int64_t q = (int64_t)b * KQ + lane + 32 * h;
+        float4 out = make_float4(0.f, 0.f, 0.f, -CUDART_INF_F);
+        float fa = -CUDART_INF_F;
+        if (fin[h]) {
+            const double dx = xt[h][0] - cb[0], dy = xt[h][1] - cb[1], dz = xt[h][2] - cb[2];
+            const double fb = -0.5 * l2e_eps * (dx * dx + dy * dy + dz * dz) - (LOG2E * Lv[h] - lref);
+            const double wq = w[q];
+            out = make_float4((float)dx, (float)dy, (float)dz, (float)fb);
+            fa = wq > 0.0 ? (float)(fb + log2(wq)) : -CUDART_INF_F;
+        }
+        qa[q] = out;
+        qb[q] = fa;
+    }
+    if (lane == 0) blk[b] = make_double4(cb[0], cb[1], cb[2], lref);
+}
+
+}  // namespace htc
+
+// Tensor-core Hessian at the potential of the last evaluation (c->psi, c->Lq,
+// c->grad must come from an untruncated evaluation).  H_dev: n x n row-major in
+// the caller's target order, double or float.
+sdot_status hessian_tc(sdot_ctx *c, void *H_dev, bool out_f32, int chunk_stages, double *ms_out)
+{
+    using namespace htc;
+    const int64_t n = c->nt;
+    const int64_t na = (n + M - 1) / M, nb = (n + N - 1) / N;
+    const int64_t npad = std::max(na * M, nb * N);
+    const int64_t nst = (c->nq + KQ - 1) / KQ;
+    if (nst > INT32_MAX / 2) return set_error(c, SDOT_EINVAL, "too many quadrature points for the tensor-core Hessian");
+    std::vector<int2> tiles;
+    tiles.reserve((size_t)(na * nb));
+    for (int64_t ta = 0; ta < na; ++ta)
+        for (int64_t tb = (ta * M) / N; tb < nb; ++tb) tiles.push_back(make_int2((int)ta, (int)tb));
+    int dev_sms = 148;
+    cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c->device);
+    const int grid = (int)std::min<int64_t>((int64_t)dev_sms, (int64_t)tiles.size());
+
+    cudaError_t e = c->htc_tdat.alloc((size_t)npad * 4);
+    if (e == cudaSuccess) e = c->htc_diag.alloc((size_t)npad);
+    if (e == cudaSuccess) e = c->htc_blk.alloc((size_t)nst * 4);
+    if (e == cudaSuccess) e = c->htc_qa.alloc((size_t)nst * KQ * 4);
+    if (e == cudaSuccess) e = c->htc_qb.alloc((size_t)nst * KQ);
+    if (e == cudaSuccess) e = c->htc_tiles.alloc(tiles.size() * 2);
+    if (e == cudaSuccess) e = c->htc_scr.alloc((size_t)grid * SCR_PER_CTA);
+    if (e == cudaSuccess) e = c->htc_err.alloc(1);
+    if (e != cudaSuccess) return cuda_error(c, e, "tensor-core Hessian buffers");
+    e = cudaMemcpyAsync(c->htc_tiles.p, tiles.data(), tiles.size() * sizeof(int2), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->htc_err.p, 0, sizeof(int), c->stream);
+    if (e != cudaSuccess) return cuda_error(c, e, "tensor-core Hessian setup");
+
+    const double l2e_eps = LOG2E / c->prm.epsilon;
+    const double *o = c->origin;
+    double4 *tdat = reinterpret_cast<double4 *>(c->htc_tdat.p);
+    double4 *blk = reinterpret_cast<double4 *>(c->htc_blk.p);
+    float4 *qa = reinterpret_cast<float4 *>(c->htc_qa.p);
+    const int tgrid = (int)std::min<int64_t>((npad + 255) / 256, 148 * 8);
+    const int pgrid = (int)((nst * 32 + 255) / 256);
+    cudaEventRecord(c->ev0, c->stream);
+    if (c->dim == 2) {
+        k_htc_targets<2><<<tgrid, 256, 0, c->stream>>>(n, npad, c->y.p, c->nu.p, c->psi.p, c->grad.p, c->perm.p, o[0],
+                                                       o[1], o[2], l2e_eps, tdat, c->htc_diag.p);
+        k_htc_points<2><<<pgrid, 256, 0, c->stream>>>(c->nq, (int)nst, c->x.p, c->Lq.p, c->w.p, o[0], o[1], o[2],
+                                                      l2e_eps, qa, c->htc_qb.p, blk);
+    } else {
+        k_htc_targets<3><<<tgrid, 256, 0, c->stream>>>(n, npad, c->y.p, c->nu.p, c->psi.p, c->grad.p, c->perm.p, o[0],
+                                                       o[1], o[2], l2e_eps, tdat, c->htc_diag.p);
+        k_htc_points<3><<<pgrid, 256, 0, c->stream>>>(c->nq, (int)nst, c->x.p, c->Lq.p, c->w.p, o[0], o[1], o[2],
+                                                      l2e_eps, qa, c->htc_qb.p, blk);
+    }
+    Args a{};
+    a.qa = qa;
+    a.qb = c->htc_qb.p;
+    a.blk = blk;
+    a.tdat = tdat;
+    a.diag = c->htc_diag.p;
+    a.tiles = reinterpret_cast<const int2 *>(c->htc_tiles.p);
+    a.ntiles = (int)tiles.size();
+    a.nst = (int)nst;
+    a.ch = std::max(1, chunk_stages);
+    a.n = n;
+    a.l2e_eps = l2e_eps;
+    a.inv_eps = 1.0 / c->prm.epsilon;
+    a.scratch = c->htc_scr.p;
+    a.H = H_dev;
+    a.err = c->htc_err.p;
+    void (*kern)(const Args) = nullptr;
+    if (c->dim == 2) kern = out_f32 ? k_hessian_tc<2, float> : k_hessian_tc<2, double>;
+    else kern = out_f32 ? k_hessian_tc<3, float> : k_hessian_tc<3, double>;
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES);
+    if (e != cudaSuccess) return cuda_error(c, e, "tensor-core Hessian attribute");
+    if (c->profiling) cudaEventRecord(c->pev[0], c->stream);
+    kern<<<grid, THREADS, SMEM_BYTES, c->stream>>>(a);
+    if (c->profiling) cudaEventRecord(c->pev[1], c->stream);
+    cudaEventRecord(c->ev1, c->stream);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_error(c, e, "tensor-core Hessian launch");
+    int herr = 0;
+    e = cudaMemcpyAsync(&herr, c->htc_err.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_error(c, e, "tensor-core Hessian");
+    if (c->profiling) {
+        float kms = 0.f;
+        cudaEventElapsedTime(&kms, c->pev[0], c->pev[1]);
+        c->hess_kernel_ms = kms;
+    }
+    if (ms_out) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        *ms_out = ms;
+    }
+    c->hess_tiles = (int64_t)tiles.size();
+    if (herr) return set_error(c, SDOT_ETIMEOUT, "tensor-core Hessian: a bounded mbarrier wait expired");
+    return SDOT_OK;
+}
+
+}  // namespace sdot

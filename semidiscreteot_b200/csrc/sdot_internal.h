@@ -164,6 +164,14 @@ struct sdot_ctx {
 
     int64_t last_pairs = 0;
 
+    // ---- tensor-core Hessian (sdot_hessian_tc.cu) and Newton solver ----
+    sdot::DevBuf<double> htc_tdat, htc_diag, htc_blk, htc_scr;
+    sdot::DevBuf<float> htc_qa, htc_qb;
+    sdot::DevBuf<int> htc_tiles, htc_err;
+    double hess_kernel_ms = 0.0;
+    int64_t hess_tiles = 0;
+    int hess_chunk = 16;               // stages (x 64 points) per FP32 accumulation chunk
+
     // ---- measurement ----
     bool profiling = false;
     cudaEvent_t pev[8] = {};
@@ -203,6 +211,14 @@ struct EvalArgs;
 sdot_status run_trunc(sdot_ctx *c, const EvalArgs &a, double r);
 // dense-layout tpack for the current psi (used by the Hessian)
 void launch_target_prep_dense(sdot_ctx *c, const EvalArgs &a);
+
+// Tensor-core Hessian (BF16 hi+lo on tcgen05, FP64 drains) at the potential of
+// the last untruncated evaluation; H_dev n x n row-major in the caller's order.
+sdot_status hessian_tc(sdot_ctx *c, void *H_dev, bool out_f32, int chunk_stages, double *ms_out);
+// Evaluation at psi_dev (caller order) followed by the Hessian by `method`.
+sdot_status hessian_device(sdot_ctx *c, const double *psi_dev, void *H_dev, int method, int out_f32,
+                           sdot_hessian_info *info);
+sdot_status ensure_eval_buffers(sdot_ctx *c);
 
 // L-BFGS helpers (device vector kernels)
 void k_axpy_launch(cudaStream_t s, double *x, const double *x0, double a, const double *p, int64_t n);

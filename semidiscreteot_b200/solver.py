@@ -188,6 +188,23 @@ class SotSolver:
             hessian_out[...] = H
         return H
 
+    def compute_hessian_device(self, psi_ptr: int, hessian_ptr: int, method: str = "auto",
+                               out_f32: bool = False) -> dict:
+        """Hessian into device memory (n x n row-major, caller order) by
+        ``method`` "fp64" | "tensor" (tcgen05, BF16 hi+lo) | "auto" (see
+        sdot_hessian_device); returns the method used and device times."""
+        info = _lib.HessianInfo()
+        self._check(self._L.sdot_hessian_device(self._h, C.c_void_p(psi_ptr), C.c_void_p(hessian_ptr),
+                                                _lib.HESSIAN_METHOD[method], int(bool(out_f32)),
+                                                C.byref(info)))
+        names = {v: k for k, v in _lib.HESSIAN_METHOD.items()}
+        return {"method": names.get(info.method, info.method), "eval_ms": info.eval_ms,
+                "hessian_ms": info.hessian_ms, "kernel_ms": info.kernel_ms, "tiles": info.tiles}
+
+    def set_hessian_chunk(self, stages: int):
+        """Stages of 64 points accumulated in FP32 between FP64 drains (tensor Hessian)."""
+        self._check(self._L.sdot_set_hessian_chunk(self._h, int(stages)))
+
     def evaluate_partial_device(self, psi_ptr: int, out_ptr: int) -> dict:
         """Source-shard evaluation into out[n_targets + 3] on the device (see
         sdot_evaluate_partial_device); the caller all-reduces and finishes."""
