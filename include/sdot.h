@@ -181,6 +181,33 @@ sdot_status sdot_hessian_device(sdot_ctx *ctx, const double *psi_dev, void *H_de
  * each FP64 drain (default 16). */
 sdot_status sdot_set_hessian_chunk(sdot_ctx *ctx, int stages);
 
+/* Newton solver with the tensor-core Hessian.  The reference declares the
+ * Hessian (SotSolver::compute_hessian, SotSolver.h:343-344) but solves only
+ * with deal.II SolverBFGS (SotSolver::solve, SotSolver.cc:105-215); this is
+ * the second-order solve the Hessian is for, with solve()'s parameters,
+ * convergence control (l1norm / componentwise / linf) and in-place potential
+ * update.  Each iteration: FP64 evaluation; Hessian by hessian_method
+ * (sdot_hessian_method; the tensor Hessian is stored in FP32); H p = -g by
+ * Jacobi-preconditioned CG with FP64 vectors, the constant null vector
+ * projected out and the true residual recomputed in FP64 every 64 steps;
+ * Armijo backtracking on J in FP64.  Non-convergence within max_iterations is
+ * SDOT_OK with converged = 0, like sdot_solve.  n_targets <= 46340. */
+typedef struct {
+    unsigned iterations;        /* Newton steps taken */
+    int converged;
+    int64_t n_evaluations;      /* functional evaluations (line search included) */
+    int64_t cg_iterations;      /* CG iterations over all steps */
+    double last_value;
+    double last_check_value;
+    int64_t total_pairs;
+    double eval_ms;             /* device time in evaluations */
+    double hessian_ms;          /* device time in Hessians */
+    double cg_ms;               /* device time in CG */
+    int hessian_method;         /* method of the last Hessian */
+} sdot_newton_info;
+sdot_status sdot_solve_newton(sdot_ctx *ctx, double *psi, const sdot_solver_params *params, int hessian_method,
+                              sdot_newton_info *info);
+
 /* Getters replacing SotSolver::get_last_functional_value, get_last_iteration_count,
  * get_convergence_status, get_last_distance_threshold, get_C_global
  * (SotSolver.h:233-255) and the setter set_distance_threshold (:261). */

@@ -33,6 +33,7 @@ EXPORTED = [
     "sdot_compute_geometric_radius_bound", "sdot_set_distance_function", "sdot_evaluate_partial_device",
     "sdot_set_state", "sdot_get_stream", "sdot_set_profiling", "sdot_get_kernel_times", "sdot_measure_peaks",
     "sdot_evaluate_device_noalloc", "sdot_hessian_device", "sdot_set_hessian_chunk",
+    "sdot_solve_newton",
 ]
 
 NOALLOC_SCRATCH_BYTES = 8 << 20  # SDOT_NOALLOC_SCRATCH_BYTES
@@ -63,6 +64,13 @@ class SolveInfo(C.Structure):
 class HessianInfo(C.Structure):
     _fields_ = [("method", C.c_int), ("eval_ms", C.c_double), ("hessian_ms", C.c_double),
                 ("kernel_ms", C.c_double), ("tiles", C.c_int64)]
+
+
+class NewtonInfo(C.Structure):
+    _fields_ = [("iterations", C.c_uint), ("converged", C.c_int), ("n_evaluations", C.c_int64),
+                ("cg_iterations", C.c_int64), ("last_value", C.c_double), ("last_check_value", C.c_double),
+                ("total_pairs", C.c_int64), ("eval_ms", C.c_double), ("hessian_ms", C.c_double),
+                ("cg_ms", C.c_double), ("hessian_method", C.c_int)]
 
 
 _lib = None
@@ -119,6 +127,8 @@ def load():
     lib.sdot_hessian_device.restype = ip
     lib.sdot_set_hessian_chunk.argtypes = [vp, ip]
     lib.sdot_set_hessian_chunk.restype = ip
+    lib.sdot_solve_newton.argtypes = [vp, vp, C.POINTER(SolverParams), ip, C.POINTER(NewtonInfo)]
+    lib.sdot_solve_newton.restype = ip
     for fn in ("sdot_evaluate_partial_device", "sdot_set_state", "sdot_set_profiling", "sdot_get_kernel_times",
                "sdot_measure_peaks"):
         getattr(lib, fn).restype = ip

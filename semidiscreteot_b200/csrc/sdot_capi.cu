@@ -1192,3 +1192,7 @@ sdot_status sdot_set_distance_threshold(sdot_ctx *c, double threshold)
 }
 
 }  // extern "C"
+
+namespace sdot {
+int solver_control_check(sdot_ctx *c, unsigned step, double *value) { return control_check(c, step, value); }
+}  // namespace sdot

@@ -130,7 +130,7 @@ __global__ void k_permute_matrix(const double *__restrict__ Hi, double *__restri
 
 // FP64 Hessian at the potential of the last evaluation into H_dev (device,
 // n x n row-major, caller order).
-static sdot_status hessian_fp64_to(sdot_ctx *c, double *H_dev)
+sdot_status hessian_fp64_to(sdot_ctx *c, double *H_dev)
 {
     const int64_t n = c->nt;
     if (n > 46340) return set_error(c, SDOT_EBUDGET, "dense Hessian limited to n_targets <= 46340");
@@ -192,6 +192,8 @@ static bool tensor_ok(const sdot_ctx *c)
     const bool dense = std::isinf(r) || !(r < c->diam * (1.0 + 1e-12));
     return dense && !std::isnan(r) && c->w_nonneg;
 }
+
+bool hessian_tensor_ok(const sdot_ctx *c) { return tensor_ok(c); }
 
 sdot_status hessian_device(sdot_ctx *c, const double *psi_dev, void *H_dev, int method, int out_f32,
                            sdot_hessian_info *info)

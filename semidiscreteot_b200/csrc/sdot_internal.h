@@ -171,6 +171,9 @@ struct sdot_ctx {
     double hess_kernel_ms = 0.0;
     int64_t hess_tiles = 0;
     int hess_chunk = 16;               // stages (x 64 points) per FP32 accumulation chunk
+    sdot::DevBuf<float> nt_H32;        // Newton: tensor-core Hessian (caller order)
+    sdot::DevBuf<double> nt_H64;       // Newton: FP64 Hessian when the tensor method does not apply
+    sdot::DevBuf<double> nt_vec;       // Newton/CG vectors (caller order)
 
     // ---- measurement ----
     bool profiling = false;
@@ -219,6 +222,9 @@ sdot_status hessian_tc(sdot_ctx *c, void *H_dev, bool out_f32, int chunk_stages,
 sdot_status hessian_device(sdot_ctx *c, const double *psi_dev, void *H_dev, int method, int out_f32,
                            sdot_hessian_info *info);
 sdot_status ensure_eval_buffers(sdot_ctx *c);
+// VerboseSolverControl::check on the last evaluation's scalars: 1 converged,
+// 0 iterate, -1 failure (max_iterations reached or NaN).
+int solver_control_check(sdot_ctx *c, unsigned step, double *value);
 
 // L-BFGS helpers (device vector kernels)
 void k_axpy_launch(cudaStream_t s, double *x, const double *x0, double a, const double *p, int64_t n);

@@ -177,6 +177,31 @@ class SotSolver:
             potential[...] = psi
         return psi
 
+    def solve_newton(self, potential: np.ndarray, params: Optional[SolverParameters] = None,
+                     hessian: str = "auto") -> np.ndarray:
+        """Newton solve with the tensor-core Hessian (sdot_solve_newton): same
+        parameters, convergence control and in-place update as ``solve``."""
+        psi = _f64(potential).copy()
+        if psi.size != self._n_targets:
+            raise ValueError("potential size does not match the number of targets")
+        if params is not None:
+            self.current_params = params
+        cp = self._cparams(self.current_params)
+        info = _lib.NewtonInfo()
+        st = self._L.sdot_solve_newton(self._h, psi.ctypes.data, C.byref(cp), _lib.HESSIAN_METHOD[hessian],
+                                       C.byref(info))
+        names = {v: k for k, v in _lib.HESSIAN_METHOD.items()}
+        self.last_solve_info = {"iterations": info.iterations, "converged": bool(info.converged),
+                                "n_evaluations": info.n_evaluations, "cg_iterations": info.cg_iterations,
+                                "last_value": info.last_value, "last_check_value": info.last_check_value,
+                                "total_pairs": info.total_pairs, "eval_ms": info.eval_ms,
+                                "hessian_ms": info.hessian_ms, "cg_ms": info.cg_ms,
+                                "hessian_method": names.get(info.hessian_method, info.hessian_method)}
+        self._check(st)
+        if isinstance(potential, np.ndarray) and potential is not psi and potential.size == psi.size:
+            potential[...] = psi
+        return psi
+
     def compute_hessian(self, potential, hessian_out: Optional[np.ndarray] = None) -> np.ndarray:
         """Dense Hessian H = (1/eps) sum_q w_q (diag(pi_q) - pi_q pi_q^T) (declared at SotSolver.h:343-344)."""
         psi = _f64(potential)
