@@ -64,10 +64,12 @@ static_assert(THREADS == ROWS + 2 * KQ, "one staging item per thread");
 constexpr uint32_t A_BYTES = M * KQ * 2;                 // 16 KB
 constexpr uint32_t B_BYTES = N * KQ * 2;                 // 32 KB
 constexpr uint32_t STAGE_BYTES = 2 * (A_BYTES + B_BYTES); // Ahi, Alo, Bhi, Blo
-constexpr uint32_t OFF_EG = 2 * STAGE_BYTES;             // float4 [2][ROWS]
-constexpr uint32_t OFF_QA = OFF_EG + 2 * ROWS * 16;      // float4 [2][KQ]
-constexpr uint32_t OFF_QB = OFF_QA + 2 * KQ * 16;        // float  [2][KQ]
-constexpr uint32_t OFF_BAR = OFF_QB + 2 * KQ * 4;        // 4 mbarriers + TMEM address
+constexpr uint32_t OFF_EG = 2 * STAGE_BYTES;             // float [2][ROWS][8]: E,E,Gx,Gx,Gy,Gy,Gz,Gz
+constexpr int QS_STRIDE = 44;                            // floats per K-chunk: dx[8] dy[8] dz[8] fb[8] fa[8] + pad
+constexpr uint32_t OFF_QS = OFF_EG + 2 * ROWS * 32;      // float [2][8][QS_STRIDE]
+constexpr uint32_t OFF_RAW = OFF_QS + 2 * 8 * QS_STRIDE * 4;  // per-stage inputs as loaded, 2 buffers:
+constexpr uint32_t RAW_BYTES = 32 + KQ * 16 + KQ * 4;    //   block {c_b, L_b}, points {d, F^B}, points F^A
+constexpr uint32_t OFF_BAR = OFF_RAW + 2 * RAW_BYTES;    // 4 mbarriers + TMEM address
 constexpr uint32_t SMEM_BYTES = OFF_BAR + 64 + 1024;     // + alignment slack
 constexpr int TMEM_COLS = 2 * N;                          // two FP32 accumulators
 constexpr int SCR_PER_CTA = M * N;                        // FP64 drain scratch per CTA
@@ -136,6 +138,46 @@ __device__ __forceinline__ void umma_commit(uint32_t bar)
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// Packed FP32 pairs (sm_100 f32x2 arithmetic).
+typedef unsigned long long f2;
+__device__ __forceinline__ f2 pack2(float a, float b)
+{
+    f2 r;
+    asm("mov.b64 %0, {%1,%2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ void unpack2(f2 v, float &a, float &b) { asm("mov.b64 {%0,%1}, %2;" : "=f"(a), "=f"(b) : "l"(v)); }
+__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c)
+{
+    f2 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ f2 add2(f2 a, f2 b)
+{
+    f2 d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2 sub2(f2 a, f2 b)
+{
+    f2 d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2 mul2(f2 a, f2 b)
+{
+    f2 d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
 
 // 32 lanes x 16 consecutive 32-bit columns; the wait is in the same asm so the
 // registers are never read before the load has landed.
@@ -179,9 +221,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
     const uint32_t raw_s = smem_u32(smem_raw);
     uint8_t *sm = smem_raw + ((1024u - (raw_s & 1023u)) & 1023u);  // 1024-aligned shared address
     const uint32_t sm_s = smem_u32(sm);
-    float4 *Eg = reinterpret_cast<float4 *>(sm + OFF_EG);
-    float4 *qA = reinterpret_cast<float4 *>(sm + OFF_QA);
-    float *qB = reinterpret_cast<float *>(sm + OFF_QB);
+    float *Eg = reinterpret_cast<float *>(sm + OFF_EG);
+    float *qs = reinterpret_cast<float *>(sm + OFF_QS);
     const uint32_t bar0 = sm_s + OFF_BAR;  // [0,1] stage buffers, [2,3] accumulators (8 bytes each)
     uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + OFF_BAR + 32);
 
@@ -201,76 +242,105 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
     tc_fence_after();
     const uint32_t tmem = *tslot;
 
-    // ---- staging of one stage's per-target and per-point data (one item per thread) ----
-    double4 pt = make_double4(0, 0, 0, 0), pb = make_double4(0, 0, 0, 0);
-    float4 pq = make_float4(0, 0, 0, 0);
-    float pqb = 0.f;
-    auto stage_load = [&](int t, int st) {
-        const int2 tl = a.tiles[t];
+    // ---- staging of the per-stage inputs ----
+    // The block and point data of stage g + 2 are copied by cp.async into
+    // raw[g % 2] while stage g is generated; at the end of stage g every
+    // thread turns one item of raw[(g + 1) % 2] (and its target row, held in
+    // registers for the whole tile) into the FP32 operands of stage g + 1.
+    uint8_t *raw = sm + OFF_RAW;
+    const uint32_t rawb_s = sm_s + OFF_RAW;
+    double4 pt = make_double4(0, 0, 0, 0);   // target row tid (tid < ROWS) of the current tile
+    auto load_target = [&](int2 tl) {
         if (tid < ROWS) {
             const int64_t j = tid < M ? (int64_t)tl.x * M + tid : (int64_t)tl.y * N + (tid - M);
             pt = a.tdat[j];
-            pb = a.blk[st];
-        } else if (tid < ROWS + KQ) {
-            pq = a.qa[(int64_t)st * KQ + (tid - ROWS)];
-        } else {
-            pqb = a.qb[(int64_t)st * KQ + (tid - ROWS - KQ)];
         }
     };
-    auto stage_store = [&](int buf) {
+    auto raw_copy = [&](int buf, int st) {   // 2 + 64 + 16 copies of 16 bytes
+        const uint32_t d = rawb_s + buf * RAW_BYTES;
+        if (tid < 2) cp_async16(d + tid * 16, reinterpret_cast<const uint8_t *>(a.blk + st) + tid * 16);
+        else if (tid < 2 + KQ) cp_async16(d + 32 + (tid - 2) * 16, a.qa + (int64_t)st * KQ + (tid - 2));
+        else if (tid < 2 + KQ + KQ / 4) cp_async16(d + 32 + KQ * 16 + (tid - 2 - KQ) * 16, a.qb + (int64_t)st * KQ + (tid - 2 - KQ) * 4);
+        cp_async_commit();
+    };
+    auto stage_store = [&](int buf) {         // raw[buf] + pt -> Eg / qs [buf]
+        const uint8_t *rb = raw + buf * RAW_BYTES;
         if (tid < ROWS) {
+            const double4 pb = *reinterpret_cast<const double4 *>(rb);
             const double dx = pt.x - pb.x, dy = pt.y - pb.y, dz = DIM == 3 ? pt.z - pb.z : 0.0;
-            const double e = pt.w - 0.5 * a.l2e_eps * (dx * dx + dy * dy + dz * dz) - pb.w;
-            Eg[buf * ROWS + tid] = make_float4((float)e, (float)(a.l2e_eps * dx), (float)(a.l2e_eps * dy),
-                                               (float)(a.l2e_eps * dz));
+            const float e = (float)(pt.w - 0.5 * a.l2e_eps * (dx * dx + dy * dy + dz * dz) - pb.w);
+            const float gx = (float)(a.l2e_eps * dx), gy = (float)(a.l2e_eps * dy), gz = (float)(a.l2e_eps * dz);
+            float4 *dst = reinterpret_cast<float4 *>(Eg + (buf * ROWS + tid) * 8);
+            dst[0] = make_float4(e, e, gx, gx);
+            dst[1] = make_float4(gy, gy, gz, gz);
         } else if (tid < ROWS + KQ) {
-            const int p = tid - ROWS;
-            qA[buf * KQ + (p & 7) * 8 + (p >> 3)] = pq;   // transposed: [i][kc] for q = kc * 8 + i
+            const int p = tid - ROWS;            // point p of the stage: K-chunk p >> 3, slot p & 7
+            const float4 pq = reinterpret_cast<const float4 *>(rb + 32)[p];
+            float *d = qs + (buf * 8 + (p >> 3)) * QS_STRIDE + (p & 7);
+            d[0] = pq.x;
+            d[8] = pq.y;
+            d[16] = pq.z;
+            d[24] = pq.w;
         } else {
             const int p = tid - ROWS - KQ;
-            qB[buf * KQ + (p & 7) * 8 + (p >> 3)] = pqb;
+            qs[(buf * 8 + (p >> 3)) * QS_STRIDE + 32 + (p & 7)] = reinterpret_cast<const float *>(rb + 32 + KQ * 16)[p];
         }
     };
 
     // ---- generation of one stage's operands into shared memory ----
+    // Per element: log2(w pi) = E + F + G.d in packed FP32 pairs, one ex2,
+    // then v = hi + lo with hi rounded to BF16 and lo = v - hi (exact),
+    // truncated to BF16 when packed.
     const int kc = lane & 7;                 // 16-byte chunk (8 points) of the 64-point stage
     const int rg = warp * 4 + (lane >> 3);   // row group
     auto generate = [&](int buf) {
-        float dx[8], dy[8], dz[8], fa[8], fb[8];
+        const float4 *qv = reinterpret_cast<const float4 *>(qs + (buf * 8 + kc) * QS_STRIDE);
+        f2 dx[4], dy[4], dz[4], fa[4], fb[4];
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const float4 t = qA[buf * KQ + i * 8 + kc];
-            dx[i] = t.x;
-            dy[i] = t.y;
-            dz[i] = t.z;
-            fb[i] = t.w;
-            fa[i] = qB[buf * KQ + i * 8 + kc];
+        for (int h = 0; h < 2; ++h) {
+            const float4 x4 = qv[0 + h], y4 = qv[2 + h], b4 = qv[6 + h], a4 = qv[8 + h];
+            dx[2 * h] = pack2(x4.x, x4.y);
+            dx[2 * h + 1] = pack2(x4.z, x4.w);
+            dy[2 * h] = pack2(y4.x, y4.y);
+            dy[2 * h + 1] = pack2(y4.z, y4.w);
+            fb[2 * h] = pack2(b4.x, b4.y);
+            fb[2 * h + 1] = pack2(b4.z, b4.w);
+            fa[2 * h] = pack2(a4.x, a4.y);
+            fa[2 * h + 1] = pack2(a4.z, a4.w);
+            if (DIM == 3) {
+                const float4 z4 = qv[4 + h];
+                dz[2 * h] = pack2(z4.x, z4.y);
+                dz[2 * h + 1] = pack2(z4.z, z4.w);
+            }
         }
         uint8_t *stage = sm + buf * STAGE_BYTES;
 #pragma unroll
         for (int it = 0; it < RPT; ++it) {
             const bool isA = it < ARPT;
             const int r = rg + RG * it;
-            const float4 e = Eg[buf * ROWS + r];
+            const float4 *eg = reinterpret_cast<const float4 *>(Eg + (buf * ROWS + r) * 8);
+            const float4 e0 = eg[0], e1 = eg[1];
+            const f2 E = pack2(e0.x, e0.y), Gx = pack2(e0.z, e0.w), Gy = pack2(e1.x, e1.y), Gz = pack2(e1.z, e1.w);
             uint32_t hw[4], lw[4];
 #pragma unroll
-            for (int k = 0; k < 8; k += 2) {
-                float u0 = e.x + (isA ? fa[k] : fb[k]);
-                float u1 = e.x + (isA ? fa[k + 1] : fb[k + 1]);
-                u0 = fmaf(e.y, dx[k], u0);
-                u1 = fmaf(e.y, dx[k + 1], u1);
-                u0 = fmaf(e.z, dy[k], u0);
-                u1 = fmaf(e.z, dy[k + 1], u1);
-                if (DIM == 3) {
-                    u0 = fmaf(e.w, dz[k], u0);
-                    u1 = fmaf(e.w, dz[k + 1], u1);
-                }
+            for (int k = 0; k < 4; ++k) {
+                f2 u = add2(E, isA ? fa[k] : fb[k]);
+                u = fma2(Gx, dx[k], u);
+                u = fma2(Gy, dy[k], u);
+                if (DIM == 3) u = fma2(Gz, dz[k], u);
+                float u0, u1;
+                unpack2(u, u0, u1);
                 const float v0 = ex2_approx(u0), v1 = ex2_approx(u1);
-                const uint32_t h0 = (__float_as_uint(v0) + 0x8000u) & 0xffff0000u;
-                const uint32_t h1 = (__float_as_uint(v1) + 0x8000u) & 0xffff0000u;
-                const float l0 = v0 - __uint_as_float(h0), l1 = v1 - __uint_as_float(h1);
-                hw[k >> 1] = __byte_perm(h0, h1, 0x7632);
-                lw[k >> 1] = __byte_perm(__float_as_uint(l0), __float_as_uint(l1), 0x7632);
+                // hi: round to 8 significant bits in the integer domain (an
+                // arithmetic split such as Veltkamp's c - (c - v) may be folded
+                // to v by the compiler); lo = v - hi is exact
+                const uint32_t hb0 = (__float_as_uint(v0) + 0x8000u) & 0xffff0000u;
+                const uint32_t hb1 = (__float_as_uint(v1) + 0x8000u) & 0xffff0000u;
+                const f2 lo = sub2(pack2(v0, v1), pack2(__uint_as_float(hb0), __uint_as_float(hb1)));
+                float l0, l1;
+                unpack2(lo, l0, l1);
+                hw[k] = __byte_perm(hb0, hb1, 0x7632);
+                lw[k] = __byte_perm(__float_as_uint(l0), __float_as_uint(l1), 0x7632);
             }
             const int rr = isA ? r : r - M;
             const uint32_t off = (uint32_t)(rr >> 3) * 1024u + (uint32_t)(rr & 7) * 128u + ((uint32_t)(kc ^ (rr & 7)) << 4);
@@ -285,10 +355,9 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
     const int quad = warp & 3, cq = warp >> 2;   // TMEM lane quadrant, 64-column quarter
     const int row = quad * 32 + lane;
     double *scr = a.scratch + (size_t)blockIdx.x * SCR_PER_CTA;
-    auto drain = [&](unsigned pc, int tile, bool first, bool last) -> bool {
+    auto drain = [&](unsigned pc, int2 tl, bool first, bool last) -> bool {
         const bool ok = mbar_wait(bar0 + 8 * (2 + (pc & 1)), (pc >> 1) & 1);
         tc_fence_after();
-        const int2 tl = a.tiles[tile];
         const int64_t ga = (int64_t)tl.x * M + row;
         const uint32_t taddr = tmem + (pc & 1) * N + cq * 64 + ((uint32_t)(quad * 32) << 16);
 #pragma unroll 1
@@ -320,15 +389,22 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
 
     int g = 0;               // global stage counter (stage-buffer phases)
     unsigned chunk = 0;      // global chunk counter (accumulator phases)
-    int pend = -1, pend_tile = 0;
+    int pend = -1;
+    int2 pend_tl = make_int2(0, 0);
     bool pend_first = false, pend_last = false;
     bool bad = false;        // this thread saw a wait expire
     bool aborted = false;
     int last_g = -1;
 
     if ((int)blockIdx.x < a.ntiles) {
-        stage_load(blockIdx.x, 0);
+        // stage 0 into Eg/qs[0]; stage 1's inputs into raw[1]
+        load_target(a.tiles[blockIdx.x]);
+        raw_copy(0, 0);
+        cp_async_wait_all();
+        __syncthreads();
         stage_store(0);
+        raw_copy(1, a.nst > 1 ? 1 : 0);
+        cp_async_wait_all();
     }
     __syncthreads();
 
@@ -336,16 +412,22 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
     // the MMA thread and orders the previous drain's TMEM reads before any MMA
     // that reuses that accumulator.
     for (int t = blockIdx.x; t < a.ntiles && !aborted; t += gridDim.x) {
+        // tile coordinates of this and the next tile, loaded once per tile
+        const int2 tl_cur = a.tiles[t];
+        const int2 tl_nxt = t + (int)gridDim.x < a.ntiles ? a.tiles[t + gridDim.x] : tl_cur;
         for (int st = 0; st < a.nst; ++st, ++g) {
             const int sb = g & 1;
-            int tn = t, sn = st + 1;
-            if (sn == a.nst) { tn = t + gridDim.x; sn = 0; }
-            const bool has_next = tn < a.ntiles;
-            if (has_next) stage_load(tn, sn);
+            const bool last_of_tile = st + 1 == a.nst;
+            const bool has_next = !last_of_tile || t + (int)gridDim.x < a.ntiles;
+            raw_copy(sb, (st + 2) % a.nst);     // inputs of stage g + 2 (its point block)
             // the MMAs that read this buffer two stages ago must be complete
             if (g >= 2 && !mbar_wait(bar0 + 8 * sb, ((g >> 1) - 1) & 1)) bad = true;
             generate(sb);
-            if (has_next) stage_store(sb ^ 1);
+            if (has_next) {
+                if (last_of_tile) load_target(tl_nxt);   // once per tile
+                stage_store(sb ^ 1);
+            }
+            cp_async_wait_all();
             fence_async_smem();
             if (__syncthreads_or(bad)) { aborted = true; break; }
             const bool first_in_chunk = (st % a.ch) == 0;
@@ -370,12 +452,12 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
             last_g = g;
             // drain the previous chunk while the tensor core works on this one
             if (first_in_chunk && pend >= 0) {
-                if (!drain((unsigned)pend, pend_tile, pend_first, pend_last)) bad = true;
+                if (!drain((unsigned)pend, pend_tl, pend_first, pend_last)) bad = true;
                 pend = -1;
             }
             if (last_in_chunk) {
                 pend = (int)chunk;
-                pend_tile = t;
+                pend_tl = tl_cur;
                 pend_first = st < a.ch;
                 pend_last = st == a.nst - 1;
                 ++chunk;
@@ -383,7 +465,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
         }
     }
     if (!aborted && pend >= 0) {
-        if (!drain((unsigned)pend, pend_tile, pend_first, pend_last)) bad = true;
+        if (!drain((unsigned)pend, pend_tl, pend_first, pend_last)) bad = true;
     }
     if (__syncthreads_or(bad)) aborted = true;
     if (aborted && tid == 0) {
