@@ -52,7 +52,13 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="trunc_3d", choices=["trunc_3d", "dense_2d", "newton_3d"])
+    ap.add_argument("--workload", default="trunc_3d",
+                    choices=["trunc_3d", "dense_2d", "newton_3d", "hessian_3d", "batched_2d", "serve_3d"])
+    ap.add_argument("--problems", type=int, default=256, help="batched_2d: problems; serve_3d: requests")
+    ap.add_argument("--rate", type=float, default=2.0, help="serve_3d: Poisson arrival rate (requests/s)")
+    ap.add_argument("--slots", type=int, default=4, help="batched_2d / serve_3d: concurrent solve slots")
+    ap.add_argument("--baseline-seconds", type=float, default=60.0,
+                    help="solve workloads: wall budget of the one-at-a-time FP64 L-BFGS baseline")
     ap.add_argument("--precision", default="hybrid", choices=["hybrid", "fp64", "mixed"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -375,10 +381,216 @@ def run_ours(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# solve-level workloads (the Newton / batched / served configurations)
+# ---------------------------------------------------------------------------
+
+def _fp64_lbfgs_baseline(problems, seconds):
+    """One-at-a-time plain FP64 GPU solves (sdot_solve, L-BFGS, no epsilon
+    scaling) on the problems in order until the wall budget is spent."""
+    from semidiscreteot_b200 import SotSolver
+    t_all, done, conv, iters = 0.0, 0, 0, []
+    for p in problems:
+        if t_all >= seconds:
+            break
+        src = p["source"]
+        s = SotSolver(dim=p["y"].shape[1], device=0, precision="fp64")
+        s.setup_source_measure(src)
+        s.setup_target(p["y"], p["nu"])
+        t0 = time.perf_counter()
+        try:
+            s.solve(np.zeros(len(p["nu"])), p["params"])
+            ok = bool(s.get_convergence_status())
+        except RuntimeError:
+            ok = False
+        t_all += time.perf_counter() - t0
+        iters.append(int(s.get_last_iteration_count()))
+        done += 1
+        conv += ok
+        s.close()
+    return {"solves_per_s": conv / t_all if t_all > 0 else 0.0, "attempted": done, "converged": conv,
+            "seconds": t_all, "iterations": iters,
+            "method": "sdot_solve (L-BFGS, FP64 sweeps), one problem at a time, psi0 = 0, no epsilon scaling"}
+
+
+def run_hessian_3d(args):
+    """Config 3: tensor-core Hessian (roofline) and the Newton solve to gradient
+    linf 1e-8, against the FP64 L-BFGS solve of the same problem."""
+    import torch
+    from semidiscreteot_b200 import SotSolver
+    wl = make_workload("newton_3d", args.scale)
+    src, y, nu, prm = wl["source"], wl["y"], wl["nu"], wl["params"]
+    N, Q = y.shape[0], src["jxw"].size
+    s = SotSolver(dim=3, device=0, precision="fp64")
+    s.setup_source_measure(src)
+    s.setup_target(y, nu)
+    s.configure(prm)
+    s.set_profiling(True)
+    psi = torch.tensor(0.2 * prm.epsilon * np.random.default_rng(0).standard_normal(N), dtype=torch.float64,
+                       device="cuda")
+    H = torch.empty((N, N), dtype=torch.float32, device="cuda")
+    for _ in range(max(3, args.warmup)):
+        s.compute_hessian_device(psi.data_ptr(), H.data_ptr(), method="tensor", out_f32=True)
+    with ClockSampler(0) as clk:
+        ks = []
+        for _ in range(args.steps):
+            info = s.compute_hessian_device(psi.data_ptr(), H.data_ptr(), method="tensor", out_f32=True)
+            ks.append(info["kernel_ms"])
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        psi_n = s.solve_newton(np.zeros(N), prm, hessian="tensor")
+        t_newton = time.perf_counter() - t0
+        ninfo = dict(s.last_solve_info)
+    conv = s.get_convergence_status()
+    g = np.zeros(N)
+    s.evaluate_functional(psi_n, g)   # FP64 sweeps
+    ninfo["final_grad_linf_fp64"] = float(np.max(np.abs(g)))
+    s.close()
+    kms = float(np.mean(ks))
+    flops = 3.0 * Q * N * N  # three BF16 products x 2 Q N^2 / 2 (upper triangle)
+    ach = flops / (kms * 1e-3) / 1e12
+    peak = _measured_peaks().get("bf16_tflops")
+    import dataclasses
+    prm_b = dataclasses.replace(prm, max_iterations=int(args.baseline_seconds * 20))  # ~50 ms per iteration
+    base = _fp64_lbfgs_baseline([{"source": src, "y": y, "nu": nu, "params": prm_b}], args.baseline_seconds)
+    line = {"metric": "Newton solves/s at grad linf 1e-8", "value": (1.0 / t_newton) if conv else 0.0,
+            "unit": "solves/s", "n_gpus": 1, "steps": args.steps, "warmup": max(3, args.warmup),
+            "ms_per_step": 1000 * t_newton, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16 hi+lo tensor-core Hessian (fp32 accumulation, fp64 drains), fp64 value/gradient/CG/line search",
+            "data": "synthetic (seeded; no published dataset)",
+            "config": {"workload": "hessian_3d", "n_quadrature": int(Q), "n_targets": int(N), "epsilon": prm.epsilon,
+                       "tau": 0.0, "tolerance": prm.tolerance},
+            "newton": ninfo, "converged": bool(conv),
+            "roofline": {"kernel": "k_hessian_tc (tcgen05 BF16 hi+lo, TMEM accumulators)", "bound": "tensor",
+                         "achieved": ach, "peak": peak, "unit": "TFLOP/s",
+                         "frac": (ach / peak) if peak else None, "traffic": None, "ms_per_launch": kms,
+                         "flops_per_launch": flops, "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)"},
+            "fp64_lbfgs_baseline": base, "clocks": clk.summary()}
+    print(json.dumps(line))
+    return 0
+
+
+def _measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+
+
+def _solve_requests_through_server(problems, slots, rate, seed):
+    from semidiscreteot_b200 import SolveServer
+    rng = np.random.default_rng(seed)
+    srv = SolveServer(n_slots=slots)
+    tickets = []
+    t0 = time.perf_counter()
+    next_t = t0
+    for p in problems:
+        if rate > 0:
+            next_t += rng.exponential(1.0 / rate)
+            while time.perf_counter() < next_t:
+                time.sleep(min(0.005, max(0.0, next_t - time.perf_counter())))
+        tickets.append(srv.submit(p["source"], p["y"], p["nu"], p["params"], method=p.get("method", "auto"),
+                                  precision="fp64", epsilon_scaling_factor=p.get("eps_factor", 10.0),
+                                  epsilon_scaling_steps=p.get("eps_steps", 1),
+                                  intermediate_tolerance=p.get("inter_tol", 0.0)))
+    res = [srv.wait(t, raise_on_error=False)[1] for t in tickets]
+    wall = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    return res, wall, st
+
+
+def run_batched_2d(args):
+    """Config 4: the batched problems solved through the solve service (Newton
+    with the tensor-core Hessian, epsilon scaling, all submitted at once),
+    against one-at-a-time plain FP64 L-BFGS solves."""
+    from semidiscreteot_b200 import workloads as W
+    probs = W.batched_2d(seed=0, n_problems=args.problems)
+    for p in probs:
+        p.update(method="newton", eps_factor=10.0, eps_steps=2, inter_tol=1e-6)
+    with ClockSampler(0) as clk:
+        res, wall, st = _solve_requests_through_server(probs, args.slots, 0.0, 0)
+    conv = sum(r["converged"] for r in res)
+    base = _fp64_lbfgs_baseline(probs, args.baseline_seconds)
+    line = {"metric": "batched solves/s at grad linf 1e-8", "value": conv / wall, "unit": "solves/s", "n_gpus": 1,
+            "steps": 1, "warmup": 0, "ms_per_step": 1000 * wall, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "bf16 hi+lo tensor-core Hessian, fp64 value/gradient/CG/line search",
+            "data": "synthetic (seeded; no published dataset)",
+            "config": {"workload": "batched_2d", "problems": len(probs), "slots": args.slots,
+                       "method": "Newton (tensor-core Hessian), epsilon scaling 2 levels x10, all submitted at once"},
+            "converged": conv, "latency_p50_ms": st["p50_ms"], "latency_p99_ms": st["p99_ms"],
+            "peak_concurrent": st["peak_running"], "iterations": [r["iterations"] for r in res],
+            "fp64_lbfgs_baseline": base,
+            "speedup_vs_fp64_lbfgs": (conv / wall) / base["solves_per_s"] if base["solves_per_s"] > 0 else None,
+            "clocks": clk.summary()}
+    print(json.dumps(line))
+    return 0
+
+
+def serve_requests(n, seed=0, scale=1.0):
+    """Config 5's request mix: 80% config-3-like (uniform density cube, uniform
+    targets, eps 5e-3), 20% 3D cubes with Gaussian-mixture targets and eps in
+    [1e-3, 1e-2]; sizes scaled by `scale` (cells per axis and targets)."""
+    from semidiscreteot_b200 import SolverParameters, structured_source
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        if rng.random() < 0.8:
+            cells = max(4, int(round(32 * scale)))
+            nt = max(64, int(20_000 * scale ** 3))
+            src = structured_source(3, cells, 2)
+            y = rng.random((nt, 3))
+            nu = np.full(nt, 1.0 / nt)
+            eps = 5e-3
+        else:
+            cells = max(4, int(round(np.exp(rng.uniform(np.log(16), np.log(64))) * scale)))
+            nt = max(64, int(np.exp(rng.uniform(np.log(5_000), np.log(50_000))) * scale ** 3))
+            src = structured_source(3, cells, 2)
+            k = 5
+            means = rng.uniform(0.2, 0.8, (k, 3))
+            comp = rng.integers(0, k, nt)
+            y = np.clip(means[comp] + 0.1 * rng.standard_normal((nt, 3)), 0, 1)
+            nu = rng.dirichlet(np.ones(nt))
+            eps = float(np.exp(rng.uniform(np.log(1e-3), np.log(1e-2))))
+        prm = SolverParameters(epsilon=eps, tau=0.0, use_log_sum_exp_trick=True, tolerance=1e-8,
+                               solver_control_type="linf", max_iterations=2000)
+        out.append({"source": src, "y": y, "nu": nu, "params": prm, "method": "auto",
+                    "eps_factor": 4.0, "eps_steps": 2 if eps < 5e-3 else 1, "inter_tol": 1e-6})
+    return out
+
+
+def run_serve_3d(args):
+    """Config 5: Poisson arrivals into the solve service; solves/s and p50/p99
+    latency at gradient tolerance 1e-8."""
+    reqs = serve_requests(args.problems, 0, args.scale)
+    with ClockSampler(0) as clk:
+        res, wall, st = _solve_requests_through_server(reqs, args.slots, args.rate, 1)
+    conv = sum(r["converged"] for r in res)
+    line = {"metric": "served solves/s at grad linf 1e-8 (p50/p99 latency)", "value": conv / wall,
+            "unit": "solves/s", "n_gpus": 1, "steps": 1, "warmup": 0, "ms_per_step": 1000 * wall,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16 hi+lo tensor-core Hessian, fp64 value/gradient/CG/line search",
+            "data": "synthetic (seeded; no published dataset)",
+            "config": {"workload": "serve_3d", "requests": len(reqs), "rate_per_s": args.rate, "slots": args.slots,
+                       "scale": args.scale},
+            "converged": conv, "latency_p50_ms": st["p50_ms"], "latency_p99_ms": st["p99_ms"],
+            "latency_mean_ms": st["mean_ms"], "peak_concurrent": st["peak_running"],
+            "methods": [r["method"] for r in res], "clocks": clk.summary()}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "hessian_3d":
+        return run_hessian_3d(args)
+    if args.workload == "batched_2d":
+        return run_batched_2d(args)
+    if args.workload == "serve_3d":
+        return run_serve_3d(args)
     return run_ours(args)
 
 

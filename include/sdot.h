@@ -89,6 +89,7 @@ typedef struct {
 } sdot_solve_info;
 
 typedef struct sdot_ctx sdot_ctx;
+typedef struct sdot_server sdot_server;
 
 /* Library identity: ABI version and the sm architecture it was built for. */
 int sdot_abi_version(void);
@@ -191,7 +192,9 @@ sdot_status sdot_set_hessian_chunk(sdot_ctx *ctx, int stages);
  * Jacobi-preconditioned CG with FP64 vectors, the constant null vector
  * projected out and the true residual recomputed in FP64 every 64 steps;
  * Armijo backtracking on J in FP64.  Non-convergence within max_iterations is
- * SDOT_OK with converged = 0, like sdot_solve.  n_targets <= 46340. */
+ * SDOT_OK with converged = 0, like sdot_solve.  n_targets <= 46340.  The
+ * evaluations use the context's precision: create it with SDOT_PREC_FP64 for
+ * tolerances below the FP32-exponential gradient error (~5e-6 max nu_j). */
 typedef struct {
     unsigned iterations;        /* Newton steps taken */
     int converged;
@@ -207,6 +210,115 @@ typedef struct {
 } sdot_newton_info;
 sdot_status sdot_solve_newton(sdot_ctx *ctx, double *psi, const sdot_solver_params *params, int hessian_method,
                               sdot_newton_info *info);
+
+/* ---- batched solves (no single reference counterpart: many SotSolver::solve
+ * calls, SotSolver.cc:105-215, each over an epsilon-scaling sequence as in
+ * SemiDiscreteOT.cc:878-922, advanced together on one GPU) ----
+ * A batch holds untruncated problems (tau <= 0, pointwise threshold) of one
+ * dimension and uneven sizes, packed in device memory.  Every batched
+ * evaluation runs all active problems in four launches (persistent sweeps
+ * over (problem, block) work units, largest first); each problem keeps its
+ * own L-BFGS state, line search (deal.II rules, as sdot_solve) and
+ * convergence control from its sdot_solver_params.  Sources use the
+ * flattened quadrature layout of sdot_set_source without the cell structure
+ * (the untruncated path never queries cells).  psi arrays concatenate the
+ * problems in the order they were added, each in its caller order. */
+typedef struct sdot_batch sdot_batch;
+typedef struct {
+    double epsilon_scaling_factor;  /* EpsilonScalingHandler factor (> 1; default 10) */
+    int epsilon_scaling_steps;      /* levels eps f^(s-1), ..., eps (1 = no scaling) */
+    double intermediate_tolerance;  /* tolerance of the levels before the last (<= 0: each problem's own) */
+    int mixed_precision;            /* 1: FP32-exponential gradient sweeps until a problem meets its tolerance,
+                                       then FP64 sweeps until it meets the same tolerance in FP64 */
+} sdot_batch_options;
+typedef struct {
+    int n_problems;
+    int converged;                  /* problems that met their tolerance (in FP64) */
+    int64_t rounds;                 /* batched evaluations */
+    int64_t evaluations;            /* problem evaluations over all rounds */
+    int64_t total_pairs;
+    double eval_ms;                 /* device time in batched evaluations */
+    double solve_ms;                /* device time of the whole solve */
+} sdot_batch_info;
+sdot_status sdot_batch_create(sdot_batch **batch, int device, int dim);
+void sdot_batch_destroy(sdot_batch *batch);
+const char *sdot_batch_last_error(const sdot_batch *batch);
+int sdot_batch_size(const sdot_batch *batch);
+/* Print each problem's iterations and line-search trials (like VerboseSolverControl). */
+sdot_status sdot_batch_set_verbose(sdot_batch *batch, int verbose);
+/* Adds one problem (copied); its index is written to *index. */
+sdot_status sdot_batch_add(sdot_batch *batch, int64_t n_q, const double *x, const double *jxw, const double *density,
+                           int64_t n_t, const double *y, const double *nu, const sdot_solver_params *params,
+                           int *index);
+/* One batched evaluation at psi (host, concatenated): gradients (host,
+ * concatenated) and each problem's J(psi) in values[n_problems]; fp32 != 0
+ * runs the gradient sweep with FP32 exponentials. */
+sdot_status sdot_batch_evaluate(sdot_batch *batch, const double *psi, double *grad, double *values, int fp32);
+/* Solves every problem; psi (host, concatenated) holds the initial
+ * potentials and receives the results.  Non-convergence is reported per
+ * problem (sdot_batch_problem_info), not as an error; a line-search failure
+ * is SDOT_ELINESEARCH after all other problems have finished. */
+sdot_status sdot_batch_solve(sdot_batch *batch, double *psi, const sdot_batch_options *opts, sdot_batch_info *info);
+sdot_status sdot_batch_problem_info(const sdot_batch *batch, int index, sdot_solve_info *info);
+
+/* ---- solve service (no reference counterpart: the reference runs one
+ * SotSolver::solve per process at a time; this admits many) ----
+ * n_slots worker threads each own one context (own CUDA stream); requests
+ * wait in a FIFO queue and start when a slot is free and their device-memory
+ * estimate fits in memory_budget (0 = no budget) beside the running ones, so
+ * requests that arrive while others run are admitted as slots and memory
+ * free up and their kernels overlap on the device.  Solves are deterministic:
+ * a request gives the same potential alone or in any mix.  Inputs are copied
+ * at submit. */
+typedef enum { SDOT_METHOD_AUTO = 0, SDOT_METHOD_NEWTON = 1, SDOT_METHOD_LBFGS = 2 } sdot_method;
+typedef struct {
+    int dim;
+    int64_t n_q;
+    const double *x, *jxw, *density;     /* as sdot_set_source */
+    int64_t n_cells;                     /* 0: points only (untruncated requests) */
+    const int64_t *cell_offsets;
+    const double *cell_centers;
+    int64_t n_t;
+    const double *y, *nu;
+    const double *psi0;                  /* warm start (NULL: zeros) */
+    sdot_solver_params params;
+    int method;                          /* sdot_method; AUTO = Newton when untruncated, rho*JxW >= 0, n_t <= 46340 */
+    int precision;                       /* sdot_precision of the evaluation sweeps (L-BFGS; Newton uses FP64) */
+    int hessian_method;                  /* sdot_hessian_method for Newton */
+    double epsilon_scaling_factor;       /* levels eps f^(s-1), ..., eps, warm started */
+    int epsilon_scaling_steps;           /* 0 or 1: no scaling */
+    double intermediate_tolerance;       /* tolerance of the levels before the last (<= 0: params.tolerance) */
+} sdot_request;
+typedef struct {
+    sdot_status status;
+    int converged;
+    int method;                          /* method used */
+    unsigned iterations;                 /* over all epsilon levels */
+    int64_t n_evaluations;
+    double last_value, last_check_value;
+    double queue_ms, run_ms, latency_ms; /* host wall clock: submit -> start, start -> done, submit -> done */
+    int slot;
+    char message[160];                   /* error text when status != SDOT_OK */
+} sdot_result;
+typedef struct {
+    int64_t completed, failed, queued;
+    int running, peak_running;
+    size_t in_use_bytes, peak_bytes;     /* admitted device-memory estimates */
+    double p50_ms, p99_ms, mean_ms;      /* latency of completed requests */
+} sdot_server_stats;
+sdot_status sdot_server_create(sdot_server **server, int device, int n_slots, size_t memory_budget);
+/* Finishes the queued and running requests, then stops the workers. */
+void sdot_server_destroy(sdot_server *server);
+const char *sdot_server_last_error(const sdot_server *server);
+/* SDOT_EBUDGET when the request alone exceeds the budget. */
+sdot_status sdot_server_submit(sdot_server *server, const sdot_request *request, int64_t *ticket);
+/* 1 done, 0 pending, -1 unknown ticket. */
+int sdot_server_poll(sdot_server *server, int64_t ticket);
+/* Waits (timeout_s <= 0: forever; SDOT_ETIMEOUT on expiry) and returns the
+ * request's status; psi receives n_t doubles.  The ticket is then released. */
+sdot_status sdot_server_wait(sdot_server *server, int64_t ticket, double timeout_s, double *psi, sdot_result *result);
+sdot_status sdot_server_get_stats(sdot_server *server, sdot_server_stats *stats);
+sdot_status sdot_server_reset_stats(sdot_server *server);
 
 /* Getters replacing SotSolver::get_last_functional_value, get_last_iteration_count,
  * get_convergence_status, get_last_distance_threshold, get_C_global

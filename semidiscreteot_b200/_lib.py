@@ -13,6 +13,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libsdot_cuda.so")
 
 SDOT_OK = 0
+SDOT_ETIMEOUT = 7
 STATUS_NAMES = {
     0: "SDOT_OK", 1: "SDOT_EINVAL", 2: "SDOT_ENOMEM", 3: "SDOT_ENONFINITE", 4: "SDOT_ELINESEARCH",
     5: "SDOT_EMAXITER", 6: "SDOT_EBUDGET", 7: "SDOT_ETIMEOUT", 8: "SDOT_ECUDA", 9: "SDOT_ESTATE",
@@ -22,6 +23,7 @@ THRESHOLD = {"pointwise": 0, "integral": 1, "geometric": 2}
 CONTROL = {"l1norm": 0, "componentwise": 1, "linf": 2}
 LINE_SEARCH = {"upstream": 0, "vendored": 1}
 HESSIAN_METHOD = {"auto": 0, "fp64": 1, "tensor": 2}
+METHOD = {"auto": 0, "newton": 1, "lbfgs": 2}
 
 # Every symbol include/sdot.h declares (checked by tests).
 EXPORTED = [
@@ -33,7 +35,10 @@ EXPORTED = [
     "sdot_compute_geometric_radius_bound", "sdot_set_distance_function", "sdot_evaluate_partial_device",
     "sdot_set_state", "sdot_get_stream", "sdot_set_profiling", "sdot_get_kernel_times", "sdot_measure_peaks",
     "sdot_evaluate_device_noalloc", "sdot_hessian_device", "sdot_set_hessian_chunk",
-    "sdot_solve_newton",
+    "sdot_solve_newton", "sdot_batch_create", "sdot_batch_destroy", "sdot_batch_last_error", "sdot_batch_size", "sdot_batch_set_verbose",
+    "sdot_batch_add", "sdot_batch_evaluate", "sdot_batch_solve", "sdot_batch_problem_info",
+    "sdot_server_create", "sdot_server_destroy", "sdot_server_last_error", "sdot_server_submit", "sdot_server_poll",
+    "sdot_server_wait", "sdot_server_get_stats", "sdot_server_reset_stats",
 ]
 
 NOALLOC_SCRATCH_BYTES = 8 << 20  # SDOT_NOALLOC_SCRATCH_BYTES
@@ -71,6 +76,39 @@ class NewtonInfo(C.Structure):
                 ("cg_iterations", C.c_int64), ("last_value", C.c_double), ("last_check_value", C.c_double),
                 ("total_pairs", C.c_int64), ("eval_ms", C.c_double), ("hessian_ms", C.c_double),
                 ("cg_ms", C.c_double), ("hessian_method", C.c_int)]
+
+
+class BatchOptions(C.Structure):
+    _fields_ = [("epsilon_scaling_factor", C.c_double), ("epsilon_scaling_steps", C.c_int),
+                ("intermediate_tolerance", C.c_double), ("mixed_precision", C.c_int)]
+
+
+class BatchInfo(C.Structure):
+    _fields_ = [("n_problems", C.c_int), ("converged", C.c_int), ("rounds", C.c_int64),
+                ("evaluations", C.c_int64), ("total_pairs", C.c_int64), ("eval_ms", C.c_double),
+                ("solve_ms", C.c_double)]
+
+
+class Request(C.Structure):
+    _fields_ = [("dim", C.c_int), ("n_q", C.c_int64), ("x", C.c_void_p), ("jxw", C.c_void_p),
+                ("density", C.c_void_p), ("n_cells", C.c_int64), ("cell_offsets", C.c_void_p),
+                ("cell_centers", C.c_void_p), ("n_t", C.c_int64), ("y", C.c_void_p), ("nu", C.c_void_p),
+                ("psi0", C.c_void_p), ("params", SolverParams), ("method", C.c_int), ("precision", C.c_int),
+                ("hessian_method", C.c_int), ("epsilon_scaling_factor", C.c_double),
+                ("epsilon_scaling_steps", C.c_int), ("intermediate_tolerance", C.c_double)]
+
+
+class Result(C.Structure):
+    _fields_ = [("status", C.c_int), ("converged", C.c_int), ("method", C.c_int), ("iterations", C.c_uint),
+                ("n_evaluations", C.c_int64), ("last_value", C.c_double), ("last_check_value", C.c_double),
+                ("queue_ms", C.c_double), ("run_ms", C.c_double), ("latency_ms", C.c_double), ("slot", C.c_int),
+                ("message", C.c_char * 160)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("completed", C.c_int64), ("failed", C.c_int64), ("queued", C.c_int64), ("running", C.c_int),
+                ("peak_running", C.c_int), ("in_use_bytes", C.c_size_t), ("peak_bytes", C.c_size_t),
+                ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("mean_ms", C.c_double)]
 
 
 _lib = None
@@ -129,6 +167,40 @@ def load():
     lib.sdot_set_hessian_chunk.restype = ip
     lib.sdot_solve_newton.argtypes = [vp, vp, C.POINTER(SolverParams), ip, C.POINTER(NewtonInfo)]
     lib.sdot_solve_newton.restype = ip
+    lib.sdot_batch_create.argtypes = [C.POINTER(vp), ip, ip]
+    lib.sdot_batch_create.restype = ip
+    lib.sdot_batch_destroy.argtypes = [vp]
+    lib.sdot_batch_destroy.restype = None
+    lib.sdot_batch_last_error.argtypes = [vp]
+    lib.sdot_batch_last_error.restype = C.c_char_p
+    lib.sdot_batch_size.argtypes = [vp]
+    lib.sdot_batch_size.restype = ip
+    lib.sdot_batch_set_verbose.argtypes = [vp, ip]
+    lib.sdot_batch_set_verbose.restype = ip
+    lib.sdot_batch_add.argtypes = [vp, i64, vp, vp, vp, i64, vp, vp, C.POINTER(SolverParams), C.POINTER(ip)]
+    lib.sdot_batch_add.restype = ip
+    lib.sdot_batch_evaluate.argtypes = [vp, vp, vp, vp, ip]
+    lib.sdot_batch_evaluate.restype = ip
+    lib.sdot_batch_solve.argtypes = [vp, vp, C.POINTER(BatchOptions), C.POINTER(BatchInfo)]
+    lib.sdot_batch_solve.restype = ip
+    lib.sdot_batch_problem_info.argtypes = [vp, ip, C.POINTER(SolveInfo)]
+    lib.sdot_batch_problem_info.restype = ip
+    lib.sdot_server_create.argtypes = [C.POINTER(vp), ip, ip, C.c_size_t]
+    lib.sdot_server_create.restype = ip
+    lib.sdot_server_destroy.argtypes = [vp]
+    lib.sdot_server_destroy.restype = None
+    lib.sdot_server_last_error.argtypes = [vp]
+    lib.sdot_server_last_error.restype = C.c_char_p
+    lib.sdot_server_submit.argtypes = [vp, C.POINTER(Request), C.POINTER(i64)]
+    lib.sdot_server_submit.restype = ip
+    lib.sdot_server_poll.argtypes = [vp, i64]
+    lib.sdot_server_poll.restype = ip
+    lib.sdot_server_wait.argtypes = [vp, i64, d, vp, C.POINTER(Result)]
+    lib.sdot_server_wait.restype = ip
+    lib.sdot_server_get_stats.argtypes = [vp, C.POINTER(ServerStats)]
+    lib.sdot_server_get_stats.restype = ip
+    lib.sdot_server_reset_stats.argtypes = [vp]
+    lib.sdot_server_reset_stats.restype = ip
     for fn in ("sdot_evaluate_partial_device", "sdot_set_state", "sdot_set_profiling", "sdot_get_kernel_times",
                "sdot_measure_peaks"):
         getattr(lib, fn).restype = ip

@@ -1,0 +1,1091 @@
+// sdot_batch.cu -- many independent entropic semi-discrete OT problems solved together.
+//
+// The reference solves one problem per SotSolver (SotSolver::solve,
+// src/solvers/SotSolver.cc:105-215), optionally over an epsilon-scaling
+// sequence (SemiDiscreteOT.cc:878-922 with EpsilonScalingHandler).  A batch
+// holds many untruncated problems of uneven size packed contiguously in HBM
+// and advances all of them together:
+//
+//  * one batched evaluation = four launches over every active problem:
+//    target packing, a persistent value sweep and a persistent gradient
+//    sweep that pull (problem, block) work units from a queue ordered by cost
+//    (largest first, atomic counter), and a finalize with one CTA per
+//    problem.  The per-unit arithmetic is the single-problem dense sweep's
+//    (sdot_dense.cuh), so a problem's gradient is bitwise the one sdot_evaluate
+//    gives for it alone;
+//  * L-BFGS per problem with deal.II's SolverBFGS / LineMinimization logic
+//    (the same rules as sdot_solve) run as a resumable state machine on the
+//    host: every problem's next trial step is evaluated in the same batched
+//    evaluation, so a round costs one evaluation of the whole batch and a few
+//    scalar read-backs;
+//  * epsilon scaling per problem (eps f^(s-1), ..., eps, warm started);
+//  * mixed precision: gradient sweeps with FP32 exponentials (FP64
+//    accumulation) until a problem's gradient is below max(tolerance, 1e-6)
+//    (or its line search fails on FP32 noise), then FP64 sweeps from that
+//    point until it meets its tolerance in FP64, so the reported convergence
+//    is the FP64 one.
+#include <float.h>
+#include <math.h>
+#include <stdio.h>
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "sdot_dense.cuh"
+#include "sdot_device.cuh"
+#include "sdot_internal.h"
+
+namespace sdot {
+namespace {
+
+constexpr int HIST = 5;            // SolverBFGS::AdditionalData::max_history_size
+constexpr int BFIN_THREADS = 256;
+
+struct BInst {
+    EvalArgs a;
+    int64_t q0, t0;     // first point / target in the packed arrays
+    int64_t part0;      // first value-block partial (4 doubles each)
+    int64_t gp0;        // first gradient partial (nks * nt doubles)
+    int64_t qslice;     // points per gradient slice
+    int nks, ntb, nvb;  // gradient slices, target blocks, value blocks
+    int fp32;           // gradient sweep with FP32 exponentials
+    double tol;         // comp tolerance (componentwise control)
+};
+
+// ---------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------
+
+template <int DIM>
+__global__ void k_batch_prep(const BInst *__restrict__ inst, const int *__restrict__ act, const double *__restrict__ y,
+                             const double *__restrict__ nu, const double *__restrict__ psi, double *__restrict__ tpack)
+{
+    const BInst &I = inst[act[blockIdx.y]];
+    const EvalArgs &a = I.a;
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < a.nt; j += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t g = I.t0 + j;
+        double yt[3], ysq = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            yt[d] = y[g * DIM + d] - a.o[d];
+            ysq += yt[d] * yt[d];
+        }
+        double *t = tpack + g * TPACK;
+        t[0] = a.s * psi[g] - a.halfs * ysq;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) t[1 + d] = a.s * yt[d];
+        t[1 + DIM] = nu[g];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) t[2 + DIM + d] = y[g * DIM + d];
+    }
+}
+
+// Persistent value sweep: units (problem, point block), largest first.
+template <int DIM>
+__global__ void __launch_bounds__(DENSE_A_THREADS)
+k_batch_value(const BInst *__restrict__ inst, const int2 *__restrict__ units, int nunits, int *__restrict__ counter,
+              const double *__restrict__ x, const double *__restrict__ rho, const double *__restrict__ jxw,
+              const double *__restrict__ tpack, double *__restrict__ Lq, double *__restrict__ part)
+{
+    __shared__ int su;
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) su = atomicAdd(counter, 1);
+        __syncthreads();
+        const int u = su;
+        if (u >= nunits) break;
+        const int2 w = units[u];
+        const BInst &I = inst[w.x];
+        dense_value_block<DIM>(x + I.q0 * DIM, rho + I.q0, jxw + I.q0, tpack + I.t0 * TPACK, I.a, w.y, Lq + I.q0,
+                               part + (I.part0 + w.y) * 4);
+    }
+}
+
+// Persistent gradient sweep: units (problem, target block, point slice).
+template <int DIM>
+__global__ void __launch_bounds__(DENSE_B_THREADS)
+k_batch_grad(const BInst *__restrict__ inst, const int4 *__restrict__ units, int nunits, int *__restrict__ counter,
+             const double *__restrict__ x, const double *__restrict__ w, const double *__restrict__ Lq,
+             const double *__restrict__ tpack, const double *__restrict__ psi, double *__restrict__ gpart)
+{
+    __shared__ int su;
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) su = atomicAdd(counter, 1);
+        __syncthreads();
+        const int u = su;
+        if (u >= nunits) break;
+        const int4 un = units[u];
+        const BInst &I = inst[un.x];
+        if (I.fp32)
+            dense_grad_block<DIM, true>(x + I.q0 * DIM, w + I.q0, Lq + I.q0, tpack + I.t0 * TPACK, psi + I.t0, I.a,
+                                        I.qslice, un.y, un.z, gpart + I.gp0);
+        else
+            dense_grad_block<DIM, false>(x + I.q0 * DIM, w + I.q0, Lq + I.q0, tpack + I.t0 * TPACK, psi + I.t0, I.a,
+                                         I.qslice, un.y, un.z, gpart + I.gp0);
+    }
+}
+
+// One CTA per problem: g = sum of slices - nu, the functional and the norms
+// the control and the line search read (same slots as an evaluation's).
+__global__ void __launch_bounds__(BFIN_THREADS)
+k_batch_final(const BInst *__restrict__ inst, const int *__restrict__ act, const double *__restrict__ gpart,
+              const double *__restrict__ part, const double *__restrict__ nu, const double *__restrict__ psi,
+              const double *__restrict__ pdir, double *__restrict__ grad, double *__restrict__ scal)
+{
+    const int pi = act[blockIdx.x];
+    const BInst &I = inst[pi];
+    const int64_t nt = I.a.nt;
+    double psinu = 0.0, l1 = 0.0, linf = 0.0, comp = -CUDART_INF, l2 = 0.0, gp = 0.0, bad = 0.0;
+    for (int64_t j = threadIdx.x; j < nt; j += BFIN_THREADS) {
+        double s = 0.0;
+        for (int k = 0; k < I.nks; ++k) s += gpart[I.gp0 + (int64_t)k * nt + j];
+        const int64_t gj = I.t0 + j;
+        const double g = s - nu[gj];
+        grad[gj] = g;
+        psinu += psi[gj] * nu[gj];
+        const double ag = fabs(g);
+        l1 += ag;
+        linf = fmax(linf, ag);
+        comp = fmax(comp, ag - nu[gj] * I.tol);
+        l2 += g * g;
+        gp += g * pdir[gj];
+        if (!isfinite(g) || !isfinite(psi[gj])) bad = 1.0;
+    }
+    double v = 0.0, c = 0.0, sk = 0.0;
+    for (int64_t b = threadIdx.x; b < I.nvb; b += BFIN_THREADS) {
+        v += part[(I.part0 + b) * 4 + 0];
+        c += part[(I.part0 + b) * 4 + 1];
+        sk += part[(I.part0 + b) * 4 + 2];
+    }
+    __shared__ double sh[10][BFIN_THREADS / 32];
+    psinu = warp_sum(psinu);
+    l1 = warp_sum(l1);
+    linf = warp_max(linf);
+    comp = warp_max(comp);
+    l2 = warp_sum(l2);
+    gp = warp_sum(gp);
+    bad = warp_max(bad);
+    v = warp_sum(v);
+    c = warp_sum(c);
+    sk = warp_sum(sk);
+    const int wi = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        sh[0][wi] = psinu; sh[1][wi] = l1; sh[2][wi] = linf; sh[3][wi] = comp; sh[4][wi] = l2;
+        sh[5][wi] = gp; sh[6][wi] = bad; sh[7][wi] = v; sh[8][wi] = c; sh[9][wi] = sk;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r[10] = {0, 0, 0, -CUDART_INF, 0, 0, 0, 0, 0, 0};
+        for (int i = 0; i < BFIN_THREADS / 32; ++i) {
+            r[0] += sh[0][i]; r[1] += sh[1][i]; r[2] = fmax(r[2], sh[2][i]); r[3] = fmax(r[3], sh[3][i]);
+            r[4] += sh[4][i]; r[5] += sh[5][i]; r[6] = fmax(r[6], sh[6][i]);
+            r[7] += sh[7][i]; r[8] += sh[8][i]; r[9] += sh[9][i];
+        }
+        double *o = scal + (int64_t)pi * SC_COUNT;
+        o[SC_VALUE] = r[7] - r[0];
+        o[SC_VALSRC] = r[7];
+        o[SC_C] = r[8];
+        o[SC_SKIPPED] = r[9];
+        o[SC_PSINU] = r[0];
+        o[SC_L1] = r[1];
+        o[SC_LINF] = r[2];
+        o[SC_COMP] = r[3];
+        o[SC_L2SQ] = r[4];
+        o[SC_DOT_GP] = r[5];
+        o[SC_NONFINITE] = (r[6] != 0.0 || !isfinite(o[SC_VALUE])) ? 1.0 : 0.0;
+        o[SC_PAIRS] = (double)I.a.nq * (double)nt;
+    }
+}
+
+// psi = x0 + alpha_p pdir for each listed problem.
+__global__ void k_batch_axpy(const BInst *__restrict__ inst, const int *__restrict__ act,
+                             const double *__restrict__ alpha, double *__restrict__ psi, const double *__restrict__ x0,
+                             const double *__restrict__ pdir)
+{
+    const int pi = act[blockIdx.y];
+    const BInst &I = inst[pi];
+    const double al = alpha[pi];
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < I.a.nt; j += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t g = I.t0 + j;
+        psi[g] = x0[g] + al * pdir[g];
+    }
+}
+
+struct BHist {
+    int m;
+    int slot[HIST + 1];
+};
+
+// Two-loop recursion per problem (the single-problem k_two_loop, one CTA per
+// problem; history slots of problem p at S + (6 t0 + slot nt)), then
+// x0 = psi and g0 = g for the line search.  out[p] = g.p.
+__global__ void __launch_bounds__(1024)
+k_batch_two_loop(const BInst *__restrict__ inst, const int *__restrict__ act, const BHist *__restrict__ hist,
+                 const double *__restrict__ S, const double *__restrict__ Y, const double *__restrict__ rho,
+                 const double *__restrict__ g, double *__restrict__ p, const double *__restrict__ psi,
+                 double *__restrict__ x0, double *__restrict__ g0, double *__restrict__ out)
+{
+    __shared__ double red[32];
+    __shared__ double bc;
+    __shared__ double c1[8];
+    const int pi = act[blockIdx.x];
+    const BInst &I = inst[pi];
+    const int64_t n = I.a.nt, t0 = I.t0;
+    const BHist h = hist[pi];
+    const double *Sb = S + 6 * t0, *Yb = Y + 6 * t0;
+    const double *rh = rho + (int64_t)pi * 8;
+    const double *gb = g + t0;
+    double *pb = p + t0;
+    const int tid = threadIdx.x;
+    auto block_dot = [&](const double *a, const double *b) -> double {
+        double s = 0.0;
+        for (int64_t i = tid; i < n; i += blockDim.x) s += a[i] * b[i];
+        s = warp_sum(s);
+        __syncthreads();
+        if ((tid & 31) == 0) red[tid >> 5] = s;
+        __syncthreads();
+        if (tid == 0) {
+            double t = 0.0;
+            for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
+            bc = t;
+        }
+        __syncthreads();
+        return bc;
+    };
+    for (int64_t i = tid; i < n; i += blockDim.x) {
+        pb[i] = gb[i];
+        x0[t0 + i] = psi[t0 + i];
+        g0[t0 + i] = gb[i];
+    }
+    __syncthreads();
+    for (int i = 0; i < h.m; ++i) {
+        const int slot = h.slot[i];
+        const double ci = rh[slot] * block_dot(Sb + (int64_t)slot * n, pb);
+        if (tid == 0) c1[i] = ci;
+        const double a = -ci;
+        const double *yv = Yb + (int64_t)slot * n;
+        for (int64_t t = tid; t < n; t += blockDim.x) pb[t] += a * yv[t];
+        __syncthreads();
+    }
+    for (int i = h.m - 1; i >= 0; --i) {
+        const int slot = h.slot[i];
+        const double c2 = rh[slot] * block_dot(Yb + (int64_t)slot * n, pb);
+        const double a = c1[i] - c2;
+        const double *sv = Sb + (int64_t)slot * n;
+        for (int64_t t = tid; t < n; t += blockDim.x) pb[t] += a * sv[t];
+        __syncthreads();
+    }
+    for (int64_t i = tid; i < n; i += blockDim.x) pb[i] *= -1.;
+    __syncthreads();
+    const double gp = block_dot(gb, pb);
+    if (tid == 0) out[pi] = gp;
+}
+
+// s = psi - x0, y = g - g0 into slot `spare` of each listed problem; out[p] = s.y
+__global__ void __launch_bounds__(1024)
+k_batch_sy(const BInst *__restrict__ inst, const int *__restrict__ act, const int *__restrict__ spare,
+           const double *__restrict__ psi, const double *__restrict__ x0, const double *__restrict__ g,
+           const double *__restrict__ g0, double *__restrict__ S, double *__restrict__ Y, double *__restrict__ out)
+{
+    __shared__ double red[32];
+    const int pi = act[blockIdx.x];
+    const BInst &I = inst[pi];
+    const int64_t n = I.a.nt, t0 = I.t0;
+    double *s = S + 6 * t0 + (int64_t)spare[pi] * n;
+    double *yv = Y + 6 * t0 + (int64_t)spare[pi] * n;
+    double acc = 0.0;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const double a = psi[t0 + i] - x0[t0 + i];
+        const double b = g[t0 + i] - g0[t0 + i];
+        s[i] = a;
+        yv[i] = b;
+        acc += a * b;
+    }
+    acc = warp_sum(acc);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
+        out[pi] = t;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// deal.II LineMinimization::line_search as a resumable state machine (same
+// rules as line_search() in sdot_capi.cu: bracketing with tau1 = 9, then
+// sectioning with tau2 = 0.1, tau3 = 0.5 and cubic -> quadratic -> bisection).
+// ---------------------------------------------------------------------------
+
+bool cubic_fit_b(double x1, double f1, double g1, double x2, double f2, double g2, double *res)
+{
+    const double beta1 = g1 + g2 - 3. * (f1 - f2) / (x1 - x2);
+    const double s = beta1 * beta1 - g1 * g2;
+    if (s < 0) return false;
+    const double beta2 = std::sqrt(s);
+    const double denom = x1 < x2 ? g2 - g1 + 2. * beta2 : g1 - g2 + 2. * beta2;
+    if (denom == 0.) return false;
+    *res = x1 < x2 ? x2 - (x2 - x1) * (g2 + beta2 - beta1) / denom : x1 - (x1 - x2) * (g1 + beta2 - beta1) / denom;
+    return true;
+}
+
+bool quadratic_fit_b(double x1, double f1, double g1, double x2, double f2, double *res)
+{
+    const double denom = (2. * g1 * x2 - 2. * g1 * x1 - 2. * f2 + 2. * f1);
+    if (denom == 0) return false;
+    *res = (g1 * (x2 * x2 - x1 * x1) + 2. * (f1 - f2) * x1) / denom;
+    return true;
+}
+
+double poly_fit_b(double x1, double f1, double g1, double x2, double f2, double g2, double b0, double b1)
+{
+    double r;
+    if (cubic_fit_b(x1, f1, g1, x2, f2, g2, &r) && r >= b0 && r <= b1) return r;
+    if (quadratic_fit_b(x1, f1, g1, x2, f2, &r) && r >= b0 && r <= b1) return r;
+    return (b0 + b1) * 0.5;
+}
+
+struct LineSearch {
+    enum { BRACKET, SECTION } phase = BRACKET;
+    double f0 = 0, g0 = 0, mu = 1e-3, eta = 0.9, a_max = DBL_MAX, f_min = 0;
+    unsigned max_evals = 20, i = 0;
+    double a_prev = 0, f_prev = 0, g_prev = 0;
+    double a_lo = NAN, f_lo = NAN, g_lo = NAN, a_hi = NAN, f_hi = NAN, g_hi = NAN;
+    double ai = 0;
+
+    void begin(double f0_, double g0_, double a1)
+    {
+        phase = BRACKET;
+        f0 = f0_;
+        g0 = g0_;
+        f_min = f0 + a_max * mu * g0;
+        i = 0;
+        a_prev = 0;
+        f_prev = f0;
+        g_prev = g0;
+        ai = a1;
+    }
+    bool w1(double a, double f) const { return f <= f0 + a * mu * g0; }
+    bool w2(double g) const { return std::fabs(g) <= eta * std::fabs(g0); }
+    void next_section()
+    {
+        const double lo_safe = a_lo + 0.1 * (a_hi - a_lo);
+        const double hi_safe = a_hi - 0.5 * (a_hi - a_lo);
+        ai = poly_fit_b(a_lo, f_lo, g_lo, a_hi, f_hi, g_hi, std::min(lo_safe, hi_safe), std::max(lo_safe, hi_safe));
+    }
+    // Feed the result at ai.  Returns 0 (accepted: alpha = ai), 1 (evaluate
+    // again at ai), -1 (no bracket within max_evals), -2 (sectioning failed).
+    int feed(double fi, double gi)
+    {
+        ++i;
+        if (phase == BRACKET) {
+            if (fi <= f_min || ai == a_max) return 0;
+            if (!w1(ai, fi) || (fi >= f_prev && i > 1)) {
+                a_lo = a_prev; f_lo = f_prev; g_lo = g_prev;
+                a_hi = ai; f_hi = fi; g_hi = gi;
+            } else {
+                if (w2(gi)) return 0;
+                if (gi >= 0) {
+                    a_lo = ai; f_lo = fi; g_lo = gi;
+                    a_hi = a_prev; f_hi = f_prev; g_hi = g_prev;
+                } else {
+                    const double ub = ai + 9. * (ai - a_prev);
+                    a_prev = ai; f_prev = fi; g_prev = gi;
+                    ai = std::min(a_max, ub);
+                    return i < max_evals ? 1 : -1;
+                }
+            }
+            if (!(i < max_evals)) return -1;
+            phase = SECTION;
+            next_section();
+            return 1;
+        }
+        if (!w1(ai, fi) || fi >= f_lo) {
+            a_hi = ai; f_hi = fi; g_hi = gi;
+        } else {
+            if (w2(gi)) return 0;
+            if (gi * (a_hi - a_lo) >= 0) { a_hi = a_lo; f_hi = f_lo; g_hi = g_lo; }
+            a_lo = ai; f_lo = fi; g_lo = gi;
+        }
+        if (!(i < max_evals)) return -2;
+        next_section();
+        return 1;
+    }
+};
+
+}  // namespace
+}  // namespace sdot
+
+using namespace sdot;
+
+// ---------------------------------------------------------------------------
+// host object
+// ---------------------------------------------------------------------------
+
+struct sdot_batch {
+    int device = 0;
+    int dim = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::string err;
+    int sms = 148;
+    int verbose = 0;
+
+    struct Prob {
+        int64_t nq, nt;
+        sdot_solver_params prm;
+        double origin[3];
+    };
+    std::vector<Prob> probs;
+    std::vector<double> hx, hrho, hjxw, hy, hnu;  // staged on the host until the first solve
+    bool uploaded = false;
+    std::vector<BInst> inst;
+    int64_t total_q = 0, total_t = 0, total_part = 0, total_gp = 0;
+
+    DevBuf<double> x, rho, jxw, w, y, nu, psi, grad, tpack, Lq, part, gpart, x0, g0, pdir, S, Y, rho_h, scal, alpha,
+        outv;
+    DevBuf<BInst> dinst;
+    DevBuf<int> act, counter, spare;
+    DevBuf<int2> vunits;
+    DevBuf<int4> gunits;
+    DevBuf<BHist> dhist;
+    std::vector<double> scal_host;
+
+    // per-problem results of the last solve
+    std::vector<sdot_solve_info> info;
+};
+
+namespace {
+
+sdot_status berr(sdot_batch *b, sdot_status s, const std::string &m)
+{
+    if (b) b->err = m;
+    return s;
+}
+
+sdot_status bcuda(sdot_batch *b, cudaError_t e, const char *where)
+{
+    if (e == cudaSuccess) return SDOT_OK;
+    return berr(b, e == cudaErrorMemoryAllocation ? SDOT_ENOMEM : SDOT_ECUDA,
+                std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define BCK(call, where)                                   \
+    do {                                                   \
+        cudaError_t e_ = (call);                           \
+        if (e_ != cudaSuccess) return bcuda(b, e_, where); \
+    } while (0)
+
+struct DevGuard {
+    int prev = -1;
+    explicit DevGuard(int d)
+    {
+        cudaGetDevice(&prev);
+        if (prev != d) cudaSetDevice(d);
+    }
+    ~DevGuard()
+    {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+// Layout of every problem in the packed arrays and its launch shapes (the
+// single-problem dense path's: value blocks of DENSE_A_THREADS * QT points,
+// gradient target blocks of DENSE_B_THREADS * TT and the same slice count).
+sdot_status upload(sdot_batch *b)
+{
+    const int D = b->dim;
+    const size_t np = b->probs.size();
+    b->inst.assign(np, BInst{});
+    int64_t q0 = 0, t0 = 0, part0 = 0, gp0 = 0;
+    for (size_t i = 0; i < np; ++i) {
+        const auto &P = b->probs[i];
+        BInst &I = b->inst[i];
+        EvalArgs &a = I.a;
+        a.qpc = 1;
+        a.ql = 1;
+        a.ngroups = 1;
+        a.lse = P.prm.use_log_sum_exp;
+        a.nq = P.nq;
+        a.ncells = P.nq;
+        a.nunits = P.nq;
+        a.nt = P.nt;
+        a.eps = P.prm.epsilon;
+        a.s = KAPPA / a.eps;
+        a.halfs = 0.5 * a.s;
+        for (int d = 0; d < 3; ++d) a.o[d] = P.origin[d];
+        a.sstar = DBL_MAX;
+        a.cull = 1e300;
+        a.c32 = LOG2E / (2.0 * a.eps);
+        a.l2e_eps = LOG2E / a.eps;
+        I.q0 = q0;
+        I.t0 = t0;
+        const int64_t per = (int64_t)DENSE_A_THREADS * DENSE_A_QT;
+        I.nvb = (int)((P.nq + per - 1) / per);
+        I.part0 = part0;
+        const int64_t tb = (P.nt + DENSE_B_THREADS * DENSE_B_TT - 1) / (DENSE_B_THREADS * DENSE_B_TT);
+        int64_t want = (148 * 8 + tb - 1) / tb;
+        int64_t maxks = (P.nq + 255) / 256;
+        int nks = (int)std::max<int64_t>(1, std::min<int64_t>(want, maxks));
+        if (nks > 64) nks = 64;
+        I.nks = nks;
+        I.ntb = (int)tb;
+        I.qslice = (P.nq + nks - 1) / nks;
+        I.gp0 = gp0;
+        I.fp32 = 0;
+        I.tol = P.prm.tolerance;
+        q0 += P.nq;
+        t0 += P.nt;
+        part0 += I.nvb;
+        gp0 += (int64_t)nks * P.nt;
+    }
+    b->total_q = q0;
+    b->total_t = t0;
+    b->total_part = part0;
+    b->total_gp = gp0;
+    BCK(b->x.alloc(q0 * D), "batch alloc");
+    BCK(b->rho.alloc(q0), "batch alloc");
+    BCK(b->jxw.alloc(q0), "batch alloc");
+    BCK(b->w.alloc(q0), "batch alloc");
+    BCK(b->Lq.alloc(q0), "batch alloc");
+    BCK(b->y.alloc(t0 * D), "batch alloc");
+    BCK(b->nu.alloc(t0), "batch alloc");
+    BCK(b->psi.alloc(t0), "batch alloc");
+    BCK(b->grad.alloc(t0), "batch alloc");
+    BCK(b->tpack.alloc(t0 * TPACK), "batch alloc");
+    BCK(b->x0.alloc(t0), "batch alloc");
+    BCK(b->g0.alloc(t0), "batch alloc");
+    BCK(b->pdir.alloc(t0), "batch alloc");
+    BCK(b->S.alloc(6 * t0), "batch alloc");
+    BCK(b->Y.alloc(6 * t0), "batch alloc");
+    BCK(b->part.alloc(part0 * 4), "batch alloc");
+    BCK(b->gpart.alloc(gp0), "batch alloc");
+    BCK(b->rho_h.alloc(np * 8), "batch alloc");
+    BCK(b->scal.alloc(np * SC_COUNT), "batch alloc");
+    BCK(b->alpha.alloc(np), "batch alloc");
+    BCK(b->outv.alloc(np), "batch alloc");
+    BCK(b->dinst.alloc(np), "batch alloc");
+    BCK(b->act.alloc(np), "batch alloc");
+    BCK(b->spare.alloc(np), "batch alloc");
+    BCK(b->dhist.alloc(np), "batch alloc");
+    BCK(b->counter.alloc(2), "batch alloc");
+    std::vector<double> w(q0);
+    for (int64_t q = 0; q < q0; ++q) w[q] = b->hrho[q] * b->hjxw[q];
+    BCK(cudaMemcpy(b->x.p, b->hx.data(), q0 * D * 8, cudaMemcpyHostToDevice), "batch upload");
+    BCK(cudaMemcpy(b->rho.p, b->hrho.data(), q0 * 8, cudaMemcpyHostToDevice), "batch upload");
+    BCK(cudaMemcpy(b->jxw.p, b->hjxw.data(), q0 * 8, cudaMemcpyHostToDevice), "batch upload");
+    BCK(cudaMemcpy(b->w.p, w.data(), q0 * 8, cudaMemcpyHostToDevice), "batch upload");
+    BCK(cudaMemcpy(b->y.p, b->hy.data(), t0 * D * 8, cudaMemcpyHostToDevice), "batch upload");
+    BCK(cudaMemcpy(b->nu.p, b->hnu.data(), t0 * 8, cudaMemcpyHostToDevice), "batch upload");
+    BCK(cudaMemset(b->pdir.p, 0, t0 * 8), "batch upload");
+    b->scal_host.assign(np * SC_COUNT, 0.0);
+    b->uploaded = true;
+    return SDOT_OK;
+}
+
+// One batched evaluation of the listed problems at b->psi (inst[].fp32 and
+// inst[].a.eps as set on the device); fills scal_host for them.
+sdot_status batch_eval(sdot_batch *b, const std::vector<int> &act, double *ms)
+{
+    if (act.empty()) return SDOT_OK;
+    const int D = b->dim;
+    cudaStream_t st = b->stream;
+    BCK(cudaMemcpyAsync(b->act.p, act.data(), act.size() * sizeof(int), cudaMemcpyHostToDevice, st), "batch act");
+    // work units, largest first
+    std::vector<int2> vu;
+    std::vector<int4> gu;
+    std::vector<std::pair<double, int>> order;
+    for (int p : act) order.push_back({-(double)b->probs[p].nq * (double)b->probs[p].nt, p});
+    std::sort(order.begin(), order.end());
+    for (auto &o : order) {
+        const BInst &I = b->inst[o.second];
+        for (int k = 0; k < I.nvb; ++k) vu.push_back(make_int2(o.second, k));
+        for (int k = 0; k < I.nks; ++k)
+            for (int t = 0; t < I.ntb; ++t) gu.push_back(make_int4(o.second, t, k, 0));
+    }
+    BCK(b->vunits.alloc(vu.size()), "batch units");
+    BCK(b->gunits.alloc(gu.size()), "batch units");
+    BCK(cudaMemcpyAsync(b->vunits.p, vu.data(), vu.size() * sizeof(int2), cudaMemcpyHostToDevice, st), "batch units");
+    BCK(cudaMemcpyAsync(b->gunits.p, gu.data(), gu.size() * sizeof(int4), cudaMemcpyHostToDevice, st), "batch units");
+    BCK(cudaMemsetAsync(b->counter.p, 0, 2 * sizeof(int), st), "batch counter");
+    int64_t maxnt = 0;
+    for (int p : act) maxnt = std::max(maxnt, b->probs[p].nt);
+    cudaEventRecord(b->ev0, st);
+    dim3 pg((unsigned)std::min<int64_t>((maxnt + 255) / 256, 64), (unsigned)act.size());
+    const int vgrid = std::min<int>((int)vu.size(), b->sms * 8);
+    const int ggrid = std::min<int>((int)gu.size(), b->sms * 8);
+    if (D == 2) {
+        k_batch_prep<2><<<pg, 256, 0, st>>>(b->dinst.p, b->act.p, b->y.p, b->nu.p, b->psi.p, b->tpack.p);
+        k_batch_value<2><<<vgrid, DENSE_A_THREADS, 0, st>>>(b->dinst.p, b->vunits.p, (int)vu.size(), b->counter.p,
+                                                            b->x.p, b->rho.p, b->jxw.p, b->tpack.p, b->Lq.p, b->part.p);
+        k_batch_grad<2><<<ggrid, DENSE_B_THREADS, 0, st>>>(b->dinst.p, b->gunits.p, (int)gu.size(), b->counter.p + 1,
+                                                           b->x.p, b->w.p, b->Lq.p, b->tpack.p, b->psi.p, b->gpart.p);
+    } else {
+        k_batch_prep<3><<<pg, 256, 0, st>>>(b->dinst.p, b->act.p, b->y.p, b->nu.p, b->psi.p, b->tpack.p);
+        k_batch_value<3><<<vgrid, DENSE_A_THREADS, 0, st>>>(b->dinst.p, b->vunits.p, (int)vu.size(), b->counter.p,
+                                                            b->x.p, b->rho.p, b->jxw.p, b->tpack.p, b->Lq.p, b->part.p);
+        k_batch_grad<3><<<ggrid, DENSE_B_THREADS, 0, st>>>(b->dinst.p, b->gunits.p, (int)gu.size(), b->counter.p + 1,
+                                                           b->x.p, b->w.p, b->Lq.p, b->tpack.p, b->psi.p, b->gpart.p);
+    }
+    k_batch_final<<<(unsigned)act.size(), BFIN_THREADS, 0, st>>>(b->dinst.p, b->act.p, b->gpart.p, b->part.p,
+                                                                  b->nu.p, b->psi.p, b->pdir.p, b->grad.p, b->scal.p);
+    cudaEventRecord(b->ev1, st);
+    BCK(cudaGetLastError(), "batch evaluate");
+    BCK(cudaMemcpyAsync(b->scal_host.data(), b->scal.p, b->scal_host.size() * 8, cudaMemcpyDeviceToHost, st),
+        "batch scalars");
+    BCK(cudaStreamSynchronize(st), "batch evaluate");
+    if (ms) {
+        float f = 0.f;
+        cudaEventElapsedTime(&f, b->ev0, b->ev1);
+        *ms += f;
+    }
+    return SDOT_OK;
+}
+
+// VerboseSolverControl check on one problem's scalars (see control_check in
+// sdot_capi.cu): 1 converged, 0 iterate, -1 failure.
+int bcheck(const sdot_solver_params &p, const double *sc, unsigned step, double tol, double *value)
+{
+    double v;
+    if (p.control_type == SDOT_CONTROL_COMPONENTWISE) {
+        v = sc[SC_COMP];
+        tol = DBL_MIN;
+    } else if (p.control_type == SDOT_CONTROL_LINF) {
+        v = sc[SC_LINF];
+    } else {
+        v = sc[SC_L1];
+    }
+    *value = v;
+    if (v <= tol) return 1;
+    if (step >= p.max_iterations || std::isnan(v)) return -1;
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+sdot_status sdot_batch_create(sdot_batch **out, int device, int dim)
+{
+    if (!out || (dim != 2 && dim != 3)) return SDOT_EINVAL;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) return SDOT_ECUDA;
+    sdot_batch *b = new sdot_batch();
+    b->device = device;
+    b->dim = dim;
+    DevGuard g(device);
+    cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, device);
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess) {
+        delete b;
+        return SDOT_ECUDA;
+    }
+    *out = b;
+    return SDOT_OK;
+}
+
+void sdot_batch_destroy(sdot_batch *b)
+{
+    if (!b) return;
+    {
+        DevGuard g(b->device);
+        cudaStreamSynchronize(b->stream);
+        b->x.release(); b->rho.release(); b->jxw.release(); b->w.release(); b->y.release(); b->nu.release();
+        b->psi.release(); b->grad.release(); b->tpack.release(); b->Lq.release(); b->part.release();
+        b->gpart.release(); b->x0.release(); b->g0.release(); b->pdir.release(); b->S.release(); b->Y.release();
+        b->rho_h.release(); b->scal.release(); b->alpha.release(); b->outv.release(); b->dinst.release();
+        b->act.release(); b->counter.release(); b->spare.release(); b->vunits.release(); b->gunits.release();
+        b->dhist.release();
+        cudaEventDestroy(b->ev0);
+        cudaEventDestroy(b->ev1);
+        cudaStreamDestroy(b->stream);
+    }
+    delete b;
+}
+
+const char *sdot_batch_last_error(const sdot_batch *b) { return b ? b->err.c_str() : "null batch"; }
+
+int sdot_batch_size(const sdot_batch *b) { return b ? (int)b->probs.size() : 0; }
+
+sdot_status sdot_batch_set_verbose(sdot_batch *b, int verbose)
+{
+    if (!b) return SDOT_EINVAL;
+    b->verbose = verbose;
+    return SDOT_OK;
+}
+
+sdot_status sdot_batch_add(sdot_batch *b, int64_t n_q, const double *x, const double *jxw, const double *density,
+                           int64_t n_t, const double *y, const double *nu, const sdot_solver_params *params,
+                           int *index)
+{
+    if (!b || !x || !jxw || !density || !y || !nu || !params || n_q <= 0 || n_t <= 0) return SDOT_EINVAL;
+    if (b->uploaded) return berr(b, SDOT_ESTATE, "problems cannot be added after the first solve");
+    if (params->tau > 0.0 || params->threshold_type != SDOT_THRESH_POINTWISE)
+        return berr(b, SDOT_EINVAL, "batched problems are untruncated: tau <= 0 with the pointwise threshold");
+    if (!(params->epsilon > 0.0)) return berr(b, SDOT_EINVAL, "epsilon must be positive");
+    if (params->line_search != SDOT_LS_UPSTREAM)
+        return berr(b, SDOT_EINVAL, "batched solves use the deal.II line search (line_search = upstream)");
+    const int D = b->dim;
+    double lo[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, hi[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+    for (int64_t q = 0; q < n_q; ++q) {
+        for (int d = 0; d < D; ++d) {
+            const double v = x[q * D + d];
+            if (!std::isfinite(v)) return berr(b, SDOT_EINVAL, "non-finite source point");
+            lo[d] = std::min(lo[d], v);
+            hi[d] = std::max(hi[d], v);
+        }
+        if (!std::isfinite(jxw[q]) || !std::isfinite(density[q])) return berr(b, SDOT_EINVAL, "non-finite weight");
+    }
+    for (int64_t j = 0; j < n_t; ++j) {
+        if (!(nu[j] >= 0.0) || !std::isfinite(nu[j])) return berr(b, SDOT_EINVAL, "target weights must be >= 0");
+        for (int d = 0; d < D; ++d) {
+            const double v = y[j * D + d];
+            if (!std::isfinite(v)) return berr(b, SDOT_EINVAL, "non-finite target point");
+            lo[d] = std::min(lo[d], v);
+            hi[d] = std::max(hi[d], v);
+        }
+    }
+    sdot_batch::Prob P;
+    P.nq = n_q;
+    P.nt = n_t;
+    P.prm = *params;
+    for (int d = 0; d < 3; ++d) P.origin[d] = d < D ? 0.5 * (lo[d] + hi[d]) : 0.0;
+    b->probs.push_back(P);
+    b->hx.insert(b->hx.end(), x, x + n_q * D);
+    b->hjxw.insert(b->hjxw.end(), jxw, jxw + n_q);
+    b->hrho.insert(b->hrho.end(), density, density + n_q);
+    b->hy.insert(b->hy.end(), y, y + n_t * D);
+    b->hnu.insert(b->hnu.end(), nu, nu + n_t);
+    if (index) *index = (int)b->probs.size() - 1;
+    return SDOT_OK;
+}
+
+sdot_status sdot_batch_evaluate(sdot_batch *b, const double *psi, double *grad, double *values, int fp32)
+{
+    if (!b || !psi || !grad || !values) return SDOT_EINVAL;
+    if (b->probs.empty()) return berr(b, SDOT_ESTATE, "empty batch");
+    DevGuard g(b->device);
+    if (!b->uploaded) {
+        sdot_status s = upload(b);
+        if (s != SDOT_OK) return s;
+    }
+    for (auto &I : b->inst) {
+        I.fp32 = fp32 ? 1 : 0;
+    }
+    BCK(cudaMemcpyAsync(b->dinst.p, b->inst.data(), b->inst.size() * sizeof(BInst), cudaMemcpyHostToDevice, b->stream),
+        "batch inst");
+    BCK(cudaMemcpyAsync(b->psi.p, psi, b->total_t * 8, cudaMemcpyHostToDevice, b->stream), "batch psi");
+    BCK(cudaMemsetAsync(b->pdir.p, 0, b->total_t * 8, b->stream), "batch pdir");
+    std::vector<int> act(b->probs.size());
+    std::iota(act.begin(), act.end(), 0);
+    sdot_status s = batch_eval(b, act, nullptr);
+    if (s != SDOT_OK) return s;
+    BCK(cudaMemcpy(grad, b->grad.p, b->total_t * 8, cudaMemcpyDeviceToHost), "batch grad");
+    for (size_t i = 0; i < b->probs.size(); ++i) values[i] = b->scal_host[i * SC_COUNT + SC_VALUE];
+    return SDOT_OK;
+}
+
+sdot_status sdot_batch_solve(sdot_batch *b, double *psi_io, const sdot_batch_options *opts, sdot_batch_info *info)
+{
+    if (!b || !psi_io) return SDOT_EINVAL;
+    if (b->probs.empty()) return berr(b, SDOT_ESTATE, "empty batch");
+    sdot_batch_options o{};
+    o.epsilon_scaling_factor = 10.0;
+    o.epsilon_scaling_steps = 1;
+    o.intermediate_tolerance = 0.0;
+    o.mixed_precision = 1;
+    if (opts) o = *opts;
+    DevGuard guard(b->device);
+    if (!b->uploaded) {
+        sdot_status s = upload(b);
+        if (s != SDOT_OK) return s;
+    }
+    const int np = (int)b->probs.size();
+    cudaStream_t st = b->stream;
+    BCK(cudaMemcpyAsync(b->psi.p, psi_io, b->total_t * 8, cudaMemcpyHostToDevice, st), "batch psi");
+    BCK(cudaMemsetAsync(b->pdir.p, 0, b->total_t * 8, st), "batch pdir");
+
+    // epsilon sequence per problem (EpsilonScalingHandler): eps f^(s-1-i), largest first
+    double fac = o.epsilon_scaling_factor;
+    if (fac <= 1.0) fac = 2.0;
+    const int levels = std::max(1, o.epsilon_scaling_steps);
+
+    enum Phase { EVAL0, LSEARCH, DONE };
+    struct St {
+        Phase ph = EVAL0;
+        int level = 0;
+        int fp32 = 0;
+        double f = 0, f_prev = 0;
+        int first_step = 1;
+        unsigned k = 0, k_total = 0;
+        int conv = 0;
+        double check = 0;
+        sdot_status err = SDOT_OK;
+        LineSearch ls;
+        std::vector<int> order;
+        std::vector<int> free_slots;
+        int spare = 0;
+        double rho[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        int64_t evals = 0, pairs = 0;
+    };
+    std::vector<St> S(np);
+    auto level_eps = [&](int p, int lev) {
+        return b->probs[p].prm.epsilon * std::pow(fac, (double)(levels - 1 - lev));
+    };
+    auto set_eps = [&](int p) {
+        BInst &I = b->inst[p];
+        const double eps = level_eps(p, S[p].level);
+        I.a.eps = eps;
+        I.a.s = KAPPA / eps;
+        I.a.halfs = 0.5 * I.a.s;
+        I.a.c32 = LOG2E / (2.0 * eps);
+        I.a.l2e_eps = LOG2E / eps;
+        I.fp32 = S[p].fp32;
+    };
+    auto reset_lbfgs = [&](int p) {
+        St &s = S[p];
+        s.ph = EVAL0;
+        s.first_step = 1;
+        s.f_prev = 0.0;
+        s.k = 0;
+        s.order.clear();
+        s.free_slots = {1, 2, 3, 4, 5};
+        s.spare = 0;
+    };
+    for (int p = 0; p < np; ++p) {
+        S[p].fp32 = o.mixed_precision ? 1 : 0;
+        reset_lbfgs(p);
+        set_eps(p);
+    }
+    // FP32-phase tolerance: the FP32 exponentials carry ~1e-7 relative error,
+    // so the FP32 phase stops at 1e-6 at the latest and FP64 finishes.
+    constexpr double FP32_PHASE_TOL = 1e-6;
+    auto level_tol = [&](int p) {
+        const bool last = S[p].level == levels - 1;
+        double t = b->probs[p].prm.tolerance;
+        if (!last && o.intermediate_tolerance > 0.0) t = o.intermediate_tolerance;
+        if (S[p].fp32) t = std::max(t, FP32_PHASE_TOL);
+        return t;
+    };
+
+    double dev_ms = 0.0;
+    int64_t rounds = 0, evals = 0, pairs = 0;
+    std::vector<double> alpha_h(np, 0.0), out_h(np, 0.0);
+    std::vector<BHist> hist_h(np);
+    std::vector<int> spare_h(np, 0);
+    bool inst_dirty = true;
+    cudaEvent_t w0, w1;
+    cudaEventCreate(&w0);
+    cudaEventCreate(&w1);
+    cudaEventRecord(w0, st);
+    for (;;) {
+        std::vector<int> ev;
+        for (int p = 0; p < np; ++p)
+            if (S[p].ph != DONE) ev.push_back(p);
+        if (ev.empty()) break;
+        if (inst_dirty) {
+            BCK(cudaMemcpyAsync(b->dinst.p, b->inst.data(), np * sizeof(BInst), cudaMemcpyHostToDevice, st),
+                "batch inst");
+            inst_dirty = false;
+        }
+        sdot_status s = batch_eval(b, ev, &dev_ms);
+        if (s != SDOT_OK) return s;
+        ++rounds;
+        evals += (int64_t)ev.size();
+        std::vector<int> need_sy, need_dir;
+        for (int p : ev) {
+            St &z = S[p];
+            const double *sc = &b->scal_host[(size_t)p * SC_COUNT];
+            ++z.evals;
+            z.pairs += (int64_t)sc[SC_PAIRS];
+            pairs += (int64_t)sc[SC_PAIRS];
+            if (z.ph == EVAL0) {
+                z.f = sc[SC_VALUE];
+                z.conv = bcheck(b->probs[p].prm, sc, z.k, level_tol(p), &z.check);
+            } else {
+                const int rc = z.ls.feed(sc[SC_VALUE], sc[SC_DOT_GP]);
+                if (b->verbose)
+                    printf("problem %d: trial %u alpha %.6e f %.17e g.p %.6e -> %d\n", p, z.ls.i, z.ls.ai,
+                           sc[SC_VALUE], sc[SC_DOT_GP], rc);
+                if (rc == 1) {
+                    alpha_h[p] = z.ls.ai;
+                    continue;
+                }
+                z.f = sc[SC_VALUE];
+                if (rc < 0) {
+                    if (z.fp32) {
+                        // FP32 gradients too noisy for the line search here:
+                        // continue this level from the current potential in FP64
+                        z.fp32 = 0;
+                        reset_lbfgs(p);
+                        set_eps(p);
+                        inst_dirty = true;
+                        continue;
+                    }
+                    z.err = SDOT_ELINESEARCH;
+                    z.ph = DONE;
+                    z.conv = -1;
+                    continue;
+                }
+                z.first_step = 0;
+                ++z.k;
+                ++z.k_total;
+                z.conv = bcheck(b->probs[p].prm, sc, z.k, level_tol(p), &z.check);
+                if (b->verbose)
+                    printf("problem %d: level %d fp32 %d iteration %u f %.17e check %.6e\n", p, z.level, z.fp32, z.k,
+                           z.f, z.check);
+                if (z.conv == 0) need_sy.push_back(p);
+            }
+            if (z.conv == 1) {
+                // level done: next epsilon, or FP64 confirmation, or finished
+                if (z.level + 1 < levels) {
+                    ++z.level;
+                    reset_lbfgs(p);
+                    set_eps(p);
+                    inst_dirty = true;
+                } else if (z.fp32) {
+                    z.fp32 = 0;
+                    reset_lbfgs(p);
+                    set_eps(p);
+                    inst_dirty = true;
+                } else {
+                    z.ph = DONE;
+                }
+                continue;
+            }
+            if (z.conv == -1) {
+                z.ph = DONE;
+                continue;
+            }
+            need_dir.push_back(p);
+        }
+        // history update for problems that completed a step
+        if (!need_sy.empty()) {
+            for (int p : need_sy) spare_h[p] = S[p].spare;
+            BCK(cudaMemcpyAsync(b->spare.p, spare_h.data(), np * sizeof(int), cudaMemcpyHostToDevice, st), "batch sy");
+            BCK(cudaMemcpyAsync(b->act.p, need_sy.data(), need_sy.size() * sizeof(int), cudaMemcpyHostToDevice, st),
+                "batch sy");
+            k_batch_sy<<<(unsigned)need_sy.size(), 1024, 0, st>>>(b->dinst.p, b->act.p, b->spare.p, b->psi.p, b->x0.p,
+                                                                  b->grad.p, b->g0.p, b->S.p, b->Y.p, b->outv.p);
+            BCK(cudaMemcpyAsync(out_h.data(), b->outv.p, np * 8, cudaMemcpyDeviceToHost, st), "batch sy");
+            BCK(cudaStreamSynchronize(st), "batch sy");
+            for (int p : need_sy) {
+                St &z = S[p];
+                const double curvature = out_h[p];
+                if (curvature > 0.) {
+                    z.rho[z.spare] = 1. / curvature;
+                    z.order.insert(z.order.begin(), z.spare);
+                    if ((int)z.order.size() > HIST) {
+                        z.spare = z.order.back();
+                        z.order.pop_back();
+                    } else {
+                        z.spare = z.free_slots.back();
+                        z.free_slots.pop_back();
+                    }
+                }
+            }
+        }
+        // new directions and first trial steps
+        if (!need_dir.empty()) {
+            std::vector<double> rho_all((size_t)np * 8, 0.0);
+            for (int p : need_dir) {
+                BHist h{};
+                h.m = (int)S[p].order.size();
+                for (int i = 0; i < h.m; ++i) h.slot[i] = S[p].order[i];
+                hist_h[p] = h;
+            }
+            for (int p = 0; p < np; ++p)
+                for (int i = 0; i < 8; ++i) rho_all[(size_t)p * 8 + i] = S[p].rho[i];
+            BCK(cudaMemcpyAsync(b->dhist.p, hist_h.data(), np * sizeof(BHist), cudaMemcpyHostToDevice, st), "batch dir");
+            BCK(cudaMemcpyAsync(b->rho_h.p, rho_all.data(), rho_all.size() * 8, cudaMemcpyHostToDevice, st),
+                "batch dir");
+            BCK(cudaMemcpyAsync(b->act.p, need_dir.data(), need_dir.size() * sizeof(int), cudaMemcpyHostToDevice, st),
+                "batch dir");
+            k_batch_two_loop<<<(unsigned)need_dir.size(), 1024, 0, st>>>(b->dinst.p, b->act.p, b->dhist.p, b->S.p,
+                                                                         b->Y.p, b->rho_h.p, b->grad.p, b->pdir.p,
+                                                                         b->psi.p, b->x0.p, b->g0.p, b->outv.p);
+            BCK(cudaMemcpyAsync(out_h.data(), b->outv.p, np * 8, cudaMemcpyDeviceToHost, st), "batch dir");
+            BCK(cudaStreamSynchronize(st), "batch dir");
+            for (int p : need_dir) {
+                St &z = S[p];
+                const double g0 = out_h[p];
+                double df = z.f_prev - z.f;
+                df = std::max(df, 100. * DBL_EPSILON);
+                const double a1 = z.first_step ? 1. : std::min(1., -1.01 * 2. * df / g0);
+                if (b->verbose) printf("problem %d: direction g.p %.6e first step %.6e\n", p, g0, a1);
+                z.f_prev = z.f;
+                z.ls.begin(z.f, g0, a1);
+                z.ph = LSEARCH;
+                alpha_h[p] = z.ls.ai;
+            }
+        }
+        // trial points of every problem in a line search
+        std::vector<int> ls;
+        for (int p = 0; p < np; ++p)
+            if (S[p].ph == LSEARCH) ls.push_back(p);
+        if (!ls.empty()) {
+            int64_t maxnt = 0;
+            for (int p : ls) maxnt = std::max(maxnt, b->probs[p].nt);
+            BCK(cudaMemcpyAsync(b->alpha.p, alpha_h.data(), np * 8, cudaMemcpyHostToDevice, st), "batch axpy");
+            BCK(cudaMemcpyAsync(b->act.p, ls.data(), ls.size() * sizeof(int), cudaMemcpyHostToDevice, st), "batch axpy");
+            k_batch_axpy<<<dim3((unsigned)std::min<int64_t>((maxnt + 255) / 256, 64), (unsigned)ls.size()), 256, 0,
+                           st>>>(b->dinst.p, b->act.p, b->alpha.p, b->psi.p, b->x0.p, b->pdir.p);
+            BCK(cudaGetLastError(), "batch axpy");
+        }
+        // problems restarting a level (new eps / FP64) evaluate at psi with p = 0
+        for (int p = 0; p < np; ++p)
+            if (S[p].ph == EVAL0) {
+                const BInst &I = b->inst[p];
+                BCK(cudaMemsetAsync(b->pdir.p + I.t0, 0, I.a.nt * 8, st), "batch pdir");
+            }
+    }
+    cudaEventRecord(w1, st);
+    BCK(cudaMemcpyAsync(psi_io, b->psi.p, b->total_t * 8, cudaMemcpyDeviceToHost, st), "batch psi");
+    BCK(cudaStreamSynchronize(st), "batch solve");
+    float wall = 0.f;
+    cudaEventElapsedTime(&wall, w0, w1);
+    cudaEventDestroy(w0);
+    cudaEventDestroy(w1);
+    b->info.assign(np, sdot_solve_info{});
+    int nconv = 0;
+    sdot_status first_err = SDOT_OK;
+    for (int p = 0; p < np; ++p) {
+        sdot_solve_info &r = b->info[p];
+        r.iterations = S[p].k_total;
+        r.converged = S[p].conv == 1 && S[p].err == SDOT_OK;
+        r.n_evaluations = S[p].evals;
+        r.last_value = S[p].f;
+        r.last_check_value = S[p].check;
+        r.total_pairs = S[p].pairs;
+        r.device_ms = 0.0;
+        nconv += r.converged;
+        if (S[p].err != SDOT_OK && first_err == SDOT_OK) first_err = S[p].err;
+    }
+    if (info) {
+        info->n_problems = np;
+        info->converged = nconv;
+        info->rounds = rounds;
+        info->evaluations = evals;
+        info->total_pairs = pairs;
+        info->eval_ms = dev_ms;
+        info->solve_ms = wall;
+    }
+    if (first_err != SDOT_OK)
+        return berr(b, first_err, "a batched problem's line search failed (see sdot_batch_problem_info)");
+    return SDOT_OK;
+}
+
+sdot_status sdot_batch_problem_info(const sdot_batch *b, int index, sdot_solve_info *info)
+{
+    if (!b || !info || index < 0 || index >= (int)b->info.size()) return SDOT_EINVAL;
+    *info = b->info[index];
+    return SDOT_OK;
+}
+
+}  // extern "C"

@@ -179,8 +179,8 @@ __device__ __forceinline__ void lse_update(double b, double nu, double &M, doubl
     S = fma(nu, exp2_16(u, tab), S);
 }
 
-// Block-level ordered sum of (value, C, skipped, pairs) -> part[blockIdx.x*4..].
-__device__ __forceinline__ void block_partials(double v, double c, double sk, double np, double *part)
+// Block-level ordered sum of (value, C, skipped, pairs) -> out4[0..3].
+__device__ __forceinline__ void block_partials_at(double v, double c, double sk, double np, double *out4)
 {
     __shared__ double sv[32], sc[32], ss[32], sp[32];
     v = warp_sum(v);
@@ -193,11 +193,17 @@ __device__ __forceinline__ void block_partials(double v, double c, double sk, do
     if (threadIdx.x == 0) {
         double tv = 0.0, tc = 0.0, ts = 0.0, tp = 0.0;
         for (int i = 0; i < (int)(blockDim.x >> 5); ++i) { tv += sv[i]; tc += sc[i]; ts += ss[i]; tp += sp[i]; }
-        part[blockIdx.x * 4 + 0] = tv;
-        part[blockIdx.x * 4 + 1] = tc;
-        part[blockIdx.x * 4 + 2] = ts;
-        part[blockIdx.x * 4 + 3] = tp;
+        out4[0] = tv;
+        out4[1] = tc;
+        out4[2] = ts;
+        out4[3] = tp;
     }
+}
+
+// Block-level ordered sum of (value, C, skipped, pairs) -> part[blockIdx.x*4..].
+__device__ __forceinline__ void block_partials(double v, double c, double sk, double np, double *part)
+{
+    block_partials_at(v, c, sk, np, part + (int64_t)blockIdx.x * 4);
 }
 
 }  // namespace sdot

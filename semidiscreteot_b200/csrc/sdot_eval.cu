@@ -27,6 +27,7 @@
 #include <mutex>
 #include <string>
 
+#include "sdot_dense.cuh"
 #include "sdot_device.cuh"
 #include "sdot_internal.h"
 
@@ -124,88 +125,13 @@ __global__ void k_target_prep_kd(int64_t nt, const double *__restrict__ y, const
     }
 }
 
-// ---------------------------------------------------------------------------
-// value sweep, dense: thread <-> DENSE_A_QT quadrature points, all targets
-// streamed through shared memory (broadcast reads).
-// ---------------------------------------------------------------------------
-
-constexpr int DA_CHUNK = 256;
-
 template <int DIM>
 __global__ void __launch_bounds__(DENSE_A_THREADS)
 k_value_dense(const double *__restrict__ x, const double *__restrict__ rho, const double *__restrict__ jxw,
               const double *__restrict__ tpack, EvalArgs a, double *__restrict__ Lq, double *__restrict__ part)
 {
-    constexpr int QT = DENSE_A_QT;
-    constexpr int TS = DIM + 2;  // A, B(DIM), nu
-    __shared__ double tab[16];
-    __shared__ double stg[DA_CHUNK * TS];
-    if (threadIdx.x < 16) tab[threadIdx.x] = c_exp2_tab[threadIdx.x];
-
-    const int64_t qbase = (int64_t)blockIdx.x * (DENSE_A_THREADS * QT) + threadIdx.x;
-    double xt[QT][DIM], M[QT], S[QT], mx[QT];
-#pragma unroll
-    for (int k = 0; k < QT; ++k) {
-        const int64_t q = qbase + (int64_t)k * DENSE_A_THREADS;
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) xt[k][d] = (q < a.nq) ? x[q * DIM + d] - a.o[d] : 0.0;
-        M[k] = -CUDART_INF;
-        S[k] = 0.0;
-        mx[k] = -CUDART_INF;
-    }
-    for (int64_t c0 = 0; c0 < a.nt; c0 += DA_CHUNK) {
-        const int cn = (int)min((int64_t)DA_CHUNK, a.nt - c0);
-        __syncthreads();
-        for (int i = threadIdx.x; i < cn * TS; i += DENSE_A_THREADS) {
-            const int t = i / TS, f = i - t * TS;
-            stg[i] = tpack[(c0 + t) * TPACK + f];
-        }
-        __syncthreads();
-#pragma unroll 2
-        for (int t = 0; t < cn; ++t) {
-            const double *tp = stg + t * TS;
-            const double A = tp[0];
-            double B[DIM];
-#pragma unroll
-            for (int d = 0; d < DIM; ++d) B[d] = tp[1 + d];
-            const double nuj = tp[1 + DIM];
-#pragma unroll
-            for (int k = 0; k < QT; ++k) {
-                double b = fma(B[0], xt[k][0], A);
-#pragma unroll
-                for (int d = 1; d < DIM; ++d) b = fma(B[d], xt[k][d], b);
-                lse_update(b, nuj, M[k], S[k], mx[k], tab);
-            }
-        }
-    }
-    double tv = 0.0, tc = 0.0, ts = 0.0;
-#pragma unroll
-    for (int k = 0; k < QT; ++k) {
-        const int64_t q = qbase + (int64_t)k * DENSE_A_THREADS;
-        if (q < a.nq) {
-            double xsq = 0.0;
-#pragma unroll
-            for (int d = 0; d < DIM; ++d) xsq += xt[k][d] * xt[k][d];
-            const double Cq = -a.halfs * xsq;
-            const double Sref = (mx[k] == -CUDART_INF) ? 0.0 : S[k] * exp2_16(M[k] - mx[k], tab);
-            double v, cv, L;
-            int sk;
-            value_epilogue(a, mx[k], Sref, Cq, rho[q], jxw[q], v, cv, L, sk);
-            Lq[q] = L;
-            tv += v;
-            tc += cv;
-            ts += sk;
-        }
-    }
-    block_partials(tv, tc, ts, 0.0, part);
+    dense_value_block<DIM>(x, rho, jxw, tpack, a, blockIdx.x, Lq, part + (int64_t)blockIdx.x * 4);
 }
-
-// ---------------------------------------------------------------------------
-// gradient sweep, dense: thread <-> DENSE_B_TT targets, q-slices streamed
-// through shared memory (broadcast reads); FP64 partial per (slice, target).
-// ---------------------------------------------------------------------------
-
-constexpr int DB_CHUNK = 256;
 
 template <int DIM, bool FP32>
 __global__ void __launch_bounds__(DENSE_B_THREADS)
@@ -213,166 +139,7 @@ k_grad_dense(const double *__restrict__ x, const double *__restrict__ w, const d
              const double *__restrict__ tpack, const double *__restrict__ psi, EvalArgs a, int64_t qslice,
              double *__restrict__ gpart)
 {
-    constexpr int TT = DENSE_B_TT;
-    constexpr int TB = DENSE_B_THREADS * TT;
-    __shared__ double tab[16];
-    __shared__ double red[2][32];
-    __shared__ __align__(16) double stgd[FP32 ? 1 : DB_CHUNK * (DIM + 2)];
-    __shared__ __align__(16) float stgf[FP32 ? DB_CHUNK * 4 : 1];
-    __shared__ float stgw[FP32 ? DB_CHUNK : 1];
-    if (threadIdx.x < 16) tab[threadIdx.x] = c_exp2_tab[threadIdx.x];
-    const int tid = threadIdx.x;
-    const int64_t j0 = (int64_t)blockIdx.x * TB;
-    const int64_t qa = (int64_t)blockIdx.y * qslice;
-    const int64_t qb = min(a.nq, qa + qslice);
-
-    // per-target data and the block centring (FP32 path)
-    double ob[3] = {0.0, 0.0, 0.0};
-    double aref = 0.0;
-    float yt[TT][3], alpha[TT];
-    double A[TT], B[TT][3], acc64[TT];
-    bool has[TT];
-    if (FP32) {
-        double lo[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, hi[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
-        double amax = -DBL_MAX;
-#pragma unroll
-        for (int k = 0; k < TT; ++k) {
-            const int64_t j = j0 + tid + k * DENSE_B_THREADS;
-            if (j < a.nt) {
-                const double *tp = tpack + j * TPACK;
-#pragma unroll
-                for (int d = 0; d < DIM; ++d) {
-                    lo[d] = fmin(lo[d], tp[2 + DIM + d]);
-                    hi[d] = fmax(hi[d], tp[2 + DIM + d]);
-                }
-                const double al = log2(tp[1 + DIM]) + a.l2e_eps * psi[j];
-                if (al > amax) amax = al;
-            }
-        }
-        // block reductions (lo/hi/amax) through shared memory
-        __shared__ double sred[7][DENSE_B_THREADS / 32];
-        for (int o = 16; o > 0; o >>= 1) {
-#pragma unroll
-            for (int d = 0; d < DIM; ++d) {
-                lo[d] = fmin(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
-                hi[d] = fmax(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
-            }
-            amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
-        }
-        if ((tid & 31) == 0) {
-#pragma unroll
-            for (int d = 0; d < DIM; ++d) { sred[d][tid >> 5] = lo[d]; sred[3 + d][tid >> 5] = hi[d]; }
-            sred[6][tid >> 5] = amax;
-        }
-        __syncthreads();
-        for (int i = 0; i < DENSE_B_THREADS / 32; ++i) {
-#pragma unroll
-            for (int d = 0; d < DIM; ++d) { lo[d] = fmin(lo[d], sred[d][i]); hi[d] = fmax(hi[d], sred[3 + d][i]); }
-            amax = fmax(amax, sred[6][i]);
-        }
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) ob[d] = 0.5 * (lo[d] + hi[d]);
-        aref = (amax > -DBL_MAX && isfinite(amax)) ? amax : 0.0;
-    }
-#pragma unroll
-    for (int k = 0; k < TT; ++k) {
-        const int64_t j = j0 + tid + k * DENSE_B_THREADS;
-        has[k] = j < a.nt;
-        acc64[k] = 0.0;
-        const double *tp = tpack + (has[k] ? j : 0) * TPACK;
-        if (FP32) {
-#pragma unroll
-            for (int d = 0; d < 3; ++d) yt[k][d] = (d < DIM && has[k]) ? (float)(tp[2 + DIM + d] - ob[d]) : 0.f;
-            alpha[k] = has[k] ? (float)(log2(tp[1 + DIM]) + a.l2e_eps * psi[j] - aref) : -INFINITY;
-        } else {
-            A[k] = tp[0];
-#pragma unroll
-            for (int d = 0; d < DIM; ++d) B[k][d] = tp[1 + d];
-        }
-    }
-    const float c32 = (float)a.c32;
-    for (int64_t c0 = qa; c0 < qb; c0 += DB_CHUNK) {
-        const int cn = (int)min((int64_t)DB_CHUNK, qb - c0);
-        __syncthreads();
-        for (int i = tid; i < cn; i += DENSE_B_THREADS) {
-            const int64_t q = c0 + i;
-            double xt[3];
-            double xsq = 0.0;
-            if (FP32) {
-#pragma unroll
-                for (int d = 0; d < DIM; ++d) xt[d] = x[q * DIM + d] - ob[d];
-                const double beta = -LOG2E * Lq[q] + aref;
-                float4 v;
-                v.x = (float)xt[0];
-                v.y = (float)xt[1];
-                v.z = DIM == 3 ? (float)xt[2] : (float)beta;
-                v.w = DIM == 3 ? (float)beta : 0.f;
-                reinterpret_cast<float4 *>(stgf)[i] = v;
-                stgw[i] = (float)w[q];
-            } else {
-#pragma unroll
-                for (int d = 0; d < DIM; ++d) {
-                    xt[d] = x[q * DIM + d] - a.o[d];
-                    xsq += xt[d] * xt[d];
-                    stgd[i * (DIM + 2) + d] = xt[d];
-                }
-                stgd[i * (DIM + 2) + DIM] = -a.halfs * xsq - KAPPA * Lq[q];
-                stgd[i * (DIM + 2) + DIM + 1] = w[q];
-            }
-        }
-        __syncthreads();
-        if (FP32) {
-            float acc[TT];
-#pragma unroll
-            for (int k = 0; k < TT; ++k) acc[k] = 0.f;
-            int t = 0;
-            for (; t < cn; ++t) {
-                const float4 v = reinterpret_cast<const float4 *>(stgf)[t];
-                const float beta = DIM == 3 ? v.w : v.z;
-                const float wq = stgw[t];
-#pragma unroll
-                for (int k = 0; k < TT; ++k) {
-                    const float d0 = v.x - yt[k][0], d1 = v.y - yt[k][1];
-                    float d2 = d0 * d0;
-                    d2 = fmaf(d1, d1, d2);
-                    if (DIM == 3) {
-                        const float dz = v.z - yt[k][2];
-                        d2 = fmaf(dz, dz, d2);
-                    }
-                    const float e = fmaf(-c32, d2, alpha[k] + beta);
-                    acc[k] = fmaf(wq, ex2_approx(e), acc[k]);
-                }
-                if ((t & 7) == 7) {
-#pragma unroll
-                    for (int k = 0; k < TT; ++k) { acc64[k] += (double)acc[k]; acc[k] = 0.f; }
-                }
-            }
-#pragma unroll
-            for (int k = 0; k < TT; ++k) acc64[k] += (double)acc[k];
-        } else {
-            for (int t = 0; t < cn; ++t) {
-                const double *v = stgd + t * (DIM + 2);
-                const double D = v[DIM], wq = v[DIM + 1];
-#pragma unroll
-                for (int k = 0; k < TT; ++k) {
-                    double u = fma(B[k][0], v[0], A[k] + D);
-#pragma unroll
-                    for (int d = 1; d < DIM; ++d) u = fma(B[k][d], v[d], u);
-                    acc64[k] = fma(wq, exp2_16(u, tab), acc64[k]);
-                }
-            }
-        }
-    }
-#pragma unroll
-    for (int k = 0; k < TT; ++k) {
-        const int64_t j = j0 + tid + k * DENSE_B_THREADS;
-        if (j < a.nt) {
-            double g = acc64[k];
-            if (!FP32) g *= tpack[j * TPACK + 1 + DIM];  // nu_j (FP32 path folds it into alpha)
-            gpart[(int64_t)blockIdx.y * a.nt + j] = g;
-        }
-    }
-    (void)red;
+    dense_grad_block<DIM, FP32>(x, w, Lq, tpack, psi, a, qslice, blockIdx.x, blockIdx.y, gpart);
 }
 
 // ---------------------------------------------------------------------------
