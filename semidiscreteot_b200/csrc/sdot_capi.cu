@@ -505,6 +505,40 @@ sdot_status sdot_set_source(sdot_ctx *c, int dim, int64_t n_q, const double *x, 
             dmax = std::max(dmax, std::sqrt(s2));
         }
     c->delta_max = dmax;
+    // Tensor-product points about the cell centre (Gauss rules on axis-aligned
+    // cells): point i = i_0 + m i_1 + m^2 i_2 of a cell has offsets
+    // (o_0[i_0], o_1[i_1], o_2[i_2]) from the centre, the same coordinate for
+    // every point with the same digit, and o_d[m-1-k] = -o_d[k].  The
+    // truncated sweeps then factor 2^(G.delta) per dimension.
+    int tm = 0;
+    double amax = 0.0;
+    for (int m = 2; m <= 3 && tm == 0; ++m) {
+        int64_t p = 1;
+        for (int d = 0; d < dim; ++d) p *= m;
+        if (p != qpc || ngroups != 1) continue;
+        bool ok = true;
+        const double tol = 1e-12 * std::max(dmax, 1e-300);
+        for (int64_t k = 0; k < n_cells && ok; ++k) {
+            const double *X = &hx[k * qpc * dim];
+            const double *C = &hc[k * dim];
+            int64_t stride = 1;
+            for (int d = 0; d < dim && ok; ++d, stride *= m) {
+                double o[3];
+                for (int i = 0; i < m; ++i) o[i] = X[(i * stride) * dim + d] - C[d];
+                for (int i = 0; i < m && ok; ++i)
+                    if (std::fabs(o[i] + o[m - 1 - i]) > tol || (i < m - 1 && !(o[i] < o[i + 1]))) ok = false;
+                for (int64_t q = 0; q < qpc && ok; ++q) {
+                    const int64_t dig = (q / stride) % m;
+                    if (X[q * dim + d] != X[(dig * stride) * dim + d]) ok = false;
+                }
+                amax = std::max(amax, std::fabs(o[m - 1]));
+            }
+        }
+        if (ok) tm = m;
+        else amax = 0.0;
+    }
+    c->tensor_m = tm;
+    c->tensor_amax = amax;
     const int64_t nsblk = (int64_t)bounds.size() - 1;
     std::vector<double> ssph(nsblk * 4);
     for (int64_t b = 0; b < nsblk; ++b) {

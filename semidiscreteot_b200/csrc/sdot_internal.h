@@ -133,6 +133,8 @@ struct sdot_ctx {
     double diam = 0;                   // diameter bound of cells U targets
     double coord_scale = 1.0;          // max |coordinate|, for FP32 cull margins
     double delta_max = 0.0;            // max distance of a quadrature point to its cell centre
+    int tensor_m = 0;                  // > 0: points form an m^dim tensor grid symmetric about the cell centre
+    double tensor_amax = 0.0;          // largest per-dimension offset of that grid
 
     // ---- truncated path: block-pair lists and gradient partials ----
     sdot::DevBuf<int64_t> fwd_cnt, fwd_off, inv_cnt, inv_off, fwd2inv;

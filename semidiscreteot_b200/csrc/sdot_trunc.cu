@@ -55,6 +55,7 @@ constexpr int FT_TS = 6;                    // doubles per staged target: y(3), 
 constexpr int FT_MAXT = 96;                 // target blocks per chunk
 constexpr int FT_MAXQ = 80;                 // quadrature points of one source block
 constexpr int SUPER = 32;                   // blocks per super-block of the pair-list hierarchy
+constexpr int FT_PREF = 192;                // forward entries of a block prefetched into smem
 
 struct FusedArgs {
     const double *x, *rho, *jxw, *w, *cell_ctr;
@@ -83,6 +84,7 @@ struct FTSmem {
     double qL[FT_MAXQ];           // L_q of the block
     __align__(16) float qb[FT_MAXQ][4];  // pass B: delta (3) as float, D_q (+ log2 w_q)
     float qw[FT_MAXQ];            // pass B: w_q
+    float qtw[FT_MAXQ];           // pass B, tensor path: w_q 2^(D_q)
     double cellc[FT_WARPS][3];    // centre of each cell of the block
     float pvw[FT_WARPS][FT_MAXS]; // gradient partial of each unit (warp) per staged target (FP32 mode)
     unsigned short cand[FT_WARPS][FT_MAXS];
@@ -94,6 +96,9 @@ struct FTSmem {
     int eacc, etot;
     int wcount[FT_WARPS];
     int nstg;
+    int ent_t[FT_PREF];            // forward entries of the block: target block,
+    int ent_j0[FT_PREF];           // its first target
+    unsigned char ent_sz[FT_PREF]; // and its size (prefetched once per block)
 };
 
 // Partial rows of the gradient sweep: FP32 in the hybrid mode (inside
@@ -299,8 +304,8 @@ __global__ void __launch_bounds__(1024) k_scan(const int64_t *__restrict__ cnt, 
 // accepted in list order while the staged total fits FT_MAXS.  Returns the
 // number of forward entries consumed; staged order = (target block, slot).
 template <int DIM>
-__device__ int stage_chunk(FTSmem &sm, const FusedArgs &f, int64_t k0, int64_t k1, const double *bc, double rcull2,
-                           bool for_b)
+__device__ int stage_chunk(FTSmem &sm, const FusedArgs &f, int64_t kb, int64_t k0, int64_t k1, const double *bc,
+                           double rcull2, bool for_b)
 {
     constexpr int SUB = 4;                       // target blocks per warp per iteration
     constexpr int PER = FT_WARPS * SUB;          // entries examined per iteration
@@ -310,18 +315,29 @@ __device__ int stage_chunk(FTSmem &sm, const FusedArgs &f, int64_t k0, int64_t k
     while (k < k1 && nb < FT_MAXT) {
         unsigned bal[SUB];
         int tt[SUB];
+        int64_t jj[SUB];
 #pragma unroll
         for (int s = 0; s < SUB; ++s) {
             const int idx = s * FT_WARPS + wp;
             const int64_t e = k + idx;
             bal[s] = 0u;
             tt[s] = -1;
+            jj[s] = 0;
             int cntv = -1;
             if (e < k1 && nb + idx < FT_MAXT) {
-                const int t = f.fwd_t[e];
+                int t, sz;
+                int64_t j0;
+                if (e - kb < FT_PREF) {
+                    t = sm.ent_t[e - kb];
+                    j0 = sm.ent_j0[e - kb];
+                    sz = sm.ent_sz[e - kb];
+                } else {
+                    t = f.fwd_t[e];
+                    j0 = f.tblk_off[t];
+                    sz = (int)(f.tblk_off[t + 1] - j0);
+                }
                 tt[s] = t;
-                const int64_t j0 = f.tblk_off[t];
-                const int sz = (int)(f.tblk_off[t + 1] - j0);
+                jj[s] = j0;
                 bool keep = false;
                 if (lane < sz) {
                     const double *tp = f.tpk + (j0 + lane) * TPACK;
@@ -367,7 +383,7 @@ __device__ int stage_chunk(FTSmem &sm, const FusedArgs &f, int64_t k0, int64_t k
             const int idx = s * FT_WARPS + wp;
             if (idx < nacc) {
                 const int slot = nb + idx;
-                const int64_t j0 = f.tblk_off[tt[s]];
+                const int64_t j0 = jj[s];
                 const bool keep = (bal[s] >> lane) & 1u;
                 short pos = -1;
                 if (keep) {
@@ -479,19 +495,27 @@ template <int DIM>
 __device__ __forceinline__ int compact_candidates(FTSmem &sm, int wp, int lane, int nstg, const double *cc,
                                                   const EvalArgs &a, double &bmax)
 {
+    constexpr int U = 4;  // staged targets per lane in flight (independent distance chains)
     int ncand = 0;
     bmax = -CUDART_INF;
-    for (int b0 = 0; b0 < nstg; b0 += 32) {
-        const int t = b0 + lane;
-        bool in = false;
-        if (t < nstg) {
-            const double d2 = stg_dist2<DIM>(sm, t, cc);
-            in = d2 <= a.sstar;
-            if (in) bmax = fmax(bmax, fma(-a.halfs, d2, sm.stg[5][t]));
+    for (int b0 = 0; b0 < nstg; b0 += 32 * U) {
+        bool in[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int t = b0 + 32 * u + lane;
+            in[u] = false;
+            if (t < nstg) {
+                const double d2 = stg_dist2<DIM>(sm, t, cc);
+                in[u] = d2 <= a.sstar;
+                if (in[u]) bmax = fmax(bmax, fma(-a.halfs, d2, sm.stg[5][t]));
+            }
         }
-        const unsigned bal = __ballot_sync(0xffffffffu, in);
-        if (in) sm.cand[wp][ncand + __popc(bal & ((1u << lane) - 1u))] = (unsigned short)t;
-        ncand += __popc(bal);
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const unsigned bal = __ballot_sync(0xffffffffu, in[u]);
+            if (in[u]) sm.cand[wp][ncand + __popc(bal & ((1u << lane) - 1u))] = (unsigned short)(b0 + 32 * u + lane);
+            ncand += __popc(bal);
+        }
     }
     bmax = warp_max(bmax);
     __syncwarp();
@@ -568,6 +592,144 @@ __device__ __forceinline__ void grad_pairs(FTSmem &sm, const FusedArgs &f, int w
     }
 }
 
+// Tensor-product points (TM per dimension, symmetric about the cell centre):
+// delta_q = (s_0 a_0, s_1 a_1, s_2 a_2) with s_d in {-1, 0, +1}, so
+// 2^(b_qj/16) = nu_j 2^(B0_Kj/16) prod_d 2^(s_d G_Kj,d a_d/16) and one
+// candidate costs 1 + DIM exponentials and DIM reciprocals for its TM^DIM
+// points.  Sums stay relative to Munit (LSE mode only).
+template <int TM, int D>
+__device__ __forceinline__ constexpr int tstride()
+{
+    return D == 0 ? 1 : (D == 1 ? TM : TM * TM);
+}
+
+// The per-q maximum exponent (the reference's m of the log-sum-exp, which
+// C_global depends on) is taken exactly, as in value_pairs, but only over the
+// candidates that can attain it: b_qj lies within s r |delta|max of B0_Kj, so
+// a candidate with B0 below (running max B0) - 2 s r |delta|max is never a
+// maximum; thr is that bound relative to Munit.
+template <int DIM, int TM>
+__device__ __forceinline__ void value_pairs_tensor(const FTSmem &sm, int wp, int lane, int ncand, int qoff,
+                                                   const double *cc, const EvalArgs &a, double Munit, double thr,
+                                                   double *S, double *mx)
+{
+    constexpr int NQ = DIM == 3 ? TM * TM * TM : TM * TM;
+    double ah[3];
+    ah[0] = sm.qd[qoff + (TM - 1) * tstride<TM, 0>()][0];
+    ah[1] = sm.qd[qoff + (TM - 1) * tstride<TM, 1>()][1];
+    ah[2] = DIM == 3 ? sm.qd[qoff + (TM - 1) * tstride<TM, 2>()][2] : 0.0;
+    for (int p = lane; p < ncand; p += 32) {
+        const int ti = sm.cand[wp][p];
+        const double g0 = sm.stg[0][ti] - cc[0], g1 = sm.stg[1][ti] - cc[1];
+        const double g2 = DIM == 3 ? sm.stg[2][ti] - cc[2] : 0.0;
+        const double d2 = DIM == 3 ? g0 * g0 + g1 * g1 + g2 * g2 : g0 * g0 + g1 * g1;
+        const double B0 = fma(-a.halfs, d2, sm.stg[5][ti]) - Munit;
+        const double P = sm.stg[3][ti] * exp2_16(B0, sm.tab);
+        const double G[3] = {a.s * g0, a.s * g1, a.s * g2};
+        if (B0 >= thr) {
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) {
+                const double *dq = sm.qd[qoff + q];
+                double bb = fma(G[0], dq[0], B0);
+                bb = fma(G[1], dq[1], bb);
+                if (DIM == 3) bb = fma(G[2], dq[2], bb);
+                mx[q] = fmax(mx[q], bb);
+            }
+        }
+        double F[3][TM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            const double xp = exp2_16(G[d] * ah[d], sm.tab);
+            F[d][0] = __drcp_rn(xp);
+            F[d][TM - 1] = xp;
+            if (TM == 3) F[d][1] = 1.0;
+        }
+#pragma unroll
+        for (int i0 = 0; i0 < TM; ++i0) {
+            const double t0 = P * F[0][i0];
+            if (DIM == 2) {
+#pragma unroll
+                for (int i1 = 0; i1 < TM; ++i1) S[i0 + TM * i1] = fma(t0, F[1][i1], S[i0 + TM * i1]);
+            } else {
+#pragma unroll
+                for (int i1 = 0; i1 < TM; ++i1) {
+                    const double t1 = t0 * F[1][i1];
+#pragma unroll
+                    for (int i2 = 0; i2 < TM; ++i2) {
+                        const int q = i0 + TM * i1 + TM * TM * i2;
+                        S[q] = fma(t1, F[2][i2], S[q]);
+                    }
+                }
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ float rcp_approx(float x)
+{
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// FP32 gradient sweep on tensor-product points: per candidate
+// 2^(e0) sum_q W_q prod_d F_d[i_d], W_q = w_q 2^(D_q), summed dimension by
+// dimension (Horner order), into the warp's partial row.
+template <int DIM, int TM>
+__device__ __forceinline__ void grad_pairs_tensor(FTSmem &sm, int wp, int lane, int ncand, int qoff,
+                                                  const double *cc, double Lref, const EvalArgs &a)
+{
+    constexpr int NQ = DIM == 3 ? TM * TM * TM : TM * TM;
+    const float sf = (float)(a.s * (1.0 / 16.0));
+    float ah[3];
+    ah[0] = (float)sm.qd[qoff + (TM - 1) * tstride<TM, 0>()][0];
+    ah[1] = (float)sm.qd[qoff + (TM - 1) * tstride<TM, 1>()][1];
+    ah[2] = DIM == 3 ? (float)sm.qd[qoff + (TM - 1) * tstride<TM, 2>()][2] : 0.f;
+    float W[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) W[q] = sm.qtw[qoff + q];
+    for (int p = lane; p < ncand; p += 32) {
+        const int ti = sm.cand[wp][p];
+        const double g0 = sm.stg[0][ti] - cc[0], g1 = sm.stg[1][ti] - cc[1];
+        const double g2 = DIM == 3 ? sm.stg[2][ti] - cc[2] : 0.0;
+        const double d2 = DIM == 3 ? g0 * g0 + g1 * g1 + g2 * g2 : g0 * g0 + g1 * g1;
+        const float e0 = (float)(sm.stg[4][ti] + (fma(-a.halfs, d2, sm.stg[5][ti]) - KAPPA * Lref) * (1.0 / 16.0));
+        const float gd[3] = {(float)g0, (float)g1, (float)g2};
+        float F[3][TM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            const float xp = ex2_approx(sf * gd[d] * ah[d]);
+            F[d][0] = rcp_approx(xp);
+            F[d][TM - 1] = xp;
+            if (TM == 3) F[d][1] = 1.f;
+        }
+        float w = 0.f;
+        if (DIM == 2) {
+#pragma unroll
+            for (int i0 = 0; i0 < TM; ++i0) {
+                float u = 0.f;
+#pragma unroll
+                for (int i1 = 0; i1 < TM; ++i1) u = fmaf(W[i0 + TM * i1], F[1][i1], u);
+                w = fmaf(u, F[0][i0], w);
+            }
+        } else {
+#pragma unroll
+            for (int i0 = 0; i0 < TM; ++i0) {
+                float u = 0.f;
+#pragma unroll
+                for (int i1 = 0; i1 < TM; ++i1) {
+                    float v = 0.f;
+#pragma unroll
+                    for (int i2 = 0; i2 < TM; ++i2) v = fmaf(W[i0 + TM * i1 + TM * TM * i2], F[2][i2], v);
+                    u = fmaf(v, F[1][i1], u);
+                }
+                w = fmaf(u, F[0][i0], w);
+            }
+        }
+        partial_rows<true>(sm)[wp * FT_MAXS + ti] = ex2_approx(e0) * w;
+    }
+}
+
 // CTA sum of the warp partial rows (warp order) and the write of every slot
 // of every pair of the chunk (zeros where a target was not staged).
 template <bool FP32B>
@@ -587,7 +749,7 @@ __device__ __forceinline__ void write_partials(FTSmem &sm, const FusedArgs &f, i
     }
 }
 
-template <int DIM, int QL, bool FP32B, int MODE>
+template <int DIM, int QL, bool FP32B, int MODE, int TQ>
 __global__ void __launch_bounds__(FT_WARPS * 32, 2)
 k_fused(FusedArgs f, EvalArgs a)
 {
@@ -610,9 +772,17 @@ k_fused(FusedArgs f, EvalArgs a)
     const double bc[3] = {bs[0], bs[1], bs[2]};
     const double rc = (f.cullt + bs[3]) * (1.0 + 1e-12) + 1e-300;
     const double rcull2 = rc * rc;
+    const int64_t k0 = f.fwd_off[b], k1 = f.fwd_off[b + 1];
     for (int i = tid; i < ncell * 3; i += blockDim.x) {
         const int c = i / 3, d = i - c * 3;
         sm.cellc[c][d] = d < DIM ? f.cell_ctr[(cb0 + c) * DIM + d] : 0.0;
+    }
+    for (int i = tid; i < (int)min((int64_t)FT_PREF, k1 - k0); i += blockDim.x) {
+        const int t = f.fwd_t[k0 + i];
+        const int64_t j0 = f.tblk_off[t];
+        sm.ent_t[i] = t;
+        sm.ent_j0[i] = (int)j0;
+        sm.ent_sz[i] = (unsigned char)(f.tblk_off[t + 1] - j0);
     }
     __syncthreads();
     for (int i = tid; i < nqb; i += blockDim.x) {
@@ -629,7 +799,6 @@ k_fused(FusedArgs f, EvalArgs a)
     }
     __syncthreads();
     const double cc[3] = {sm.cellc[cl][0], sm.cellc[cl][1], sm.cellc[cl][2]};
-    const int64_t k0 = f.fwd_off[b], k1 = f.fwd_off[b + 1];
     int chunks = 0;
     int64_t single_end = -1;  // end of the only chunk, when everything fit in one
     int ncand_single = 0;
@@ -650,9 +819,10 @@ k_fused(FusedArgs f, EvalArgs a)
         double dqmax = 0.0;
         for (int q = 0; q < nql; ++q) dqmax = fmax(dqmax, sm.qn[qoff + q]);
         double npairs = 0.0;
+        double bmax_run = -CUDART_INF;  // largest B0 of the candidates so far
         const double sr = a.s * a.cull;
         for (int64_t k = k0; k < k1;) {
-            const int nt = stage_chunk<DIM>(sm, f, k, k1, bc, rcull2, f.do_b != 0);
+            const int nt = stage_chunk<DIM>(sm, f, k0, k, k1, bc, rcull2, f.do_b != 0);
             const int nstg = sm.nstg;
             ++chunks;
             if (valid) {
@@ -674,7 +844,11 @@ k_fused(FusedArgs f, EvalArgs a)
                         Munit = mnew;
                     }
                 }
-                if (nql == QL)
+                if (bmax > bmax_run) bmax_run = bmax;
+                if constexpr (TQ > 0)
+                    value_pairs_tensor<DIM, TQ>(sm, wp, lane, ncand, qoff, cc, a, Munit,
+                                                bmax_run - 2.0 * sr * dqmax - Munit, S, mx);
+                else if (nql == QL)
                     value_pairs<DIM, QL, QL, MODE>(sm, wp, lane, ncand, qoff, cc[0], cc[1], cc[2], a, Munit, M, S, mx);
                 else
                     value_pairs_partial<DIM, QL, MODE>(sm, wp, lane, ncand, qoff, nql, cc[0], cc[1], cc[2], a, Munit,
@@ -740,6 +914,7 @@ k_fused(FusedArgs f, EvalArgs a)
             sm.qb[i][2] = (float)sm.qd[i][2];
             sm.qb[i][3] = (float)(f.w_nonneg ? D + log2(wq) : D);  // w_q folded in: p = 2^e directly
             sm.qw[i] = (float)wq;
+            if (TQ > 0) sm.qtw[i] = (float)(wq * exp2(D));
         }
         __syncwarp();
     }
@@ -750,7 +925,10 @@ k_fused(FusedArgs f, EvalArgs a)
         if (valid) {
             for (int t = lane; t < nstg; t += 32) partial_rows<FP32B>(sm)[wp * FT_MAXS + t] = 0;
             __syncwarp();
-            if (isfinite(Lref)) grad_pairs<DIM, FP32B>(sm, f, wp, lane, ncand_single, qoff, nql, cc, Lref, qblk0, a);
+            if (isfinite(Lref)) {
+                if constexpr (TQ > 0 && FP32B) grad_pairs_tensor<DIM, TQ>(sm, wp, lane, ncand_single, qoff, cc, Lref, a);
+                else grad_pairs<DIM, FP32B>(sm, f, wp, lane, ncand_single, qoff, nql, cc, Lref, qblk0, a);
+            }
         }
         if (tid < nt) {
             const int tb = sm.ctb[tid];
@@ -762,14 +940,17 @@ k_fused(FusedArgs f, EvalArgs a)
         return;
     }
     for (int64_t k = k0; k < k1;) {
-        const int nt = stage_chunk<DIM>(sm, f, k, k1, bc, rcull2, true);
+        const int nt = stage_chunk<DIM>(sm, f, k0, k, k1, bc, rcull2, true);
         const int nstg = sm.nstg;
         if (valid) {
             double bmax;
             const int ncand = compact_candidates<DIM>(sm, wp, lane, nstg, cc, a, bmax);
             for (int t = lane; t < nstg; t += 32) partial_rows<FP32B>(sm)[wp * FT_MAXS + t] = 0;
             __syncwarp();
-            if (isfinite(Lref)) grad_pairs<DIM, FP32B>(sm, f, wp, lane, ncand, qoff, nql, cc, Lref, qblk0, a);
+            if (isfinite(Lref)) {
+                if constexpr (TQ > 0 && FP32B) grad_pairs_tensor<DIM, TQ>(sm, wp, lane, ncand, qoff, cc, Lref, a);
+                else grad_pairs<DIM, FP32B>(sm, f, wp, lane, ncand, qoff, nql, cc, Lref, qblk0, a);
+            }
         }
         __syncthreads();
         write_partials<FP32B>(sm, f, nt, nunit);
@@ -802,18 +983,18 @@ k_grad_reduce(const int64_t *__restrict__ tblk_off, const int64_t *__restrict__ 
     }
 }
 
-template <int DIM, int QL, bool FP32B, int MODE>
+template <int DIM, int QL, bool FP32B, int MODE, int TQ>
 static void launch_fused(sdot_ctx *c, const FusedArgs &f, const EvalArgs &a, size_t smem, int nb)
 {
-    cudaFuncSetAttribute(k_fused<DIM, QL, FP32B, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_fused<DIM, QL, FP32B, MODE><<<(unsigned)nb, FT_WARPS * 32, smem, c->stream>>>(f, a);
+    cudaFuncSetAttribute(k_fused<DIM, QL, FP32B, MODE, TQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_fused<DIM, QL, FP32B, MODE, TQ><<<(unsigned)nb, FT_WARPS * 32, smem, c->stream>>>(f, a);
 }
 
-template <int DIM, int QL, int MODE>
+template <int DIM, int QL, int MODE, int TQ = 0>
 static void dispatch_fused_b(sdot_ctx *c, const FusedArgs &f, const EvalArgs &a, bool fp32b, int nb)
 {
-    if (fp32b) launch_fused<DIM, QL, true, MODE>(c, f, a, sizeof(FTSmem), nb);
-    else launch_fused<DIM, QL, false, MODE>(c, f, a, sizeof(FTSmem) + FT_ROWS64_BYTES, nb);
+    if (fp32b) launch_fused<DIM, QL, true, MODE, TQ>(c, f, a, sizeof(FTSmem), nb);
+    else launch_fused<DIM, QL, false, MODE, TQ>(c, f, a, sizeof(FTSmem) + FT_ROWS64_BYTES, nb);
 }
 
 template <int DIM, int MODE>
@@ -839,8 +1020,33 @@ static void dispatch_fused(sdot_ctx *c, const FusedArgs &f, const EvalArgs &a, b
 {
     const double gap = 2.0 * a.s * a.cull * c->delta_max;
     const double umin = -a.s * (psi_range + 0.5 * a.cull * a.cull + 2.0 * a.cull * c->delta_max);
-    if (gap >= 16.0 * 500.0) dispatch_fused_q<DIM, 2>(c, f, a, fp32b, nb);
-    else if (umin > -15000.0) dispatch_fused_q<DIM, 0>(c, f, a, fp32b, nb);
+    // tensor-product points: per-dimension factors 2^(+-G a/16) stay within
+    // 2^300 (FP64 value sweep) and 2^40 (FP32 gradient sweep)
+    const double fac = a.s * a.cull * c->tensor_amax / 16.0;
+    const bool tensor = c->tensor_m > 0 && a.lse && a.ngroups == 1 && fac <= 40.0 && umin > -15000.0 &&
+                        gap < 16.0 * 500.0;
+    if (gap >= 16.0 * 500.0) {
+        dispatch_fused_q<DIM, 2>(c, f, a, fp32b, nb);
+        return;
+    }
+    if (tensor) {
+        if constexpr (DIM == 3) {
+            if (c->tensor_m == 2 && a.ql == 8) {
+                dispatch_fused_b<3, 8, 0, 2>(c, f, a, fp32b, nb);
+                return;
+            }
+        } else {
+            if (c->tensor_m == 3 && a.ql == 9) {
+                dispatch_fused_b<2, 9, 0, 3>(c, f, a, fp32b, nb);
+                return;
+            }
+            if (c->tensor_m == 2 && a.ql == 4) {
+                dispatch_fused_b<2, 4, 0, 2>(c, f, a, fp32b, nb);
+                return;
+            }
+        }
+    }
+    if (umin > -15000.0) dispatch_fused_q<DIM, 0>(c, f, a, fp32b, nb);
     else dispatch_fused_q<DIM, 1>(c, f, a, fp32b, nb);
 }
 
