@@ -211,6 +211,22 @@ typedef struct {
 sdot_status sdot_solve_newton(sdot_ctx *ctx, double *psi, const sdot_solver_params *params, int hessian_method,
                               sdot_newton_info *info);
 
+/* Replaces SoftmaxRefinement::compute_refinement (src/solvers/SoftmaxRefinement.cc
+ * :61-280), the softmax transfer of potentials from a coarse target level to
+ * its children used by SemiDiscreteOT::assign_potentials_by_hierarchy
+ * (SemiDiscreteOT.cc:748-828).  The context's source is the source measure
+ * and its target measure (sdot_set_target) is the COARSE level; psi_coarse
+ * holds its potentials (caller order).  Fine level: n_fine points y_fine and
+ * the children of coarse target i at child_indices[child_offsets[i] ..
+ * child_offsets[i+1]) (each fine target the child of at most one coarse
+ * target).  epsilon is the regularisation (lambda), threshold the distance
+ * threshold r (the reference passes the last solve's), use_log_sum_exp the
+ * reference's flag.  psi_fine[k] = -epsilon log(sum) where the sum of
+ * contributions is positive, else 0.  Up to 32 quadrature points per cell. */
+sdot_status sdot_softmax_refinement(sdot_ctx *ctx, const double *psi_coarse, double epsilon, double threshold,
+                                    int use_log_sum_exp, int64_t n_fine, const double *y_fine,
+                                    const int64_t *child_offsets, const int64_t *child_indices, double *psi_fine);
+
 /* ---- batched solves (no single reference counterpart: many SotSolver::solve
  * calls, SotSolver.cc:105-215, each over an epsilon-scaling sequence as in
  * SemiDiscreteOT.cc:878-922, advanced together on one GPU) ----

@@ -435,7 +435,7 @@ void sdot_destroy(sdot_ctx *c)
         c->tblk_off.release(); c->tblk_sph32.release(); c->part.release(); c->fwd_t.release();
         c->fwd_cnt.release(); c->fwd_off.release(); c->shit.release(); c->spidx.release(); c->scount.release();
         c->inv_cnt.release(); c->inv_off.release(); c->inv_b.release(); c->fwd2inv.release();
-        c->pmask.release(); c->pmpre.release(); c->superpair.release(); c->ssup_sph32.release(); c->tsup_sph32.release();
+        c->pmask.release(); c->pmpre.release(); c->superpair.release(); c->superpairT.release(); c->ssup_sph32.release(); c->tsup_sph32.release();
         c->y.release(); c->nu.release();
         c->perm.release(); c->tblk_sph.release(); c->psi.release(); c->grad.release(); c->tpack.release();
         c->Lq.release(); c->gpart.release(); c->blkpart.release(); c->scal.release(); c->redpart.release();

@@ -140,7 +140,7 @@ struct sdot_ctx {
     sdot::DevBuf<int64_t> fwd_cnt, fwd_off, inv_cnt, inv_off, fwd2inv;
     sdot::DevBuf<int> fwd_t, inv_b, shit, spidx, scount, pmpre;
     sdot::DevBuf<unsigned> pmask;
-    sdot::DevBuf<unsigned char> superpair;
+    sdot::DevBuf<unsigned char> superpair, superpairT;
     sdot::DevBuf<float4> ssup_sph32, tsup_sph32;  // super-block spheres (32 blocks each)
     sdot::DevBuf<double> part;
     size_t part_cap_bytes = (size_t)4 << 30;

@@ -132,15 +132,19 @@ __device__ __forceinline__ bool pair_test(float4 s, float4 t, float cr)
 
 // Super-block pairs: sp[si * nts + ti] = 1 iff source super-block si and
 // target super-block ti may hold a pair (the same conservative test; a
-// super-sphere contains its member spheres, so no block pair is lost).
+// super-sphere contains its member spheres, so no block pair is lost).  The
+// transposed copy spt[ti * nss + si] lets the inverse-list scan read a target
+// super-block's column contiguously.
 __global__ void __launch_bounds__(256)
 k_super_pairs(const float4 *__restrict__ ssph, int nss, const float4 *__restrict__ tsph, int nts, float cr,
-              unsigned char *__restrict__ sp)
+              unsigned char *__restrict__ sp, unsigned char *__restrict__ spt)
 {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= (int64_t)nss * nts) return;
     const int si = (int)(i / nts), ti = (int)(i - (int64_t)si * nts);
-    sp[i] = pair_test(ssph[si], tsph[ti], cr) ? 1 : 0;
+    const unsigned char v = pair_test(ssph[si], tsph[ti], cr) ? 1 : 0;
+    sp[i] = v;
+    spt[(int64_t)ti * nss + si] = v;
 }
 
 // Warp <-> source super-block: its paired target super-blocks in ascending
@@ -219,7 +223,7 @@ k_fwd_fill(int nsb, int nts, int hmax, const int *__restrict__ shit, const int *
 template <bool FILL>
 __global__ void __launch_bounds__(256)
 k_inv_list(const float4 *__restrict__ sph, int nsb, int nss, const float4 *__restrict__ tph, int ntb, int nts,
-           float cr, const unsigned char *__restrict__ sp, const int64_t *__restrict__ off, int64_t *__restrict__ cnt,
+           float cr, const unsigned char *__restrict__ spt, const int64_t *__restrict__ off, int64_t *__restrict__ cnt,
            int *__restrict__ out)
 {
     const int t = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
@@ -230,7 +234,7 @@ k_inv_list(const float4 *__restrict__ sph, int nsb, int nss, const float4 *__res
     int64_t k = FILL ? off[t] : 0;
     for (int s0 = 0; s0 < nss; s0 += 32) {
         const int sl = s0 + lane;
-        unsigned sbal = __ballot_sync(0xffffffffu, sl < nss && sp[(int64_t)sl * nts + ti]);
+        unsigned sbal = __ballot_sync(0xffffffffu, sl < nss && spt[(int64_t)ti * nss + sl]);
         while (sbal) {
             const int si = s0 + __ffs(sbal) - 1;
             sbal &= sbal - 1;
@@ -1060,12 +1064,13 @@ sdot_status run_trunc(sdot_ctx *c, const EvalArgs &a, double r)
     cudaError_t e = c->fwd_cnt.alloc(nsb + 1);
     if (e == cudaSuccess) e = c->fwd_off.alloc(nsb + 1);
     if (e == cudaSuccess) e = c->superpair.alloc((size_t)nss * nts);
+    if (e == cudaSuccess) e = c->superpairT.alloc((size_t)nss * nts);
     if (e == cudaSuccess) e = c->shit.alloc((size_t)nss * nts);
     if (e == cudaSuccess) e = c->spidx.alloc((size_t)nss * nts);
     if (e == cudaSuccess) e = c->scount.alloc(nss + 1);
     if (e != cudaSuccess) return cuda_error(c, e, "pair list alloc");
     k_super_pairs<<<(unsigned)(((int64_t)nss * nts + 255) / 256), 256, 0, st>>>(c->ssup_sph32.p, nss, c->tsup_sph32.p,
-                                                                             nts, cr, c->superpair.p);
+                                                                             nts, cr, c->superpair.p, c->superpairT.p);
     k_super_compact<<<(unsigned)(((int64_t)nss * 32 + 255) / 256), 256, 0, st>>>(c->superpair.p, nss, nts, c->shit.p,
                                                                               c->scount.p, c->spidx.p);
     std::vector<int> sc((size_t)nss);
@@ -1085,7 +1090,7 @@ sdot_status run_trunc(sdot_ctx *c, const EvalArgs &a, double r)
     if (e == cudaSuccess) e = c->inv_off.alloc(ntb + 1);
     if (e != cudaSuccess) return cuda_error(c, e, "pair list alloc");
     const unsigned gt = (unsigned)(((int64_t)ntb * 32 + 255) / 256);
-    k_inv_list<false><<<gt, 256, 0, st>>>(c->sblk_sph32.p, nsb, nss, c->tblk_sph32.p, ntb, nts, cr, c->superpair.p,
+    k_inv_list<false><<<gt, 256, 0, st>>>(c->sblk_sph32.p, nsb, nss, c->tblk_sph32.p, ntb, nts, cr, c->superpairT.p,
                                           nullptr, c->inv_cnt.p, nullptr);
     k_scan<<<1, 1024, 0, st>>>(c->inv_cnt.p, ntb, c->inv_off.p);
     int64_t tot[2] = {0, 0};
@@ -1100,7 +1105,7 @@ sdot_status run_trunc(sdot_ctx *c, const EvalArgs &a, double r)
     if (e == cudaSuccess) e = c->fwd2inv.alloc(npairs + 1);
     if (e != cudaSuccess) return cuda_error(c, e, "pair list alloc");
     k_fwd_fill<<<gw, 256, 0, st>>>(nsb, nts, hmax, c->shit.p, c->scount.p, c->pmask.p, c->fwd_off.p, c->fwd_t.p);
-    k_inv_list<true><<<gt, 256, 0, st>>>(c->sblk_sph32.p, nsb, nss, c->tblk_sph32.p, ntb, nts, cr, c->superpair.p,
+    k_inv_list<true><<<gt, 256, 0, st>>>(c->sblk_sph32.p, nsb, nss, c->tblk_sph32.p, ntb, nts, cr, c->superpairT.p,
                                          c->inv_off.p, nullptr, c->inv_b.p);
     k_fwd2inv<<<gw, 256, 0, st>>>(nsb, c->fwd_off.p, c->fwd_t.p, c->inv_off.p, c->inv_b.p, c->fwd2inv.p);
     c->klaunch[6] += 9;

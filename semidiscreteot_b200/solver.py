@@ -202,6 +202,24 @@ class SotSolver:
             potential[...] = psi
         return psi
 
+    def softmax_refinement(self, potential_coarse, epsilon: float, threshold: float, y_fine, child_offsets,
+                           child_indices, use_log_sum_exp: Optional[bool] = None) -> np.ndarray:
+        """SoftmaxRefinement::compute_refinement (SoftmaxRefinement.cc:61-280): fine-level
+        potentials from this solver's targets (the coarse level) and their potentials.
+        child_offsets / child_indices: CSR children of each coarse target."""
+        psi = _f64(potential_coarse)
+        yf = _f64(y_fine).reshape(-1, self.dim)
+        co = np.ascontiguousarray(child_offsets, dtype=np.int64)
+        ci = np.ascontiguousarray(child_indices, dtype=np.int64)
+        if psi.size != self._n_targets or co.size != self._n_targets + 1:
+            raise ValueError("coarse potentials / child offsets do not match the coarse targets")
+        lse = self.current_params.use_log_sum_exp_trick if use_log_sum_exp is None else use_log_sum_exp
+        out = np.zeros(yf.shape[0])
+        self._check(self._L.sdot_softmax_refinement(self._h, psi.ctypes.data, float(epsilon), float(threshold),
+                                                    int(bool(lse)), yf.shape[0], yf.ctypes.data, co.ctypes.data,
+                                                    ci.ctypes.data, out.ctypes.data))
+        return out
+
     def compute_hessian(self, potential, hessian_out: Optional[np.ndarray] = None) -> np.ndarray:
         """Dense Hessian H = (1/eps) sum_q w_q (diag(pi_q) - pi_q pi_q^T) (declared at SotSolver.h:343-344)."""
         psi = _f64(potential)

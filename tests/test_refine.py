@@ -1,0 +1,66 @@
+"""Softmax potential transfer (SoftmaxRefinement::compute_refinement) against the oracle.
+
+Fine potentials -lambda log(sum) agree with the oracle's restatement to 1e-12
+(absolute, lambda <= 5e-2): the sums are FP64 with a different but fixed
+summation order, and the candidate sets (centre test) are bit-exact.
+"""
+import numpy as np
+import pytest
+
+from semidiscreteot_b200 import SolverParameters, SotSolver, structured_source
+
+pytestmark = pytest.mark.gpu
+
+
+def hierarchy(rng, n_coarse, dim, kids):
+    """Coarse points with `kids` children each, scattered around their parent."""
+    yc = rng.random((n_coarse, dim))
+    yf = np.clip(np.repeat(yc, kids, axis=0) + 0.02 * rng.standard_normal((n_coarse * kids, dim)), 0, 1)
+    perm = rng.permutation(n_coarse * kids)          # fine indices in shuffled order
+    inv = np.empty_like(perm)
+    inv[perm] = np.arange(perm.size)
+    yf = yf[perm]
+    co = np.arange(n_coarse + 1, dtype=np.int64) * kids
+    ci = inv.astype(np.int64)                        # children of coarse i: fine positions of rows i*kids..
+    return yc, yf, co, ci
+
+
+@pytest.mark.parametrize("dim,lse", [(2, True), (2, False), (3, True)])
+def test_refinement_matches_oracle(oracle_mod, dim, lse):
+    rng = np.random.default_rng(3 + dim)
+    src = structured_source(dim, 12 if dim == 2 else 6, 3 if dim == 2 else 2,
+                            nodal_density=lambda p: 0.5 + np.exp(-np.sum((p - 0.5) ** 2, axis=1) / 0.1))
+    yc, yf, co, ci = hierarchy(rng, 60, dim, 4)
+    nu = rng.dirichlet(np.ones(len(yc)) * 3)
+    eps = 3e-2 if lse else 5e-2
+    psi = 0.5 * eps * rng.standard_normal(len(yc))
+    s = SotSolver(dim=dim, device=0, precision="fp64")
+    s.setup_source(src["x"], src["jxw"], src["density"], src["cell_offsets"], src["cell_centers"])
+    s.setup_target(yc, nu)
+    s.configure(SolverParameters(epsilon=eps, tau=0.0, use_log_sum_exp_trick=lse))
+    P = oracle_mod.Problem(src["x"], src["jxw"], src["density"], src["cell_offsets"], src["cell_centers"], yc, nu)
+    for r in (1e300, 0.35, 0.2):
+        got = s.softmax_refinement(psi, eps, r, yf, co, ci, use_log_sum_exp=lse)
+        want = P.softmax_refinement(psi, eps, r, lse, yf, co, ci)
+        assert np.array_equal(got == 0.0, want == 0.0)
+        assert np.max(np.abs(got - want)) <= 1e-12, (r, np.max(np.abs(got - want)))
+    s.close()
+
+
+def test_refinement_rejects_bad_hierarchies():
+    rng = np.random.default_rng(0)
+    src = structured_source(2, 6, 2)
+    yc, yf, co, ci = hierarchy(rng, 10, 2, 2)
+    s = SotSolver(dim=2, device=0, precision="fp64")
+    s.setup_source(src["x"], src["jxw"], src["density"], src["cell_offsets"], src["cell_centers"])
+    s.setup_target(yc, np.full(10, 0.1))
+    s.configure(SolverParameters(epsilon=1e-2, tau=0.0))
+    bad = ci.copy()
+    bad[1] = bad[0]                                  # a fine target with two parents
+    with pytest.raises(RuntimeError, match="two coarse"):
+        s.softmax_refinement(np.zeros(10), 1e-2, 0.5, yf, co, bad)
+    bad = ci.copy()
+    bad[0] = len(yf)                                 # out of range
+    with pytest.raises(RuntimeError, match="range"):
+        s.softmax_refinement(np.zeros(10), 1e-2, 0.5, yf, co, bad)
+    s.close()
