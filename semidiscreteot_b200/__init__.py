@@ -6,12 +6,14 @@ CUDA kernels behind the C ABI in ``include/sdot.h`` (``libsdot_cuda.so``).
 """
 from .parameters import (MultilevelParameters, SolverParameters, distribute_epsilon_values, epsilon_sequence,
                          read_prm, solver_parameters_from_prm, multilevel_parameters_from_prm)
+from . import io
 from .batch import BatchSolver
+from .multilevel import build_hierarchy, run_target_multilevel
 from .server import SolveServer
 from .solver import SotSolver
 from .source import structured_source
 
 __all__ = [
-    "SotSolver", "BatchSolver", "SolveServer", "SolverParameters", "MultilevelParameters", "read_prm", "solver_parameters_from_prm",
+    "SotSolver", "BatchSolver", "SolveServer", "SolverParameters", "build_hierarchy", "run_target_multilevel", "io", "MultilevelParameters", "read_prm", "solver_parameters_from_prm",
     "multilevel_parameters_from_prm", "epsilon_sequence", "distribute_epsilon_values", "structured_source",
 ]

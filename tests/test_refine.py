@@ -64,3 +64,34 @@ def test_refinement_rejects_bad_hierarchies():
     with pytest.raises(RuntimeError, match="range"):
         s.softmax_refinement(np.zeros(10), 1e-2, 0.5, yf, co, bad)
     s.close()
+
+
+def test_target_multilevel_solve_matches_direct_solve():
+    """Coarse-to-fine solves with softmax transfer reach the direct solve's
+    potential (up to the constant shift) and start the finest level closer."""
+    from semidiscreteot_b200.multilevel import build_hierarchy, run_target_multilevel
+    rng = np.random.default_rng(5)
+    src = structured_source(2, 16, 3)
+    y = rng.random((1200, 2))
+    nu = rng.dirichlet(np.ones(1200) * 4)
+    h = build_hierarchy(y, nu, min_points=60, max_points=300, seed=1)
+    assert len(h["points"]) >= 3
+    prm = SolverParameters(epsilon=1e-2, tau=1e-10, use_log_sum_exp_trick=True, tolerance=1e-9,
+                           solver_control_type="linf", max_iterations=5000)
+    s = SotSolver(dim=2, device=0, precision="fp64")
+    s.setup_source(src["x"], src["jxw"], src["density"], src["cell_offsets"], src["cell_centers"])
+    s.configure(prm)
+    levels = run_target_multilevel(s, h, prm, use_softmax=True)
+    assert [lv["level"] for lv in levels] == list(range(len(h["points"]) - 1, -1, -1))
+    assert all(lv["converged"] for lv in levels)
+    psi_ml = levels[-1]["potentials"]
+    s.setup_target(y, nu)
+    psi_direct = s.solve(np.zeros(len(nu)), prm)
+    direct_its = s.get_last_iteration_count()
+    d = (psi_ml - psi_ml.mean()) - (psi_direct - psi_direct.mean())
+    assert np.max(np.abs(d)) <= 1e-6
+    assert levels[-1]["iterations"] < direct_its
+    # direct (parent potential) transfer also converges
+    levels2 = run_target_multilevel(s, h, prm, use_softmax=False)
+    assert levels2[-1]["converged"]
+    s.close()
