@@ -227,6 +227,27 @@ sdot_status sdot_softmax_refinement(sdot_ctx *ctx, const double *psi_coarse, dou
                                     int use_log_sum_exp, int64_t n_fine, const double *y_fine,
                                     const int64_t *child_offsets, const int64_t *child_indices, double *psi_fine);
 
+/* Replaces SotSolver::evaluate_weighted_barycenters for the euclidean distance
+ * (SotSolver.cc:584-660) through compute_weighted_barycenters_euclidean
+ * (:871-971).  Evaluates at psi (caller order) with the configured parameters
+ * (threshold recomputed as there), then
+ *   barycenters[j*dim + d] = sum_q rho_q JxW_q pi_qj x_q[d] / nu_j,
+ *   pi_qj = nu_j e^(t_qj) / sum_i nu_i e^(t_qi) over the candidates of cell(q),
+ * skipped points (no candidate or zero sum) excluded.  n_targets x dim out. */
+sdot_status sdot_weighted_barycenters(sdot_ctx *ctx, const double *psi, double *barycenters);
+
+/* Replaces SotSolver::get_potential_conditioned_density (SotSolver.cc:973-1046).
+ * For each of n_points query points (the reference's DoF support points) with
+ * the source density there, and each requested target k = indices[i]:
+ *   out[i*n_points + p] = density(p) e^(t_k(p) - m) / sum_j nu_j e^(t_j(p) - m)
+ * when target k lies within `threshold` of the point, else 0 (also 0 when the
+ * point has no candidate).  t_j(p) = (psi_j - |p - y_j|^2 / 2) / epsilon; m the
+ * largest t over the candidates.  The reference uses its current epsilon and
+ * last distance threshold; pass them. */
+sdot_status sdot_conditioned_densities(sdot_ctx *ctx, const double *psi, double epsilon, double threshold,
+                                       int64_t n_points, const double *points, const double *density_at_points,
+                                       int64_t n_indices, const int64_t *indices, double *out);
+
 /* ---- batched solves (no single reference counterpart: many SotSolver::solve
  * calls, SotSolver.cc:105-215, each over an epsilon-scaling sequence as in
  * SemiDiscreteOT.cc:878-922, advanced together on one GPU) ----

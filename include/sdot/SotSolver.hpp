@@ -107,6 +107,58 @@ public:
         hessian_out.resize(n_ * n_);
         check(sdot_hessian(ctx_, potential.data(), hessian_out.data()), "compute_hessian");
     }
+    // Newton with the tensor-core (or FP64) Hessian; same parameters and controls as solve.
+    void solve_newton(std::vector<double> &potential, const SolverParameters &params,
+                      int hessian_method = SDOT_HESS_AUTO) {
+        current_params = params;
+        if (potential.size() != n_) potential.assign(n_, 0.0);
+        const sdot_solver_params p = params.c();
+        sdot_newton_info info{};
+        check(sdot_solve_newton(ctx_, potential.data(), &p, hessian_method, &info), "solve_newton");
+    }
+    // SotSolver::evaluate_weighted_barycenters, euclidean distance (SotSolver.cc:584-660).
+    void evaluate_weighted_barycenters(const std::vector<double> &potentials, std::vector<Point> &barycenters_out,
+                                       const SolverParameters &params) {
+        if (potentials.size() != n_) throw std::runtime_error("evaluate_weighted_barycenters: potential size");
+        (void)params;  // like the reference, the current parameters' epsilon is used
+        barycenters_out.resize(n_);
+        check(sdot_weighted_barycenters(ctx_, potentials.data(), barycenters_out.data()->data()),
+              "evaluate_weighted_barycenters");
+    }
+    // SotSolver::get_potential_conditioned_density (SotSolver.cc:973-1046) at given support
+    // points and the source density there; one vector per requested potential index.
+    void get_potential_conditioned_density(const std::vector<Point> &support_points,
+                                           const std::vector<double> &density_at_points,
+                                           const std::vector<double> &potential,
+                                           const std::vector<unsigned int> &potential_indices,
+                                           std::vector<std::vector<double>> &conditioned_densities) {
+        if (support_points.size() != density_at_points.size() || potential.size() != n_)
+            throw std::runtime_error("get_potential_conditioned_density: sizes");
+        const int64_t np = (int64_t)support_points.size(), ni = (int64_t)potential_indices.size();
+        std::vector<int64_t> idx(potential_indices.begin(), potential_indices.end());
+        std::vector<double> out((size_t)(np * ni));
+        check(sdot_conditioned_densities(ctx_, potential.data(), current_params.epsilon,
+                                         get_last_distance_threshold(), np, support_points.data()->data(),
+                                         density_at_points.data(), ni, idx.data(), out.data()),
+              "get_potential_conditioned_density");
+        conditioned_densities.assign((size_t)ni, std::vector<double>((size_t)np));
+        for (int64_t k = 0; k < ni; ++k)
+            std::copy(out.begin() + k * np, out.begin() + (k + 1) * np, conditioned_densities[k].begin());
+    }
+    // SoftmaxRefinement::compute_refinement (SoftmaxRefinement.cc:61-280): this solver's
+    // targets are the coarse level; children CSR per coarse target.
+    std::vector<double> softmax_refinement(const std::vector<double> &potential_coarse, double epsilon,
+                                           double threshold, const std::vector<Point> &fine_points,
+                                           const std::vector<int64_t> &child_offsets,
+                                           const std::vector<int64_t> &child_indices) {
+        std::vector<double> fine(fine_points.size(), 0.0);
+        check(sdot_softmax_refinement(ctx_, potential_coarse.data(), epsilon, threshold,
+                                      current_params.use_log_sum_exp_trick ? 1 : 0, (int64_t)fine_points.size(),
+                                      fine_points.data()->data(), child_offsets.data(), child_indices.data(),
+                                      fine.data()),
+              "softmax_refinement");
+        return fine;
+    }
     double get_last_functional_value() const { return sdot_get_last_functional_value(ctx_); }
     unsigned get_last_iteration_count() const { return sdot_get_last_iteration_count(ctx_); }
     bool get_convergence_status() const { return sdot_get_convergence_status(ctx_) != 0; }

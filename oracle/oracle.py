@@ -99,6 +99,8 @@ def lib():
         _lib.orc_solve.restype = ip
         _lib.orc_hessian.argtypes = [vp, vp, d, vp, vp, ip]
         _lib.orc_softmax_refinement.argtypes = [vp, vp, d, d, ip, i64, vp, vp, vp, vp, ip]
+        _lib.orc_weighted_barycenters.argtypes = [vp, vp, d, vp, vp, ip]
+        _lib.orc_conditioned_densities.argtypes = [vp, vp, d, d, i64, vp, vp, i64, vp, vp]
         _lib.orc_epsilon_sequence.argtypes = [d, d, C.c_uint, vp]
         _lib.orc_epsilon_sequence.restype = ip
     return _lib
@@ -247,6 +249,23 @@ class Problem:
                                      yf.shape[0], _p(yf), _p(co), _p(ci), _p(out), threads)
         return out
 
+
+    def weighted_barycenters(self, psi, prm: Params, r, threads=0):
+        psi = np.ascontiguousarray(psi, dtype=np.float64)
+        out = np.zeros((self.N, self.dim))
+        pc = prm.c()
+        lib().orc_weighted_barycenters(C.byref(self._c), C.byref(pc), r, _p(psi), _p(out), threads)
+        return out
+
+    def conditioned_densities(self, psi, eps, r, points, density, indices):
+        psi = np.ascontiguousarray(psi, dtype=np.float64)
+        P = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, self.dim)
+        rho = np.ascontiguousarray(density, dtype=np.float64)
+        idx = np.ascontiguousarray(indices, dtype=np.int64)
+        out = np.zeros((idx.size, P.shape[0]))
+        lib().orc_conditioned_densities(C.byref(self._c), _p(psi), eps, r, P.shape[0], _p(P), _p(rho),
+                                        idx.size, _p(idx), _p(out))
+        return out
 
 def epsilon_sequence(eps, factor, steps):
     out = np.zeros(max(int(steps), 1))

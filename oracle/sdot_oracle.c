@@ -887,6 +887,111 @@ void orc_softmax_refinement(const orc_problem *cp, const double *psi_coarse,
     free(acc);
 }
 
+/* ------------------------------------------------------------------ */
+/* compute_weighted_barycenters_euclidean (SotSolver.cc:871-971) through */
+/* local_assemble (:770-869): per point the candidate terms of cell(q),   */
+/* scale = rho JxW / total, barycenter += scale * term * x where term > 0 */
+/* ------------------------------------------------------------------ */
+
+void orc_weighted_barycenters(const orc_problem *p, const orc_params *prm, double r,
+                              const double *psi, double *bary, int n_threads)
+{
+    const int dim = p->dim;
+    const int64_t N = p->n_targets;
+    const double epsilon_inv = 1.0 / prm->epsilon;
+    const int nt = orc_threads(n_threads);
+    double *acc = (double *)calloc((size_t)nt * N * dim, sizeof(double));
+#pragma omp parallel num_threads(nt)
+    {
+#ifdef _OPENMP
+        const int t = omp_get_thread_num();
+#else
+        const int t = 0;
+#endif
+        double *pl = acc + (size_t)t * N * dim;
+        int64_t *cand = (int64_t *)malloc(sizeof(int64_t) * (N + 1));
+        double *et = (double *)malloc(sizeof(double) * (N + 1));
+#pragma omp for schedule(static)
+        for (int64_t c = 0; c < p->n_cells; ++c) {
+            const int64_t nc = orc_candidates(p, p->cell_centers + c * dim, r, cand);
+            if (nc == 0) continue;
+            for (int64_t q = p->cell_offsets[c]; q < p->cell_offsets[c + 1]; ++q) {
+                const double *x = p->xq + q * dim;
+                double total = 0.0, maxe = -DBL_MAX;
+                if (prm->use_log_sum_exp) {
+                    for (int64_t i = 0; i < nc; ++i) {
+                        const int64_t j = cand[i];
+                        const double d2 = pow(orc_dist(dim, x, p->y + j * dim), 2);
+                        const double e = (psi[j] - 0.5 * d2) * epsilon_inv;
+                        maxe = maxe > e ? maxe : e;
+                    }
+                    for (int64_t i = 0; i < nc; ++i) {
+                        const int64_t j = cand[i];
+                        const double d2 = pow(orc_dist(dim, x, p->y + j * dim), 2);
+                        et[i] = p->nu[j] * exp((psi[j] - 0.5 * d2) * epsilon_inv - maxe);
+                        total += et[i];
+                    }
+                } else {
+                    for (int64_t i = 0; i < nc; ++i) {
+                        const int64_t j = cand[i];
+                        const double d2 = pow(orc_dist(dim, x, p->y + j * dim), 2);
+                        et[i] = p->nu[j] * exp((psi[j] - 0.5 * d2) * epsilon_inv);
+                        total += et[i];
+                    }
+                }
+                if (total <= 0.0) continue;
+                const double scale = p->rho[q] * p->jxw[q] / total;
+                for (int64_t i = 0; i < nc; ++i)
+                    if (et[i] > 0.0)
+                        for (int d = 0; d < dim; ++d) pl[cand[i] * dim + d] += scale * et[i] * x[d];
+            }
+        }
+        free(cand); free(et);
+    }
+    for (int64_t k = 0; k < N * dim; ++k) {
+        double v = 0.0;
+        for (int t = 0; t < nt; ++t) v += acc[(size_t)t * N * dim + k];
+        bary[k] = v / p->nu[k / dim];
+    }
+    free(acc);
+}
+
+/* SotSolver::get_potential_conditioned_density (SotSolver.cc:973-1046) at
+ * n_points support points with the source density there. */
+void orc_conditioned_densities(const orc_problem *p, const double *psi, double eps, double r,
+                               int64_t n_points, const double *points, const double *density,
+                               int64_t n_idx, const int64_t *idx, double *out)
+{
+    const int dim = p->dim;
+    const int64_t N = p->n_targets;
+    const double epsilon_inv = 1.0 / eps;
+    int64_t *cand = (int64_t *)malloc(sizeof(int64_t) * (N + 1));
+    double *ex = (double *)malloc(sizeof(double) * (N + 1));
+    char *in = (char *)malloc((size_t)N + 1);
+    for (int64_t k = 0; k < n_idx * n_points; ++k) out[k] = 0.0;
+    for (int64_t pt = 0; pt < n_points; ++pt) {
+        const double *x = points + pt * dim;
+        const int64_t nc = orc_candidates(p, x, r, cand);
+        for (int64_t j = 0; j < N; ++j) { ex[j] = 0.0; in[j] = 0; }
+        double total = 0.0, maxe = -DBL_MAX;
+        for (int64_t i = 0; i < nc; ++i) {
+            const int64_t j = cand[i];
+            const double e = (psi[j] - 0.5 * pow(orc_dist(dim, x, p->y + j * dim), 2)) * epsilon_inv;
+            maxe = maxe > e ? maxe : e;
+        }
+        for (int64_t i = 0; i < nc; ++i) {
+            const int64_t j = cand[i];
+            ex[j] = exp((psi[j] - 0.5 * pow(orc_dist(dim, x, p->y + j * dim), 2)) * epsilon_inv - maxe);
+            in[j] = 1;
+            total += p->nu[j] * ex[j];
+        }
+        if (total > 0.0)
+            for (int64_t k = 0; k < n_idx; ++k)
+                if (in[idx[k]]) out[k * n_points + pt] = density[pt] * (ex[idx[k]] / total);
+    }
+    free(cand); free(ex); free(in);
+}
+
 /* EpsilonScalingHandler (EpsilonScalingHandler.cc:6-42). */
 int orc_epsilon_sequence(double eps, double factor, unsigned steps, double *out)
 {

@@ -157,6 +157,17 @@ void orc_softmax_refinement(const orc_problem *coarse, const double *psi_coarse,
                             const int64_t *child_offsets, const int64_t *child_indices,
                             double *psi_fine, int n_threads);
 
+/* SotSolver::compute_weighted_barycenters_euclidean (SotSolver.cc:871-971):
+ * bary (n_targets x dim) = sum_q rho JxW pi_qj x_q / nu_j at threshold r. */
+void orc_weighted_barycenters(const orc_problem *p, const orc_params *prm, double r,
+                              const double *psi, double *bary, int n_threads);
+
+/* SotSolver::get_potential_conditioned_density (SotSolver.cc:973-1046):
+ * out[k * n_points + pt] for the requested targets idx[k]. */
+void orc_conditioned_densities(const orc_problem *p, const double *psi, double eps, double r,
+                               int64_t n_points, const double *points, const double *density,
+                               int64_t n_idx, const int64_t *idx, double *out);
+
 /* EpsilonScalingHandler (src/solvers/EpsilonScalingHandler.cc:30-90). */
 int orc_epsilon_sequence(double eps, double factor, unsigned steps, double *out);
 

@@ -8,12 +8,13 @@ from .parameters import (MultilevelParameters, SolverParameters, distribute_epsi
                          read_prm, solver_parameters_from_prm, multilevel_parameters_from_prm)
 from . import io
 from .batch import BatchSolver
+from .lloyd import run_lloyd
 from .multilevel import build_hierarchy, run_target_multilevel
 from .server import SolveServer
 from .solver import SotSolver
 from .source import structured_source
 
 __all__ = [
-    "SotSolver", "BatchSolver", "SolveServer", "SolverParameters", "build_hierarchy", "run_target_multilevel", "io", "MultilevelParameters", "read_prm", "solver_parameters_from_prm",
+    "SotSolver", "BatchSolver", "SolveServer", "SolverParameters", "build_hierarchy", "run_target_multilevel", "run_lloyd", "io", "MultilevelParameters", "read_prm", "solver_parameters_from_prm",
     "multilevel_parameters_from_prm", "epsilon_sequence", "distribute_epsilon_values", "structured_source",
 ]

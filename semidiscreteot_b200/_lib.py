@@ -35,7 +35,8 @@ EXPORTED = [
     "sdot_compute_geometric_radius_bound", "sdot_set_distance_function", "sdot_evaluate_partial_device",
     "sdot_set_state", "sdot_get_stream", "sdot_set_profiling", "sdot_get_kernel_times", "sdot_measure_peaks",
     "sdot_evaluate_device_noalloc", "sdot_hessian_device", "sdot_set_hessian_chunk",
-    "sdot_solve_newton", "sdot_softmax_refinement", "sdot_batch_create", "sdot_batch_destroy", "sdot_batch_last_error", "sdot_batch_size", "sdot_batch_set_verbose",
+    "sdot_solve_newton", "sdot_softmax_refinement", "sdot_weighted_barycenters", "sdot_conditioned_densities",
+    "sdot_batch_create", "sdot_batch_destroy", "sdot_batch_last_error", "sdot_batch_size", "sdot_batch_set_verbose",
     "sdot_batch_add", "sdot_batch_evaluate", "sdot_batch_solve", "sdot_batch_problem_info",
     "sdot_server_create", "sdot_server_destroy", "sdot_server_last_error", "sdot_server_submit", "sdot_server_poll",
     "sdot_server_wait", "sdot_server_get_stats", "sdot_server_reset_stats",
@@ -169,6 +170,10 @@ def load():
     lib.sdot_solve_newton.restype = ip
     lib.sdot_softmax_refinement.argtypes = [vp, vp, d, d, ip, i64, vp, vp, vp, vp]
     lib.sdot_softmax_refinement.restype = ip
+    lib.sdot_weighted_barycenters.argtypes = [vp, vp, vp]
+    lib.sdot_weighted_barycenters.restype = ip
+    lib.sdot_conditioned_densities.argtypes = [vp, vp, d, d, i64, vp, vp, i64, vp, vp]
+    lib.sdot_conditioned_densities.restype = ip
     lib.sdot_batch_create.argtypes = [C.POINTER(vp), ip, ip]
     lib.sdot_batch_create.restype = ip
     lib.sdot_batch_destroy.argtypes = [vp]

@@ -20,6 +20,10 @@
   children of a level-L point are level L-1 indices).
 - ``write_potentials`` / ``read_potentials``: potentials as written by
   save_results (write_vector of the potential vector).
+- ``write_ply`` / ``read_ply``: the ASCII point files of
+  Lloyd::run_centroid_iteration (src/core/Lloyd.cc:139-171): a PLY header with
+  one float property per coordinate, then each point's coordinates at the
+  default stream precision, each followed by a space.
 """
 from __future__ import annotations
 
@@ -218,3 +222,34 @@ def child_csr_from_parents(parent: np.ndarray, n_coarse: int) -> Tuple[np.ndarra
     off = np.zeros(n_coarse + 1, dtype=np.int64)
     off[1:] = np.cumsum(counts)
     return off, order.astype(np.int64)
+
+
+def write_ply(points, path: str) -> str:
+    P = np.asarray(points, dtype=np.float64)
+    P = P.reshape(P.shape[0], -1)
+    d = os.path.dirname(path)
+    if d:
+        os.makedirs(d, exist_ok=True)
+    with open(path, "w") as f:
+        f.write("ply\nformat ascii 1.0\n")
+        f.write(f"element vertex {P.shape[0]}\n")
+        for k in range(P.shape[1]):
+            f.write(f"property float {'xyz'[k]}\n")
+        f.write("end_header\n")
+        f.writelines("".join(_fmt6(v) + " " for v in row) + "\n" for row in P)
+    return path
+
+
+def read_ply(path: str) -> np.ndarray:
+    with open(path) as f:
+        lines = f.read().splitlines()
+    n, dim, k = 0, 0, 0
+    while lines[k] != "end_header":
+        t = lines[k].split()
+        if t[:2] == ["element", "vertex"]:
+            n = int(t[2])
+        elif t[:1] == ["property"]:
+            dim += 1
+        k += 1
+    rows = [[float(v) for v in line.split()] for line in lines[k + 1:k + 1 + n]]
+    return np.array(rows, dtype=np.float64).reshape(n, dim)

@@ -197,9 +197,10 @@ class SotSolver:
                                 "total_pairs": info.total_pairs, "eval_ms": info.eval_ms,
                                 "hessian_ms": info.hessian_ms, "cg_ms": info.cg_ms,
                                 "hessian_method": names.get(info.hessian_method, info.hessian_method)}
-        self._check(st)
+        # in place also after a failure, like solve (the library writes the last iterate back)
         if isinstance(potential, np.ndarray) and potential is not psi and potential.size == psi.size:
             potential[...] = psi
+        self._check(st)
         return psi
 
     def softmax_refinement(self, potential_coarse, epsilon: float, threshold: float, y_fine, child_offsets,
@@ -218,6 +219,43 @@ class SotSolver:
         self._check(self._L.sdot_softmax_refinement(self._h, psi.ctypes.data, float(epsilon), float(threshold),
                                                     int(bool(lse)), yf.shape[0], yf.ctypes.data, co.ctypes.data,
                                                     ci.ctypes.data, out.ctypes.data))
+        return out
+
+    def evaluate_weighted_barycenters(self, potential, params: Optional[SolverParameters] = None) -> np.ndarray:
+        """SotSolver::evaluate_weighted_barycenters, euclidean distance (SotSolver.cc:584-660,
+        871-971): barycenter_j = sum_q rho_q JxW_q pi_qj x_q / nu_j at the given potentials,
+        threshold recomputed there; (n_targets, dim).  `params` configures the solver first;
+        the computation reads the configured epsilon as the reference's current_params does."""
+        if params is not None:
+            self.configure(params)
+        psi = _f64(potential)
+        if psi.size != self._n_targets:
+            raise ValueError("potential size differs from the number of targets")
+        out = np.empty((self._n_targets, self.dim))
+        self._check(self._L.sdot_weighted_barycenters(self._h, psi.ctypes.data, out.ctypes.data))
+        return out
+
+    def get_potential_conditioned_density(self, points, density_at_points, potential, potential_indices,
+                                          epsilon: Optional[float] = None,
+                                          threshold: Optional[float] = None) -> np.ndarray:
+        """SotSolver::get_potential_conditioned_density (SotSolver.cc:973-1046) at the given
+        support points: row i is density(p) e^(t_k - m) / sum_j nu_j e^(t_j - m) for target
+        k = potential_indices[i] where k is within the threshold of p, else 0.  epsilon and
+        threshold default to the configured epsilon and the last distance threshold."""
+        P = _f64(points).reshape(-1, self.dim)
+        rho = _f64(density_at_points)
+        psi = _f64(potential)
+        idx = np.ascontiguousarray(potential_indices, dtype=np.int64)
+        if rho.size != P.shape[0]:
+            raise ValueError("one density value per support point expected")
+        if psi.size != self._n_targets:
+            raise ValueError("potential size differs from the number of targets")
+        eps = self.current_params.epsilon if epsilon is None else float(epsilon)
+        thr = self.get_last_distance_threshold() if threshold is None else float(threshold)
+        out = np.zeros((idx.size, P.shape[0]))
+        self._check(self._L.sdot_conditioned_densities(self._h, psi.ctypes.data, eps, thr, P.shape[0],
+                                                       P.ctypes.data, rho.ctypes.data, idx.size,
+                                                       idx.ctypes.data, out.ctypes.data))
         return out
 
     def compute_hessian(self, potential, hessian_out: Optional[np.ndarray] = None) -> np.ndarray:

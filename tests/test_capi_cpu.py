@@ -66,7 +66,8 @@ def test_header_compiles_as_c_and_cpp(tmp_path):
                    check=True)
     facade = os.path.join(ROOT, "include", "sdot", "SotSolver.hpp")
     cpp = tmp_path / "t.cpp"
-    cpp.write_text('#include "sdot/SotSolver.hpp"\nint main(){ return 0; }\n')
+    cpp.write_text('#include "sdot/SotSolver.hpp"\ntemplate class sdot::SotSolver<2>;\n'
+                   'template class sdot::SotSolver<3>;\nint main(){ return 0; }\n')
     subprocess.run(["g++", "-std=c++17", "-Wall", "-Werror", "-fsyntax-only", "-I", os.path.join(ROOT, "include"),
                     str(cpp)], check=True)
     assert os.path.exists(facade)

@@ -66,3 +66,21 @@ def test_hierarchy_files(tmp_path):
     off2, idx2 = sio.child_csr_from_parents(parent, 3)
     assert np.array_equal(off, off2) and np.array_equal(idx, idx2)
     assert np.max(np.abs(h["points"][0] - fine)) < 1e-5   # 6 significant digits
+
+
+def test_ply_round_trip(tmp_path):
+    from semidiscreteot_b200.io import read_ply, write_ply
+    P = np.array([[0.125, 0.5, 1.0 / 3.0], [2.0, -1e-7, 123456.789]])
+    path = write_ply(P, str(tmp_path / "barycenters_0.ply"))
+    text = open(path).read().splitlines()
+    assert text[:7] == ["ply", "format ascii 1.0", "element vertex 2", "property float x", "property float y",
+                        "property float z", "end_header"]
+    assert text[7] == "0.125 0.5 0.333333 "
+    np.testing.assert_allclose(read_ply(path), P, rtol=1e-5)
+
+
+def test_lloyd_step_norm():
+    from semidiscreteot_b200.lloyd import step_norm
+    a = np.zeros((4, 2))
+    b = np.array([[3.0, 4.0], [0, 0], [0, 0], [0, 0]])
+    assert step_norm(b, a) == np.sqrt(25.0 / 4)

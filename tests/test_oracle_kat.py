@@ -227,3 +227,37 @@ def test_softmax_refinement_single_child(oracle_mod):
     # psi_fine_j = psi_j - eps log((g_j + nu_j)/nu_j): equal up to eps*|g|/nu
     d = (fine - fine.mean()) - (psi - psi.mean())
     assert np.max(np.abs(d)) < 1e-6
+
+
+def test_weighted_barycenters_known_answers(oracle_mod):
+    """Single target: the barycenter is sum_q w_q x_q / nu.  Several targets,
+    untruncated: sum_j nu_j B_j = sum_q w_q x_q (the plan's rows sum to w_q),
+    for both log-sum-exp settings."""
+    xq, jxw, rho, off, ctr = unit_square(oracle_mod, 8, 3)
+    w = rho * jxw
+    P1 = oracle_mod.Problem(xq, jxw, rho, off, ctr, np.array([[0.3, 0.6]]), [0.7])
+    B1 = P1.weighted_barycenters([0.2], oracle_mod.Params(epsilon=0.05, tau=0.0), 1e300)
+    np.testing.assert_allclose(B1[0], (w @ xq) / 0.7, rtol=1e-13)
+    P, rng = random_problem(oracle_mod, 8, N=15)
+    psi = 0.02 * rng.standard_normal(P.N)
+    wsum = (P.rho * P.jxw) @ P.xq.reshape(-1, 2)
+    for lse in (True, False):
+        B = P.weighted_barycenters(psi, oracle_mod.Params(epsilon=0.03, tau=0.0, use_log_sum_exp=lse), 1e300)
+        np.testing.assert_allclose(P.nu @ B, wsum, rtol=1e-12)
+
+
+def test_conditioned_densities_known_answers(oracle_mod):
+    """Untruncated: sum_k nu_k c_k(p) = density(p); a target outside the
+    threshold of a point gets 0 there."""
+    P, rng = random_problem(oracle_mod, 6, N=12)
+    psi = 0.02 * rng.standard_normal(P.N)
+    pts = rng.random((40, 2))
+    dens = rng.random(40) + 0.5
+    c = P.conditioned_densities(psi, 0.04, 1e300, pts, dens, np.arange(P.N))
+    np.testing.assert_allclose(P.nu @ c, dens, rtol=1e-13)
+    r = 0.3
+    ct = P.conditioned_densities(psi, 0.04, r, pts, dens, np.arange(P.N))
+    d = np.linalg.norm(P.y.reshape(-1, 2)[:, None, :] - pts[None, :, :], axis=2)
+    assert np.all(ct[d > r] == 0.0)
+    has = (d <= r).any(axis=0)
+    np.testing.assert_allclose((P.nu @ ct)[has], dens[has], rtol=1e-13)
