@@ -9,12 +9,13 @@ from .parameters import (MultilevelParameters, SolverParameters, distribute_epsi
 from . import io
 from .batch import BatchSolver
 from .lloyd import run_lloyd
-from .multilevel import build_hierarchy, run_target_multilevel
+from .multilevel import build_hierarchy, run_source_multilevel, run_target_multilevel
 from .server import SolveServer
 from .solver import SotSolver
+from .simplex import simplex_source
 from .source import structured_source
 
 __all__ = [
-    "SotSolver", "BatchSolver", "SolveServer", "SolverParameters", "build_hierarchy", "run_target_multilevel", "run_lloyd", "io", "MultilevelParameters", "read_prm", "solver_parameters_from_prm",
+    "SotSolver", "BatchSolver", "SolveServer", "SolverParameters", "build_hierarchy", "run_target_multilevel", "run_source_multilevel", "run_lloyd", "simplex_source", "io", "MultilevelParameters", "read_prm", "solver_parameters_from_prm",
     "multilevel_parameters_from_prm", "epsilon_sequence", "distribute_epsilon_values", "structured_source",
 ]

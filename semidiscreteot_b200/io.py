@@ -20,6 +20,11 @@
   children of a level-L point are level L-1 indices).
 - ``write_potentials`` / ``read_potentials``: potentials as written by
   save_results (write_vector of the potential vector).
+- ``read_msh`` / ``write_msh``: gmsh 2.2 ASCII meshes as deal.II's
+  GridIn::read_msh takes them for the simplex source meshes (tutorial_0 reads
+  its source.msh, examples/tutorial_0/src/tutorial_0.cc:37-47): nodes, and the
+  elements of the highest dimension present (triangles, type 2, or
+  tetrahedra, type 4) as cells; lower-dimensional elements are boundary data.
 - ``write_ply`` / ``read_ply``: the ASCII point files of
   Lloyd::run_centroid_iteration (src/core/Lloyd.cc:139-171): a PLY header with
   one float property per coordinate, then each point's coordinates at the
@@ -253,3 +258,73 @@ def read_ply(path: str) -> np.ndarray:
         k += 1
     rows = [[float(v) for v in line.split()] for line in lines[k + 1:k + 1 + n]]
     return np.array(rows, dtype=np.float64).reshape(n, dim)
+
+
+_MSH_NODES = {1: 2, 2: 3, 3: 4, 4: 4, 5: 8, 15: 1}
+_MSH_DIM = {1: 1, 2: 2, 3: 2, 4: 3, 5: 3, 15: 0}
+
+
+def read_msh(path: str) -> Dict[str, np.ndarray]:
+    """gmsh 2.2 ASCII: {"nodes": (V, 3), "cells": (C, dim+1) vertex indices,
+    "dim": 2 or 3, "cell_tags": (C, ntags) physical/elementary tags}.  Only
+    simplex cells (triangles, tetrahedra) are accepted as the top dimension."""
+    with open(path) as f:
+        lines = f.read().split("\n")
+    k = 0
+    nodes = None
+    ids: Dict[int, int] = {}
+    elems: Dict[int, list] = {}
+    tags: Dict[int, list] = {}
+    while k < len(lines):
+        t = lines[k].strip()
+        if t == "$MeshFormat":
+            ver = lines[k + 1].split()
+            if not ver or not ver[0].startswith("2") or ver[1] != "0":
+                raise ValueError("only gmsh 2.x ASCII meshes are read")
+            k += 2
+        elif t == "$Nodes":
+            n = int(lines[k + 1])
+            nodes = np.empty((n, 3))
+            for i in range(n):
+                v = lines[k + 2 + i].split()
+                ids[int(v[0])] = i
+                nodes[i] = [float(v[1]), float(v[2]), float(v[3])]
+            k += n + 2
+        elif t == "$Elements":
+            n = int(lines[k + 1])
+            for i in range(n):
+                v = [int(a) for a in lines[k + 2 + i].split()]
+                et, nt = v[1], v[2]
+                if et not in _MSH_NODES:
+                    raise ValueError(f"unsupported gmsh element type {et}")
+                elems.setdefault(et, []).append(v[3 + nt:3 + nt + _MSH_NODES[et]])
+                tags.setdefault(et, []).append(v[3:3 + nt])
+            k += n + 2
+        else:
+            k += 1
+    if nodes is None or not elems:
+        raise ValueError(f"{path}: no nodes or elements")
+    top = max(_MSH_DIM[et] for et in elems)
+    if top == 3 and 5 in elems or top == 2 and 3 in elems:
+        raise ValueError("hexahedra / quadrilaterals: use a structured Q1 source")
+    et = 4 if top == 3 else 2
+    cells = np.array([[ids[a] for a in c] for c in elems[et]], dtype=np.int64)
+    return {"nodes": nodes, "cells": cells, "dim": top, "cell_tags": np.array(tags[et], dtype=np.int64)}
+
+
+def write_msh(path: str, nodes, cells) -> str:
+    """gmsh 2.2 ASCII with one element block (triangles or tetrahedra)."""
+    P = np.asarray(nodes, dtype=np.float64)
+    T = np.asarray(cells, dtype=np.int64)
+    et = {3: 2, 4: 4}[T.shape[1]]
+    if P.shape[1] == 2:
+        P = np.hstack([P, np.zeros((P.shape[0], 1))])
+    with open(path, "w") as f:
+        f.write("$MeshFormat\n2.2 0 8\n$EndMeshFormat\n$Nodes\n")
+        f.write(f"{P.shape[0]}\n")
+        f.writelines(f"{i + 1} {_fmt17(p[0])} {_fmt17(p[1])} {_fmt17(p[2])}\n" for i, p in enumerate(P))
+        f.write("$EndNodes\n$Elements\n")
+        f.write(f"{T.shape[0]}\n")
+        f.writelines(f"{i + 1} {et} 2 0 0 " + " ".join(str(int(a) + 1) for a in c) + "\n" for i, c in enumerate(T))
+        f.write("$EndElements\n")
+    return path

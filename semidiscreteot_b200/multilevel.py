@@ -11,6 +11,15 @@ Mirrors SemiDiscreteOT::run_target_multilevel (src/core/SemiDiscreteOT.cc
   EpsilonScalingHandler::compute_epsilon_distribution gives, or the
   parameters' epsilon).
 
+``run_source_multilevel`` mirrors SemiDiscreteOT::run_source_multilevel
+(SemiDiscreteOT.cc:1325-1522): the same targets are solved against a list of
+source measures, coarsest first; each level starts from the previous level's
+potentials (the first from ``initial_potential`` or zero) and runs its share
+of the epsilon-scaling sequence (EpsilonScalingHandler distribution over the
+source levels), or params.epsilon when there is none.  The levels are given as
+flattened sources (``setup_source`` dicts); ``nearest_vertex_density`` moves a
+nodal density to a coarser mesh's vertices.
+
 ``build_hierarchy`` is a seeded k-means coarsening (k-means++ seeds, Lloyd
 iterations) with the level sizes of PointCloudHierarchyManager::getPointsForLevel
 (src/core/PointCloudHierarchy.cc:63-76): level 1 holds min(N, max_points) points,
@@ -126,6 +135,57 @@ def run_target_multilevel(solver, hierarchy: Dict[str, list], params: SolverPara
                 psi = solver.solve(psi, p)
             its += solver.get_last_iteration_count()
         out.append({"level": L, "potentials": psi.copy(), "iterations": its,
+                    "converged": bool(solver.get_convergence_status()),
+                    "threshold": solver.get_last_distance_threshold()})
+    return out
+
+
+def nearest_vertex_density(fine_vertices, fine_density, coarse_vertices) -> np.ndarray:
+    """Nodal density on a coarse mesh: each coarse vertex takes the value of the
+    nearest fine vertex (a nearest-neighbour transfer in the spirit of
+    Utils::interpolate_non_conforming_nearest, utils.h:504-600; ties go to the
+    lowest fine index)."""
+    F = np.asarray(fine_vertices, dtype=np.float64)
+    d = np.asarray(fine_density, dtype=np.float64)
+    Cv = np.asarray(coarse_vertices, dtype=np.float64)
+    out = np.empty(Cv.shape[0])
+    for k0 in range(0, Cv.shape[0], 2048):
+        blk = Cv[k0:k0 + 2048]
+        d2 = ((blk[:, None, :] - F[None, :, :]) ** 2).sum(-1) if F.shape[0] * blk.shape[0] <= 2 ** 26 else None
+        if d2 is None:
+            idx = np.array([int(np.argmin(np.sum((F - x) ** 2, axis=1))) for x in blk])
+        else:
+            idx = np.argmin(d2, axis=1)
+        out[k0:k0 + blk.shape[0]] = d[idx]
+    return out
+
+
+def run_source_multilevel(solver, sources: Sequence[dict], target_points, target_density, params: SolverParameters,
+                          epsilon_distribution: Optional[Sequence[Sequence[float]]] = None,
+                          initial_potential: Optional[np.ndarray] = None, method: str = "lbfgs") -> List[dict]:
+    """sources: flattened source measures, coarsest first.  Returns per level
+    (coarsest first) its index, potentials, iterations, convergence and last
+    threshold; the last entry holds the finest level's potentials."""
+    y = np.asarray(target_points, dtype=np.float64)
+    nu = np.asarray(target_density, dtype=np.float64)
+    psi = np.zeros(len(nu)) if initial_potential is None else np.array(initial_potential, dtype=np.float64)
+    if psi.size != len(nu):
+        raise ValueError("initial potential does not match the target points")
+    out: List[dict] = []
+    for i, src in enumerate(sources):
+        solver.setup_source(src["x"], src["jxw"], src["density"], src["cell_offsets"], src["cell_centers"])
+        solver.setup_target(y, nu)
+        eps_list = list(epsilon_distribution[i]) if epsilon_distribution is not None and \
+            i < len(epsilon_distribution) and len(epsilon_distribution[i]) else [params.epsilon]
+        its = 0
+        for eps in eps_list:
+            p = dataclasses.replace(params, epsilon=float(eps))
+            if method == "newton":
+                psi = solver.solve_newton(psi, p)
+            else:
+                psi = solver.solve(psi, p)
+            its += solver.get_last_iteration_count()
+        out.append({"level": len(sources) - 1 - i, "potentials": psi.copy(), "iterations": its,
                     "converged": bool(solver.get_convergence_status()),
                     "threshold": solver.get_last_distance_threshold()})
     return out
