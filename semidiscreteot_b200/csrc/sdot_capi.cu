@@ -199,6 +199,7 @@ size_t device_bytes(const sdot_ctx *c)
     return c->x.bytes() + c->rho.bytes() + c->jxw.bytes() + c->w.bytes() + c->cell_ctr.bytes() +
            c->sblk_sph.bytes() + c->sblk_sph32.bytes() + c->sblk_cell.bytes() + c->tblk_off.bytes() +
            c->tblk_sph32.bytes() + c->part.bytes() + c->fwd_t.bytes() + c->pmask.bytes() + c->pmpre.bytes() +
+           c->inv_b.bytes() + c->fwd2inv.bytes() + c->inv_tmpb.bytes() + c->inv_tmpk.bytes() + c->inv_off.bytes() +
            c->y.bytes() + c->nu.bytes() + c->perm.bytes() +
            c->tblk_sph.bytes() + c->psi.bytes() + c->grad.bytes() + c->tpack.bytes() + c->Lq.bytes() +
            c->gpart.bytes() + c->blkpart.bytes() + c->scal.bytes() + c->redpart.bytes() + c->io_a.bytes() +
@@ -435,7 +436,8 @@ void sdot_destroy(sdot_ctx *c)
         c->tblk_off.release(); c->tblk_sph32.release(); c->part.release(); c->fwd_t.release();
         c->fwd_cnt.release(); c->fwd_off.release(); c->shit.release(); c->spidx.release(); c->scount.release();
         c->inv_cnt.release(); c->inv_off.release(); c->inv_b.release(); c->fwd2inv.release();
-        c->pmask.release(); c->pmpre.release(); c->superpair.release(); c->superpairT.release(); c->ssup_sph32.release(); c->tsup_sph32.release();
+        c->inv_tmpb.release(); c->inv_tmpk.release();
+        c->pmask.release(); c->pmpre.release(); c->superpair.release(); c->ssup_sph32.release(); c->tsup_sph32.release();
         c->y.release(); c->nu.release();
         c->perm.release(); c->tblk_sph.release(); c->psi.release(); c->grad.release(); c->tpack.release();
         c->Lq.release(); c->gpart.release(); c->blkpart.release(); c->scal.release(); c->redpart.release();

@@ -138,9 +138,10 @@ struct sdot_ctx {
 
     // ---- truncated path: block-pair lists and gradient partials ----
     sdot::DevBuf<int64_t> fwd_cnt, fwd_off, inv_cnt, inv_off, fwd2inv;
-    sdot::DevBuf<int> fwd_t, inv_b, shit, spidx, scount, pmpre;
+    sdot::DevBuf<int> fwd_t, inv_b, shit, spidx, scount, pmpre, inv_tmpb;
+    sdot::DevBuf<int64_t> inv_tmpk;    // inverse-list scatter (forward position per entry)
     sdot::DevBuf<unsigned> pmask;
-    sdot::DevBuf<unsigned char> superpair, superpairT;
+    sdot::DevBuf<unsigned char> superpair;
     sdot::DevBuf<float4> ssup_sph32, tsup_sph32;  // super-block spheres (32 blocks each)
     sdot::DevBuf<double> part;
     size_t part_cap_bytes = (size_t)4 << 30;

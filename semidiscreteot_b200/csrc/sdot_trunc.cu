@@ -132,19 +132,15 @@ __device__ __forceinline__ bool pair_test(float4 s, float4 t, float cr)
 
 // Super-block pairs: sp[si * nts + ti] = 1 iff source super-block si and
 // target super-block ti may hold a pair (the same conservative test; a
-// super-sphere contains its member spheres, so no block pair is lost).  The
-// transposed copy spt[ti * nss + si] lets the inverse-list scan read a target
-// super-block's column contiguously.
+// super-sphere contains its member spheres, so no block pair is lost).
 __global__ void __launch_bounds__(256)
 k_super_pairs(const float4 *__restrict__ ssph, int nss, const float4 *__restrict__ tsph, int nts, float cr,
-              unsigned char *__restrict__ sp, unsigned char *__restrict__ spt)
+              unsigned char *__restrict__ sp)
 {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= (int64_t)nss * nts) return;
     const int si = (int)(i / nts), ti = (int)(i - (int64_t)si * nts);
-    const unsigned char v = pair_test(ssph[si], tsph[ti], cr) ? 1 : 0;
-    sp[i] = v;
-    spt[(int64_t)ti * nss + si] = v;
+    sp[i] = pair_test(ssph[si], tsph[ti], cr) ? 1 : 0;
 }
 
 // Warp <-> source super-block: its paired target super-blocks in ascending
@@ -217,56 +213,160 @@ k_fwd_fill(int nsb, int nts, int hmax, const int *__restrict__ shit, const int *
     }
 }
 
-// Inverse list (warp <-> target block t): source blocks b paired with t,
-// ascending b, visiting the source super-blocks paired with t's super-block.
-// Evaluates pair_test(b, t) with the same operands as k_fwd_masks.
-template <bool FILL>
+// Inverse lists by transposing the forward lists (the same pair set by
+// construction).  Warp <-> source block b, lanes over its forward entries:
+// count the pairs of each target block (integer atomics, exact totals).
 __global__ void __launch_bounds__(256)
-k_inv_list(const float4 *__restrict__ sph, int nsb, int nss, const float4 *__restrict__ tph, int ntb, int nts,
-           float cr, const unsigned char *__restrict__ spt, const int64_t *__restrict__ off, int64_t *__restrict__ cnt,
-           int *__restrict__ out)
+k_inv_count(int nsb, const int64_t *__restrict__ fwd_off, const int *__restrict__ fwd_t,
+            unsigned long long *__restrict__ cnt)
 {
-    const int t = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+    const int b = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
-    if (t >= ntb) return;
-    const float4 me = tph[t];
-    const int ti = t / SUPER;
-    int64_t k = FILL ? off[t] : 0;
-    for (int s0 = 0; s0 < nss; s0 += 32) {
-        const int sl = s0 + lane;
-        unsigned sbal = __ballot_sync(0xffffffffu, sl < nss && spt[(int64_t)ti * nss + sl]);
-        while (sbal) {
-            const int si = s0 + __ffs(sbal) - 1;
-            sbal &= sbal - 1;
-            const int b = si * SUPER + lane;
-            const bool hit = b < nsb && pair_test(sph[b], me, cr);
-            const unsigned bal = __ballot_sync(0xffffffffu, hit);
-            if (FILL && hit) out[k + __popc(bal & ((1u << lane) - 1u))] = b;
-            k += __popc(bal);
-        }
-    }
-    if (!FILL && lane == 0) cnt[t] = k;
+    if (b >= nsb) return;
+    for (int64_t k = fwd_off[b] + lane; k < fwd_off[b + 1]; k += 32) atomicAdd(&cnt[fwd_t[k]], 1ull);
 }
 
-// fwd2inv[k] = inverse position of forward pair k (warp <-> source block b,
-// lane <-> its pairs; binary search of b in the inverse list of t; -1 if absent).
+// Scatter each forward pair (b, t) into t's segment of the inverse list, in
+// arrival order: tmp_b = b, tmp_k = forward position.  k_inv_order then
+// fixes the order.
 __global__ void __launch_bounds__(256)
-k_fwd2inv(int nsb, const int64_t *__restrict__ fwd_off, const int *__restrict__ fwd_t,
-          const int64_t *__restrict__ inv_off, const int *__restrict__ inv_b, int64_t *__restrict__ fwd2inv)
+k_inv_scatter(int nsb, const int64_t *__restrict__ fwd_off, const int *__restrict__ fwd_t,
+              const int64_t *__restrict__ inv_off, unsigned long long *__restrict__ fill, int *__restrict__ tmp_b,
+              int64_t *__restrict__ tmp_k)
 {
     const int b = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
     if (b >= nsb) return;
     for (int64_t k = fwd_off[b] + lane; k < fwd_off[b + 1]; k += 32) {
         const int t = fwd_t[k];
-        int64_t lo = inv_off[t], hi = inv_off[t + 1];
-        const int64_t end = hi;
-        while (lo < hi) {
-            const int64_t mid = (lo + hi) >> 1;
-            if (inv_b[mid] < b) lo = mid + 1;
-            else hi = mid;
+        const int64_t pos = inv_off[t] + (int64_t)atomicAdd(&fill[t], 1ull);
+        tmp_b[pos] = b;
+        tmp_k[pos] = k;
+    }
+}
+
+// CTA <-> target block t: order its segment by source block (distinct within
+// a segment).  With at most 32 * INV_TILE source blocks: a bitmap of the
+// segment's blocks in shared memory, an exclusive scan of its word
+// popcounts, and rank(b) = prefix[b / 32] + popc(bits of the word below b).
+// Otherwise, up to INV_TILE entries: bitonic sort of (b, entry); longer
+// segments: the rank of each entry = the number of entries with a smaller b,
+// counted against INV_TILE-entry tiles.  Every way, inv_b[off + rank] = b
+// (ascending b, the order the gradient reduction sums in) and
+// fwd2inv[k] = off + rank.
+constexpr int INV_TILE = 2048;
+constexpr int INV_PER = INV_TILE / 256;
+__global__ void __launch_bounds__(256)
+k_inv_order(int nsb, const int64_t *__restrict__ inv_off, const int *__restrict__ tmp_b,
+            const int64_t *__restrict__ tmp_k, int *__restrict__ inv_b, int64_t *__restrict__ fwd2inv)
+{
+    __shared__ int sb[INV_TILE];
+    __shared__ short si[INV_TILE];
+    __shared__ unsigned bm[INV_TILE];
+    __shared__ int pre[INV_TILE];
+    __shared__ int wsum[8];
+    const int t = blockIdx.x, tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
+    const int64_t off = inv_off[t];
+    const int64_t L = inv_off[t + 1] - off;
+    const int W = (nsb + 31) >> 5;
+    if (W <= INV_TILE) {
+        for (int i = tid; i < W; i += 256) bm[i] = 0u;
+        __syncthreads();
+        for (int64_t i = tid; i < L; i += 256) {
+            const int b = tmp_b[off + i];
+            atomicOr(&bm[b >> 5], 1u << (b & 31));
         }
-        fwd2inv[k] = (lo < end && inv_b[lo] == b) ? lo : -1;
+        __syncthreads();
+        int loc[INV_PER], run = 0;
+#pragma unroll
+        for (int u = 0; u < INV_PER; ++u) {
+            const int w = tid * INV_PER + u;
+            loc[u] = run;
+            run += w < W ? __popc(bm[w]) : 0;
+        }
+        int x = run;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += v;
+        }
+        if (lane == 31) wsum[wp] = x;
+        __syncthreads();
+        int base = x - run;
+        for (int w = 0; w < wp; ++w) base += wsum[w];
+#pragma unroll
+        for (int u = 0; u < INV_PER; ++u) {
+            const int w = tid * INV_PER + u;
+            if (w < W) pre[w] = base + loc[u];
+        }
+        __syncthreads();
+        for (int64_t i = tid; i < L; i += 256) {
+            const int b = tmp_b[off + i];
+            const int r = pre[b >> 5] + __popc(bm[b >> 5] & ((1u << (b & 31)) - 1u));
+            inv_b[off + r] = b;
+            fwd2inv[tmp_k[off + i]] = off + r;
+        }
+        return;
+    }
+    if (L <= INV_TILE) {
+        int n = 2;
+        while (n < L) n <<= 1;
+        for (int i = tid; i < n; i += 256) {
+            sb[i] = i < L ? tmp_b[off + i] : 0x7fffffff;
+            si[i] = (short)i;
+        }
+        __syncthreads();
+        for (int k = 2; k <= n; k <<= 1) {
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                for (int i = tid; i < n; i += 256) {
+                    const int p = i ^ j;
+                    if (p > i) {
+                        const int a = sb[i], b = sb[p];
+                        if ((a > b) == ((i & k) == 0)) {
+                            sb[i] = b;
+                            sb[p] = a;
+                            const short x = si[i];
+                            si[i] = si[p];
+                            si[p] = x;
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        for (int i = tid; i < L; i += 256) {
+            inv_b[off + i] = sb[i];
+            fwd2inv[tmp_k[off + si[i]]] = off + i;
+        }
+        return;
+    }
+    for (int64_t i0 = 0; i0 < L; i0 += INV_TILE) {
+        int mine[INV_PER], rank[INV_PER];
+#pragma unroll
+        for (int u = 0; u < INV_PER; ++u) {
+            const int64_t i = i0 + tid + 256 * u;
+            mine[u] = i < L ? tmp_b[off + i] : 0x7fffffff;
+            rank[u] = 0;
+        }
+        for (int64_t j0 = 0; j0 < L; j0 += INV_TILE) {
+            const int nj = (int)min((int64_t)INV_TILE, L - j0);
+            __syncthreads();
+            for (int j = tid; j < nj; j += 256) sb[j] = tmp_b[off + j0 + j];
+            __syncthreads();
+            for (int j = 0; j < nj; ++j) {
+                const int v = sb[j];
+#pragma unroll
+                for (int u = 0; u < INV_PER; ++u) rank[u] += v < mine[u] ? 1 : 0;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < INV_PER; ++u) {
+            const int64_t i = i0 + tid + 256 * u;
+            if (i < L) {
+                inv_b[off + rank[u]] = mine[u];
+                fwd2inv[tmp_k[off + i]] = off + rank[u];
+            }
+        }
     }
 }
 
@@ -1064,13 +1164,12 @@ sdot_status run_trunc(sdot_ctx *c, const EvalArgs &a, double r)
     cudaError_t e = c->fwd_cnt.alloc(nsb + 1);
     if (e == cudaSuccess) e = c->fwd_off.alloc(nsb + 1);
     if (e == cudaSuccess) e = c->superpair.alloc((size_t)nss * nts);
-    if (e == cudaSuccess) e = c->superpairT.alloc((size_t)nss * nts);
     if (e == cudaSuccess) e = c->shit.alloc((size_t)nss * nts);
     if (e == cudaSuccess) e = c->spidx.alloc((size_t)nss * nts);
     if (e == cudaSuccess) e = c->scount.alloc(nss + 1);
     if (e != cudaSuccess) return cuda_error(c, e, "pair list alloc");
     k_super_pairs<<<(unsigned)(((int64_t)nss * nts + 255) / 256), 256, 0, st>>>(c->ssup_sph32.p, nss, c->tsup_sph32.p,
-                                                                             nts, cr, c->superpair.p, c->superpairT.p);
+                                                                             nts, cr, c->superpair.p);
     k_super_compact<<<(unsigned)(((int64_t)nss * 32 + 255) / 256), 256, 0, st>>>(c->superpair.p, nss, nts, c->shit.p,
                                                                               c->scount.p, c->spidx.p);
     std::vector<int> sc((size_t)nss);
@@ -1086,28 +1185,28 @@ sdot_status run_trunc(sdot_ctx *c, const EvalArgs &a, double r)
     k_fwd_masks<<<gw, 256, 0, st>>>(c->sblk_sph32.p, nsb, c->tblk_sph32.p, ntb, nts, hmax, cr, c->shit.p, c->scount.p,
                                     c->pmask.p, c->pmpre.p, c->fwd_cnt.p);
     k_scan<<<1, 1024, 0, st>>>(c->fwd_cnt.p, nsb, c->fwd_off.p);
-    e = c->inv_cnt.alloc(ntb + 1);
-    if (e == cudaSuccess) e = c->inv_off.alloc(ntb + 1);
-    if (e != cudaSuccess) return cuda_error(c, e, "pair list alloc");
-    const unsigned gt = (unsigned)(((int64_t)ntb * 32 + 255) / 256);
-    k_inv_list<false><<<gt, 256, 0, st>>>(c->sblk_sph32.p, nsb, nss, c->tblk_sph32.p, ntb, nts, cr, c->superpairT.p,
-                                          nullptr, c->inv_cnt.p, nullptr);
-    k_scan<<<1, 1024, 0, st>>>(c->inv_cnt.p, ntb, c->inv_off.p);
-    int64_t tot[2] = {0, 0};
-    e = cudaMemcpyAsync(&tot[0], c->fwd_off.p + nsb, 8, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&tot[1], c->inv_off.p + ntb, 8, cudaMemcpyDeviceToHost, st);
+    int64_t npairs = 0;
+    e = cudaMemcpyAsync(&npairs, c->fwd_off.p + nsb, 8, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return cuda_error(c, e, "pair list count");
-    if (tot[0] != tot[1]) return set_error(c, SDOT_ECUDA, "block-pair lists disagree");
-    const int64_t npairs = tot[0];
     e = c->fwd_t.alloc(npairs + 1);
     if (e == cudaSuccess) e = c->inv_b.alloc(npairs + 1);
     if (e == cudaSuccess) e = c->fwd2inv.alloc(npairs + 1);
+    if (e == cudaSuccess) e = c->inv_tmpb.alloc(npairs + 1);
+    if (e == cudaSuccess) e = c->inv_tmpk.alloc(npairs + 1);
+    if (e == cudaSuccess) e = c->inv_cnt.alloc(ntb + 1);
+    if (e == cudaSuccess) e = c->inv_off.alloc(ntb + 1);
     if (e != cudaSuccess) return cuda_error(c, e, "pair list alloc");
     k_fwd_fill<<<gw, 256, 0, st>>>(nsb, nts, hmax, c->shit.p, c->scount.p, c->pmask.p, c->fwd_off.p, c->fwd_t.p);
-    k_inv_list<true><<<gt, 256, 0, st>>>(c->sblk_sph32.p, nsb, nss, c->tblk_sph32.p, ntb, nts, cr, c->superpairT.p,
-                                         c->inv_off.p, nullptr, c->inv_b.p);
-    k_fwd2inv<<<gw, 256, 0, st>>>(nsb, c->fwd_off.p, c->fwd_t.p, c->inv_off.p, c->inv_b.p, c->fwd2inv.p);
+    unsigned long long *icnt = reinterpret_cast<unsigned long long *>(c->inv_cnt.p);
+    e = cudaMemsetAsync(c->inv_cnt.p, 0, (ntb + 1) * sizeof(int64_t), st);
+    if (e != cudaSuccess) return cuda_error(c, e, "pair list clear");
+    k_inv_count<<<gw, 256, 0, st>>>(nsb, c->fwd_off.p, c->fwd_t.p, icnt);
+    k_scan<<<1, 1024, 0, st>>>(c->inv_cnt.p, ntb, c->inv_off.p);
+    e = cudaMemsetAsync(c->inv_cnt.p, 0, (ntb + 1) * sizeof(int64_t), st);
+    if (e != cudaSuccess) return cuda_error(c, e, "pair list clear");
+    k_inv_scatter<<<gw, 256, 0, st>>>(nsb, c->fwd_off.p, c->fwd_t.p, c->inv_off.p, icnt, c->inv_tmpb.p, c->inv_tmpk.p);
+    k_inv_order<<<(unsigned)ntb, 256, 0, st>>>(nsb, c->inv_off.p, c->inv_tmpb.p, c->inv_tmpk.p, c->inv_b.p, c->fwd2inv.p);
     c->klaunch[6] += 9;
     if (c->profiling) cudaEventRecord(c->pev[7], st);
     // 2. partial buffer (inverse order): all pairs at once under the cap, else target-block groups
