@@ -51,6 +51,14 @@ namespace sdot {
 
 constexpr int FT_WARPS = 8;
 constexpr int FT_MAXS = 1024;               // staged targets per chunk
+// The 3D tensor-factored hybrid sweeps stage at most 624 targets per chunk so that
+// their shared memory (75,312 B) lets 3 CTAs share an SM (24 warps instead of
+// 16; registers capped at 80): measured 3.99 ms per trunc_3d evaluation against
+// 4.19 ms with 1,024 targets and 2 CTAs, although more blocks need several chunks.
+constexpr int FT_MAXS_TENSOR = 624;
+__host__ __device__ constexpr bool fused_small(int dim, int tq, bool fp32b) { return dim == 3 && tq > 0 && fp32b; }
+__host__ __device__ constexpr int fused_cap(int dim, int tq, bool fp32b) { return fused_small(dim, tq, fp32b) ? FT_MAXS_TENSOR : FT_MAXS; }
+__host__ __device__ constexpr int fused_min_blocks(int dim, int tq, bool fp32b) { return fused_small(dim, tq, fp32b) ? 3 : 2; }
 constexpr int FT_TS = 6;                    // doubles per staged target: y(3), nu, log2 nu, s*psi
 constexpr int FT_MAXT = 96;                 // target blocks per chunk
 constexpr int FT_MAXQ = 80;                 // quadrature points of one source block
@@ -76,9 +84,11 @@ struct FusedArgs {
     double cullt;                // per-target cull radius addend (r, enlarged)
 };
 
+template <int CAP>
 struct FTSmem {
+    static constexpr int MAXS = CAP;
     double tab[16];
-    double stg[FT_TS][FT_MAXS];    // staged targets, structure of arrays (conflict-free lane access)
+    double stg[FT_TS][CAP];    // staged targets, structure of arrays (conflict-free lane access)
     double qd[FT_MAXQ][4];        // delta_q (FP64) and C'_q
     double qn[FT_MAXQ];           // |delta_q|
     double qL[FT_MAXQ];           // L_q of the block
@@ -86,8 +96,8 @@ struct FTSmem {
     float qw[FT_MAXQ];            // pass B: w_q
     float qtw[FT_MAXQ];           // pass B, tensor path: w_q 2^(D_q)
     double cellc[FT_WARPS][3];    // centre of each cell of the block
-    float pvw[FT_WARPS][FT_MAXS]; // gradient partial of each unit (warp) per staged target (FP32 mode)
-    unsigned short cand[FT_WARPS][FT_MAXS];
+    float pvw[FT_WARPS][CAP];     // gradient partial of each unit (warp) per staged target (FP32 mode)
+    unsigned short cand[FT_WARPS][CAP];
     short smap[FT_MAXT][TBLK_KD]; // (chunk target block, slot) -> staged position or -1
     int ctb[FT_MAXT];             // target blocks of the chunk
     int64_t cpos[FT_MAXT];        // their partial base index
@@ -107,13 +117,13 @@ struct FTSmem {
 // the warps' rows).
 template <bool FP32B> struct PRow { using T = double; };
 template <> struct PRow<true> { using T = float; };
-constexpr size_t FT_ROWS64_BYTES = sizeof(double) * FT_WARPS * FT_MAXS;
+__host__ __device__ constexpr size_t ft_rows64_bytes(int cap) { return sizeof(double) * FT_WARPS * cap; }
 
-template <bool FP32B>
-__device__ __forceinline__ typename PRow<FP32B>::T *partial_rows(FTSmem &sm)
+template <bool FP32B, class SM>
+__device__ __forceinline__ typename PRow<FP32B>::T *partial_rows(SM &sm)
 {
     if constexpr (FP32B) return &sm.pvw[0][0];
-    else return reinterpret_cast<double *>(reinterpret_cast<unsigned char *>(&sm) + sizeof(FTSmem));
+    else return reinterpret_cast<double *>(reinterpret_cast<unsigned char *>(&sm) + sizeof(SM));
 }
 
 // ---------------------------------------------------------------------------
@@ -407,8 +417,8 @@ __global__ void __launch_bounds__(1024) k_scan(const int64_t *__restrict__ cnt, 
 // target), counts its survivors with a ballot, and whole target blocks are
 // accepted in list order while the staged total fits FT_MAXS.  Returns the
 // number of forward entries consumed; staged order = (target block, slot).
-template <int DIM>
-__device__ int stage_chunk(FTSmem &sm, const FusedArgs &f, int64_t kb, int64_t k0, int64_t k1, const double *bc,
+template <int DIM, class SM>
+__device__ int stage_chunk(SM &sm, const FusedArgs &f, int64_t kb, int64_t k0, int64_t k1, const double *bc,
                            double rcull2, bool for_b)
 {
     constexpr int SUB = 4;                       // target blocks per warp per iteration
@@ -470,7 +480,7 @@ __device__ int stage_chunk(FTSmem &sm, const FusedArgs &f, int64_t kb, int64_t k
                 if (lane >= o) incl += v;
             }
             const int excl = incl - (cv < 0 ? 0 : cv);
-            const unsigned bad = __ballot_sync(0xffffffffu, cv < 0 || total + incl > FT_MAXS);
+            const unsigned bad = __ballot_sync(0xffffffffu, cv < 0 || total + incl > SM::MAXS);
             const int na = bad ? __ffs(bad) - 1 : 32;
             sm.epre[lane] = total + excl;
             const int accsum = __shfl_sync(0xffffffffu, incl, na > 0 ? na - 1 : 0);
@@ -518,8 +528,8 @@ __device__ int stage_chunk(FTSmem &sm, const FusedArgs &f, int64_t kb, int64_t k
 }
 
 // Exact squared distance from a staged target (SoA) to a cell centre.
-template <int DIM>
-__device__ __forceinline__ double stg_dist2(const FTSmem &sm, int t, const double *c)
+template <int DIM, class SM>
+__device__ __forceinline__ double stg_dist2(const SM &sm, int t, const double *c)
 {
     const double y[3] = {sm.stg[0][t], sm.stg[1][t], DIM == 3 ? sm.stg[2][t] : 0.0};
     return dist2_exact<DIM>(y, c);
@@ -531,8 +541,8 @@ __device__ __forceinline__ double stg_dist2(const FTSmem &sm, int t, const doubl
 //         (when the bound could sit more than 2^500 above the true maximum).
 // NQ: quadrature points handled (== QL for full units: straight-line code
 //     whose NQ exponential chains interleave).
-template <int DIM, int QL, int NQ, int MODE>
-__device__ __forceinline__ void value_pairs(const FTSmem &sm, int wp, int lane, int ncand, int qoff, double cc0,
+template <int DIM, int QL, int NQ, int MODE, class SM>
+__device__ __forceinline__ void value_pairs(const SM &sm, int wp, int lane, int ncand, int qoff, double cc0,
                                             double cc1, double cc2, const EvalArgs &a, double Munit, double *M,
                                             double *S, double *mx)
 {
@@ -561,8 +571,8 @@ __device__ __forceinline__ void value_pairs(const FTSmem &sm, int wp, int lane, 
 }
 
 // Units with fewer than QL quadrature points (the last q-group of a cell).
-template <int DIM, int QL, int MODE>
-__device__ __noinline__ void value_pairs_partial(const FTSmem &sm, int wp, int lane, int ncand, int qoff, int nql,
+template <int DIM, int QL, int MODE, class SM>
+__device__ __noinline__ void value_pairs_partial(const SM &sm, int wp, int lane, int ncand, int qoff, int nql,
                                                  double cc0, double cc1, double cc2, const EvalArgs &a, double Munit,
                                                  double *M, double *S, double *mx)
 {
@@ -595,8 +605,8 @@ __device__ __noinline__ void value_pairs_partial(const FTSmem &sm, int wp, int l
 // Exact candidate test of the staged targets for the warp's cell, in-order
 // compaction into sm.cand[wp]; returns the count and (through bmax) the
 // largest B0_Kj = kappa (psi_j - d2/2)/eps over the candidates.
-template <int DIM>
-__device__ __forceinline__ int compact_candidates(FTSmem &sm, int wp, int lane, int nstg, const double *cc,
+template <int DIM, class SM>
+__device__ __forceinline__ int compact_candidates(SM &sm, int wp, int lane, int nstg, const double *cc,
                                                   const EvalArgs &a, double &bmax)
 {
     constexpr int U = 4;  // staged targets per lane in flight (independent distance chains)
@@ -630,8 +640,8 @@ __device__ __forceinline__ int compact_candidates(FTSmem &sm, int wp, int lane, 
 // candidate target j (lane-strided) the unit's part of sum_q w_q nu_j
 // e^{t_qj - L_q}, written to the warp's partial row (FP32).  E0 and G' are
 // formed in FP64 per (cell, target) so that every FP32 operand is small.
-template <int DIM, bool FP32B>
-__device__ __forceinline__ void grad_pairs(FTSmem &sm, const FusedArgs &f, int wp, int lane, int ncand, int qoff,
+template <int DIM, bool FP32B, class SM>
+__device__ __forceinline__ void grad_pairs(SM &sm, const FusedArgs &f, int wp, int lane, int ncand, int qoff,
                                            int nql, const double *cc, double Lref, int64_t qblk0, const EvalArgs &a)
 {
     const float sf = (float)(a.s * (1.0 / 16.0));
@@ -692,7 +702,7 @@ __device__ __forceinline__ void grad_pairs(FTSmem &sm, const FusedArgs &f, int w
             }
             val = acc;
         }
-        partial_rows<FP32B>(sm)[wp * FT_MAXS + ti] = (typename PRow<FP32B>::T)val;
+        partial_rows<FP32B>(sm)[wp * SM::MAXS + ti] = (typename PRow<FP32B>::T)val;
     }
 }
 
@@ -712,8 +722,8 @@ __device__ __forceinline__ constexpr int tstride()
 // candidates that can attain it: b_qj lies within s r |delta|max of B0_Kj, so
 // a candidate with B0 below (running max B0) - 2 s r |delta|max is never a
 // maximum; thr is that bound relative to Munit.
-template <int DIM, int TM>
-__device__ __forceinline__ void value_pairs_tensor(const FTSmem &sm, int wp, int lane, int ncand, int qoff,
+template <int DIM, int TM, class SM>
+__device__ __forceinline__ void value_pairs_tensor(const SM &sm, int wp, int lane, int ncand, int qoff,
                                                    const double *cc, const EvalArgs &a, double Munit, double thr,
                                                    double *S, double *mx)
 {
@@ -779,8 +789,8 @@ __device__ __forceinline__ float rcp_approx(float x)
 // FP32 gradient sweep on tensor-product points: per candidate
 // 2^(e0) sum_q W_q prod_d F_d[i_d], W_q = w_q 2^(D_q), summed dimension by
 // dimension (Horner order), into the warp's partial row.
-template <int DIM, int TM>
-__device__ __forceinline__ void grad_pairs_tensor(FTSmem &sm, int wp, int lane, int ncand, int qoff,
+template <int DIM, int TM, class SM>
+__device__ __forceinline__ void grad_pairs_tensor(SM &sm, int wp, int lane, int ncand, int qoff,
                                                   const double *cc, double Lref, const EvalArgs &a)
 {
     constexpr int NQ = DIM == 3 ? TM * TM * TM : TM * TM;
@@ -830,14 +840,14 @@ __device__ __forceinline__ void grad_pairs_tensor(FTSmem &sm, int wp, int lane, 
                 w = fmaf(u, F[0][i0], w);
             }
         }
-        partial_rows<true>(sm)[wp * FT_MAXS + ti] = ex2_approx(e0) * w;
+        partial_rows<true>(sm)[wp * SM::MAXS + ti] = ex2_approx(e0) * w;
     }
 }
 
 // CTA sum of the warp partial rows (warp order) and the write of every slot
 // of every pair of the chunk (zeros where a target was not staged).
-template <bool FP32B>
-__device__ __forceinline__ void write_partials(FTSmem &sm, const FusedArgs &f, int nt, int nunit)
+template <bool FP32B, class SM>
+__device__ __forceinline__ void write_partials(SM &sm, const FusedArgs &f, int nt, int nunit)
 {
     const typename PRow<FP32B>::T *rows = partial_rows<FP32B>(sm);
     const int tid = threadIdx.x;
@@ -848,17 +858,18 @@ __device__ __forceinline__ void write_partials(FTSmem &sm, const FusedArgs &f, i
         const short p = sm.smap[ti][sl];
         double v = 0.0;
         if (p >= 0)
-            for (int w = 0; w < nunit; ++w) v += (double)rows[w * FT_MAXS + p];
+            for (int w = 0; w < nunit; ++w) v += (double)rows[w * SM::MAXS + p];
         f.part[base + sl] = v;
     }
 }
 
 template <int DIM, int QL, bool FP32B, int MODE, int TQ>
-__global__ void __launch_bounds__(FT_WARPS * 32, 2)
+__global__ void __launch_bounds__(FT_WARPS * 32, fused_min_blocks(DIM, TQ, FP32B))
 k_fused(FusedArgs f, EvalArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    FTSmem &sm = *reinterpret_cast<FTSmem *>(smem_raw);
+    using SMem = FTSmem<fused_cap(DIM, TQ, FP32B)>;
+    SMem &sm = *reinterpret_cast<SMem *>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
     const int b = blockIdx.x;
     if (tid < 16) sm.tab[tid] = c_exp2_tab[tid];
@@ -1027,7 +1038,7 @@ k_fused(FusedArgs f, EvalArgs a)
         const int nt = (int)(single_end - k0);
         const int nstg = sm.nstg;
         if (valid) {
-            for (int t = lane; t < nstg; t += 32) partial_rows<FP32B>(sm)[wp * FT_MAXS + t] = 0;
+            for (int t = lane; t < nstg; t += 32) partial_rows<FP32B>(sm)[wp * SMem::MAXS + t] = 0;
             __syncwarp();
             if (isfinite(Lref)) {
                 if constexpr (TQ > 0 && FP32B) grad_pairs_tensor<DIM, TQ>(sm, wp, lane, ncand_single, qoff, cc, Lref, a);
@@ -1049,7 +1060,7 @@ k_fused(FusedArgs f, EvalArgs a)
         if (valid) {
             double bmax;
             const int ncand = compact_candidates<DIM>(sm, wp, lane, nstg, cc, a, bmax);
-            for (int t = lane; t < nstg; t += 32) partial_rows<FP32B>(sm)[wp * FT_MAXS + t] = 0;
+            for (int t = lane; t < nstg; t += 32) partial_rows<FP32B>(sm)[wp * SMem::MAXS + t] = 0;
             __syncwarp();
             if (isfinite(Lref)) {
                 if constexpr (TQ > 0 && FP32B) grad_pairs_tensor<DIM, TQ>(sm, wp, lane, ncand, qoff, cc, Lref, a);
@@ -1091,14 +1102,18 @@ template <int DIM, int QL, bool FP32B, int MODE, int TQ>
 static void launch_fused(sdot_ctx *c, const FusedArgs &f, const EvalArgs &a, size_t smem, int nb)
 {
     cudaFuncSetAttribute(k_fused<DIM, QL, FP32B, MODE, TQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_fused<DIM, QL, FP32B, MODE, TQ>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         (int)cudaSharedmemCarveoutMaxShared);
     k_fused<DIM, QL, FP32B, MODE, TQ><<<(unsigned)nb, FT_WARPS * 32, smem, c->stream>>>(f, a);
 }
 
 template <int DIM, int QL, int MODE, int TQ = 0>
 static void dispatch_fused_b(sdot_ctx *c, const FusedArgs &f, const EvalArgs &a, bool fp32b, int nb)
 {
-    if (fp32b) launch_fused<DIM, QL, true, MODE, TQ>(c, f, a, sizeof(FTSmem), nb);
-    else launch_fused<DIM, QL, false, MODE, TQ>(c, f, a, sizeof(FTSmem) + FT_ROWS64_BYTES, nb);
+    if (fp32b) launch_fused<DIM, QL, true, MODE, TQ>(c, f, a, sizeof(FTSmem<fused_cap(DIM, TQ, true)>), nb);
+    else
+        launch_fused<DIM, QL, false, MODE, TQ>(c, f, a, sizeof(FTSmem<fused_cap(DIM, TQ, false)>) + ft_rows64_bytes(fused_cap(DIM, TQ, false)),
+                                               nb);
 }
 
 template <int DIM, int MODE>
