@@ -29,7 +29,7 @@ namespace sdot {
 constexpr int SBLK_UNITS = 8;        // warp units (cell, q-group) per source block
 constexpr int TBLK_KD = 32;          // max targets per target block (k-d tree leaf)
 constexpr int DENSE_A_THREADS = 128; // dense value sweep: threads per CTA
-constexpr int DENSE_A_QT = 4;        // dense value sweep: quadrature points per thread
+constexpr int DENSE_A_QT = 1;        // dense value sweep: quadrature points per thread (1: the most CTAs for small sources)
 constexpr int DENSE_B_THREADS = 128; // dense gradient sweep: threads per CTA
 constexpr int DENSE_B_TT = 2;        // dense gradient sweep: targets per thread
 constexpr int TPACK = 8;             // doubles per packed target
