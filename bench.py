@@ -54,16 +54,23 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="trunc_3d",
                     choices=["trunc_3d", "dense_2d", "newton_3d", "hessian_3d", "batched_2d", "serve_3d"])
-    ap.add_argument("--problems", type=int, default=256, help="batched_2d: problems; serve_3d: requests")
-    ap.add_argument("--rate", type=float, default=2.0, help="serve_3d: Poisson arrival rate (requests/s)")
+    ap.add_argument("--problems", type=int, default=None,
+                    help="batched_2d: problems (default 256); serve_3d: requests (default 60)")
+    ap.add_argument("--rate", type=float, default=4.0, help="serve_3d: Poisson arrival rate (requests/s)")
     ap.add_argument("--slots", type=int, default=4, help="batched_2d / serve_3d: concurrent solve slots")
     ap.add_argument("--baseline-seconds", type=float, default=60.0,
                     help="solve workloads: wall budget of the one-at-a-time FP64 L-BFGS baseline")
     ap.add_argument("--precision", default="hybrid", choices=["hybrid", "fp64", "mixed"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--scale", type=float, default=1.0, help="shrink the workload (tests only)")
-    return ap.parse_args()
+    ap.add_argument("--scale", type=float, default=None,
+                    help="shrink the workload (default 1; serve_3d: 0.5, the request sizes it is documented at)")
+    args = ap.parse_args()
+    if args.problems is None:
+        args.problems = 60 if args.workload == "serve_3d" else 256
+    if args.scale is None:
+        args.scale = 0.5 if args.workload == "serve_3d" else 1.0
+    return args
 
 
 def make_workload(name: str, scale: float):
