@@ -383,29 +383,39 @@ k_inv_order(int nsb, const int64_t *__restrict__ inv_off, const int *__restrict_
 // exclusive scan of n counts into off[0..n] (single CTA, order-fixed)
 __global__ void __launch_bounds__(1024) k_scan(const int64_t *__restrict__ cnt, int64_t n, int64_t *__restrict__ off)
 {
-    __shared__ int64_t part[1024];
-    const int tid = threadIdx.x;
-    const int64_t per = (n + 1023) / 1024;
-    const int64_t a = tid * per, b = min(n, a + per);
-    int64_t s = 0;
-    for (int64_t i = a; i < b; ++i) s += cnt[i];
-    part[tid] = s;
-    __syncthreads();
-    if (tid == 0) {
-        int64_t acc = 0;
-        for (int i = 0; i < 1024; ++i) {
-            const int64_t v = part[i];
-            part[i] = acc;
-            acc += v;
+    // coalesced tiles of 1,024 counts: warp-shuffle inclusive scans, the warp
+    // totals scanned by warp 0, a running carry across tiles (integer sums:
+    // exact in any order)
+    __shared__ long long wsum[32];
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    long long carry = 0;
+    for (int64_t t0 = 0; t0 < n; t0 += 1024) {
+        const int64_t i = t0 + tid;
+        const long long v = i < n ? (long long)cnt[i] : 0;
+        long long x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
         }
-        off[n] = acc;
+        if (lane == 31) wsum[w] = x;
+        __syncthreads();
+        if (w == 0) {
+            long long z = wsum[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const long long y = __shfl_up_sync(0xffffffffu, z, o);
+                if (lane >= o) z += y;
+            }
+            wsum[lane] = z;
+        }
+        __syncthreads();
+        const long long before = w > 0 ? wsum[w - 1] : 0;
+        if (i < n) off[i] = (int64_t)(carry + before + x - v);
+        carry += wsum[31];
+        __syncthreads();  // wsum is rewritten by the next tile
     }
-    __syncthreads();
-    s = part[tid];
-    for (int64_t i = a; i < b; ++i) {
-        off[i] = s;
-        s += cnt[i];
-    }
+    if (tid == 0) off[n] = (int64_t)carry;
 }
 
 // ---------------------------------------------------------------------------
