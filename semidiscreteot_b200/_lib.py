@@ -35,7 +35,7 @@ EXPORTED = [
     "sdot_compute_geometric_radius_bound", "sdot_set_distance_function", "sdot_evaluate_partial_device",
     "sdot_set_state", "sdot_get_stream", "sdot_set_profiling", "sdot_get_kernel_times", "sdot_measure_peaks",
     "sdot_evaluate_device_noalloc", "sdot_hessian_device", "sdot_set_hessian_chunk",
-    "sdot_solve_newton", "sdot_softmax_refinement", "sdot_weighted_barycenters", "sdot_conditioned_densities",
+    "sdot_solve_newton", "sdot_set_newton_hessian_reuse", "sdot_softmax_refinement", "sdot_weighted_barycenters", "sdot_conditioned_densities",
     "sdot_batch_create", "sdot_batch_destroy", "sdot_batch_last_error", "sdot_batch_size", "sdot_batch_set_verbose",
     "sdot_batch_add", "sdot_batch_evaluate", "sdot_batch_solve", "sdot_batch_problem_info",
     "sdot_server_create", "sdot_server_destroy", "sdot_server_last_error", "sdot_server_submit", "sdot_server_poll",
@@ -76,7 +76,7 @@ class NewtonInfo(C.Structure):
     _fields_ = [("iterations", C.c_uint), ("converged", C.c_int), ("n_evaluations", C.c_int64),
                 ("cg_iterations", C.c_int64), ("last_value", C.c_double), ("last_check_value", C.c_double),
                 ("total_pairs", C.c_int64), ("eval_ms", C.c_double), ("hessian_ms", C.c_double),
-                ("cg_ms", C.c_double), ("hessian_method", C.c_int)]
+                ("cg_ms", C.c_double), ("hessian_method", C.c_int), ("n_hessians", C.c_int64)]
 
 
 class BatchOptions(C.Structure):
@@ -168,6 +168,8 @@ def load():
     lib.sdot_set_hessian_chunk.restype = ip
     lib.sdot_solve_newton.argtypes = [vp, vp, C.POINTER(SolverParams), ip, C.POINTER(NewtonInfo)]
     lib.sdot_solve_newton.restype = ip
+    lib.sdot_set_newton_hessian_reuse.argtypes = [vp, d]
+    lib.sdot_set_newton_hessian_reuse.restype = ip
     lib.sdot_softmax_refinement.argtypes = [vp, vp, d, d, ip, i64, vp, vp, vp, vp]
     lib.sdot_softmax_refinement.restype = ip
     lib.sdot_weighted_barycenters.argtypes = [vp, vp, vp]

@@ -312,9 +312,16 @@ extern "C" sdot_status sdot_solve_newton(sdot_ctx *c, double *psi, const sdot_so
     unsigned k = 0;
     int conv = solver_control_check(c, k, &check);
     sdot_status result = SDOT_OK;
+    bool have_H = false;             // a Hessian of an earlier step is in nt_H32 / nt_H64
+    double g2_prev = 0.0, alpha_prev = 0.0;
+    int64_t n_hess = 0;
+    bool tensor = false;
     while (conv == 0) {
+        const double g2 = std::sqrt(c->scal_host[SC_L2SQ]);
+        // keep the previous Hessian after a full step that contracted |g|_2 by newton_reuse
+        const bool reuse = have_H && c->newton_reuse > 0.0 && alpha_prev == 1.0 && g2 <= c->newton_reuse * g2_prev;
         // Hessian at psi (uses L_q, g and the threshold of the evaluation just made)
-        const bool tensor = hessian_method != SDOT_HESS_FP64 && hessian_tensor_ok(c);
+        if (!reuse) tensor = hessian_method != SDOT_HESS_FP64 && hessian_tensor_ok(c);
         if (hessian_method == SDOT_HESS_TENSOR && !tensor) {
             result = set_error(c, SDOT_EINVAL,
                                "tensor-core Hessian needs an untruncated evaluation (tau <= 0 or a threshold above "
@@ -323,18 +330,23 @@ extern "C" sdot_status sdot_solve_newton(sdot_ctx *c, double *psi, const sdot_so
         }
         used_method = tensor ? SDOT_HESS_TENSOR : SDOT_HESS_FP64;
         if ((s = launch_scatter(c, v.gc, c->grad.p, n)) != SDOT_OK) { result = s; break; }
-        cudaEventRecord(t0, c->stream);
-        if (tensor) {
-            if ((e = c->nt_H32.alloc((size_t)n * n)) != cudaSuccess) { result = cuda_error(c, e, "alloc Hessian"); break; }
-            s = hessian_tc(c, c->nt_H32.p, true, c->hess_chunk, nullptr);
-        } else {
-            if ((e = c->nt_H64.alloc((size_t)n * n)) != cudaSuccess) { result = cuda_error(c, e, "alloc Hessian"); break; }
-            s = hessian_fp64_to(c, c->nt_H64.p);
+        if (!reuse) {
+            cudaEventRecord(t0, c->stream);
+            if (tensor) {
+                if ((e = c->nt_H32.alloc((size_t)n * n)) != cudaSuccess) { result = cuda_error(c, e, "alloc Hessian"); break; }
+                s = hessian_tc(c, c->nt_H32.p, true, c->hess_chunk, nullptr);
+            } else {
+                if ((e = c->nt_H64.alloc((size_t)n * n)) != cudaSuccess) { result = cuda_error(c, e, "alloc Hessian"); break; }
+                s = hessian_fp64_to(c, c->nt_H64.p);
+            }
+            cudaEventRecord(t1, c->stream);
+            if (s != SDOT_OK) { result = s; break; }
+            cudaEventSynchronize(t1);
+            hess_ms += elapsed(t0, t1);
+            have_H = true;
+            ++n_hess;
         }
-        cudaEventRecord(t1, c->stream);
-        if (s != SDOT_OK) { result = s; break; }
-        cudaEventSynchronize(t1);
-        hess_ms += elapsed(t0, t1);
+        g2_prev = g2;
 
         // inexact Newton forcing term: eta = min(0.5, sqrt(|g|_2)), floored at 1e-10
         const double gnorm = std::sqrt(c->scal_host[SC_L2SQ]);
@@ -387,6 +399,7 @@ extern "C" sdot_status sdot_solve_newton(sdot_ctx *c, double *psi, const sdot_so
             result = set_error(c, SDOT_ELINESEARCH, "Newton: no sufficient decrease after 40 step halvings");
             break;
         }
+        alpha_prev = alpha;
         ++k;
         conv = solver_control_check(c, k, &check);
         if (c->verbose)
@@ -412,7 +425,17 @@ extern "C" sdot_status sdot_solve_newton(sdot_ctx *c, double *psi, const sdot_so
         info->hessian_ms = hess_ms;
         info->cg_ms = cg_ms;
         info->hessian_method = used_method;
+        info->n_hessians = n_hess;
     }
     if (result != SDOT_OK) return result;
     return s2;
+}
+
+extern "C" sdot_status sdot_set_newton_hessian_reuse(sdot_ctx *c, double contraction)
+{
+    if (!c) return SDOT_EINVAL;
+    if (!(contraction >= 0.0 && contraction < 1.0))
+        return set_error(c, SDOT_EINVAL, "Hessian reuse contraction must be in [0, 1)");
+    c->newton_reuse = contraction;
+    return SDOT_OK;
 }

@@ -196,12 +196,19 @@ class SotSolver:
                                 "last_value": info.last_value, "last_check_value": info.last_check_value,
                                 "total_pairs": info.total_pairs, "eval_ms": info.eval_ms,
                                 "hessian_ms": info.hessian_ms, "cg_ms": info.cg_ms,
-                                "hessian_method": names.get(info.hessian_method, info.hessian_method)}
+                                "hessian_method": names.get(info.hessian_method, info.hessian_method),
+                                "n_hessians": info.n_hessians}
         # in place also after a failure, like solve (the library writes the last iterate back)
         if isinstance(potential, np.ndarray) and potential is not psi and potential.size == psi.size:
             potential[...] = psi
         self._check(st)
         return psi
+
+    def set_newton_hessian_reuse(self, contraction: float):
+        """Lagged Hessians in solve_newton (sdot_set_newton_hessian_reuse): keep the
+        previous Hessian after a full step that reduced |g|_2 by `contraction`;
+        0 recomputes it every step."""
+        self._check(self._L.sdot_set_newton_hessian_reuse(self._h, float(contraction)))
 
     def softmax_refinement(self, potential_coarse, epsilon: float, threshold: float, y_fine, child_offsets,
                            child_indices, use_log_sum_exp: Optional[bool] = None) -> np.ndarray:
