@@ -116,6 +116,11 @@ public:
         sdot_newton_info info{};
         check(sdot_solve_newton(ctx_, potential.data(), &p, hessian_method, &info), "solve_newton");
     }
+    // Lagged Hessians in solve_newton: keep the Hessian after a full step that reduced |g|_2 by `contraction`
+    // (default 0.1; 0 recomputes it every step).
+    void set_newton_hessian_reuse(double contraction) {
+        check(sdot_set_newton_hessian_reuse(ctx_, contraction), "set_newton_hessian_reuse");
+    }
     // SotSolver::evaluate_weighted_barycenters, euclidean distance (SotSolver.cc:584-660).
     void evaluate_weighted_barycenters(const std::vector<double> &potentials, std::vector<Point> &barycenters_out,
                                        const SolverParameters &params) {
