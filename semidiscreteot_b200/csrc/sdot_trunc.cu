@@ -924,8 +924,8 @@ k_fused(FusedArgs f, EvalArgs a)
     }
     __syncthreads();
     const double cc[3] = {sm.cellc[cl][0], sm.cellc[cl][1], sm.cellc[cl][2]};
-    int chunks = 0;
-    int64_t single_end = -1;  // end of the only chunk, when everything fit in one
+    int64_t tail_start = -1;  // first entry of the value sweep's last chunk, still staged for the gradient sweep
+    int tail_nt = 0;
     int ncand_single = 0;
 
     // ---------------- value sweep ----------------
@@ -949,7 +949,6 @@ k_fused(FusedArgs f, EvalArgs a)
         for (int64_t k = k0; k < k1;) {
             const int nt = stage_chunk<DIM>(sm, f, k0, k, k1, bc, rcull2, f.do_b != 0);
             const int nstg = sm.nstg;
-            ++chunks;
             if (valid) {
                 double bmax;
                 const int ncand = compact_candidates<DIM>(sm, wp, lane, nstg, cc, a, bmax);
@@ -980,8 +979,9 @@ k_fused(FusedArgs f, EvalArgs a)
                                                        M, S, mx);
             }
             k += nt;
-            if (k >= k1 && chunks == 1) {
-                single_end = k;
+            if (k >= k1) {
+                tail_start = k - nt;  // kept staged (with each warp's candidates) for the gradient sweep
+                tail_nt = nt;
             } else {
                 __syncthreads();  // the next chunk overwrites the staged targets
             }
@@ -1043,9 +1043,14 @@ k_fused(FusedArgs f, EvalArgs a)
         }
         __syncwarp();
     }
-    if (single_end >= 0) {
-        // the single chunk's staged targets and this warp's candidates are still in smem
-        const int nt = (int)(single_end - k0);
+    // The value sweep's last chunk (the only one when everything fit) is still
+    // staged with each warp's candidates: its gradient comes first, then the
+    // earlier chunks are staged again (the same chunks: the greedy rule over
+    // [k0, tail_start) ends where the value sweep's did).  Every pair's partial
+    // is written once, so the order of the chunks does not change any sum.
+    int64_t kend = k1;
+    if (tail_start >= 0) {
+        const int nt = tail_nt;
         const int nstg = sm.nstg;
         if (valid) {
             for (int t = lane; t < nstg; t += 32) partial_rows<FP32B>(sm)[wp * SMem::MAXS + t] = 0;
@@ -1057,15 +1062,17 @@ k_fused(FusedArgs f, EvalArgs a)
         }
         if (tid < nt) {
             const int tb = sm.ctb[tid];
-            const int64_t ip = f.fwd2inv[k0 + tid];
+            const int64_t ip = f.fwd2inv[tail_start + tid];
             sm.cpos[tid] = (ip >= 0 && tb >= f.tlo && tb < f.thi) ? (ip - f.part_base) * TBLK_KD : (int64_t)-1;
         }
         __syncthreads();
         write_partials<FP32B>(sm, f, nt, nunit);
-        return;
+        if (tail_start == k0) return;
+        kend = tail_start;
+        __syncthreads();  // the earlier chunks overwrite the staged targets
     }
-    for (int64_t k = k0; k < k1;) {
-        const int nt = stage_chunk<DIM>(sm, f, k0, k, k1, bc, rcull2, true);
+    for (int64_t k = k0; k < kend;) {
+        const int nt = stage_chunk<DIM>(sm, f, k0, k, kend, bc, rcull2, true);
         const int nstg = sm.nstg;
         if (valid) {
             double bmax;
