@@ -924,7 +924,7 @@ k_fused(FusedArgs f, EvalArgs a)
     }
     __syncthreads();
     const double cc[3] = {sm.cellc[cl][0], sm.cellc[cl][1], sm.cellc[cl][2]};
-    int64_t tail_start = -1;  // first entry of the value sweep's last chunk, still staged for the gradient sweep
+    int tail_off = -1;  // first entry (minus k0) of the value sweep's last chunk, still staged for the gradient sweep
     int tail_nt = 0;
     int ncand_single = 0;
 
@@ -980,7 +980,7 @@ k_fused(FusedArgs f, EvalArgs a)
             }
             k += nt;
             if (k >= k1) {
-                tail_start = k - nt;  // kept staged (with each warp's candidates) for the gradient sweep
+                tail_off = (int)(k - nt - k0);  // kept staged (with each warp's candidates) for the gradient sweep
                 tail_nt = nt;
             } else {
                 __syncthreads();  // the next chunk overwrites the staged targets
@@ -1046,10 +1046,10 @@ k_fused(FusedArgs f, EvalArgs a)
     // The value sweep's last chunk (the only one when everything fit) is still
     // staged with each warp's candidates: its gradient comes first, then the
     // earlier chunks are staged again (the same chunks: the greedy rule over
-    // [k0, tail_start) ends where the value sweep's did).  Every pair's partial
+    // [k0, k0 + tail_off) ends where the value sweep's did).  Every pair's partial
     // is written once, so the order of the chunks does not change any sum.
     int64_t kend = k1;
-    if (tail_start >= 0) {
+    if (tail_off >= 0) {
         const int nt = tail_nt;
         const int nstg = sm.nstg;
         if (valid) {
@@ -1062,13 +1062,13 @@ k_fused(FusedArgs f, EvalArgs a)
         }
         if (tid < nt) {
             const int tb = sm.ctb[tid];
-            const int64_t ip = f.fwd2inv[tail_start + tid];
+            const int64_t ip = f.fwd2inv[k0 + tail_off + tid];
             sm.cpos[tid] = (ip >= 0 && tb >= f.tlo && tb < f.thi) ? (ip - f.part_base) * TBLK_KD : (int64_t)-1;
         }
         __syncthreads();
         write_partials<FP32B>(sm, f, nt, nunit);
-        if (tail_start == k0) return;
-        kend = tail_start;
+        if (tail_off == 0) return;
+        kend = k0 + tail_off;
         __syncthreads();  // the earlier chunks overwrite the staged targets
     }
     for (int64_t k = k0; k < kend;) {
