@@ -182,6 +182,24 @@ sdot_status sdot_hessian_device(sdot_ctx *ctx, const double *psi_dev, void *H_de
  * each FP64 drain (default 16). */
 sdot_status sdot_set_hessian_chunk(sdot_ctx *ctx, int stages);
 
+/* The tensor-core Hessian in pieces, for sharding it over GPUs by output tiles
+ * (no reference counterpart: the reference's Hessian is declared only,
+ * SotSolver.h:343-344).  The upper triangle is covered by
+ * sdot_hessian_tile_count tiles of 128 x 256 entries, each entry (a <= b) in
+ * exactly one tile.  sdot_hessian_tiles_device evaluates at psi_dev like
+ * sdot_hessian_device, then computes tiles [tile_begin, tile_end) only,
+ * writing their entries and the mirrored ones of H_dev and leaving every other
+ * entry untouched: with H_dev zeroed first, the matrices of disjoint ranges sum
+ * to the full Hessian, and each one's product with x to its share of H x.
+ * sdot_hessian_matvec_device: y = H x with FP64 accumulation over an n x n
+ * row-major H (float when f32, else double), the product the Newton CG uses;
+ * it returns after the product is complete. */
+sdot_status sdot_hessian_tile_count(sdot_ctx *ctx, int64_t *count);
+sdot_status sdot_hessian_tiles_device(sdot_ctx *ctx, const double *psi_dev, void *H_dev, int out_f32,
+                                      int64_t tile_begin, int64_t tile_end, sdot_hessian_info *info);
+sdot_status sdot_hessian_matvec_device(sdot_ctx *ctx, const void *H_dev, int f32, const double *x_dev,
+                                       double *y_dev);
+
 /* Newton solver with the tensor-core Hessian.  The reference declares the
  * Hessian (SotSolver::compute_hessian, SotSolver.h:343-344) but solves only
  * with deal.II SolverBFGS (SotSolver::solve, SotSolver.cc:105-215); this is

@@ -35,7 +35,8 @@ EXPORTED = [
     "sdot_compute_geometric_radius_bound", "sdot_set_distance_function", "sdot_evaluate_partial_device",
     "sdot_set_state", "sdot_get_stream", "sdot_set_profiling", "sdot_get_kernel_times", "sdot_measure_peaks",
     "sdot_evaluate_device_noalloc", "sdot_hessian_device", "sdot_set_hessian_chunk",
-    "sdot_solve_newton", "sdot_set_newton_hessian_reuse", "sdot_softmax_refinement", "sdot_weighted_barycenters", "sdot_conditioned_densities",
+    "sdot_solve_newton", "sdot_set_newton_hessian_reuse", "sdot_hessian_tile_count", "sdot_hessian_tiles_device",
+    "sdot_hessian_matvec_device", "sdot_softmax_refinement", "sdot_weighted_barycenters", "sdot_conditioned_densities",
     "sdot_batch_create", "sdot_batch_destroy", "sdot_batch_last_error", "sdot_batch_size", "sdot_batch_set_verbose",
     "sdot_batch_add", "sdot_batch_evaluate", "sdot_batch_solve", "sdot_batch_problem_info",
     "sdot_server_create", "sdot_server_destroy", "sdot_server_last_error", "sdot_server_submit", "sdot_server_poll",
@@ -169,6 +170,12 @@ def load():
     lib.sdot_solve_newton.argtypes = [vp, vp, C.POINTER(SolverParams), ip, C.POINTER(NewtonInfo)]
     lib.sdot_solve_newton.restype = ip
     lib.sdot_set_newton_hessian_reuse.argtypes = [vp, d]
+    lib.sdot_hessian_tile_count.argtypes = [vp, C.POINTER(i64)]
+    lib.sdot_hessian_tile_count.restype = ip
+    lib.sdot_hessian_tiles_device.argtypes = [vp, vp, vp, ip, i64, i64, C.POINTER(HessianInfo)]
+    lib.sdot_hessian_tiles_device.restype = ip
+    lib.sdot_hessian_matvec_device.argtypes = [vp, vp, ip, vp, vp]
+    lib.sdot_hessian_matvec_device.restype = ip
     lib.sdot_set_newton_hessian_reuse.restype = ip
     lib.sdot_softmax_refinement.argtypes = [vp, vp, d, d, ip, i64, vp, vp, vp, vp]
     lib.sdot_softmax_refinement.restype = ip

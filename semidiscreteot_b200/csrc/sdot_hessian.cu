@@ -254,6 +254,45 @@ extern "C" sdot_status sdot_hessian_device(sdot_ctx *c, const double *psi_dev, v
     return s;
 }
 
+extern "C" sdot_status sdot_hessian_tile_count(sdot_ctx *c, int64_t *count)
+{
+    if (!c || !count) return SDOT_EINVAL;
+    if (c->nt == 0) return sdot::set_error(c, SDOT_ESTATE, "targets not set");
+    *count = sdot::hessian_tc_tiles(c->nt);
+    return SDOT_OK;
+}
+
+extern "C" sdot_status sdot_hessian_tiles_device(sdot_ctx *c, const double *psi_dev, void *H_dev, int out_f32,
+                                                 int64_t tile_begin, int64_t tile_end, sdot_hessian_info *info)
+{
+    if (!c || !psi_dev || !H_dev) return SDOT_EINVAL;
+    if (c->nq == 0 || c->nt == 0) return sdot::set_error(c, SDOT_ESTATE, "measures not set");
+    const int64_t nt = sdot::hessian_tc_tiles(c->nt);
+    if (tile_begin < 0 || tile_end < tile_begin || tile_end > nt)
+        return sdot::set_error(c, SDOT_EINVAL, "tile range outside [0, sdot_hessian_tile_count]");
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != c->device) cudaSetDevice(c->device);
+    sdot_status s = sdot::ensure_eval_buffers(c);
+    double ems = 0, hms = 0;
+    if (s == SDOT_OK) s = sdot::launch_gather(c, c->psi.p, psi_dev, c->nt);
+    if (s == SDOT_OK) s = sdot::evaluate_internal(c, nullptr, c->prm.tolerance, &ems);
+    if (s == SDOT_OK && !sdot::tensor_ok(c))
+        s = sdot::set_error(c, SDOT_EINVAL,
+                            "tensor-core Hessian needs an untruncated evaluation (tau <= 0 or a threshold above the "
+                            "domain diameter) and rho*JxW >= 0");
+    if (s == SDOT_OK) s = sdot::hessian_tc(c, H_dev, out_f32 != 0, c->hess_chunk, &hms, tile_begin, tile_end);
+    if (s == SDOT_OK && info) {
+        info->method = SDOT_HESS_TENSOR;
+        info->eval_ms = ems;
+        info->hessian_ms = hms;
+        info->tiles = c->hess_tiles;
+        info->kernel_ms = c->hess_kernel_ms;
+    }
+    if (prev >= 0 && prev != c->device) cudaSetDevice(prev);
+    return s;
+}
+
 extern "C" sdot_status sdot_set_hessian_chunk(sdot_ctx *c, int stages)
 {
     if (!c || stages < 1) return SDOT_EINVAL;

@@ -570,7 +570,17 @@ __global__ void k_htc_points(int64_t nq, int nst, const double *__restrict__ x, 
 // Tensor-core Hessian at the potential of the last evaluation (c->psi, c->Lq,
 // c->grad must come from an untruncated evaluation).  H_dev: n x n row-major in
 // the caller's target order, double or float.
-sdot_status hessian_tc(sdot_ctx *c, void *H_dev, bool out_f32, int chunk_stages, double *ms_out)
+int64_t hessian_tc_tiles(int64_t n)
+{
+    using namespace htc;
+    const int64_t na = (n + M - 1) / M, nb = (n + N - 1) / N;
+    int64_t k = 0;
+    for (int64_t ta = 0; ta < na; ++ta) k += nb - (ta * M) / N;
+    return k;
+}
+
+sdot_status hessian_tc(sdot_ctx *c, void *H_dev, bool out_f32, int chunk_stages, double *ms_out, int64_t tile_begin,
+                       int64_t tile_end)
 {
     using namespace htc;
     const int64_t n = c->nt;
@@ -582,6 +592,15 @@ sdot_status hessian_tc(sdot_ctx *c, void *H_dev, bool out_f32, int chunk_stages,
     tiles.reserve((size_t)(na * nb));
     for (int64_t ta = 0; ta < na; ++ta)
         for (int64_t tb = (ta * M) / N; tb < nb; ++tb) tiles.push_back(make_int2((int)ta, (int)tb));
+    if (tile_end < 0 || tile_end > (int64_t)tiles.size()) tile_end = (int64_t)tiles.size();
+    if (tile_begin < 0) tile_begin = 0;
+    if (tile_begin > tile_end) tile_begin = tile_end;
+    tiles = std::vector<int2>(tiles.begin() + tile_begin, tiles.begin() + tile_end);
+    if (tiles.empty()) {
+        c->hess_tiles = 0;
+        if (ms_out) *ms_out = 0.0;
+        return SDOT_OK;
+    }
     int dev_sms = 148;
     cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c->device);
     const int grid = (int)std::min<int64_t>((int64_t)dev_sms, (int64_t)tiles.size());

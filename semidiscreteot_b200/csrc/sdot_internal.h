@@ -221,7 +221,12 @@ void launch_target_prep_dense(sdot_ctx *c, const EvalArgs &a);
 
 // Tensor-core Hessian (BF16 hi+lo on tcgen05, FP64 drains) at the potential of
 // the last untruncated evaluation; H_dev n x n row-major in the caller's order.
-sdot_status hessian_tc(sdot_ctx *c, void *H_dev, bool out_f32, int chunk_stages, double *ms_out);
+// Tiles [tile_begin, tile_end) of the upper-triangle tile list only (tile_end < 0: all); entries of other tiles
+// are left untouched.
+sdot_status hessian_tc(sdot_ctx *c, void *H_dev, bool out_f32, int chunk_stages, double *ms_out,
+                       int64_t tile_begin = 0, int64_t tile_end = -1);
+// Number of 128 x 256 tiles of the upper triangle for n targets.
+int64_t hessian_tc_tiles(int64_t n);
 // Evaluation at psi_dev (caller order) followed by the Hessian by `method`.
 sdot_status hessian_device(sdot_ctx *c, const double *psi_dev, void *H_dev, int method, int out_f32,
                            sdot_hessian_info *info);

@@ -439,3 +439,19 @@ extern "C" sdot_status sdot_set_newton_hessian_reuse(sdot_ctx *c, double contrac
     c->newton_reuse = contraction;
     return SDOT_OK;
 }
+
+extern "C" sdot_status sdot_hessian_matvec_device(sdot_ctx *c, const void *H_dev, int f32, const double *x_dev,
+                                                  double *y_dev)
+{
+    if (!c || !H_dev || !x_dev || !y_dev) return SDOT_EINVAL;
+    if (c->nt == 0) return set_error(c, SDOT_ESTATE, "targets not set");
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != c->device) cudaSetDevice(c->device);
+    if (f32) launch_matvec<float>(c, static_cast<const float *>(H_dev), x_dev, y_dev, c->nt);
+    else launch_matvec<double>(c, static_cast<const double *>(H_dev), x_dev, y_dev, c->nt);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (prev >= 0 && prev != c->device) cudaSetDevice(prev);
+    return cuda_error(c, e, "Hessian matvec");
+}

@@ -43,6 +43,7 @@ class SotSolver:
         if st != _lib.SDOT_OK:
             raise _lib.SdotError(st, "sdot_create failed (no CUDA device?)")
         self._h = h
+        self.device = int(device)
         self.precision = precision
         self.current_params = SolverParameters()
         self._n_targets = 0
@@ -288,6 +289,28 @@ class SotSolver:
         names = {v: k for k, v in _lib.HESSIAN_METHOD.items()}
         return {"method": names.get(info.method, info.method), "eval_ms": info.eval_ms,
                 "hessian_ms": info.hessian_ms, "kernel_ms": info.kernel_ms, "tiles": info.tiles}
+
+    def hessian_tile_count(self) -> int:
+        """Number of 128 x 256 upper-triangle tiles of the tensor-core Hessian (sdot_hessian_tile_count)."""
+        k = C.c_int64(0)
+        self._check(self._L.sdot_hessian_tile_count(self._h, C.byref(k)))
+        return k.value
+
+    def compute_hessian_tiles_device(self, psi_ptr: int, hessian_ptr: int, tile_begin: int, tile_end: int,
+                                     out_f32: bool = True) -> dict:
+        """Tiles [tile_begin, tile_end) of the tensor-core Hessian at psi (sdot_hessian_tiles_device):
+        their entries and mirrors are written, every other entry of the n x n buffer is left as it is."""
+        info = _lib.HessianInfo()
+        self._check(self._L.sdot_hessian_tiles_device(self._h, C.c_void_p(psi_ptr), C.c_void_p(hessian_ptr),
+                                                      int(bool(out_f32)), int(tile_begin), int(tile_end),
+                                                      C.byref(info)))
+        return {"eval_ms": info.eval_ms, "hessian_ms": info.hessian_ms, "kernel_ms": info.kernel_ms,
+                "tiles": info.tiles}
+
+    def hessian_matvec_device(self, hessian_ptr: int, x_ptr: int, y_ptr: int, f32: bool = True):
+        """y = H x with FP64 accumulation (sdot_hessian_matvec_device); returns when y is complete."""
+        self._check(self._L.sdot_hessian_matvec_device(self._h, C.c_void_p(hessian_ptr), int(bool(f32)),
+                                                       C.c_void_p(x_ptr), C.c_void_p(y_ptr)))
 
     def set_hessian_chunk(self, stages: int):
         """Stages of 64 points accumulated in FP32 between FP64 drains (tensor Hessian)."""
