@@ -20,6 +20,14 @@ source levels), or params.epsilon when there is none.  The levels are given as
 flattened sources (``setup_source`` dicts); ``nearest_vertex_density`` moves a
 nodal density to a coarser mesh's vertices.
 
+``run_combined_multilevel`` mirrors SemiDiscreteOT::run_combined_multilevel
+(SemiDiscreteOT.cc:1524-1766): max(source levels, target levels) combined
+levels, coarsest first; the hierarchy with more levels advances every level,
+the other starts once the remaining depths line up (both reach their finest
+level together).  When the target level moves one level finer, the potentials
+are transferred (softmax or parent copy, as in the target multilevel driver)
+before the solver is re-targeted; when it does not change they are kept.
+
 ``build_hierarchy`` is a seeded k-means coarsening (k-means++ seeds, Lloyd
 iterations) with the level sizes of PointCloudHierarchyManager::getPointsForLevel
 (src/core/PointCloudHierarchy.cc:63-76): level 1 holds min(N, max_points) points,
@@ -188,4 +196,64 @@ def run_source_multilevel(solver, sources: Sequence[dict], target_points, target
         out.append({"level": len(sources) - 1 - i, "potentials": psi.copy(), "iterations": its,
                     "converged": bool(solver.get_convergence_status()),
                     "threshold": solver.get_last_distance_threshold()})
+    return out
+
+
+def combined_level_indices(n_source: int, n_target: int):
+    """(source index, target index) per combined level, coarsest first, indices
+    counted from the coarsest level of each hierarchy (SemiDiscreteOT.cc:1598-1607)."""
+    out = []
+    for i in range(max(n_source, n_target)):
+        if n_source >= n_target:
+            out.append((i, i - (n_source - n_target) if i >= n_source - n_target else 0))
+        else:
+            out.append((i - (n_target - n_source) if i >= n_target - n_source else 0, i))
+    return out
+
+
+def run_combined_multilevel(solver, sources: Sequence[dict], hierarchy: Dict[str, list], params: SolverParameters,
+                            use_softmax: bool = True,
+                            epsilon_distribution: Optional[Sequence[Sequence[float]]] = None,
+                            initial_potential: Optional[np.ndarray] = None, method: str = "lbfgs") -> List[dict]:
+    """sources: flattened source measures, coarsest first; hierarchy: target
+    levels as from build_hierarchy / io.load_hierarchy (level 0 finest).
+    Returns per combined level its source and target levels, potentials,
+    iterations, convergence and last threshold."""
+    pts, dens, ch = hierarchy["points"], hierarchy["densities"], hierarchy["children"]
+    nt_levels = len(pts)
+    out: List[dict] = []
+    psi = None
+    prev_tl = None
+    for i, (si, ti) in enumerate(combined_level_indices(len(sources), nt_levels)):
+        tl = nt_levels - 1 - ti                       # actual target level (0 = finest)
+        if i == 0:
+            psi = np.zeros(len(dens[tl])) if initial_potential is None else np.array(initial_potential, dtype=np.float64)
+            if psi.size != len(dens[tl]):
+                raise ValueError("initial potential does not match the coarsest target level")
+        elif tl != prev_tl:
+            if prev_tl != tl + 1:
+                raise ValueError("target levels must advance one at a time")
+            off, idx = ch[tl]                         # children (level tl) of the level tl+1 points
+            if use_softmax:
+                psi = solver.softmax_refinement(psi, params.epsilon, solver.get_last_distance_threshold(), pts[tl],
+                                                off, idx, use_log_sum_exp=params.use_log_sum_exp_trick)
+            else:
+                fine = np.zeros(len(dens[tl]))
+                for j in range(len(off) - 1):
+                    fine[idx[off[j]:off[j + 1]]] = psi[j]
+                psi = fine
+        src = sources[si]
+        solver.setup_source(src["x"], src["jxw"], src["density"], src["cell_offsets"], src["cell_centers"])
+        solver.setup_target(pts[tl], dens[tl])
+        eps_list = list(epsilon_distribution[i]) if epsilon_distribution is not None and \
+            i < len(epsilon_distribution) and len(epsilon_distribution[i]) else [params.epsilon]
+        its = 0
+        for eps in eps_list:
+            p = dataclasses.replace(params, epsilon=float(eps))
+            psi = solver.solve_newton(psi, p) if method == "newton" else solver.solve(psi, p)
+            its += solver.get_last_iteration_count()
+        out.append({"source_level": len(sources) - 1 - si, "target_level": tl, "potentials": psi.copy(),
+                    "iterations": its, "converged": bool(solver.get_convergence_status()),
+                    "threshold": solver.get_last_distance_threshold()})
+        prev_tl = tl
     return out

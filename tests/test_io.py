@@ -84,3 +84,13 @@ def test_lloyd_step_norm():
     a = np.zeros((4, 2))
     b = np.array([[3.0, 4.0], [0, 0], [0, 0], [0, 0]])
     assert step_norm(b, a) == np.sqrt(25.0 / 4)
+
+
+def test_combined_level_schedule():
+    from semidiscreteot_b200.multilevel import combined_level_indices
+    assert combined_level_indices(3, 5) == [(0, 0), (0, 1), (0, 2), (1, 3), (2, 4)]
+    assert combined_level_indices(4, 2) == [(0, 0), (1, 0), (2, 0), (3, 1)]
+    for s, t in ((1, 1), (2, 7), (6, 3)):
+        idx = combined_level_indices(s, t)
+        assert len(idx) == max(s, t) and idx[-1] == (s - 1, t - 1)
+        assert all(b[0] - a[0] in (0, 1) and b[1] - a[1] in (0, 1) for a, b in zip(idx, idx[1:]))

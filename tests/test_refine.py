@@ -95,3 +95,34 @@ def test_target_multilevel_solve_matches_direct_solve():
     levels2 = run_target_multilevel(s, h, prm, use_softmax=False)
     assert levels2[-1]["converged"]
     s.close()
+
+
+def test_combined_multilevel_matches_direct_solve():
+    """Source levels (8^2, 16^2 cells) and target levels advanced together
+    (SemiDiscreteOT::run_combined_multilevel): every level converges and the
+    finest one reaches the direct solve's potential up to the shift."""
+    from semidiscreteot_b200.multilevel import build_hierarchy, run_combined_multilevel
+    rng = np.random.default_rng(6)
+    dens = lambda p: 0.5 + np.exp(-np.sum((p - 0.5) ** 2, axis=1) / 0.1)   # noqa: E731
+    sources = [structured_source(2, n, 3, nodal_density=dens) for n in (8, 16)]
+    y = rng.random((900, 2))
+    nu = rng.dirichlet(np.ones(900) * 4)
+    h = build_hierarchy(y, nu, min_points=60, max_points=300, seed=2)
+    nl = len(h["points"])
+    assert nl >= 3
+    prm = SolverParameters(epsilon=1e-2, tau=0.0, use_log_sum_exp_trick=True, tolerance=1e-9,
+                           solver_control_type="linf", max_iterations=5000)
+    s = SotSolver(dim=2, device=0, precision="fp64")
+    s.configure(prm)
+    levels = run_combined_multilevel(s, sources, h, prm, use_softmax=True)
+    assert len(levels) == nl and levels[-1]["source_level"] == 0 and levels[-1]["target_level"] == 0
+    assert [lv["target_level"] for lv in levels] == list(range(nl - 1, -1, -1))
+    assert all(lv["converged"] for lv in levels)
+    psi_ml = levels[-1]["potentials"]
+    fine = sources[-1]
+    s.setup_source(fine["x"], fine["jxw"], fine["density"], fine["cell_offsets"], fine["cell_centers"])
+    s.setup_target(y, nu)
+    psi_direct = s.solve(np.zeros(len(nu)), prm)
+    d = (psi_ml - psi_ml.mean()) - (psi_direct - psi_direct.mean())
+    assert np.max(np.abs(d)) <= 1e-6
+    s.close()
