@@ -195,11 +195,13 @@ k_finalize_grad(int64_t nt, int nks, const double *__restrict__ gpart, const dou
     }
 }
 
-__global__ void __launch_bounds__(256)
+// one CTA of FIN_SCALAR_THREADS: thread i sums blocks i, i + FIN_SCALAR_THREADS, ... (a fixed tree)
+constexpr int FIN_SCALAR_THREADS = 1024;
+__global__ void __launch_bounds__(FIN_SCALAR_THREADS)
 k_finalize_scalars(int nred, const double *__restrict__ redpart, int64_t nval, const double *__restrict__ valpart,
                    double *__restrict__ scal)
 {
-    __shared__ double sh[11][8];
+    __shared__ double sh[11][FIN_SCALAR_THREADS / 32];
     double v = 0.0, c = 0.0, sk = 0.0, np = 0.0;
     for (int64_t b = threadIdx.x; b < nval; b += blockDim.x) {
         v += valpart[b * 4 + 0];
@@ -382,7 +384,7 @@ static sdot_status run_eval(sdot_ctx *c, const EvalArgs &a, bool dense, const do
     if (dense) mark(3);
     k_finalize_grad<<<FIN_BLOCKS, FIN_THREADS, 0, st>>>(a.nt, nks, c->gpart.p, c->nu.p, c->psi.p, pdir, tol,
                                                        partial ? 0 : 1, c->grad.p, c->redpart.p);
-    k_finalize_scalars<<<1, 256, 0, st>>>(FIN_BLOCKS, c->redpart.p, nval, c->blkpart.p, c->scal.p);
+    k_finalize_scalars<<<1, FIN_SCALAR_THREADS, 0, st>>>(FIN_BLOCKS, c->redpart.p, nval, c->blkpart.p, c->scal.p);
     mark(4);
     c->klaunch[1] += 1;
     if (dense) {
@@ -576,7 +578,7 @@ static void noalloc_launch(sdot_ctx *c, const EvalArgs &a, double *S, const Noal
         k_grad_dense<DIM, true><<<g, DENSE_B_THREADS, 0, st>>>(c->x.p, c->w.p, Lq, tpack, psi, a, qslice, gpart);
     k_finalize_grad<<<FIN_BLOCKS, FIN_THREADS, 0, st>>>(a.nt, L.nks, gpart, c->nu.p, psi, nullptr,
                                                        c->prm.tolerance, 1, grad, redpart);
-    k_finalize_scalars<<<1, 256, 0, st>>>(FIN_BLOCKS, redpart, L.nval, blkpart, scal);
+    k_finalize_scalars<<<1, FIN_SCALAR_THREADS, 0, st>>>(FIN_BLOCKS, redpart, L.nval, blkpart, scal);
 }
 
 }  // namespace sdot
