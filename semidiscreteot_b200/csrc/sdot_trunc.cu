@@ -748,7 +748,6 @@ __device__ __forceinline__ void value_pairs_tensor(const SM &sm, int wp, int lan
         const double g2 = DIM == 3 ? sm.stg[2][ti] - cc[2] : 0.0;
         const double d2 = DIM == 3 ? g0 * g0 + g1 * g1 + g2 * g2 : g0 * g0 + g1 * g1;
         const double B0 = fma(-a.halfs, d2, sm.stg[5][ti]) - Munit;
-        const double P = sm.stg[3][ti] * exp2_16(B0, sm.tab);
         const double G[3] = {a.s * g0, a.s * g1, a.s * g2};
         if (B0 >= thr) {
 #pragma unroll
@@ -760,13 +759,31 @@ __device__ __forceinline__ void value_pairs_tensor(const SM &sm, int wp, int lan
                 mx[q] = fmax(mx[q], bb);
             }
         }
+        // per-dimension factors 2^(G_d delta_d): with tshift, relative to the lowest
+        // point (1, r, r^2 with the shift folded into P); otherwise 2^(-G a), (1), 2^(G a)
         double F[3][TM];
+        double P;
+        if (a.tshift) {
+            double sga = 0.0;
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) {
-            const double xp = exp2_16(G[d] * ah[d], sm.tab);
-            F[d][0] = __drcp_rn(xp);
-            F[d][TM - 1] = xp;
-            if (TM == 3) F[d][1] = 1.0;
+            for (int d = 0; d < DIM; ++d) {
+                const double ga = G[d] * ah[d];
+                sga += ga;
+                const double r = exp2_16(TM == 2 ? 2.0 * ga : ga, sm.tab);
+                F[d][0] = 1.0;
+                F[d][1] = r;
+                if (TM == 3) F[d][2] = r * r;
+            }
+            P = sm.stg[3][ti] * exp2_16(B0 - sga, sm.tab);
+        } else {
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                const double xp = exp2_16(G[d] * ah[d], sm.tab);
+                F[d][0] = __drcp_rn(xp);
+                F[d][TM - 1] = xp;
+                if (TM == 3) F[d][1] = 1.0;
+            }
+            P = sm.stg[3][ti] * exp2_16(B0, sm.tab);
         }
 #pragma unroll
         for (int i0 = 0; i0 < TM; ++i0) {
@@ -817,15 +834,27 @@ __device__ __forceinline__ void grad_pairs_tensor(SM &sm, int wp, int lane, int 
         const double g0 = sm.stg[0][ti] - cc[0], g1 = sm.stg[1][ti] - cc[1];
         const double g2 = DIM == 3 ? sm.stg[2][ti] - cc[2] : 0.0;
         const double d2 = DIM == 3 ? g0 * g0 + g1 * g1 + g2 * g2 : g0 * g0 + g1 * g1;
-        const float e0 = (float)(sm.stg[4][ti] + (fma(-a.halfs, d2, sm.stg[5][ti]) - KAPPA * Lref) * (1.0 / 16.0));
+        float e0 = (float)(sm.stg[4][ti] + (fma(-a.halfs, d2, sm.stg[5][ti]) - KAPPA * Lref) * (1.0 / 16.0));
         const float gd[3] = {(float)g0, (float)g1, (float)g2};
         float F[3][TM];
+        if (a.tshift) {
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) {
-            const float xp = ex2_approx(sf * gd[d] * ah[d]);
-            F[d][0] = rcp_approx(xp);
-            F[d][TM - 1] = xp;
-            if (TM == 3) F[d][1] = 1.f;
+            for (int d = 0; d < DIM; ++d) {
+                const float ga = sf * gd[d] * ah[d];
+                e0 -= ga;
+                const float r = ex2_approx(TM == 2 ? 2.f * ga : ga);
+                F[d][0] = 1.f;
+                F[d][1] = r;
+                if (TM == 3) F[d][2] = r * r;
+            }
+        } else {
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                const float xp = ex2_approx(sf * gd[d] * ah[d]);
+                F[d][0] = rcp_approx(xp);
+                F[d][TM - 1] = xp;
+                if (TM == 3) F[d][1] = 1.f;
+            }
         }
         float w = 0.f;
         if (DIM == 2) {
@@ -1166,18 +1195,20 @@ static void dispatch_fused(sdot_ctx *c, const FusedArgs &f, const EvalArgs &a, b
         return;
     }
     if (tensor) {
+        EvalArgs at = a;
+        at.tshift = fac <= 4.0 ? 1 : 0;   // factors <= 2^8 per dimension: relative form, no reciprocals
         if constexpr (DIM == 3) {
             if (c->tensor_m == 2 && a.ql == 8) {
-                dispatch_fused_b<3, 8, 0, 2>(c, f, a, fp32b, nb);
+                dispatch_fused_b<3, 8, 0, 2>(c, f, at, fp32b, nb);
                 return;
             }
         } else {
             if (c->tensor_m == 3 && a.ql == 9) {
-                dispatch_fused_b<2, 9, 0, 3>(c, f, a, fp32b, nb);
+                dispatch_fused_b<2, 9, 0, 3>(c, f, at, fp32b, nb);
                 return;
             }
             if (c->tensor_m == 2 && a.ql == 4) {
-                dispatch_fused_b<2, 4, 0, 2>(c, f, a, fp32b, nb);
+                dispatch_fused_b<2, 4, 0, 2>(c, f, at, fp32b, nb);
                 return;
             }
         }
