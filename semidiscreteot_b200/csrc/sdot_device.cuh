@@ -131,8 +131,6 @@ struct EvalArgs {
     double cull;      // block cull radius r (slightly enlarged)
     double c32;       // log2(e) / (2 eps) (FP32 gradient sweep)
     double l2e_eps;   // log2(e) / eps
-    int tshift;       // tensor-product sweeps: per-dimension factors taken relative to the lowest point
-                      // (set when they stay within 2^8, so that no reciprocal is needed)
 };
 
 // ---------------------------------------------------------------------------

@@ -732,7 +732,7 @@ __device__ __forceinline__ constexpr int tstride()
 // candidates that can attain it: b_qj lies within s r |delta|max of B0_Kj, so
 // a candidate with B0 below (running max B0) - 2 s r |delta|max is never a
 // maximum; thr is that bound relative to Munit.
-template <int DIM, int TM, class SM>
+template <int DIM, int TM, bool TS, class SM>
 __device__ __forceinline__ void value_pairs_tensor(const SM &sm, int wp, int lane, int ncand, int qoff,
                                                    const double *cc, const EvalArgs &a, double Munit, double thr,
                                                    double *S, double *mx)
@@ -759,11 +759,11 @@ __device__ __forceinline__ void value_pairs_tensor(const SM &sm, int wp, int lan
                 mx[q] = fmax(mx[q], bb);
             }
         }
-        // per-dimension factors 2^(G_d delta_d): with tshift, relative to the lowest
+        // per-dimension factors 2^(G_d delta_d): with TS, relative to the lowest
         // point (1, r, r^2 with the shift folded into P); otherwise 2^(-G a), (1), 2^(G a)
         double F[3][TM];
         double P;
-        if (a.tshift) {
+        if constexpr (TS) {
             double sga = 0.0;
 #pragma unroll
             for (int d = 0; d < DIM; ++d) {
@@ -816,7 +816,7 @@ __device__ __forceinline__ float rcp_approx(float x)
 // FP32 gradient sweep on tensor-product points: per candidate
 // 2^(e0) sum_q W_q prod_d F_d[i_d], W_q = w_q 2^(D_q), summed dimension by
 // dimension (Horner order), into the warp's partial row.
-template <int DIM, int TM, class SM>
+template <int DIM, int TM, bool TS, class SM>
 __device__ __forceinline__ void grad_pairs_tensor(SM &sm, int wp, int lane, int ncand, int qoff,
                                                   const double *cc, double Lref, const EvalArgs &a)
 {
@@ -837,7 +837,7 @@ __device__ __forceinline__ void grad_pairs_tensor(SM &sm, int wp, int lane, int 
         float e0 = (float)(sm.stg[4][ti] + (fma(-a.halfs, d2, sm.stg[5][ti]) - KAPPA * Lref) * (1.0 / 16.0));
         const float gd[3] = {(float)g0, (float)g1, (float)g2};
         float F[3][TM];
-        if (a.tshift) {
+        if constexpr (TS) {
 #pragma unroll
             for (int d = 0; d < DIM; ++d) {
                 const float ga = sf * gd[d] * ah[d];
@@ -902,7 +902,7 @@ __device__ __forceinline__ void write_partials(SM &sm, const FusedArgs &f, int n
     }
 }
 
-template <int DIM, int QL, bool FP32B, int MODE, int TQ>
+template <int DIM, int QL, bool FP32B, int MODE, int TQ, bool TS>
 __global__ void __launch_bounds__(FT_WARPS * 32, fused_min_blocks(DIM, TQ, FP32B))
 k_fused(FusedArgs f, EvalArgs a)
 {
@@ -999,7 +999,7 @@ k_fused(FusedArgs f, EvalArgs a)
                 }
                 if (bmax > bmax_run) bmax_run = bmax;
                 if constexpr (TQ > 0)
-                    value_pairs_tensor<DIM, TQ>(sm, wp, lane, ncand, qoff, cc, a, Munit,
+                    value_pairs_tensor<DIM, TQ, TS>(sm, wp, lane, ncand, qoff, cc, a, Munit,
                                                 bmax_run - 2.0 * sr * dqmax - Munit, S, mx);
                 else if (nql == QL)
                     value_pairs<DIM, QL, QL, MODE>(sm, wp, lane, ncand, qoff, cc[0], cc[1], cc[2], a, Munit, M, S, mx);
@@ -1085,7 +1085,7 @@ k_fused(FusedArgs f, EvalArgs a)
             for (int t = lane; t < nstg; t += 32) partial_rows<FP32B>(sm)[wp * SMem::MAXS + t] = 0;
             __syncwarp();
             if (isfinite(Lref)) {
-                if constexpr (TQ > 0 && FP32B) grad_pairs_tensor<DIM, TQ>(sm, wp, lane, ncand_single, qoff, cc, Lref, a);
+                if constexpr (TQ > 0 && FP32B) grad_pairs_tensor<DIM, TQ, TS>(sm, wp, lane, ncand_single, qoff, cc, Lref, a);
                 else grad_pairs<DIM, FP32B>(sm, f, wp, lane, ncand_single, qoff, nql, cc, Lref, qblk0, a);
             }
         }
@@ -1109,7 +1109,7 @@ k_fused(FusedArgs f, EvalArgs a)
             for (int t = lane; t < nstg; t += 32) partial_rows<FP32B>(sm)[wp * SMem::MAXS + t] = 0;
             __syncwarp();
             if (isfinite(Lref)) {
-                if constexpr (TQ > 0 && FP32B) grad_pairs_tensor<DIM, TQ>(sm, wp, lane, ncand, qoff, cc, Lref, a);
+                if constexpr (TQ > 0 && FP32B) grad_pairs_tensor<DIM, TQ, TS>(sm, wp, lane, ncand, qoff, cc, Lref, a);
                 else grad_pairs<DIM, FP32B>(sm, f, wp, lane, ncand, qoff, nql, cc, Lref, qblk0, a);
             }
         }
@@ -1144,21 +1144,21 @@ k_grad_reduce(const int64_t *__restrict__ tblk_off, const int64_t *__restrict__ 
     }
 }
 
-template <int DIM, int QL, bool FP32B, int MODE, int TQ>
+template <int DIM, int QL, bool FP32B, int MODE, int TQ, bool TS>
 static void launch_fused(sdot_ctx *c, const FusedArgs &f, const EvalArgs &a, size_t smem, int nb)
 {
-    cudaFuncSetAttribute(k_fused<DIM, QL, FP32B, MODE, TQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(k_fused<DIM, QL, FP32B, MODE, TQ>, cudaFuncAttributePreferredSharedMemoryCarveout,
+    cudaFuncSetAttribute(k_fused<DIM, QL, FP32B, MODE, TQ, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_fused<DIM, QL, FP32B, MODE, TQ, TS>, cudaFuncAttributePreferredSharedMemoryCarveout,
                          (int)cudaSharedmemCarveoutMaxShared);
-    k_fused<DIM, QL, FP32B, MODE, TQ><<<(unsigned)nb, FT_WARPS * 32, smem, c->stream>>>(f, a);
+    k_fused<DIM, QL, FP32B, MODE, TQ, TS><<<(unsigned)nb, FT_WARPS * 32, smem, c->stream>>>(f, a);
 }
 
-template <int DIM, int QL, int MODE, int TQ = 0>
+template <int DIM, int QL, int MODE, int TQ = 0, bool TS = false>
 static void dispatch_fused_b(sdot_ctx *c, const FusedArgs &f, const EvalArgs &a, bool fp32b, int nb)
 {
-    if (fp32b) launch_fused<DIM, QL, true, MODE, TQ>(c, f, a, sizeof(FTSmem<fused_cap(DIM, TQ, true)>), nb);
+    if (fp32b) launch_fused<DIM, QL, true, MODE, TQ, TS>(c, f, a, sizeof(FTSmem<fused_cap(DIM, TQ, true)>), nb);
     else
-        launch_fused<DIM, QL, false, MODE, TQ>(c, f, a, sizeof(FTSmem<fused_cap(DIM, TQ, false)>) + ft_rows64_bytes(fused_cap(DIM, TQ, false)),
+        launch_fused<DIM, QL, false, MODE, TQ, TS>(c, f, a, sizeof(FTSmem<fused_cap(DIM, TQ, false)>) + ft_rows64_bytes(fused_cap(DIM, TQ, false)),
                                                nb);
 }
 
@@ -1195,20 +1195,23 @@ static void dispatch_fused(sdot_ctx *c, const FusedArgs &f, const EvalArgs &a, b
         return;
     }
     if (tensor) {
-        EvalArgs at = a;
-        at.tshift = fac <= 4.0 ? 1 : 0;   // factors <= 2^8 per dimension: relative form, no reciprocals
+        // factors <= 2^8 per dimension: the relative form (no reciprocals, the lowest point's factor 1)
+        const bool ts = fac <= 4.0;
         if constexpr (DIM == 3) {
             if (c->tensor_m == 2 && a.ql == 8) {
-                dispatch_fused_b<3, 8, 0, 2>(c, f, at, fp32b, nb);
+                if (ts) dispatch_fused_b<3, 8, 0, 2, true>(c, f, a, fp32b, nb);
+                else dispatch_fused_b<3, 8, 0, 2, false>(c, f, a, fp32b, nb);
                 return;
             }
         } else {
             if (c->tensor_m == 3 && a.ql == 9) {
-                dispatch_fused_b<2, 9, 0, 3>(c, f, at, fp32b, nb);
+                if (ts) dispatch_fused_b<2, 9, 0, 3, true>(c, f, a, fp32b, nb);
+                else dispatch_fused_b<2, 9, 0, 3, false>(c, f, a, fp32b, nb);
                 return;
             }
             if (c->tensor_m == 2 && a.ql == 4) {
-                dispatch_fused_b<2, 4, 0, 2>(c, f, at, fp32b, nb);
+                if (ts) dispatch_fused_b<2, 4, 0, 2, true>(c, f, a, fp32b, nb);
+                else dispatch_fused_b<2, 4, 0, 2, false>(c, f, a, fp32b, nb);
                 return;
             }
         }
