@@ -11,7 +11,7 @@
 //    and, for every stage of 64 quadrature points, regenerates the 128 rows
 //    w_q pi_qa and the 256 rows pi_qb straight into 128B-swizzled K-major
 //    shared memory, where one elected thread hands them to tcgen05.mma.
-//  * BF16 hi+lo split: v = hi + lo with hi = bf16_rn(v), lo = bf16_rz(v - hi);
+//  * BF16 hi+lo split: v = hi + lo with hi = bf16_rn(v) (nearest even), lo = bf16_rz(v - hi);
 //    S ~ Ahi.Bhi + Ahi.Blo + Alo.Bhi (the lo.lo term, ~2^-18 relative, dropped).
 //  * Exponents in FP32 with FP64-formed offsets: log2(w_q pi_qj) =
 //    E_bj + G_bj . d_q + F_q, where b is the 64-point block of q, c_b its
@@ -152,6 +152,13 @@ __device__ __forceinline__ f2 pack2(float a, float b)
     f2 r;
     asm("mov.b64 %0, {%1,%2};" : "=l"(r) : "f"(a), "f"(b));
     return r;
+}
+// v0, v1 rounded to BF16 (round to nearest even), packed with v0 in the low half.
+__device__ __forceinline__ uint32_t bf16x2_rn(float v0, float v1)
+{
+    uint32_t d;
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(v1), "f"(v0));
+    return d;
 }
 __device__ __forceinline__ void unpack2(f2 v, float &a, float &b) { asm("mov.b64 {%0,%1}, %2;" : "=f"(a), "=f"(b) : "l"(v)); }
 __device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c)
@@ -331,15 +338,13 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
                 float u0, u1;
                 unpack2(u, u0, u1);
                 const float v0 = ex2_approx(u0), v1 = ex2_approx(u1);
-                // hi: round to 8 significant bits in the integer domain (an
-                // arithmetic split such as Veltkamp's c - (c - v) may be folded
-                // to v by the compiler); lo = v - hi is exact
-                const uint32_t hb0 = (__float_as_uint(v0) + 0x8000u) & 0xffff0000u;
-                const uint32_t hb1 = (__float_as_uint(v1) + 0x8000u) & 0xffff0000u;
-                const f2 lo = sub2(pack2(v0, v1), pack2(__uint_as_float(hb0), __uint_as_float(hb1)));
+                // hi: both values rounded to BF16 (nearest even) and packed by one
+                // cvt; widened back (shift / mask), lo = v - hi is exact
+                const uint32_t hp = bf16x2_rn(v0, v1);
+                const f2 lo = sub2(pack2(v0, v1), pack2(__uint_as_float(hp << 16), __uint_as_float(hp & 0xffff0000u)));
                 float l0, l1;
                 unpack2(lo, l0, l1);
-                hw[k] = __byte_perm(hb0, hb1, 0x7632);
+                hw[k] = hp;
                 lw[k] = __byte_perm(__float_as_uint(l0), __float_as_uint(l1), 0x7632);
             }
             const int rr = isA ? r : r - M;
