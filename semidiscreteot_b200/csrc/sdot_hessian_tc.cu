@@ -321,13 +321,20 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
             }
         }
         uint8_t *stage = sm + buf * STAGE_BYTES;
+        // each row's E/G are loaded one row ahead, before the previous row's
+        // stores, so that the rows' chains can overlap
+        const float4 *eg0 = reinterpret_cast<const float4 *>(Eg + (buf * ROWS + rg) * 8);
+        float4 e0 = eg0[0], e1 = eg0[1];
 #pragma unroll
         for (int it = 0; it < RPT; ++it) {
             const bool isA = it < ARPT;
             const int r = rg + RG * it;
-            const float4 *eg = reinterpret_cast<const float4 *>(Eg + (buf * ROWS + r) * 8);
-            const float4 e0 = eg[0], e1 = eg[1];
             const f2 E = pack2(e0.x, e0.y), Gx = pack2(e0.z, e0.w), Gy = pack2(e1.x, e1.y), Gz = pack2(e1.z, e1.w);
+            if (it + 1 < RPT) {
+                const float4 *egn = reinterpret_cast<const float4 *>(Eg + (buf * ROWS + r + RG) * 8);
+                e0 = egn[0];
+                e1 = egn[1];
+            }
             uint32_t hw[4], lw[4];
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
