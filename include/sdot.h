@@ -179,7 +179,7 @@ typedef struct {
 sdot_status sdot_hessian_device(sdot_ctx *ctx, const double *psi_dev, void *H_dev, int method, int out_f32,
                                 sdot_hessian_info *info);
 /* Tuning of the tensor method: stages of 64 points accumulated in FP32 before
- * each FP64 drain (default 16). */
+ * each FP64 drain (default 64). */
 sdot_status sdot_set_hessian_chunk(sdot_ctx *ctx, int stages);
 
 /* The tensor-core Hessian in pieces, for sharding it over GPUs by output tiles
