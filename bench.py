@@ -505,6 +505,7 @@ def _solve_requests_through_server(problems, slots, rate, seed, warmup=()):
     srv = SolveServer(n_slots=slots)
     for t in [_submit(srv, p) for p in warmup]:
         srv.wait(t, raise_on_error=False)
+    srv.reset_stats()   # latencies and peak concurrency of the timed requests only
     tickets = []
     t0 = time.perf_counter()
     next_t = t0
@@ -518,9 +519,6 @@ def _solve_requests_through_server(problems, slots, rate, seed, warmup=()):
     wall = time.perf_counter() - t0
     st = srv.stats()
     srv.close()
-    lat = np.array([r["latency_ms"] for r in res]) if res else np.zeros(1)
-    st = {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-          "mean_ms": float(lat.mean()), "peak_running": st["peak_running"]}
     return res, wall, st
 
 

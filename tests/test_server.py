@@ -89,6 +89,8 @@ def test_points_only_requests_and_warm_start():
         t1 = srv.submit(src, y, nu, prm, method="newton", with_cells=False)
         p1, r1 = srv.wait(t1)
         assert r1["converged"]
+        srv.reset_stats()                          # statistics from here on
+        assert srv.stats()["completed"] == 0
         t2 = srv.submit(src, y, nu, prm, method="newton", psi0=p1)
         p2, r2 = srv.wait(t2)
         assert r2["converged"] and r2["iterations"] <= 1
@@ -96,5 +98,8 @@ def test_points_only_requests_and_warm_start():
                         intermediate_tolerance=1e-6)
         p3, r3 = srv.wait(t3)
         assert r3["converged"]
+        st = srv.stats()
+        assert st["completed"] == 2 and st["failed"] == 0, st
+        assert st["p99_ms"] >= st["p50_ms"] > 0
     for p in (p1, p2, p3):
         assert check_fp64(src, y, nu, prm, p) <= 1e-9
