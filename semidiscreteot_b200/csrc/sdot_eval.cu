@@ -62,7 +62,22 @@ __global__ void k_minmax(const double *v, int64_t n, double *out)
     __shared__ int sbad[32];
     double mx = -DBL_MAX, mn = DBL_MAX;
     int bad = 0;
-    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+    // four independent loads in flight per thread (max, min and the flag do not depend on the order)
+    const int64_t step = blockDim.x;
+    int64_t i = threadIdx.x;
+    for (; i + 3 * step < n; i += 4 * step) {
+        const double a0 = v[i], a1 = v[i + step], a2 = v[i + 2 * step], a3 = v[i + 3 * step];
+        if (!isfinite(a0) || !isfinite(a1) || !isfinite(a2) || !isfinite(a3)) bad = 1;
+        mx = a0 > mx ? a0 : mx;
+        mn = a0 < mn ? a0 : mn;
+        mx = a1 > mx ? a1 : mx;
+        mn = a1 < mn ? a1 : mn;
+        mx = a2 > mx ? a2 : mx;
+        mn = a2 < mn ? a2 : mn;
+        mx = a3 > mx ? a3 : mx;
+        mn = a3 < mn ? a3 : mn;
+    }
+    for (; i < n; i += step) {
         const double a = v[i];
         if (!isfinite(a)) bad = 1;
         mx = a > mx ? a : mx;
