@@ -1,6 +1,6 @@
 """GPU parity: the CUDA path (through the C ABI) against the FP64 CPU oracle.
 
-Tolerances (the north-star bar): dual value 1e-10 relative (|J| floored at
+Tolerances: dual value 1e-10 relative (|J| floored at
 1e-6), gradient 1e-8 absolute (1e-12 in FP64 mode, whose exponentials carry
 1.5e-13 relative error).  The HYBRID/MIXED gradient sweep runs its
 exponentials in FP32: its bound is max(1e-8, 5e-6 * max nu_j) and the tests
