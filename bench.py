@@ -21,6 +21,16 @@ N > 1 : one process per GPU (torchrun); source cells sharded, one NCCL
 --impl reference: the FP64 CPU restatement of the reference's evaluation
         (oracle/, all host threads, WorkStream-like per-cell O(N) overheads)
         on a bounded sample of the same workload's cells, rank 0 only.
+
+With the default workload the line also carries (unless --no-extra):
+  precision_fp64 : the same evaluation with FP64 exponentials in both sweeps;
+  config1        : the dense 2D configuration (64 x 64 cells x 3 x 3 Gauss
+                   points = 36,864 points, 1,000 uniform targets, eps = 1e-2,
+                   no truncation) with its own value, e2e, roofline, the
+                   reference-faithful CPU evaluation over every cell, and the
+                   full L-BFGS solve to |g|_inf <= 1e-8 on the GPU and on the
+                   CPU (time, iterations).
+Clocks are sampled through NVML every 2 ms during every timed region.
 """
 from __future__ import annotations
 
@@ -63,6 +73,8 @@ def parse():
     ap.add_argument("--precision", default="hybrid", choices=["hybrid", "fp64", "mixed"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="trunc_3d: skip the other-precision figure and the dense 2D (config1) sub-object")
     ap.add_argument("--scale", type=float, default=None,
                     help="shrink the workload (default 1; serve_3d: 0.5, the request sizes it is documented at)")
     args = ap.parse_args()
@@ -138,78 +150,187 @@ def cpu_sample(wl, seconds: float, threads: int = 0):
 
 
 # ---------------------------------------------------------------------------
-# clocks during the timed region
+# clocks during the timed regions
 # ---------------------------------------------------------------------------
 
 class ClockSampler:
+    """SM clock, its maximum and the clock-event reasons, sampled every 2 ms
+    through NVML while a timed region is open (``with clk.region(): ...``);
+    nvidia-smi at 100 ms when NVML is unavailable.  Read-only: no setting of
+    the GPU is changed."""
+
+    PERIOD_S = 0.002
+
     def __init__(self, index: int):
         self.index = index
-        self.lines = []
-        self.proc = None
+        self.samples = []          # (sm_mhz, max_mhz, reasons set)
+        self._active = threading.Event()
+        self._stop = threading.Event()
+        self._th = None
+        self._smi = None
+        self._smi_lines = []
+        self._nvml = None
+
+    def _handle(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            try:
+                import torch
+                uuid = str(torch.cuda.get_device_properties(self.index).uuid)
+                h = pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+            except Exception:
+                h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            return pynvml, h
+        except Exception:
+            return None
 
     def __enter__(self):
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
-        try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.th = threading.Thread(target=self._read, daemon=True)
-            self.th.start()
-        except (OSError, ValueError):
-            self.proc = None
+        self._nvml = self._handle()
+        if self._nvml is not None:
+            self._th = threading.Thread(target=self._run_nvml, daemon=True)
+            self._th.start()
+        else:
+            q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+            try:
+                self._smi = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                              "--format=csv,noheader,nounits", "-lms", "100"],
+                                             stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                self._th = threading.Thread(target=self._run_smi, daemon=True)
+                self._th.start()
+            except (OSError, ValueError):
+                self._smi = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _run_nvml(self):
+        nv, h = self._nvml
+        bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        while not self._stop.is_set():
+            if self._active.is_set():
+                try:
+                    sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                    mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+                    r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.samples.append((float(sm), float(mx), {k for k, b in bits.items() if r & b}))
+                except Exception:
+                    pass
+                time.sleep(self.PERIOD_S)
+            else:
+                self._active.wait(0.05)
 
-    def __exit__(self, *exc):
-        if self.proc is not None:
-            time.sleep(0.25)
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
-
-    def summary(self):
-        sm, mx, reasons = [], 0.0, set()
+    def _run_smi(self):
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ln in self._smi.stdout:
+            if not self._active.is_set():
+                continue
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
             try:
-                sm.append(float(f[1]))
-                mx = max(mx, float(f[2]))
+                self.samples.append((float(f[1]), float(f[2]),
+                                     {k for k, v in zip(names, f[5:9]) if v.lower().startswith("active")}))
             except ValueError:
                 continue
-            for k, v in zip(names, f[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(k)
-        if not sm:
+
+    class _Region:
+        def __init__(self, owner):
+            self.owner = owner
+
+        def __enter__(self):
+            self.owner._active.set()
+
+        def __exit__(self, *exc):
+            self.owner._active.clear()
+
+    def region(self):
+        return ClockSampler._Region(self)
+
+    def __exit__(self, *exc):
+        self._active.clear()
+        self._stop.set()
+        if self._smi is not None:
+            self._smi.terminate()
+            try:
+                self._smi.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self._smi.kill()
+        if self._th is not None:
+            self._th.join(timeout=5)
+
+    def summary(self):
+        if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        sm = [s[0] for s in self.samples]
+        reasons = set().union(*[s[2] for s in self.samples])
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(s[1] for s in self.samples),
+                "reasons": sorted(reasons), "samples": len(sm),
+                "source": "NVML every 2 ms" if self._nvml is not None else "nvidia-smi every 100 ms"}
 
 
-def read_traffic(kernel: str, workload: str):
-    """DRAM bytes per launch of a kernel from the committed ncu summary
-    profiles/<kernel>_<workload>.md (line 'traffic_bytes_per_launch: X')."""
-    path = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.md")
-    try:
-        for line in open(path):
-            if line.startswith("traffic_bytes_per_launch:"):
-                return float(line.split(":", 1)[1].split()[0])
-    except OSError:
-        pass
-    return None
+# DRAM traffic per launch of the dominant kernels (dram__bytes_read.sum +
+# dram__bytes_write.sum), from one ncu capture each:
+#   k_fused, trunc_3d (2,097,152 points x 100,000 targets):
+#     ncu --clock-control none --metrics dram__bytes_read.sum,dram__bytes_write.sum
+#         -k regex:k_fused -s 3 -c 1 python bench.py --steps 1 --warmup 3 --no-cpu-baseline --no-extra
+#   k_value_dense / k_grad_dense, dense_2d: the inputs (0.9 MB) stay in L2, so
+#     DRAM traffic is not a meaningful bound there (null).
+TRAFFIC_BYTES = {
+    ("trunc_3d", "hybrid"): 487960576.0,
+}
 
 
 # ---------------------------------------------------------------------------
 # arms
 # ---------------------------------------------------------------------------
+
+def cpu_full(wl, seconds: float, threads: int = 0):
+    """The reference-faithful evaluation over every cell of a (small) workload,
+    repeated for about `seconds`; returns (pairs/s, cores, description)."""
+    from oracle import oracle as orc
+    src = wl["source"]
+    prm = wl["params"]
+    op = orc.Params(epsilon=prm.epsilon, tau=prm.tau, use_log_sum_exp=prm.use_log_sum_exp_trick)
+    P = orc.Problem(src["x"], src["jxw"], src["density"], src["cell_offsets"], src["cell_centers"], wl["y"], wl["nu"])
+    psi = np.zeros(wl["y"].shape[0])
+    nthr = threads if threads > 0 else (os.cpu_count() or 1)
+    r = P.distance_threshold(psi, op)
+    ncell = P.ctr.shape[0]
+    reps, pairs, t_all = 0, 0, 0.0
+    while t_all < seconds or reps < 2:
+        t0 = time.perf_counter()
+        _, _, _, pp = P.evaluate_cells(psi, op, r, 0, ncell, faithful=True, threads=nthr)
+        t_all += time.perf_counter() - t0
+        pairs += pp
+        reps += 1
+    desc = (f"all {ncell} cells x {reps} evaluations, full target set, psi=0; {pairs} pairs in {t_all:.2f}s; "
+            f"reference-faithful FP64 (per-cell O(N) CopyData zeroing + serialised in-order merge), "
+            f"OpenMP {nthr} threads")
+    return pairs / t_all, nthr, desc
+
+
+def cpu_solve(wl, threads: int = 0):
+    """The oracle's reference-faithful L-BFGS solve (SotSolver::solve with
+    deal.II SolverBFGS) from psi = 0 to the workload's tolerance."""
+    from oracle import oracle as orc
+    src = wl["source"]
+    prm = wl["params"]
+    op = orc.Params(epsilon=prm.epsilon, tau=prm.tau, use_log_sum_exp=prm.use_log_sum_exp_trick,
+                    tolerance=prm.tolerance, solver_control_type=prm.solver_control_type,
+                    max_iterations=prm.max_iterations)
+    P = orc.Problem(src["x"], src["jxw"], src["density"], src["cell_offsets"], src["cell_centers"], wl["y"], wl["nu"])
+    nthr = threads if threads > 0 else (os.cpu_count() or 1)
+    t0 = time.perf_counter()
+    psi, info = P.solve(np.zeros(wl["y"].shape[0]), op, threads=nthr, faithful=True)
+    dt = time.perf_counter() - t0
+    return {"seconds": dt, "iterations": info["iterations"], "evaluations": info["n_evaluations"],
+            "converged": info["converged"], "final_grad_linf": info["last_check_value"], "cores": nthr,
+            "kind": "port", "method": "reference-faithful FP64 L-BFGS (deal.II SolverBFGS rules), psi0 = 0"}
+
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
@@ -235,8 +356,154 @@ def run_reference(args):
             "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": cores, "kind": "port",
                              "sample": descs[-1]},
             "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if args.workload == "trunc_3d" and not args.no_extra:
+        c1 = make_workload("dense_2d", 1.0)
+        v1, cores1, desc1 = cpu_full(c1, max(2.0, args.cpu_seconds / 4))
+        line["config1"] = {"workload": "dense_2d", "value": v1, "unit": "pairs/s", "cores": cores1, "kind": "port",
+                           "sample": desc1, "solve": cpu_solve(c1)}
     print(json.dumps(line))
     return 0
+
+
+def _make_single(wl, precision, local):
+    from semidiscreteot_b200 import SotSolver
+    s = SotSolver(dim=wl["dim"], device=local, precision=precision)
+    s.setup_source_measure(wl["source"])
+    s.setup_target(wl["y"], wl["nu"])
+    s.configure(wl["params"])
+    return s
+
+
+def measure_single(wl, precision, steps, warmup, local, clk, flush, e2e=True):
+    """Device-timed evaluations of one workload on one GPU (inputs resident,
+    L2 flushed before each step, CUDA events on the library's stream), then
+    the same through the host API with pinned host buffers (e2e)."""
+    import torch
+    dev = torch.device("cuda", local)
+    solver = _make_single(wl, precision, local)
+    stream = torch.cuda.ExternalStream(solver.stream_handle, device=dev)
+    N = wl["y"].shape[0]
+    psi = torch.zeros(N, dtype=torch.float64, device=dev)
+    grad = torch.empty(N, dtype=torch.float64, device=dev)
+    for _ in range(max(3, warmup)):
+        solver.evaluate_functional_device(psi.data_ptr(), grad.data_ptr())
+    torch.cuda.synchronize()
+    solver.set_profiling(True)
+    solver.kernel_times(reset=True)
+    times = []
+    torch.cuda.synchronize()
+    with clk.region():
+        for _ in range(steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            solver.evaluate_functional_device(psi.data_ptr(), grad.data_ptr())
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        torch.cuda.synchronize()
+    kt = solver.kernel_times(reset=True)
+    solver.set_profiling(False)
+    pairs = solver.last_eval_info["n_pairs"]
+    ms = float(np.mean(times))
+    out = {"value": pairs / (ms * 1e-3), "ms_per_step": ms, "pairs_per_step": pairs, "kt": kt,
+           "gpu_launches": int(sum(v["launches"] for v in kt.values()))}
+    if e2e:
+        hpsi = torch.zeros(N, dtype=torch.float64).pin_memory()
+        hgrad = torch.empty(N, dtype=torch.float64).pin_memory()
+        psi_np, grad_np = hpsi.numpy(), hgrad.numpy()
+        for _ in range(2):
+            solver.evaluate_functional(psi_np, grad_np)
+        et = []
+        with clk.region():
+            for _ in range(steps):
+                with torch.cuda.stream(stream):
+                    flush.fill_(1.0)
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                solver.evaluate_functional(psi_np, grad_np)
+                e1.record(stream)
+                e1.synchronize()
+                et.append(e0.elapsed_time(e1))
+        out["e2e"] = {"value": pairs / (float(np.mean(et)) * 1e-3), "unit": "pairs/s",
+                      "h2d_bytes_per_step": int(N * 8), "d2h_bytes_per_step": int(N * 8 + 8),
+                      "ms_per_step": float(np.mean(et))}
+    solver.close()
+    return out
+
+
+def roofline_of(m, wl, peaks, precision):
+    """Roofline of the dominant kernel from the per-phase CUDA-event times."""
+    kt = m["kt"]
+    dim = wl["dim"]
+    tv = kt["value_sweep"]["ms"] / max(1, kt["value_sweep"]["launches"])
+    tg = kt["gradient_sweep"]["ms"] / max(1, kt["gradient_sweep"]["launches"])
+    pairs = m["pairs_per_step"]
+    truncated = wl["params"].tau > 0
+    if tv >= tg or truncated:
+        ach = VALUE_FLOPS_PER_PAIR[dim] * pairs / (tv * 1e-3) / 1e12
+        kname = ("k_fused (FP64 exp2 value sweep + FP32 ex2 gradient sweep, one kernel)" if truncated else
+                 "k_value_dense (FP64 exp2 value sweep)")
+        return {"kernel": kname, "bound": "fp64", "achieved": ach, "peak": peaks["fp64_tflops"], "unit": "TFLOP/s",
+                "frac": ach / peaks["fp64_tflops"], "traffic": TRAFFIC_BYTES.get((wl["name"], precision)),
+                "flops_per_pair": VALUE_FLOPS_PER_PAIR[dim], "ms_per_launch": tv,
+                "peak_source": "measured on this GPU by sdot_measure_peaks (FP64 FMA chains); "
+                               "MEASURED_PEAKS.json has no FP64 figure"}
+    ach = pairs / (tg * 1e-3) / 1e9
+    return {"kernel": "k_grad_dense (FP32 ex2 gradient sweep)" if precision != "fp64" else
+            "k_grad_dense (FP64 exp2 gradient sweep)", "bound": "mufu", "achieved": ach,
+            "peak": peaks["ex2_gops"], "unit": "Gex2/s", "frac": ach / peaks["ex2_gops"],
+            "traffic": TRAFFIC_BYTES.get((wl["name"], precision)), "ms_per_launch": tg,
+            "peak_source": "measured on this GPU by sdot_measure_peaks (ex2.approx chains)"}
+
+
+def measure_config1(args, local, clk, flush, peaks):
+    """The dense 2D configuration (64 x 64 cells x 3 x 3 Gauss points, 1,000
+    targets, eps = 1e-2, untruncated): evaluation throughput (device and e2e),
+    its roofline, the reference-faithful CPU evaluation over every cell, and
+    the full L-BFGS solve to |g|_inf <= 1e-8 on the GPU and on the CPU."""
+    import torch
+    wl = make_workload("dense_2d", 1.0)
+    steps = max(args.steps, 200)   # 0.3 ms steps: enough of them for a timed region the clocks cover
+    m = measure_single(wl, args.precision, steps, args.warmup, local, clk, flush)
+    out = {"workload": "dense_2d", "n_quadrature": int(wl["source"]["jxw"].size), "n_targets": int(wl["y"].shape[0]),
+           "epsilon": wl["params"].epsilon, "tau": 0.0, "precision": args.precision, "steps": steps,
+           "value": m["value"], "unit": "pairs/s", "ms_per_step": m["ms_per_step"],
+           "pairs_per_step": m["pairs_per_step"], "e2e": m["e2e"], "roofline": roofline_of(m, wl, peaks, args.precision),
+           "kernel_ms_per_step": {k: v["ms"] / steps for k, v in m["kt"].items()},
+           "gpu_launches": m["gpu_launches"]}
+    # full solve on the GPU (FP64 sweeps, L-BFGS like the reference)
+    s = _make_single(wl, "fp64", local)
+    N = wl["y"].shape[0]
+    s.solve(np.zeros(N), wl["params"])   # warm-up (first-use costs)
+    torch.cuda.synchronize()
+    with clk.region():
+        t0 = time.perf_counter()
+        psi = s.solve(np.zeros(N), wl["params"])
+        t_gpu = time.perf_counter() - t0
+    gpu = {"seconds": t_gpu, "iterations": int(s.get_last_iteration_count()),
+           "evaluations": int(s.last_solve_info.get("n_evaluations", 0)), "converged": bool(s.get_convergence_status()),
+           "final_grad_linf": float(s.last_solve_info.get("last_check_value", float("nan"))),
+           "method": "sdot_solve (L-BFGS, FP64 sweeps), psi0 = 0, host wall clock"}
+    s.close()
+    if not args.no_cpu_baseline:
+        from oracle import oracle as orc
+        src = wl["source"]
+        P = orc.Problem(src["x"], src["jxw"], src["density"], src["cell_offsets"], src["cell_centers"],
+                        wl["y"], wl["nu"])
+        op = orc.Params(epsilon=wl["params"].epsilon, tau=0.0, use_log_sum_exp=True)
+        _, go, _ = P.evaluate(psi, op)
+        gpu["oracle_grad_linf_at_gpu_psi"] = float(np.max(np.abs(go)))
+        v, cores, desc = cpu_full(wl, max(2.0, args.cpu_seconds / 4))
+        out["cpu_baseline"] = {"value": v, "unit": "pairs/s", "cores": cores, "kind": "port", "sample": desc}
+        cpu = cpu_solve(wl)
+        out["solve"] = {"gpu": gpu, "cpu": cpu, "speedup": cpu["seconds"] / t_gpu if t_gpu > 0 else None}
+    else:
+        out["solve"] = {"gpu": gpu}
+    return out
 
 
 def run_ours(args):
@@ -252,139 +519,97 @@ def run_ours(args):
         return 2
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     wl = make_workload(args.workload, args.scale)
-    src, y, nu, prm, dim = wl["source"], wl["y"], wl["nu"], wl["params"], wl["dim"]
-    N = y.shape[0]
-    if world > 1:
-        solver = DistributedSotSolver(dim, rank, world, device=local, precision=args.precision)
-        solver.setup_source(src)
-        solver.setup_target(y, nu)
-        solver.configure(prm)
-        lib = solver.local
-    else:
-        solver = SotSolver(dim=dim, device=local, precision=args.precision)
-        solver.setup_source_measure(src)
-        solver.setup_target(y, nu)
-        solver.configure(prm)
-        lib = solver
+    dim = wl["dim"]
+
+    if world == 1:
+        with ClockSampler(local) as clk:
+            m = measure_single(wl, args.precision, args.steps, args.warmup, local, clk, flush)
+            peaks = SotSolver.measure_peaks(local)
+            extra = {}
+            if args.workload == "trunc_3d" and not args.no_extra:
+                other = "fp64" if args.precision != "fp64" else "hybrid"
+                mo = measure_single(wl, other, args.steps, args.warmup, local, clk, flush, e2e=False)
+                extra[f"precision_{other}"] = {"value": mo["value"], "unit": "pairs/s",
+                                               "ms_per_step": mo["ms_per_step"],
+                                               "pairs_per_step": mo["pairs_per_step"],
+                                               "kernel_ms_per_step": {k: v["ms"] / args.steps
+                                                                      for k, v in mo["kt"].items()}}
+                extra["config1"] = measure_config1(args, local, clk, flush, peaks)
+        t_ms = m["ms_per_step"]
+        pairs = m["pairs_per_step"]
+        line = {"metric": "LSE dual-gradient pairs/s", "value": m["value"], "unit": "pairs/s", "n_gpus": 1,
+                "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": t_ms, "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None,
+                "dtype": "f64" if args.precision == "fp64" else "f64 value sweep + f32 exp gradient sweep",
+                "data": "synthetic (seeded; no published dataset)", "config": workload_config(wl, args, 1),
+                "pairs_per_step": pairs, "roofline": roofline_of(m, wl, peaks, args.precision),
+                "kernel_ms_per_step": {k: v["ms"] / args.steps for k, v in m["kt"].items()},
+                "gpu_launches": m["gpu_launches"], "clocks": clk.summary(), "peaks_measured": peaks,
+                "e2e": m["e2e"]}
+        if not args.no_cpu_baseline:
+            v, cores, desc, _ = cpu_sample(wl, args.cpu_seconds)
+            line["cpu_baseline"] = {"value": v, "unit": "pairs/s", "cores": cores, "kind": "port", "sample": desc}
+        line.update(extra)
+        print(json.dumps(line))
+        return 0
+
+    # N > 1: source cells sharded over the ranks, one all-reduce of n_targets + 3 doubles per step
+    import datetime
+    import torch.distributed as dist
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    N = wl["y"].shape[0]
+    solver = DistributedSotSolver(dim, rank, world, device=local, precision=args.precision)
+    solver.setup_source(wl["source"])
+    solver.setup_target(wl["y"], wl["nu"])
+    solver.configure(wl["params"])
+    lib = solver.local
     stream = torch.cuda.ExternalStream(lib.stream_handle, device=dev)
     psi = torch.zeros(N, dtype=torch.float64, device=dev)
-    grad = torch.empty(N, dtype=torch.float64, device=dev)
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-
-    def step():
-        if world > 1:
-            J, g, C, pairs = solver.evaluate(psi)
-            return pairs
-        solver.evaluate_functional_device(psi.data_ptr(), grad.data_ptr())
-        return solver.last_eval_info["n_pairs"]
-
     for _ in range(max(3, args.warmup)):
-        step()
+        solver.evaluate(psi)
     torch.cuda.synchronize()
     lib.set_profiling(True)
     lib.kernel_times(reset=True)
     times, pairs = [], 0.0
-    if world > 1:
-        torch.distributed.barrier()
+    dist.barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
-        for _ in range(args.steps):
-            with torch.cuda.stream(stream):
-                flush.fill_(1.0)
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            pairs = step()
-            e1.record(stream)
-            e1.synchronize()
-            times.append(e0.elapsed_time(e1))
-        torch.cuda.synchronize()
+        with clk.region():
+            for _ in range(args.steps):
+                with torch.cuda.stream(stream):
+                    flush.fill_(1.0)
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                _, _, _, pairs = solver.evaluate(psi)
+                e1.record(stream)
+                e1.synchronize()
+                times.append(e0.elapsed_time(e1))
+            torch.cuda.synchronize()
     kt = lib.kernel_times(reset=True)
     lib.set_profiling(False)
-    t_ms = float(np.mean(times))
-    if world > 1:
-        t = torch.tensor([t_ms], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        t_ms = float(t.item())
-        torch.distributed.barrier()
-    value = pairs / (t_ms * 1e-3)
-
-    # e2e through the public host API (pinned host psi in, host gradient out)
-    e2e = None
-    if world == 1:
-        hpsi = torch.zeros(N, dtype=torch.float64).pin_memory()
-        hgrad = torch.empty(N, dtype=torch.float64).pin_memory()
-        psi_np, grad_np = hpsi.numpy(), hgrad.numpy()
-        for _ in range(2):
-            solver.evaluate_functional(psi_np, grad_np)
-        et = []
-        for _ in range(args.steps):
-            with torch.cuda.stream(stream):
-                flush.fill_(1.0)
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            solver.evaluate_functional(psi_np, grad_np)
-            e1.record(stream)
-            e1.synchronize()
-            et.append(e0.elapsed_time(e1))
-        e2e = {"value": pairs / (float(np.mean(et)) * 1e-3), "unit": "pairs/s",
-               "h2d_bytes_per_step": int(N * 8), "d2h_bytes_per_step": int(N * 8 + 8),
-               "ms_per_step": float(np.mean(et))}
-
-    if rank != 0:
-        if world > 1:
-            solver.close()
-            torch.distributed.destroy_process_group()
-        return 0
-
-    # roofline of the dominant kernel (device time per launch from CUDA events)
-    peaks = SotSolver.measure_peaks(local)
-    nsteps = args.steps
-    tv = kt["value_sweep"]["ms"] / max(1, kt["value_sweep"]["launches"])
-    tg = kt["gradient_sweep"]["ms"] / max(1, kt["gradient_sweep"]["launches"])
-    local_pairs = lib.last_eval_info["n_pairs"]
-    if tv >= tg:
-        ach = VALUE_FLOPS_PER_PAIR[dim] * local_pairs / (tv * 1e-3) / 1e12
-        kname = ("k_value_dense (FP64 exp2 value sweep)" if prm.tau <= 0 else
-                 "k_fused (FP64 exp2 value sweep + FP32 ex2 gradient sweep, one kernel)")
-        roof = {"kernel": kname,
-                "bound": "fp64", "achieved": ach, "peak": peaks["fp64_tflops"], "unit": "TFLOP/s",
-                "frac": ach / peaks["fp64_tflops"],
-                "traffic": read_traffic("value_sweep", wl["name"]),
-                "flops_per_pair": VALUE_FLOPS_PER_PAIR[dim], "ms_per_launch": tv,
-                "peak_source": "measured on this GPU by sdot_measure_peaks (FP64 FMA chains); "
-                               "MEASURED_PEAKS.json has no FP64 figure"}
-    else:
-        ach = local_pairs / (tg * 1e-3) / 1e9
-        roof = {"kernel": "gradient sweep (FP32 ex2)", "bound": "mufu", "achieved": ach,
-                "peak": peaks["ex2_gops"], "unit": "Gex2/s", "frac": ach / peaks["ex2_gops"],
-                "traffic": read_traffic("gradient_sweep", wl["name"]), "ms_per_launch": tg,
-                "peak_source": "measured on this GPU by sdot_measure_peaks (ex2.approx chains)"}
-    launches = sum(v["launches"] for v in kt.values())
-    line = {"metric": "LSE dual-gradient pairs/s", "value": value, "unit": "pairs/s", "n_gpus": world,
-            "steps": nsteps, "warmup": max(3, args.warmup), "ms_per_step": t_ms, "higher_is_better": True,
-            "scaling": "strong", "vs_baseline": None,
-            "dtype": "f64" if args.precision == "fp64" else "f64 value sweep + f32 exp gradient sweep",
-            "data": "synthetic (seeded; no published dataset)", "config": workload_config(wl, args, world),
-            "pairs_per_step": pairs, "roofline": roof,
-            "kernel_ms_per_step": {k: v["ms"] / nsteps for k, v in kt.items()},
-            "gpu_launches": int(launches), "clocks": clk.summary(), "peaks_measured": peaks}
-    if e2e is not None:
-        line["e2e"] = e2e
-    if not args.no_cpu_baseline and world == 1:
-        v, cores, desc, _ = cpu_sample(wl, args.cpu_seconds)
-        line["cpu_baseline"] = {"value": v, "unit": "pairs/s", "cores": cores, "kind": "port", "sample": desc}
-    print(json.dumps(line))
-    if world > 1:
-        solver.close()
-        torch.distributed.destroy_process_group()
+    t = torch.tensor([float(np.mean(times))], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    t_ms = float(t.item())
+    dist.barrier()
+    if rank == 0:
+        value = pairs / (t_ms * 1e-3)
+        peaks = SotSolver.measure_peaks(local)
+        m = {"kt": kt, "pairs_per_step": lib.last_eval_info["n_pairs"]}
+        line = {"metric": "LSE dual-gradient pairs/s", "value": value, "unit": "pairs/s", "n_gpus": world,
+                "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": t_ms, "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None,
+                "dtype": "f64" if args.precision == "fp64" else "f64 value sweep + f32 exp gradient sweep",
+                "data": "synthetic (seeded; no published dataset)", "config": workload_config(wl, args, world),
+                "pairs_per_step": pairs, "roofline": roofline_of(m, wl, peaks, args.precision),
+                "kernel_ms_per_step": {k: v["ms"] / args.steps for k, v in kt.items()},
+                "gpu_launches": int(sum(v["launches"] for v in kt.values())), "clocks": clk.summary(),
+                "peaks_measured": peaks}
+        print(json.dumps(line))
+    solver.close()
+    dist.destroy_process_group()
     return 0
 
 
@@ -438,7 +663,7 @@ def run_hessian_3d(args):
     H = torch.empty((N, N), dtype=torch.float32, device="cuda")
     for _ in range(max(3, args.warmup)):
         s.compute_hessian_device(psi.data_ptr(), H.data_ptr(), method="tensor", out_f32=True)
-    with ClockSampler(0) as clk:
+    with ClockSampler(0) as clk, clk.region():
         ks = []
         for _ in range(args.steps):
             info = s.compute_hessian_device(psi.data_ptr(), H.data_ptr(), method="tensor", out_f32=True)
@@ -532,7 +757,7 @@ def run_batched_2d(args):
     warm = W.batched_2d(seed=1, n_problems=nw)   # other problems of the same distribution
     for p in probs + warm:
         p.update(method="newton", eps_factor=10.0, eps_steps=2, inter_tol=1e-6)
-    with ClockSampler(0) as clk:
+    with ClockSampler(0) as clk, clk.region():
         res, wall, st = _solve_requests_through_server(probs, args.slots, 0.0, 0, warm)
     conv = sum(r["converged"] for r in res)
     base = _fp64_lbfgs_baseline(probs, args.baseline_seconds)
@@ -590,7 +815,7 @@ def run_serve_3d(args):
     reqs = serve_requests(args.problems, 0, args.scale)
     nw = max(args.warmup, 2 * args.slots)
     warm = serve_requests(nw, 12345, args.scale)   # other requests of the same mix
-    with ClockSampler(0) as clk:
+    with ClockSampler(0) as clk, clk.region():
         res, wall, st = _solve_requests_through_server(reqs, args.slots, args.rate, 1, warm)
     conv = sum(r["converged"] for r in res)
     line = {"metric": "served solves/s at grad linf 1e-8 (p50/p99 latency)", "value": conv / wall,

@@ -181,6 +181,16 @@ sdot_status sdot_hessian_device(sdot_ctx *ctx, const double *psi_dev, void *H_de
 /* Tuning of the tensor method: stages of 64 points accumulated in FP32 before
  * each FP64 drain (default 64). */
 sdot_status sdot_set_hessian_chunk(sdot_ctx *ctx, int stages);
+/* Bound of the tensor method's device-side waits (no reference counterpart:
+ * the reference has no device code).  The kernel's stage loop waits on
+ * mbarriers for its tensor-core products; a wait that takes more than
+ * `clocks` SM clock cycles makes the kernel stop, wait (with the default
+ * bound) for the products already issued, release its tensor memory and
+ * report SDOT_ETIMEOUT, leaving the context usable.  clocks <= 0 restores
+ * the default, 2e9 cycles (about 1 s at 1.965 GHz).  A bound below the
+ * products' own latency (a few thousand cycles) makes every call time out:
+ * that is how the failure path is tested. */
+sdot_status sdot_set_hessian_wait_limit(sdot_ctx *ctx, int64_t clocks);
 
 /* The tensor-core Hessian in pieces, for sharding it over GPUs by output tiles
  * (no reference counterpart: the reference's Hessian is declared only,
@@ -453,9 +463,13 @@ sdot_status sdot_measure_peaks(int device, double *out);
  *   - The scratch is shared by all contexts of the process on a device: calls
  *     whose executions overlap (other threads, streams or contexts on the same
  *     device) race and corrupt each other's results.  Serialise them.
- *   - The first call on a device does one-time set-up (it looks up the
- *     scratch address with cudaGetSymbolAddress, which may load the module);
- *     make it before any stream capture.
+ *   - The first call on a device does one-time set-up: it looks up the
+ *     scratch address with cudaGetSymbolAddress, which may load the module,
+ *     so make that first call before any stream capture.  The address is
+ *     kept for the life of the process; a cudaDeviceReset invalidates it, so
+ *     make no no-alloc call after one.
+ *   - Every call ends by synchronising the context's stream and reading the
+ *     scalars (J, C_global, norms) back to the host.
  * psi_dev, grad_dev: device arrays of n_targets doubles in caller order;
  * *value receives J.  Updates the same state as sdot_evaluate_device. */
 #define SDOT_NOALLOC_SCRATCH_BYTES (8u << 20)

@@ -20,8 +20,11 @@
 
 namespace sdot {
 
-// SotParameterManager::SolverParameters (ParameterManager.h:56-72), the
-// fields on the accelerated path.
+// SotParameterManager::SolverParameters (ParameterManager.h:56-72), every
+// field with the reference's default, plus the line-search variant.  Fields
+// the solve itself does not read (solver_type, quadrature_order, nb_points,
+// n_threads, the epsilon-scaling settings) are kept for the callers that
+// read them, as in the reference.
 struct SolverParameters {
     unsigned max_iterations = 1000;
     double tolerance = 1;
@@ -29,6 +32,14 @@ struct SolverParameters {
     double epsilon = 1e-3;
     double tau = 1e-8;
     std::string distance_threshold_type = "pointwise";  // pointwise | integral | geometric
+    bool verbose_output = true;
+    std::string solver_type = "BFGS";
+    unsigned quadrature_order = 3;
+    unsigned nb_points = 1000;
+    unsigned n_threads = 0;
+    bool use_epsilon_scaling = false;
+    double epsilon_scaling_factor = 2.0;
+    unsigned epsilon_scaling_steps = 5;
     bool use_log_sum_exp_trick = false;
     std::string line_search = "upstream";  // upstream | vendored
 

@@ -97,6 +97,8 @@ def lib():
         _lib.orc_evaluate_cells.restype = d
         _lib.orc_solve.argtypes = [vp, vp, vp, vp, vp, vp, i64, ip]
         _lib.orc_solve.restype = ip
+        _lib.orc_solve_ex.argtypes = [vp, vp, vp, vp, vp, vp, i64, ip, ip]
+        _lib.orc_solve_ex.restype = ip
         _lib.orc_hessian.argtypes = [vp, vp, d, vp, vp, ip]
         _lib.orc_softmax_refinement.argtypes = [vp, vp, d, d, ip, i64, vp, vp, vp, vp, ip]
         _lib.orc_weighted_barycenters.argtypes = [vp, vp, d, vp, vp, ip]
@@ -218,13 +220,13 @@ class Problem:
                                      C.byref(Cv), C.byref(npairs), int(faithful), threads)
         return J, g, Cv.value, npairs.value
 
-    def solve(self, psi0, prm: Params, threads=0, trace_cap=100000):
+    def solve(self, psi0, prm: Params, threads=0, trace_cap=100000, faithful=False):
         psi = np.array(psi0, dtype=np.float64, copy=True)
         info = _SolveInfo()
         trace = np.zeros((trace_cap, 3))
         pc = prm.c()
-        lib().orc_solve(C.byref(self._c), C.byref(pc), C.byref(self.state), _p(psi),
-                        C.byref(info), _p(trace), trace_cap, threads)
+        lib().orc_solve_ex(C.byref(self._c), C.byref(pc), C.byref(self.state), _p(psi),
+                           C.byref(info), _p(trace), trace_cap, threads, int(bool(faithful)))
         n = info.iterations + 1
         return psi, {"iterations": info.iterations, "converged": bool(info.converged),
                      "status": info.status, "n_evaluations": info.n_evaluations,

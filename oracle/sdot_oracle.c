@@ -485,6 +485,7 @@ typedef struct {
     const orc_params *prm;
     orc_state *s;
     int n_threads;
+    int faithful;
     int64_t n_evals;
     double *x, *x0, *g, *pdir;
     int64_t N;
@@ -500,7 +501,7 @@ static double dot(const double *a, const double *b, int64_t n)
 static double compute_fg(bfgs_ctx *c)
 {
     c->n_evals++;
-    return orc_evaluate(c->p, c->prm, c->s, c->x, c->g, NULL, 0, c->n_threads);
+    return orc_evaluate(c->p, c->prm, c->s, c->x, c->g, NULL, c->faithful, c->n_threads);
 }
 
 /* line_func of the default line search: x = x0 + a p; f = compute(x, g) */
@@ -631,10 +632,18 @@ int orc_solve(const orc_problem *p, const orc_params *prm, orc_state *s,
               double *psi, orc_solve_info *info, double *trace, int64_t trace_cap,
               int n_threads)
 {
+    return orc_solve_ex(p, prm, s, psi, info, trace, trace_cap, n_threads, 0);
+}
+
+int orc_solve_ex(const orc_problem *p, const orc_params *prm, orc_state *s,
+                 double *psi, orc_solve_info *info, double *trace, int64_t trace_cap,
+                 int n_threads, int faithful_overheads)
+{
     const int64_t N = p->n_targets;
     const int M = 5; /* SolverBFGS::AdditionalData::max_history_size */
     bfgs_ctx c;
     c.p = p; c.prm = prm; c.s = s; c.n_threads = n_threads; c.n_evals = 0; c.N = N;
+    c.faithful = faithful_overheads;
     c.x = psi;
     c.x0 = (double *)calloc(N, sizeof(double));
     c.g = (double *)calloc(N, sizeof(double));

@@ -140,6 +140,12 @@ double orc_evaluate_cells(const orc_problem *p, const orc_params *prm, double r,
 int orc_solve(const orc_problem *p, const orc_params *prm, orc_state *s,
               double *psi, orc_solve_info *info, double *trace, int64_t trace_cap,
               int n_threads);
+/* The same solve; faithful_overheads != 0 evaluates with the reference's
+ * per-cell O(N) CopyData zeroing and serialised merge (as orc_evaluate), for
+ * timing the reference-faithful full solve. */
+int orc_solve_ex(const orc_problem *p, const orc_params *prm, orc_state *s,
+                 double *psi, orc_solve_info *info, double *trace, int64_t trace_cap,
+                 int n_threads, int faithful_overheads);
 
 /* Dense Hessian of the dual functional (declared at SotSolver.h:343-344,
  * never defined in the reference):

@@ -13,6 +13,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libsdot_cuda.so")
 
 SDOT_OK = 0
+SDOT_ELINESEARCH = 4
 SDOT_ETIMEOUT = 7
 STATUS_NAMES = {
     0: "SDOT_OK", 1: "SDOT_EINVAL", 2: "SDOT_ENOMEM", 3: "SDOT_ENONFINITE", 4: "SDOT_ELINESEARCH",
@@ -34,7 +35,7 @@ EXPORTED = [
     "sdot_get_C_global", "sdot_set_distance_threshold", "sdot_compute_covering_radius",
     "sdot_compute_geometric_radius_bound", "sdot_set_distance_function", "sdot_evaluate_partial_device",
     "sdot_set_state", "sdot_get_stream", "sdot_set_profiling", "sdot_get_kernel_times", "sdot_measure_peaks",
-    "sdot_evaluate_device_noalloc", "sdot_hessian_device", "sdot_set_hessian_chunk",
+    "sdot_evaluate_device_noalloc", "sdot_hessian_device", "sdot_set_hessian_chunk", "sdot_set_hessian_wait_limit",
     "sdot_solve_newton", "sdot_set_newton_hessian_reuse", "sdot_hessian_tile_count", "sdot_hessian_tiles_device",
     "sdot_hessian_matvec_device", "sdot_softmax_refinement", "sdot_weighted_barycenters", "sdot_conditioned_densities",
     "sdot_batch_create", "sdot_batch_destroy", "sdot_batch_last_error", "sdot_batch_size", "sdot_batch_set_verbose",
@@ -167,6 +168,8 @@ def load():
     lib.sdot_hessian_device.restype = ip
     lib.sdot_set_hessian_chunk.argtypes = [vp, ip]
     lib.sdot_set_hessian_chunk.restype = ip
+    lib.sdot_set_hessian_wait_limit.argtypes = [vp, C.c_int64]
+    lib.sdot_set_hessian_wait_limit.restype = ip
     lib.sdot_solve_newton.argtypes = [vp, vp, C.POINTER(SolverParams), ip, C.POINTER(NewtonInfo)]
     lib.sdot_solve_newton.restype = ip
     lib.sdot_set_newton_hessian_reuse.argtypes = [vp, d]

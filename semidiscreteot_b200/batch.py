@@ -88,7 +88,14 @@ class BatchSolver:
         return vals, self.split(g)
 
     def solve(self, psis=None, epsilon_scaling_factor: float = 10.0, epsilon_scaling_steps: int = 1,
-              intermediate_tolerance: float = 0.0, mixed_precision: bool = True) -> List[np.ndarray]:
+              intermediate_tolerance: float = 0.0, mixed_precision: bool = True,
+              raise_on_line_search: bool = True) -> List[np.ndarray]:
+        """Solves every problem and returns the potentials.  A line-search
+        failure of some problem (SDOT_ELINESEARCH, reported after all other
+        problems have finished) raises, unless raise_on_line_search is False:
+        then the potentials are returned all the same, the failed problems
+        report converged = False in problem_info, and last_info["status"]
+        holds the status."""
         if psis is None:
             flat = np.zeros(sum(self.sizes))
         else:
@@ -99,7 +106,9 @@ class BatchSolver:
         st = self._L.sdot_batch_solve(self._h, flat.ctypes.data, C.byref(opts), C.byref(info))
         self.last_info = {"n_problems": info.n_problems, "converged": info.converged, "rounds": info.rounds,
                           "evaluations": info.evaluations, "total_pairs": info.total_pairs,
-                          "eval_ms": info.eval_ms, "solve_ms": info.solve_ms}
+                          "eval_ms": info.eval_ms, "solve_ms": info.solve_ms, "status": int(st)}
+        if st == _lib.SDOT_ELINESEARCH and not raise_on_line_search:
+            return self.split(flat)
         self._check(st)
         return self.split(flat)
 

@@ -357,6 +357,27 @@ double host_threshold(sdot_ctx *c, double maxpsi, double minpsi)
     return std::sqrt(std::max(0.0, r2));
 }
 
+// Launch shape of the dense sweeps, shared by every dense evaluation path so
+// that they sum in the same order: value-sweep CTAs (one quadrature point per
+// thread), gradient target blocks, and q-slices of the gradient sweep (about
+// eight CTAs per SM in all, at least 256 points per slice, at most 64 slices).
+struct DenseShape {
+    int64_t nval, tb;
+    int nks;
+};
+static DenseShape dense_shape(int64_t nq, int64_t nt)
+{
+    DenseShape d{};
+    const int64_t per = (int64_t)DENSE_A_THREADS * DENSE_A_QT;
+    d.nval = (nq + per - 1) / per;
+    d.tb = (nt + DENSE_B_THREADS * DENSE_B_TT - 1) / (DENSE_B_THREADS * DENSE_B_TT);
+    const int64_t want = (148 * 8 + d.tb - 1) / d.tb;
+    const int64_t maxks = (nq + 255) / 256;
+    d.nks = (int)std::max<int64_t>(1, std::min<int64_t>(want, maxks));
+    if (d.nks > 64) d.nks = 64;
+    return d;
+}
+
 template <int DIM>
 static sdot_status run_eval(sdot_ctx *c, const EvalArgs &a, bool dense, const double *pdir, double tol, bool partial)
 {
@@ -371,17 +392,14 @@ static sdot_status run_eval(sdot_ctx *c, const EvalArgs &a, bool dense, const do
     int64_t nval = 0;
     int nks = 1;
     if (dense) {
-        const int64_t per = (int64_t)DENSE_A_THREADS * DENSE_A_QT;
-        nval = (a.nq + per - 1) / per;
+        const DenseShape ds = dense_shape(a.nq, a.nt);
+        nval = ds.nval;
         k_value_dense<DIM><<<(unsigned)nval, DENSE_A_THREADS, 0, st>>>(c->x.p, c->rho.p, c->jxw.p, c->tpack.p, a,
                                                                        c->Lq.p, c->blkpart.p);
         mark(2);
-        // gradient: target blocks x q-slices, ~4 waves of CTAs
-        const int64_t tb = (a.nt + DENSE_B_THREADS * DENSE_B_TT - 1) / (DENSE_B_THREADS * DENSE_B_TT);
-        int64_t want = (148 * 8 + tb - 1) / tb;
-        int64_t maxks = (a.nq + 255) / 256;
-        nks = (int)std::max<int64_t>(1, std::min<int64_t>(want, maxks));
-        if (nks > 64) nks = 64;
+        // gradient: target blocks x q-slices
+        const int64_t tb = ds.tb;
+        nks = ds.nks;
         const int64_t qslice = (a.nq + nks - 1) / nks;
         dim3 g((unsigned)tb, (unsigned)nks);
         if (prec == SDOT_PREC_FP64)
@@ -511,11 +529,14 @@ sdot_status evaluate_internal(sdot_ctx *c, const double *p_dir, double comp_tol,
 // targets, L_q, gradient partials per q-slice, value / reduction partials,
 // scalars) lives in one file-scope device array of NOALLOC_BYTES instead of
 // the context's lazily allocated evaluation buffers.  Its device address is
-// looked up once per device with cudaGetSymbolAddress and cached.  Every
-// scratch word the evaluation reads is written earlier by the same
-// evaluation on the same stream: nothing has to start at zero, and nothing
-// carries over between calls.  The array is shared by every context of the
-// process on a device, so calls whose executions overlap corrupt each other.
+// looked up once per device with cudaGetSymbolAddress and cached for the
+// life of the process; a cudaDeviceReset by the host application frees the
+// module instance the cached address points into, so no-alloc calls must not
+// follow one.  Every scratch word the evaluation reads is written earlier by
+// the same evaluation on the same stream: nothing has to start at zero, and
+// only the scalar slots the evaluation writes are copied back to the context.
+// The array is shared by every context of the process on a device, so calls
+// whose executions overlap corrupt each other.
 // ---------------------------------------------------------------------------
 
 namespace sdot {
@@ -539,14 +560,9 @@ static NoallocLayout noalloc_layout(int64_t nq, int64_t nt)
 {
     auto up = [](int64_t n) { return (n + 31) / 32 * 32; };
     NoallocLayout L{};
-    const int64_t per = (int64_t)DENSE_A_THREADS * DENSE_A_QT;
-    L.nval = (nq + per - 1) / per;
-    // q-slices of the gradient sweep: the same rule as the dense branch of run_eval
-    const int64_t tb = (nt + DENSE_B_THREADS * DENSE_B_TT - 1) / (DENSE_B_THREADS * DENSE_B_TT);
-    const int64_t want = (148 * 8 + tb - 1) / tb;
-    const int64_t maxks = (nq + 255) / 256;
-    L.nks = (int)std::max<int64_t>(1, std::min<int64_t>(want, maxks));
-    if (L.nks > 64) L.nks = 64;
+    const DenseShape ds = dense_shape(nq, nt);  // the launch shape of the allocating dense path
+    L.nval = ds.nval;
+    L.nks = ds.nks;
     int64_t o = 0;
     L.psi = o;     o += up(nt);
     L.grad = o;    o += up(nt);
@@ -584,7 +600,7 @@ static void noalloc_launch(sdot_ctx *c, const EvalArgs &a, double *S, const Noal
     k_target_prep<DIM><<<grid_for(a.nt, 256), 256, 0, st>>>(a.nt, c->y.p, c->nu.p, psi, a, tpack);
     k_value_dense<DIM><<<(unsigned)L.nval, DENSE_A_THREADS, 0, st>>>(c->x.p, c->rho.p, c->jxw.p, tpack, a, Lq,
                                                                       blkpart);
-    const int64_t tb = (a.nt + DENSE_B_THREADS * DENSE_B_TT - 1) / (DENSE_B_THREADS * DENSE_B_TT);
+    const int64_t tb = dense_shape(a.nq, a.nt).tb;
     const int64_t qslice = (a.nq + L.nks - 1) / L.nks;
     dim3 g((unsigned)tb, (unsigned)L.nks);
     if (c->precision == SDOT_PREC_FP64)
@@ -655,9 +671,19 @@ extern "C" sdot_status sdot_evaluate_device_noalloc(sdot_ctx *c, const double *p
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_error(c, e, "no-alloc evaluation launch");
     if ((s = launch_scatter(c, grad_dev, S + L.grad, c->nt)) != SDOT_OK) return s;
-    e = cudaMemcpyAsync(c->scal_host, S + L.scal, SC_COUNT * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    // k_finalize_scalars writes slots SC_VALUE .. SC_VALSRC except the psi range,
+    // the psi check and the threshold slots (the untruncated path needs none of
+    // them); those are set on the host below, so nothing an earlier call left in
+    // the shared array reaches the context.
+    e = cudaMemcpyAsync(c->scal_host, S + L.scal, (SC_VALSRC + 1) * sizeof(double), cudaMemcpyDeviceToHost,
+                        c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) return cuda_error(c, e, "no-alloc evaluation");
+    c->scal_host[SC_MAXPSI] = NAN;
+    c->scal_host[SC_MINPSI] = NAN;
+    c->scal_host[SC_PSIBAD] = 0.0;
+    c->scal_host[SC_SSTAR] = a.sstar;
+    for (int i = SC_VALSRC + 1; i < SC_COUNT; ++i) c->scal_host[i] = 0.0;
     c->klaunch[1] += 1;
     c->klaunch[2] += 1;
     c->klaunch[3] += 1;

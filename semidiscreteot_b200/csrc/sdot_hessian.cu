@@ -300,6 +300,13 @@ extern "C" sdot_status sdot_set_hessian_chunk(sdot_ctx *c, int stages)
     return SDOT_OK;
 }
 
+extern "C" sdot_status sdot_set_hessian_wait_limit(sdot_ctx *c, int64_t clocks)
+{
+    if (!c) return SDOT_EINVAL;
+    c->hess_wait_limit = clocks > 0 ? (long long)clocks : 0;
+    return SDOT_OK;
+}
+
 extern "C" sdot_status sdot_hessian(sdot_ctx *c, const double *psi, double *H)
 {
     if (!c || !psi || !H) return SDOT_EINVAL;

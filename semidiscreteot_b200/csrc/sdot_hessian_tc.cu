@@ -79,6 +79,10 @@ constexpr int SCR_PER_CTA = M * N;                        // FP64 drain scratch 
 constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
                            ((uint32_t)(M >> 4) << 24);
 
+// Waits of the stage loop give up after a limit of SM clocks set per context
+// (sdot_set_hessian_wait_limit; default WAIT_LIMIT, about 1 s).  The error
+// path's wait for the MMAs in flight always uses WAIT_LIMIT, so the tensor
+// memory is released only after the last commit has landed.
 constexpr long long WAIT_LIMIT = 2000000000ll;  // SM clocks (~1 s)
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -102,12 +106,12 @@ __device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity)
 }
 
 // Bounded wait for the completion of the phase with the given parity.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long limit)
 {
     if (mbar_test(bar, parity)) return true;
     const long long t0 = clock64();
     while (!mbar_test(bar, parity))
-        if (clock64() - t0 > WAIT_LIMIT) return false;
+        if (clock64() - t0 > limit) return false;
     return true;
 }
 
@@ -219,6 +223,7 @@ struct Args {
     double *scratch;        // SCR_PER_CTA doubles per CTA
     void *H;
     int *err;
+    long long wait_limit;   // SM clocks a stage-loop wait may take before the kernel aborts
 };
 
 template <int DIM, typename OutT>
@@ -368,8 +373,15 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
     const int row = quad * 32 + lane;
     double *scr = a.scratch + (size_t)blockIdx.x * SCR_PER_CTA;
     auto drain = [&](unsigned pc, int2 tl, bool first, bool last) -> bool {
-        const bool ok = mbar_wait(bar0 + 8 * (2 + (pc & 1)), (pc >> 1) & 1);
+        const bool ok = mbar_wait(bar0 + 8 * (2 + (pc & 1)), (pc >> 1) & 1, a.wait_limit);
         tc_fence_after();
+        // a warp reads its accumulator lanes only when every lane saw the
+        // commit land (tcgen05.ld is warp-collective); otherwise the kernel is
+        // aborting and the chunk is dropped
+        if (!__all_sync(0xffffffffu, ok)) {
+            tc_fence_before();
+            return false;
+        }
         const int64_t ga = (int64_t)tl.x * M + row;
         const uint32_t taddr = tmem + (pc & 1) * N + cq * 64 + ((uint32_t)(quad * 32) << 16);
 #pragma unroll 1
@@ -406,7 +418,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
     bool pend_first = false, pend_last = false;
     bool bad = false;        // this thread saw a wait expire
     bool aborted = false;
-    int last_g = -1;
+    unsigned ncommit[4] = {0, 0, 0, 0};  // commits issued per mbarrier (thread 0)
 
     if ((int)blockIdx.x < a.ntiles) {
         // stage 0 into Eg/qs[0]; stage 1's inputs into raw[1]
@@ -433,7 +445,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
             const bool has_next = !last_of_tile || t + (int)gridDim.x < a.ntiles;
             raw_copy(sb, (st + 2) % a.nst);     // inputs of stage g + 2 (its point block)
             // the MMAs that read this buffer two stages ago must be complete
-            if (g >= 2 && !mbar_wait(bar0 + 8 * sb, ((g >> 1) - 1) & 1)) bad = true;
+            if (g >= 2 && !mbar_wait(bar0 + 8 * sb, ((g >> 1) - 1) & 1, a.wait_limit)) bad = true;
             generate(sb);
             if (has_next) {
                 if (last_of_tile) load_target(tl_nxt);   // once per tile
@@ -459,9 +471,12 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
                     umma_bf16(dcol, al, bh, 1u);
                 }
                 umma_commit(bar0 + 8 * sb);
-                if (last_in_chunk) umma_commit(bar0 + 8 * (2 + cb));
+                ++ncommit[sb];
+                if (last_in_chunk) {
+                    umma_commit(bar0 + 8 * (2 + cb));
+                    ++ncommit[2 + cb];
+                }
             }
-            last_g = g;
             // drain the previous chunk while the tensor core works on this one
             if (first_in_chunk && pend >= 0) {
                 if (!drain((unsigned)pend, pend_tl, pend_first, pend_last)) bad = true;
@@ -482,8 +497,13 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
     if (__syncthreads_or(bad)) aborted = true;
     if (aborted && tid == 0) {
         atomicExch(a.err, 1);
-        // let the MMAs in flight finish before the tensor memory is released
-        if (last_g >= 0) mbar_wait(bar0 + 8 * (last_g & 1), (last_g >> 1) & 1);
+        // Let the MMAs in flight finish, and every commit arrive, before the
+        // tensor memory is released and the CTA exits.  Each mbarrier has at
+        // most one phase outstanding here (every earlier phase was waited for
+        // successfully, or the loop would have stopped there), so waiting for
+        // the phase of its last commit, in order, covers them all.
+        for (int i = 0; i < 4; ++i)
+            if (ncommit[i] > 0) mbar_wait(bar0 + 8 * i, (ncommit[i] - 1) & 1, WAIT_LIMIT);
     }
     tc_fence_before();
     __syncthreads();
@@ -665,6 +685,7 @@ sdot_status hessian_tc(sdot_ctx *c, void *H_dev, bool out_f32, int chunk_stages,
     a.scratch = c->htc_scr.p;
     a.H = H_dev;
     a.err = c->htc_err.p;
+    a.wait_limit = c->hess_wait_limit > 0 ? c->hess_wait_limit : WAIT_LIMIT;
     void (*kern)(const Args) = nullptr;
     if (c->dim == 2) kern = out_f32 ? k_hessian_tc<2, float> : k_hessian_tc<2, double>;
     else kern = out_f32 ? k_hessian_tc<3, float> : k_hessian_tc<3, double>;

@@ -174,6 +174,7 @@ struct sdot_ctx {
     double hess_kernel_ms = 0.0;
     int64_t hess_tiles = 0;
     int hess_chunk = 64;               // stages (x 64 points) per FP32 accumulation chunk
+    long long hess_wait_limit = 0;     // SM clocks per stage-loop mbarrier wait (<= 0: the default, ~1 s)
     double newton_reuse = 0.1;         // lagged-Hessian contraction threshold (0: recompute every step)
     sdot::DevBuf<float> nt_H32;        // Newton: tensor-core Hessian (caller order)
     sdot::DevBuf<double> nt_H64;       // Newton: FP64 Hessian when the tensor method does not apply

@@ -5,7 +5,9 @@
 names and defaults; ``MultilevelParameters`` mirrors ``MultilevelParameters``
 (:78-98).  ``read_prm`` understands the deal.II ParameterHandler grammar the
 reference's parameter files use (``subsection NAME`` / ``set key = value`` /
-``end``, ``#`` comments; src/utils/ParameterManager.cc:20-158, run/parameters.prm).
+``end``, ``#`` comments, a trailing backslash continuing a line;
+src/utils/ParameterManager.cc:20-158, run/parameters.prm).  The C++ reader
+``include/sdot/ParameterFile.hpp`` parses the same grammar the same way.
 Keys of this implementation that the reference does not have live in a
 separate ``subsection b200`` (precision, line_search).
 """
@@ -82,8 +84,17 @@ def read_prm(path_or_text: str, is_text: bool = False) -> Dict[str, Any]:
     text = path_or_text if is_text else open(path_or_text).read()
     root: Dict[str, Any] = {}
     stack = [root]
+    pending, start = "", 0
     for lineno, raw in enumerate(text.splitlines(), 1):
-        line = raw.split("#", 1)[0].strip()
+        if not pending:
+            start = lineno
+        part = raw.split("#", 1)[0]
+        if "#" not in raw and part.strip().endswith("\\"):   # continued on the next line
+            pending += part.strip()[:-1] + " "
+            continue
+        line = (pending + part).strip()
+        pending = ""
+        lineno = start
         if not line:
             continue
         if line.startswith("subsection "):
@@ -102,6 +113,8 @@ def read_prm(path_or_text: str, is_text: bool = False) -> Dict[str, Any]:
             stack[-1][k.strip()] = v.strip()
         else:
             raise ValueError(f"line {lineno}: cannot parse {raw!r}")
+    if pending:
+        raise ValueError(f"line {start}: line continuation at end of file")
     if len(stack) != 1:
         raise ValueError("unterminated subsection")
     return root
@@ -140,6 +153,8 @@ def b200_options_from_prm(tree: Dict[str, Any]) -> Dict[str, Any]:
     out: Dict[str, Any] = {}
     if "precision" in node:
         out["precision"] = node["precision"].strip()
+        if out["precision"] not in ("fp64", "hybrid", "mixed"):
+            raise ValueError(f"b200.precision: unknown precision {out['precision']!r}")
     if "device" in node:
         out["device"] = int(node["device"])
     return out

@@ -316,6 +316,11 @@ class SotSolver:
         """Stages of 64 points accumulated in FP32 between FP64 drains (tensor Hessian)."""
         self._check(self._L.sdot_set_hessian_chunk(self._h, int(stages)))
 
+    def set_hessian_wait_limit(self, clocks: int):
+        """SM clocks a device-side wait of the tensor Hessian may take before the
+        call fails with SDOT_ETIMEOUT (<= 0: the default, about 1 s)."""
+        self._check(self._L.sdot_set_hessian_wait_limit(self._h, int(clocks)))
+
     def evaluate_partial_device(self, psi_ptr: int, out_ptr: int) -> dict:
         """Source-shard evaluation into out[n_targets + 3] on the device (see
         sdot_evaluate_partial_device); the caller all-reduces and finishes."""

@@ -122,31 +122,27 @@ def test_batch_solve_mixed_precision_meets_fp64_tolerance():
     b = BatchSolver(dim=2)
     for src, y, nu, prm in probs:
         b.add_source(src, y, nu, prm)
-    try:
-        res = b.solve(mixed_precision=True)
-    except RuntimeError as e:
-        assert "line search" in str(e)
-        res = None
+    # a line-search failure of one problem (the reference's line search may
+    # fail near a tight tolerance on the last bits of J) still returns every
+    # problem's potential; the failed one reports converged = False
+    res = b.solve(mixed_precision=True, raise_on_line_search=False)
+    assert b.last_info["status"] in (0, 4)
+    assert len(res) == len(probs)
     n_conv = 0
-    for i, ((src, y, nu, prm), (psi_r, _, conv_r)) in enumerate(zip(probs, ref)):
-        pi = b.problem_info(i)
-        if not pi["converged"]:
+    for i, ((src, y, nu, prm), psi, (psi_r, _, conv_r)) in enumerate(zip(probs, res, ref)):
+        if not b.problem_info(i)["converged"]:
             continue
         n_conv += 1
-        assert res is not None or True
+        s = single(src, y, nu, prm)
+        g = np.zeros(len(nu))
+        s.evaluate_functional(psi, g)
+        s.close()
+        assert np.max(np.abs(g)) <= 1e-8           # met in FP64
+        if psi_r is not None:
+            d = (psi - psi.mean()) - (psi_r - psi_r.mean())
+            assert np.max(np.abs(d)) <= 1e-5   # two 1e-8-stationary points: |dpsi| ~ eps tol / nu_min
     assert n_conv >= sum(r[2] for r in ref) - 1
-    if res is not None:
-        for i, ((src, y, nu, prm), psi, (psi_r, _, _)) in enumerate(zip(probs, res, ref)):
-            if not b.problem_info(i)["converged"]:
-                continue
-            s = single(src, y, nu, prm)
-            g = np.zeros(len(nu))
-            s.evaluate_functional(psi, g)
-            s.close()
-            assert np.max(np.abs(g)) <= 1e-8           # met in FP64
-            if psi_r is not None:
-                d = (psi - psi.mean()) - (psi_r - psi_r.mean())
-                assert np.max(np.abs(d)) <= 1e-5   # two 1e-8-stationary points: |dpsi| ~ eps tol / nu_min
+    assert b.last_info["converged"] == n_conv
     b.close()
 
 

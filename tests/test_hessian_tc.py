@@ -140,3 +140,31 @@ def test_tensor_hessian_rejects_truncated():
     _, info = hessian(s, psi, "auto")
     assert info["method"] == "fp64"
     s.close()
+
+
+def test_wait_timeout_reports_and_recovers():
+    """The tensor Hessian's device-side waits are bounded.  With a bound far
+    below the latency of one stage's tensor-core products (12 MMAs of
+    128 x 256 x 16, some 1,600 SM cycles), the wait for the last chunk's
+    accumulator expires: the kernel stops, waits (with the default bound) for
+    the products in flight, releases its tensor memory and reports
+    SDOT_ETIMEOUT.  The context stays usable: with the default bound restored,
+    the next Hessian equals one computed before the timeout, bit for bit."""
+    from semidiscreteot_b200 import _lib
+    src, y, nu, eps = problem("dense3d", seed=5)
+    s = make(src, y, nu, eps)
+    N = len(nu)
+    psi = 0.2 * eps * np.random.default_rng(4).standard_normal(N)
+    H0, _ = hessian(s, psi, "tensor")
+    s.set_hessian_wait_limit(100)
+    with pytest.raises(_lib.SdotError) as ei:
+        hessian(s, psi, "tensor")
+    assert ei.value.status == _lib.SDOT_ETIMEOUT
+    s.set_hessian_wait_limit(0)
+    H1, _ = hessian(s, psi, "tensor")
+    assert np.array_equal(H0, H1)
+    # evaluations on the same context are unaffected
+    g = np.zeros(N)
+    s.evaluate_functional(psi, g)
+    assert np.all(np.isfinite(g))
+    s.close()
