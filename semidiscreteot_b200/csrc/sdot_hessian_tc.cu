@@ -105,11 +105,35 @@ __device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity)
     return ok != 0;
 }
 
+// Non-blocking test of the same phase (mbarrier.test_wait never suspends).
+__device__ __forceinline__ bool mbar_test_nb(uint32_t bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
 // Bounded wait for the completion of the phase with the given parity.
+// mbarrier.try_wait may suspend the thread in hardware until the phase
+// completes (up to a system-dependent time), so with a bound below about
+// 1e5 SM clocks the wait polls with the non-blocking test instead, which
+// honours the bound to within one poll.
+constexpr long long WAIT_POLL_BELOW = 100000;
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long limit)
 {
-    if (mbar_test(bar, parity)) return true;
+    if (mbar_test_nb(bar, parity)) return true;
     const long long t0 = clock64();
+    if (limit < WAIT_POLL_BELOW) {
+        while (!mbar_test_nb(bar, parity))
+            if (clock64() - t0 > limit) return false;
+        return true;
+    }
     while (!mbar_test(bar, parity))
         if (clock64() - t0 > limit) return false;
     return true;

@@ -197,23 +197,34 @@ def test_bad_inputs():
     s.close()
 
 
-def test_partial_groups_identical(oracle_mod, monkeypatch):
-    """A tiny cap on the gradient-partial buffer forces the truncated path to
-    process source blocks in several groups; results must not change."""
-    src, y, nu, kw = make_problem("trunc3d")
-    prm = SolverParameters(epsilon=kw["epsilon"], tau=kw["tau"], use_log_sum_exp_trick=True)
-    psi = np.linspace(-2e-3, 2e-3, len(nu))
-    s = product(src, y, nu, 3, "hybrid")
+@pytest.mark.parametrize("precision", ["fp64", "hybrid"])
+def test_clustered_targets_need_several_chunks(oracle_mod, precision):
+    """4,000 targets in one tight cluster: every source block near it stages
+    all of them, several chunks of at most 1,024, so the value sweep carries
+    its online sums across chunks and records candidate masks chunk by chunk
+    for the gradient gather.  Compared with the oracle at the parity
+    tolerances; repeated evaluations are bitwise identical."""
+    rng = np.random.default_rng(21)
+    src = structured_source(3, 8, 2)
+    N = 4000
+    y = np.clip(0.5 + 0.02 * rng.standard_normal((N, 3)), 0, 1)
+    nu = rng.dirichlet(np.ones(N) * 2)
+    eps, tau = 4e-3, 1e-10
+    prm = SolverParameters(epsilon=eps, tau=tau, use_log_sum_exp_trick=True)
+    s = product(src, y, nu, 3, precision)
     s.configure(prm)
-    g1 = np.zeros(len(nu))
-    J1 = s.evaluate_functional(psi, g1)
+    psi = 1e-3 * rng.standard_normal(N)
+    g = np.zeros(N)
+    J = s.evaluate_functional(psi, g)
+    P = oracle_problem(oracle_mod, src, y, nu)
+    Jo, go, st = P.evaluate(psi, oracle_mod.Params(epsilon=eps, tau=tau, use_log_sum_exp=True))
+    assert s.last_eval_info["n_pairs"] == st["n_pairs"]
+    ctr = np.asarray(src["cell_centers"]).reshape(-1, 3)
+    near = ctr[np.argmin(np.sum((ctr - 0.5) ** 2, axis=1))]
+    assert P.candidates(near, st["threshold"]).size > 3 * 1024   # one cell alone needs four chunks
+    assert abs(J - Jo) <= 1e-10 * abs(Jo)
+    assert np.max(np.abs(g - go)) <= grad_tol(nu, precision)
+    assert abs(s.get_C_global() - st["C_global"]) <= 1e-10 * abs(st["C_global"])
+    g2 = np.zeros(N)
+    assert s.evaluate_functional(psi, g2) == J and np.array_equal(g, g2)
     s.close()
-    monkeypatch.setenv("SDOT_PART_CAP_BYTES", str(64 * 1024))
-    s = product(src, y, nu, 3, "hybrid")
-    s.configure(prm)
-    g2 = np.zeros(len(nu))
-    J2 = s.evaluate_functional(psi, g2)
-    s.close()
-    assert J1 == J2
-    # group sums add partials in the same order per target; allow last-bit drift
-    assert np.max(np.abs(g1 - g2)) <= 1e-15
