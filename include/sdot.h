@@ -455,8 +455,10 @@ sdot_status sdot_measure_peaks(int device, double *out);
  * latency-bound loop that cannot absorb cudaMalloc / cudaFree and the
  * synchronisation they imply.  The set-up calls (sdot_create,
  * sdot_set_source, sdot_set_target) still allocate, as before.
- *   - Requests whose scratch exceeds the limit (about 8 * n_q + (10 + slices)
- *     * 8 * n_targets bytes, slices <= 64) are rejected with SDOT_EINVAL and
+ *   - Requests whose scratch exceeds the limit (about 8 * n_q * (1 + 2 * vs)
+ *     + (10 + slices) * 8 * n_targets bytes, where vs <= 16 is the number of
+ *     target slices of the value sweep when n_q < 75,776 and 0 otherwise, and
+ *     slices <= 64 that of the gradient sweep) are rejected with SDOT_EINVAL and
  *     a message giving the need and the limit; truncated problems likewise.
  *   - Nothing in the scratch has to start at zero: every word a call reads is
  *     written earlier by the same call on the context's stream.

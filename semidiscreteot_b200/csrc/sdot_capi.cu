@@ -203,7 +203,8 @@ size_t device_bytes(const sdot_ctx *c)
            c->inv_b.bytes() + c->inv2fwd.bytes() + c->inv_tmpb.bytes() + c->inv_tmpk.bytes() + c->inv_off.bytes() +
            c->y.bytes() + c->nu.bytes() + c->perm.bytes() +
            c->tblk_sph.bytes() + c->psi.bytes() + c->grad.bytes() + c->tpack.bytes() + c->Lq.bytes() +
-           c->gpart.bytes() + c->blkpart.bytes() + c->scal.bytes() + c->redpart.bytes() + c->io_a.bytes() +
+           c->gpart.bytes() + c->blkpart.bytes() + c->scal.bytes() + c->redpart.bytes() + c->vpart.bytes() +
+           c->io_a.bytes() +
            c->io_b.bytes() + c->x0.bytes() + c->pdir.bytes() + c->sk.bytes() + c->yk.bytes() + c->hist_s.bytes() +
            c->hist_y.bytes() + c->gtmp.bytes() + c->htc_tdat.bytes() + c->htc_diag.bytes() + c->htc_blk.bytes() +
            c->htc_scr.bytes() + c->htc_qa.bytes() + c->htc_qb.bytes() + c->htc_tiles.bytes() + c->htc_err.bytes();
@@ -437,6 +438,7 @@ void sdot_destroy(sdot_ctx *c)
         c->y.release(); c->nu.release();
         c->perm.release(); c->tblk_sph.release(); c->psi.release(); c->grad.release(); c->tpack.release();
         c->Lq.release(); c->gpart.release(); c->blkpart.release(); c->scal.release(); c->redpart.release();
+        c->vpart.release();
         c->io_a.release(); c->io_b.release(); c->x0.release(); c->pdir.release(); c->sk.release(); c->yk.release();
         c->hist_s.release(); c->hist_y.release(); c->gtmp.release();
         if (c->scal_host) cudaFreeHost(c->scal_host);

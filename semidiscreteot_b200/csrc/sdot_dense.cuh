@@ -90,6 +90,90 @@ __device__ __forceinline__ void dense_value_block(const double *__restrict__ x, 
     block_partials_at(tv, tc, ts, 0.0, out4);
 }
 
+// The same sweep over one slice of the targets [t0, t1), for problems too
+// small to fill the GPU with one CTA per point block: per point it writes
+// the slice's largest scaled exponent mx and the sum relative to it,
+// ms[2 q] = mx, ms[2 q + 1] = sum_j nu_j 2^((b_qj - mx)/16); the merge
+// (dense_value_merge) combines the slices in slice order and finishes.
+template <int DIM>
+__device__ __forceinline__ void dense_value_slice(const double *__restrict__ x, const double *__restrict__ tpack,
+                                                  const EvalArgs &a, int64_t blk, int64_t t0, int64_t t1,
+                                                  double *__restrict__ ms)
+{
+    constexpr int TS = DIM + 2;  // A, B(DIM), nu
+    __shared__ double tab[16];
+    __shared__ double stg[DA_CHUNK * TS];
+    if (threadIdx.x < 16) tab[threadIdx.x] = c_exp2_tab[threadIdx.x];
+    const int64_t q = blk * DENSE_A_THREADS + threadIdx.x;
+    double xt[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) xt[d] = (q < a.nq) ? x[q * DIM + d] - a.o[d] : 0.0;
+    double M = -CUDART_INF, S = 0.0, mx = -CUDART_INF;
+    for (int64_t c0 = t0; c0 < t1; c0 += DA_CHUNK) {
+        const int cn = (int)min((int64_t)DA_CHUNK, t1 - c0);
+        __syncthreads();
+        for (int i = threadIdx.x; i < cn * TS; i += DENSE_A_THREADS) {
+            const int t = i / TS, f = i - t * TS;
+            stg[i] = tpack[(c0 + t) * TPACK + f];
+        }
+        __syncthreads();
+#pragma unroll 2
+        for (int t = 0; t < cn; ++t) {
+            const double *tp = stg + t * TS;
+            double b = fma(tp[1], xt[0], tp[0]);
+#pragma unroll
+            for (int d = 1; d < DIM; ++d) b = fma(tp[1 + d], xt[d], b);
+            lse_update(b, tp[1 + DIM], M, S, mx, tab);
+        }
+    }
+    if (q < a.nq) {
+        ms[2 * q] = mx;
+        ms[2 * q + 1] = (mx == -CUDART_INF) ? 0.0 : S * exp2_16(M - mx, tab);
+    }
+}
+
+// Merge of the target slices of point block blk (slice s of point q at
+// ms[s * 2 nq + 2 q ..]): the largest exponent over the slices, the sums
+// rescaled to it and added in slice order, then the epilogue of
+// dense_value_block (L_q, value, C, skipped) and the block's partials.
+template <int DIM>
+__device__ __forceinline__ void dense_value_merge(const double *__restrict__ x, const double *__restrict__ rho,
+                                                  const double *__restrict__ jxw, const double *__restrict__ ms,
+                                                  int nslice, const EvalArgs &a, int64_t blk,
+                                                  double *__restrict__ Lq, double *__restrict__ out4)
+{
+    __shared__ double tab[16];
+    if (threadIdx.x < 16) tab[threadIdx.x] = c_exp2_tab[threadIdx.x];
+    __syncthreads();
+    const int64_t q = blk * DENSE_A_THREADS + threadIdx.x;
+    double tv = 0.0, tc = 0.0, ts = 0.0;
+    if (q < a.nq) {
+        double mx = -CUDART_INF;
+        for (int s = 0; s < nslice; ++s) mx = fmax(mx, ms[(int64_t)s * 2 * a.nq + 2 * q]);
+        double S = 0.0;
+        if (mx > -CUDART_INF)
+            for (int s = 0; s < nslice; ++s) {
+                const double m = ms[(int64_t)s * 2 * a.nq + 2 * q];
+                if (m > -CUDART_INF) S += ms[(int64_t)s * 2 * a.nq + 2 * q + 1] * exp2_16(m - mx, tab);
+            }
+        double xsq = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            const double xt = x[q * DIM + d] - a.o[d];
+            xsq += xt * xt;
+        }
+        const double Cq = -a.halfs * xsq;
+        double v, cv, L;
+        int sk;
+        value_epilogue(a, mx, S, Cq, rho[q], jxw[q], v, cv, L, sk);
+        Lq[q] = L;
+        tv = v;
+        tc = cv;
+        ts = sk;
+    }
+    block_partials_at(tv, tc, ts, 0.0, out4);
+}
+
 // ---------------------------------------------------------------------------
 // gradient sweep, dense: thread <-> DENSE_B_TT targets, q-slices streamed
 // through shared memory (broadcast reads); FP64 partial per (slice, target).

@@ -148,6 +148,27 @@ k_value_dense(const double *__restrict__ x, const double *__restrict__ rho, cons
     dense_value_block<DIM>(x, rho, jxw, tpack, a, blockIdx.x, Lq, part + (int64_t)blockIdx.x * 4);
 }
 
+static_assert(DENSE_A_QT == 1, "the sliced dense value sweep keeps one point per thread");
+
+template <int DIM>
+__global__ void __launch_bounds__(DENSE_A_THREADS)
+k_value_dense_slice(const double *__restrict__ x, const double *__restrict__ tpack, EvalArgs a, int64_t tslice,
+                    double *__restrict__ ms)
+{
+    const int64_t t0 = blockIdx.y * tslice;
+    const int64_t t1 = min(a.nt, t0 + tslice);
+    dense_value_slice<DIM>(x, tpack, a, blockIdx.x, t0, t1, ms + (int64_t)blockIdx.y * 2 * a.nq);
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(DENSE_A_THREADS)
+k_value_dense_merge(const double *__restrict__ x, const double *__restrict__ rho, const double *__restrict__ jxw,
+                    const double *__restrict__ ms, int nslice, EvalArgs a, double *__restrict__ Lq,
+                    double *__restrict__ part)
+{
+    dense_value_merge<DIM>(x, rho, jxw, ms, nslice, a, blockIdx.x, Lq, part + (int64_t)blockIdx.x * 4);
+}
+
 template <int DIM, bool FP32>
 __global__ void __launch_bounds__(DENSE_B_THREADS)
 k_grad_dense(const double *__restrict__ x, const double *__restrict__ w, const double *__restrict__ Lq,
@@ -358,18 +379,30 @@ double host_threshold(sdot_ctx *c, double maxpsi, double minpsi)
 }
 
 // Launch shape of the dense sweeps, shared by every dense evaluation path so
-// that they sum in the same order: value-sweep CTAs (one quadrature point per
-// thread), gradient target blocks, and q-slices of the gradient sweep (about
-// eight CTAs per SM in all, at least 256 points per slice, at most 64 slices).
+// that they sum in the same order: value-sweep point blocks (one quadrature
+// point per thread) and, when those are too few to fill the GPU (fewer than
+// four per SM), target slices of the value sweep (about twelve CTAs per SM in
+// all, at least 64 targets per slice, at most 16 slices) merged per point;
+// gradient target blocks, and q-slices of the gradient sweep (about eight
+// CTAs per SM in all, at least 256 points per slice, at most 64 slices).
 struct DenseShape {
     int64_t nval, tb;
     int nks;
+    int nvs;          // target slices of the value sweep (1: unsliced)
+    int64_t tslice;   // targets per value slice
 };
 static DenseShape dense_shape(int64_t nq, int64_t nt)
 {
     DenseShape d{};
     const int64_t per = (int64_t)DENSE_A_THREADS * DENSE_A_QT;
     d.nval = (nq + per - 1) / per;
+    d.nvs = 1;
+    if (d.nval < 148 * 4) {
+        const int64_t want = (148 * 12 + d.nval - 1) / d.nval;
+        const int64_t maxs = std::max<int64_t>(1, nt / 64);
+        d.nvs = (int)std::max<int64_t>(1, std::min<int64_t>(16, std::min(want, maxs)));
+    }
+    d.tslice = (nt + d.nvs - 1) / d.nvs;
     d.tb = (nt + DENSE_B_THREADS * DENSE_B_TT - 1) / (DENSE_B_THREADS * DENSE_B_TT);
     const int64_t want = (148 * 8 + d.tb - 1) / d.tb;
     const int64_t maxks = (nq + 255) / 256;
@@ -394,8 +427,18 @@ static sdot_status run_eval(sdot_ctx *c, const EvalArgs &a, bool dense, const do
     if (dense) {
         const DenseShape ds = dense_shape(a.nq, a.nt);
         nval = ds.nval;
-        k_value_dense<DIM><<<(unsigned)nval, DENSE_A_THREADS, 0, st>>>(c->x.p, c->rho.p, c->jxw.p, c->tpack.p, a,
-                                                                       c->Lq.p, c->blkpart.p);
+        if (ds.nvs > 1) {
+            const cudaError_t e = c->vpart.alloc((size_t)2 * ds.nvs * a.nq);
+            if (e != cudaSuccess) return cuda_error(c, e, "dense value slices");
+            k_value_dense_slice<DIM><<<dim3((unsigned)nval, (unsigned)ds.nvs), DENSE_A_THREADS, 0, st>>>(
+                c->x.p, c->tpack.p, a, ds.tslice, c->vpart.p);
+            k_value_dense_merge<DIM><<<(unsigned)nval, DENSE_A_THREADS, 0, st>>>(c->x.p, c->rho.p, c->jxw.p,
+                                                                                 c->vpart.p, ds.nvs, a, c->Lq.p,
+                                                                                 c->blkpart.p);
+        } else {
+            k_value_dense<DIM><<<(unsigned)nval, DENSE_A_THREADS, 0, st>>>(c->x.p, c->rho.p, c->jxw.p, c->tpack.p, a,
+                                                                           c->Lq.p, c->blkpart.p);
+        }
         mark(2);
         // gradient: target blocks x q-slices
         const int64_t tb = ds.tb;
@@ -551,9 +594,11 @@ static std::mutex g_noalloc_mu;
 
 // Scratch segments of an evaluation, each rounded up to 256 bytes.
 struct NoallocLayout {
-    int64_t psi, grad, tpack, Lq, gpart, blkpart, redpart, scal, total;  // offsets in doubles
+    int64_t psi, grad, tpack, Lq, gpart, blkpart, redpart, scal, vpart, total;  // offsets in doubles
     int64_t nval;
     int nks;
+    int nvs;
+    int64_t tslice;
 };
 
 static NoallocLayout noalloc_layout(int64_t nq, int64_t nt)
@@ -563,6 +608,8 @@ static NoallocLayout noalloc_layout(int64_t nq, int64_t nt)
     const DenseShape ds = dense_shape(nq, nt);  // the launch shape of the allocating dense path
     L.nval = ds.nval;
     L.nks = ds.nks;
+    L.nvs = ds.nvs;
+    L.tslice = ds.tslice;
     int64_t o = 0;
     L.psi = o;     o += up(nt);
     L.grad = o;    o += up(nt);
@@ -572,6 +619,7 @@ static NoallocLayout noalloc_layout(int64_t nq, int64_t nt)
     L.blkpart = o; o += up(4 * L.nval);
     L.redpart = o; o += up((int64_t)FIN_BLOCKS * NRED);
     L.scal = o;    o += up(SC_COUNT);
+    L.vpart = o;   o += L.nvs > 1 ? up((int64_t)2 * L.nvs * nq) : 0;
     L.total = o;
     return L;
 }
@@ -598,8 +646,16 @@ static void noalloc_launch(sdot_ctx *c, const EvalArgs &a, double *S, const Noal
     double *psi = S + L.psi, *grad = S + L.grad, *tpack = S + L.tpack, *Lq = S + L.Lq, *gpart = S + L.gpart;
     double *blkpart = S + L.blkpart, *redpart = S + L.redpart, *scal = S + L.scal;
     k_target_prep<DIM><<<grid_for(a.nt, 256), 256, 0, st>>>(a.nt, c->y.p, c->nu.p, psi, a, tpack);
-    k_value_dense<DIM><<<(unsigned)L.nval, DENSE_A_THREADS, 0, st>>>(c->x.p, c->rho.p, c->jxw.p, tpack, a, Lq,
-                                                                      blkpart);
+    if (L.nvs > 1) {
+        double *vpart = S + L.vpart;
+        k_value_dense_slice<DIM><<<dim3((unsigned)L.nval, (unsigned)L.nvs), DENSE_A_THREADS, 0, st>>>(
+            c->x.p, tpack, a, L.tslice, vpart);
+        k_value_dense_merge<DIM><<<(unsigned)L.nval, DENSE_A_THREADS, 0, st>>>(c->x.p, c->rho.p, c->jxw.p, vpart,
+                                                                               L.nvs, a, Lq, blkpart);
+    } else {
+        k_value_dense<DIM><<<(unsigned)L.nval, DENSE_A_THREADS, 0, st>>>(c->x.p, c->rho.p, c->jxw.p, tpack, a, Lq,
+                                                                          blkpart);
+    }
     const int64_t tb = dense_shape(a.nq, a.nt).tb;
     const int64_t qslice = (a.nq + L.nks - 1) / L.nks;
     dim3 g((unsigned)tb, (unsigned)L.nks);

@@ -150,6 +150,7 @@ struct sdot_ctx {
 
     // ---- per-evaluation buffers ----
     sdot::DevBuf<double> psi, grad, tpack, Lq, gpart, blkpart, scal, redpart;
+    sdot::DevBuf<double> vpart;        // dense value sweep: per (target slice, point) largest exponent and sum
     sdot::DevBuf<double> io_a, io_b;   // caller-order staging
     double *scal_host = nullptr;       // pinned, SC_COUNT doubles
 

@@ -1047,18 +1047,26 @@ __device__ __forceinline__ double grad_term(const GatherArgs &g, const EvalArgs 
 }
 
 // gacc[j] = sum over the candidates (K, j) of the cell's gradient term, for
-// the targets j of target block t (lane <-> target).  Warp w takes the
-// block pairs w, w + 8, ... of t's inverse list (ascending source block);
-// per pair it reads the value sweep's candidate masks of the source block's
-// cells (one 32-bit word per cell, the bits of t's targets), so neither the
-// exact test nor the staging is repeated.  The 8 warp sums are added in warp
+// the targets j of target block t (lane <-> target).  Warp w takes an equal
+// contiguous share of t's inverse list (ascending source block) and walks it
+// in batches of 32 block pairs: lane i loads pair i's source block, cells and
+// the value sweep's candidate masks of its cells (one 32-bit word per cell,
+// the bits of t's targets), so neither the exact test nor the staging is
+// repeated and the loads of a batch are issued together.  Scanning the
+// masks, each lane queues its own candidate cells (GQ deep, in shared
+// memory); a step computes one queued cell per lane, taken when every lane
+// has one (or a queue is full), so the lanes stay busy although a mask word
+// holds about a quarter of the block's targets.  Each lane adds its terms in
+// queue order, i.e. in (pair, cell) order; the 8 warp sums are added in warp
 // order: no atomics, the order is fixed.
+constexpr int GQ = 16;
 template <int DIM, int TM, bool TS, bool FP32B>
 __global__ void __launch_bounds__(256)
 k_grad_gather(GatherArgs g, EvalArgs a)
 {
     __shared__ double ws[8][32];
     __shared__ double tab[16];
+    __shared__ int queue[8][GQ][32];
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     if (tid < 16) tab[tid] = c_exp2_tab[tid];
     __syncthreads();
@@ -1074,23 +1082,56 @@ k_grad_gather(GatherArgs g, EvalArgs a)
         l2nu = tp[4];
         spsi = tp[5];
     }
+    int *qw = &queue[w][0][0];
+    int head = 0, tail = 0;
     double acc = 0.0;
-    const int64_t p1 = g.inv_off[t + 1];
-    for (int64_t p = g.inv_off[t] + w; p < p1; p += 8) {
-        const int b = g.inv_b[p];
-        const int64_t k = g.inv2fwd[p];
-        const int64_t K0 = g.sblk_cell[b];
-        const int nc = (int)(g.sblk_cell[b + 1] - K0);
-        const unsigned *mk = g.cmask + k * FT_WARPS;
-        for (int c = 0; c < nc; ++c) {
-            const unsigned m = mk[c];
-            if (m == 0u) continue;
-            if ((m >> lane) & 1u) {
-                const double4 cd = g.gcell[K0 + c];
-                if (cd.w < CUDART_INF) acc += grad_term<DIM, TM, TS, FP32B>(g, a, K0 + c, cd, y, l2nu, spsi, tab);
+    auto step = [&]() {
+        if (tail > head) {
+            const int K = qw[(head % GQ) * 32 + lane];
+            ++head;
+            const double4 cd = g.gcell[K];
+            if (cd.w < CUDART_INF) acc += grad_term<DIM, TM, TS, FP32B>(g, a, K, cd, y, l2nu, spsi, tab);
+        }
+    };
+    const int64_t q0 = g.inv_off[t], L = g.inv_off[t + 1] - q0;
+    const int64_t pa = q0 + (L * w) / 8, pb = q0 + (L * (w + 1)) / 8;
+    for (int64_t p0 = pa; p0 < pb; p0 += 32) {
+        const int64_t p = p0 + lane;
+        int K0 = 0, nc = 0;
+        uint4 m0 = make_uint4(0u, 0u, 0u, 0u), m1 = m0;
+        if (p < pb) {
+            const int b = g.inv_b[p];
+            const int64_t k = g.inv2fwd[p];
+            const int64_t c0 = g.sblk_cell[b];
+            K0 = (int)c0;
+            nc = (int)(g.sblk_cell[b + 1] - c0);
+            const uint4 *mk = reinterpret_cast<const uint4 *>(g.cmask + k * FT_WARPS);
+            m0 = mk[0];
+            if (nc > 4) m1 = mk[1];
+        }
+        const int np = (int)min((int64_t)32, pb - p0);
+        for (int i = 0; i < np; ++i) {
+            const int K0i = __shfl_sync(0xffffffffu, K0, i), nci = __shfl_sync(0xffffffffu, nc, i);
+            unsigned mw[8];
+            mw[0] = __shfl_sync(0xffffffffu, m0.x, i);
+            mw[1] = __shfl_sync(0xffffffffu, m0.y, i);
+            mw[2] = __shfl_sync(0xffffffffu, m0.z, i);
+            mw[3] = __shfl_sync(0xffffffffu, m0.w, i);
+            mw[4] = __shfl_sync(0xffffffffu, m1.x, i);
+            mw[5] = __shfl_sync(0xffffffffu, m1.y, i);
+            mw[6] = __shfl_sync(0xffffffffu, m1.z, i);
+            mw[7] = __shfl_sync(0xffffffffu, m1.w, i);
+#pragma unroll
+            for (int c = 0; c < FT_WARPS; ++c) {
+                if (c < nci && ((mw[c] >> lane) & 1u)) {
+                    qw[(tail % GQ) * 32 + lane] = K0i + c;
+                    ++tail;
+                }
+                if (__all_sync(0xffffffffu, tail > head) || __any_sync(0xffffffffu, tail - head == GQ)) step();
             }
         }
     }
+    while (__any_sync(0xffffffffu, tail > head)) step();
     ws[w][lane] = acc;
     __syncthreads();
     if (w == 0 && have) {
