@@ -273,13 +273,15 @@ class ClockSampler:
 
 
 # DRAM traffic per launch of the dominant kernels (dram__bytes_read.sum +
-# dram__bytes_write.sum), from one ncu capture each (null until captured):
-#   k_value_trunc, trunc_3d (2,097,152 points x 100,000 targets):
-#     ncu --set full --clock-control none -k regex:k_value_trunc -s 3 -c 1
+# dram__bytes_write.sum), from one ncu capture each:
+#   k_fused, trunc_3d (2,097,152 points x 100,000 targets), HYBRID:
+#     ncu --set full --clock-control none -k regex:k_fused -s 3 -c 1
 #         python bench.py --steps 1 --warmup 3 --no-cpu-baseline --no-extra
 #   k_value_dense / k_grad_dense, dense_2d: the inputs (0.9 MB) stay in L2, so
 #     DRAM traffic is not a meaningful bound there (null).
-TRAFFIC_BYTES = {}
+TRAFFIC_BYTES = {
+    ("trunc_3d", "hybrid"): 487960576.0,
+}
 
 
 # ---------------------------------------------------------------------------
@@ -443,7 +445,7 @@ def roofline_of(m, wl, peaks, precision):
     truncated = wl["params"].tau > 0
     if tv >= tg or truncated:
         ach = VALUE_FLOPS_PER_PAIR[dim] * pairs / (tv * 1e-3) / 1e12
-        kname = ("k_value_trunc (FP64 exp2 value sweep, exact candidate test, candidate masks)" if truncated else
+        kname = ("k_fused (FP64 exp2 value sweep + FP32 ex2 gradient sweep, one kernel)" if truncated else
                  "k_value_dense (FP64 exp2 value sweep)")
         return {"kernel": kname, "bound": "fp64", "achieved": ach, "peak": peaks["fp64_tflops"], "unit": "TFLOP/s",
                 "frac": ach / peaks["fp64_tflops"], "traffic": TRAFFIC_BYTES.get((wl["name"], precision)),

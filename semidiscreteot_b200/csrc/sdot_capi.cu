@@ -198,9 +198,8 @@ size_t device_bytes(const sdot_ctx *c)
 {
     return c->x.bytes() + c->rho.bytes() + c->jxw.bytes() + c->w.bytes() + c->cell_ctr.bytes() +
            c->sblk_sph.bytes() + c->sblk_sph32.bytes() + c->sblk_cell.bytes() + c->tblk_off.bytes() +
-           c->tblk_sph32.bytes() + c->cmask.bytes() + c->gcell.bytes() + c->gten.bytes() + c->gq.bytes() +
-           c->gqw.bytes() + c->fwd_t.bytes() + c->pmask.bytes() + c->pmpre.bytes() +
-           c->inv_b.bytes() + c->inv2fwd.bytes() + c->inv_tmpb.bytes() + c->inv_tmpk.bytes() + c->inv_off.bytes() +
+           c->tblk_sph32.bytes() + c->part.bytes() + c->fwd_t.bytes() + c->pmask.bytes() + c->pmpre.bytes() +
+           c->inv_b.bytes() + c->fwd2inv.bytes() + c->inv_tmpb.bytes() + c->inv_tmpk.bytes() + c->inv_off.bytes() +
            c->y.bytes() + c->nu.bytes() + c->perm.bytes() +
            c->tblk_sph.bytes() + c->psi.bytes() + c->grad.bytes() + c->tpack.bytes() + c->Lq.bytes() +
            c->gpart.bytes() + c->blkpart.bytes() + c->scal.bytes() + c->redpart.bytes() + c->vpart.bytes() +
@@ -417,6 +416,12 @@ sdot_status sdot_create(sdot_ctx **out, const sdot_options *opts)
     }
     memset(c->scal_host, 0, SC_COUNT * sizeof(double));
     sdot_default_params(&c->prm);
+    // cap on the gradient-partial buffer of the truncated path (bytes); above
+    // it the source blocks are processed in groups
+    if (const char *cap = getenv("SDOT_PART_CAP_BYTES")) {
+        const long long v = atoll(cap);
+        if (v > 0) c->part_cap_bytes = (size_t)v;
+    }
     *out = c;
     return SDOT_OK;
 }
@@ -429,10 +434,9 @@ void sdot_destroy(sdot_ctx *c)
         if (c->stream) cudaStreamSynchronize(c->stream);
         c->x.release(); c->rho.release(); c->jxw.release(); c->w.release();
         c->cell_ctr.release(); c->sblk_sph.release(); c->sblk_sph32.release(); c->sblk_cell.release();
-        c->tblk_off.release(); c->tblk_sph32.release(); c->fwd_t.release();
-        c->cmask.release(); c->gcell.release(); c->gten.release(); c->gq.release(); c->gqw.release();
+        c->tblk_off.release(); c->tblk_sph32.release(); c->part.release(); c->fwd_t.release();
         c->fwd_cnt.release(); c->fwd_off.release(); c->shit.release(); c->spidx.release(); c->scount.release();
-        c->inv_cnt.release(); c->inv_off.release(); c->inv_b.release(); c->inv2fwd.release();
+        c->inv_cnt.release(); c->inv_off.release(); c->inv_b.release(); c->fwd2inv.release();
         c->inv_tmpb.release(); c->inv_tmpk.release();
         c->pmask.release(); c->pmpre.release(); c->superpair.release(); c->ssup_sph32.release(); c->tsup_sph32.release();
         c->y.release(); c->nu.release();

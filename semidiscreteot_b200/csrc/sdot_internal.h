@@ -136,17 +136,15 @@ struct sdot_ctx {
     int tensor_m = 0;                  // > 0: points form an m^dim tensor grid symmetric about the cell centre
     double tensor_amax = 0.0;          // largest per-dimension offset of that grid
 
-    // ---- truncated path: block-pair lists, candidate masks, gradient gather data ----
-    sdot::DevBuf<int64_t> fwd_cnt, fwd_off, inv_cnt, inv_off, inv2fwd;
+    // ---- truncated path: block-pair lists and gradient partials ----
+    sdot::DevBuf<int64_t> fwd_cnt, fwd_off, inv_cnt, inv_off, fwd2inv;
     sdot::DevBuf<int> fwd_t, inv_b, shit, spidx, scount, pmpre, inv_tmpb;
     sdot::DevBuf<int64_t> inv_tmpk;    // inverse-list scatter (forward position per entry)
     sdot::DevBuf<unsigned> pmask;
     sdot::DevBuf<unsigned char> superpair;
     sdot::DevBuf<float4> ssup_sph32, tsup_sph32;  // super-block spheres (32 blocks each)
-    sdot::DevBuf<unsigned> cmask;      // candidate masks, 8 words per forward block pair
-    sdot::DevBuf<double> gcell;        // per cell: centre, reference L (4 doubles)
-    sdot::DevBuf<float> gten;          // per cell, tensor points: offsets and point weights (16 floats)
-    sdot::DevBuf<double> gq, gqw;      // per point: offset and exponent term, weight (other sweeps)
+    sdot::DevBuf<double> part;
+    size_t part_cap_bytes = (size_t)4 << 30;
 
     // ---- per-evaluation buffers ----
     sdot::DevBuf<double> psi, grad, tpack, Lq, gpart, blkpart, scal, redpart;

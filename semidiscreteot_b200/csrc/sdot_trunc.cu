@@ -51,9 +51,14 @@ namespace sdot {
 
 constexpr int FT_WARPS = 8;
 constexpr int FT_MAXS = 1024;               // staged targets per chunk
-// Registers per thread follow from the CTAs an SM holds: the 3D tensor-factored
-// value sweep runs three CTAs per SM (24 warps, 80 registers), the others two.
-__host__ __device__ constexpr int value_min_blocks(int dim, int tq) { return dim == 3 && tq > 0 ? 3 : 2; }
+// The 3D tensor-factored hybrid sweeps stage at most 624 targets per chunk so that
+// their shared memory (75,312 B) lets 3 CTAs share an SM (24 warps instead of
+// 16; registers capped at 80): measured 3.99 ms per trunc_3d evaluation against
+// 4.19 ms with 1,024 targets and 2 CTAs, although more blocks need several chunks.
+constexpr int FT_MAXS_TENSOR = 624;
+__host__ __device__ constexpr bool fused_small(int dim, int tq, bool fp32b) { return dim == 3 && tq > 0 && fp32b; }
+__host__ __device__ constexpr int fused_cap(int dim, int tq, bool fp32b) { return fused_small(dim, tq, fp32b) ? FT_MAXS_TENSOR : FT_MAXS; }
+__host__ __device__ constexpr int fused_min_blocks(int dim, int tq, bool fp32b) { return fused_small(dim, tq, fp32b) ? 3 : 2; }
 constexpr int FT_TS = 6;                    // doubles per staged target: y(3), nu, log2 nu, s*psi
 constexpr int FT_MAXT = 96;                 // target blocks per chunk
 constexpr int FT_MAXQ = 80;                 // quadrature points of one source block
@@ -61,37 +66,65 @@ constexpr int SUPER = 32;                   // blocks per super-block of the pai
 constexpr int FT_PREF = 192;                // forward entries of a block prefetched into smem
 
 struct FusedArgs {
-    const double *x, *rho, *jxw, *cell_ctr;
+    const double *x, *rho, *jxw, *w, *cell_ctr;
     const double *tpk;           // per target: y(3), nu, log2 nu, s*psi, -, -
     const int64_t *sblk_cell;    // source block -> first cell (nsblk + 1)
     const double *sblk_sph;      // FP64 centre(3), radius
     const int64_t *tblk_off;     // target block -> first target (ntblk + 1)
     const int64_t *fwd_off;
     const int *fwd_t;
-    unsigned *cmask;             // candidate masks: FT_WARPS per forward pair (cell-major within the pair)
+    const int64_t *fwd2inv;      // inverse position of each forward pair
+    double *part;                // partials, 32 per pair, at inverse positions minus part_base
     double *Lq;                  // per q (written by the value sweep)
     double *valpart;             // per source block: value, C, skipped, pairs
+    int do_a, do_b;
+    int w_nonneg;                // all w_q >= 0: log2 w_q folded into the FP32 exponent
+    int tlo, thi;                // gradient partials only for target blocks [tlo, thi)
+    int64_t part_base;           // inverse position of the first pair of tlo
     double cullt;                // per-target cull radius addend (r, enlarged)
 };
 
-// Shared memory of the value sweep: 71 KB, so that three CTAs share an SM.
+template <int CAP>
 struct FTSmem {
+    static constexpr int MAXS = CAP;
     double tab[16];
-    double stg[FT_TS][FT_MAXS];   // staged targets, structure of arrays (conflict-free lane access)
+    double stg[FT_TS][CAP];    // staged targets, structure of arrays (conflict-free lane access)
     double qd[FT_MAXQ][4];        // delta_q (FP64) and C'_q
     double qn[FT_MAXQ];           // |delta_q|
+    double qL[FT_MAXQ];           // L_q of the block
+    __align__(16) float qb[FT_MAXQ][4];  // pass B: delta (3) as float, D_q (+ log2 w_q)
+    float qw[FT_MAXQ];            // pass B: w_q
+    float qtw[FT_MAXQ];           // pass B, tensor path: w_q 2^(D_q)
     double cellc[FT_WARPS][3];    // centre of each cell of the block
-    unsigned short cand[FT_WARPS][FT_MAXS];
-    unsigned cbits[FT_WARPS][FT_MAXS / 32];  // candidate bits of each unit by staged position
-    unsigned ebal[FT_MAXT];       // surviving lanes of each entry of the chunk
-    short epos[FT_MAXT];          // staged position of each entry's first survivor
+    float pvw[FT_WARPS][CAP];     // gradient partial of each unit (warp) per staged target (FP32 mode)
+    unsigned short cand[FT_WARPS][CAP];
+    short smap[FT_MAXT][TBLK_KD]; // (chunk target block, slot) -> staged position or -1
+    int ctb[FT_MAXT];             // target blocks of the chunk
+    int64_t cpos[FT_MAXT];        // their partial base index
     int ecnt[32];                 // survivors per examined forward entry (-1: none)
     int epre[32];                 // staged position of the first survivor of each accepted entry
     int eacc, etot;
+    int wcount[FT_WARPS];
     int nstg;
-    int ent_j0[FT_PREF];           // forward entries of the block: first target of the target block
+    int ent_t[FT_PREF];            // forward entries of the block: target block,
+    int ent_j0[FT_PREF];           // its first target
     unsigned char ent_sz[FT_PREF]; // and its size (prefetched once per block)
 };
+
+// Partial rows of the gradient sweep: FP32 in the hybrid mode (inside
+// FTSmem), FP64 in the FP64 mode (appended after FTSmem in dynamic shared
+// memory, so that the FP64 gradient keeps its precision through the sum of
+// the warps' rows).
+template <bool FP32B> struct PRow { using T = double; };
+template <> struct PRow<true> { using T = float; };
+__host__ __device__ constexpr size_t ft_rows64_bytes(int cap) { return sizeof(double) * FT_WARPS * cap; }
+
+template <bool FP32B, class SM>
+__device__ __forceinline__ typename PRow<FP32B>::T *partial_rows(SM &sm)
+{
+    if constexpr (FP32B) return &sm.pvw[0][0];
+    else return reinterpret_cast<double *>(reinterpret_cast<unsigned char *>(&sm) + sizeof(SM));
+}
 
 // ---------------------------------------------------------------------------
 // block-pair lists
@@ -229,13 +262,13 @@ k_inv_scatter(int nsb, const int64_t *__restrict__ fwd_off, const int *__restric
 // Otherwise, up to INV_TILE entries: bitonic sort of (b, entry); longer
 // segments: the rank of each entry = the number of entries with a smaller b,
 // counted against INV_TILE-entry tiles.  Every way, inv_b[off + rank] = b
-// (ascending b, the order the gradient gather sums in) and
-// inv2fwd[off + rank] = k, the forward position of the same pair.
+// (ascending b, the order the gradient reduction sums in) and
+// fwd2inv[k] = off + rank.
 constexpr int INV_TILE = 2048;
 constexpr int INV_PER = INV_TILE / 256;
 __global__ void __launch_bounds__(256)
 k_inv_order(int nsb, const int64_t *__restrict__ inv_off, const int *__restrict__ tmp_b,
-            const int64_t *__restrict__ tmp_k, int *__restrict__ inv_b, int64_t *__restrict__ inv2fwd)
+            const int64_t *__restrict__ tmp_k, int *__restrict__ inv_b, int64_t *__restrict__ fwd2inv)
 {
     __shared__ int sb[INV_TILE];
     __shared__ short si[INV_TILE];
@@ -281,7 +314,7 @@ k_inv_order(int nsb, const int64_t *__restrict__ inv_off, const int *__restrict_
             const int b = tmp_b[off + i];
             const int r = pre[b >> 5] + __popc(bm[b >> 5] & ((1u << (b & 31)) - 1u));
             inv_b[off + r] = b;
-            inv2fwd[off + r] = tmp_k[off + i];
+            fwd2inv[tmp_k[off + i]] = off + r;
         }
         return;
     }
@@ -313,7 +346,7 @@ k_inv_order(int nsb, const int64_t *__restrict__ inv_off, const int *__restrict_
         }
         for (int i = tid; i < L; i += 256) {
             inv_b[off + i] = sb[i];
-            inv2fwd[off + i] = tmp_k[off + si[i]];
+            fwd2inv[tmp_k[off + si[i]]] = off + i;
         }
         return;
     }
@@ -341,7 +374,7 @@ k_inv_order(int nsb, const int64_t *__restrict__ inv_off, const int *__restrict_
             const int64_t i = i0 + tid + 256 * u;
             if (i < L) {
                 inv_b[off + rank[u]] = mine[u];
-                inv2fwd[off + rank[u]] = tmp_k[off + i];
+                fwd2inv[tmp_k[off + i]] = off + rank[u];
             }
         }
     }
@@ -386,7 +419,7 @@ __global__ void __launch_bounds__(1024) k_scan(const int64_t *__restrict__ cnt, 
 }
 
 // ---------------------------------------------------------------------------
-// value sweep (CTA <-> source block)
+// fused value + gradient sweeps
 // ---------------------------------------------------------------------------
 
 // Stage the targets of the forward pairs [k0, k1) of block b, culled per
@@ -394,11 +427,9 @@ __global__ void __launch_bounds__(1024) k_scan(const int64_t *__restrict__ cnt, 
 // target), counts its survivors with a ballot, and whole target blocks are
 // accepted in list order while the staged total fits FT_MAXS.  Returns the
 // number of forward entries consumed; staged order = (target block, slot).
-// Per accepted entry e of the chunk: ebal[e] = its surviving lanes, epos[e] =
-// the staged position of the first survivor.
-template <int DIM>
-__device__ int stage_chunk(FTSmem &sm, const FusedArgs &f, int64_t kb, int64_t k0, int64_t k1, const double *bc,
-                           double rcull2)
+template <int DIM, class SM>
+__device__ int stage_chunk(SM &sm, const FusedArgs &f, int64_t kb, int64_t k0, int64_t k1, const double *bc,
+                           double rcull2, bool for_b)
 {
     constexpr int SUB = 4;                       // target blocks per warp per iteration
     constexpr int PER = FT_WARPS * SUB;          // entries examined per iteration
@@ -407,25 +438,29 @@ __device__ int stage_chunk(FTSmem &sm, const FusedArgs &f, int64_t kb, int64_t k
     int64_t k = k0;
     while (k < k1 && nb < FT_MAXT) {
         unsigned bal[SUB];
+        int tt[SUB];
         int64_t jj[SUB];
 #pragma unroll
         for (int s = 0; s < SUB; ++s) {
             const int idx = s * FT_WARPS + wp;
             const int64_t e = k + idx;
             bal[s] = 0u;
+            tt[s] = -1;
             jj[s] = 0;
             int cntv = -1;
             if (e < k1 && nb + idx < FT_MAXT) {
-                int sz;
+                int t, sz;
                 int64_t j0;
                 if (e - kb < FT_PREF) {
+                    t = sm.ent_t[e - kb];
                     j0 = sm.ent_j0[e - kb];
                     sz = sm.ent_sz[e - kb];
                 } else {
-                    const int t = f.fwd_t[e];
+                    t = f.fwd_t[e];
                     j0 = f.tblk_off[t];
                     sz = (int)(f.tblk_off[t + 1] - j0);
                 }
+                tt[s] = t;
                 jj[s] = j0;
                 bool keep = false;
                 if (lane < sz) {
@@ -455,7 +490,7 @@ __device__ int stage_chunk(FTSmem &sm, const FusedArgs &f, int64_t kb, int64_t k
                 if (lane >= o) incl += v;
             }
             const int excl = incl - (cv < 0 ? 0 : cv);
-            const unsigned bad = __ballot_sync(0xffffffffu, cv < 0 || total + incl > FT_MAXS);
+            const unsigned bad = __ballot_sync(0xffffffffu, cv < 0 || total + incl > SM::MAXS);
             const int na = bad ? __ffs(bad) - 1 : 32;
             sm.epre[lane] = total + excl;
             const int accsum = __shfl_sync(0xffffffffu, incl, na > 0 ? na - 1 : 0);
@@ -471,16 +506,23 @@ __device__ int stage_chunk(FTSmem &sm, const FusedArgs &f, int64_t kb, int64_t k
         for (int s = 0; s < SUB; ++s) {
             const int idx = s * FT_WARPS + wp;
             if (idx < nacc) {
+                const int slot = nb + idx;
                 const int64_t j0 = jj[s];
-                if ((bal[s] >> lane) & 1u) {
-                    const int pos = sm.epre[idx] + __popc(bal[s] & ((1u << lane) - 1u));
+                const bool keep = (bal[s] >> lane) & 1u;
+                short pos = -1;
+                if (keep) {
+                    pos = (short)(sm.epre[idx] + __popc(bal[s] & ((1u << lane) - 1u)));
                     const double *tp = f.tpk + (j0 + lane) * TPACK;
 #pragma unroll
                     for (int d = 0; d < FT_TS; ++d) sm.stg[d][pos] = tp[d];
                 }
+                sm.smap[slot][lane] = pos;
                 if (lane == 0) {
-                    sm.ebal[nb + idx] = bal[s];
-                    sm.epos[nb + idx] = (short)sm.epre[idx];
+                    const int tb = tt[s];
+                    sm.ctb[slot] = tb;
+                    const int64_t ip = f.fwd2inv[k + idx];
+                    sm.cpos[slot] = (for_b && ip >= 0 && tb >= f.tlo && tb < f.thi) ? (ip - f.part_base) * TBLK_KD
+                                                                                    : (int64_t)-1;
                 }
             }
         }
@@ -496,8 +538,8 @@ __device__ int stage_chunk(FTSmem &sm, const FusedArgs &f, int64_t kb, int64_t k
 }
 
 // Exact squared distance from a staged target (SoA) to a cell centre.
-template <int DIM>
-__device__ __forceinline__ double stg_dist2(const FTSmem &sm, int t, const double *c)
+template <int DIM, class SM>
+__device__ __forceinline__ double stg_dist2(const SM &sm, int t, const double *c)
 {
     const double y[3] = {sm.stg[0][t], sm.stg[1][t], DIM == 3 ? sm.stg[2][t] : 0.0};
     return dist2_exact<DIM>(y, c);
@@ -509,8 +551,8 @@ __device__ __forceinline__ double stg_dist2(const FTSmem &sm, int t, const doubl
 //         (when the bound could sit more than 2^500 above the true maximum).
 // NQ: quadrature points handled (== QL for full units: straight-line code
 //     whose NQ exponential chains interleave).
-template <int DIM, int QL, int NQ, int MODE>
-__device__ __forceinline__ void value_pairs(const FTSmem &sm, int wp, int lane, int ncand, int qoff, double cc0,
+template <int DIM, int QL, int NQ, int MODE, class SM>
+__device__ __forceinline__ void value_pairs(const SM &sm, int wp, int lane, int ncand, int qoff, double cc0,
                                             double cc1, double cc2, const EvalArgs &a, double Munit, double *M,
                                             double *S, double *mx)
 {
@@ -539,8 +581,8 @@ __device__ __forceinline__ void value_pairs(const FTSmem &sm, int wp, int lane, 
 }
 
 // Units with fewer than QL quadrature points (the last q-group of a cell).
-template <int DIM, int QL, int MODE>
-__device__ __noinline__ void value_pairs_partial(const FTSmem &sm, int wp, int lane, int ncand, int qoff, int nql,
+template <int DIM, int QL, int MODE, class SM>
+__device__ __noinline__ void value_pairs_partial(const SM &sm, int wp, int lane, int ncand, int qoff, int nql,
                                                  double cc0, double cc1, double cc2, const EvalArgs &a, double Munit,
                                                  double *M, double *S, double *mx)
 {
@@ -571,11 +613,10 @@ __device__ __noinline__ void value_pairs_partial(const FTSmem &sm, int wp, int l
 }
 
 // Exact candidate test of the staged targets for the warp's cell, in-order
-// compaction into sm.cand[wp] and the candidate bits by staged position into
-// sm.cbits[wp]; returns the count and (through bmax) the largest
-// B0_Kj = kappa (psi_j - d2/2)/eps over the candidates.
-template <int DIM>
-__device__ __forceinline__ int compact_candidates(FTSmem &sm, int wp, int lane, int nstg, const double *cc,
+// compaction into sm.cand[wp]; returns the count and (through bmax) the
+// largest B0_Kj = kappa (psi_j - d2/2)/eps over the candidates.
+template <int DIM, class SM>
+__device__ __forceinline__ int compact_candidates(SM &sm, int wp, int lane, int nstg, const double *cc,
                                                   const EvalArgs &a, double &bmax)
 {
     constexpr int U = 4;  // staged targets per lane in flight (independent distance chains)
@@ -597,7 +638,6 @@ __device__ __forceinline__ int compact_candidates(FTSmem &sm, int wp, int lane, 
         for (int u = 0; u < U; ++u) {
             const unsigned bal = __ballot_sync(0xffffffffu, in[u]);
             if (in[u]) sm.cand[wp][ncand + __popc(bal & ((1u << lane) - 1u))] = (unsigned short)(b0 + 32 * u + lane);
-            if (lane == 0 && b0 + 32 * u < nstg) sm.cbits[wp][(b0 >> 5) + u] = bal;
             ncand += __popc(bal);
         }
     }
@@ -606,21 +646,73 @@ __device__ __forceinline__ int compact_candidates(FTSmem &sm, int wp, int lane, 
     return ncand;
 }
 
-// Candidate masks of the chunk's entries for the warp's cell: bit l of
-// cmask[(k + e) * FT_WARPS + cell] is set iff target l of the entry's target
-// block is a candidate of the cell (staged, and passed the exact test).
-__device__ __forceinline__ void write_masks(const FTSmem &sm, const FusedArgs &f, int wp, int lane, int cl,
-                                            int64_t k, int nt)
+// Gradient sweep of one unit over its compacted candidates: for each
+// candidate target j (lane-strided) the unit's part of sum_q w_q nu_j
+// e^{t_qj - L_q}, written to the warp's partial row (FP32).  E0 and G' are
+// formed in FP64 per (cell, target) so that every FP32 operand is small.
+template <int DIM, bool FP32B, class SM>
+__device__ __forceinline__ void grad_pairs(SM &sm, const FusedArgs &f, int wp, int lane, int ncand, int qoff,
+                                           int nql, const double *cc, double Lref, int64_t qblk0, const EvalArgs &a)
 {
-    for (int e = 0; e < nt; ++e) {
-        const unsigned eb = sm.ebal[e];
-        bool c = false;
-        if ((eb >> lane) & 1u) {
-            const int pos = sm.epos[e] + __popc(eb & ((1u << lane) - 1u));
-            c = (sm.cbits[wp][pos >> 5] >> (pos & 31)) & 1u;
+    const float sf = (float)(a.s * (1.0 / 16.0));
+    for (int p = lane; p < ncand; p += 32) {
+        const int ti = sm.cand[wp][p];
+        const double g0 = sm.stg[0][ti] - cc[0], g1 = sm.stg[1][ti] - cc[1];
+        const double g2 = DIM == 3 ? sm.stg[2][ti] - cc[2] : 0.0;
+        const double d2 = DIM == 3 ? g0 * g0 + g1 * g1 + g2 * g2 : g0 * g0 + g1 * g1;
+        double val;
+        if (FP32B) {
+            const float e0 = (float)(sm.stg[4][ti] + (fma(-a.halfs, d2, sm.stg[5][ti]) - KAPPA * Lref) * (1.0 / 16.0));
+            const float G0 = sf * (float)g0, G1 = sf * (float)g1, G2 = sf * (float)g2;
+            float acc0 = 0.f, acc1 = 0.f;
+            if (f.w_nonneg) {
+                int q = 0;
+                for (; q + 1 < nql; q += 2) {
+                    const float4 v0 = *reinterpret_cast<const float4 *>(sm.qb[qoff + q]);
+                    const float4 v1 = *reinterpret_cast<const float4 *>(sm.qb[qoff + q + 1]);
+                    float ea = fmaf(G0, v0.x, e0 + v0.w), eb = fmaf(G0, v1.x, e0 + v1.w);
+                    ea = fmaf(G1, v0.y, ea);
+                    eb = fmaf(G1, v1.y, eb);
+                    if (DIM == 3) {
+                        ea = fmaf(G2, v0.z, ea);
+                        eb = fmaf(G2, v1.z, eb);
+                    }
+                    acc0 += ex2_approx(ea);
+                    acc1 += ex2_approx(eb);
+                }
+                if (q < nql) {
+                    const float4 v0 = *reinterpret_cast<const float4 *>(sm.qb[qoff + q]);
+                    float ea = fmaf(G0, v0.x, e0 + v0.w);
+                    ea = fmaf(G1, v0.y, ea);
+                    if (DIM == 3) ea = fmaf(G2, v0.z, ea);
+                    acc0 += ex2_approx(ea);
+                }
+            } else {
+                for (int q = 0; q < nql; ++q) {
+                    const float *qb = sm.qb[qoff + q];
+                    float e = fmaf(G0, qb[0], e0 + qb[3]);
+                    e = fmaf(G1, qb[1], e);
+                    if (DIM == 3) e = fmaf(G2, qb[2], e);
+                    acc0 = fmaf(sm.qw[qoff + q], ex2_approx(e), acc0);
+                }
+            }
+            val = (double)(acc0 + acc1);
+        } else {
+            const double U0 = 16.0 * sm.stg[4][ti] + fma(-a.halfs, d2, sm.stg[5][ti]) - KAPPA * Lref;
+            const double G0 = a.s * g0, G1 = a.s * g1, G2 = a.s * g2;
+            double acc = 0.0;
+            for (int q = 0; q < nql; ++q) {
+                const double *dq = sm.qd[qoff + q];
+                const double L = sm.qL[qoff + q];
+                if (!isfinite(L)) continue;
+                double u = fma(G0, dq[0], U0 + dq[3] - KAPPA * (L - Lref));
+                u = fma(G1, dq[1], u);
+                if (DIM == 3) u = fma(G2, dq[2], u);
+                acc = fma(f.w[qblk0 + qoff + q], exp2_16(u, sm.tab), acc);
+            }
+            val = acc;
         }
-        const unsigned m = __ballot_sync(0xffffffffu, c);
-        if (lane == 0) f.cmask[(k + e) * FT_WARPS + cl] = m;
+        partial_rows<FP32B>(sm)[wp * SM::MAXS + ti] = (typename PRow<FP32B>::T)val;
     }
 }
 
@@ -630,7 +722,7 @@ __device__ __forceinline__ void write_masks(const FTSmem &sm, const FusedArgs &f
 // candidate costs 1 + DIM exponentials and DIM reciprocals for its TM^DIM
 // points.  Sums stay relative to Munit (LSE mode only).
 template <int TM, int D>
-__host__ __device__ __forceinline__ constexpr int tstride()
+__device__ __forceinline__ constexpr int tstride()
 {
     return D == 0 ? 1 : (D == 1 ? TM : TM * TM);
 }
@@ -640,8 +732,8 @@ __host__ __device__ __forceinline__ constexpr int tstride()
 // candidates that can attain it: b_qj lies within s r |delta|max of B0_Kj, so
 // a candidate with B0 below (running max B0) - 2 s r |delta|max is never a
 // maximum; thr is that bound relative to Munit.
-template <int DIM, int TM, bool TS>
-__device__ __forceinline__ void value_pairs_tensor(const FTSmem &sm, int wp, int lane, int ncand, int qoff,
+template <int DIM, int TM, bool TS, class SM>
+__device__ __forceinline__ void value_pairs_tensor(const SM &sm, int wp, int lane, int ncand, int qoff,
                                                    const double *cc, const EvalArgs &a, double Munit, double thr,
                                                    double *S, double *mx)
 {
@@ -714,16 +806,109 @@ __device__ __forceinline__ void value_pairs_tensor(const FTSmem &sm, int wp, int
     }
 }
 
-// Value sweep: per source block, stage its paired targets chunk by chunk,
-// find each cell's candidates exactly (and record them as masks per block
-// pair for the gradient gather), accumulate the per-point online
-// log-sum-exp, and finish each point (L_q, value, C_global, skipped).
-template <int DIM, int QL, int MODE, int TQ, bool TS>
-__global__ void __launch_bounds__(FT_WARPS * 32, value_min_blocks(DIM, TQ))
-k_value_trunc(FusedArgs f, EvalArgs a)
+__device__ __forceinline__ float rcp_approx(float x)
+{
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// FP32 gradient sweep on tensor-product points: per candidate
+// 2^(e0) sum_q W_q prod_d F_d[i_d], W_q = w_q 2^(D_q), summed dimension by
+// dimension (Horner order), into the warp's partial row.
+template <int DIM, int TM, bool TS, class SM>
+__device__ __forceinline__ void grad_pairs_tensor(SM &sm, int wp, int lane, int ncand, int qoff,
+                                                  const double *cc, double Lref, const EvalArgs &a)
+{
+    constexpr int NQ = DIM == 3 ? TM * TM * TM : TM * TM;
+    const float sf = (float)(a.s * (1.0 / 16.0));
+    float ah[3];
+    ah[0] = (float)sm.qd[qoff + (TM - 1) * tstride<TM, 0>()][0];
+    ah[1] = (float)sm.qd[qoff + (TM - 1) * tstride<TM, 1>()][1];
+    ah[2] = DIM == 3 ? (float)sm.qd[qoff + (TM - 1) * tstride<TM, 2>()][2] : 0.f;
+    float W[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) W[q] = sm.qtw[qoff + q];
+    for (int p = lane; p < ncand; p += 32) {
+        const int ti = sm.cand[wp][p];
+        const double g0 = sm.stg[0][ti] - cc[0], g1 = sm.stg[1][ti] - cc[1];
+        const double g2 = DIM == 3 ? sm.stg[2][ti] - cc[2] : 0.0;
+        const double d2 = DIM == 3 ? g0 * g0 + g1 * g1 + g2 * g2 : g0 * g0 + g1 * g1;
+        float e0 = (float)(sm.stg[4][ti] + (fma(-a.halfs, d2, sm.stg[5][ti]) - KAPPA * Lref) * (1.0 / 16.0));
+        const float gd[3] = {(float)g0, (float)g1, (float)g2};
+        float F[3][TM];
+        if constexpr (TS) {
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                const float ga = sf * gd[d] * ah[d];
+                e0 -= ga;
+                const float r = ex2_approx(TM == 2 ? 2.f * ga : ga);
+                F[d][0] = 1.f;
+                F[d][1] = r;
+                if (TM == 3) F[d][2] = r * r;
+            }
+        } else {
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                const float xp = ex2_approx(sf * gd[d] * ah[d]);
+                F[d][0] = rcp_approx(xp);
+                F[d][TM - 1] = xp;
+                if (TM == 3) F[d][1] = 1.f;
+            }
+        }
+        float w = 0.f;
+        if (DIM == 2) {
+#pragma unroll
+            for (int i0 = 0; i0 < TM; ++i0) {
+                float u = 0.f;
+#pragma unroll
+                for (int i1 = 0; i1 < TM; ++i1) u = fmaf(W[i0 + TM * i1], F[1][i1], u);
+                w = fmaf(u, F[0][i0], w);
+            }
+        } else {
+#pragma unroll
+            for (int i0 = 0; i0 < TM; ++i0) {
+                float u = 0.f;
+#pragma unroll
+                for (int i1 = 0; i1 < TM; ++i1) {
+                    float v = 0.f;
+#pragma unroll
+                    for (int i2 = 0; i2 < TM; ++i2) v = fmaf(W[i0 + TM * i1 + TM * TM * i2], F[2][i2], v);
+                    u = fmaf(v, F[1][i1], u);
+                }
+                w = fmaf(u, F[0][i0], w);
+            }
+        }
+        partial_rows<true>(sm)[wp * SM::MAXS + ti] = ex2_approx(e0) * w;
+    }
+}
+
+// CTA sum of the warp partial rows (warp order) and the write of every slot
+// of every pair of the chunk (zeros where a target was not staged).
+template <bool FP32B, class SM>
+__device__ __forceinline__ void write_partials(SM &sm, const FusedArgs &f, int nt, int nunit)
+{
+    const typename PRow<FP32B>::T *rows = partial_rows<FP32B>(sm);
+    const int tid = threadIdx.x;
+    for (int i = tid; i < nt * TBLK_KD; i += blockDim.x) {
+        const int ti = i / TBLK_KD, sl = i - ti * TBLK_KD;
+        const int64_t base = sm.cpos[ti];
+        if (base < 0) continue;
+        const short p = sm.smap[ti][sl];
+        double v = 0.0;
+        if (p >= 0)
+            for (int w = 0; w < nunit; ++w) v += (double)rows[w * SM::MAXS + p];
+        f.part[base + sl] = v;
+    }
+}
+
+template <int DIM, int QL, bool FP32B, int MODE, int TQ, bool TS>
+__global__ void __launch_bounds__(FT_WARPS * 32, fused_min_blocks(DIM, TQ, FP32B))
+k_fused(FusedArgs f, EvalArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    FTSmem &sm = *reinterpret_cast<FTSmem *>(smem_raw);
+    using SMem = FTSmem<fused_cap(DIM, TQ, FP32B)>;
+    SMem &sm = *reinterpret_cast<SMem *>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
     const int b = blockIdx.x;
     if (tid < 16) sm.tab[tid] = c_exp2_tab[tid];
@@ -733,7 +918,6 @@ k_value_trunc(FusedArgs f, EvalArgs a)
     const bool valid = wp < nunit;
     const int cl = valid ? wp / a.ngroups : 0;          // cell of this warp (block-local)
     const int grp = valid ? wp - cl * a.ngroups : 0;
-    const bool masks = valid && grp == 0;               // one warp per cell records the masks
     const int qoff = cl * a.qpc + grp * a.ql;           // block-local index of the unit's first q
     const int nql = valid ? min(a.ql, a.qpc - grp * a.ql) : 0;
     const int64_t qblk0 = cb0 * a.qpc;                  // first q of the block
@@ -750,6 +934,7 @@ k_value_trunc(FusedArgs f, EvalArgs a)
     for (int i = tid; i < (int)min((int64_t)FT_PREF, k1 - k0); i += blockDim.x) {
         const int t = f.fwd_t[k0 + i];
         const int64_t j0 = f.tblk_off[t];
+        sm.ent_t[i] = t;
         sm.ent_j0[i] = (int)j0;
         sm.ent_sz[i] = (unsigned char)(f.tblk_off[t + 1] - j0);
     }
@@ -768,497 +953,271 @@ k_value_trunc(FusedArgs f, EvalArgs a)
     }
     __syncthreads();
     const double cc[3] = {sm.cellc[cl][0], sm.cellc[cl][1], sm.cellc[cl][2]};
+    int tail_off = -1;  // first entry (minus k0) of the value sweep's last chunk, still staged for the gradient sweep
+    int tail_nt = 0;
+    int ncand_single = 0;
 
-    // Shift of the online sums.  MODE 0/1: Munit = max_j B0_Kj + s r
-    // max_q |delta_q| bounds every exponent of the unit from above (|G_Kj| <=
-    // s r for a candidate), so no per-pair rescale is needed; exponents are
-    // kept relative to Munit (mx too) and a chunk that raises the bound
-    // rescales S once.  MODE 2 keeps a per-q lazy shift M[q].
-    double M[MODE == 2 ? QL : 1], S[QL], mx[QL];
+    // ---------------- value sweep ----------------
+    if (f.do_a) {
+        // Shift of the online sums.  MODE 0/1: Munit = max_j B0_Kj + s r
+        // max_q |delta_q| bounds every exponent of the unit from above
+        // (|G_Kj| <= s r for a candidate), so no per-pair rescale is needed;
+        // exponents are kept relative to Munit (mx too) and a chunk that raises
+        // the bound rescales S once.  MODE 2 keeps a per-q lazy shift M[q].
+        double M[MODE == 2 ? QL : 1], S[QL], mx[QL];
 #pragma unroll
-    for (int k = 0; k < QL; ++k) { S[k] = 0.0; mx[k] = -CUDART_INF; }
+        for (int k = 0; k < QL; ++k) { S[k] = 0.0; mx[k] = -CUDART_INF; }
 #pragma unroll
-    for (int k = 0; k < (MODE == 2 ? QL : 1); ++k) M[k] = -CUDART_INF;
-    double Munit = -CUDART_INF;
-    double dqmax = 0.0;
-    for (int q = 0; q < nql; ++q) dqmax = fmax(dqmax, sm.qn[qoff + q]);
-    double npairs = 0.0;
-    double bmax_run = -CUDART_INF;  // largest B0 of the candidates so far
-    const double sr = a.s * a.cull;
-    for (int64_t k = k0; k < k1;) {
-        const int nt = stage_chunk<DIM>(sm, f, k0, k, k1, bc, rcull2);
+        for (int k = 0; k < (MODE == 2 ? QL : 1); ++k) M[k] = -CUDART_INF;
+        double Munit = -CUDART_INF;
+        double dqmax = 0.0;
+        for (int q = 0; q < nql; ++q) dqmax = fmax(dqmax, sm.qn[qoff + q]);
+        double npairs = 0.0;
+        double bmax_run = -CUDART_INF;  // largest B0 of the candidates so far
+        const double sr = a.s * a.cull;
+        for (int64_t k = k0; k < k1;) {
+            const int nt = stage_chunk<DIM>(sm, f, k0, k, k1, bc, rcull2, f.do_b != 0);
+            const int nstg = sm.nstg;
+            if (valid) {
+                double bmax;
+                const int ncand = compact_candidates<DIM>(sm, wp, lane, nstg, cc, a, bmax);
+                ncand_single = ncand;
+                npairs += (double)ncand * nql;
+                if (MODE != 2 && bmax > -CUDART_INF) {
+                    const double mnew = bmax + sr * dqmax;
+                    if (mnew > Munit) {
+                        if (Munit > -CUDART_INF) {
+                            const double sc = exp2_16(Munit - mnew, sm.tab);
+#pragma unroll
+                            for (int q = 0; q < QL; ++q) {
+                                S[q] *= sc;
+                                mx[q] += Munit - mnew;
+                            }
+                        }
+                        Munit = mnew;
+                    }
+                }
+                if (bmax > bmax_run) bmax_run = bmax;
+                if constexpr (TQ > 0)
+                    value_pairs_tensor<DIM, TQ, TS>(sm, wp, lane, ncand, qoff, cc, a, Munit,
+                                                bmax_run - 2.0 * sr * dqmax - Munit, S, mx);
+                else if (nql == QL)
+                    value_pairs<DIM, QL, QL, MODE>(sm, wp, lane, ncand, qoff, cc[0], cc[1], cc[2], a, Munit, M, S, mx);
+                else
+                    value_pairs_partial<DIM, QL, MODE>(sm, wp, lane, ncand, qoff, nql, cc[0], cc[1], cc[2], a, Munit,
+                                                       M, S, mx);
+            }
+            k += nt;
+            if (k >= k1) {
+                tail_off = (int)(k - nt - k0);  // kept staged (with each warp's candidates) for the gradient sweep
+                tail_nt = nt;
+            } else {
+                __syncthreads();  // the next chunk overwrites the staged targets
+            }
+        }
+        // merge the lanes of each q (warp max / sum); lane q keeps q's totals
+        // and runs q's epilogue, so the QL epilogues proceed in parallel
+        double my_mx = -CUDART_INF, my_S = 0.0;
+#pragma unroll
+        for (int q = 0; q < QL; ++q) {
+            const double mxw = warp_max(mx[q]);
+            // shift of this lane's sum: Munit (exponents relative to it: 0) or the lazy M[q]
+            const double Ml = MODE == 2 ? M[MODE == 2 ? q : 0] : (Munit > -CUDART_INF ? 0.0 : -CUDART_INF);
+            const double sl = (Ml == -CUDART_INF || mxw == -CUDART_INF) ? 0.0 : S[q] * exp2_16(Ml - mxw, sm.tab);
+            const double Sw = warp_sum(sl);
+            if (lane == q) {
+                my_mx = mxw;
+                my_S = Sw;
+            }
+        }
+        double tv = 0.0, tcv = 0.0, tsk = 0.0;
+        if (valid && lane < nql) {
+            const int qi = qoff + lane;
+            const int64_t qg = qblk0 + qi;
+            double v, cv, L;
+            int sk;
+            value_epilogue(a, MODE == 2 ? my_mx : my_mx + Munit, my_S, sm.qd[qi][3], f.rho[qg], f.jxw[qg], v, cv, L,
+                           sk);
+            f.Lq[qg] = L;
+            sm.qL[qi] = L;
+            tv = v;
+            tcv = cv;
+            tsk = sk;
+        }
+        block_partials(tv, tcv, tsk, lane == 0 ? npairs : 0.0, f.valpart);  // contains __syncthreads
+    } else {
+        for (int i = tid; i < nqb; i += blockDim.x) sm.qL[i] = f.Lq[qblk0 + i];
+        __syncthreads();
+    }
+    if (!f.do_b) return;
+
+    // ---------------- gradient sweep ----------------
+    // per-unit reference L_Kref = min L over the unit's q; per-q FP32 data
+    double Lref = CUDART_INF;
+    if (valid) {
+        double lv = lane < nql ? sm.qL[qoff + lane] : CUDART_INF;
+        Lref = -warp_max(-lv);
+        if (lane < nql) {
+            const int i = qoff + lane;
+            const double L = sm.qL[i];
+            const double D = (!isfinite(Lref) || !isfinite(L)) ? -CUDART_INF
+                                                                : (sm.qd[i][3] - KAPPA * (L - Lref)) * (1.0 / 16.0);
+            const double wq = f.w[qblk0 + i];
+            sm.qb[i][0] = (float)sm.qd[i][0];
+            sm.qb[i][1] = (float)sm.qd[i][1];
+            sm.qb[i][2] = (float)sm.qd[i][2];
+            sm.qb[i][3] = (float)(f.w_nonneg ? D + log2(wq) : D);  // w_q folded in: p = 2^e directly
+            sm.qw[i] = (float)wq;
+            if (TQ > 0) sm.qtw[i] = (float)(wq * exp2(D));
+        }
+        __syncwarp();
+    }
+    // The value sweep's last chunk (the only one when everything fit) is still
+    // staged with each warp's candidates: its gradient comes first, then the
+    // earlier chunks are staged again (the same chunks: the greedy rule over
+    // [k0, k0 + tail_off) ends where the value sweep's did).  Every pair's partial
+    // is written once, so the order of the chunks does not change any sum.
+    int64_t kend = k1;
+    if (tail_off >= 0) {
+        const int nt = tail_nt;
+        const int nstg = sm.nstg;
+        if (valid) {
+            for (int t = lane; t < nstg; t += 32) partial_rows<FP32B>(sm)[wp * SMem::MAXS + t] = 0;
+            __syncwarp();
+            if (isfinite(Lref)) {
+                if constexpr (TQ > 0 && FP32B) grad_pairs_tensor<DIM, TQ, TS>(sm, wp, lane, ncand_single, qoff, cc, Lref, a);
+                else grad_pairs<DIM, FP32B>(sm, f, wp, lane, ncand_single, qoff, nql, cc, Lref, qblk0, a);
+            }
+        }
+        if (tid < nt) {
+            const int tb = sm.ctb[tid];
+            const int64_t ip = f.fwd2inv[k0 + tail_off + tid];
+            sm.cpos[tid] = (ip >= 0 && tb >= f.tlo && tb < f.thi) ? (ip - f.part_base) * TBLK_KD : (int64_t)-1;
+        }
+        __syncthreads();
+        write_partials<FP32B>(sm, f, nt, nunit);
+        if (tail_off == 0) return;
+        kend = k0 + tail_off;
+        __syncthreads();  // the earlier chunks overwrite the staged targets
+    }
+    for (int64_t k = k0; k < kend;) {
+        const int nt = stage_chunk<DIM>(sm, f, k0, k, kend, bc, rcull2, true);
         const int nstg = sm.nstg;
         if (valid) {
             double bmax;
             const int ncand = compact_candidates<DIM>(sm, wp, lane, nstg, cc, a, bmax);
-            if (masks) write_masks(sm, f, wp, lane, cl, k, nt);
-            npairs += (double)ncand * nql;
-            if (MODE != 2 && bmax > -CUDART_INF) {
-                const double mnew = bmax + sr * dqmax;
-                if (mnew > Munit) {
-                    if (Munit > -CUDART_INF) {
-                        const double sc = exp2_16(Munit - mnew, sm.tab);
-#pragma unroll
-                        for (int q = 0; q < QL; ++q) {
-                            S[q] *= sc;
-                            mx[q] += Munit - mnew;
-                        }
-                    }
-                    Munit = mnew;
-                }
+            for (int t = lane; t < nstg; t += 32) partial_rows<FP32B>(sm)[wp * SMem::MAXS + t] = 0;
+            __syncwarp();
+            if (isfinite(Lref)) {
+                if constexpr (TQ > 0 && FP32B) grad_pairs_tensor<DIM, TQ, TS>(sm, wp, lane, ncand, qoff, cc, Lref, a);
+                else grad_pairs<DIM, FP32B>(sm, f, wp, lane, ncand, qoff, nql, cc, Lref, qblk0, a);
             }
-            if (bmax > bmax_run) bmax_run = bmax;
-            if constexpr (TQ > 0)
-                value_pairs_tensor<DIM, TQ, TS>(sm, wp, lane, ncand, qoff, cc, a, Munit,
-                                                bmax_run - 2.0 * sr * dqmax - Munit, S, mx);
-            else if (nql == QL)
-                value_pairs<DIM, QL, QL, MODE>(sm, wp, lane, ncand, qoff, cc[0], cc[1], cc[2], a, Munit, M, S, mx);
-            else
-                value_pairs_partial<DIM, QL, MODE>(sm, wp, lane, ncand, qoff, nql, cc[0], cc[1], cc[2], a, Munit, M,
-                                                   S, mx);
         }
+        __syncthreads();
+        write_partials<FP32B>(sm, f, nt, nunit);
         k += nt;
-        __syncthreads();  // the next chunk overwrites the staged targets
+        __syncthreads();
     }
-    // merge the lanes of each q (warp max / sum); lane q keeps q's totals
-    // and runs q's epilogue, so the QL epilogues proceed in parallel
-    double my_mx = -CUDART_INF, my_S = 0.0;
-#pragma unroll
-    for (int q = 0; q < QL; ++q) {
-        const double mxw = warp_max(mx[q]);
-        // shift of this lane's sum: Munit (exponents relative to it: 0) or the lazy M[q]
-        const double Ml = MODE == 2 ? M[MODE == 2 ? q : 0] : (Munit > -CUDART_INF ? 0.0 : -CUDART_INF);
-        const double sl = (Ml == -CUDART_INF || mxw == -CUDART_INF) ? 0.0 : S[q] * exp2_16(Ml - mxw, sm.tab);
-        const double Sw = warp_sum(sl);
-        if (lane == q) {
-            my_mx = mxw;
-            my_S = Sw;
-        }
-    }
-    double tv = 0.0, tcv = 0.0, tsk = 0.0;
-    if (valid && lane < nql) {
-        const int qi = qoff + lane;
-        const int64_t qg = qblk0 + qi;
-        double v, cv, L;
-        int sk;
-        value_epilogue(a, MODE == 2 ? my_mx : my_mx + Munit, my_S, sm.qd[qi][3], f.rho[qg], f.jxw[qg], v, cv, L, sk);
-        f.Lq[qg] = L;
-        tv = v;
-        tcv = cv;
-        tsk = sk;
-    }
-    block_partials(tv, tcv, tsk, lane == 0 ? npairs : 0.0, f.valpart);
 }
 
-// ---------------------------------------------------------------------------
-// gradient gather (CTA <-> target block)
-// ---------------------------------------------------------------------------
-
-// Per-cell (and per-point) data of the gradient from the value sweep's L_q.
-// Each cell's reference L_K = min over its points of L_q keeps every FP32
-// operand small: with delta_q = x_q - c_K and C'_q = -kappa |delta_q|^2/(2 eps),
-//   w_q nu_j e^(t_qj - L_q) = 2^(e0_Kj + G'_Kj.delta_q + D_q) w_q,
-//   e0_Kj = log2 nu_j + (kappa (psi_j - |y_j - c_K|^2/2)/eps - kappa L_K)/16,
-//   G'_Kj = kappa (y_j - c_K)/(16 eps),  D_q = (C'_q - kappa (L_q - L_K))/16.
-//   gcell[K] = {c_K, L_K};
-//   FP32, tensor points: gten[16 K ..] = {a_0, a_1, a_2, -, W_q = w_q 2^D_q};
-//   FP32 otherwise: gq (float4) = {delta_q, D_q + log2 w_q (w >= 0) or D_q}, gqw = w_q;
-//   FP64: gq (double4) = {delta_q, C'_q - kappa (L_q - L_K)} (-inf for a
-//         skipped point), gqw = w_q.
-template <int DIM, int TM, bool FP32B>
+// gradient of target block t = sum of its pair partials in inverse order
+// (ascending source block), lane <-> target.  CTA <-> target block: warp w
+// sums rows w, w+8, ...; the 8 warp sums are added in warp order.
 __global__ void __launch_bounds__(256)
-k_grad_prep(int64_t ncells, int qpc, const double *__restrict__ x, const double *__restrict__ cell_ctr,
-            const double *__restrict__ Lq, const double *__restrict__ w, int w_nonneg, EvalArgs a,
-            double4 *__restrict__ gcell, float *__restrict__ gten, void *__restrict__ gq, void *__restrict__ gqw)
-{
-    const int64_t K = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (K >= ncells) return;
-    const double c[3] = {cell_ctr[K * DIM], cell_ctr[K * DIM + 1], DIM == 3 ? cell_ctr[K * DIM + 2] : 0.0};
-    const int64_t q0 = K * qpc;
-    double Lref = CUDART_INF;
-    for (int q = 0; q < qpc; ++q) Lref = fmin(Lref, Lq[q0 + q]);
-    gcell[K] = make_double4(c[0], c[1], c[2], Lref);
-    for (int q = 0; q < qpc; ++q) {
-        double dl[3], dsq = 0.0;
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            dl[d] = d < DIM ? x[(q0 + q) * DIM + d] - c[d] : 0.0;
-            dsq += dl[d] * dl[d];
-        }
-        const double Cq = -a.halfs * dsq;
-        const double L = Lq[q0 + q];
-        const bool fin = isfinite(Lref) && isfinite(L);
-        const double wq = w[q0 + q];
-        if (FP32B) {
-            const double D = fin ? (Cq - KAPPA * (L - Lref)) * (1.0 / 16.0) : -CUDART_INF;
-            if (TM > 0) {
-                gten[K * 16 + 4 + q] = (float)(wq * exp2(D));
-            } else {
-                reinterpret_cast<float4 *>(gq)[q0 + q] =
-                    make_float4((float)dl[0], (float)dl[1], (float)dl[2], (float)(w_nonneg ? D + log2(wq) : D));
-                reinterpret_cast<float *>(gqw)[q0 + q] = (float)wq;
-            }
-        } else {
-            reinterpret_cast<double4 *>(gq)[q0 + q] =
-                make_double4(dl[0], dl[1], dl[2], fin ? Cq - KAPPA * (L - Lref) : -CUDART_INF);
-            reinterpret_cast<double *>(gqw)[q0 + q] = wq;
-        }
-        if (TM > 0) {
-            // per-dimension offsets of the tensor grid: those of its last point along each axis
-#pragma unroll
-            for (int d = 0; d < DIM; ++d) {
-                const int qa = (TM - 1) * (d == 0 ? 1 : (d == 1 ? TM : TM * TM));
-                if (q == qa) gten[K * 16 + d] = (float)dl[d];
-            }
-        }
-    }
-}
-
-struct GatherArgs {
-    const double *tpk;            // per target (internal order): y(3), nu, log2 nu, s*psi
-    const int64_t *tblk_off, *inv_off, *inv2fwd;
-    const int *inv_b;
-    const int64_t *sblk_cell;
-    const unsigned *cmask;        // candidate masks per (forward pair, block-local cell)
-    const double4 *gcell;
-    const float *gten;
-    const void *gq, *gqw;
-    int qpc;
-    int w_nonneg;
-    double *gacc;                 // per target (internal order): sum_q w_q pi_qj
-};
-
-// One candidate (cell K, target j): sum over the cell's points of
-// w_q nu_j e^(t_qj - L_q), with the expansion of k_grad_prep.
-template <int DIM, int TM, bool TS, bool FP32B>
-__device__ __forceinline__ double grad_term(const GatherArgs &g, const EvalArgs &a, int64_t K, const double4 cd,
-                                            const double *y, double l2nu, double spsi, const double *tab)
-{
-    const double g0 = y[0] - cd.x, g1 = y[1] - cd.y, g2 = DIM == 3 ? y[2] - cd.z : 0.0;
-    const double d2 = DIM == 3 ? g0 * g0 + g1 * g1 + g2 * g2 : g0 * g0 + g1 * g1;
-    if constexpr (FP32B) {
-        float e0 = (float)(l2nu + (fma(-a.halfs, d2, spsi) - KAPPA * cd.w) * (1.0 / 16.0));
-        const float sf = (float)(a.s * (1.0 / 16.0));
-        const float G[3] = {sf * (float)g0, sf * (float)g1, sf * (float)g2};
-        if constexpr (TM > 0) {
-            constexpr int NQ = DIM == 3 ? TM * TM * TM : TM * TM;
-            const float *ct = g.gten + K * 16;
-            const float4 ah = *reinterpret_cast<const float4 *>(ct);
-            const float ahv[3] = {ah.x, ah.y, ah.z};
-            float W[NQ];
-#pragma unroll
-            for (int q = 0; q < NQ; ++q) W[q] = ct[4 + q];
-            float F[3][TM];
-            if constexpr (TS) {
-#pragma unroll
-                for (int d = 0; d < DIM; ++d) {
-                    const float ga = G[d] * ahv[d];
-                    e0 -= ga;
-                    const float r = ex2_approx(TM == 2 ? 2.f * ga : ga);
-                    F[d][0] = 1.f;
-                    F[d][1] = r;
-                    if (TM == 3) F[d][2] = r * r;
-                }
-            } else {
-#pragma unroll
-                for (int d = 0; d < DIM; ++d) {
-                    const float xp = ex2_approx(G[d] * ahv[d]);
-                    F[d][0] = __frcp_rn(xp);
-                    F[d][TM - 1] = xp;
-                    if (TM == 3) F[d][1] = 1.f;
-                }
-            }
-            float wsum = 0.f;
-            if (DIM == 2) {
-#pragma unroll
-                for (int i0 = 0; i0 < TM; ++i0) {
-                    float u = 0.f;
-#pragma unroll
-                    for (int i1 = 0; i1 < TM; ++i1) u = fmaf(W[i0 + TM * i1], F[1][i1], u);
-                    wsum = fmaf(u, F[0][i0], wsum);
-                }
-            } else {
-#pragma unroll
-                for (int i0 = 0; i0 < TM; ++i0) {
-                    float u = 0.f;
-#pragma unroll
-                    for (int i1 = 0; i1 < TM; ++i1) {
-                        float v = 0.f;
-#pragma unroll
-                        for (int i2 = 0; i2 < TM; ++i2) v = fmaf(W[i0 + TM * i1 + TM * TM * i2], F[2][i2], v);
-                        u = fmaf(v, F[1][i1], u);
-                    }
-                    wsum = fmaf(u, F[0][i0], wsum);
-                }
-            }
-            return (double)(ex2_approx(e0) * wsum);
-        } else {
-            const float4 *qb = reinterpret_cast<const float4 *>(g.gq) + K * g.qpc;
-            const float *qw = reinterpret_cast<const float *>(g.gqw) + K * g.qpc;
-            float acc0 = 0.f, acc1 = 0.f;
-            if (g.w_nonneg) {
-                int q = 0;
-                for (; q + 1 < g.qpc; q += 2) {
-                    const float4 v0 = qb[q], v1 = qb[q + 1];
-                    float ea = fmaf(G[0], v0.x, e0 + v0.w), eb = fmaf(G[0], v1.x, e0 + v1.w);
-                    ea = fmaf(G[1], v0.y, ea);
-                    eb = fmaf(G[1], v1.y, eb);
-                    if (DIM == 3) {
-                        ea = fmaf(G[2], v0.z, ea);
-                        eb = fmaf(G[2], v1.z, eb);
-                    }
-                    acc0 += ex2_approx(ea);
-                    acc1 += ex2_approx(eb);
-                }
-                if (q < g.qpc) {
-                    const float4 v0 = qb[q];
-                    float ea = fmaf(G[0], v0.x, e0 + v0.w);
-                    ea = fmaf(G[1], v0.y, ea);
-                    if (DIM == 3) ea = fmaf(G[2], v0.z, ea);
-                    acc0 += ex2_approx(ea);
-                }
-            } else {
-                for (int q = 0; q < g.qpc; ++q) {
-                    const float4 v = qb[q];
-                    float e = fmaf(G[0], v.x, e0 + v.w);
-                    e = fmaf(G[1], v.y, e);
-                    if (DIM == 3) e = fmaf(G[2], v.z, e);
-                    acc0 = fmaf(qw[q], ex2_approx(e), acc0);
-                }
-            }
-            return (double)(acc0 + acc1);
-        }
-    } else {
-        const double U0 = 16.0 * l2nu + fma(-a.halfs, d2, spsi) - KAPPA * cd.w;
-        const double G0 = a.s * g0, G1 = a.s * g1, G2 = a.s * g2;
-        const double4 *qd = reinterpret_cast<const double4 *>(g.gq) + K * g.qpc;
-        const double *qw = reinterpret_cast<const double *>(g.gqw) + K * g.qpc;
-        double acc = 0.0;
-        for (int q = 0; q < g.qpc; ++q) {
-            const double4 v = qd[q];
-            if (v.w == -CUDART_INF) continue;   // skipped point
-            double u = fma(G0, v.x, U0 + v.w);
-            u = fma(G1, v.y, u);
-            if (DIM == 3) u = fma(G2, v.z, u);
-            acc = fma(qw[q], exp2_16(u, tab), acc);
-        }
-        return acc;
-    }
-}
-
-// gacc[j] = sum over the candidates (K, j) of the cell's gradient term, for
-// the targets j of target block t (lane <-> target).  Warp w takes an equal
-// contiguous share of t's inverse list (ascending source block) and walks it
-// in batches of 32 block pairs: lane i loads pair i's source block, cells and
-// the value sweep's candidate masks of its cells (one 32-bit word per cell,
-// the bits of t's targets), so neither the exact test nor the staging is
-// repeated and the loads of a batch are issued together.  Scanning the
-// masks, each lane queues its own candidate cells (GQ deep, in shared
-// memory); a step computes one queued cell per lane, taken when every lane
-// has one (or a queue is full), so the lanes stay busy although a mask word
-// holds about a quarter of the block's targets.  Each lane adds its terms in
-// queue order, i.e. in (pair, cell) order; the 8 warp sums are added in warp
-// order: no atomics, the order is fixed.
-constexpr int GQ = 16;
-template <int DIM, int TM, bool TS, bool FP32B>
-__global__ void __launch_bounds__(256)
-k_grad_gather(GatherArgs g, EvalArgs a)
+k_grad_reduce(const int64_t *__restrict__ tblk_off, const int64_t *__restrict__ inv_off, int tlo, int thi,
+              int64_t part_base, const double *__restrict__ part, double *__restrict__ gacc)
 {
     __shared__ double ws[8][32];
-    __shared__ double tab[16];
-    __shared__ int queue[8][GQ][32];
-    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    if (tid < 16) tab[tid] = c_exp2_tab[tid];
-    __syncthreads();
-    const int t = blockIdx.x;
-    const int64_t j = g.tblk_off[t] + lane;
-    const bool have = j < g.tblk_off[t + 1];
-    double y[3] = {0.0, 0.0, 0.0}, l2nu = 0.0, spsi = 0.0;
-    if (have) {
-        const double *tp = g.tpk + j * TPACK;
-        y[0] = tp[0];
-        y[1] = tp[1];
-        y[2] = DIM == 3 ? tp[2] : 0.0;
-        l2nu = tp[4];
-        spsi = tp[5];
-    }
-    int *qw = &queue[w][0][0];
-    int head = 0, tail = 0;
+    const int t = tlo + blockIdx.x;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t p0 = inv_off[t], p1 = inv_off[t + 1];
     double acc = 0.0;
-    auto step = [&]() {
-        if (tail > head) {
-            const int K = qw[(head % GQ) * 32 + lane];
-            ++head;
-            const double4 cd = g.gcell[K];
-            if (cd.w < CUDART_INF) acc += grad_term<DIM, TM, TS, FP32B>(g, a, K, cd, y, l2nu, spsi, tab);
-        }
-    };
-    const int64_t q0 = g.inv_off[t], L = g.inv_off[t + 1] - q0;
-    const int64_t pa = q0 + (L * w) / 8, pb = q0 + (L * (w + 1)) / 8;
-    for (int64_t p0 = pa; p0 < pb; p0 += 32) {
-        const int64_t p = p0 + lane;
-        int K0 = 0, nc = 0;
-        uint4 m0 = make_uint4(0u, 0u, 0u, 0u), m1 = m0;
-        if (p < pb) {
-            const int b = g.inv_b[p];
-            const int64_t k = g.inv2fwd[p];
-            const int64_t c0 = g.sblk_cell[b];
-            K0 = (int)c0;
-            nc = (int)(g.sblk_cell[b + 1] - c0);
-            const uint4 *mk = reinterpret_cast<const uint4 *>(g.cmask + k * FT_WARPS);
-            m0 = mk[0];
-            if (nc > 4) m1 = mk[1];
-        }
-        const int np = (int)min((int64_t)32, pb - p0);
-        for (int i = 0; i < np; ++i) {
-            const int K0i = __shfl_sync(0xffffffffu, K0, i), nci = __shfl_sync(0xffffffffu, nc, i);
-            unsigned mw[8];
-            mw[0] = __shfl_sync(0xffffffffu, m0.x, i);
-            mw[1] = __shfl_sync(0xffffffffu, m0.y, i);
-            mw[2] = __shfl_sync(0xffffffffu, m0.z, i);
-            mw[3] = __shfl_sync(0xffffffffu, m0.w, i);
-            mw[4] = __shfl_sync(0xffffffffu, m1.x, i);
-            mw[5] = __shfl_sync(0xffffffffu, m1.y, i);
-            mw[6] = __shfl_sync(0xffffffffu, m1.z, i);
-            mw[7] = __shfl_sync(0xffffffffu, m1.w, i);
-#pragma unroll
-            for (int c = 0; c < FT_WARPS; ++c) {
-                if (c < nci && ((mw[c] >> lane) & 1u)) {
-                    qw[(tail % GQ) * 32 + lane] = K0i + c;
-                    ++tail;
-                }
-                if (__all_sync(0xffffffffu, tail > head) || __any_sync(0xffffffffu, tail - head == GQ)) step();
-            }
-        }
-    }
-    while (__any_sync(0xffffffffu, tail > head)) step();
+    for (int64_t p = p0 + w; p < p1; p += 8) acc += part[(p - part_base) * TBLK_KD + lane];
     ws[w][lane] = acc;
     __syncthreads();
-    if (w == 0 && have) {
+    if (w == 0) {
         double s = 0.0;
 #pragma unroll
         for (int i = 0; i < 8; ++i) s += ws[i][lane];
-        g.gacc[j] = s;
+        const int64_t j = tblk_off[t] + lane;
+        if (j < tblk_off[t + 1]) gacc[j] = s;
     }
 }
 
-// ---------------------------------------------------------------------------
-// dispatch
-// ---------------------------------------------------------------------------
-
-template <int DIM, int QL, int MODE, int TQ, bool TS>
-static void launch_value(sdot_ctx *c, const FusedArgs &f, const EvalArgs &a, int nb)
+template <int DIM, int QL, bool FP32B, int MODE, int TQ, bool TS>
+static void launch_fused(sdot_ctx *c, const FusedArgs &f, const EvalArgs &a, size_t smem, int nb)
 {
-    const size_t smem = sizeof(FTSmem);
-    cudaFuncSetAttribute(k_value_trunc<DIM, QL, MODE, TQ, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(k_value_trunc<DIM, QL, MODE, TQ, TS>, cudaFuncAttributePreferredSharedMemoryCarveout,
+    cudaFuncSetAttribute(k_fused<DIM, QL, FP32B, MODE, TQ, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_fused<DIM, QL, FP32B, MODE, TQ, TS>, cudaFuncAttributePreferredSharedMemoryCarveout,
                          (int)cudaSharedmemCarveoutMaxShared);
-    k_value_trunc<DIM, QL, MODE, TQ, TS><<<(unsigned)nb, FT_WARPS * 32, smem, c->stream>>>(f, a);
+    k_fused<DIM, QL, FP32B, MODE, TQ, TS><<<(unsigned)nb, FT_WARPS * 32, smem, c->stream>>>(f, a);
+}
+
+template <int DIM, int QL, int MODE, int TQ = 0, bool TS = false>
+static void dispatch_fused_b(sdot_ctx *c, const FusedArgs &f, const EvalArgs &a, bool fp32b, int nb)
+{
+    if (fp32b) launch_fused<DIM, QL, true, MODE, TQ, TS>(c, f, a, sizeof(FTSmem<fused_cap(DIM, TQ, true)>), nb);
+    else
+        launch_fused<DIM, QL, false, MODE, TQ, TS>(c, f, a, sizeof(FTSmem<fused_cap(DIM, TQ, false)>) + ft_rows64_bytes(fused_cap(DIM, TQ, false)),
+                                               nb);
 }
 
 template <int DIM, int MODE>
-static void dispatch_value_q(sdot_ctx *c, const FusedArgs &f, const EvalArgs &a, int nb)
+static void dispatch_fused_q(sdot_ctx *c, const FusedArgs &f, const EvalArgs &a, bool fp32b, int nb)
 {
     // 2D: units of 4 (order 2) or 9 (order 3 and groups of 9); 3D: 8 or 9.
     if constexpr (DIM == 2) {
-        if (a.ql <= 4) launch_value<DIM, 4, MODE, 0, false>(c, f, a, nb);
-        else launch_value<DIM, 9, MODE, 0, false>(c, f, a, nb);
+        if (a.ql <= 4) dispatch_fused_b<DIM, 4, MODE>(c, f, a, fp32b, nb);
+        else dispatch_fused_b<DIM, 9, MODE>(c, f, a, fp32b, nb);
     } else {
-        if (a.ql <= 8) launch_value<DIM, 8, MODE, 0, false>(c, f, a, nb);
-        else launch_value<DIM, 9, MODE, 0, false>(c, f, a, nb);
+        if (a.ql <= 8) dispatch_fused_b<DIM, 8, MODE>(c, f, a, fp32b, nb);
+        else dispatch_fused_b<DIM, 9, MODE>(c, f, a, fp32b, nb);
     }
 }
 
-// Variant of the sweeps for this evaluation.  The shift Munit may exceed the
-// true maximum exponent of a q by up to 2 s r |delta|max (units of
-// 2^(1/16)); beyond 2^500 the lazy form (MODE 2) is used.  Exponents u
-// relative to Munit satisfy u >= -s (psi_max - psi_min + r^2/2 + 2 r
-// |delta|max); when that is above -16000 the clamp of exp2 is provably
-// inactive and dropped (MODE 0).  Tensor-product points: per-dimension
-// factors 2^(+-G a/16) stay within 2^300 (FP64 value sweep) and 2^40 (FP32
-// gradient); within 2^8 the relative form (no reciprocals) applies (ts).
-struct SweepPlan {
-    int mode;   // 0, 1, 2
-    int tm;     // tensor points per dimension (0: not factored)
-    bool ts;
-};
-
-static SweepPlan plan_sweeps(const sdot_ctx *c, const EvalArgs &a, double psi_range)
+// MODE selection.  The shift Munit may exceed the true maximum exponent of a
+// q by up to 2 s r |delta|max (units of 2^(1/16)); beyond 2^500 the lazy form
+// is used.  Exponents u relative to Munit satisfy
+// u >= -s (psi_max - psi_min + r^2/2 + 2 r |delta|max); when that is above
+// -16000 the clamp of exp2 is provably inactive and dropped.
+template <int DIM>
+static void dispatch_fused(sdot_ctx *c, const FusedArgs &f, const EvalArgs &a, bool fp32b, int nb, double psi_range)
 {
-    SweepPlan p{0, 0, false};
     const double gap = 2.0 * a.s * a.cull * c->delta_max;
     const double umin = -a.s * (psi_range + 0.5 * a.cull * a.cull + 2.0 * a.cull * c->delta_max);
+    // tensor-product points: per-dimension factors 2^(+-G a/16) stay within
+    // 2^300 (FP64 value sweep) and 2^40 (FP32 gradient sweep)
     const double fac = a.s * a.cull * c->tensor_amax / 16.0;
+    const bool tensor = c->tensor_m > 0 && a.lse && a.ngroups == 1 && fac <= 40.0 && umin > -15000.0 &&
+                        gap < 16.0 * 500.0;
     if (gap >= 16.0 * 500.0) {
-        p.mode = 2;
-        return p;
-    }
-    p.mode = umin > -15000.0 ? 0 : 1;
-    const bool tensor = c->tensor_m > 0 && a.lse && a.ngroups == 1 && fac <= 40.0 && umin > -15000.0;
-    if (tensor && ((c->dim == 3 && c->tensor_m == 2 && a.ql == 8) ||
-                   (c->dim == 2 && ((c->tensor_m == 3 && a.ql == 9) || (c->tensor_m == 2 && a.ql == 4))))) {
-        p.mode = 0;
-        p.tm = c->tensor_m;
-        p.ts = fac <= 4.0;
-    }
-    return p;
-}
-
-template <int DIM>
-static void dispatch_value(sdot_ctx *c, const FusedArgs &f, const EvalArgs &a, int nb, const SweepPlan &p)
-{
-    if (p.tm > 0) {
-        if constexpr (DIM == 3) {
-            if (p.ts) launch_value<3, 8, 0, 2, true>(c, f, a, nb);
-            else launch_value<3, 8, 0, 2, false>(c, f, a, nb);
-        } else {
-            if (p.tm == 3) {
-                if (p.ts) launch_value<2, 9, 0, 3, true>(c, f, a, nb);
-                else launch_value<2, 9, 0, 3, false>(c, f, a, nb);
-            } else {
-                if (p.ts) launch_value<2, 4, 0, 2, true>(c, f, a, nb);
-                else launch_value<2, 4, 0, 2, false>(c, f, a, nb);
-            }
-        }
+        dispatch_fused_q<DIM, 2>(c, f, a, fp32b, nb);
         return;
     }
-    if (p.mode == 2) dispatch_value_q<DIM, 2>(c, f, a, nb);
-    else if (p.mode == 1) dispatch_value_q<DIM, 1>(c, f, a, nb);
-    else dispatch_value_q<DIM, 0>(c, f, a, nb);
-}
-
-template <int DIM, int TM, bool TS, bool FP32B>
-static void launch_gather(sdot_ctx *c, const GatherArgs &g, const EvalArgs &a, int ntb)
-{
-    const unsigned cg = (unsigned)((c->ncells + 255) / 256);
-    k_grad_prep<DIM, TM, FP32B><<<cg, 256, 0, c->stream>>>(c->ncells, c->qpc, c->x.p, c->cell_ctr.p, c->Lq.p, c->w.p,
-                                                           c->w_nonneg ? 1 : 0, a,
-                                                           reinterpret_cast<double4 *>(c->gcell.p), c->gten.p,
-                                                           c->gq.p, c->gqw.p);
-    k_grad_gather<DIM, TM, TS, FP32B><<<(unsigned)ntb, 256, 0, c->stream>>>(g, a);
-}
-
-template <int DIM>
-static void dispatch_gather(sdot_ctx *c, const GatherArgs &g, const EvalArgs &a, int ntb, const SweepPlan &p,
-                            bool fp32b)
-{
-    if (fp32b && p.tm > 0) {
+    if (tensor) {
+        // factors <= 2^8 per dimension: the relative form (no reciprocals, the lowest point's factor 1)
+        const bool ts = fac <= 4.0;
         if constexpr (DIM == 3) {
-            if (p.ts) launch_gather<3, 2, true, true>(c, g, a, ntb);
-            else launch_gather<3, 2, false, true>(c, g, a, ntb);
+            if (c->tensor_m == 2 && a.ql == 8) {
+                if (ts) dispatch_fused_b<3, 8, 0, 2, true>(c, f, a, fp32b, nb);
+                else dispatch_fused_b<3, 8, 0, 2, false>(c, f, a, fp32b, nb);
+                return;
+            }
         } else {
-            if (p.tm == 3) {
-                if (p.ts) launch_gather<2, 3, true, true>(c, g, a, ntb);
-                else launch_gather<2, 3, false, true>(c, g, a, ntb);
-            } else {
-                if (p.ts) launch_gather<2, 2, true, true>(c, g, a, ntb);
-                else launch_gather<2, 2, false, true>(c, g, a, ntb);
+            if (c->tensor_m == 3 && a.ql == 9) {
+                if (ts) dispatch_fused_b<2, 9, 0, 3, true>(c, f, a, fp32b, nb);
+                else dispatch_fused_b<2, 9, 0, 3, false>(c, f, a, fp32b, nb);
+                return;
+            }
+            if (c->tensor_m == 2 && a.ql == 4) {
+                if (ts) dispatch_fused_b<2, 4, 0, 2, true>(c, f, a, fp32b, nb);
+                else dispatch_fused_b<2, 4, 0, 2, false>(c, f, a, fp32b, nb);
+                return;
             }
         }
-        return;
     }
-    if (fp32b) launch_gather<DIM, 0, false, true>(c, g, a, ntb);
-    else launch_gather<DIM, 0, false, false>(c, g, a, ntb);
+    if (umin > -15000.0) dispatch_fused_q<DIM, 0>(c, f, a, fp32b, nb);
+    else dispatch_fused_q<DIM, 1>(c, f, a, fp32b, nb);
 }
 
 sdot_status run_trunc(sdot_ctx *c, const EvalArgs &a, double r)
@@ -1298,12 +1257,11 @@ sdot_status run_trunc(sdot_ctx *c, const EvalArgs &a, double r)
     if (e != cudaSuccess) return cuda_error(c, e, "pair list count");
     e = c->fwd_t.alloc(npairs + 1);
     if (e == cudaSuccess) e = c->inv_b.alloc(npairs + 1);
-    if (e == cudaSuccess) e = c->inv2fwd.alloc(npairs + 1);
+    if (e == cudaSuccess) e = c->fwd2inv.alloc(npairs + 1);
     if (e == cudaSuccess) e = c->inv_tmpb.alloc(npairs + 1);
     if (e == cudaSuccess) e = c->inv_tmpk.alloc(npairs + 1);
     if (e == cudaSuccess) e = c->inv_cnt.alloc(ntb + 1);
     if (e == cudaSuccess) e = c->inv_off.alloc(ntb + 1);
-    if (e == cudaSuccess) e = c->cmask.alloc((size_t)(npairs + 1) * FT_WARPS);
     if (e != cudaSuccess) return cuda_error(c, e, "pair list alloc");
     k_fwd_fill<<<gw, 256, 0, st>>>(nsb, nts, hmax, c->shit.p, c->scount.p, c->pmask.p, c->fwd_off.p, c->fwd_t.p);
     unsigned long long *icnt = reinterpret_cast<unsigned long long *>(c->inv_cnt.p);
@@ -1314,45 +1272,58 @@ sdot_status run_trunc(sdot_ctx *c, const EvalArgs &a, double r)
     e = cudaMemsetAsync(c->inv_cnt.p, 0, (ntb + 1) * sizeof(int64_t), st);
     if (e != cudaSuccess) return cuda_error(c, e, "pair list clear");
     k_inv_scatter<<<gw, 256, 0, st>>>(nsb, c->fwd_off.p, c->fwd_t.p, c->inv_off.p, icnt, c->inv_tmpb.p, c->inv_tmpk.p);
-    k_inv_order<<<(unsigned)ntb, 256, 0, st>>>(nsb, c->inv_off.p, c->inv_tmpb.p, c->inv_tmpk.p, c->inv_b.p,
-                                               c->inv2fwd.p);
+    k_inv_order<<<(unsigned)ntb, 256, 0, st>>>(nsb, c->inv_off.p, c->inv_tmpb.p, c->inv_tmpk.p, c->inv_b.p, c->fwd2inv.p);
     c->klaunch[6] += 9;
     if (c->profiling) cudaEventRecord(c->pev[7], st);
-
-    // 2. value sweep (L_q, value partials, candidate masks per block pair)
-    const bool fp32b = c->precision != SDOT_PREC_FP64;
-    const double prange = c->scal_host[SC_MAXPSI] - c->scal_host[SC_MINPSI];
-    const SweepPlan plan = plan_sweeps(c, a, std::isfinite(prange) ? prange : 1e300);
-    const bool gq_needed = !(fp32b && plan.tm > 0);
-    e = c->gcell.alloc((size_t)c->ncells * 4);
-    if (e == cudaSuccess) e = c->gten.alloc((size_t)c->ncells * 16);
-    if (e == cudaSuccess && gq_needed) e = c->gq.alloc((size_t)c->nq * 4);
-    if (e == cudaSuccess && gq_needed) e = c->gqw.alloc((size_t)c->nq);
-    if (e != cudaSuccess) return cuda_error(c, e, "gradient gather buffers");
+    // 2. partial buffer (inverse order): all pairs at once under the cap, else target-block groups
+    const int64_t cap_pairs = std::max<int64_t>(1, (int64_t)(c->part_cap_bytes / (TBLK_KD * sizeof(double))));
+    std::vector<std::pair<int, int>> groups;
+    std::vector<int64_t> inv_host;
+    int64_t part_pairs = npairs;
+    if (npairs <= cap_pairs) {
+        groups.push_back({0, ntb});
+    } else {
+        inv_host.resize((size_t)ntb + 1);
+        e = cudaMemcpyAsync(inv_host.data(), c->inv_off.p, (ntb + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return cuda_error(c, e, "pair list copy");
+        part_pairs = 0;
+        int t0 = 0;
+        while (t0 < ntb) {
+            int t1 = t0 + 1;
+            while (t1 < ntb && inv_host[t1 + 1] - inv_host[t0] <= cap_pairs) ++t1;
+            groups.push_back({t0, t1});
+            part_pairs = std::max(part_pairs, inv_host[t1] - inv_host[t0]);
+            t0 = t1;
+        }
+    }
+    e = c->part.alloc((size_t)std::max<int64_t>(1, part_pairs) * TBLK_KD);
+    if (e != cudaSuccess) return cuda_error(c, e, "partial buffer alloc");
     FusedArgs f{};
-    f.x = c->x.p; f.rho = c->rho.p; f.jxw = c->jxw.p; f.cell_ctr = c->cell_ctr.p;
+    f.x = c->x.p; f.rho = c->rho.p; f.jxw = c->jxw.p; f.w = c->w.p; f.cell_ctr = c->cell_ctr.p;
     f.tpk = c->tpack.p; f.sblk_cell = c->sblk_cell.p; f.sblk_sph = c->sblk_sph.p; f.tblk_off = c->tblk_off.p;
-    f.fwd_off = c->fwd_off.p; f.fwd_t = c->fwd_t.p; f.cmask = c->cmask.p;
-    f.Lq = c->Lq.p; f.valpart = c->blkpart.p;
+    f.fwd_off = c->fwd_off.p; f.fwd_t = c->fwd_t.p; f.fwd2inv = c->fwd2inv.p;
+    f.part = c->part.p; f.Lq = c->Lq.p; f.valpart = c->blkpart.p;
     f.cullt = std::isnan(r) ? 0.0 : std::min(r, 1e300);
-    if (c->dim == 2) dispatch_value<2>(c, f, a, nsb, plan);
-    else dispatch_value<3>(c, f, a, nsb, plan);
-    if (c->profiling) cudaEventRecord(c->pev[2], st);
-
-    // 3. gradient gather (per target block, no atomics, fixed order)
-    GatherArgs g{};
-    g.tpk = c->tpack.p; g.tblk_off = c->tblk_off.p; g.inv_off = c->inv_off.p; g.inv2fwd = c->inv2fwd.p;
-    g.inv_b = c->inv_b.p; g.sblk_cell = c->sblk_cell.p; g.cmask = c->cmask.p;
-    g.gcell = reinterpret_cast<const double4 *>(c->gcell.p); g.gten = c->gten.p;
-    g.gq = gq_needed ? (const void *)c->gq.p : nullptr;
-    g.gqw = gq_needed ? (const void *)c->gqw.p : nullptr;
-    g.qpc = c->qpc;
-    g.w_nonneg = c->w_nonneg ? 1 : 0;
-    g.gacc = c->gpart.p;
-    if (c->dim == 2) dispatch_gather<2>(c, g, a, ntb, plan, fp32b);
-    else dispatch_gather<3>(c, g, a, ntb, plan, fp32b);
-    c->klaunch[2] += 1;
-    c->klaunch[3] += 2;
+    f.w_nonneg = c->w_nonneg ? 1 : 0;
+    const bool fp32b = c->precision != SDOT_PREC_FP64;
+    for (size_t gi = 0; gi < groups.size(); ++gi) {
+        f.do_a = gi == 0;
+        f.do_b = 1;
+        f.tlo = groups[gi].first;
+        f.thi = groups[gi].second;
+        f.part_base = groups.size() == 1 ? 0 : inv_host[f.tlo];
+        const double prange = c->scal_host[SC_MAXPSI] - c->scal_host[SC_MINPSI];
+        if (c->dim == 2) dispatch_fused<2>(c, f, a, fp32b, nsb, std::isfinite(prange) ? prange : 1e300);
+        else dispatch_fused<3>(c, f, a, fp32b, nsb, std::isfinite(prange) ? prange : 1e300);
+        if (c->profiling && gi + 1 == groups.size()) cudaEventRecord(c->pev[2], st);
+        const int nw = f.thi - f.tlo;
+        k_grad_reduce<<<(unsigned)nw, 256, 0, st>>>(c->tblk_off.p, c->inv_off.p, f.tlo,
+                                                                                 f.thi, f.part_base, c->part.p,
+                                                                                 c->gpart.p);
+        c->klaunch[2] += 1;
+        c->klaunch[3] += 1;
+    }
     if (c->profiling) cudaEventRecord(c->pev[3], st);
     return cuda_error(c, cudaGetLastError(), "truncated evaluation");
 }

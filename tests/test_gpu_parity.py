@@ -200,10 +200,11 @@ def test_bad_inputs():
 @pytest.mark.parametrize("precision", ["fp64", "hybrid"])
 def test_clustered_targets_need_several_chunks(oracle_mod, precision):
     """4,000 targets in one tight cluster: every source block near it stages
-    all of them, several chunks of at most 1,024, so the value sweep carries
-    its online sums across chunks and records candidate masks chunk by chunk
-    for the gradient gather.  Compared with the oracle at the parity
-    tolerances; repeated evaluations are bitwise identical."""
+    all of them in several chunks (at most 1,024, or 624 in the 3D tensor
+    sweeps, per chunk), so the value sweep carries its online sums across
+    chunks and the gradient sweep stages the earlier chunks again.  Compared
+    with the oracle at the parity tolerances; repeated evaluations are
+    bitwise identical."""
     rng = np.random.default_rng(21)
     src = structured_source(3, 8, 2)
     N = 4000
@@ -228,3 +229,25 @@ def test_clustered_targets_need_several_chunks(oracle_mod, precision):
     g2 = np.zeros(N)
     assert s.evaluate_functional(psi, g2) == J and np.array_equal(g, g2)
     s.close()
+
+
+def test_partial_groups_identical(oracle_mod, monkeypatch):
+    """A tiny cap on the gradient-partial buffer forces the truncated path to
+    process source blocks in several groups; results must not change."""
+    src, y, nu, kw = make_problem("trunc3d")
+    prm = SolverParameters(epsilon=kw["epsilon"], tau=kw["tau"], use_log_sum_exp_trick=True)
+    psi = np.linspace(-2e-3, 2e-3, len(nu))
+    s = product(src, y, nu, 3, "hybrid")
+    s.configure(prm)
+    g1 = np.zeros(len(nu))
+    J1 = s.evaluate_functional(psi, g1)
+    s.close()
+    monkeypatch.setenv("SDOT_PART_CAP_BYTES", str(64 * 1024))
+    s = product(src, y, nu, 3, "hybrid")
+    s.configure(prm)
+    g2 = np.zeros(len(nu))
+    J2 = s.evaluate_functional(psi, g2)
+    s.close()
+    assert J1 == J2
+    # group sums add partials in the same order per target; allow last-bit drift
+    assert np.max(np.abs(g1 - g2)) <= 1e-15
