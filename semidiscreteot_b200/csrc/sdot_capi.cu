@@ -203,8 +203,6 @@ size_t device_bytes(const sdot_ctx *c)
            c->y.bytes() + c->nu.bytes() + c->perm.bytes() +
            c->tblk_sph.bytes() + c->psi.bytes() + c->grad.bytes() + c->tpack.bytes() + c->Lq.bytes() +
            c->gpart.bytes() + c->blkpart.bytes() + c->scal.bytes() + c->redpart.bytes() + c->vpart.bytes() +
-           c->ccache_stg.bytes() + c->ccache_cand.bytes() + c->ccache_smap.bytes() + c->ccache_meta.bytes() +
-           c->ccache_cnt.bytes() +
            c->io_a.bytes() +
            c->io_b.bytes() + c->x0.bytes() + c->pdir.bytes() + c->sk.bytes() + c->yk.bytes() + c->hist_s.bytes() +
            c->hist_y.bytes() + c->gtmp.bytes() + c->htc_tdat.bytes() + c->htc_diag.bytes() + c->htc_blk.bytes() +
@@ -445,8 +443,6 @@ void sdot_destroy(sdot_ctx *c)
         c->perm.release(); c->tblk_sph.release(); c->psi.release(); c->grad.release(); c->tpack.release();
         c->Lq.release(); c->gpart.release(); c->blkpart.release(); c->scal.release(); c->redpart.release();
         c->vpart.release();
-        c->ccache_stg.release(); c->ccache_cand.release(); c->ccache_smap.release(); c->ccache_meta.release();
-        c->ccache_cnt.release();
         c->io_a.release(); c->io_b.release(); c->x0.release(); c->pdir.release(); c->sk.release(); c->yk.release();
         c->hist_s.release(); c->hist_y.release(); c->gtmp.release();
         if (c->scal_host) cudaFreeHost(c->scal_host);

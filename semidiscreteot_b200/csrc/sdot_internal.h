@@ -145,13 +145,6 @@ struct sdot_ctx {
     sdot::DevBuf<float4> ssup_sph32, tsup_sph32;  // super-block spheres (32 blocks each)
     sdot::DevBuf<double> part;
     size_t part_cap_bytes = (size_t)4 << 30;
-    // chunk cache of the truncated sweeps (staged targets of multi-chunk source blocks)
-    sdot::DevBuf<double> ccache_stg;
-    sdot::DevBuf<unsigned short> ccache_cand;
-    sdot::DevBuf<short> ccache_smap;
-    sdot::DevBuf<int> ccache_meta;
-    sdot::DevBuf<unsigned long long> ccache_cnt;
-    bool ccache_seen = false;          // an evaluation has reported its cache use
 
     // ---- per-evaluation buffers ----
     sdot::DevBuf<double> psi, grad, tpack, Lq, gpart, blkpart, scal, redpart;

@@ -82,25 +82,7 @@ struct FusedArgs {
     int tlo, thi;                // gradient partials only for target blocks [tlo, thi)
     int64_t part_base;           // inverse position of the first pair of tlo
     double cullt;                // per-target cull radius addend (r, enlarged)
-    // Chunk cache of multi-chunk source blocks (ccap = 0: none).  The value
-    // sweep stores every chunk but the last, and the gradient sweep reloads
-    // it instead of staging it again:
-    //   cmeta[k * CM_INTS ..] at the chunk's first forward entry k: entries,
-    //     staged targets, cache offset (two ints, -1: not cached), and the
-    //     candidate count of each warp;
-    //   csmap[(k + e) * 32 + lane]: staged position of the entry's targets;
-    //   cstg[(off + i) * 5 ..]: y (3), log2 nu, s psi of staged target i;
-    //   ccand[off * 8 + w * nstg + p]: warp w's candidate list.
-    // Space is reserved per chunk by an atomic counter (cused); a chunk that
-    // does not fit the capacity is staged again as before.
-    double *cstg;
-    unsigned short *ccand;
-    short *csmap;
-    int *cmeta;
-    unsigned long long *cused;
-    int64_t ccap;                // capacity in staged targets
 };
-constexpr int CM_INTS = 4 + FT_WARPS;
 
 template <int CAP>
 struct FTSmem {
@@ -122,7 +104,7 @@ struct FTSmem {
     int ecnt[32];                 // survivors per examined forward entry (-1: none)
     int epre[32];                 // staged position of the first survivor of each accepted entry
     int eacc, etot;
-    int64_t coff;                 // cache offset of the current chunk (-1: not cached)
+    int wcount[FT_WARPS];
     int nstg;
     int ent_t[FT_PREF];            // forward entries of the block: target block,
     int ent_j0[FT_PREF];           // its first target
@@ -996,38 +978,10 @@ k_fused(FusedArgs f, EvalArgs a)
         for (int64_t k = k0; k < k1;) {
             const int nt = stage_chunk<DIM>(sm, f, k0, k, k1, bc, rcull2, f.do_b != 0);
             const int nstg = sm.nstg;
-            const bool cache_it = f.ccap > 0 && f.do_b && k + nt < k1;   // a chunk the gradient sweep needs again
-            if (cache_it) {
-                if (tid == 0) {
-                    const unsigned long long o = atomicAdd(f.cused, (unsigned long long)nstg);
-                    const int64_t off = (int64_t)o + nstg <= f.ccap ? (int64_t)o : (int64_t)-1;
-                    sm.coff = off;
-                    int *m = f.cmeta + k * CM_INTS;
-                    m[0] = nt;
-                    m[1] = nstg;
-                    m[2] = (int)(unsigned)(off & 0xffffffffll);
-                    m[3] = (int)(off >> 32);
-                }
-                for (int i = tid; i < nt * TBLK_KD; i += blockDim.x)
-                    f.csmap[k * TBLK_KD + i] = sm.smap[i / TBLK_KD][i % TBLK_KD];
-                __syncthreads();
-                const int64_t off = sm.coff;
-                if (off >= 0)
-                    for (int i = tid; i < nstg * 5; i += blockDim.x) {
-                        const int t = i / 5, d = i - t * 5;
-                        f.cstg[off * 5 + i] = sm.stg[d < 3 ? d : d + 1][t];
-                    }
-            }
             if (valid) {
                 double bmax;
                 const int ncand = compact_candidates<DIM>(sm, wp, lane, nstg, cc, a, bmax);
                 ncand_single = ncand;
-                if (cache_it) {
-                    const int64_t off = sm.coff;
-                    if (off >= 0)
-                        for (int p = lane; p < ncand; p += 32) f.ccand[off * FT_WARPS + wp * nstg + p] = sm.cand[wp][p];
-                    if (lane == 0) f.cmeta[k * CM_INTS + 4 + wp] = ncand;
-                }
                 npairs += (double)ncand * nql;
                 if (MODE != 2 && bmax > -CUDART_INF) {
                     const double mnew = bmax + sr * dqmax;
@@ -1147,42 +1101,11 @@ k_fused(FusedArgs f, EvalArgs a)
         __syncthreads();  // the earlier chunks overwrite the staged targets
     }
     for (int64_t k = k0; k < kend;) {
-        // a chunk the value sweep cached is reloaded (staged targets, slot
-        // maps, candidate lists); any other is staged and tested again
-        int64_t off = -1;
-        const int *cm = f.cmeta + k * CM_INTS;
-        if (f.ccap > 0) off = (int64_t)(unsigned)cm[2] | ((int64_t)cm[3] << 32);
-        int nt, nstg;
-        if (off >= 0) {
-            nt = cm[0];
-            nstg = cm[1];
-            for (int i = tid; i < nstg * 5; i += blockDim.x) {
-                const int t = i / 5, d = i - t * 5;
-                sm.stg[d < 3 ? d : d + 1][t] = f.cstg[off * 5 + i];
-            }
-            for (int i = tid; i < nt * TBLK_KD; i += blockDim.x)
-                sm.smap[i / TBLK_KD][i % TBLK_KD] = f.csmap[k * TBLK_KD + i];
-            if (tid < nt) {
-                const int tb = f.fwd_t[k + tid];
-                const int64_t ip = f.fwd2inv[k + tid];
-                sm.ctb[tid] = tb;
-                sm.cpos[tid] = (ip >= 0 && tb >= f.tlo && tb < f.thi) ? (ip - f.part_base) * TBLK_KD : (int64_t)-1;
-            }
-            __syncthreads();
-        } else {
-            nt = stage_chunk<DIM>(sm, f, k0, k, kend, bc, rcull2, true);
-            nstg = sm.nstg;
-        }
+        const int nt = stage_chunk<DIM>(sm, f, k0, k, kend, bc, rcull2, true);
+        const int nstg = sm.nstg;
         if (valid) {
-            int ncand;
-            if (off >= 0) {
-                ncand = cm[4 + wp];
-                for (int p = lane; p < ncand; p += 32) sm.cand[wp][p] = f.ccand[off * FT_WARPS + wp * nstg + p];
-                __syncwarp();
-            } else {
-                double bmax;
-                ncand = compact_candidates<DIM>(sm, wp, lane, nstg, cc, a, bmax);
-            }
+            double bmax;
+            const int ncand = compact_candidates<DIM>(sm, wp, lane, nstg, cc, a, bmax);
             for (int t = lane; t < nstg; t += 32) partial_rows<FP32B>(sm)[wp * SMem::MAXS + t] = 0;
             __syncwarp();
             if (isfinite(Lref)) {
@@ -1329,10 +1252,7 @@ sdot_status run_trunc(sdot_ctx *c, const EvalArgs &a, double r)
                                     c->pmask.p, c->pmpre.p, c->fwd_cnt.p);
     k_scan<<<1, 1024, 0, st>>>(c->fwd_cnt.p, nsb, c->fwd_off.p);
     int64_t npairs = 0;
-    unsigned long long cache_used = 0;   // chunk-cache reservations of the previous evaluation
     e = cudaMemcpyAsync(&npairs, c->fwd_off.p + nsb, 8, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess && c->ccache_cnt.p)
-        e = cudaMemcpyAsync(&cache_used, c->ccache_cnt.p, sizeof(cache_used), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return cuda_error(c, e, "pair list count");
     e = c->fwd_t.alloc(npairs + 1);
@@ -1386,29 +1306,6 @@ sdot_status run_trunc(sdot_ctx *c, const EvalArgs &a, double r)
     f.part = c->part.p; f.Lq = c->Lq.p; f.valpart = c->blkpart.p;
     f.cullt = std::isnan(r) ? 0.0 : std::min(r, 1e300);
     f.w_nonneg = c->w_nonneg ? 1 : 0;
-    // Chunk cache: sized from what the previous evaluation reserved (a quarter
-    // more), or 4 staged targets per block pair the first time; never above
-    // the 32 per pair a chunk can stage.  Only with a single group (the cache
-    // is filled by the value sweep of the first group).
-    f.ccap = 0;
-    if (groups.size() == 1 && npairs > 0) {
-        int64_t want = c->ccache_seen ? (int64_t)(cache_used + cache_used / 4) + 4096 : 4 * npairs;
-        want = std::min<int64_t>(want, (int64_t)TBLK_KD * npairs);
-        e = c->ccache_meta.alloc((size_t)npairs * CM_INTS);
-        if (e == cudaSuccess) e = c->ccache_smap.alloc((size_t)npairs * TBLK_KD);
-        if (e == cudaSuccess) e = c->ccache_cnt.alloc(1);
-        if (e == cudaSuccess && want > 0) e = c->ccache_stg.alloc((size_t)want * 5);
-        if (e == cudaSuccess && want > 0) e = c->ccache_cand.alloc((size_t)want * FT_WARPS);
-        if (e == cudaSuccess) e = cudaMemsetAsync(c->ccache_cnt.p, 0, sizeof(unsigned long long), st);
-        if (e != cudaSuccess) return cuda_error(c, e, "chunk cache alloc");
-        f.ccap = want;
-        f.cstg = c->ccache_stg.p;
-        f.ccand = c->ccache_cand.p;
-        f.csmap = c->ccache_smap.p;
-        f.cmeta = c->ccache_meta.p;
-        f.cused = c->ccache_cnt.p;
-        c->ccache_seen = true;
-    }
     const bool fp32b = c->precision != SDOT_PREC_FP64;
     for (size_t gi = 0; gi < groups.size(); ++gi) {
         f.do_a = gi == 0;
