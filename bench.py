@@ -70,6 +70,10 @@ def parse():
     ap.add_argument("--slots", type=int, default=4, help="batched_2d / serve_3d: concurrent solve slots")
     ap.add_argument("--baseline-seconds", type=float, default=60.0,
                     help="solve workloads: wall budget of the one-at-a-time FP64 L-BFGS baseline")
+    ap.add_argument("--like-for-like", type=int, default=16,
+                    help="batched_2d: problems of the common subset for the like-for-like arms (0: skip)")
+    ap.add_argument("--batched-eval", type=int, default=1,
+                    help="batched_2d: time one batched evaluation with default and autotuned shapes (0: skip)")
     ap.add_argument("--precision", default="hybrid", choices=["hybrid", "fp64", "mixed"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -747,10 +751,83 @@ def _solve_requests_through_server(problems, slots, rate, seed, warmup=()):
     return res, wall, st
 
 
+def _one_at_a_time(problems, seconds, method, hessian="fp64"):
+    """Each problem alone (one context, no concurrency), in order, until the
+    wall budget is spent: method "newton" (sdot_solve_newton with the given
+    Hessian method) or "lbfgs" (sdot_solve); FP64 evaluations; the problem's
+    epsilon scaling (levels eps f^(s-1), ..., eps, warm started, intermediate
+    tolerance), as the solve service applies it.  Convergence is the FP64
+    gradient's linf norm at the final epsilon."""
+    import dataclasses
+    from semidiscreteot_b200 import SotSolver
+    t_all, done, conv, iters = 0.0, 0, 0, []
+    for p in problems:
+        if t_all >= seconds:
+            break
+        s = SotSolver(dim=p["y"].shape[1], device=0, precision="fp64")
+        s.setup_source_measure(p["source"])
+        s.setup_target(p["y"], p["nu"])
+        prm = p["params"]
+        f, steps, inter = p.get("eps_factor", 10.0), max(1, p.get("eps_steps", 1)), p.get("inter_tol", 0.0)
+        psi = np.zeros(len(p["nu"]))
+        it = 0
+        t0 = time.perf_counter()
+        try:
+            for lvl in range(steps):
+                last = lvl == steps - 1
+                pl = dataclasses.replace(prm, epsilon=prm.epsilon * f ** (steps - 1 - lvl),
+                                         tolerance=prm.tolerance if (last or inter <= 0) else inter)
+                psi = s.solve_newton(psi, pl, hessian=hessian) if method == "newton" else s.solve(psi, pl)
+                it += int(s.get_last_iteration_count())
+            ok = bool(s.get_convergence_status())
+        except RuntimeError:
+            ok = False
+        t_all += time.perf_counter() - t0
+        iters.append(it)
+        done += 1
+        conv += ok
+        s.close()
+    return {"solves_per_s": conv / t_all if t_all > 0 else 0.0, "attempted": done, "converged": conv,
+            "seconds": t_all, "iterations": iters}
+
+
+def _batched_evaluation(probs, reps=5):
+    """One batched evaluation of every problem in one persistent launch
+    (sdot_batch, FP32-exponential gradient sweep): device time with the
+    default launch shape and with the shape the batch's autotuner picks."""
+    from semidiscreteot_b200 import BatchSolver
+    b = BatchSolver(dim=2)
+    for p in probs:
+        b.add_source(p["source"], p["y"], p["nu"], p["params"])
+    psis = [np.zeros(len(p["nu"])) for p in probs]
+    pairs = float(sum(p["source"]["jxw"].size * len(p["nu"]) for p in probs))
+
+    def timed():
+        b.evaluate(psis, fp32=True)   # warm-up
+        ms = []
+        for _ in range(reps):
+            b.evaluate(psis, fp32=True)
+            ms.append(b.last_eval_ms())
+        return float(np.median(ms))
+
+    default_shape = b.shape
+    t_default = timed()
+    t0 = time.perf_counter()
+    shape, cached = b.autotune(psis, fp32=True, reps=3)
+    tune_s = time.perf_counter() - t0
+    t_tuned = timed()
+    b.close()
+    return {"problems": len(probs), "pairs": pairs, "default_shape": default_shape, "default_ms": t_default,
+            "default_pairs_per_s": pairs / (t_default * 1e-3), "tuned_shape": shape, "tuned_ms": t_tuned,
+            "tuned_pairs_per_s": pairs / (t_tuned * 1e-3), "tuning_seconds": tune_s, "cached": cached,
+            "shape_fields": "[value CTAs/SM, gradient CTAs/SM, gradient slice target per SM]"}
+
+
 def run_batched_2d(args):
     """Config 4: the batched problems solved through the solve service (Newton
     with the tensor-core Hessian, epsilon scaling, all submitted at once),
-    against one-at-a-time plain FP64 L-BFGS solves."""
+    against one-at-a-time plain FP64 L-BFGS solves; like-for-like comparisons
+    on a common subset; the batched evaluation with autotuned launch shapes."""
     from semidiscreteot_b200 import workloads as W
     probs = W.batched_2d(seed=0, n_problems=args.problems)
     nw = max(args.warmup, args.slots)
@@ -773,6 +850,25 @@ def run_batched_2d(args):
             "fp64_lbfgs_baseline": base,
             "speedup_vs_fp64_lbfgs": (conv / wall) / base["solves_per_s"] if base["solves_per_s"] > 0 else None,
             "clocks": clk.summary()}
+    if args.like_for_like > 0:
+        # the same problems (the first K), the same epsilon scaling and FP64 convergence test in every arm
+        sub = probs[:args.like_for_like]
+        with clk.region():
+            rs, wall_s, _ = _solve_requests_through_server(sub, args.slots, 0.0, 0)
+        served = sum(r["converged"] for r in rs) / wall_s
+        arms = {"service_tc_newton": {"solves_per_s": served, "converged": sum(r["converged"] for r in rs),
+                                      "attempted": len(sub), "seconds": wall_s},
+                "one_at_a_time_tc_newton": _one_at_a_time(sub, args.baseline_seconds, "newton", "tensor"),
+                "one_at_a_time_fp64_newton": _one_at_a_time(sub, args.baseline_seconds, "newton", "fp64"),
+                "one_at_a_time_fp64_lbfgs": _one_at_a_time(sub, args.baseline_seconds, "lbfgs")}
+        ref = arms["one_at_a_time_fp64_newton"]["solves_per_s"]
+        line["like_for_like"] = {
+            "problems": len(sub), "arms": arms,
+            "service_vs_fp64_newton": served / ref if ref > 0 else None,
+            "note": "service = mixed precision (BF16 tensor-core Hessian) + concurrency; one_at_a_time_tc_newton "
+                    "isolates the precision; one_at_a_time_fp64_newton is the plain FP64 path of the same method"}
+    if args.batched_eval:
+        line["batched_evaluation"] = _batched_evaluation(probs)
     print(json.dumps(line))
     return 0
 

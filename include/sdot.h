@@ -334,6 +334,27 @@ sdot_status sdot_batch_evaluate(sdot_batch *batch, const double *psi, double *gr
  * is SDOT_ELINESEARCH after all other problems have finished. */
 sdot_status sdot_batch_solve(sdot_batch *batch, double *psi, const sdot_batch_options *opts, sdot_batch_info *info);
 sdot_status sdot_batch_problem_info(const sdot_batch *batch, int index, sdot_solve_info *info);
+/* Launch shape of the batched sweeps (no reference counterpart): shape[0]
+ * and shape[1] are the persistent CTAs per SM of the value and gradient
+ * sweeps, shape[2] the gradient sweep's slice target (each problem's points
+ * are cut into slices until its (target block, slice) units number about
+ * shape[2] per SM; 8 gives the single-problem path's slicing).  Default
+ * {8, 8, 8}; each value in [1, 64].  The slicing changes only the order in
+ * which each target's FP64 partial sums are added. */
+sdot_status sdot_batch_set_shape(sdot_batch *batch, const int *shape);
+sdot_status sdot_batch_get_shape(const sdot_batch *batch, int *shape);
+/* Device milliseconds (CUDA events) of the batch's last batched evaluation. */
+double sdot_batch_last_eval_ms(const sdot_batch *batch);
+/* The batch's own autotuner: times `reps` batched evaluations at psi (host,
+ * concatenated; gradient sweep in FP32 when fp32 != 0) for each candidate
+ * of one shape entry at a time (slice target 4/8/16/32, then CTAs per SM
+ * 4/8/12/16 for the value and the gradient sweep), keeps the fastest, and
+ * leaves the batch on the result, written to shape_out[3].  The result is
+ * remembered for the life of the process per bucket (dimension, log2 of the
+ * batch's pairs, log2 of its problem count, fp32); a batch of a tuned
+ * bucket takes the remembered shape without timing (*cached = 1). */
+sdot_status sdot_batch_autotune(sdot_batch *batch, const double *psi, int fp32, int reps, int *shape_out,
+                                int *cached);
 
 /* ---- solve service (no reference counterpart: the reference runs one
  * SotSolver::solve per process at a time; this admits many) ----

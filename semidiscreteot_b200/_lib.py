@@ -40,6 +40,7 @@ EXPORTED = [
     "sdot_hessian_matvec_device", "sdot_softmax_refinement", "sdot_weighted_barycenters", "sdot_conditioned_densities",
     "sdot_batch_create", "sdot_batch_destroy", "sdot_batch_last_error", "sdot_batch_size", "sdot_batch_set_verbose",
     "sdot_batch_add", "sdot_batch_evaluate", "sdot_batch_solve", "sdot_batch_problem_info",
+    "sdot_batch_set_shape", "sdot_batch_get_shape", "sdot_batch_last_eval_ms", "sdot_batch_autotune",
     "sdot_server_create", "sdot_server_destroy", "sdot_server_last_error", "sdot_server_submit", "sdot_server_poll",
     "sdot_server_wait", "sdot_server_get_stats", "sdot_server_reset_stats",
 ]
@@ -204,6 +205,14 @@ def load():
     lib.sdot_batch_solve.restype = ip
     lib.sdot_batch_problem_info.argtypes = [vp, ip, C.POINTER(SolveInfo)]
     lib.sdot_batch_problem_info.restype = ip
+    lib.sdot_batch_set_shape.argtypes = [vp, vp]
+    lib.sdot_batch_set_shape.restype = ip
+    lib.sdot_batch_get_shape.argtypes = [vp, vp]
+    lib.sdot_batch_get_shape.restype = ip
+    lib.sdot_batch_last_eval_ms.argtypes = [vp]
+    lib.sdot_batch_last_eval_ms.restype = C.c_double
+    lib.sdot_batch_autotune.argtypes = [vp, vp, ip, ip, vp, vp]
+    lib.sdot_batch_autotune.restype = ip
     lib.sdot_server_create.argtypes = [C.POINTER(vp), ip, ip, C.c_size_t]
     lib.sdot_server_create.restype = ip
     lib.sdot_server_destroy.argtypes = [vp]

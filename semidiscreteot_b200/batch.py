@@ -112,6 +112,33 @@ class BatchSolver:
         self._check(st)
         return self.split(flat)
 
+    @property
+    def shape(self) -> List[int]:
+        """Launch shape of the batched sweeps: [value CTAs/SM, gradient CTAs/SM, gradient slice target]."""
+        out = np.zeros(3, dtype=np.int32)
+        self._check(self._L.sdot_batch_get_shape(self._h, out.ctypes.data))
+        return [int(v) for v in out]
+
+    def set_shape(self, shape):
+        arr = np.ascontiguousarray(shape, dtype=np.int32)
+        self._check(self._L.sdot_batch_set_shape(self._h, arr.ctypes.data))
+
+    def last_eval_ms(self) -> float:
+        """Device milliseconds of the last batched evaluation."""
+        return float(self._L.sdot_batch_last_eval_ms(self._h))
+
+    def autotune(self, psis=None, fp32: bool = True, reps: int = 3):
+        """The batch's autotuner (sdot_batch_autotune): returns (shape, cached)."""
+        if psis is None:
+            flat = np.zeros(sum(self.sizes))
+        else:
+            flat = np.ascontiguousarray(np.concatenate([np.asarray(p, dtype=np.float64) for p in psis]))
+        out = np.zeros(3, dtype=np.int32)
+        cached = C.c_int(0)
+        self._check(self._L.sdot_batch_autotune(self._h, flat.ctypes.data, int(bool(fp32)), int(reps),
+                                                out.ctypes.data, C.byref(cached)))
+        return [int(v) for v in out], bool(cached.value)
+
     def problem_info(self, index: int) -> dict:
         r = _lib.SolveInfo()
         self._check(self._L.sdot_batch_problem_info(self._h, int(index), C.byref(r)))

@@ -30,7 +30,10 @@
 
 #include <algorithm>
 #include <cmath>
+#include <map>
+#include <mutex>
 #include <numeric>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -434,6 +437,12 @@ struct sdot_batch {
     std::string err;
     int sms = 148;
     int verbose = 0;
+    // Launch shape of the persistent sweeps (sdot_batch_autotune): CTAs per
+    // SM of the value sweep and of the gradient sweep, and the gradient
+    // sweep's slice target (each problem's points are cut into slices until
+    // its (target block, slice) units number about shape[2] per SM).
+    int shape[3] = {8, 8, 8};
+    double last_eval_ms = 0.0;
 
     struct Prob {
         int64_t nq, nt;
@@ -495,6 +504,31 @@ struct DevGuard {
     }
 };
 
+// Gradient slices of every problem for the slice target b->shape[2] (at 8:
+// the single-problem dense path's count): target blocks of DENSE_B_THREADS *
+// TT, slices of at least 256 points, at most 64.  Sets nks, ntb, qslice and
+// the partial offsets gp0; returns the total partial count.
+int64_t plan_slices(sdot_batch *b)
+{
+    int64_t gp0 = 0;
+    for (size_t i = 0; i < b->probs.size(); ++i) {
+        const auto &P = b->probs[i];
+        BInst &I = b->inst[i];
+        const int64_t tb = (P.nt + DENSE_B_THREADS * DENSE_B_TT - 1) / (DENSE_B_THREADS * DENSE_B_TT);
+        const int64_t want = ((int64_t)148 * b->shape[2] + tb - 1) / tb;
+        const int64_t maxks = (P.nq + 255) / 256;
+        int nks = (int)std::max<int64_t>(1, std::min<int64_t>(want, maxks));
+        if (nks > 64) nks = 64;
+        I.nks = nks;
+        I.ntb = (int)tb;
+        I.qslice = (P.nq + nks - 1) / nks;
+        I.gp0 = gp0;
+        gp0 += (int64_t)nks * P.nt;
+    }
+    b->total_gp = gp0;
+    return gp0;
+}
+
 // Layout of every problem in the packed arrays and its launch shapes (the
 // single-problem dense path's: value blocks of DENSE_A_THREADS * QT points,
 // gradient target blocks of DENSE_B_THREADS * TT and the same slice count).
@@ -503,7 +537,7 @@ sdot_status upload(sdot_batch *b)
     const int D = b->dim;
     const size_t np = b->probs.size();
     b->inst.assign(np, BInst{});
-    int64_t q0 = 0, t0 = 0, part0 = 0, gp0 = 0;
+    int64_t q0 = 0, t0 = 0, part0 = 0;
     for (size_t i = 0; i < np; ++i) {
         const auto &P = b->probs[i];
         BInst &I = b->inst[i];
@@ -529,26 +563,16 @@ sdot_status upload(sdot_batch *b)
         const int64_t per = (int64_t)DENSE_A_THREADS * DENSE_A_QT;
         I.nvb = (int)((P.nq + per - 1) / per);
         I.part0 = part0;
-        const int64_t tb = (P.nt + DENSE_B_THREADS * DENSE_B_TT - 1) / (DENSE_B_THREADS * DENSE_B_TT);
-        int64_t want = (148 * 8 + tb - 1) / tb;
-        int64_t maxks = (P.nq + 255) / 256;
-        int nks = (int)std::max<int64_t>(1, std::min<int64_t>(want, maxks));
-        if (nks > 64) nks = 64;
-        I.nks = nks;
-        I.ntb = (int)tb;
-        I.qslice = (P.nq + nks - 1) / nks;
-        I.gp0 = gp0;
         I.fp32 = 0;
         I.tol = P.prm.tolerance;
         q0 += P.nq;
         t0 += P.nt;
         part0 += I.nvb;
-        gp0 += (int64_t)nks * P.nt;
     }
     b->total_q = q0;
     b->total_t = t0;
     b->total_part = part0;
-    b->total_gp = gp0;
+    const int64_t gp0 = plan_slices(b);
     BCK(b->x.alloc(q0 * D), "batch alloc");
     BCK(b->rho.alloc(q0), "batch alloc");
     BCK(b->jxw.alloc(q0), "batch alloc");
@@ -618,8 +642,8 @@ sdot_status batch_eval(sdot_batch *b, const std::vector<int> &act, double *ms)
     for (int p : act) maxnt = std::max(maxnt, b->probs[p].nt);
     cudaEventRecord(b->ev0, st);
     dim3 pg((unsigned)std::min<int64_t>((maxnt + 255) / 256, 64), (unsigned)act.size());
-    const int vgrid = std::min<int>((int)vu.size(), b->sms * 8);
-    const int ggrid = std::min<int>((int)gu.size(), b->sms * 8);
+    const int vgrid = std::min<int>((int)vu.size(), b->sms * b->shape[0]);
+    const int ggrid = std::min<int>((int)gu.size(), b->sms * b->shape[1]);
     if (D == 2) {
         k_batch_prep<2><<<pg, 256, 0, st>>>(b->dinst.p, b->act.p, b->y.p, b->nu.p, b->psi.p, b->tpack.p);
         k_batch_value<2><<<vgrid, DENSE_A_THREADS, 0, st>>>(b->dinst.p, b->vunits.p, (int)vu.size(), b->counter.p,
@@ -640,11 +664,10 @@ sdot_status batch_eval(sdot_batch *b, const std::vector<int> &act, double *ms)
     BCK(cudaMemcpyAsync(b->scal_host.data(), b->scal.p, b->scal_host.size() * 8, cudaMemcpyDeviceToHost, st),
         "batch scalars");
     BCK(cudaStreamSynchronize(st), "batch evaluate");
-    if (ms) {
-        float f = 0.f;
-        cudaEventElapsedTime(&f, b->ev0, b->ev1);
-        *ms += f;
-    }
+    float f = 0.f;
+    cudaEventElapsedTime(&f, b->ev0, b->ev1);
+    b->last_eval_ms = f;
+    if (ms) *ms += f;
     return SDOT_OK;
 }
 
@@ -1078,6 +1101,116 @@ sdot_status sdot_batch_solve(sdot_batch *b, double *psi_io, const sdot_batch_opt
     }
     if (first_err != SDOT_OK)
         return berr(b, first_err, "a batched problem's line search failed (see sdot_batch_problem_info)");
+    return SDOT_OK;
+}
+
+// ---- launch-shape autotuner ----
+// Tuned shapes are kept for the life of the process per bucket (dimension,
+// log2 of the batch's pairs, log2 of its problem count, gradient precision),
+// so later batches of the same kind reuse them without timing.
+static std::mutex g_tune_mu;
+static std::map<std::tuple<int, int, int, int>, std::vector<int>> g_tune;
+
+sdot_status sdot_batch_set_shape(sdot_batch *b, const int *shape)
+{
+    if (!b || !shape) return SDOT_EINVAL;
+    for (int i = 0; i < 3; ++i)
+        if (shape[i] < 1 || shape[i] > 64) return berr(b, SDOT_EINVAL, "batch launch shape out of range [1, 64]");
+    const bool reslice = shape[2] != b->shape[2];
+    for (int i = 0; i < 3; ++i) b->shape[i] = shape[i];
+    if (reslice && b->uploaded) {
+        DevGuard g(b->device);
+        const int64_t gp = plan_slices(b);
+        BCK(b->gpart.alloc(gp), "batch slices");
+        BCK(cudaMemcpyAsync(b->dinst.p, b->inst.data(), b->inst.size() * sizeof(BInst), cudaMemcpyHostToDevice,
+                            b->stream),
+            "batch inst");
+    }
+    return SDOT_OK;
+}
+
+sdot_status sdot_batch_get_shape(const sdot_batch *b, int *shape)
+{
+    if (!b || !shape) return SDOT_EINVAL;
+    for (int i = 0; i < 3; ++i) shape[i] = b->shape[i];
+    return SDOT_OK;
+}
+
+double sdot_batch_last_eval_ms(const sdot_batch *b) { return b ? b->last_eval_ms : 0.0; }
+
+sdot_status sdot_batch_autotune(sdot_batch *b, const double *psi, int fp32, int reps, int *shape_out, int *cached)
+{
+    if (!b || !psi) return SDOT_EINVAL;
+    if (b->probs.empty()) return berr(b, SDOT_ESTATE, "empty batch");
+    if (reps < 1) reps = 1;
+    DevGuard g(b->device);
+    if (!b->uploaded) {
+        sdot_status s = upload(b);
+        if (s != SDOT_OK) return s;
+    }
+    double pairs = 0.0;
+    for (const auto &P : b->probs) pairs += (double)P.nq * (double)P.nt;
+    const auto key = std::make_tuple(b->dim, (int)std::floor(std::log2(std::max(pairs, 1.0))),
+                                     (int)std::floor(std::log2((double)b->probs.size())), fp32 ? 1 : 0);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune.find(key);
+        if (it != g_tune.end()) {
+            sdot_status s = sdot_batch_set_shape(b, it->second.data());
+            if (s != SDOT_OK) return s;
+            if (shape_out)
+                for (int i = 0; i < 3; ++i) shape_out[i] = b->shape[i];
+            if (cached) *cached = 1;
+            return SDOT_OK;
+        }
+    }
+    for (auto &I : b->inst) I.fp32 = fp32 ? 1 : 0;
+    BCK(cudaMemcpyAsync(b->dinst.p, b->inst.data(), b->inst.size() * sizeof(BInst), cudaMemcpyHostToDevice, b->stream),
+        "batch inst");
+    BCK(cudaMemcpyAsync(b->psi.p, psi, b->total_t * 8, cudaMemcpyHostToDevice, b->stream), "batch psi");
+    BCK(cudaMemsetAsync(b->pdir.p, 0, b->total_t * 8, b->stream), "batch pdir");
+    std::vector<int> act(b->probs.size());
+    std::iota(act.begin(), act.end(), 0);
+    auto timed = [&](double *out) -> sdot_status {
+        double ms = 0.0;
+        for (int r = 0; r < reps; ++r) {
+            sdot_status s = batch_eval(b, act, &ms);
+            if (s != SDOT_OK) return s;
+        }
+        *out = ms / reps;
+        return SDOT_OK;
+    };
+    double t = 0.0;
+    sdot_status s = timed(&t);  // warm-up
+    if (s != SDOT_OK) return s;
+    // coordinate search: the slice target, then the CTAs per SM of each sweep
+    static const int cand_slice[] = {4, 8, 16, 32};
+    static const int cand_grid[] = {4, 8, 12, 16};
+    const int axes[3] = {2, 0, 1};
+    for (int ax : axes) {
+        int best = b->shape[ax];
+        double best_t = 1e300;
+        for (int k = 0; k < 4; ++k) {
+            int sh[3] = {b->shape[0], b->shape[1], b->shape[2]};
+            sh[ax] = ax == 2 ? cand_slice[k] : cand_grid[k];
+            if ((s = sdot_batch_set_shape(b, sh)) != SDOT_OK) return s;
+            if ((s = timed(&t)) != SDOT_OK) return s;
+            if (t < best_t) {
+                best_t = t;
+                best = sh[ax];
+            }
+        }
+        int sh[3] = {b->shape[0], b->shape[1], b->shape[2]};
+        sh[ax] = best;
+        if ((s = sdot_batch_set_shape(b, sh)) != SDOT_OK) return s;
+    }
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune[key] = std::vector<int>(b->shape, b->shape + 3);
+    }
+    if (shape_out)
+        for (int i = 0; i < 3; ++i) shape_out[i] = b->shape[i];
+    if (cached) *cached = 0;
     return SDOT_OK;
 }
 

@@ -168,3 +168,36 @@ def test_batch_epsilon_scaling_and_errors():
     with pytest.raises(RuntimeError, match="untruncated"):
         b2.add_source(src, y, nu, SolverParameters(epsilon=1e-2, tau=1e-8))
     b2.close()
+
+
+def test_batch_autotune_shapes_and_results():
+    """The batch's autotuner times candidate launch shapes and leaves the batch
+    on the fastest; the shape changes only the order of the FP64 partial sums,
+    so values and gradients stay within 1e-13 relative / 1e-15 absolute of the
+    default shape's.  A second batch of the same kind takes the remembered
+    shape without timing; out-of-range shapes are rejected."""
+    probs = problems(9, n=6)
+    b = BatchSolver(dim=2)
+    for src, y, nu, prm in probs:
+        b.add_source(src, y, nu, prm)
+    rng = np.random.default_rng(4)
+    psis = [0.2 * prm.epsilon * rng.standard_normal(len(nu)) for (_, _, nu, prm) in probs]
+    assert b.shape == [8, 8, 8]
+    v0, g0 = b.evaluate(psis, fp32=False)
+    assert b.last_eval_ms() > 0.0
+    shape, cached = b.autotune(psis, fp32=False, reps=1)
+    assert not cached and b.shape == shape
+    assert shape[2] in (4, 8, 16, 32) and shape[0] in (4, 8, 12, 16) and shape[1] in (4, 8, 12, 16)
+    v1, g1 = b.evaluate(psis, fp32=False)
+    assert np.allclose(v1, v0, rtol=1e-13, atol=0.0)
+    for a, c in zip(g0, g1):
+        assert np.max(np.abs(a - c)) <= 1e-15
+    with pytest.raises(RuntimeError):
+        b.set_shape([0, 8, 8])
+    b.close()
+    b2 = BatchSolver(dim=2)
+    for src, y, nu, prm in probs:
+        b2.add_source(src, y, nu, prm)
+    shape2, cached2 = b2.autotune(psis, fp32=False, reps=1)
+    assert cached2 and shape2 == shape
+    b2.close()
