@@ -465,6 +465,18 @@ sdot_status sdot_get_kernel_times(sdot_ctx *ctx, double *ms, int64_t *launches, 
  * Gop/s, out[3] SM clock (MHz) reported by the device. */
 sdot_status sdot_measure_peaks(int device, double *out);
 
+/* ---- failure injection for tests (no counterpart in the reference) ----
+ * sdot_debug_fail_allocation(k): the library's device allocations (the
+ * buffers of every context and batch of the process) count down from k, and
+ * the allocation that finds the count at 0 fails as if the device were out
+ * of memory, without calling cudaMalloc: the call making it returns
+ * SDOT_ENOMEM.  k < 0 turns the injection off.  Returns the previous count
+ * (-1: off).  sdot_debug_allocation_count: allocations made or failed so far
+ * in the process.  After a failed set-up call the context holds no source
+ * (or no target) and evaluations return SDOT_ESTATE until it is set again. */
+int64_t sdot_debug_fail_allocation(int64_t after);
+int64_t sdot_debug_allocation_count(void);
+
 /* ---- no-allocation evaluation (no counterpart in the reference) ----
  * Same results as sdot_evaluate_device (same kernels, same launch shapes) for
  * an untruncated problem (pointwise threshold with tau <= 0), but the call

@@ -13,8 +13,10 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libsdot_cuda.so")
 
 SDOT_OK = 0
+SDOT_ENOMEM = 2
 SDOT_ELINESEARCH = 4
 SDOT_ETIMEOUT = 7
+SDOT_ESTATE = 9
 STATUS_NAMES = {
     0: "SDOT_OK", 1: "SDOT_EINVAL", 2: "SDOT_ENOMEM", 3: "SDOT_ENONFINITE", 4: "SDOT_ELINESEARCH",
     5: "SDOT_EMAXITER", 6: "SDOT_EBUDGET", 7: "SDOT_ETIMEOUT", 8: "SDOT_ECUDA", 9: "SDOT_ESTATE",
@@ -41,6 +43,7 @@ EXPORTED = [
     "sdot_batch_create", "sdot_batch_destroy", "sdot_batch_last_error", "sdot_batch_size", "sdot_batch_set_verbose",
     "sdot_batch_add", "sdot_batch_evaluate", "sdot_batch_solve", "sdot_batch_problem_info",
     "sdot_batch_set_shape", "sdot_batch_get_shape", "sdot_batch_last_eval_ms", "sdot_batch_autotune",
+    "sdot_debug_fail_allocation", "sdot_debug_allocation_count",
     "sdot_server_create", "sdot_server_destroy", "sdot_server_last_error", "sdot_server_submit", "sdot_server_poll",
     "sdot_server_wait", "sdot_server_get_stats", "sdot_server_reset_stats",
 ]
@@ -213,6 +216,10 @@ def load():
     lib.sdot_batch_last_eval_ms.restype = C.c_double
     lib.sdot_batch_autotune.argtypes = [vp, vp, ip, ip, vp, vp]
     lib.sdot_batch_autotune.restype = ip
+    lib.sdot_debug_fail_allocation.argtypes = [C.c_int64]
+    lib.sdot_debug_fail_allocation.restype = C.c_int64
+    lib.sdot_debug_allocation_count.argtypes = []
+    lib.sdot_debug_allocation_count.restype = C.c_int64
     lib.sdot_server_create.argtypes = [C.POINTER(vp), ip, ip, C.c_size_t]
     lib.sdot_server_create.restype = ip
     lib.sdot_server_destroy.argtypes = [vp]

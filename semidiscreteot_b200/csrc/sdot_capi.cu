@@ -141,9 +141,9 @@ bool all_finite(const double *v, int64_t n)
     return true;
 }
 
-void update_geometry(sdot_ctx *c)
+cudaError_t update_geometry(sdot_ctx *c)
 {
-    if (c->nq == 0 || c->nt == 0) return;
+    if (c->nq == 0 || c->nt == 0) return cudaSuccess;
     double lo[3], hi[3], s = 0.0;
     for (int d = 0; d < 3; ++d) {
         lo[d] = std::min(c->src_lo[d], c->tgt_lo[d]);
@@ -159,8 +159,10 @@ void update_geometry(sdot_ctx *c)
     std::vector<float4> s32(c->nsblk), t32(c->ntblk);
     for (int64_t b = 0; b < c->nsblk; ++b) s32[b] = sphere32(&c->src_sph_host[b * 4], sc);
     for (int64_t b = 0; b < c->ntblk; ++b) t32[b] = sphere32(&c->tgt_sph_host[b * 4], sc);
-    cudaMemcpy(c->sblk_sph32.p, s32.data(), s32.size() * sizeof(float4), cudaMemcpyHostToDevice);
-    cudaMemcpy(c->tblk_sph32.p, t32.data(), t32.size() * sizeof(float4), cudaMemcpyHostToDevice);
+    cudaError_t e = cudaMemcpy(c->sblk_sph32.p, s32.data(), s32.size() * sizeof(float4), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(c->tblk_sph32.p, t32.data(), t32.size() * sizeof(float4), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return e;
     // super-blocks of 32 consecutive blocks: sphere containing the member spheres
     auto supers = [&](const std::vector<double> &sph, int64_t nb, std::vector<float4> &out) {
         const int64_t ns = (nb + 31) / 32;
@@ -188,10 +190,13 @@ void update_geometry(sdot_ctx *c)
     std::vector<float4> ss, ts;
     supers(c->src_sph_host, c->nsblk, ss);
     supers(c->tgt_sph_host, c->ntblk, ts);
-    c->ssup_sph32.alloc(ss.size());
-    c->tsup_sph32.alloc(ts.size());
-    cudaMemcpy(c->ssup_sph32.p, ss.data(), ss.size() * sizeof(float4), cudaMemcpyHostToDevice);
-    cudaMemcpy(c->tsup_sph32.p, ts.data(), ts.size() * sizeof(float4), cudaMemcpyHostToDevice);
+    e = c->ssup_sph32.alloc(ss.size());
+    if (e == cudaSuccess) e = c->tsup_sph32.alloc(ts.size());
+    if (e == cudaSuccess)
+        e = cudaMemcpy(c->ssup_sph32.p, ss.data(), ss.size() * sizeof(float4), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(c->tsup_sph32.p, ts.data(), ts.size() * sizeof(float4), cudaMemcpyHostToDevice);
+    return e;
 }
 
 size_t device_bytes(const sdot_ctx *c)
@@ -569,6 +574,11 @@ sdot_status sdot_set_source(sdot_ctx *c, int dim, int64_t n_q, const double *x, 
         }
     for (int d = dim; d < 3; ++d) c->src_lo[d] = c->src_hi[d] = 0.0;
     c->cell_ctr_host = hc;
+    // Until the buffers below are in place the context holds no usable source:
+    // a failure leaves it "source not set" (SDOT_ESTATE for evaluations), never
+    // with sizes that outrun its buffers.
+    c->nq = 0;
+    c->ncells = 0;
     const size_t need = (size_t)(n_q * (dim + 4) + n_cells * dim + nsblk * 7) * sizeof(double);
     if (c->budget && need > c->budget) return set_error(c, SDOT_EBUDGET, "set_source: exceeds the memory budget");
     CK(c->x.alloc(n_q * dim), "alloc x");
@@ -588,7 +598,14 @@ sdot_status sdot_set_source(sdot_ctx *c, int dim, int64_t n_q, const double *x, 
     CK(cudaMemcpy(c->sblk_cell.p, bounds.data(), bounds.size() * 8, cudaMemcpyHostToDevice), "copy blocks");
     c->src_sph_host = ssph;
     c->covering_radius = 0.0;  // reference: recomputed by the next solve
-    update_geometry(c);
+    c->nq = n_q;
+    c->ncells = n_cells;
+    const cudaError_t eg = update_geometry(c);
+    if (eg != cudaSuccess) {
+        c->nq = 0;
+        c->ncells = 0;
+        return cuda_error(c, eg, "set_source: block spheres");
+    }
     return SDOT_OK;
 }
 
@@ -617,6 +634,7 @@ sdot_status sdot_set_target(sdot_ctx *c, int64_t n, const double *y, const doubl
         for (int64_t k = bounds[b]; k < bounds[b + 1]; ++k) idx.push_back(k);
         sphere_of(hy.data(), idx, dim, &tsph[b * 4]);
     }
+    c->nt = 0;  // no usable target until its buffers are in place (see set_source)
     CK(c->y.alloc(n * dim), "alloc y");
     CK(c->nu.alloc(n), "alloc nu");
     CK(c->perm.alloc(n), "alloc perm");
@@ -645,7 +663,11 @@ sdot_status sdot_set_target(sdot_ctx *c, int64_t n, const double *y, const doubl
             c->tgt_hi[d] = std::max(c->tgt_hi[d], hy[k * dim + d]);
         }
     }
-    update_geometry(c);
+    const cudaError_t eg = update_geometry(c);
+    if (eg != cudaSuccess) {
+        c->nt = 0;
+        return cuda_error(c, eg, "set_target: block spheres");
+    }
     return SDOT_OK;
 }
 
@@ -1087,6 +1109,13 @@ sdot_status sdot_evaluate_partial_device(sdot_ctx *c, const double *psi_dev, dou
     if (info) info->value = c->scal_host[SC_VALSRC];
     return s;
 }
+
+int64_t sdot_debug_fail_allocation(int64_t after)
+{
+    return (int64_t)g_alloc_countdown.exchange(after < 0 ? -1 : (long long)after);
+}
+
+int64_t sdot_debug_allocation_count(void) { return (int64_t)g_alloc_count.load(); }
 
 sdot_status sdot_set_state(sdot_ctx *c, double global_functional, double C_global)
 {

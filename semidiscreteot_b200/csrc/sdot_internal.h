@@ -19,6 +19,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+
 #include <string>
 #include <vector>
 
@@ -59,6 +61,14 @@ enum ScalarSlot {
     SC_COUNT = 20
 };
 
+// Allocation-failure injection for tests (sdot_debug_fail_allocation): when
+// the countdown is >= 0, every device allocation made through DevBuf counts
+// it down, and the one that finds it at 0 fails with
+// cudaErrorMemoryAllocation without calling cudaMalloc.  -1: off.  The
+// counter counts the allocations that reached cudaMalloc or were failed.
+inline std::atomic<long long> g_alloc_countdown{-1};
+inline std::atomic<long long> g_alloc_count{0};
+
 template <class T>
 struct DevBuf {
     T *p = nullptr;
@@ -76,6 +86,11 @@ struct DevBuf {
         if (count <= n && p) return cudaSuccess;
         release();
         if (count == 0) count = 1;
+        g_alloc_count.fetch_add(1);
+        long long left = g_alloc_countdown.load();
+        while (left >= 0 && !g_alloc_countdown.compare_exchange_weak(left, left - 1)) {
+        }
+        if (left == 0) return cudaErrorMemoryAllocation;
         cudaError_t e = cudaMalloc(&p, count * sizeof(T));
         if (e == cudaSuccess) n = count;
         else p = nullptr;
