@@ -432,8 +432,30 @@ sdot_status sdot_compute_covering_radius(sdot_ctx *ctx, double *radius);
 sdot_status sdot_compute_geometric_radius_bound(sdot_ctx *ctx, const double *psi, double epsilon,
                                                 double tolerance, double *radius);
 /* Replaces SotSolver::set_distance_function (SotSolver.h:305; SotSolver.cc:22-41):
- * only "euclidean" is on the accelerated path; anything else is SDOT_EINVAL. */
+ * "euclidean" (the default, the accelerated path) or "spherical" (the
+ * great-circle distance acos(clamp(a.b / (|a| |b|))) of Distance.h, for
+ * points on a sphere about the origin).  With "spherical", evaluations and
+ * sdot_solve use it for the candidate predicate and the cost, through FP64
+ * sweeps over every (point, target) pair and the pointwise threshold only;
+ * the Hessian, Newton, the softmax refinement, the conditioned densities, the
+ * euclidean barycenters and the no-allocation evaluation return SDOT_EINVAL.
+ * Anything else is SDOT_EINVAL. */
 sdot_status sdot_set_distance_function(sdot_ctx *ctx, const char *name);
+
+/* Replaces SotSolver::evaluate_weighted_barycenters with the spherical
+ * distance (SotSolver.cc:612-650, compute_weighted_barycenters_non_euclidean
+ * :662-767): evaluates at psi (caller order), then iterates at most
+ * max_iterations times: G_j = sum_q w_q pi_qj grad_b d^2(b_j, x_q)
+ * (spherical_distance_gradient, Distance.h) over the candidates; stop when
+ * ||G||_2 < tolerance, else b_j <- exp_{b_j}(-G_j) (spherical_distance_exp_map).
+ * bary (n_targets * dim, caller order) holds the starting points and receives
+ * the result; *iterations the gradient evaluations run, *grad_norm the last
+ * ||G||_2.  At a zero distance d/sin(d) is taken as 1 and a zero step leaves
+ * the point in place (the reference divides 0 by 0 there).  Needs
+ * sdot_set_distance_function(ctx, "spherical"). */
+sdot_status sdot_weighted_barycenters_spherical(sdot_ctx *ctx, const double *psi, double *bary,
+                                                unsigned max_iterations, double tolerance, unsigned *iterations,
+                                                double *grad_norm);
 
 /* ---- multi-GPU sharding (no reference counterpart as one call: it replaces
  * the MPI sums of SotSolver.cc:316-319 by letting the caller all-reduce). ----

@@ -24,6 +24,7 @@ _LIB_PATH = os.path.join(_HERE, "_build", "libsdot_oracle.so")
 THRESH = {"pointwise": 0, "integral": 1, "geometric": 2}
 CONTROL = {"l1norm": 0, "componentwise": 1, "linf": 2}
 LINE_SEARCH = {"upstream": 0, "vendored": 1}
+DISTANCE = {"euclidean": 0, "spherical": 1}
 
 
 def build(force: bool = False) -> str:
@@ -39,7 +40,7 @@ class _Problem(C.Structure):
         ("dim", C.c_int), ("n_q", C.c_int64), ("n_cells", C.c_int64), ("n_targets", C.c_int64),
         ("xq", C.c_void_p), ("jxw", C.c_void_p), ("rho", C.c_void_p),
         ("cell_offsets", C.c_void_p), ("cell_centers", C.c_void_p),
-        ("y", C.c_void_p), ("nu", C.c_void_p),
+        ("y", C.c_void_p), ("nu", C.c_void_p), ("distance", C.c_int),
     ]
 
 
@@ -103,6 +104,8 @@ def lib():
         _lib.orc_softmax_refinement.argtypes = [vp, vp, d, d, ip, i64, vp, vp, vp, vp, ip]
         _lib.orc_weighted_barycenters.argtypes = [vp, vp, d, vp, vp, ip]
         _lib.orc_conditioned_densities.argtypes = [vp, vp, d, d, i64, vp, vp, i64, vp, vp]
+        _lib.orc_spherical_barycenters.argtypes = [vp, vp, d, vp, vp, C.c_uint, d, vp]
+        _lib.orc_spherical_barycenters.restype = ip
         _lib.orc_epsilon_sequence.argtypes = [d, d, C.c_uint, vp]
         _lib.orc_epsilon_sequence.restype = ip
     return _lib
@@ -156,7 +159,7 @@ class Params:
 class Problem:
     """Holds contiguous FP64 copies of a problem and the reference-like solver state."""
 
-    def __init__(self, xq, jxw, rho, cell_offsets, cell_centers, y, nu):
+    def __init__(self, xq, jxw, rho, cell_offsets, cell_centers, y, nu, distance="euclidean"):
         self.xq = np.ascontiguousarray(xq, dtype=np.float64)
         self.dim = self.xq.shape[1]
         self.jxw = np.ascontiguousarray(jxw, dtype=np.float64)
@@ -167,7 +170,7 @@ class Problem:
         self.nu = np.ascontiguousarray(nu, dtype=np.float64)
         self._c = _Problem(self.dim, self.xq.shape[0], self.ctr.shape[0], self.y.shape[0],
                            _p(self.xq), _p(self.jxw), _p(self.rho), _p(self.off), _p(self.ctr),
-                           _p(self.y), _p(self.nu))
+                           _p(self.y), _p(self.nu), DISTANCE[distance])
         self.state = _State(0.0, 0.0, 0.0, 0.0, 1e-1)
 
     @property
@@ -258,6 +261,16 @@ class Problem:
         pc = prm.c()
         lib().orc_weighted_barycenters(C.byref(self._c), C.byref(pc), r, _p(psi), _p(out), threads)
         return out
+
+    def spherical_barycenters(self, psi, prm: Params, r, bary0, max_iterations, tolerance):
+        """Spherical weighted-barycenter iteration; returns (barycenters, iterations, last gradient norm)."""
+        psi = np.ascontiguousarray(psi, dtype=np.float64)
+        b = np.array(bary0, dtype=np.float64, copy=True).reshape(self.N, self.dim)
+        nrm = C.c_double(0.0)
+        pc = prm.c()
+        it = lib().orc_spherical_barycenters(C.byref(self._c), C.byref(pc), r, _p(psi), _p(b),
+                                             int(max_iterations), float(tolerance), C.byref(nrm))
+        return b, it, nrm.value
 
     def conditioned_densities(self, psi, eps, r, points, density, indices):
         psi = np.ascontiguousarray(psi, dtype=np.float64)

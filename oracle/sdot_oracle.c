@@ -177,6 +177,25 @@ static inline double orc_dist(int dim, const double *a, const double *b)
     return sqrt(s);
 }
 
+/* spherical_distance (Distance.h): acos of the normalised dot product,
+ * clamped to [-1, 1]; norms as Point::norm (sqrt of the ordered sum). */
+static inline double orc_sph_dist(int dim, const double *a, const double *b)
+{
+    double dot = 0.0, na = 0.0, nb = 0.0;
+    for (int d = 0; d < dim; ++d) dot += a[d] * b[d];
+    for (int d = 0; d < dim; ++d) na += a[d] * a[d];
+    for (int d = 0; d < dim; ++d) nb += b[d] * b[d];
+    double c = dot / (sqrt(na) * sqrt(nb));
+    c = c > 1.0 ? 1.0 : (c < -1.0 ? -1.0 : c);
+    return acos(c);
+}
+
+/* The problem's distance_function (SotSolver.cc:22-41). */
+static inline double orc_pdist(const orc_problem *p, const double *a, const double *b)
+{
+    return p->distance == ORC_DIST_SPHERICAL ? orc_sph_dist(p->dim, a, b) : orc_dist(p->dim, a, b);
+}
+
 static double vmax(const double *v, int64_t n)
 {
     double m = v[0];
@@ -264,7 +283,7 @@ int64_t orc_candidates(const orc_problem *p, const double *c, double r, int64_t 
 {
     int64_t k = 0;
     for (int64_t j = 0; j < p->n_targets; ++j)
-        if (orc_dist(p->dim, p->y + j * p->dim, c) <= r) out[k++] = j;
+        if (orc_pdist(p, p->y + j * p->dim, c) <= r) out[k++] = j;
     return k;
 }
 
@@ -308,19 +327,19 @@ static double cell_assemble(const orc_problem *p, const orc_params *prm, double 
         *n_pairs += nc;
         if (prm->use_log_sum_exp) {
             for (int64_t i = 0; i < nc; ++i) {
-                const double d2 = pow(orc_dist(dim, x, sc->ty + i * dim), 2);
+                const double d2 = pow(orc_pdist(p, x, sc->ty + i * dim), 2);
                 const double e = (sc->tpsi[i] - 0.5 * d2) * epsilon_inv;
                 maxe = maxe > e ? maxe : e;
             }
             for (int64_t i = 0; i < nc; ++i) {
-                const double d2 = pow(orc_dist(dim, x, sc->ty + i * dim), 2);
+                const double d2 = pow(orc_pdist(p, x, sc->ty + i * dim), 2);
                 const double se = exp((sc->tpsi[i] - 0.5 * d2) * epsilon_inv - maxe);
                 sc->et[i] = sc->tnu[i] * se;
                 total += sc->et[i];
             }
         } else {
             for (int64_t i = 0; i < nc; ++i) {
-                const double d2 = pow(orc_dist(dim, x, sc->ty + i * dim), 2);
+                const double d2 = pow(orc_pdist(p, x, sc->ty + i * dim), 2);
                 sc->et[i] = sc->tnu[i] * exp((sc->tpsi[i] - 0.5 * d2) * epsilon_inv);
                 total += sc->et[i];
             }
@@ -963,6 +982,87 @@ void orc_weighted_barycenters(const orc_problem *p, const orc_params *prm, doubl
         bary[k] = v / p->nu[k / dim];
     }
     free(acc);
+}
+
+/* spherical_distance_gradient(a, b) (Distance.h): -2 (d / sin d) (b - (a.b) a),
+ * d the spherical distance, a.b the raw dot product; d / sin d -> 1 at d = 0. */
+static void orc_sph_grad(int dim, const double *a, const double *b, double *g)
+{
+    const double dist = orc_sph_dist(dim, a, b);
+    double dot = 0.0;
+    for (int d = 0; d < dim; ++d) dot += a[d] * b[d];
+    const double f = dist > 0.0 ? dist / sin(dist) : 1.0;
+    for (int d = 0; d < dim; ++d) g[d] = -2 * f * (b[d] - dot * a[d]);
+}
+
+int orc_spherical_barycenters(const orc_problem *p, const orc_params *prm, double r, const double *psi,
+                              double *bary, unsigned max_iterations, double tolerance, double *grad_norm)
+{
+    const int dim = p->dim;
+    const int64_t N = p->n_targets;
+    const double epsilon_inv = 1.0 / prm->epsilon;
+    double *G = (double *)calloc((size_t)N * dim, sizeof(double));
+    int64_t *cand = (int64_t *)malloc(sizeof(int64_t) * (N + 1));
+    double *et = (double *)malloc(sizeof(double) * (N + 1));
+    unsigned it = 0;
+    double l2 = 0.0;
+    for (it = 0; it < max_iterations; ++it) {
+        for (int64_t k = 0; k < N * dim; ++k) G[k] = 0.0;
+        for (int64_t c = 0; c < p->n_cells; ++c) {
+            const int64_t nc = orc_candidates(p, p->cell_centers + c * dim, r, cand);
+            if (nc == 0) continue;
+            for (int64_t q = p->cell_offsets[c]; q < p->cell_offsets[c + 1]; ++q) {
+                const double *x = p->xq + q * dim;
+                double total = 0.0, maxe = -DBL_MAX;
+                if (prm->use_log_sum_exp) {
+                    for (int64_t i = 0; i < nc; ++i) {
+                        const int64_t j = cand[i];
+                        const double d2 = pow(orc_pdist(p, x, p->y + j * dim), 2);
+                        const double e = (psi[j] - 0.5 * d2) * epsilon_inv;
+                        maxe = maxe > e ? maxe : e;
+                    }
+                    for (int64_t i = 0; i < nc; ++i) {
+                        const int64_t j = cand[i];
+                        const double d2 = pow(orc_pdist(p, x, p->y + j * dim), 2);
+                        et[i] = p->nu[j] * exp((psi[j] - 0.5 * d2) * epsilon_inv - maxe);
+                        total += et[i];
+                    }
+                } else {
+                    for (int64_t i = 0; i < nc; ++i) {
+                        const int64_t j = cand[i];
+                        const double d2 = pow(orc_pdist(p, x, p->y + j * dim), 2);
+                        et[i] = p->nu[j] * exp((psi[j] - 0.5 * d2) * epsilon_inv);
+                        total += et[i];
+                    }
+                }
+                if (total <= 0.0) continue;
+                const double scale = p->rho[q] * p->jxw[q] / total;
+                for (int64_t i = 0; i < nc; ++i) {
+                    if (!(et[i] > 0.0)) continue;
+                    const int64_t j = cand[i];
+                    double v[3];
+                    orc_sph_grad(dim, bary + j * dim, x, v);
+                    for (int d = 0; d < dim; ++d) G[j * dim + d] += scale * et[i] * v[d];
+                }
+            }
+        }
+        double s2 = 0.0;
+        for (int64_t k = 0; k < N * dim; ++k) s2 += G[k] * G[k];
+        l2 = sqrt(s2);
+        if (l2 < tolerance) { ++it; break; }
+        /* exp map at b_j of the step -G_j: cos|v| b + sin|v| v / |v| */
+        for (int64_t j = 0; j < N; ++j) {
+            double nv = 0.0;
+            for (int d = 0; d < dim; ++d) nv += G[j * dim + d] * G[j * dim + d];
+            nv = sqrt(nv);
+            if (!(nv > 0.0)) continue;
+            const double cs = cos(nv), sn = sin(nv);
+            for (int d = 0; d < dim; ++d) bary[j * dim + d] = cs * bary[j * dim + d] + sn * (-G[j * dim + d] / nv);
+        }
+    }
+    free(G); free(cand); free(et);
+    if (grad_norm) *grad_norm = l2;
+    return (int)it;
 }
 
 /* SotSolver::get_potential_conditioned_density (SotSolver.cc:973-1046) at

@@ -49,7 +49,13 @@ typedef struct {
     const double *cell_centers;    /* n_cells * dim */
     const double *y;               /* n_targets * dim */
     const double *nu;              /* n_targets */
+    int distance;                  /* ORC_DIST_*: the candidate predicate and cost of
+                                      orc_evaluate / orc_solve / orc_candidates */
 } orc_problem;
+
+/* SotSolver::set_distance_function (SotSolver.cc:22-41): "euclidean" or
+ * "spherical" (Distance.h). */
+enum { ORC_DIST_EUCLIDEAN = 0, ORC_DIST_SPHERICAL = 1 };
 
 enum { ORC_THRESH_POINTWISE = 0, ORC_THRESH_INTEGRAL = 1, ORC_THRESH_GEOMETRIC = 2 };
 enum { ORC_CONTROL_L1 = 0, ORC_CONTROL_COMPONENTWISE = 1, ORC_CONTROL_LINF = 2 };
@@ -146,6 +152,19 @@ int orc_solve(const orc_problem *p, const orc_params *prm, orc_state *s,
 int orc_solve_ex(const orc_problem *p, const orc_params *prm, orc_state *s,
                  double *psi, orc_solve_info *info, double *trace, int64_t trace_cap,
                  int n_threads, int faithful_overheads);
+
+/* SotSolver::evaluate_weighted_barycenters with the spherical distance
+ * (SotSolver.cc:612-650) through compute_weighted_barycenters_non_euclidean
+ * (:662-767): Riemannian gradient steps on the barycenters, bary (n_targets *
+ * dim, in/out) the starting points.  Per iteration the accumulator
+ * G_j = sum_q w_q pi_qj grad_b d^2(b_j, x_q) (spherical_distance_gradient,
+ * Distance.h) over the candidates of each cell is formed; if ||G||_2 <
+ * tolerance the iteration stops, else b_j = exp_map(b_j, -G_j).  Returns the
+ * iterations run (gradient evaluations) and ||G||_2 of the last one.  At a
+ * zero distance the factor dist/sin(dist) is taken as its limit 1, and a zero
+ * step leaves the point where it is (the reference divides 0 by 0 there). */
+int orc_spherical_barycenters(const orc_problem *p, const orc_params *prm, double r, const double *psi,
+                              double *bary, unsigned max_iterations, double tolerance, double *grad_norm);
 
 /* Dense Hessian of the dual functional (declared at SotSolver.h:343-344,
  * never defined in the reference):

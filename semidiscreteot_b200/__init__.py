@@ -13,9 +13,9 @@ from .multilevel import build_hierarchy, run_source_multilevel, run_target_multi
 from .server import SolveServer
 from .solver import SotSolver
 from .simplex import simplex_source
-from .source import structured_source
+from .source import sphere_source, structured_source
 
 __all__ = [
     "SotSolver", "BatchSolver", "SolveServer", "SolverParameters", "build_hierarchy", "run_target_multilevel", "run_source_multilevel", "run_lloyd", "simplex_source", "io", "MultilevelParameters", "read_prm", "solver_parameters_from_prm",
-    "multilevel_parameters_from_prm", "epsilon_sequence", "distribute_epsilon_values", "structured_source",
+    "multilevel_parameters_from_prm", "epsilon_sequence", "distribute_epsilon_values", "structured_source", "sphere_source",
 ]

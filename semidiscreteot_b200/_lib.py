@@ -43,7 +43,7 @@ EXPORTED = [
     "sdot_batch_create", "sdot_batch_destroy", "sdot_batch_last_error", "sdot_batch_size", "sdot_batch_set_verbose",
     "sdot_batch_add", "sdot_batch_evaluate", "sdot_batch_solve", "sdot_batch_problem_info",
     "sdot_batch_set_shape", "sdot_batch_get_shape", "sdot_batch_last_eval_ms", "sdot_batch_autotune",
-    "sdot_debug_fail_allocation", "sdot_debug_allocation_count",
+    "sdot_debug_fail_allocation", "sdot_debug_allocation_count", "sdot_weighted_barycenters_spherical",
     "sdot_server_create", "sdot_server_destroy", "sdot_server_last_error", "sdot_server_submit", "sdot_server_poll",
     "sdot_server_wait", "sdot_server_get_stats", "sdot_server_reset_stats",
 ]
@@ -220,6 +220,8 @@ def load():
     lib.sdot_debug_fail_allocation.restype = C.c_int64
     lib.sdot_debug_allocation_count.argtypes = []
     lib.sdot_debug_allocation_count.restype = C.c_int64
+    lib.sdot_weighted_barycenters_spherical.argtypes = [vp, vp, vp, C.c_uint, C.c_double, vp, vp]
+    lib.sdot_weighted_barycenters_spherical.restype = ip
     lib.sdot_server_create.argtypes = [C.POINTER(vp), ip, ip, C.c_size_t]
     lib.sdot_server_create.restype = ip
     lib.sdot_server_destroy.argtypes = [vp]

@@ -195,6 +195,9 @@ extern "C" sdot_status sdot_weighted_barycenters(sdot_ctx *c, const double *psi,
 {
     if (!c || !psi || !barycenters) return SDOT_EINVAL;
     if (c->nq == 0 || c->nt == 0) return set_error(c, SDOT_ESTATE, "Invalid measures configuration");
+    if (c->distance != 0)
+        return set_error(c, SDOT_EINVAL,
+                         "with the spherical distance use sdot_weighted_barycenters_spherical (an iteration)");
     int prev = -1;
     cudaGetDevice(&prev);
     if (prev != c->device) cudaSetDevice(c->device);
@@ -236,6 +239,8 @@ extern "C" sdot_status sdot_conditioned_densities(sdot_ctx *c, const double *psi
                                                  const double *density_at_points, int64_t n_indices,
                                                  const int64_t *indices, double *out)
 {
+    if (c && c->distance != 0)
+        return set_error(c, SDOT_EINVAL, "conditioned densities support the euclidean distance only");
     if (!c || !psi || !points || !density_at_points || !indices || !out || n_points < 0 || n_indices < 0)
         return SDOT_EINVAL;
     if (c->nt == 0 || c->dim == 0) return set_error(c, SDOT_ESTATE, "Invalid measures configuration");

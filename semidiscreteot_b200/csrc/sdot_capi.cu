@@ -685,8 +685,9 @@ sdot_status sdot_configure(sdot_ctx *c, const sdot_solver_params *p)
 sdot_status sdot_set_distance_function(sdot_ctx *c, const char *name)
 {
     if (!c || !name) return SDOT_EINVAL;
-    if (strcmp(name, "euclidean") != 0)
-        return set_error(c, SDOT_EINVAL, std::string("Unknown distance function: ") + name);
+    if (strcmp(name, "euclidean") == 0) c->distance = 0;
+    else if (strcmp(name, "spherical") == 0) c->distance = 1;
+    else return set_error(c, SDOT_EINVAL, std::string("Unknown distance function: ") + name);
     return SDOT_OK;
 }
 

@@ -424,7 +424,16 @@ static sdot_status run_eval(sdot_ctx *c, const EvalArgs &a, bool dense, const do
     mark(1);
     int64_t nval = 0;
     int nks = 1;
-    if (dense) {
+    if (c->distance == 1) {
+        // spherical distance: its own sweeps over every (point, target) pair
+        mark(7);
+        sdot_status s = run_spherical(c, a, c->current_distance_threshold, &nval);
+        if (s != SDOT_OK) return s;
+        mark(2);
+        mark(3);
+        c->klaunch[2] += 1;
+        c->klaunch[3] += 1;
+    } else if (dense) {
         const DenseShape ds = dense_shape(a.nq, a.nt);
         nval = ds.nval;
         if (ds.nvs > 1) {
@@ -463,7 +472,7 @@ static sdot_status run_eval(sdot_ctx *c, const EvalArgs &a, bool dense, const do
     k_finalize_scalars<<<1, FIN_SCALAR_THREADS, 0, st>>>(FIN_BLOCKS, c->redpart.p, nval, c->blkpart.p, c->scal.p);
     mark(4);
     c->klaunch[1] += 1;
-    if (dense) {
+    if (dense && c->distance == 0) {
         c->klaunch[2] += 1;
         c->klaunch[3] += 1;
     }
@@ -476,6 +485,8 @@ sdot_status evaluate_internal(sdot_ctx *c, const double *p_dir, double comp_tol,
     if (c->dim == 0 || c->nq == 0) return set_error(c, SDOT_ESTATE, "source measure not set");
     if (c->nt == 0) return set_error(c, SDOT_ESTATE, "target measure not set");
     const sdot_solver_params &p = c->prm;
+    if (c->distance == 1 && p.threshold_type != SDOT_THRESH_POINTWISE)
+        return set_error(c, SDOT_EINVAL, "the spherical distance is supported with the pointwise threshold");
     // threshold (host, exact libm), from device max/min of psi
     double r = DBL_MAX;
     const bool may_truncate = (p.threshold_type != SDOT_THRESH_POINTWISE) ||
@@ -681,6 +692,7 @@ extern "C" sdot_status sdot_evaluate_device_noalloc(sdot_ctx *c, const double *p
     if (p.threshold_type != SDOT_THRESH_POINTWISE || p.tau > 0)
         return set_error(c, SDOT_EINVAL,
                          "no-alloc evaluation covers untruncated problems only (pointwise threshold, tau <= 0)");
+    if (c->distance != 0) return set_error(c, SDOT_EINVAL, "no-alloc evaluation covers the euclidean distance only");
     const NoallocLayout L = noalloc_layout(c->nq, c->nt);
     const size_t need = (size_t)L.total * sizeof(double);
     if (need > NOALLOC_BYTES)

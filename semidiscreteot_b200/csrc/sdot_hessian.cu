@@ -200,6 +200,7 @@ sdot_status hessian_device(sdot_ctx *c, const double *psi_dev, void *H_dev, int 
 {
     if (method != SDOT_HESS_AUTO && method != SDOT_HESS_FP64 && method != SDOT_HESS_TENSOR)
         return set_error(c, SDOT_EINVAL, "unknown Hessian method");
+    if (c->distance != 0) return set_error(c, SDOT_EINVAL, "the Hessian supports the euclidean distance only");
     sdot_status s = launch_gather(c, c->psi.p, psi_dev, c->nt);
     if (s != SDOT_OK) return s;
     double ems = 0, hms = 0;
@@ -267,6 +268,7 @@ extern "C" sdot_status sdot_hessian_tiles_device(sdot_ctx *c, const double *psi_
 {
     if (!c || !psi_dev || !H_dev) return SDOT_EINVAL;
     if (c->nq == 0 || c->nt == 0) return sdot::set_error(c, SDOT_ESTATE, "measures not set");
+    if (c->distance != 0) return sdot::set_error(c, SDOT_EINVAL, "the Hessian supports the euclidean distance only");
     const int64_t nt = sdot::hessian_tc_tiles(c->nt);
     if (tile_begin < 0 || tile_end < tile_begin || tile_end > nt)
         return sdot::set_error(c, SDOT_EINVAL, "tile range outside [0, sdot_hessian_tile_count]");
@@ -311,6 +313,7 @@ extern "C" sdot_status sdot_hessian(sdot_ctx *c, const double *psi, double *H)
 {
     if (!c || !psi || !H) return SDOT_EINVAL;
     if (c->nq == 0 || c->nt == 0) return sdot::set_error(c, SDOT_ESTATE, "measures not set");
+    if (c->distance != 0) return sdot::set_error(c, SDOT_EINVAL, "the Hessian supports the euclidean distance only");
     int prev = -1;
     cudaGetDevice(&prev);
     if (prev != c->device) cudaSetDevice(c->device);

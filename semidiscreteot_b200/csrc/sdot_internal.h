@@ -189,6 +189,7 @@ struct sdot_ctx {
     sdot::DevBuf<int> htc_tiles, htc_err;
     double hess_kernel_ms = 0.0;
     int64_t hess_tiles = 0;
+    int distance = 0;                  // distance function: 0 euclidean, 1 spherical (sdot_set_distance_function)
     int hess_chunk = 64;               // stages (x 64 points) per FP32 accumulation chunk
     long long hess_wait_limit = 0;     // SM clocks per stage-loop mbarrier wait (<= 0: the default, ~1 s)
     double newton_reuse = 0.1;         // lagged-Hessian contraction threshold (0: recompute every step)
@@ -233,6 +234,9 @@ sdot_status launch_minmax(sdot_ctx *c, const double *v, int64_t n, double *mx, d
 struct EvalArgs;
 // truncated evaluation (block-pair lists, fused sweeps, partial reduction)
 sdot_status run_trunc(sdot_ctx *c, const EvalArgs &a, double r);
+// value and gradient sweeps with the spherical distance (sdot_spherical.cu);
+// *nval: the value blocks whose partials k_finalize_scalars sums
+sdot_status run_spherical(sdot_ctx *c, const EvalArgs &a, double r, int64_t *nval);
 // dense-layout tpack for the current psi (used by the Hessian)
 void launch_target_prep_dense(sdot_ctx *c, const EvalArgs &a);
 

@@ -248,6 +248,7 @@ extern "C" sdot_status sdot_solve_newton(sdot_ctx *c, double *psi, const sdot_so
                                          int hessian_method, sdot_newton_info *info)
 {
     if (!c || !psi) return SDOT_EINVAL;
+    if (c->distance != 0) return sdot::set_error(c, SDOT_EINVAL, "Newton supports the euclidean distance only");
     if (hessian_method != SDOT_HESS_AUTO && hessian_method != SDOT_HESS_FP64 && hessian_method != SDOT_HESS_TENSOR)
         return set_error(c, SDOT_EINVAL, "unknown Hessian method");
     if (params) {

@@ -287,6 +287,8 @@ extern "C" sdot_status sdot_softmax_refinement(sdot_ctx *c, const double *psi_co
                                               const int64_t *child_offsets, const int64_t *child_indices,
                                               double *psi_fine)
 {
+    if (c && c->distance != 0)
+        return sdot::set_error(c, SDOT_EINVAL, "the softmax refinement supports the euclidean distance only");
     if (!c || !psi_coarse || !y_fine || !child_offsets || !child_indices || !psi_fine || n_fine <= 0)
         return SDOT_EINVAL;
     if (c->nq == 0 || c->nt == 0) return set_error(c, SDOT_ESTATE, "measures not set (the targets are the coarse level)");

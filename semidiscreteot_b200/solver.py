@@ -115,7 +115,9 @@ class SotSolver:
         self._check(self._L.sdot_configure(self._h, C.byref(cp)))
 
     def set_distance_function(self, name: str):
+        """SotSolver::set_distance_function: "euclidean" or "spherical"."""
         self._check(self._L.sdot_set_distance_function(self._h, name.encode()))
+        self.distance = name
 
     # ------------------------------------------------------------- hot path
     def evaluate_functional(self, potential, gradient_out: Optional[np.ndarray] = None) -> float:
@@ -229,16 +231,33 @@ class SotSolver:
                                                     ci.ctypes.data, out.ctypes.data))
         return out
 
-    def evaluate_weighted_barycenters(self, potential, params: Optional[SolverParameters] = None) -> np.ndarray:
-        """SotSolver::evaluate_weighted_barycenters, euclidean distance (SotSolver.cc:584-660,
-        871-971): barycenter_j = sum_q rho_q JxW_q pi_qj x_q / nu_j at the given potentials,
-        threshold recomputed there; (n_targets, dim).  `params` configures the solver first;
-        the computation reads the configured epsilon as the reference's current_params does."""
+    def evaluate_weighted_barycenters(self, potential, params: Optional[SolverParameters] = None,
+                                      barycenters=None) -> np.ndarray:
+        """SotSolver::evaluate_weighted_barycenters (SotSolver.cc:584-660).  Euclidean distance
+        (:871-971): barycenter_j = sum_q rho_q JxW_q pi_qj x_q / nu_j at the given potentials,
+        threshold recomputed there.  Spherical distance (:612-650, 662-767): Riemannian gradient
+        steps from `barycenters` (the starting points, as the reference's barycenters_out) with
+        the parameters' tolerance and max_iterations; the iterations run and the last gradient
+        norm are left in last_barycenter_info.  Returns (n_targets, dim).  `params` configures
+        the solver first; the computation reads the configured epsilon as the reference's
+        current_params does."""
         if params is not None:
             self.configure(params)
         psi = _f64(potential)
         if psi.size != self._n_targets:
             raise ValueError("potential size differs from the number of targets")
+        if getattr(self, "distance", "euclidean") == "spherical":
+            if barycenters is None:
+                raise ValueError("the spherical barycenter iteration needs starting points")
+            b = np.array(barycenters, dtype=np.float64, copy=True).reshape(self._n_targets, self.dim)
+            it = C.c_uint(0)
+            nrm = C.c_double(0.0)
+            p = self.current_params
+            self._check(self._L.sdot_weighted_barycenters_spherical(self._h, psi.ctypes.data, b.ctypes.data,
+                                                                     int(p.max_iterations), float(p.tolerance),
+                                                                     C.byref(it), C.byref(nrm)))
+            self.last_barycenter_info = {"iterations": int(it.value), "grad_norm": float(nrm.value)}
+            return b
         out = np.empty((self._n_targets, self.dim))
         self._check(self._L.sdot_weighted_barycenters(self._h, psi.ctypes.data, out.ctypes.data))
         return out

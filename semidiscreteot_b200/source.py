@@ -92,3 +92,42 @@ def structured_source(dim: int, n: int, order: int, lo: float = 0.0, hi: float =
     offsets = np.arange(ncell + 1, dtype=np.int64) * qpc
     return {"x": np.ascontiguousarray(x), "jxw": jxw, "density": rho, "cell_offsets": offsets,
             "cell_centers": np.ascontiguousarray(centers), "nodal": nodal, "dim": dim, "n": n, "order": order}
+
+
+def sphere_source(n_theta: int, n_phi: int, order: int, theta_max: float = np.pi, density=None,
+                  normalize: bool = True) -> dict:
+    """Quadrature data of the spherical cap {polar angle <= theta_max} of the
+    unit sphere (the whole sphere at pi), for the spherical distance.
+
+    Cells are the (polar angle, azimuth) rectangles of an n_theta x n_phi
+    grid; each holds order^2 Gauss points of the rectangle mapped to the
+    sphere, with JxW = Gauss weight x cell extents x sin(polar angle) (the
+    area element), and the cell centre is the image of the rectangle's centre.
+    density: a callable f(points) at the quadrature points, or None for a
+    uniform density; normalised by sum_q |rho_q| JxW_q like the structured
+    sources.  Returns the layout of structured_source (points in 3D)."""
+    g, w = gauss_legendre01(order)
+    ht, hp = theta_max / n_theta, 2.0 * np.pi / n_phi
+    T0, P0 = np.meshgrid(np.arange(n_theta) * ht, np.arange(n_phi) * hp, indexing="ij")
+    T0, P0 = T0.ravel(), P0.ravel()
+    gt, gp = np.meshgrid(g, g, indexing="ij")
+    wt = np.outer(w, w).ravel()
+    th = T0[:, None] + gt.ravel()[None, :] * ht          # (ncell, order^2)
+    ph = P0[:, None] + gp.ravel()[None, :] * hp
+
+    def to_xyz(t, p):
+        return np.stack([np.sin(t) * np.cos(p), np.sin(t) * np.sin(p), np.cos(t)], axis=-1)
+
+    x = to_xyz(th, ph).reshape(-1, 3)
+    jxw = (wt[None, :] * ht * hp * np.sin(th)).ravel()
+    centers = to_xyz(T0 + 0.5 * ht, P0 + 0.5 * hp)
+    rho = np.ones(x.shape[0]) if density is None else np.asarray(density(x), dtype=np.float64)
+    if normalize:
+        l1 = np.sum(np.abs(rho) * jxw)
+        if l1 > 0:
+            rho = rho / l1
+    qpc = order * order
+    ncell = T0.size
+    return {"x": np.ascontiguousarray(x), "jxw": jxw, "density": rho,
+            "cell_offsets": np.arange(ncell + 1, dtype=np.int64) * qpc,
+            "cell_centers": np.ascontiguousarray(centers), "dim": 3, "order": order}
