@@ -1238,12 +1238,19 @@ sdot_status run_trunc(sdot_ctx *c, const EvalArgs &a, double r)
                                                                              nts, cr, c->superpair.p);
     k_super_compact<<<(unsigned)(((int64_t)nss * 32 + 255) / 256), 256, 0, st>>>(c->superpair.p, nss, nts, c->shit.p,
                                                                               c->scount.p, c->spidx.p);
-    std::vector<int> sc((size_t)nss);
-    e = cudaMemcpyAsync(sc.data(), c->scount.p, nss * sizeof(int), cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return cuda_error(c, e, "pair list count");
-    int hmax = 1;
-    for (int v : sc) hmax = std::max(hmax, v);
+    // Row length of the per-block pair masks: the most target super-blocks any
+    // source super-block pairs with.  Every count is at most nts, so when the
+    // nts-wide rows are small (<= 128 MiB for both arrays) they are used as
+    // they are and the counts are not read back (one host round trip fewer).
+    int hmax = std::max(1, nts);
+    if ((size_t)nsb * (size_t)nts * 2 * sizeof(int) > ((size_t)128 << 20)) {
+        std::vector<int> sc((size_t)nss);
+        e = cudaMemcpyAsync(sc.data(), c->scount.p, nss * sizeof(int), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return cuda_error(c, e, "pair list count");
+        hmax = 1;
+        for (int v : sc) hmax = std::max(hmax, v);
+    }
     e = c->pmask.alloc((size_t)nsb * hmax);
     if (e == cudaSuccess) e = c->pmpre.alloc((size_t)nsb * hmax);
     if (e != cudaSuccess) return cuda_error(c, e, "pair mask alloc");
