@@ -211,7 +211,8 @@ size_t device_bytes(const sdot_ctx *c)
            c->io_a.bytes() +
            c->io_b.bytes() + c->x0.bytes() + c->pdir.bytes() + c->sk.bytes() + c->yk.bytes() + c->hist_s.bytes() +
            c->hist_y.bytes() + c->gtmp.bytes() + c->htc_tdat.bytes() + c->htc_diag.bytes() + c->htc_blk.bytes() +
-           c->htc_scr.bytes() + c->htc_qa.bytes() + c->htc_qb.bytes() + c->htc_tiles.bytes() + c->htc_err.bytes();
+           c->htc_scr.bytes() + c->htc_qa.bytes() + c->htc_qb.bytes() + c->htc_tiles.bytes() + c->htc_err.bytes() +
+           c->htc_cd.bytes() + c->htc_qw.bytes();
 }
 
 }  // namespace

@@ -302,6 +302,14 @@ extern "C" sdot_status sdot_set_hessian_chunk(sdot_ctx *c, int stages)
     return SDOT_OK;
 }
 
+extern "C" sdot_status sdot_set_hessian_generation(sdot_ctx *c, int factored, int *last_factored)
+{
+    if (!c) return SDOT_EINVAL;
+    if (factored >= 0) c->hess_factored = factored != 0;
+    if (last_factored) *last_factored = c->hess_last_factored ? 1 : 0;
+    return SDOT_OK;
+}
+
 extern "C" sdot_status sdot_set_hessian_wait_limit(sdot_ctx *c, int64_t clocks)
 {
     if (!c) return SDOT_EINVAL;

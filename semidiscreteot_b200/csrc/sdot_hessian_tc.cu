@@ -248,9 +248,21 @@ struct Args {
     void *H;
     int *err;
     long long wait_limit;   // SM clocks a stage-loop wait may take before the kernel aborts
+    // factored generation (2 x 2 x 2 Gauss cells, one per 8-point chunk):
+    const float4 *cd;       // per chunk: {dc (3), F_c^B}, {a (3), F_c^A}: cell centre - c_b, half spacing, max F
+    const float2 *qw;       // per q: {2^(F^B - F_c^B), 2^(F^A - F_c^A)}
 };
 
-template <int DIM, typename OutT>
+// FACT: the stage's 8-point chunks are 2 x 2 x 2 Gauss cells (x fastest,
+// offsets +-a about the cell centre), so per (row, cell)
+//   2^(E + F_q + G.d_q) = 2^(E + G.dc - G.a + F_c) * prod_d r_d^(i_d) * 2^(F_q - F_c),
+//   r_d = 2^(2 G_d a_d), i_d the point's index bit along d, F_c = max_q F_q,
+// one ex2 for the cell and one per dimension instead of one per point; the
+// point factors 2^(F_q - F_c) <= 1 are formed once per point (k_htc_points).
+// Every intermediate is a corner value 2^(E + G.d_q + F_c), within
+// prod_d r_d^(+-1) of the cell's largest value, so none leaves FP32 where
+// the per-point form would not.
+template <int DIM, typename OutT, bool FACT>
 __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
 {
     extern __shared__ uint8_t smem_raw[];
@@ -292,11 +304,18 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
             pt = a.tdat[j];
         }
     };
-    auto raw_copy = [&](int buf, int st) {   // 2 + 64 + 16 copies of 16 bytes
+    auto raw_copy = [&](int buf, int st) {   // 2 + 64 + 16 copies of 16 bytes (FACT: 2 + 16 + 32)
         const uint32_t d = rawb_s + buf * RAW_BYTES;
         if (tid < 2) cp_async16(d + tid * 16, reinterpret_cast<const uint8_t *>(a.blk + st) + tid * 16);
-        else if (tid < 2 + KQ) cp_async16(d + 32 + (tid - 2) * 16, a.qa + (int64_t)st * KQ + (tid - 2));
-        else if (tid < 2 + KQ + KQ / 4) cp_async16(d + 32 + KQ * 16 + (tid - 2 - KQ) * 16, a.qb + (int64_t)st * KQ + (tid - 2 - KQ) * 4);
+        else if constexpr (FACT) {
+            // chunk data: 8 chunks x 2 float4; point factors: 64 float2 = 32 x 16 bytes
+            if (tid < 2 + 16) cp_async16(d + 32 + (tid - 2) * 16, a.cd + (int64_t)st * 16 + (tid - 2));
+            else if (tid < 2 + 16 + 32)
+                cp_async16(d + 32 + 256 + (tid - 18) * 16, a.qw + (int64_t)st * KQ + (tid - 18) * 2);
+        } else {
+            if (tid < 2 + KQ) cp_async16(d + 32 + (tid - 2) * 16, a.qa + (int64_t)st * KQ + (tid - 2));
+            else if (tid < 2 + KQ + KQ / 4) cp_async16(d + 32 + KQ * 16 + (tid - 2 - KQ) * 16, a.qb + (int64_t)st * KQ + (tid - 2 - KQ) * 4);
+        }
         cp_async_commit();
     };
     auto stage_store = [&](int buf) {         // raw[buf] + pt -> Eg / qs [buf]
@@ -309,6 +328,19 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
             float4 *dst = reinterpret_cast<float4 *>(Eg + (buf * ROWS + tid) * 8);
             dst[0] = make_float4(e, e, gx, gx);
             dst[1] = make_float4(gy, gy, gz, gz);
+        } else if constexpr (FACT) {
+            // chunk layout in qs: [0, 3) dc, 3 F_c^B, [4, 7) a, 7 F_c^A,
+            // [8, 16) 2^(F^B - F_c^B), [16, 24) 2^(F^A - F_c^A)
+            if (tid < ROWS + KQ) {
+                const int p = tid - ROWS;
+                const float2 wv = reinterpret_cast<const float2 *>(rb + 32 + 256)[p];
+                float *d = qs + (buf * 8 + (p >> 3)) * QS_STRIDE + (p & 7);
+                d[8] = wv.x;
+                d[16] = wv.y;
+            } else {
+                const int t = tid - ROWS - KQ;       // 64 threads: chunk t >> 3, float t & 7
+                qs[(buf * 8 + (t >> 3)) * QS_STRIDE + (t & 7)] = reinterpret_cast<const float *>(rb + 32)[t];
+            }
         } else if (tid < ROWS + KQ) {
             const int p = tid - ROWS;            // point p of the stage: K-chunk p >> 3, slot p & 7
             const float4 pq = reinterpret_cast<const float4 *>(rb + 32)[p];
@@ -378,6 +410,70 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
                 // cvt; widened back (shift / mask), lo = v - hi is exact
                 const uint32_t hp = bf16x2_rn(v0, v1);
                 const f2 lo = sub2(pack2(v0, v1), pack2(__uint_as_float(hp << 16), __uint_as_float(hp & 0xffff0000u)));
+                float l0, l1;
+                unpack2(lo, l0, l1);
+                hw[k] = hp;
+                lw[k] = __byte_perm(__float_as_uint(l0), __float_as_uint(l1), 0x7632);
+            }
+            const int rr = isA ? r : r - M;
+            const uint32_t off = (uint32_t)(rr >> 3) * 1024u + (uint32_t)(rr & 7) * 128u + ((uint32_t)(kc ^ (rr & 7)) << 4);
+            uint8_t *hi = stage + (isA ? 0u : 2u * A_BYTES);
+            uint8_t *lo = hi + (isA ? A_BYTES : B_BYTES);
+            *reinterpret_cast<uint4 *>(hi + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+            *reinterpret_cast<uint4 *>(lo + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+        }
+    };
+
+    // ---- factored generation (FACT): per (row, cell) one ex2 for the cell and
+    // one per dimension; the 8 values by products with the point factors ----
+    auto generate_fact = [&](int buf) {
+        const float *qc = qs + (buf * 8 + kc) * QS_STRIDE;
+        const float4 dc4 = *reinterpret_cast<const float4 *>(qc);
+        const float4 a4 = *reinterpret_cast<const float4 *>(qc + 4);
+        f2 wb[4], wa[4];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const float4 b4 = *reinterpret_cast<const float4 *>(qc + 8 + 4 * h);
+            const float4 c4 = *reinterpret_cast<const float4 *>(qc + 16 + 4 * h);
+            wb[2 * h] = pack2(b4.x, b4.y);
+            wb[2 * h + 1] = pack2(b4.z, b4.w);
+            wa[2 * h] = pack2(c4.x, c4.y);
+            wa[2 * h + 1] = pack2(c4.z, c4.w);
+        }
+        uint8_t *stage = sm + buf * STAGE_BYTES;
+        const float4 *eg0 = reinterpret_cast<const float4 *>(Eg + (buf * ROWS + rg) * 8);
+        float4 e0 = eg0[0], e1 = eg0[1];
+#pragma unroll
+        for (int it = 0; it < RPT; ++it) {
+            const bool isA = it < ARPT;
+            const int r = rg + RG * it;
+            const float E = e0.x, Gx = e0.z, Gy = e1.x, Gz = e1.z;
+            if (it + 1 < RPT) {
+                const float4 *egn = reinterpret_cast<const float4 *>(Eg + (buf * ROWS + r + RG) * 8);
+                e0 = egn[0];
+                e1 = egn[1];
+            }
+            const float gx = Gx * a4.x, gy = Gy * a4.y, gz = Gz * a4.z;
+            float ub = fmaf(Gx, dc4.x, E);
+            ub = fmaf(Gy, dc4.y, ub);
+            ub = fmaf(Gz, dc4.z, ub);
+            ub = ub - (gx + gy + gz) + (isA ? a4.w : dc4.w);
+            const float B = ex2_approx(ub);
+            const float r0 = ex2_approx(gx + gx), r1 = ex2_approx(gy + gy), r2 = ex2_approx(gz + gz);
+            // corners in point order (x fastest): c_q = B * prod_d r_d^(bit d of q)
+            f2 cp[4];
+            cp[0] = pack2(B, B * r0);
+            cp[1] = mul2(cp[0], pack2(r1, r1));
+            cp[2] = mul2(cp[0], pack2(r2, r2));
+            cp[3] = mul2(cp[1], pack2(r2, r2));
+            uint32_t hw[4], lw[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const f2 v = mul2(cp[k], isA ? wa[k] : wb[k]);
+                float v0, v1;
+                unpack2(v, v0, v1);
+                const uint32_t hp = bf16x2_rn(v0, v1);
+                const f2 lo = sub2(v, pack2(__uint_as_float(hp << 16), __uint_as_float(hp & 0xffff0000u)));
                 float l0, l1;
                 unpack2(lo, l0, l1);
                 hw[k] = hp;
@@ -470,7 +566,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
             raw_copy(sb, (st + 2) % a.nst);     // inputs of stage g + 2 (its point block)
             // the MMAs that read this buffer two stages ago must be complete
             if (g >= 2 && !mbar_wait(bar0 + 8 * sb, ((g >> 1) - 1) & 1, a.wait_limit)) bad = true;
-            generate(sb);
+            if constexpr (FACT) generate_fact(sb);
+            else generate(sb);
             if (has_next) {
                 if (last_of_tile) load_target(tl_nxt);   // once per tile
                 stage_store(sb ^ 1);
@@ -563,7 +660,8 @@ __global__ void k_htc_targets(int64_t n, int64_t npad, const double *__restrict_
 template <int DIM>
 __global__ void k_htc_points(int64_t nq, int nst, const double *__restrict__ x, const double *__restrict__ Lq,
                              const double *__restrict__ w, double ox, double oy, double oz, double l2e_eps,
-                             float4 *__restrict__ qa, float *__restrict__ qb, double4 *__restrict__ blk)
+                             float4 *__restrict__ qa, float *__restrict__ qb, double4 *__restrict__ blk,
+                             float4 *__restrict__ cd, float2 *__restrict__ qw)
 {
     const int lane = threadIdx.x & 31;
     const int b = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
@@ -617,6 +715,41 @@ __global__ void k_htc_points(int64_t nq, int nst, const double *__restrict__ x, 
         }
         qa[q] = out;
         qb[q] = fa;
+        if (cd) {
+            // factored generation: per 8-point chunk (a 2 x 2 x 2 cell, all
+            // points valid or none) its centre relative to c_b, its half
+            // spacing per dimension and the largest F^B, F^A of its points,
+            // rounded to FP32 first so that F_c + (F - F_c) is exact
+            const double fbv = fin[h] ? (double)out.w : -CUDART_INF, fav = (double)fa;
+            double clo[3], chi[3], mb = fbv, ma = fav;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) clo[d] = chi[d] = xt[h][d];
+#pragma unroll
+            for (int o2 = 1; o2 < 8; o2 <<= 1) {
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    clo[d] = fmin(clo[d], __shfl_xor_sync(0xffffffffu, clo[d], o2));
+                    chi[d] = fmax(chi[d], __shfl_xor_sync(0xffffffffu, chi[d], o2));
+                }
+                mb = fmax(mb, __shfl_xor_sync(0xffffffffu, mb, o2));
+                ma = fmax(ma, __shfl_xor_sync(0xffffffffu, ma, o2));
+            }
+            const float mbf = (float)mb, maf = (float)ma;
+            qw[q] = make_float2(fbv > -CUDART_INF ? (float)exp2(fbv - (double)mbf) : 0.f,
+                                fav > -CUDART_INF ? (float)exp2(fav - (double)maf) : 0.f);
+            if ((lane & 7) == 0) {
+                const int64_t k = (int64_t)b * 8 + ((lane + 32 * h) >> 3);
+                float4 m4 = make_float4(0.f, 0.f, 0.f, -CUDART_INF_F), s4 = m4;
+                if (valid[h]) {
+                    m4 = make_float4((float)(0.5 * (clo[0] + chi[0]) - cb[0]), (float)(0.5 * (clo[1] + chi[1]) - cb[1]),
+                                     (float)(0.5 * (clo[2] + chi[2]) - cb[2]), mbf);
+                    s4 = make_float4((float)(0.5 * (chi[0] - clo[0])), (float)(0.5 * (chi[1] - clo[1])),
+                                     (float)(0.5 * (chi[2] - clo[2])), maf);
+                }
+                cd[2 * k] = m4;
+                cd[2 * k + 1] = s4;
+            }
+        }
     }
     if (lane == 0) blk[b] = make_double4(cb[0], cb[1], cb[2], lref);
 }
@@ -669,7 +802,16 @@ sdot_status hessian_tc(sdot_ctx *c, void *H_dev, bool out_f32, int chunk_stages,
     if (e == cudaSuccess) e = c->htc_tiles.alloc(tiles.size() * 2);
     if (e == cudaSuccess) e = c->htc_scr.alloc((size_t)grid * SCR_PER_CTA);
     if (e == cudaSuccess) e = c->htc_err.alloc(1);
+    // Factored generation: 2 x 2 x 2 Gauss cells (8-point chunks of the
+    // 64-point stages), with the per-dimension factors r_d = 2^(2 G_d a_d)
+    // bounded by 2^16 (|G| <= l2e_eps diam), so no product leaves FP32.
+    const bool fact = c->hess_factored && c->dim == 3 && c->tensor_m == 2 && c->qpc == 8 &&
+                      2.0 * (LOG2E / c->prm.epsilon) * c->diam * c->tensor_amax <= 16.0;
+    if (e == cudaSuccess && fact) e = c->htc_cd.alloc((size_t)nst * 16 * 4);
+    if (e == cudaSuccess && fact) e = c->htc_qw.alloc((size_t)nst * KQ * 2);
     if (e != cudaSuccess) return cuda_error(c, e, "tensor-core Hessian buffers");
+    float4 *cdp = fact ? reinterpret_cast<float4 *>(c->htc_cd.p) : nullptr;
+    float2 *qwp = fact ? reinterpret_cast<float2 *>(c->htc_qw.p) : nullptr;
     e = cudaMemcpyAsync(c->htc_tiles.p, tiles.data(), tiles.size() * sizeof(int2), cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(c->htc_err.p, 0, sizeof(int), c->stream);
     if (e != cudaSuccess) return cuda_error(c, e, "tensor-core Hessian setup");
@@ -686,12 +828,12 @@ sdot_status hessian_tc(sdot_ctx *c, void *H_dev, bool out_f32, int chunk_stages,
         k_htc_targets<2><<<tgrid, 256, 0, c->stream>>>(n, npad, c->y.p, c->nu.p, c->psi.p, c->grad.p, c->perm.p, o[0],
                                                        o[1], o[2], l2e_eps, tdat, c->htc_diag.p);
         k_htc_points<2><<<pgrid, 256, 0, c->stream>>>(c->nq, (int)nst, c->x.p, c->Lq.p, c->w.p, o[0], o[1], o[2],
-                                                      l2e_eps, qa, c->htc_qb.p, blk);
+                                                      l2e_eps, qa, c->htc_qb.p, blk, nullptr, nullptr);
     } else {
         k_htc_targets<3><<<tgrid, 256, 0, c->stream>>>(n, npad, c->y.p, c->nu.p, c->psi.p, c->grad.p, c->perm.p, o[0],
                                                        o[1], o[2], l2e_eps, tdat, c->htc_diag.p);
         k_htc_points<3><<<pgrid, 256, 0, c->stream>>>(c->nq, (int)nst, c->x.p, c->Lq.p, c->w.p, o[0], o[1], o[2],
-                                                      l2e_eps, qa, c->htc_qb.p, blk);
+                                                      l2e_eps, qa, c->htc_qb.p, blk, cdp, qwp);
     }
     Args a{};
     a.qa = qa;
@@ -710,9 +852,13 @@ sdot_status hessian_tc(sdot_ctx *c, void *H_dev, bool out_f32, int chunk_stages,
     a.H = H_dev;
     a.err = c->htc_err.p;
     a.wait_limit = c->hess_wait_limit > 0 ? c->hess_wait_limit : WAIT_LIMIT;
+    a.cd = cdp;
+    a.qw = qwp;
     void (*kern)(const Args) = nullptr;
-    if (c->dim == 2) kern = out_f32 ? k_hessian_tc<2, float> : k_hessian_tc<2, double>;
-    else kern = out_f32 ? k_hessian_tc<3, float> : k_hessian_tc<3, double>;
+    if (c->dim == 2) kern = out_f32 ? k_hessian_tc<2, float, false> : k_hessian_tc<2, double, false>;
+    else if (fact) kern = out_f32 ? k_hessian_tc<3, float, true> : k_hessian_tc<3, double, true>;
+    else kern = out_f32 ? k_hessian_tc<3, float, false> : k_hessian_tc<3, double, false>;
+    c->hess_last_factored = fact;
     e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES);
     if (e != cudaSuccess) return cuda_error(c, e, "tensor-core Hessian attribute");
     if (c->profiling) cudaEventRecord(c->pev[0], c->stream);

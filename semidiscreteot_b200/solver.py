@@ -335,6 +335,15 @@ class SotSolver:
         """Stages of 64 points accumulated in FP32 between FP64 drains (tensor Hessian)."""
         self._check(self._L.sdot_set_hessian_chunk(self._h, int(stages)))
 
+    def set_hessian_generation(self, factored: Optional[bool] = None) -> bool:
+        """Factored operand generation of the tensor Hessian on 2x2x2 Gauss cells
+        (True: where it applies, the default; False: never; None: unchanged).
+        Returns whether the last tensor Hessian used it."""
+        last = C.c_int(0)
+        self._check(self._L.sdot_set_hessian_generation(self._h, -1 if factored is None else int(bool(factored)),
+                                                        C.byref(last)))
+        return bool(last.value)
+
     def set_hessian_wait_limit(self, clocks: int):
         """SM clocks a device-side wait of the tensor Hessian may take before the
         call fails with SDOT_ETIMEOUT (<= 0: the default, about 1 s)."""

@@ -168,3 +168,51 @@ def test_wait_timeout_reports_and_recovers():
     s.evaluate_functional(psi, g)
     assert np.all(np.isfinite(g))
     s.close()
+
+
+
+def test_factored_generation_matches_per_point(oracle_mod):
+    """On 2 x 2 x 2 Gauss cells the tensor Hessian's operands are generated
+    per cell (one ex2 for the cell and one per dimension, the 8 values by
+    products); the result agrees with the per-point generation and with the
+    FP64 oracle within the tensor method's bounds.  11^3 cells (10,648 points,
+    not a multiple of the 64-point stage), 501 targets, eps = 1.5e-2: the
+    per-dimension factors stay within 2^9."""
+    rng = np.random.default_rng(2)
+
+    def dens(p):
+        return np.exp(-np.sum((p - 0.3) ** 2, axis=1) / (2 * 0.15 ** 2)) + 0.05
+
+    src = structured_source(3, 11, 2, nodal_density=dens)
+    N, eps = 501, 1.5e-2
+    y = rng.random((N, 3))
+    nu = rng.dirichlet(np.ones(N) * 4)
+    s = make(src, y, nu, eps)
+    psi = 0.2 * eps * rng.standard_normal(N)
+    Hf, _ = hessian(s, psi, "tensor")
+    assert s.set_hessian_generation(None) is True
+    s.set_hessian_generation(False)
+    Hp, _ = hessian(s, psi, "tensor")
+    assert s.set_hessian_generation(None) is False
+    s.set_hessian_generation(True)
+    P = oracle_mod.Problem(src["x"], src["jxw"], src["density"], src["cell_offsets"], src["cell_centers"], y, nu)
+    Ho = P.hessian(psi, oracle_mod.Params(epsilon=eps, tau=0.0, use_log_sum_exp=True), 1e300)
+    for H in (Hf, Hp):
+        fro, mx = rel_errors(H, Ho)
+        print(f"tensor Hessian vs FP64: Frobenius {fro:.2e}, max {mx:.2e}")
+        assert fro <= FRO_TOL and mx <= MAX_TOL, (fro, mx)
+        assert np.array_equal(H, H.T)
+    Hf2, _ = hessian(s, psi, "tensor")
+    assert np.array_equal(Hf, Hf2)
+    s.close()
+
+
+def test_factored_generation_not_used_outside_its_bound():
+    """7^3 cells at eps = 1e-2: a per-dimension factor could reach 2^20.6, so
+    the per-point generation runs even though the cells are Gauss grids."""
+    src, y, nu, eps = problem("dense3d", seed=2)
+    s = make(src, y, nu, eps)
+    psi = np.zeros(len(nu))
+    hessian(s, psi, "tensor")
+    assert s.set_hessian_generation(None) is False
+    s.close()
