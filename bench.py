@@ -392,24 +392,33 @@ def measure_single(wl, precision, steps, warmup, local, clk, flush, e2e=True):
     for _ in range(max(3, warmup)):
         solver.evaluate_functional_device(psi.data_ptr(), grad.data_ptr())
     torch.cuda.synchronize()
-    solver.set_profiling(True)
-    solver.kernel_times(reset=True)
-    times = []
-    torch.cuda.synchronize()
-    with clk.region():
-        for _ in range(steps):
-            with torch.cuda.stream(stream):
-                flush.fill_(1.0)
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            solver.evaluate_functional_device(psi.data_ptr(), grad.data_ptr())
-            e1.record(stream)
-            e1.synchronize()
-            times.append(e0.elapsed_time(e1))
+
+    def timed(profiled):
+        solver.set_profiling(profiled)
+        solver.kernel_times(reset=True)
+        ts = []
         torch.cuda.synchronize()
-    kt = solver.kernel_times(reset=True)
-    solver.set_profiling(False)
+        with clk.region():
+            for _ in range(steps):
+                with torch.cuda.stream(stream):
+                    flush.fill_(1.0)
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                solver.evaluate_functional_device(psi.data_ptr(), grad.data_ptr())
+                e1.record(stream)
+                e1.synchronize()
+                ts.append(e0.elapsed_time(e1))
+            torch.cuda.synchronize()
+        k = solver.kernel_times(reset=True)
+        solver.set_profiling(False)
+        return ts, k
+
+    # the step time without the library's per-phase events (which add a few
+    # microseconds per evaluation), then the same steps with them: the
+    # per-kernel CUDA-event times of the roofline and the launch count
+    times, _ = timed(False)
+    _, kt = timed(True)
     pairs = solver.last_eval_info["n_pairs"]
     ms = float(np.mean(times))
     out = {"value": pairs / (ms * 1e-3), "ms_per_step": ms, "pairs_per_step": pairs, "kt": kt,
@@ -672,6 +681,12 @@ def run_hessian_3d(args):
         for _ in range(args.steps):
             info = s.compute_hessian_device(psi.data_ptr(), H.data_ptr(), method="tensor", out_f32=True)
             ks.append(info["kernel_ms"])
+        factored = s.set_hessian_generation(None)
+        # the per-point operand generation on the same problem, for comparison
+        s.set_hessian_generation(False)
+        kp = [s.compute_hessian_device(psi.data_ptr(), H.data_ptr(), method="tensor", out_f32=True)["kernel_ms"]
+              for _ in range(2)]
+        s.set_hessian_generation(True)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         psi_n = s.solve_newton(np.zeros(N), prm, hessian="tensor")
@@ -701,7 +716,9 @@ def run_hessian_3d(args):
             "roofline": {"kernel": "k_hessian_tc (tcgen05 BF16 hi+lo, TMEM accumulators)", "bound": "tensor",
                          "achieved": ach, "peak": peak, "unit": "TFLOP/s",
                          "frac": (ach / peak) if peak else None, "traffic": None, "ms_per_launch": kms,
-                         "flops_per_launch": flops, "peak_source": mp["source"] + ": bf16_tflops (burst)"},
+                         "flops_per_launch": flops, "peak_source": mp["source"] + ": bf16_tflops (burst)",
+                         "operand_generation": "factored per 2x2x2 cell" if factored else "per point",
+                         "per_point_generation_ms_per_launch": float(np.mean(kp))},
             "fp64_lbfgs_baseline": base, "clocks": clk.summary()}
     print(json.dumps(line))
     return 0
@@ -875,12 +892,15 @@ def run_batched_2d(args):
 
 def serve_requests(n, seed=0, scale=1.0):
     """Config 5's request mix: 80% config-3-like (uniform density cube, uniform
-    targets, eps 5e-3), 20% 3D cubes with Gaussian-mixture targets and eps in
-    [1e-3, 1e-2]; sizes scaled by `scale` (cells per axis and targets)."""
+    targets, eps 5e-3, untruncated: Newton with the tensor-core Hessian), 20%
+    3D cubes with Gaussian-mixture targets and eps in [1e-3, 1e-2] at the
+    reference's default truncation tau = 1e-8 (so L-BFGS over truncated
+    evaluations); sizes scaled by `scale` (cells per axis and targets)."""
     from semidiscreteot_b200 import SolverParameters, structured_source
     rng = np.random.default_rng(seed)
     out = []
     for i in range(n):
+        tau, maxit, kind = 0.0, 2000, "config3"
         if rng.random() < 0.8:
             cells = max(4, int(round(32 * scale)))
             nt = max(64, int(20_000 * scale ** 3))
@@ -889,6 +909,7 @@ def serve_requests(n, seed=0, scale=1.0):
             nu = np.full(nt, 1.0 / nt)
             eps = 5e-3
         else:
+            tau, maxit, kind = 1e-8, 20000, "mixture_cube"
             cells = max(4, int(round(np.exp(rng.uniform(np.log(16), np.log(64))) * scale)))
             nt = max(64, int(np.exp(rng.uniform(np.log(5_000), np.log(50_000))) * scale ** 3))
             src = structured_source(3, cells, 2)
@@ -898,9 +919,9 @@ def serve_requests(n, seed=0, scale=1.0):
             y = np.clip(means[comp] + 0.1 * rng.standard_normal((nt, 3)), 0, 1)
             nu = rng.dirichlet(np.ones(nt))
             eps = float(np.exp(rng.uniform(np.log(1e-3), np.log(1e-2))))
-        prm = SolverParameters(epsilon=eps, tau=0.0, use_log_sum_exp_trick=True, tolerance=1e-8,
-                               solver_control_type="linf", max_iterations=2000)
-        out.append({"source": src, "y": y, "nu": nu, "params": prm, "method": "auto",
+        prm = SolverParameters(epsilon=eps, tau=tau, use_log_sum_exp_trick=True, tolerance=1e-8,
+                               solver_control_type="linf", max_iterations=maxit)
+        out.append({"source": src, "y": y, "nu": nu, "params": prm, "method": "auto", "kind": kind,
                     "eps_factor": 4.0, "eps_steps": 2 if eps < 5e-3 else 1, "inter_tol": 1e-6})
     return out
 
@@ -923,7 +944,12 @@ def run_serve_3d(args):
                        "scale": args.scale},
             "converged": conv, "latency_p50_ms": st["p50_ms"], "latency_p99_ms": st["p99_ms"],
             "latency_mean_ms": st["mean_ms"], "peak_concurrent": st["peak_running"],
-            "methods": [r["method"] for r in res], "clocks": clk.summary()}
+            "methods": [r["method"] for r in res], "clocks": clk.summary(),
+            "requests_detail": [{"kind": p["kind"], "n_q": int(p["source"]["jxw"].size), "n_t": int(len(p["nu"])),
+                                 "epsilon": p["params"].epsilon, "tau": p["params"].tau, "method": r["method"],
+                                 "iterations": int(r["iterations"]), "converged": bool(r["converged"]),
+                                 "queue_ms": round(r["queue_ms"], 1), "run_ms": round(r["run_ms"], 1)}
+                                for p, r in zip(reqs, res)]}
     print(json.dumps(line))
     return 0
 

@@ -452,6 +452,7 @@ void sdot_destroy(sdot_ctx *c)
         c->io_a.release(); c->io_b.release(); c->x0.release(); c->pdir.release(); c->sk.release(); c->yk.release();
         c->hist_s.release(); c->hist_y.release(); c->gtmp.release();
         if (c->scal_host) cudaFreeHost(c->scal_host);
+        if (c->dg_exec) cudaGraphExecDestroy(c->dg_exec);
         for (int i = 0; i < 8; ++i)
             if (c->pev[i]) cudaEventDestroy(c->pev[i]);
         if (c->ev0) cudaEventDestroy(c->ev0);
@@ -722,12 +723,17 @@ sdot_status sdot_evaluate(sdot_ctx *c, const double *psi, double *grad, double *
     CK(cudaMemcpyAsync(c->io_a.p, psi, c->nt * 8, cudaMemcpyHostToDevice, c->stream), "copy psi");
     if ((s = launch_gather(c, c->psi.p, c->io_a.p, c->nt)) != SDOT_OK) return s;
     double ms = 0;
-    s = evaluate_internal(c, nullptr, c->prm.tolerance, &ms);
+    // one wait for the stream: the gradient's scatter and copy are queued behind the evaluation
+    EvalPending pend;
+    s = evaluate_enqueue(c, nullptr, c->prm.tolerance, false, pend);
     if (s != SDOT_OK && s != SDOT_ENONFINITE) return s;
+    const bool queued = s == SDOT_OK;   // ENONFINITE here: non-finite psi, nothing was queued
     sdot_status s2 = launch_scatter(c, c->io_b.p, c->grad.p, c->nt);
     if (s2 != SDOT_OK) return s2;
     CK(cudaMemcpyAsync(grad, c->io_b.p, c->nt * 8, cudaMemcpyDeviceToHost, c->stream), "copy grad");
     CK(cudaStreamSynchronize(c->stream), "evaluate sync");
+    if (queued) s = evaluate_complete(c, pend, &ms);
+    if (s != SDOT_OK && s != SDOT_ENONFINITE) return s;
     if (value) *value = c->scal_host[SC_VALUE];
     fill_eval_info(c, info, ms);
     return s;
@@ -742,11 +748,15 @@ sdot_status sdot_evaluate_device(sdot_ctx *c, const double *psi_dev, double *gra
     if (s != SDOT_OK) return s;
     if ((s = launch_gather(c, c->psi.p, psi_dev, c->nt)) != SDOT_OK) return s;
     double ms = 0;
-    s = evaluate_internal(c, nullptr, c->prm.tolerance, &ms);
+    EvalPending pend;
+    s = evaluate_enqueue(c, nullptr, c->prm.tolerance, false, pend);
     if (s != SDOT_OK && s != SDOT_ENONFINITE) return s;
+    const bool queued = s == SDOT_OK;
     sdot_status s2 = launch_scatter(c, grad_dev, c->grad.p, c->nt);
     if (s2 != SDOT_OK) return s2;
     CK(cudaStreamSynchronize(c->stream), "evaluate sync");
+    if (queued) s = evaluate_complete(c, pend, &ms);
+    if (s != SDOT_OK && s != SDOT_ENONFINITE) return s;
     if (value) *value = c->scal_host[SC_VALUE];
     fill_eval_info(c, info, ms);
     return s;
@@ -1100,13 +1110,17 @@ sdot_status sdot_evaluate_partial_device(sdot_ctx *c, const double *psi_dev, dou
     if (s != SDOT_OK) return s;
     if ((s = launch_gather(c, c->psi.p, psi_dev, c->nt)) != SDOT_OK) return s;
     double ms = 0;
-    s = evaluate_internal(c, nullptr, c->prm.tolerance, &ms, true);
+    EvalPending pend;
+    s = evaluate_enqueue(c, nullptr, c->prm.tolerance, true, pend);
     if (s != SDOT_OK && s != SDOT_ENONFINITE) return s;
+    const bool queued = s == SDOT_OK;
     sdot_status s2 = launch_scatter(c, out_dev, c->grad.p, c->nt);
     if (s2 != SDOT_OK) return s2;
     k_partial_tail<<<1, 1, 0, c->stream>>>(c->scal.p, out_dev + c->nt);
     CK(cudaGetLastError(), "partial tail");
     CK(cudaStreamSynchronize(c->stream), "partial sync");
+    if (queued) s = evaluate_complete(c, pend, &ms);
+    if (s != SDOT_OK && s != SDOT_ENONFINITE) return s;
     fill_eval_info(c, info, ms);
     if (info) info->value = c->scal_host[SC_VALSRC];
     return s;

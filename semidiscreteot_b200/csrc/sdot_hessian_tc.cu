@@ -804,9 +804,11 @@ sdot_status hessian_tc(sdot_ctx *c, void *H_dev, bool out_f32, int chunk_stages,
     if (e == cudaSuccess) e = c->htc_err.alloc(1);
     // Factored generation: 2 x 2 x 2 Gauss cells (8-point chunks of the
     // 64-point stages), with the per-dimension factors r_d = 2^(2 G_d a_d)
-    // bounded by 2^16 (|G| <= l2e_eps diam), so no product leaves FP32.
+    // within 2^(+-24) (|G_d| <= l2e_eps diam): a cell's corner values then stay
+    // within 2^72 of its largest value, far inside FP32, and a value lost to
+    // an underflowing point factor is below 2^-54 of that largest value.
     const bool fact = c->hess_factored && c->dim == 3 && c->tensor_m == 2 && c->qpc == 8 &&
-                      2.0 * (LOG2E / c->prm.epsilon) * c->diam * c->tensor_amax <= 16.0;
+                      2.0 * (LOG2E / c->prm.epsilon) * c->diam * c->tensor_amax <= 24.0;
     if (e == cudaSuccess && fact) e = c->htc_cd.alloc((size_t)nst * 16 * 4);
     if (e == cudaSuccess && fact) e = c->htc_qw.alloc((size_t)nst * KQ * 2);
     if (e != cudaSuccess) return cuda_error(c, e, "tensor-core Hessian buffers");

@@ -207,6 +207,15 @@ struct sdot_ctx {
     // layout (gather/scatter), block-pair lists
     double kms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int64_t klaunch[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+
+    // ---- CUDA graph of the untruncated evaluation (sdot_eval.cu) ----
+    // Captured on the second consecutive evaluation with the same launch key
+    // (sizes, parameters, buffer addresses), replayed while the key holds.
+    cudaGraphExec_t dg_exec = nullptr;
+    std::vector<unsigned char> dg_key;
+    bool dg_armed = false;
+    bool graphs_off = false;           // set when capture failed: every evaluation runs eagerly
+    int64_t dg_launches[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 };
 
 namespace sdot {
@@ -217,11 +226,20 @@ sdot_status cuda_error(sdot_ctx *c, cudaError_t e, const char *where);
 
 // Evaluate J and grad at c->psi (internal order, device).  p_dir (device,
 // internal order) may be null; when given, g.p is computed too.  Fills
-// c->scal_host and updates the persistent state.  r_host: threshold computed
-// on the host (integral/geometric) or NaN to let the device compute the
-// pointwise threshold.
+// c->scal_host and updates the persistent state.
 sdot_status evaluate_internal(sdot_ctx *c, const double *p_dir, double comp_tol,
                               double *ms_out, bool partial = false);
+// The same in two halves, so that a caller can queue more work (the
+// gradient's scatter, its copy to the host) before the one wait for the
+// stream: evaluate_enqueue queues the evaluation and the copy of its scalars
+// to c->scal_host; after the caller has synchronised c->stream,
+// evaluate_complete reads them (and the timing events) and updates the state.
+struct EvalPending {
+    double r = 0.0;
+    bool dense = false;
+};
+sdot_status evaluate_enqueue(sdot_ctx *c, const double *p_dir, double comp_tol, bool partial, EvalPending &pend);
+sdot_status evaluate_complete(sdot_ctx *c, const EvalPending &pend, double *ms_out);
 
 // Threshold for the current psi (host computation mirroring
 // SotSolver::compute_distance_threshold), using device reductions for max/min.

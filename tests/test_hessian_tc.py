@@ -208,9 +208,9 @@ def test_factored_generation_matches_per_point(oracle_mod):
 
 
 def test_factored_generation_not_used_outside_its_bound():
-    """7^3 cells at eps = 1e-2: a per-dimension factor could reach 2^20.6, so
+    """9^3 cells at eps = 5e-3: a per-dimension factor could reach 2^32, so
     the per-point generation runs even though the cells are Gauss grids."""
-    src, y, nu, eps = problem("dense3d", seed=2)
+    src, y, nu, eps = problem("dense3d_small_eps", seed=2)
     s = make(src, y, nu, eps)
     psi = np.zeros(len(nu))
     hessian(s, psi, "tensor")
