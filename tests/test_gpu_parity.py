@@ -193,7 +193,7 @@ def test_bad_inputs():
     with pytest.raises(RuntimeError):
         s.setup_target(y, -nu)
     with pytest.raises(RuntimeError):
-        s.set_distance_function("spherical")
+        s.set_distance_function("manhattan")
     s.close()
 
 
