@@ -193,7 +193,7 @@ sdot_status sdot_set_hessian_chunk(sdot_ctx *ctx, int stages);
 sdot_status sdot_set_hessian_wait_limit(sdot_ctx *ctx, int64_t clocks);
 /* Operand generation of the tensor method (no reference counterpart).  When
  * the source's cells are 2 x 2 x 2 Gauss grids (3D, QGauss(2)) and the
- * per-dimension factors stay within 2^16, each generated row takes one ex2
+ * per-dimension factors stay within 2^24, each generated row takes one ex2
  * per cell and one per dimension instead of one per point: the 8 values of a
  * cell are products of those factors and a per-point factor formed once per
  * point.  factored = 1 (default) uses it where it applies, 0 never, < 0 leaves
