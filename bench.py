@@ -892,10 +892,9 @@ def run_batched_2d(args):
 
 def serve_requests(n, seed=0, scale=1.0):
     """Config 5's request mix: 80% config-3-like (uniform density cube, uniform
-    targets, eps 5e-3, untruncated: Newton with the tensor-core Hessian), 20%
-    3D cubes with Gaussian-mixture targets and eps in [1e-3, 1e-2] at the
-    reference's default truncation tau = 1e-8 (so L-BFGS over truncated
-    evaluations); sizes scaled by `scale` (cells per axis and targets)."""
+    targets, eps 5e-3), 20% 3D cubes with Gaussian-mixture targets and eps in
+    [1e-3, 1e-2]; all untruncated (Newton with the tensor-core Hessian up to
+    46,340 targets); sizes scaled by `scale` (cells per axis and targets)."""
     from semidiscreteot_b200 import SolverParameters, structured_source
     rng = np.random.default_rng(seed)
     out = []
@@ -909,7 +908,7 @@ def serve_requests(n, seed=0, scale=1.0):
             nu = np.full(nt, 1.0 / nt)
             eps = 5e-3
         else:
-            tau, maxit, kind = 1e-8, 20000, "mixture_cube"
+            kind = "mixture_cube"
             cells = max(4, int(round(np.exp(rng.uniform(np.log(16), np.log(64))) * scale)))
             nt = max(64, int(np.exp(rng.uniform(np.log(5_000), np.log(50_000))) * scale ** 3))
             src = structured_source(3, cells, 2)

