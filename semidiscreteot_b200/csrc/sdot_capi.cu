@@ -659,6 +659,7 @@ sdot_status sdot_set_target(sdot_ctx *c, int64_t n, const double *y, const doubl
     c->nt = n;
     c->ntblk = ntblk;
     c->nu_host.assign(nu, nu + n);
+    c->nu_min = *std::min_element(c->nu_host.begin(), c->nu_host.end());
     c->y_host.assign(y, y + n * dim);
     for (int d = 0; d < 3; ++d) {
         c->tgt_lo[d] = 0.0;
@@ -809,8 +810,7 @@ sdot_status sdot_compute_geometric_radius_bound(sdot_ctx *c, const double *psi, 
         mn = std::min(mn, psi[i]);
     }
     const double range = mx - mn;
-    const double mind = c->min_target_density > 0.0 ? c->min_target_density
-                                                     : *std::min_element(c->nu_host.begin(), c->nu_host.end());
+    const double mind = c->min_target_density > 0.0 ? c->min_target_density : c->nu_min;
     double fv = std::fabs(c->global_functional);
     if (fv < 1e-10) fv = 1e-10;
     const double log_term = std::log(epsilon / (mind * tolerance * fv));
@@ -989,7 +989,7 @@ sdot_status sdot_solve(sdot_ctx *c, double *psi, const sdot_solver_params *param
     double cov = 0.0;
     if ((s = sdot_compute_covering_radius(c, &cov)) != SDOT_OK) return s;
     c->covering_radius = cov * 1.1;
-    c->min_target_density = *std::min_element(c->nu_host.begin(), c->nu_host.end());
+    c->min_target_density = c->nu_min;
     c->have_solve = true;
 
     Solver S{c, n};

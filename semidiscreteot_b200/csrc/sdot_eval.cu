@@ -337,11 +337,6 @@ double sstar_of(double r)
     return s;
 }
 
-static double vmin_host(const std::vector<double> &v)
-{
-    return *std::min_element(v.begin(), v.end());
-}
-
 // SotSolver::compute_distance_threshold (SotSolver.cc:379-429), on the host
 // with the same libm calls and operation order as the reference.
 double host_threshold(sdot_ctx *c, double maxpsi, double minpsi)
@@ -365,7 +360,7 @@ double host_threshold(sdot_ctx *c, double maxpsi, double minpsi)
             r0 = rr;
         }
         const double range = maxpsi - minpsi;
-        const double mind = c->min_target_density > 0.0 ? c->min_target_density : vmin_host(c->nu_host);
+        const double mind = c->min_target_density > 0.0 ? c->min_target_density : c->nu_min;
         double fv = std::fabs(c->global_functional);
         if (fv < 1e-10) fv = 1e-10;
         const double log_term = std::log(p.epsilon / (mind * p.tau * fv));
@@ -373,7 +368,7 @@ double host_threshold(sdot_ctx *c, double maxpsi, double minpsi)
         if (r2 < r0 * r0) r2 = r0 * r0;
         return std::sqrt(r2);
     }
-    const double numin = c->min_target_density > 0.0 ? c->min_target_density : vmin_host(c->nu_host);
+    const double numin = c->min_target_density > 0.0 ? c->min_target_density : c->nu_min;
     if (numin <= 0 || p.tau <= 0) return DBL_MAX;
     const double r2 = -2.0 * p.epsilon * std::log(p.tau / numin) + 2.0 * maxpsi;
     return std::sqrt(std::max(0.0, r2));
@@ -561,7 +556,7 @@ sdot_status evaluate_enqueue(sdot_ctx *c, const double *p_dir, double comp_tol, 
     double r = DBL_MAX;
     const bool may_truncate = (p.threshold_type != SDOT_THRESH_POINTWISE) ||
                               (p.tau > 0 && (c->min_target_density > 0.0 ? c->min_target_density
-                                                                          : vmin_host(c->nu_host)) > 0);
+                                                                          : c->nu_min) > 0);
     cudaEventRecord(c->ev0, c->stream);
     double mm[3] = {0, 0, 0};
     auto launch_minmax = [&] {

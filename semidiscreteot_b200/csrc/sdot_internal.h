@@ -141,6 +141,7 @@ struct sdot_ctx {
     sdot::DevBuf<double> tblk_sph;     // 4 per block
     sdot::DevBuf<float4> tblk_sph32;
     std::vector<double> nu_host;       // caller order
+    double nu_min = 0.0;               // min of nu_host (set with the targets)
     std::vector<double> y_host;        // caller order
     double tgt_lo[3] = {0, 0, 0}, tgt_hi[3] = {0, 0, 0};
 

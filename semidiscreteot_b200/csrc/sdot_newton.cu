@@ -285,7 +285,7 @@ extern "C" sdot_status sdot_solve_newton(sdot_ctx *c, double *psi, const sdot_so
     double cov = 0.0;
     if ((s = sdot_compute_covering_radius(c, &cov)) != SDOT_OK) return s;
     c->covering_radius = cov * 1.1;
-    c->min_target_density = *std::min_element(c->nu_host.begin(), c->nu_host.end());
+    c->min_target_density = c->nu_min;
     c->have_solve = true;
 
     e = cudaMemcpyAsync(c->io_a.p, psi, n * 8, cudaMemcpyHostToDevice, c->stream);
