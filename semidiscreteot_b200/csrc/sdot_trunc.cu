@@ -74,7 +74,8 @@ struct FusedArgs {
     const int64_t *fwd_off;
     const int *fwd_t;
     const int64_t *fwd2inv;      // inverse position of each forward pair
-    double *part;                // partials, 32 per pair, at inverse positions minus part_base
+    double *part;                // partials, 32 per pair, at inverse positions minus part_base (FP64 sweeps)
+    float *part32;               // the same in FP32 (hybrid sweeps: their rows are FP32 already)
     double *Lq;                  // per q (written by the value sweep)
     double *valpart;             // per source block: value, C, skipped, pairs
     int do_a, do_b;
@@ -923,7 +924,8 @@ __device__ __forceinline__ void write_partials(SM &sm, const FusedArgs &f, int n
         double v = 0.0;
         if (p >= 0)
             for (int w = 0; w < nunit; ++w) v += (double)rows[w * SM::MAXS + p];
-        f.part[base + sl] = v;
+        if constexpr (FP32B) f.part32[base + sl] = (float)v;
+        else f.part[base + sl] = v;
     }
 }
 
@@ -1191,16 +1193,17 @@ k_fused(FusedArgs f, EvalArgs a)
 // gradient of target block t = sum of its pair partials in inverse order
 // (ascending source block), lane <-> target.  CTA <-> target block: warp w
 // sums rows w, w+8, ...; the 8 warp sums are added in warp order.
+template <typename PT>
 __global__ void __launch_bounds__(256)
 k_grad_reduce(const int64_t *__restrict__ tblk_off, const int64_t *__restrict__ inv_off, int tlo, int thi,
-              int64_t part_base, const double *__restrict__ part, double *__restrict__ gacc)
+              int64_t part_base, const PT *__restrict__ part, double *__restrict__ gacc)
 {
     __shared__ double ws[8][32];
     const int t = tlo + blockIdx.x;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int64_t p0 = inv_off[t], p1 = inv_off[t + 1];
     double acc = 0.0;
-    for (int64_t p = p0 + w; p < p1; p += 8) acc += part[(p - part_base) * TBLK_KD + lane];
+    for (int64_t p = p0 + w; p < p1; p += 8) acc += (double)part[(p - part_base) * TBLK_KD + lane];
     ws[w][lane] = acc;
     __syncthreads();
     if (w == 0) {
@@ -1386,7 +1389,10 @@ sdot_status run_trunc(sdot_ctx *c, const EvalArgs &a, double r)
     c->klaunch[6] += 9;
     if (c->profiling) cudaEventRecord(c->pev[7], st);
     // 2. partial buffer (inverse order): all pairs at once under the cap, else target-block groups
-    const int64_t cap_pairs = std::max<int64_t>(1, (int64_t)(c->part_cap_bytes / (TBLK_KD * sizeof(double))));
+    // partials are FP32 in the hybrid mode (the sweeps' rows are FP32), FP64 otherwise
+    const bool fp32b = c->precision != SDOT_PREC_FP64;
+    const size_t pel = fp32b ? sizeof(float) : sizeof(double);
+    const int64_t cap_pairs = std::max<int64_t>(1, (int64_t)(c->part_cap_bytes / (TBLK_KD * pel)));
     std::vector<std::pair<int, int>> groups;
     std::vector<int64_t> inv_host;
     int64_t part_pairs = npairs;
@@ -1407,16 +1413,15 @@ sdot_status run_trunc(sdot_ctx *c, const EvalArgs &a, double r)
             t0 = t1;
         }
     }
-    e = c->part.alloc((size_t)std::max<int64_t>(1, part_pairs) * TBLK_KD);
+    e = c->part.alloc(((size_t)std::max<int64_t>(1, part_pairs) * TBLK_KD * pel + sizeof(double) - 1) / sizeof(double));
     if (e != cudaSuccess) return cuda_error(c, e, "partial buffer alloc");
     FusedArgs f{};
     f.x = c->x.p; f.rho = c->rho.p; f.jxw = c->jxw.p; f.w = c->w.p; f.cell_ctr = c->cell_ctr.p;
     f.tpk = c->tpack.p; f.sblk_cell = c->sblk_cell.p; f.sblk_sph = c->sblk_sph.p; f.tblk_off = c->tblk_off.p;
     f.fwd_off = c->fwd_off.p; f.fwd_t = c->fwd_t.p; f.fwd2inv = c->fwd2inv.p;
-    f.part = c->part.p; f.Lq = c->Lq.p; f.valpart = c->blkpart.p;
+    f.part = c->part.p; f.part32 = reinterpret_cast<float *>(c->part.p); f.Lq = c->Lq.p; f.valpart = c->blkpart.p;
     f.cullt = std::isnan(r) ? 0.0 : std::min(r, 1e300);
     f.w_nonneg = c->w_nonneg ? 1 : 0;
-    const bool fp32b = c->precision != SDOT_PREC_FP64;
     const double prange0 = c->scal_host[SC_MAXPSI] - c->scal_host[SC_MINPSI];
     const double prange = std::isfinite(prange0) ? prange0 : 1e300;
     const int tmode = fused_tensor_mode(c, a, prange);
@@ -1444,9 +1449,12 @@ sdot_status run_trunc(sdot_ctx *c, const EvalArgs &a, double r)
         else dispatch_fused<3>(c, f, a, fp32b, nsb, prange, tmode);
         if (c->profiling && gi + 1 == groups.size()) cudaEventRecord(c->pev[2], st);
         const int nw = f.thi - f.tlo;
-        k_grad_reduce<<<(unsigned)nw, 256, 0, st>>>(c->tblk_off.p, c->inv_off.p, f.tlo,
-                                                                                 f.thi, f.part_base, c->part.p,
-                                                                                 c->gpart.p);
+        if (fp32b)
+            k_grad_reduce<float><<<(unsigned)nw, 256, 0, st>>>(c->tblk_off.p, c->inv_off.p, f.tlo, f.thi, f.part_base,
+                                                               f.part32, c->gpart.p);
+        else
+            k_grad_reduce<double><<<(unsigned)nw, 256, 0, st>>>(c->tblk_off.p, c->inv_off.p, f.tlo, f.thi,
+                                                                f.part_base, c->part.p, c->gpart.p);
         c->klaunch[2] += 1;
         c->klaunch[3] += 1;
     }
