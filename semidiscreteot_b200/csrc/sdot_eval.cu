@@ -63,20 +63,21 @@ __global__ void k_minmax(const double *v, int64_t n, double *out)
     __shared__ int sbad[32];
     double mx = -DBL_MAX, mn = DBL_MAX;
     int bad = 0;
-    // four independent loads in flight per thread (max, min and the flag do not depend on the order)
+    // sixteen independent loads in flight per thread (max, min and the flag do
+    // not depend on the order): the single CTA is bound by load latency
+    constexpr int U = 16;
     const int64_t step = blockDim.x;
     int64_t i = threadIdx.x;
-    for (; i + 3 * step < n; i += 4 * step) {
-        const double a0 = v[i], a1 = v[i + step], a2 = v[i + 2 * step], a3 = v[i + 3 * step];
-        if (!isfinite(a0) || !isfinite(a1) || !isfinite(a2) || !isfinite(a3)) bad = 1;
-        mx = a0 > mx ? a0 : mx;
-        mn = a0 < mn ? a0 : mn;
-        mx = a1 > mx ? a1 : mx;
-        mn = a1 < mn ? a1 : mn;
-        mx = a2 > mx ? a2 : mx;
-        mn = a2 < mn ? a2 : mn;
-        mx = a3 > mx ? a3 : mx;
-        mn = a3 < mn ? a3 : mn;
+    for (; i + (U - 1) * step < n; i += U * step) {
+        double a[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) a[u] = v[i + u * step];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (!isfinite(a[u])) bad = 1;
+            mx = a[u] > mx ? a[u] : mx;
+            mn = a[u] < mn ? a[u] : mn;
+        }
     }
     for (; i < n; i += step) {
         const double a = v[i];
@@ -239,13 +240,32 @@ k_finalize_scalars(int nred, const double *__restrict__ redpart, int64_t nval, c
                    double *__restrict__ scal)
 {
     __shared__ double sh[11][FIN_SCALAR_THREADS / 32];
-    double v = 0.0, c = 0.0, sk = 0.0, np = 0.0;
-    for (int64_t b = threadIdx.x; b < nval; b += blockDim.x) {
-        v += valpart[b * 4 + 0];
-        c += valpart[b * 4 + 1];
-        sk += valpart[b * 4 + 2];
-        np += valpart[b * 4 + 3];
+    // four block partials per thread and pass, each into its own accumulator
+    // (loads in flight), the accumulators added in a fixed order
+    double va[4] = {0, 0, 0, 0}, ca[4] = {0, 0, 0, 0}, ska[4] = {0, 0, 0, 0}, npa[4] = {0, 0, 0, 0};
+    const int64_t bs = blockDim.x;
+    int64_t b0 = threadIdx.x;
+    for (; b0 + 3 * bs < nval; b0 += 4 * bs) {
+        double4 t[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) t[u] = reinterpret_cast<const double4 *>(valpart)[b0 + u * bs];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            va[u] += t[u].x;
+            ca[u] += t[u].y;
+            ska[u] += t[u].z;
+            npa[u] += t[u].w;
+        }
     }
+    for (int u = 0; b0 < nval; b0 += bs, ++u) {
+        const double4 t = reinterpret_cast<const double4 *>(valpart)[b0];
+        va[u] += t.x;
+        ca[u] += t.y;
+        ska[u] += t.z;
+        npa[u] += t.w;
+    }
+    double v = (va[0] + va[1]) + (va[2] + va[3]), c = (ca[0] + ca[1]) + (ca[2] + ca[3]);
+    double sk = (ska[0] + ska[1]) + (ska[2] + ska[3]), np = (npa[0] + npa[1]) + (npa[2] + npa[3]);
     double r[7] = {0, 0, 0, -CUDART_INF, 0, 0, 0};
     for (int b = threadIdx.x; b < nred; b += blockDim.x) {
         const double *p = redpart + b * NRED;

@@ -400,16 +400,22 @@ k_inv_order(int nsb, const int64_t *__restrict__ inv_off, const int *__restrict_
 // exclusive scan of n counts into off[0..n] (single CTA, order-fixed)
 __global__ void __launch_bounds__(1024) k_scan(const int64_t *__restrict__ cnt, int64_t n, int64_t *__restrict__ off)
 {
-    // coalesced tiles of 1,024 counts: warp-shuffle inclusive scans, the warp
-    // totals scanned by warp 0, a running carry across tiles (integer sums:
-    // exact in any order)
+    // passes of 1,024 x SP counts: each thread loads SP consecutive counts at
+    // once (the CTA is bound by load latency), the thread sums are scanned by
+    // warp shuffles and warp 0, and a running carry crosses the passes
+    // (integer sums: exact in any order)
+    constexpr int SP = 8;
     __shared__ long long wsum[32];
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     long long carry = 0;
-    for (int64_t t0 = 0; t0 < n; t0 += 1024) {
-        const int64_t i = t0 + tid;
-        const long long v = i < n ? (long long)cnt[i] : 0;
-        long long x = v;
+    for (int64_t t0 = 0; t0 < n; t0 += 1024 * SP) {
+        const int64_t base = t0 + (int64_t)tid * SP;
+        long long v[SP], tsum = 0;
+#pragma unroll
+        for (int k = 0; k < SP; ++k) v[k] = base + k < n ? (long long)cnt[base + k] : 0;
+#pragma unroll
+        for (int k = 0; k < SP; ++k) tsum += v[k];
+        long long x = tsum;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const long long y = __shfl_up_sync(0xffffffffu, x, o);
@@ -427,10 +433,14 @@ __global__ void __launch_bounds__(1024) k_scan(const int64_t *__restrict__ cnt, 
             wsum[lane] = z;
         }
         __syncthreads();
-        const long long before = w > 0 ? wsum[w - 1] : 0;
-        if (i < n) off[i] = (int64_t)(carry + before + x - v);
+        long long run = carry + (w > 0 ? wsum[w - 1] : 0) + x - tsum;
+#pragma unroll
+        for (int k = 0; k < SP; ++k) {
+            if (base + k < n) off[base + k] = (int64_t)run;
+            run += v[k];
+        }
         carry += wsum[31];
-        __syncthreads();  // wsum is rewritten by the next tile
+        __syncthreads();  // wsum is rewritten by the next pass
     }
     if (tid == 0) off[n] = (int64_t)carry;
 }
