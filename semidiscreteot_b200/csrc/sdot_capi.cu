@@ -212,7 +212,7 @@ size_t device_bytes(const sdot_ctx *c)
            c->io_b.bytes() + c->x0.bytes() + c->pdir.bytes() + c->sk.bytes() + c->yk.bytes() + c->hist_s.bytes() +
            c->hist_y.bytes() + c->gtmp.bytes() + c->htc_tdat.bytes() + c->htc_diag.bytes() + c->htc_blk.bytes() +
            c->htc_scr.bytes() + c->htc_qa.bytes() + c->htc_qb.bytes() + c->htc_tiles.bytes() + c->htc_err.bytes() +
-           c->htc_cd.bytes() + c->htc_qw.bytes() + c->tsep.bytes();
+           c->htc_cd.bytes() + c->htc_qw.bytes();
 }
 
 }  // namespace
@@ -448,7 +448,7 @@ void sdot_destroy(sdot_ctx *c)
         c->y.release(); c->nu.release();
         c->perm.release(); c->tblk_sph.release(); c->psi.release(); c->grad.release(); c->tpack.release();
         c->Lq.release(); c->gpart.release(); c->blkpart.release(); c->scal.release(); c->redpart.release();
-        c->vpart.release(); c->tsep.release();
+        c->vpart.release();
         c->io_a.release(); c->io_b.release(); c->x0.release(); c->pdir.release(); c->sk.release(); c->yk.release();
         c->hist_s.release(); c->hist_y.release(); c->gtmp.release();
         if (c->scal_host) cudaFreeHost(c->scal_host);
@@ -523,14 +523,11 @@ sdot_status sdot_set_source(sdot_ctx *c, int dim, int64_t n_q, const double *x, 
     // truncated sweeps then factor 2^(G.delta) per dimension.
     int tm = 0;
     double amax = 0.0;
-    bool uni = true;
-    double au[3] = {0, 0, 0};
     for (int m = 2; m <= 3 && tm == 0; ++m) {
         int64_t p = 1;
         for (int d = 0; d < dim; ++d) p *= m;
         if (p != qpc || ngroups != 1) continue;
         bool ok = true;
-        uni = true;
         const double tol = 1e-12 * std::max(dmax, 1e-300);
         for (int64_t k = 0; k < n_cells && ok; ++k) {
             const double *X = &hx[k * qpc * dim];
@@ -546,8 +543,6 @@ sdot_status sdot_set_source(sdot_ctx *c, int dim, int64_t n_q, const double *x, 
                     if (X[q * dim + d] != X[(dig * stride) * dim + d]) ok = false;
                 }
                 amax = std::max(amax, std::fabs(o[m - 1]));
-                if (k == 0) au[d] = o[m - 1];
-                else if (std::fabs(o[m - 1] - au[d]) > tol) uni = false;
             }
         }
         if (ok) tm = m;
@@ -555,8 +550,6 @@ sdot_status sdot_set_source(sdot_ctx *c, int dim, int64_t n_q, const double *x, 
     }
     c->tensor_m = tm;
     c->tensor_amax = amax;
-    c->tensor_uniform = tm > 0 && uni;
-    for (int d = 0; d < 3; ++d) c->tensor_a[d] = (tm > 0 && d < dim) ? au[d] : 0.0;
     const int64_t nsblk = (int64_t)bounds.size() - 1;
     std::vector<double> ssph(nsblk * 4);
     for (int64_t b = 0; b < nsblk; ++b) {

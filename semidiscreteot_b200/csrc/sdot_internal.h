@@ -151,8 +151,6 @@ struct sdot_ctx {
     double delta_max = 0.0;            // max distance of a quadrature point to its cell centre
     int tensor_m = 0;                  // > 0: points form an m^dim tensor grid symmetric about the cell centre
     double tensor_amax = 0.0;          // largest per-dimension offset of that grid
-    bool tensor_uniform = false;       // every cell's grid has the same offsets (tensor_a, to 1e-12 relative)
-    double tensor_a[3] = {0, 0, 0};    // per dimension: the largest offset of every cell's grid
 
     // ---- truncated path: block-pair lists and gradient partials ----
     sdot::DevBuf<int64_t> fwd_cnt, fwd_off, inv_cnt, inv_off, fwd2inv;
@@ -191,7 +189,6 @@ struct sdot_ctx {
     sdot::DevBuf<float> htc_qa, htc_qb;
     sdot::DevBuf<int> htc_tiles, htc_err;
     sdot::DevBuf<float> htc_cd, htc_qw;  // factored generation: per-chunk cell data, per-point factors
-    sdot::DevBuf<double> tsep;         // truncated value sweep: per-target separable factors (4 per target)
     bool hess_factored = true;         // factored generation where the source allows it (sdot_set_hessian_generation)
     bool hess_last_factored = false;   // the last tensor Hessian used it
     double hess_kernel_ms = 0.0;

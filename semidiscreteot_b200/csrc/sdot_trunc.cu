@@ -83,10 +83,6 @@ struct FusedArgs {
     int tlo, thi;                // gradient partials only for target blocks [tlo, thi)
     int64_t part_base;           // inverse position of the first pair of tlo
     double cullt;                // per-target cull radius addend (r, enlarged)
-    // separable per-dimension factors of the tensor value sweep (TS == 2):
-    // 2^(ka_d (y_d - c_d) / 16) = tsep[j][d] * 2^(-ka_d (c_d - o_d) / 16)
-    const double *tsep;          // per target: 2^(ka_d (y_d - o_d) / 16), d < 3, and a pad
-    double ka[3];
 };
 
 template <int CAP>
@@ -101,9 +97,7 @@ struct FTSmem {
     float qw[FT_MAXQ];            // pass B: w_q
     float qtw[FT_MAXQ];           // pass B, tensor path: w_q 2^(D_q)
     double cellc[FT_WARPS][3];    // centre of each cell of the block
-    __align__(16) float pvw[FT_WARPS][CAP];  // gradient partial of each unit (warp) per staged target (FP32
-                                  // mode); in the value sweep with separable factors: their per-target
-                                  // parts, 3 doubles per staged target (sep_rows)
+    float pvw[FT_WARPS][CAP];     // gradient partial of each unit (warp) per staged target (FP32 mode)
     unsigned short cand[FT_WARPS][CAP];
     short smap[FT_MAXT][TBLK_KD]; // (chunk target block, slot) -> staged position or -1
     int ctb[FT_MAXT];             // target blocks of the chunk
@@ -125,16 +119,6 @@ struct FTSmem {
 template <bool FP32B> struct PRow { using T = double; };
 template <> struct PRow<true> { using T = float; };
 __host__ __device__ constexpr size_t ft_rows64_bytes(int cap) { return sizeof(double) * FT_WARPS * cap; }
-
-// Per-target separable factors of the staged targets ([3][MAXS] doubles),
-// kept where the gradient sweep's FP32 partial rows go: the value sweep
-// reads them, the gradient sweep overwrites them.
-template <class SM>
-__device__ __forceinline__ double *sep_rows(SM &sm)
-{
-    static_assert(3 * sizeof(double) * SM::MAXS <= sizeof(sm.pvw), "separable factors fit the partial rows");
-    return reinterpret_cast<double *>(&sm.pvw[0][0]);
-}
 
 template <bool FP32B, class SM>
 __device__ __forceinline__ typename PRow<FP32B>::T *partial_rows(SM &sm)
@@ -454,8 +438,7 @@ __global__ void __launch_bounds__(1024) k_scan(const int64_t *__restrict__ cnt, 
 // target), counts its survivors with a ballot, and whole target blocks are
 // accepted in list order while the staged total fits FT_MAXS.  Returns the
 // number of forward entries consumed; staged order = (target block, slot).
-// SEP: also stage each target's separable factors (sep_rows).
-template <int DIM, bool SEP, class SM>
+template <int DIM, class SM>
 __device__ int stage_chunk(SM &sm, const FusedArgs &f, int64_t kb, int64_t k0, int64_t k1, const double *bc,
                            double rcull2, bool for_b)
 {
@@ -543,11 +526,6 @@ __device__ int stage_chunk(SM &sm, const FusedArgs &f, int64_t kb, int64_t k0, i
                     const double *tp = f.tpk + (j0 + lane) * TPACK;
 #pragma unroll
                     for (int d = 0; d < FT_TS; ++d) sm.stg[d][pos] = tp[d];
-                    if constexpr (SEP) {
-                        const double *ts = f.tsep + (j0 + lane) * 4;
-#pragma unroll
-                        for (int d = 0; d < 3; ++d) sep_rows(sm)[d * SM::MAXS + pos] = ts[d];
-                    }
                 }
                 sm.smap[slot][lane] = pos;
                 if (lane == 0) {
@@ -766,9 +744,9 @@ __device__ __forceinline__ constexpr int tstride()
 // a candidate with B0 below (running max B0) - 2 s r |delta|max is never a
 // maximum; thr is that bound relative to Munit.
 template <int DIM, int TM, int TS, class SM>
-__device__ __forceinline__ void value_pairs_tensor(SM &sm, int wp, int lane, int ncand, int qoff,
+__device__ __forceinline__ void value_pairs_tensor(const SM &sm, int wp, int lane, int ncand, int qoff,
                                                    const double *cc, const EvalArgs &a, double Munit, double thr,
-                                                   const double *Cd, double *S, double *mx)
+                                                   double *S, double *mx)
 {
     constexpr int NQ = DIM == 3 ? TM * TM * TM : TM * TM;
     double ah[3];
@@ -793,8 +771,7 @@ __device__ __forceinline__ void value_pairs_tensor(SM &sm, int wp, int lane, int
             }
         }
         // per-dimension factors 2^(G_d delta_d): with TS, relative to the lowest
-        // point (1, r, r^2 with the shift folded into P); otherwise 2^(-G a), (1), 2^(G a).
-        // TS == 2: r = (per-target factor) x (per-cell factor Cd), no exponential
+        // point (1, r, r^2 with the shift folded into P); otherwise 2^(-G a), (1), 2^(G a)
         double F[3][TM];
         double P;
         if constexpr (TS >= 1) {
@@ -803,9 +780,7 @@ __device__ __forceinline__ void value_pairs_tensor(SM &sm, int wp, int lane, int
             for (int d = 0; d < DIM; ++d) {
                 const double ga = G[d] * ah[d];
                 sga += ga;
-                double r;
-                if constexpr (TS == 2) r = sep_rows(sm)[d * SM::MAXS + ti] * Cd[d];
-                else r = exp2_16(TM == 2 ? 2.0 * ga : ga, sm.tab);
+                const double r = exp2_16(TM == 2 ? 2.0 * ga : ga, sm.tab);
                 F[d][0] = 1.0;
                 F[d][1] = r;
                 if (TM == 3) F[d][2] = r * r;
@@ -1011,15 +986,9 @@ k_fused(FusedArgs f, EvalArgs a)
         for (int q = 0; q < nql; ++q) dqmax = fmax(dqmax, sm.qn[qoff + q]);
         double npairs = 0.0;
         double bmax_run = -CUDART_INF;  // largest B0 of the candidates so far
-        // per-cell parts of the separable factors (TS == 2)
-        double Cd[3] = {1.0, 1.0, 1.0};
-        if constexpr (TS == 2) {
-#pragma unroll
-            for (int d = 0; d < DIM; ++d) Cd[d] = exp2_16(-f.ka[d] * (cc[d] - a.o[d]), sm.tab);
-        }
         const double sr = a.s * a.cull;
         for (int64_t k = k0; k < k1;) {
-            const int nt = stage_chunk<DIM, TS == 2>(sm, f, k0, k, k1, bc, rcull2, f.do_b != 0);
+            const int nt = stage_chunk<DIM>(sm, f, k0, k, k1, bc, rcull2, f.do_b != 0);
             const int nstg = sm.nstg;
             if (valid) {
                 double bmax;
@@ -1043,7 +1012,7 @@ k_fused(FusedArgs f, EvalArgs a)
                 if (bmax > bmax_run) bmax_run = bmax;
                 if constexpr (TQ > 0)
                     value_pairs_tensor<DIM, TQ, TS>(sm, wp, lane, ncand, qoff, cc, a, Munit,
-                                                    bmax_run - 2.0 * sr * dqmax - Munit, Cd, S, mx);
+                                                    bmax_run - 2.0 * sr * dqmax - Munit, S, mx);
                 else if (nql == QL)
                     value_pairs<DIM, QL, QL, MODE>(sm, wp, lane, ncand, qoff, cc[0], cc[1], cc[2], a, Munit, M, S, mx);
                 else
@@ -1181,7 +1150,7 @@ k_fused(FusedArgs f, EvalArgs a)
         __syncthreads();  // the earlier chunks overwrite the staged targets
     }
     for (int64_t k = k0; k < kend;) {
-        const int nt = stage_chunk<DIM, false>(sm, f, k0, k, kend, bc, rcull2, true);
+        const int nt = stage_chunk<DIM>(sm, f, k0, k, kend, bc, rcull2, true);
         const int nstg = sm.nstg;
         if (valid) {
             double bmax;
@@ -1264,14 +1233,7 @@ static void dispatch_fused_q(sdot_ctx *c, const FusedArgs &f, const EvalArgs &a,
 //
 // Tensor form of the sweeps (tensor-product points with an instantiation):
 // -1 none (per-point sweeps), 0 symmetric factors 2^(+-G a), 1 factors
-// relative to the lowest point, 2 the same with each factor split into a
-// per-target and a per-cell part (cells whose grids share their offsets).
-static double separable_rate(const sdot_ctx *c, const EvalArgs &a, int d)
-{
-    // the factor between neighbouring points along d: 2^(s (step) (y_d - c_d) / 16), step = 2a (m = 2) or a (m = 3)
-    return (c->tensor_m == 2 ? 2.0 : 1.0) * a.s * c->tensor_a[d];
-}
-
+// relative to the lowest point.
 static int fused_tensor_mode(const sdot_ctx *c, const EvalArgs &a, double psi_range)
 {
     const double gap = 2.0 * a.s * a.cull * c->delta_max;
@@ -1285,12 +1247,7 @@ static int fused_tensor_mode(const sdot_ctx *c, const EvalArgs &a, double psi_ra
                        (c->dim == 2 && c->tensor_m == 3 && a.ql == 9) || (c->dim == 2 && c->tensor_m == 2 && a.ql == 4);
     if (!tensor || !shape) return -1;
     // factors <= 2^8 per dimension: the relative form (no reciprocals, the lowest point's factor 1)
-    if (fac > 4.0) return 0;
-    // separable parts 2^(+-ka_d |x_d - o_d| / 16) within 2^900 for every point of the domain
-    bool sep = c->tensor_uniform;
-    for (int d = 0; d < c->dim; ++d)
-        if (!(separable_rate(c, a, d) * 0.5 * c->diam <= 16.0 * 900.0)) sep = false;
-    return sep ? 2 : 1;
+    return fac > 4.0 ? 0 : 1;
 }
 
 template <int DIM>
@@ -1305,35 +1262,19 @@ static void dispatch_fused(sdot_ctx *c, const FusedArgs &f, const EvalArgs &a, b
     }
     if (tmode >= 0) {
         if constexpr (DIM == 3) {
-            if (tmode == 2) dispatch_fused_b<3, 8, 0, 2, 2>(c, f, a, fp32b, nb);
-            else if (tmode == 1) dispatch_fused_b<3, 8, 0, 2, 1>(c, f, a, fp32b, nb);
+            if (tmode == 1) dispatch_fused_b<3, 8, 0, 2, 1>(c, f, a, fp32b, nb);
             else dispatch_fused_b<3, 8, 0, 2, 0>(c, f, a, fp32b, nb);
         } else if (c->tensor_m == 3) {
-            if (tmode == 2) dispatch_fused_b<2, 9, 0, 3, 2>(c, f, a, fp32b, nb);
-            else if (tmode == 1) dispatch_fused_b<2, 9, 0, 3, 1>(c, f, a, fp32b, nb);
+            if (tmode == 1) dispatch_fused_b<2, 9, 0, 3, 1>(c, f, a, fp32b, nb);
             else dispatch_fused_b<2, 9, 0, 3, 0>(c, f, a, fp32b, nb);
         } else {
-            if (tmode == 2) dispatch_fused_b<2, 4, 0, 2, 2>(c, f, a, fp32b, nb);
-            else if (tmode == 1) dispatch_fused_b<2, 4, 0, 2, 1>(c, f, a, fp32b, nb);
+            if (tmode == 1) dispatch_fused_b<2, 4, 0, 2, 1>(c, f, a, fp32b, nb);
             else dispatch_fused_b<2, 4, 0, 2, 0>(c, f, a, fp32b, nb);
         }
         return;
     }
     if (umin > -15000.0) dispatch_fused_q<DIM, 0>(c, f, a, fp32b, nb);
     else dispatch_fused_q<DIM, 1>(c, f, a, fp32b, nb);
-}
-
-// Per-target separable factors tsep[j][d] = 2^(ka_d (y_jd - o_d) / 16).
-template <int DIM>
-__global__ void k_trunc_tsep(int64_t nt, const double *__restrict__ y, double ox, double oy, double oz, double k0,
-                             double k1, double k2, double *__restrict__ tsep)
-{
-    const double o[3] = {ox, oy, oz}, k[3] = {k0, k1, k2};
-    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nt; j += (int64_t)gridDim.x * blockDim.x) {
-#pragma unroll
-        for (int d = 0; d < 3; ++d) tsep[j * 4 + d] = d < DIM ? exp2_16(k[d] * (y[j * DIM + d] - o[d]), c_exp2_tab) : 1.0;
-        tsep[j * 4 + 3] = 0.0;
-    }
 }
 
 sdot_status run_trunc(sdot_ctx *c, const EvalArgs &a, double r)
@@ -1435,20 +1376,6 @@ sdot_status run_trunc(sdot_ctx *c, const EvalArgs &a, double r)
     const double prange0 = c->scal_host[SC_MAXPSI] - c->scal_host[SC_MINPSI];
     const double prange = std::isfinite(prange0) ? prange0 : 1e300;
     const int tmode = fused_tensor_mode(c, a, prange);
-    if (tmode == 2) {
-        e = c->tsep.alloc((size_t)a.nt * 4);
-        if (e != cudaSuccess) return cuda_error(c, e, "separable factor alloc");
-        for (int d = 0; d < 3; ++d) f.ka[d] = d < c->dim ? separable_rate(c, a, d) : 0.0;
-        const unsigned tg = (unsigned)std::min<int64_t>((a.nt + 255) / 256, 148 * 8);
-        if (c->dim == 2)
-            k_trunc_tsep<2><<<tg, 256, 0, st>>>(a.nt, c->y.p, a.o[0], a.o[1], a.o[2], f.ka[0],
-                                                                 f.ka[1], f.ka[2], c->tsep.p);
-        else
-            k_trunc_tsep<3><<<tg, 256, 0, st>>>(a.nt, c->y.p, a.o[0], a.o[1], a.o[2], f.ka[0],
-                                                                 f.ka[1], f.ka[2], c->tsep.p);
-        c->klaunch[1] += 1;
-        f.tsep = c->tsep.p;
-    }
     for (size_t gi = 0; gi < groups.size(); ++gi) {
         f.do_a = gi == 0;
         f.do_b = 1;
