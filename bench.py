@@ -278,13 +278,15 @@ class ClockSampler:
 
 # DRAM traffic per launch of the dominant kernels (dram__bytes_read.sum +
 # dram__bytes_write.sum), from one ncu capture each:
-#   k_fused, trunc_3d (2,097,152 points x 100,000 targets), HYBRID:
-#     ncu --set full --clock-control none -k regex:k_fused -s 3 -c 1
+#   k_fused, trunc_3d (2,097,152 points x 100,000 targets), HYBRID (FP32
+#   gradient partials): 130,609,408 read + 167,453,952 written, from
+#     ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum
+#         --clock-control none -k regex:k_fused -s 3 -c 1 --csv
 #         python bench.py --steps 1 --warmup 3 --no-cpu-baseline --no-extra
 #   k_value_dense / k_grad_dense, dense_2d: the inputs (0.9 MB) stay in L2, so
 #     DRAM traffic is not a meaningful bound there (null).
 TRAFFIC_BYTES = {
-    ("trunc_3d", "hybrid"): 487960576.0,
+    ("trunc_3d", "hybrid"): 298063360.0,
 }
 
 
