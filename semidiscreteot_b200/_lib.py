@@ -38,7 +38,7 @@ EXPORTED = [
     "sdot_compute_geometric_radius_bound", "sdot_set_distance_function", "sdot_evaluate_partial_device",
     "sdot_set_state", "sdot_get_stream", "sdot_set_profiling", "sdot_get_kernel_times", "sdot_measure_peaks",
     "sdot_evaluate_device_noalloc", "sdot_hessian_device", "sdot_set_hessian_chunk", "sdot_set_hessian_wait_limit",
-    "sdot_set_hessian_generation",
+    "sdot_set_hessian_generation", "sdot_set_hessian_pairs",
     "sdot_solve_newton", "sdot_set_newton_hessian_reuse", "sdot_hessian_tile_count", "sdot_hessian_tiles_device",
     "sdot_hessian_matvec_device", "sdot_softmax_refinement", "sdot_weighted_barycenters", "sdot_conditioned_densities",
     "sdot_batch_create", "sdot_batch_destroy", "sdot_batch_last_error", "sdot_batch_size", "sdot_batch_set_verbose",
@@ -177,6 +177,8 @@ def load():
     lib.sdot_set_hessian_wait_limit.restype = ip
     lib.sdot_set_hessian_generation.argtypes = [vp, ip, vp]
     lib.sdot_set_hessian_generation.restype = ip
+    lib.sdot_set_hessian_pairs.argtypes = [vp, ip, vp]
+    lib.sdot_set_hessian_pairs.restype = ip
     lib.sdot_solve_newton.argtypes = [vp, vp, C.POINTER(SolverParams), ip, C.POINTER(NewtonInfo)]
     lib.sdot_solve_newton.restype = ip
     lib.sdot_set_newton_hessian_reuse.argtypes = [vp, d]

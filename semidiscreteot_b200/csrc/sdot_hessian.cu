@@ -310,6 +310,14 @@ extern "C" sdot_status sdot_set_hessian_generation(sdot_ctx *c, int factored, in
     return SDOT_OK;
 }
 
+extern "C" sdot_status sdot_set_hessian_pairs(sdot_ctx *c, int pairs, int *last_pairs)
+{
+    if (!c) return SDOT_EINVAL;
+    if (pairs >= 0) c->hess_pair = pairs != 0;
+    if (last_pairs) *last_pairs = c->hess_last_pair ? 1 : 0;
+    return SDOT_OK;
+}
+
 extern "C" sdot_status sdot_set_hessian_wait_limit(sdot_ctx *c, int64_t clocks)
 {
     if (!c) return SDOT_EINVAL;

@@ -214,6 +214,90 @@ __device__ __forceinline__ f2 mul2(f2 a, f2 b)
     return d;
 }
 
+// Shared-memory layout per CTA.  PAIR: the CTA is one of an SM pair that
+// runs M = 256 products together (tcgen05 cta_group::2): each CTA holds its
+// 128 A rows and half of the 256 B rows of a stage, and its TMEM holds its
+// 128 rows x 256 columns of the tile.
+template <bool PAIR>
+struct Lay {
+    static constexpr int NB = PAIR ? N / 2 : N;          // B rows this CTA generates per stage
+    static constexpr int ROWS = M + NB;
+    static constexpr int RPT = ROWS / RG;
+    static constexpr uint32_t B_BYTES = NB * KQ * 2;
+    static constexpr uint32_t STAGE_BYTES = 2 * (A_BYTES + B_BYTES);
+    static constexpr uint32_t OFF_EG = 2 * STAGE_BYTES;
+    static constexpr uint32_t OFF_QS = OFF_EG + 2 * ROWS * 32;
+    static constexpr uint32_t OFF_RAW = OFF_QS + 2 * 8 * QS_STRIDE * 4;
+    static constexpr uint32_t OFF_BAR = OFF_RAW + 2 * RAW_BYTES;
+    static constexpr uint32_t SMEM_BYTES = OFF_BAR + 64 + 1024;
+    static constexpr int TILE_ROWS = PAIR ? 2 * M : M;     // rows a of a tile
+    static_assert(ROWS % RG == 0 && THREADS >= ROWS + 2 * KQ, "row split");
+};
+// M = 256 over the pair: M >> 4 = 16 at bits 24-28.
+constexpr uint32_t IDESC2 = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | (16u << 24);
+
+__device__ __forceinline__ void umma_bf16_pair(uint32_t dtmem, uint64_t ad, uint64_t bd, uint32_t accum)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(dtmem),
+        "l"(ad), "l"(bd), "r"(IDESC2), "r"(accum));
+}
+
+// Arrive on the mbarrier at the same offset in every CTA of the mask once the
+// pair's products issued so far are complete.
+__device__ __forceinline__ void umma_commit_pair(uint32_t bar, uint16_t mask)
+{
+    asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(bar),
+                 "h"(mask)
+                 : "memory");
+}
+
+__device__ __forceinline__ uint32_t cluster_rank()
+{
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+__device__ __forceinline__ void cluster_sync_all()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// Arrive (release, cluster scope) on the mbarrier at offset bar of CTA cta of the cluster.
+__device__ __forceinline__ void mbar_arrive_remote(uint32_t bar, uint32_t cta)
+{
+    asm volatile(
+        "{\n\t.reg .b32 ra;\n\t"
+        "mapa.shared::cluster.u32 ra, %0, %1;\n\t"
+        "mbarrier.arrive.release.cluster.shared::cluster.b64 _, [ra];\n\t}" ::"r"(bar),
+        "r"(cta)
+        : "memory");
+}
+
+// Bounded wait with acquire at cluster scope (the phase completed by a remote arrive).
+__device__ __forceinline__ bool mbar_wait_cluster(uint32_t bar, uint32_t parity, long long limit)
+{
+    auto test = [&]() -> bool {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.test_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        return ok != 0;
+    };
+    if (test()) return true;
+    const long long t0 = clock64();
+    while (!test())
+        if (clock64() - t0 > limit) return false;
+    return true;
+}
+
 // 32 lanes x 16 consecutive 32-bit columns; the wait is in the same asm so the
 // registers are never read before the load has landed.
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
@@ -262,45 +346,67 @@ struct Args {
 // Every intermediate is a corner value 2^(E + G.d_q + F_c), within
 // prod_d r_d^(+-1) of the cell's largest value, so none leaves FP32 where
 // the per-point form would not.
-template <int DIM, typename OutT, bool FACT>
+template <int DIM, typename OutT, bool FACT, bool PAIR>
 __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
 {
+    using L = Lay<PAIR>;
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw_s = smem_u32(smem_raw);
     uint8_t *sm = smem_raw + ((1024u - (raw_s & 1023u)) & 1023u);  // 1024-aligned shared address
     const uint32_t sm_s = smem_u32(sm);
-    float *Eg = reinterpret_cast<float *>(sm + OFF_EG);
-    float *qs = reinterpret_cast<float *>(sm + OFF_QS);
-    const uint32_t bar0 = sm_s + OFF_BAR;  // [0,1] stage buffers, [2,3] accumulators (8 bytes each)
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + OFF_BAR + 32);
+    float *Eg = reinterpret_cast<float *>(sm + L::OFF_EG);
+    float *qs = reinterpret_cast<float *>(sm + L::OFF_QS);
+    // mbarriers (8 bytes each): [0,1] stage buffers, [2,3] accumulators, and
+    // with PAIR [5,6] (offsets 40, 48): the peer's half of stage buffer 0 / 1
+    // is in its shared memory (used by the pair's leader, rank 0)
+    const uint32_t bar0 = sm_s + L::OFF_BAR;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + L::OFF_BAR + 32);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t rank = PAIR ? cluster_rank() : 0u;
     if (tid == 0) {
         for (int i = 0; i < 4; ++i) mbar_init(bar0 + 8 * i, 1);
+        if constexpr (PAIR) {
+            mbar_init(bar0 + 40, 1);
+            mbar_init(bar0 + 48, 1);
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
-                     "r"(TMEM_COLS)
-                     : "memory");
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+        if constexpr (PAIR) {
+            asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                         "r"(TMEM_COLS)
+                         : "memory");
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+        } else {
+            asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                         "r"(TMEM_COLS)
+                         : "memory");
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+        }
     }
     tc_fence_before();
     __syncthreads();
+    if constexpr (PAIR) cluster_sync_all();   // both CTAs' barriers are initialised before any remote arrive
     tc_fence_after();
     const uint32_t tmem = *tslot;
+    // tiles: one per CTA, or one per pair (PAIR: TILE_ROWS = 256 rows a, this CTA's half at 128 rank)
+    const int t0 = PAIR ? (int)(blockIdx.x >> 1) : (int)blockIdx.x;
+    const int tstride = PAIR ? (int)(gridDim.x >> 1) : (int)gridDim.x;
+    const int64_t rhalf = PAIR ? (int64_t)M * rank : 0;
 
     // ---- staging of the per-stage inputs ----
     // The block and point data of stage g + 2 are copied by cp.async into
     // raw[g % 2] while stage g is generated; at the end of stage g every
     // thread turns one item of raw[(g + 1) % 2] (and its target row, held in
     // registers for the whole tile) into the FP32 operands of stage g + 1.
-    uint8_t *raw = sm + OFF_RAW;
-    const uint32_t rawb_s = sm_s + OFF_RAW;
-    double4 pt = make_double4(0, 0, 0, 0);   // target row tid (tid < ROWS) of the current tile
+    uint8_t *raw = sm + L::OFF_RAW;
+    const uint32_t rawb_s = sm_s + L::OFF_RAW;
+    double4 pt = make_double4(0, 0, 0, 0);   // target row tid (tid < L::ROWS) of the current tile
     auto load_target = [&](int2 tl) {
-        if (tid < ROWS) {
-            const int64_t j = tid < M ? (int64_t)tl.x * M + tid : (int64_t)tl.y * N + (tid - M);
+        if (tid < L::ROWS) {
+            const int64_t j = tid < M ? (int64_t)tl.x * L::TILE_ROWS + rhalf + tid
+                                      : (int64_t)tl.y * N + rhalf + (tid - M);
             pt = a.tdat[j];
         }
     };
@@ -320,37 +426,37 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
     };
     auto stage_store = [&](int buf) {         // raw[buf] + pt -> Eg / qs [buf]
         const uint8_t *rb = raw + buf * RAW_BYTES;
-        if (tid < ROWS) {
+        if (tid < L::ROWS) {
             const double4 pb = *reinterpret_cast<const double4 *>(rb);
             const double dx = pt.x - pb.x, dy = pt.y - pb.y, dz = DIM == 3 ? pt.z - pb.z : 0.0;
             const float e = (float)(pt.w - 0.5 * a.l2e_eps * (dx * dx + dy * dy + dz * dz) - pb.w);
             const float gx = (float)(a.l2e_eps * dx), gy = (float)(a.l2e_eps * dy), gz = (float)(a.l2e_eps * dz);
-            float4 *dst = reinterpret_cast<float4 *>(Eg + (buf * ROWS + tid) * 8);
+            float4 *dst = reinterpret_cast<float4 *>(Eg + (buf * L::ROWS + tid) * 8);
             dst[0] = make_float4(e, e, gx, gx);
             dst[1] = make_float4(gy, gy, gz, gz);
         } else if constexpr (FACT) {
             // chunk layout in qs: [0, 3) dc, 3 F_c^B, [4, 7) a, 7 F_c^A,
             // [8, 16) 2^(F^B - F_c^B), [16, 24) 2^(F^A - F_c^A)
-            if (tid < ROWS + KQ) {
-                const int p = tid - ROWS;
+            if (tid < L::ROWS + KQ) {
+                const int p = tid - L::ROWS;
                 const float2 wv = reinterpret_cast<const float2 *>(rb + 32 + 256)[p];
                 float *d = qs + (buf * 8 + (p >> 3)) * QS_STRIDE + (p & 7);
                 d[8] = wv.x;
                 d[16] = wv.y;
-            } else {
-                const int t = tid - ROWS - KQ;       // 64 threads: chunk t >> 3, float t & 7
+            } else if (tid < L::ROWS + 2 * KQ) {
+                const int t = tid - L::ROWS - KQ;       // 64 threads: chunk t >> 3, float t & 7
                 qs[(buf * 8 + (t >> 3)) * QS_STRIDE + (t & 7)] = reinterpret_cast<const float *>(rb + 32)[t];
             }
-        } else if (tid < ROWS + KQ) {
-            const int p = tid - ROWS;            // point p of the stage: K-chunk p >> 3, slot p & 7
+        } else if (tid < L::ROWS + KQ) {
+            const int p = tid - L::ROWS;            // point p of the stage: K-chunk p >> 3, slot p & 7
             const float4 pq = reinterpret_cast<const float4 *>(rb + 32)[p];
             float *d = qs + (buf * 8 + (p >> 3)) * QS_STRIDE + (p & 7);
             d[0] = pq.x;
             d[8] = pq.y;
             d[16] = pq.z;
             d[24] = pq.w;
-        } else {
-            const int p = tid - ROWS - KQ;
+        } else if (tid < L::ROWS + 2 * KQ) {
+            const int p = tid - L::ROWS - KQ;
             qs[(buf * 8 + (p >> 3)) * QS_STRIDE + 32 + (p & 7)] = reinterpret_cast<const float *>(rb + 32 + KQ * 16)[p];
         }
     };
@@ -381,18 +487,18 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
                 dz[2 * h + 1] = pack2(z4.z, z4.w);
             }
         }
-        uint8_t *stage = sm + buf * STAGE_BYTES;
+        uint8_t *stage = sm + buf * L::STAGE_BYTES;
         // each row's E/G are loaded one row ahead, before the previous row's
         // stores, so that the rows' chains can overlap
-        const float4 *eg0 = reinterpret_cast<const float4 *>(Eg + (buf * ROWS + rg) * 8);
+        const float4 *eg0 = reinterpret_cast<const float4 *>(Eg + (buf * L::ROWS + rg) * 8);
         float4 e0 = eg0[0], e1 = eg0[1];
 #pragma unroll
-        for (int it = 0; it < RPT; ++it) {
+        for (int it = 0; it < L::RPT; ++it) {
             const bool isA = it < ARPT;
             const int r = rg + RG * it;
             const f2 E = pack2(e0.x, e0.y), Gx = pack2(e0.z, e0.w), Gy = pack2(e1.x, e1.y), Gz = pack2(e1.z, e1.w);
-            if (it + 1 < RPT) {
-                const float4 *egn = reinterpret_cast<const float4 *>(Eg + (buf * ROWS + r + RG) * 8);
+            if (it + 1 < L::RPT) {
+                const float4 *egn = reinterpret_cast<const float4 *>(Eg + (buf * L::ROWS + r + RG) * 8);
                 e0 = egn[0];
                 e1 = egn[1];
             }
@@ -418,7 +524,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
             const int rr = isA ? r : r - M;
             const uint32_t off = (uint32_t)(rr >> 3) * 1024u + (uint32_t)(rr & 7) * 128u + ((uint32_t)(kc ^ (rr & 7)) << 4);
             uint8_t *hi = stage + (isA ? 0u : 2u * A_BYTES);
-            uint8_t *lo = hi + (isA ? A_BYTES : B_BYTES);
+            uint8_t *lo = hi + (isA ? A_BYTES : L::B_BYTES);
             *reinterpret_cast<uint4 *>(hi + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
             *reinterpret_cast<uint4 *>(lo + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
         }
@@ -440,16 +546,16 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
             wa[2 * h] = pack2(c4.x, c4.y);
             wa[2 * h + 1] = pack2(c4.z, c4.w);
         }
-        uint8_t *stage = sm + buf * STAGE_BYTES;
-        const float4 *eg0 = reinterpret_cast<const float4 *>(Eg + (buf * ROWS + rg) * 8);
+        uint8_t *stage = sm + buf * L::STAGE_BYTES;
+        const float4 *eg0 = reinterpret_cast<const float4 *>(Eg + (buf * L::ROWS + rg) * 8);
         float4 e0 = eg0[0], e1 = eg0[1];
 #pragma unroll
-        for (int it = 0; it < RPT; ++it) {
+        for (int it = 0; it < L::RPT; ++it) {
             const bool isA = it < ARPT;
             const int r = rg + RG * it;
             const float E = e0.x, Gx = e0.z, Gy = e1.x, Gz = e1.z;
-            if (it + 1 < RPT) {
-                const float4 *egn = reinterpret_cast<const float4 *>(Eg + (buf * ROWS + r + RG) * 8);
+            if (it + 1 < L::RPT) {
+                const float4 *egn = reinterpret_cast<const float4 *>(Eg + (buf * L::ROWS + r + RG) * 8);
                 e0 = egn[0];
                 e1 = egn[1];
             }
@@ -482,7 +588,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
             const int rr = isA ? r : r - M;
             const uint32_t off = (uint32_t)(rr >> 3) * 1024u + (uint32_t)(rr & 7) * 128u + ((uint32_t)(kc ^ (rr & 7)) << 4);
             uint8_t *hi = stage + (isA ? 0u : 2u * A_BYTES);
-            uint8_t *lo = hi + (isA ? A_BYTES : B_BYTES);
+            uint8_t *lo = hi + (isA ? A_BYTES : L::B_BYTES);
             *reinterpret_cast<uint4 *>(hi + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
             *reinterpret_cast<uint4 *>(lo + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
         }
@@ -502,7 +608,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
             tc_fence_before();
             return false;
         }
-        const int64_t ga = (int64_t)tl.x * M + row;
+        const int64_t ga = (int64_t)tl.x * L::TILE_ROWS + rhalf + row;
         const uint32_t taddr = tmem + (pc & 1) * N + cq * 64 + ((uint32_t)(quad * 32) << 16);
 #pragma unroll 1
         for (int c16 = 0; c16 < 4; ++c16) {
@@ -540,9 +646,9 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
     bool aborted = false;
     unsigned ncommit[4] = {0, 0, 0, 0};  // commits issued per mbarrier (thread 0)
 
-    if ((int)blockIdx.x < a.ntiles) {
+    if (t0 < a.ntiles) {
         // stage 0 into Eg/qs[0]; stage 1's inputs into raw[1]
-        load_target(a.tiles[blockIdx.x]);
+        load_target(a.tiles[t0]);
         raw_copy(0, 0);
         cp_async_wait_all();
         __syncthreads();
@@ -555,14 +661,14 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
     // One block-wide barrier per stage: it publishes the stage's operands to
     // the MMA thread and orders the previous drain's TMEM reads before any MMA
     // that reuses that accumulator.
-    for (int t = blockIdx.x; t < a.ntiles && !aborted; t += gridDim.x) {
+    for (int t = t0; t < a.ntiles && !aborted; t += tstride) {
         // tile coordinates of this and the next tile, loaded once per tile
         const int2 tl_cur = a.tiles[t];
-        const int2 tl_nxt = t + (int)gridDim.x < a.ntiles ? a.tiles[t + gridDim.x] : tl_cur;
+        const int2 tl_nxt = t + tstride < a.ntiles ? a.tiles[t + tstride] : tl_cur;
         for (int st = 0; st < a.nst; ++st, ++g) {
             const int sb = g & 1;
             const bool last_of_tile = st + 1 == a.nst;
-            const bool has_next = !last_of_tile || t + (int)gridDim.x < a.ntiles;
+            const bool has_next = !last_of_tile || t + tstride < a.ntiles;
             raw_copy(sb, (st + 2) % a.nst);     // inputs of stage g + 2 (its point block)
             // the MMAs that read this buffer two stages ago must be complete
             if (g >= 2 && !mbar_wait(bar0 + 8 * sb, ((g >> 1) - 1) & 1, a.wait_limit)) bad = true;
@@ -579,23 +685,54 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
             const bool last_in_chunk = (st % a.ch) == a.ch - 1 || st == a.nst - 1;
             const unsigned cb = chunk & 1;
             if (tid == 0) {
-                tc_fence_after();
-                const uint32_t sbase = sm_s + sb * STAGE_BYTES;
-                const uint32_t dcol = tmem + cb * N;
+                if constexpr (PAIR) {
+                    if (rank != 0) {
+                        // this CTA's half of stage g is written (and fenced for the async proxy)
+                        mbar_arrive_remote(bar0 + 40 + 8 * sb, 0);
+                        // the leader's commits arrive here too
+                        ++ncommit[sb];
+                        if (last_in_chunk) ++ncommit[2 + cb];
+                    } else if (!mbar_wait_cluster(bar0 + 40 + 8 * sb, (g >> 1) & 1, a.wait_limit)) {
+                        bad = true;
+                    } else {
+                        tc_fence_after();
+                        const uint32_t sbase = sm_s + sb * L::STAGE_BYTES;
+                        const uint32_t dcol = tmem + cb * N;
 #pragma unroll
-                for (int kk = 0; kk < KQ / 16; ++kk) {
-                    const uint64_t ah = sdesc(sbase + kk * 32), al = sdesc(sbase + A_BYTES + kk * 32);
-                    const uint64_t bh = sdesc(sbase + 2 * A_BYTES + kk * 32);
-                    const uint64_t bl = sdesc(sbase + 2 * A_BYTES + B_BYTES + kk * 32);
-                    umma_bf16(dcol, ah, bh, (first_in_chunk && kk == 0) ? 0u : 1u);
-                    umma_bf16(dcol, ah, bl, 1u);
-                    umma_bf16(dcol, al, bh, 1u);
-                }
-                umma_commit(bar0 + 8 * sb);
-                ++ncommit[sb];
-                if (last_in_chunk) {
-                    umma_commit(bar0 + 8 * (2 + cb));
-                    ++ncommit[2 + cb];
+                        for (int kk = 0; kk < KQ / 16; ++kk) {
+                            const uint64_t ah = sdesc(sbase + kk * 32), al = sdesc(sbase + A_BYTES + kk * 32);
+                            const uint64_t bh = sdesc(sbase + 2 * A_BYTES + kk * 32);
+                            const uint64_t bl = sdesc(sbase + 2 * A_BYTES + L::B_BYTES + kk * 32);
+                            umma_bf16_pair(dcol, ah, bh, (first_in_chunk && kk == 0) ? 0u : 1u);
+                            umma_bf16_pair(dcol, ah, bl, 1u);
+                            umma_bf16_pair(dcol, al, bh, 1u);
+                        }
+                        umma_commit_pair(bar0 + 8 * sb, 3);
+                        ++ncommit[sb];
+                        if (last_in_chunk) {
+                            umma_commit_pair(bar0 + 8 * (2 + cb), 3);
+                            ++ncommit[2 + cb];
+                        }
+                    }
+                } else {
+                    tc_fence_after();
+                    const uint32_t sbase = sm_s + sb * L::STAGE_BYTES;
+                    const uint32_t dcol = tmem + cb * N;
+#pragma unroll
+                    for (int kk = 0; kk < KQ / 16; ++kk) {
+                        const uint64_t ah = sdesc(sbase + kk * 32), al = sdesc(sbase + A_BYTES + kk * 32);
+                        const uint64_t bh = sdesc(sbase + 2 * A_BYTES + kk * 32);
+                        const uint64_t bl = sdesc(sbase + 2 * A_BYTES + L::B_BYTES + kk * 32);
+                        umma_bf16(dcol, ah, bh, (first_in_chunk && kk == 0) ? 0u : 1u);
+                        umma_bf16(dcol, ah, bl, 1u);
+                        umma_bf16(dcol, al, bh, 1u);
+                    }
+                    umma_commit(bar0 + 8 * sb);
+                    ++ncommit[sb];
+                    if (last_in_chunk) {
+                        umma_commit(bar0 + 8 * (2 + cb));
+                        ++ncommit[2 + cb];
+                    }
                 }
             }
             // drain the previous chunk while the tensor core works on this one
@@ -628,9 +765,15 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
     }
     tc_fence_before();
     __syncthreads();
+    // PAIR: neither CTA frees its tensor memory or exits while the pair's
+    // products or commits may still reach it
+    if constexpr (PAIR) cluster_sync_all();
     tc_fence_after();
     if (warp == 0) {
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+        if constexpr (PAIR)
+            asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+        else
+            asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
     }
 }
 
@@ -774,17 +917,30 @@ sdot_status hessian_tc(sdot_ctx *c, void *H_dev, bool out_f32, int chunk_stages,
     using namespace htc;
     const int64_t n = c->nt;
     const int64_t na = (n + M - 1) / M, nb = (n + N - 1) / N;
-    const int64_t npad = std::max(na * M, nb * N);
     const int64_t nst = (c->nq + KQ - 1) / KQ;
     if (nst > INT32_MAX / 2) return set_error(c, SDOT_EINVAL, "too many quadrature points for the tensor-core Hessian");
     std::vector<int2> tiles;
     tiles.reserve((size_t)(na * nb));
     for (int64_t ta = 0; ta < na; ++ta)
         for (int64_t tb = (ta * M) / N; tb < nb; ++tb) tiles.push_back(make_int2((int)ta, (int)tb));
-    if (tile_end < 0 || tile_end > (int64_t)tiles.size()) tile_end = (int64_t)tiles.size();
+    const int64_t ntile1 = (int64_t)tiles.size();
+    if (tile_end < 0 || tile_end > ntile1) tile_end = ntile1;
     if (tile_begin < 0) tile_begin = 0;
     if (tile_begin > tile_end) tile_begin = tile_end;
-    tiles = std::vector<int2>(tiles.begin() + tile_begin, tiles.begin() + tile_end);
+    // The whole matrix runs on SM pairs (256 x 256 tiles, M = 256 products
+    // over two SMs) unless that is switched off; a range of the 128 x 256
+    // tiles (sharding) runs on single SMs.
+    const bool pair = c->hess_pair && tile_begin == 0 && tile_end == ntile1;
+    int64_t npad = std::max(na * M, nb * N);
+    if (pair) {
+        const int64_t n2 = (n + 2 * M - 1) / (2 * M);
+        npad = std::max(npad, n2 * 2 * M);
+        tiles.clear();
+        for (int64_t ta = 0; ta < n2; ++ta)
+            for (int64_t tb = ta; tb < n2; ++tb) tiles.push_back(make_int2((int)ta, (int)tb));
+    } else {
+        tiles = std::vector<int2>(tiles.begin() + tile_begin, tiles.begin() + tile_end);
+    }
     if (tiles.empty()) {
         c->hess_tiles = 0;
         if (ms_out) *ms_out = 0.0;
@@ -792,7 +948,9 @@ sdot_status hessian_tc(sdot_ctx *c, void *H_dev, bool out_f32, int chunk_stages,
     }
     int dev_sms = 148;
     cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c->device);
-    const int grid = (int)std::min<int64_t>((int64_t)dev_sms, (int64_t)tiles.size());
+    // PAIR: two CTAs (one cluster) per tile at a time, one CTA per SM
+    const int grid = pair ? 2 * (int)std::min<int64_t>((int64_t)(dev_sms / 2), (int64_t)tiles.size())
+                          : (int)std::min<int64_t>((int64_t)dev_sms, (int64_t)tiles.size());
 
     cudaError_t e = c->htc_tdat.alloc((size_t)npad * 4);
     if (e == cudaSuccess) e = c->htc_diag.alloc((size_t)npad);
@@ -857,14 +1015,39 @@ sdot_status hessian_tc(sdot_ctx *c, void *H_dev, bool out_f32, int chunk_stages,
     a.cd = cdp;
     a.qw = qwp;
     void (*kern)(const Args) = nullptr;
-    if (c->dim == 2) kern = out_f32 ? k_hessian_tc<2, float, false> : k_hessian_tc<2, double, false>;
-    else if (fact) kern = out_f32 ? k_hessian_tc<3, float, true> : k_hessian_tc<3, double, true>;
-    else kern = out_f32 ? k_hessian_tc<3, float, false> : k_hessian_tc<3, double, false>;
+    if (pair) {
+        if (c->dim == 2) kern = out_f32 ? k_hessian_tc<2, float, false, true> : k_hessian_tc<2, double, false, true>;
+        else if (fact) kern = out_f32 ? k_hessian_tc<3, float, true, true> : k_hessian_tc<3, double, true, true>;
+        else kern = out_f32 ? k_hessian_tc<3, float, false, true> : k_hessian_tc<3, double, false, true>;
+    } else {
+        if (c->dim == 2) kern = out_f32 ? k_hessian_tc<2, float, false, false> : k_hessian_tc<2, double, false, false>;
+        else if (fact) kern = out_f32 ? k_hessian_tc<3, float, true, false> : k_hessian_tc<3, double, true, false>;
+        else kern = out_f32 ? k_hessian_tc<3, float, false, false> : k_hessian_tc<3, double, false, false>;
+    }
     c->hess_last_factored = fact;
-    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES);
+    c->hess_last_pair = pair;
+    const uint32_t smem = pair ? Lay<true>::SMEM_BYTES : Lay<false>::SMEM_BYTES;
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return cuda_error(c, e, "tensor-core Hessian attribute");
     if (c->profiling) cudaEventRecord(c->pev[0], c->stream);
-    kern<<<grid, THREADS, SMEM_BYTES, c->stream>>>(a);
+    if (pair) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)grid);
+        cfg.blockDim = dim3(THREADS);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = c->stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = 2;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        e = cudaLaunchKernelEx(&cfg, kern, a);
+        if (e != cudaSuccess) return cuda_error(c, e, "tensor-core Hessian launch (SM pairs)");
+    } else {
+        kern<<<grid, THREADS, smem, c->stream>>>(a);
+    }
     if (c->profiling) cudaEventRecord(c->pev[1], c->stream);
     cudaEventRecord(c->ev1, c->stream);
     e = cudaGetLastError();

@@ -344,6 +344,14 @@ class SotSolver:
                                                         C.byref(last)))
         return bool(last.value)
 
+    def set_hessian_pairs(self, pairs: Optional[bool] = None) -> bool:
+        """Whole tensor Hessians on SM pairs (tcgen05 cta_group::2 over 256 x 256
+        tiles; True: on, False: off, the default; None: unchanged).  Returns
+        whether the last tensor Hessian ran on pairs."""
+        last = C.c_int(0)
+        self._check(self._L.sdot_set_hessian_pairs(self._h, -1 if pairs is None else int(bool(pairs)), C.byref(last)))
+        return bool(last.value)
+
     def set_hessian_wait_limit(self, clocks: int):
         """SM clocks a device-side wait of the tensor Hessian may take before the
         call fails with SDOT_ETIMEOUT (<= 0: the default, about 1 s)."""

@@ -216,3 +216,32 @@ def test_factored_generation_not_used_outside_its_bound():
     hessian(s, psi, "tensor")
     assert s.set_hessian_generation(None) is False
     s.close()
+
+
+@pytest.mark.parametrize("kind", ["dense2d", "dense3d", "dense3d_small_eps"])
+def test_sm_pairs_match_single_sm(oracle_mod, kind):
+    """Whole Hessians on SM pairs (tcgen05 cta_group::2 over 256 x 256 tiles)
+    agree with the FP64 oracle within the tensor method's bounds, are exactly
+    symmetric and repeatable, and agree with the single-SM kernel."""
+    src, y, nu, eps = problem(kind, seed=4)
+    N = len(nu)
+    s = make(src, y, nu, eps)
+    psi = 0.3 * eps * np.random.default_rng(8).standard_normal(N)
+    H1, _ = hessian(s, psi, "tensor")
+    assert s.set_hessian_pairs(None) is False
+    s.set_hessian_pairs(True)
+    H2, _ = hessian(s, psi, "tensor")
+    assert s.set_hessian_pairs(None) is True
+    H3, _ = hessian(s, psi, "tensor")
+    s.set_hessian_pairs(False)
+    P = oracle_mod.Problem(src["x"], src["jxw"], src["density"], src["cell_offsets"], src["cell_centers"], y, nu)
+    Ho = P.hessian(psi, oracle_mod.Params(epsilon=eps, tau=0.0, use_log_sum_exp=True), 1e300)
+    assert np.all(np.isfinite(H2))
+    assert np.array_equal(H2, H2.T)
+    assert np.array_equal(H2, H3)
+    fro, mx = rel_errors(H2, Ho)
+    print(f"SM pairs vs FP64: Frobenius {fro:.2e}, max {mx:.2e}; single SM: {rel_errors(H1, Ho)}")
+    assert fro <= FRO_TOL and mx <= MAX_TOL, (fro, mx)
+    fro12, _ = rel_errors(H2, H1)
+    assert fro12 <= FRO_TOL
+    s.close()
