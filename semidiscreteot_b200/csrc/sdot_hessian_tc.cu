@@ -225,12 +225,20 @@ struct Lay {
     static constexpr int RPT = ROWS / RG;
     static constexpr uint32_t B_BYTES = NB * KQ * 2;
     static constexpr uint32_t STAGE_BYTES = 2 * (A_BYTES + B_BYTES);
-    static constexpr uint32_t OFF_EG = 2 * STAGE_BYTES;
+    static constexpr int NS = PAIR ? 3 : 2;                 // operand stage buffers (PAIR: 64 KB each)
+    static constexpr uint32_t OFF_EG = NS * STAGE_BYTES;
     static constexpr uint32_t OFF_QS = OFF_EG + 2 * ROWS * 32;
     static constexpr uint32_t OFF_RAW = OFF_QS + 2 * 8 * QS_STRIDE * 4;
     static constexpr uint32_t OFF_BAR = OFF_RAW + 2 * RAW_BYTES;
-    static constexpr uint32_t SMEM_BYTES = OFF_BAR + 64 + 1024;
+    // mbarriers (8 bytes each) from OFF_BAR: NS stage buffers, 2 accumulators,
+    // the TMEM address, and with PAIR NS more: the peer's half of each stage
+    // buffer is in its shared memory (waited on by the pair's leader)
+    static constexpr uint32_t BAR_ACC = 8 * NS;
+    static constexpr uint32_t BAR_TSLOT = 8 * (NS + 2);
+    static constexpr uint32_t BAR_FULL = 8 * (NS + 3);
+    static constexpr uint32_t SMEM_BYTES = OFF_BAR + 128 + 1024;
     static constexpr int TILE_ROWS = PAIR ? 2 * M : M;     // rows a of a tile
+    static_assert(BAR_FULL + 8 * NS <= 128, "barrier region");
     static_assert(ROWS % RG == 0 && THREADS >= ROWS + 2 * KQ, "row split");
 };
 // M = 256 over the pair: M >> 4 = 16 at bits 24-28.
@@ -356,20 +364,15 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
     const uint32_t sm_s = smem_u32(sm);
     float *Eg = reinterpret_cast<float *>(sm + L::OFF_EG);
     float *qs = reinterpret_cast<float *>(sm + L::OFF_QS);
-    // mbarriers (8 bytes each): [0,1] stage buffers, [2,3] accumulators, and
-    // with PAIR [5,6] (offsets 40, 48): the peer's half of stage buffer 0 / 1
-    // is in its shared memory (used by the pair's leader, rank 0)
-    const uint32_t bar0 = sm_s + L::OFF_BAR;
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + L::OFF_BAR + 32);
+    const uint32_t bar0 = sm_s + L::OFF_BAR;   // mbarriers: see Lay
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + L::OFF_BAR + L::BAR_TSLOT);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t rank = PAIR ? cluster_rank() : 0u;
     if (tid == 0) {
-        for (int i = 0; i < 4; ++i) mbar_init(bar0 + 8 * i, 1);
-        if constexpr (PAIR) {
-            mbar_init(bar0 + 40, 1);
-            mbar_init(bar0 + 48, 1);
-        }
+        for (int i = 0; i < L::NS + 2; ++i) mbar_init(bar0 + 8 * i, 1);
+        if constexpr (PAIR)
+            for (int i = 0; i < L::NS; ++i) mbar_init(bar0 + L::BAR_FULL + 8 * i, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -467,7 +470,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
     // truncated to BF16 when packed.
     const int kc = lane & 7;                 // 16-byte chunk (8 points) of the 64-point stage
     const int rg = warp * 4 + (lane >> 3);   // row group
-    auto generate = [&](int buf) {
+    auto generate = [&](int buf, int sb) {
         const float4 *qv = reinterpret_cast<const float4 *>(qs + (buf * 8 + kc) * QS_STRIDE);
         f2 dx[4], dy[4], dz[4], fa[4], fb[4];
 #pragma unroll
@@ -487,7 +490,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
                 dz[2 * h + 1] = pack2(z4.z, z4.w);
             }
         }
-        uint8_t *stage = sm + buf * L::STAGE_BYTES;
+        uint8_t *stage = sm + sb * L::STAGE_BYTES;
         // each row's E/G are loaded one row ahead, before the previous row's
         // stores, so that the rows' chains can overlap
         const float4 *eg0 = reinterpret_cast<const float4 *>(Eg + (buf * L::ROWS + rg) * 8);
@@ -532,7 +535,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
 
     // ---- factored generation (FACT): per (row, cell) one ex2 for the cell and
     // one per dimension; the 8 values by products with the point factors ----
-    auto generate_fact = [&](int buf) {
+    auto generate_fact = [&](int buf, int sb) {
         const float *qc = qs + (buf * 8 + kc) * QS_STRIDE;
         const float4 dc4 = *reinterpret_cast<const float4 *>(qc);
         const float4 a4 = *reinterpret_cast<const float4 *>(qc + 4);
@@ -546,7 +549,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
             wa[2 * h] = pack2(c4.x, c4.y);
             wa[2 * h + 1] = pack2(c4.z, c4.w);
         }
-        uint8_t *stage = sm + buf * L::STAGE_BYTES;
+        uint8_t *stage = sm + sb * L::STAGE_BYTES;
         const float4 *eg0 = reinterpret_cast<const float4 *>(Eg + (buf * L::ROWS + rg) * 8);
         float4 e0 = eg0[0], e1 = eg0[1];
 #pragma unroll
@@ -599,7 +602,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
     const int row = quad * 32 + lane;
     double *scr = a.scratch + (size_t)blockIdx.x * SCR_PER_CTA;
     auto drain = [&](unsigned pc, int2 tl, bool first, bool last) -> bool {
-        const bool ok = mbar_wait(bar0 + 8 * (2 + (pc & 1)), (pc >> 1) & 1, a.wait_limit);
+        const bool ok = mbar_wait(bar0 + L::BAR_ACC + 8 * (pc & 1), (pc >> 1) & 1, a.wait_limit);
         tc_fence_after();
         // a warp reads its accumulator lanes only when every lane saw the
         // commit land (tcgen05.ld is warp-collective); otherwise the kernel is
@@ -644,7 +647,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
     bool pend_first = false, pend_last = false;
     bool bad = false;        // this thread saw a wait expire
     bool aborted = false;
-    unsigned ncommit[4] = {0, 0, 0, 0};  // commits issued per mbarrier (thread 0)
+    unsigned ncommit[L::NS + 2] = {};  // commits issued (or, in a pair's second CTA, due) per mbarrier (thread 0)
 
     if (t0 < a.ntiles) {
         // stage 0 into Eg/qs[0]; stage 1's inputs into raw[1]
@@ -666,17 +669,18 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
         const int2 tl_cur = a.tiles[t];
         const int2 tl_nxt = t + tstride < a.ntiles ? a.tiles[t + tstride] : tl_cur;
         for (int st = 0; st < a.nst; ++st, ++g) {
-            const int sb = g & 1;
+            const int eb = g & 1;          // stage inputs and E/G, point data: double-buffered
+            const int sb = g % L::NS;      // operand stage buffer
             const bool last_of_tile = st + 1 == a.nst;
             const bool has_next = !last_of_tile || t + tstride < a.ntiles;
-            raw_copy(sb, (st + 2) % a.nst);     // inputs of stage g + 2 (its point block)
-            // the MMAs that read this buffer two stages ago must be complete
-            if (g >= 2 && !mbar_wait(bar0 + 8 * sb, ((g >> 1) - 1) & 1, a.wait_limit)) bad = true;
-            if constexpr (FACT) generate_fact(sb);
-            else generate(sb);
+            raw_copy(eb, (st + 2) % a.nst);     // inputs of stage g + 2 (its point block)
+            // the MMAs that read this buffer NS stages ago must be complete
+            if (g >= L::NS && !mbar_wait(bar0 + 8 * sb, ((g / L::NS) - 1) & 1, a.wait_limit)) bad = true;
+            if constexpr (FACT) generate_fact(eb, sb);
+            else generate(eb, sb);
             if (has_next) {
                 if (last_of_tile) load_target(tl_nxt);   // once per tile
-                stage_store(sb ^ 1);
+                stage_store(eb ^ 1);
             }
             cp_async_wait_all();
             fence_async_smem();
@@ -688,11 +692,11 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
                 if constexpr (PAIR) {
                     if (rank != 0) {
                         // this CTA's half of stage g is written (and fenced for the async proxy)
-                        mbar_arrive_remote(bar0 + 40 + 8 * sb, 0);
+                        mbar_arrive_remote(bar0 + L::BAR_FULL + 8 * sb, 0);
                         // the leader's commits arrive here too
                         ++ncommit[sb];
-                        if (last_in_chunk) ++ncommit[2 + cb];
-                    } else if (!mbar_wait_cluster(bar0 + 40 + 8 * sb, (g >> 1) & 1, a.wait_limit)) {
+                        if (last_in_chunk) ++ncommit[L::NS + cb];
+                    } else if (!mbar_wait_cluster(bar0 + L::BAR_FULL + 8 * sb, (g / L::NS) & 1, a.wait_limit)) {
                         bad = true;
                     } else {
                         tc_fence_after();
@@ -710,8 +714,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
                         umma_commit_pair(bar0 + 8 * sb, 3);
                         ++ncommit[sb];
                         if (last_in_chunk) {
-                            umma_commit_pair(bar0 + 8 * (2 + cb), 3);
-                            ++ncommit[2 + cb];
+                            umma_commit_pair(bar0 + L::BAR_ACC + 8 * cb, 3);
+                            ++ncommit[L::NS + cb];
                         }
                     }
                 } else {
@@ -730,8 +734,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
                     umma_commit(bar0 + 8 * sb);
                     ++ncommit[sb];
                     if (last_in_chunk) {
-                        umma_commit(bar0 + 8 * (2 + cb));
-                        ++ncommit[2 + cb];
+                        umma_commit(bar0 + L::BAR_ACC + 8 * cb);
+                        ++ncommit[L::NS + cb];
                     }
                 }
             }
@@ -760,7 +764,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
         // most one phase outstanding here (every earlier phase was waited for
         // successfully, or the loop would have stopped there), so waiting for
         // the phase of its last commit, in order, covers them all.
-        for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < L::NS + 2; ++i)
             if (ncommit[i] > 0) mbar_wait(bar0 + 8 * i, (ncommit[i] - 1) & 1, WAIT_LIMIT);
     }
     tc_fence_before();
