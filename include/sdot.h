@@ -203,7 +203,7 @@ sdot_status sdot_set_hessian_generation(sdot_ctx *ctx, int factored, int *last_f
 /* Whole tensor Hessians on SM pairs (no reference counterpart): 256 x 256
  * tiles whose products run over two SMs (tcgen05 cta_group::2, a cluster of
  * two CTAs), so that each SM generates two thirds of the operand rows it
- * would alone.  pairs = 1 on, 0 off (default), < 0 leaves the setting;
+ * would alone.  pairs = 1 on (default), 0 off, < 0 leaves the setting;
  * *last_pairs (may be NULL) tells whether the last tensor Hessian of the
  * context ran on pairs.  A range of tiles (sdot_hessian_tiles_device) always
  * runs on single SMs. */

@@ -191,7 +191,7 @@ struct sdot_ctx {
     sdot::DevBuf<float> htc_cd, htc_qw;  // factored generation: per-chunk cell data, per-point factors
     bool hess_factored = true;         // factored generation where the source allows it (sdot_set_hessian_generation)
     bool hess_last_factored = false;   // the last tensor Hessian used it
-    bool hess_pair = false;            // whole tensor Hessians on SM pairs (sdot_set_hessian_pairs)
+    bool hess_pair = true;             // whole tensor Hessians on SM pairs (sdot_set_hessian_pairs)
     bool hess_last_pair = false;       // the last tensor Hessian ran on SM pairs
     double hess_kernel_ms = 0.0;
     int64_t hess_tiles = 0;

@@ -346,7 +346,7 @@ class SotSolver:
 
     def set_hessian_pairs(self, pairs: Optional[bool] = None) -> bool:
         """Whole tensor Hessians on SM pairs (tcgen05 cta_group::2 over 256 x 256
-        tiles; True: on, False: off, the default; None: unchanged).  Returns
+        tiles; True: on, the default; False: off; None: unchanged).  Returns
         whether the last tensor Hessian ran on pairs."""
         last = C.c_int(0)
         self._check(self._L.sdot_set_hessian_pairs(self._h, -1 if pairs is None else int(bool(pairs)), C.byref(last)))

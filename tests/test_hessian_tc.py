@@ -125,7 +125,13 @@ def test_tensor_hessian_larger_against_fp64_kernel():
     fro, mx = rel_errors(Ht, Hf)
     print(f"2000 targets: Frobenius {fro:.2e}, max {mx:.2e}, tiles {info['tiles']}")
     assert fro <= FRO_TOL and mx <= MAX_TOL
-    assert info["tiles"] == sum(max(0, 8 - (ta * 128) // 256) for ta in range(16))
+    # SM pairs (the default): 256 x 256 tiles of the upper triangle, 8 x 9 / 2
+    assert s.set_hessian_pairs(None) is True and info["tiles"] == 36
+    s.set_hessian_pairs(False)
+    Hs, info = hessian(s, psi, "tensor")
+    assert info["tiles"] == sum(max(0, 8 - (ta * 128) // 256) for ta in range(16))   # single SMs: 128 x 256
+    assert rel_errors(Hs, Hf)[0] <= FRO_TOL
+    s.set_hessian_pairs(True)
     # rows sum to ~0: H 1 = 0 for the exact Hessian (mass conservation)
     assert np.max(np.abs(Ht.sum(axis=1))) <= 1e-3 * np.max(np.abs(Ht))
     s.close()
@@ -220,20 +226,20 @@ def test_factored_generation_not_used_outside_its_bound():
 
 @pytest.mark.parametrize("kind", ["dense2d", "dense3d", "dense3d_small_eps"])
 def test_sm_pairs_match_single_sm(oracle_mod, kind):
-    """Whole Hessians on SM pairs (tcgen05 cta_group::2 over 256 x 256 tiles)
-    agree with the FP64 oracle within the tensor method's bounds, are exactly
-    symmetric and repeatable, and agree with the single-SM kernel."""
+    """Whole Hessians on SM pairs (tcgen05 cta_group::2 over 256 x 256 tiles,
+    the default) agree with the FP64 oracle within the tensor method's bounds,
+    are exactly symmetric and repeatable, and agree with the single-SM kernel."""
     src, y, nu, eps = problem(kind, seed=4)
     N = len(nu)
     s = make(src, y, nu, eps)
     psi = 0.3 * eps * np.random.default_rng(8).standard_normal(N)
-    H1, _ = hessian(s, psi, "tensor")
-    assert s.set_hessian_pairs(None) is False
-    s.set_hessian_pairs(True)
-    H2, _ = hessian(s, psi, "tensor")
+    H2, _ = hessian(s, psi, "tensor")          # SM pairs: the default
     assert s.set_hessian_pairs(None) is True
     H3, _ = hessian(s, psi, "tensor")
     s.set_hessian_pairs(False)
+    H1, _ = hessian(s, psi, "tensor")
+    assert s.set_hessian_pairs(None) is False
+    s.set_hessian_pairs(True)
     P = oracle_mod.Problem(src["x"], src["jxw"], src["density"], src["cell_offsets"], src["cell_centers"], y, nu)
     Ho = P.hessian(psi, oracle_mod.Params(epsilon=eps, tau=0.0, use_log_sum_exp=True), 1e300)
     assert np.all(np.isfinite(H2))
