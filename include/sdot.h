@@ -203,10 +203,12 @@ sdot_status sdot_set_hessian_generation(sdot_ctx *ctx, int factored, int *last_f
 /* Whole tensor Hessians on SM pairs (no reference counterpart): 256 x 256
  * tiles whose products run over two SMs (tcgen05 cta_group::2, a cluster of
  * two CTAs), so that each SM generates two thirds of the operand rows it
- * would alone.  pairs = 1 on (default), 0 off, < 0 leaves the setting;
- * *last_pairs (may be NULL) tells whether the last tensor Hessian of the
- * context ran on pairs.  A range of tiles (sdot_hessian_tiles_device) always
- * runs on single SMs. */
+ * would alone.  pairs = 2 (default): SM pairs, each CTA's operand generation
+ * split into two groups of warps that take alternate stages, with a warp of
+ * its own issuing the products; 1: SM pairs, one generating group; 0: single
+ * SMs (128 x 256 tiles); < 0 leaves the setting.  *last_pairs (may be NULL)
+ * receives the mode the last tensor Hessian of the context ran in.  A range
+ * of tiles (sdot_hessian_tiles_device) always runs on single SMs. */
 sdot_status sdot_set_hessian_pairs(sdot_ctx *ctx, int pairs, int *last_pairs);
 
 /* The tensor-core Hessian in pieces, for sharding it over GPUs by output tiles

@@ -313,8 +313,9 @@ extern "C" sdot_status sdot_set_hessian_generation(sdot_ctx *c, int factored, in
 extern "C" sdot_status sdot_set_hessian_pairs(sdot_ctx *c, int pairs, int *last_pairs)
 {
     if (!c) return SDOT_EINVAL;
-    if (pairs >= 0) c->hess_pair = pairs != 0;
-    if (last_pairs) *last_pairs = c->hess_last_pair ? 1 : 0;
+    if (pairs > 2) return sdot::set_error(c, SDOT_EINVAL, "sdot_set_hessian_pairs: mode 0, 1 or 2");
+    if (pairs >= 0) c->hess_pair_mode = pairs;
+    if (last_pairs) *last_pairs = c->hess_last_pair;
     return SDOT_OK;
 }
 

@@ -236,9 +236,11 @@ struct Lay {
     static constexpr uint32_t BAR_ACC = 8 * NS;
     static constexpr uint32_t BAR_TSLOT = 8 * (NS + 2);
     static constexpr uint32_t BAR_FULL = 8 * (NS + 3);
+    static constexpr uint32_t BAR_READY = BAR_FULL + 8 * NS;   // dual groups: a group's stage is written
+    static constexpr uint32_t ABORT_FLAG = BAR_READY + 8 * NS; // dual groups: an int, set on any failed wait
     static constexpr uint32_t SMEM_BYTES = OFF_BAR + 128 + 1024;
     static constexpr int TILE_ROWS = PAIR ? 2 * M : M;     // rows a of a tile
-    static_assert(BAR_FULL + 8 * NS <= 128, "barrier region");
+    static_assert(ABORT_FLAG + 4 <= 128, "barrier region");
     static_assert(ROWS % RG == 0 && THREADS >= ROWS + 2 * KQ, "row split");
 };
 // M = 256 over the pair: M >> 4 = 16 at bits 24-28.
@@ -283,6 +285,27 @@ __device__ __forceinline__ void mbar_arrive_remote(uint32_t bar, uint32_t cta)
         "mbarrier.arrive.release.cluster.shared::cluster.b64 _, [ra];\n\t}" ::"r"(bar),
         "r"(cta)
         : "memory");
+}
+
+// Named barrier of one generation group (256 threads); returns the OR of v
+// over the group, so that the group leaves its loop together.
+__device__ __forceinline__ bool group_bar_or(int id, bool v)
+{
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 q, %1, 0;\n\t"
+        "bar.red.or.pred p, %2, 256, q;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(r)
+        : "r"((uint32_t)v), "r"(id)
+        : "memory");
+    return r != 0;
+}
+__device__ __forceinline__ void group_bar(int id) { asm volatile("bar.sync %0, 256;" ::"r"(id) : "memory"); }
+__device__ __forceinline__ void mbar_arrive_local(uint32_t bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
 // Bounded wait with acquire at cluster scope (the phase completed by a remote arrive).
@@ -354,10 +377,21 @@ struct Args {
 // Every intermediate is a corner value 2^(E + G.d_q + F_c), within
 // prod_d r_d^(+-1) of the cell's largest value, so none leaves FP32 where
 // the per-point form would not.
-template <int DIM, typename OutT, bool FACT, bool PAIR>
-__global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
+// DG (dual groups, with PAIR): warps 0-7 and 8-15 generate alternate stages,
+// each group synchronising on its own named barrier, and warp 16 issues the
+// products in stage order once a stage's group has signalled it (and, in the
+// pair's leader, once the peer's half has arrived); a group drains its half of
+// the accumulator columns.  One group's barrier waits then overlap the other
+// group's generation.
+constexpr int DG_THREADS = THREADS + 32;
+template <int DIM, typename OutT, bool FACT, bool PAIR, bool DG>
+__global__ void __launch_bounds__(DG ? DG_THREADS : THREADS, 1) k_hessian_tc(const Args a)
 {
+    static_assert(!DG || PAIR, "dual groups run on SM pairs");
     using L = Lay<PAIR>;
+    constexpr int RGX = DG ? RG / 2 : RG;          // row groups of one generating group
+    constexpr int RPTX = L::ROWS / RGX;            // rows per thread per stage
+    constexpr int ARPTX = M / RGX;                 // of which A rows
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw_s = smem_u32(smem_raw);
     uint8_t *sm = smem_raw + ((1024u - (raw_s & 1023u)) & 1023u);  // 1024-aligned shared address
@@ -373,6 +407,10 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
         for (int i = 0; i < L::NS + 2; ++i) mbar_init(bar0 + 8 * i, 1);
         if constexpr (PAIR)
             for (int i = 0; i < L::NS; ++i) mbar_init(bar0 + L::BAR_FULL + 8 * i, 1);
+        if constexpr (DG) {
+            for (int i = 0; i < L::NS; ++i) mbar_init(bar0 + L::BAR_READY + 8 * i, 1);
+            *reinterpret_cast<volatile int *>(sm + L::OFF_BAR + L::ABORT_FLAG) = 0;
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -405,16 +443,19 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
     // registers for the whole tile) into the FP32 operands of stage g + 1.
     uint8_t *raw = sm + L::OFF_RAW;
     const uint32_t rawb_s = sm_s + L::OFF_RAW;
-    double4 pt = make_double4(0, 0, 0, 0);   // target row tid (tid < L::ROWS) of the current tile
+    // staging items are indexed by tid, or with DG by the thread's index in its group
+    const int sid = DG ? (tid & 255) : tid;
+    double4 pt = make_double4(0, 0, 0, 0);   // target row sid (sid < L::ROWS) of the current tile
     auto load_target = [&](int2 tl) {
-        if (tid < L::ROWS) {
-            const int64_t j = tid < M ? (int64_t)tl.x * L::TILE_ROWS + rhalf + tid
-                                      : (int64_t)tl.y * N + rhalf + (tid - M);
+        if (sid < L::ROWS) {
+            const int64_t j = sid < M ? (int64_t)tl.x * L::TILE_ROWS + rhalf + sid
+                                      : (int64_t)tl.y * N + rhalf + (sid - M);
             pt = a.tdat[j];
         }
     };
     auto raw_copy = [&](int buf, int st) {   // 2 + 64 + 16 copies of 16 bytes (FACT: 2 + 16 + 32)
         const uint32_t d = rawb_s + buf * RAW_BYTES;
+        const int tid = sid;
         if (tid < 2) cp_async16(d + tid * 16, reinterpret_cast<const uint8_t *>(a.blk + st) + tid * 16);
         else if constexpr (FACT) {
             // chunk data: 8 chunks x 2 float4; point factors: 64 float2 = 32 x 16 bytes
@@ -427,7 +468,9 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
         }
         cp_async_commit();
     };
-    auto stage_store = [&](int buf) {         // raw[buf] + pt -> Eg / qs [buf]
+    // raw[buf] + pt -> Eg / qs [buf]: item tid (rows, then points); with DG a
+    // group's 256 threads take the rows and then, the first 128, the points
+    auto stage_store = [&](int buf, int tid) {
         const uint8_t *rb = raw + buf * RAW_BYTES;
         if (tid < L::ROWS) {
             const double4 pb = *reinterpret_cast<const double4 *>(rb);
@@ -469,7 +512,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
     // then v = hi + lo with hi rounded to BF16 and lo = v - hi (exact),
     // truncated to BF16 when packed.
     const int kc = lane & 7;                 // 16-byte chunk (8 points) of the 64-point stage
-    const int rg = warp * 4 + (lane >> 3);   // row group
+    const int rg = (DG ? (warp & 7) : warp) * 4 + (lane >> 3);   // row group (of the thread's generating group)
     auto generate = [&](int buf, int sb) {
         const float4 *qv = reinterpret_cast<const float4 *>(qs + (buf * 8 + kc) * QS_STRIDE);
         f2 dx[4], dy[4], dz[4], fa[4], fb[4];
@@ -496,12 +539,12 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
         const float4 *eg0 = reinterpret_cast<const float4 *>(Eg + (buf * L::ROWS + rg) * 8);
         float4 e0 = eg0[0], e1 = eg0[1];
 #pragma unroll
-        for (int it = 0; it < L::RPT; ++it) {
-            const bool isA = it < ARPT;
-            const int r = rg + RG * it;
+        for (int it = 0; it < RPTX; ++it) {
+            const bool isA = it < ARPTX;
+            const int r = rg + RGX * it;
             const f2 E = pack2(e0.x, e0.y), Gx = pack2(e0.z, e0.w), Gy = pack2(e1.x, e1.y), Gz = pack2(e1.z, e1.w);
-            if (it + 1 < L::RPT) {
-                const float4 *egn = reinterpret_cast<const float4 *>(Eg + (buf * L::ROWS + r + RG) * 8);
+            if (it + 1 < RPTX) {
+                const float4 *egn = reinterpret_cast<const float4 *>(Eg + (buf * L::ROWS + r + RGX) * 8);
                 e0 = egn[0];
                 e1 = egn[1];
             }
@@ -553,12 +596,12 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
         const float4 *eg0 = reinterpret_cast<const float4 *>(Eg + (buf * L::ROWS + rg) * 8);
         float4 e0 = eg0[0], e1 = eg0[1];
 #pragma unroll
-        for (int it = 0; it < L::RPT; ++it) {
-            const bool isA = it < ARPT;
-            const int r = rg + RG * it;
+        for (int it = 0; it < RPTX; ++it) {
+            const bool isA = it < ARPTX;
+            const int r = rg + RGX * it;
             const float E = e0.x, Gx = e0.z, Gy = e1.x, Gz = e1.z;
-            if (it + 1 < L::RPT) {
-                const float4 *egn = reinterpret_cast<const float4 *>(Eg + (buf * L::ROWS + r + RG) * 8);
+            if (it + 1 < RPTX) {
+                const float4 *egn = reinterpret_cast<const float4 *>(Eg + (buf * L::ROWS + r + RGX) * 8);
                 e0 = egn[0];
                 e1 = egn[1];
             }
@@ -640,85 +683,45 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
         return ok;
     };
 
-    int g = 0;               // global stage counter (stage-buffer phases)
-    unsigned chunk = 0;      // global chunk counter (accumulator phases)
-    int pend = -1;
-    int2 pend_tl = make_int2(0, 0);
-    bool pend_first = false, pend_last = false;
-    bool bad = false;        // this thread saw a wait expire
-    bool aborted = false;
-    unsigned ncommit[L::NS + 2] = {};  // commits issued (or, in a pair's second CTA, due) per mbarrier (thread 0)
-
-    if (t0 < a.ntiles) {
-        // stage 0 into Eg/qs[0]; stage 1's inputs into raw[1]
-        load_target(a.tiles[t0]);
-        raw_copy(0, 0);
-        cp_async_wait_all();
-        __syncthreads();
-        stage_store(0);
-        raw_copy(1, a.nst > 1 ? 1 : 0);
-        cp_async_wait_all();
-    }
-    __syncthreads();
-
-    // One block-wide barrier per stage: it publishes the stage's operands to
-    // the MMA thread and orders the previous drain's TMEM reads before any MMA
-    // that reuses that accumulator.
-    for (int t = t0; t < a.ntiles && !aborted; t += tstride) {
-        // tile coordinates of this and the next tile, loaded once per tile
-        const int2 tl_cur = a.tiles[t];
-        const int2 tl_nxt = t + tstride < a.ntiles ? a.tiles[t + tstride] : tl_cur;
-        for (int st = 0; st < a.nst; ++st, ++g) {
-            const int eb = g & 1;          // stage inputs and E/G, point data: double-buffered
-            const int sb = g % L::NS;      // operand stage buffer
-            const bool last_of_tile = st + 1 == a.nst;
-            const bool has_next = !last_of_tile || t + tstride < a.ntiles;
-            raw_copy(eb, (st + 2) % a.nst);     // inputs of stage g + 2 (its point block)
-            // the MMAs that read this buffer NS stages ago must be complete
-            if (g >= L::NS && !mbar_wait(bar0 + 8 * sb, ((g / L::NS) - 1) & 1, a.wait_limit)) bad = true;
-            if constexpr (FACT) generate_fact(eb, sb);
-            else generate(eb, sb);
-            if (has_next) {
-                if (last_of_tile) load_target(tl_nxt);   // once per tile
-                stage_store(eb ^ 1);
-            }
-            cp_async_wait_all();
-            fence_async_smem();
-            if (__syncthreads_or(bad)) { aborted = true; break; }
-            const bool first_in_chunk = (st % a.ch) == 0;
-            const bool last_in_chunk = (st % a.ch) == a.ch - 1 || st == a.nst - 1;
-            const unsigned cb = chunk & 1;
-            if (tid == 0) {
-                if constexpr (PAIR) {
-                    if (rank != 0) {
-                        // this CTA's half of stage g is written (and fenced for the async proxy)
-                        mbar_arrive_remote(bar0 + L::BAR_FULL + 8 * sb, 0);
-                        // the leader's commits arrive here too
-                        ++ncommit[sb];
-                        if (last_in_chunk) ++ncommit[L::NS + cb];
-                    } else if (!mbar_wait_cluster(bar0 + L::BAR_FULL + 8 * sb, (g / L::NS) & 1, a.wait_limit)) {
-                        bad = true;
-                    } else {
-                        tc_fence_after();
-                        const uint32_t sbase = sm_s + sb * L::STAGE_BYTES;
-                        const uint32_t dcol = tmem + cb * N;
-#pragma unroll
-                        for (int kk = 0; kk < KQ / 16; ++kk) {
-                            const uint64_t ah = sdesc(sbase + kk * 32), al = sdesc(sbase + A_BYTES + kk * 32);
-                            const uint64_t bh = sdesc(sbase + 2 * A_BYTES + kk * 32);
-                            const uint64_t bl = sdesc(sbase + 2 * A_BYTES + L::B_BYTES + kk * 32);
-                            umma_bf16_pair(dcol, ah, bh, (first_in_chunk && kk == 0) ? 0u : 1u);
-                            umma_bf16_pair(dcol, ah, bl, 1u);
-                            umma_bf16_pair(dcol, al, bh, 1u);
-                        }
-                        umma_commit_pair(bar0 + 8 * sb, 3);
-                        ++ncommit[sb];
-                        if (last_in_chunk) {
-                            umma_commit_pair(bar0 + L::BAR_ACC + 8 * cb, 3);
-                            ++ncommit[L::NS + cb];
-                        }
+    if constexpr (DG) {
+        // ---- two generation groups (warps 0-7, 8-15) and the MMA warp (16) ----
+        volatile int *abort_flag = reinterpret_cast<volatile int *>(sm + L::OFF_BAR + L::ABORT_FLAG);
+        const int ntile_cta = t0 < a.ntiles ? (a.ntiles - 1 - t0) / tstride + 1 : 0;
+        const int nch = (a.nst + a.ch - 1) / a.ch;            // accumulation chunks per tile
+        const int64_t total = (int64_t)ntile_cta * a.nst;      // stages of this CTA
+        const int64_t total_ch = (int64_t)ntile_cta * nch;    // chunks of this CTA
+        auto tile_of = [&](int64_t gg) { return a.tiles[t0 + (int)(gg / a.nst) * tstride]; };
+        if (warp == 2 * (WARPS / 2)) {
+            if (lane == 0) {
+                bool fail = false;
+                unsigned nc[L::NS + 2] = {};   // commits issued (or, in the pair's second CTA, due) per mbarrier
+                for (int64_t gg = 0; gg < total; ++gg) {
+                    if (*abort_flag) {
+                        fail = true;
+                        break;
                     }
-                } else {
+                    const int sb = (int)(gg % L::NS);
+                    const int st = (int)(gg % a.nst);
+                    const int64_t c = (gg / a.nst) * nch + st / a.ch;
+                    const unsigned cb = (unsigned)(c & 1);
+                    const bool first_in_chunk = (st % a.ch) == 0;
+                    const bool last_in_chunk = (st % a.ch) == a.ch - 1 || st == a.nst - 1;
+                    const uint32_t par = (uint32_t)((gg / L::NS) & 1);
+                    // the stage's group has written and fenced it
+                    if (!mbar_wait(bar0 + L::BAR_READY + 8 * sb, par, a.wait_limit)) {
+                        fail = true;
+                        break;
+                    }
+                    if (rank != 0) {
+                        mbar_arrive_remote(bar0 + L::BAR_FULL + 8 * sb, 0);
+                        ++nc[sb];
+                        if (last_in_chunk) ++nc[L::NS + cb];
+                        continue;
+                    }
+                    if (!mbar_wait_cluster(bar0 + L::BAR_FULL + 8 * sb, par, a.wait_limit)) {
+                        fail = true;
+                        break;
+                    }
                     tc_fence_after();
                     const uint32_t sbase = sm_s + sb * L::STAGE_BYTES;
                     const uint32_t dcol = tmem + cb * N;
@@ -727,45 +730,207 @@ __global__ void __launch_bounds__(THREADS, 1) k_hessian_tc(const Args a)
                         const uint64_t ah = sdesc(sbase + kk * 32), al = sdesc(sbase + A_BYTES + kk * 32);
                         const uint64_t bh = sdesc(sbase + 2 * A_BYTES + kk * 32);
                         const uint64_t bl = sdesc(sbase + 2 * A_BYTES + L::B_BYTES + kk * 32);
-                        umma_bf16(dcol, ah, bh, (first_in_chunk && kk == 0) ? 0u : 1u);
-                        umma_bf16(dcol, ah, bl, 1u);
-                        umma_bf16(dcol, al, bh, 1u);
+                        umma_bf16_pair(dcol, ah, bh, (first_in_chunk && kk == 0) ? 0u : 1u);
+                        umma_bf16_pair(dcol, ah, bl, 1u);
+                        umma_bf16_pair(dcol, al, bh, 1u);
                     }
-                    umma_commit(bar0 + 8 * sb);
-                    ++ncommit[sb];
+                    umma_commit_pair(bar0 + 8 * sb, 3);
+                    ++nc[sb];
                     if (last_in_chunk) {
-                        umma_commit(bar0 + L::BAR_ACC + 8 * cb);
-                        ++ncommit[L::NS + cb];
+                        umma_commit_pair(bar0 + L::BAR_ACC + 8 * cb, 3);
+                        ++nc[L::NS + cb];
                     }
                 }
+                if (fail) *abort_flag = 1;
+                // every commit issued (or due) lands before the tensor memory is released;
+                // each mbarrier has at most one phase outstanding here
+                for (int i = 0; i < L::NS + 2; ++i)
+                    if (nc[i] > 0) mbar_wait(bar0 + 8 * i, (nc[i] - 1) & 1, WAIT_LIMIT);
             }
-            // drain the previous chunk while the tensor core works on this one
-            if (first_in_chunk && pend >= 0) {
-                if (!drain((unsigned)pend, pend_tl, pend_first, pend_last)) bad = true;
-                pend = -1;
+            __syncwarp();
+        } else {
+            const int grp = warp >> 3;           // stages grp, grp + 2, ...
+            const int gbar = 1 + grp;            // the group's named barrier
+            bool gbad = false;
+            int64_t next_drain = 0;              // next chunk whose half of the columns this group drains
+            auto drain_upto = [&](int64_t cend) {
+                while (next_drain < cend) {
+                    const int64_t c = next_drain++;
+                    const int ci = (int)(c % nch);
+                    if (!drain((unsigned)c, a.tiles[t0 + (int)(c / nch) * tstride], ci == 0, ci == nch - 1)) gbad = true;
+                }
+            };
+            int64_t gg = grp;
+            if (gg < total) {
+                // the inputs of the group's first stage
+                load_target(tile_of(gg));
+                raw_copy(grp, (int)(gg % a.nst));
+                cp_async_wait_all();
+                group_bar(gbar);
+                stage_store(grp, sid);
+                if (sid < 2 * KQ) stage_store(grp, L::ROWS + sid);
+                group_bar(gbar);
             }
-            if (last_in_chunk) {
-                pend = (int)chunk;
-                pend_tl = tl_cur;
-                pend_first = st < a.ch;
-                pend_last = st == a.nst - 1;
-                ++chunk;
+            bool stop = false;
+            for (; gg < total; gg += 2) {
+                const int sb = (int)(gg % L::NS);
+                const int st = (int)(gg % a.nst);
+                const int64_t c = (gg / a.nst) * nch + st / a.ch;
+                const bool more = gg + 2 < total;
+                // raw[grp] was read by the stage_store of this stage: the inputs of stage gg + 2 go there
+                if (more) raw_copy(grp, (int)((gg + 2) % a.nst));
+                drain_upto(c);
+                // the products that read this buffer NS stages ago must be complete
+                if (gg >= L::NS && !mbar_wait(bar0 + 8 * sb, (uint32_t)(((gg / L::NS) - 1) & 1), a.wait_limit))
+                    gbad = true;
+                if constexpr (FACT) generate_fact(grp, sb);
+                else generate(grp, sb);
+                fence_async_smem();
+                cp_async_wait_all();
+                stop = group_bar_or(gbar, gbad || *abort_flag != 0);
+                if (stop) break;
+                if (sid == 0) mbar_arrive_local(bar0 + L::BAR_READY + 8 * sb);
+                if (more) {
+                    if ((gg + 2) / a.nst != gg / a.nst) load_target(tile_of(gg + 2));
+                    stage_store(grp, sid);
+                    if (sid < 2 * KQ) stage_store(grp, L::ROWS + sid);
+                }
+                group_bar(gbar);
+            }
+            if (!stop) stop = group_bar_or(gbar, gbad || *abort_flag != 0);
+            if (!stop) drain_upto(total_ch);
+            if ((stop || gbad) && sid == 0) *abort_flag = 1;
+        }
+        __syncthreads();
+        if (tid == 0 && *abort_flag) atomicExch(a.err, 1);
+    } else {
+        int g = 0;               // global stage counter (stage-buffer phases)
+        unsigned chunk = 0;      // global chunk counter (accumulator phases)
+        int pend = -1;
+        int2 pend_tl = make_int2(0, 0);
+        bool pend_first = false, pend_last = false;
+        bool bad = false;        // this thread saw a wait expire
+        bool aborted = false;
+        unsigned ncommit[L::NS + 2] = {};  // commits issued (or, in a pair's second CTA, due) per mbarrier (thread 0)
+
+        if (t0 < a.ntiles) {
+            // stage 0 into Eg/qs[0]; stage 1's inputs into raw[1]
+            load_target(a.tiles[t0]);
+            raw_copy(0, 0);
+            cp_async_wait_all();
+            __syncthreads();
+            stage_store(0, tid);
+            raw_copy(1, a.nst > 1 ? 1 : 0);
+            cp_async_wait_all();
+        }
+        __syncthreads();
+
+        // One block-wide barrier per stage: it publishes the stage's operands to
+        // the MMA thread and orders the previous drain's TMEM reads before any MMA
+        // that reuses that accumulator.
+        for (int t = t0; t < a.ntiles && !aborted; t += tstride) {
+            // tile coordinates of this and the next tile, loaded once per tile
+            const int2 tl_cur = a.tiles[t];
+            const int2 tl_nxt = t + tstride < a.ntiles ? a.tiles[t + tstride] : tl_cur;
+            for (int st = 0; st < a.nst; ++st, ++g) {
+                const int eb = g & 1;          // stage inputs and E/G, point data: double-buffered
+                const int sb = g % L::NS;      // operand stage buffer
+                const bool last_of_tile = st + 1 == a.nst;
+                const bool has_next = !last_of_tile || t + tstride < a.ntiles;
+                raw_copy(eb, (st + 2) % a.nst);     // inputs of stage g + 2 (its point block)
+                // the MMAs that read this buffer NS stages ago must be complete
+                if (g >= L::NS && !mbar_wait(bar0 + 8 * sb, ((g / L::NS) - 1) & 1, a.wait_limit)) bad = true;
+                if constexpr (FACT) generate_fact(eb, sb);
+                else generate(eb, sb);
+                if (has_next) {
+                    if (last_of_tile) load_target(tl_nxt);   // once per tile
+                    stage_store(eb ^ 1, tid);
+                }
+                cp_async_wait_all();
+                fence_async_smem();
+                if (__syncthreads_or(bad)) { aborted = true; break; }
+                const bool first_in_chunk = (st % a.ch) == 0;
+                const bool last_in_chunk = (st % a.ch) == a.ch - 1 || st == a.nst - 1;
+                const unsigned cb = chunk & 1;
+                if (tid == 0) {
+                    if constexpr (PAIR) {
+                        if (rank != 0) {
+                            // this CTA's half of stage g is written (and fenced for the async proxy)
+                            mbar_arrive_remote(bar0 + L::BAR_FULL + 8 * sb, 0);
+                            // the leader's commits arrive here too
+                            ++ncommit[sb];
+                            if (last_in_chunk) ++ncommit[L::NS + cb];
+                        } else if (!mbar_wait_cluster(bar0 + L::BAR_FULL + 8 * sb, (g / L::NS) & 1, a.wait_limit)) {
+                            bad = true;
+                        } else {
+                            tc_fence_after();
+                            const uint32_t sbase = sm_s + sb * L::STAGE_BYTES;
+                            const uint32_t dcol = tmem + cb * N;
+    #pragma unroll
+                            for (int kk = 0; kk < KQ / 16; ++kk) {
+                                const uint64_t ah = sdesc(sbase + kk * 32), al = sdesc(sbase + A_BYTES + kk * 32);
+                                const uint64_t bh = sdesc(sbase + 2 * A_BYTES + kk * 32);
+                                const uint64_t bl = sdesc(sbase + 2 * A_BYTES + L::B_BYTES + kk * 32);
+                                umma_bf16_pair(dcol, ah, bh, (first_in_chunk && kk == 0) ? 0u : 1u);
+                                umma_bf16_pair(dcol, ah, bl, 1u);
+                                umma_bf16_pair(dcol, al, bh, 1u);
+                            }
+                            umma_commit_pair(bar0 + 8 * sb, 3);
+                            ++ncommit[sb];
+                            if (last_in_chunk) {
+                                umma_commit_pair(bar0 + L::BAR_ACC + 8 * cb, 3);
+                                ++ncommit[L::NS + cb];
+                            }
+                        }
+                    } else {
+                        tc_fence_after();
+                        const uint32_t sbase = sm_s + sb * L::STAGE_BYTES;
+                        const uint32_t dcol = tmem + cb * N;
+    #pragma unroll
+                        for (int kk = 0; kk < KQ / 16; ++kk) {
+                            const uint64_t ah = sdesc(sbase + kk * 32), al = sdesc(sbase + A_BYTES + kk * 32);
+                            const uint64_t bh = sdesc(sbase + 2 * A_BYTES + kk * 32);
+                            const uint64_t bl = sdesc(sbase + 2 * A_BYTES + L::B_BYTES + kk * 32);
+                            umma_bf16(dcol, ah, bh, (first_in_chunk && kk == 0) ? 0u : 1u);
+                            umma_bf16(dcol, ah, bl, 1u);
+                            umma_bf16(dcol, al, bh, 1u);
+                        }
+                        umma_commit(bar0 + 8 * sb);
+                        ++ncommit[sb];
+                        if (last_in_chunk) {
+                            umma_commit(bar0 + L::BAR_ACC + 8 * cb);
+                            ++ncommit[L::NS + cb];
+                        }
+                    }
+                }
+                // drain the previous chunk while the tensor core works on this one
+                if (first_in_chunk && pend >= 0) {
+                    if (!drain((unsigned)pend, pend_tl, pend_first, pend_last)) bad = true;
+                    pend = -1;
+                }
+                if (last_in_chunk) {
+                    pend = (int)chunk;
+                    pend_tl = tl_cur;
+                    pend_first = st < a.ch;
+                    pend_last = st == a.nst - 1;
+                    ++chunk;
+                }
             }
         }
-    }
-    if (!aborted && pend >= 0) {
-        if (!drain((unsigned)pend, pend_tl, pend_first, pend_last)) bad = true;
-    }
-    if (__syncthreads_or(bad)) aborted = true;
-    if (aborted && tid == 0) {
-        atomicExch(a.err, 1);
-        // Let the MMAs in flight finish, and every commit arrive, before the
-        // tensor memory is released and the CTA exits.  Each mbarrier has at
-        // most one phase outstanding here (every earlier phase was waited for
-        // successfully, or the loop would have stopped there), so waiting for
-        // the phase of its last commit, in order, covers them all.
-        for (int i = 0; i < L::NS + 2; ++i)
-            if (ncommit[i] > 0) mbar_wait(bar0 + 8 * i, (ncommit[i] - 1) & 1, WAIT_LIMIT);
+        if (!aborted && pend >= 0) {
+            if (!drain((unsigned)pend, pend_tl, pend_first, pend_last)) bad = true;
+        }
+        if (__syncthreads_or(bad)) aborted = true;
+        if (aborted && tid == 0) {
+            atomicExch(a.err, 1);
+            // Let the MMAs in flight finish, and every commit arrive, before the
+            // tensor memory is released and the CTA exits.  Each mbarrier has at
+            // most one phase outstanding here (every earlier phase was waited for
+            // successfully, or the loop would have stopped there), so waiting for
+            // the phase of its last commit, in order, covers them all.
+            for (int i = 0; i < L::NS + 2; ++i)
+                if (ncommit[i] > 0) mbar_wait(bar0 + 8 * i, (ncommit[i] - 1) & 1, WAIT_LIMIT);
+        }
     }
     tc_fence_before();
     __syncthreads();
@@ -934,7 +1099,7 @@ sdot_status hessian_tc(sdot_ctx *c, void *H_dev, bool out_f32, int chunk_stages,
     // The whole matrix runs on SM pairs (256 x 256 tiles, M = 256 products
     // over two SMs) unless that is switched off; a range of the 128 x 256
     // tiles (sharding) runs on single SMs.
-    const bool pair = c->hess_pair && tile_begin == 0 && tile_end == ntile1;
+    const bool pair = c->hess_pair_mode > 0 && tile_begin == 0 && tile_end == ntile1;
     int64_t npad = std::max(na * M, nb * N);
     if (pair) {
         const int64_t n2 = (n + 2 * M - 1) / (2 * M);
@@ -1019,17 +1184,22 @@ sdot_status hessian_tc(sdot_ctx *c, void *H_dev, bool out_f32, int chunk_stages,
     a.cd = cdp;
     a.qw = qwp;
     void (*kern)(const Args) = nullptr;
-    if (pair) {
-        if (c->dim == 2) kern = out_f32 ? k_hessian_tc<2, float, false, true> : k_hessian_tc<2, double, false, true>;
-        else if (fact) kern = out_f32 ? k_hessian_tc<3, float, true, true> : k_hessian_tc<3, double, true, true>;
-        else kern = out_f32 ? k_hessian_tc<3, float, false, true> : k_hessian_tc<3, double, false, true>;
+    const bool dual = pair && c->hess_pair_mode == 2;
+    if (dual) {
+        if (c->dim == 2) kern = out_f32 ? k_hessian_tc<2, float, false, true, true> : k_hessian_tc<2, double, false, true, true>;
+        else if (fact) kern = out_f32 ? k_hessian_tc<3, float, true, true, true> : k_hessian_tc<3, double, true, true, true>;
+        else kern = out_f32 ? k_hessian_tc<3, float, false, true, true> : k_hessian_tc<3, double, false, true, true>;
+    } else if (pair) {
+        if (c->dim == 2) kern = out_f32 ? k_hessian_tc<2, float, false, true, false> : k_hessian_tc<2, double, false, true, false>;
+        else if (fact) kern = out_f32 ? k_hessian_tc<3, float, true, true, false> : k_hessian_tc<3, double, true, true, false>;
+        else kern = out_f32 ? k_hessian_tc<3, float, false, true, false> : k_hessian_tc<3, double, false, true, false>;
     } else {
-        if (c->dim == 2) kern = out_f32 ? k_hessian_tc<2, float, false, false> : k_hessian_tc<2, double, false, false>;
-        else if (fact) kern = out_f32 ? k_hessian_tc<3, float, true, false> : k_hessian_tc<3, double, true, false>;
-        else kern = out_f32 ? k_hessian_tc<3, float, false, false> : k_hessian_tc<3, double, false, false>;
+        if (c->dim == 2) kern = out_f32 ? k_hessian_tc<2, float, false, false, false> : k_hessian_tc<2, double, false, false, false>;
+        else if (fact) kern = out_f32 ? k_hessian_tc<3, float, true, false, false> : k_hessian_tc<3, double, true, false, false>;
+        else kern = out_f32 ? k_hessian_tc<3, float, false, false, false> : k_hessian_tc<3, double, false, false, false>;
     }
     c->hess_last_factored = fact;
-    c->hess_last_pair = pair;
+    c->hess_last_pair = pair ? (dual ? 2 : 1) : 0;
     const uint32_t smem = pair ? Lay<true>::SMEM_BYTES : Lay<false>::SMEM_BYTES;
     e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return cuda_error(c, e, "tensor-core Hessian attribute");
@@ -1037,7 +1207,7 @@ sdot_status hessian_tc(sdot_ctx *c, void *H_dev, bool out_f32, int chunk_stages,
     if (pair) {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3((unsigned)grid);
-        cfg.blockDim = dim3(THREADS);
+        cfg.blockDim = dim3(dual ? DG_THREADS : THREADS);
         cfg.dynamicSmemBytes = smem;
         cfg.stream = c->stream;
         cudaLaunchAttribute attr[1];

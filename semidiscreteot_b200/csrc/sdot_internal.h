@@ -191,8 +191,9 @@ struct sdot_ctx {
     sdot::DevBuf<float> htc_cd, htc_qw;  // factored generation: per-chunk cell data, per-point factors
     bool hess_factored = true;         // factored generation where the source allows it (sdot_set_hessian_generation)
     bool hess_last_factored = false;   // the last tensor Hessian used it
-    bool hess_pair = true;             // whole tensor Hessians on SM pairs (sdot_set_hessian_pairs)
-    bool hess_last_pair = false;       // the last tensor Hessian ran on SM pairs
+    int hess_pair_mode = 2;            // whole tensor Hessians: 0 single SMs, 1 SM pairs, 2 SM pairs with two
+                                       // generation groups (sdot_set_hessian_pairs)
+    int hess_last_pair = 0;            // the mode the last tensor Hessian ran in
     double hess_kernel_ms = 0.0;
     int64_t hess_tiles = 0;
     int distance = 0;                  // distance function: 0 euclidean, 1 spherical (sdot_set_distance_function)

@@ -344,13 +344,15 @@ class SotSolver:
                                                         C.byref(last)))
         return bool(last.value)
 
-    def set_hessian_pairs(self, pairs: Optional[bool] = None) -> bool:
+    def set_hessian_pairs(self, mode: Optional[int] = None) -> int:
         """Whole tensor Hessians on SM pairs (tcgen05 cta_group::2 over 256 x 256
-        tiles; True: on, the default; False: off; None: unchanged).  Returns
-        whether the last tensor Hessian ran on pairs."""
+        tiles): 2 (default) with two generation groups and an MMA warp per CTA,
+        1 with one group, 0 on single SMs; None leaves the setting (True / False
+        mean 2 / 0).  Returns the mode the last tensor Hessian ran in."""
         last = C.c_int(0)
-        self._check(self._L.sdot_set_hessian_pairs(self._h, -1 if pairs is None else int(bool(pairs)), C.byref(last)))
-        return bool(last.value)
+        m = -1 if mode is None else (2 if mode is True else (0 if mode is False else int(mode)))
+        self._check(self._L.sdot_set_hessian_pairs(self._h, m, C.byref(last)))
+        return int(last.value)
 
     def set_hessian_wait_limit(self, clocks: int):
         """SM clocks a device-side wait of the tensor Hessian may take before the

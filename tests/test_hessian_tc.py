@@ -126,12 +126,12 @@ def test_tensor_hessian_larger_against_fp64_kernel():
     print(f"2000 targets: Frobenius {fro:.2e}, max {mx:.2e}, tiles {info['tiles']}")
     assert fro <= FRO_TOL and mx <= MAX_TOL
     # SM pairs (the default): 256 x 256 tiles of the upper triangle, 8 x 9 / 2
-    assert s.set_hessian_pairs(None) is True and info["tiles"] == 36
-    s.set_hessian_pairs(False)
+    assert s.set_hessian_pairs(None) == 2 and info["tiles"] == 36
+    s.set_hessian_pairs(0)
     Hs, info = hessian(s, psi, "tensor")
     assert info["tiles"] == sum(max(0, 8 - (ta * 128) // 256) for ta in range(16))   # single SMs: 128 x 256
     assert rel_errors(Hs, Hf)[0] <= FRO_TOL
-    s.set_hessian_pairs(True)
+    s.set_hessian_pairs(2)
     # rows sum to ~0: H 1 = 0 for the exact Hessian (mass conservation)
     assert np.max(np.abs(Ht.sum(axis=1))) <= 1e-3 * np.max(np.abs(Ht))
     s.close()
@@ -226,20 +226,24 @@ def test_factored_generation_not_used_outside_its_bound():
 
 @pytest.mark.parametrize("kind", ["dense2d", "dense3d", "dense3d_small_eps"])
 def test_sm_pairs_match_single_sm(oracle_mod, kind):
-    """Whole Hessians on SM pairs (tcgen05 cta_group::2 over 256 x 256 tiles,
-    the default) agree with the FP64 oracle within the tensor method's bounds,
-    are exactly symmetric and repeatable, and agree with the single-SM kernel."""
+    """Whole Hessians on SM pairs (tcgen05 cta_group::2 over 256 x 256 tiles),
+    with two generation groups (the default) or one, agree with the FP64
+    oracle within the tensor method's bounds, are exactly symmetric and
+    repeatable, and agree with the single-SM kernel."""
     src, y, nu, eps = problem(kind, seed=4)
     N = len(nu)
     s = make(src, y, nu, eps)
     psi = 0.3 * eps * np.random.default_rng(8).standard_normal(N)
-    H2, _ = hessian(s, psi, "tensor")          # SM pairs: the default
-    assert s.set_hessian_pairs(None) is True
+    H2, _ = hessian(s, psi, "tensor")          # SM pairs, two generation groups: the default
+    assert s.set_hessian_pairs(None) == 2
     H3, _ = hessian(s, psi, "tensor")
-    s.set_hessian_pairs(False)
-    H1, _ = hessian(s, psi, "tensor")
-    assert s.set_hessian_pairs(None) is False
-    s.set_hessian_pairs(True)
+    s.set_hessian_pairs(1)
+    H1p, _ = hessian(s, psi, "tensor")         # SM pairs, one generation group
+    assert s.set_hessian_pairs(None) == 1
+    s.set_hessian_pairs(0)
+    H1, _ = hessian(s, psi, "tensor")          # single SMs
+    assert s.set_hessian_pairs(None) == 0
+    s.set_hessian_pairs(2)
     P = oracle_mod.Problem(src["x"], src["jxw"], src["density"], src["cell_offsets"], src["cell_centers"], y, nu)
     Ho = P.hessian(psi, oracle_mod.Params(epsilon=eps, tau=0.0, use_log_sum_exp=True), 1e300)
     assert np.all(np.isfinite(H2))
@@ -248,6 +252,8 @@ def test_sm_pairs_match_single_sm(oracle_mod, kind):
     fro, mx = rel_errors(H2, Ho)
     print(f"SM pairs vs FP64: Frobenius {fro:.2e}, max {mx:.2e}; single SM: {rel_errors(H1, Ho)}")
     assert fro <= FRO_TOL and mx <= MAX_TOL, (fro, mx)
-    fro12, _ = rel_errors(H2, H1)
-    assert fro12 <= FRO_TOL
+    for Hx in (H1, H1p):
+        assert rel_errors(Hx, Ho)[0] <= FRO_TOL
+        assert rel_errors(H2, Hx)[0] <= FRO_TOL
+    assert np.array_equal(H1p, H1p.T)
     s.close()
