@@ -54,23 +54,13 @@ constexpr int N = 256;               // columns b per tile (MMA N)
 constexpr int KQ = 64;               // quadrature points per stage (one 128-byte swizzle row of BF16)
 constexpr int WARPS = 16;
 constexpr int THREADS = WARPS * 32;
-constexpr int ROWS = M + N;          // generated operand rows per stage
 constexpr int RG = WARPS * 4;        // row groups (4 per warp, 8 lanes = 8 K-chunks each)
-constexpr int RPT = ROWS / RG;       // rows per thread per stage
-constexpr int ARPT = M / RG;         // of which A rows
-static_assert(ROWS % RG == 0 && M % RG == 0, "row split");
-static_assert(THREADS == ROWS + 2 * KQ, "one staging item per thread");
+static_assert(M % RG == 0, "row split");
 
 constexpr uint32_t A_BYTES = M * KQ * 2;                 // 16 KB
-constexpr uint32_t B_BYTES = N * KQ * 2;                 // 32 KB
-constexpr uint32_t STAGE_BYTES = 2 * (A_BYTES + B_BYTES); // Ahi, Alo, Bhi, Blo
-constexpr uint32_t OFF_EG = 2 * STAGE_BYTES;             // float [2][ROWS][8]: E,E,Gx,Gx,Gy,Gy,Gz,Gz
 constexpr int QS_STRIDE = 44;                            // floats per K-chunk: dx[8] dy[8] dz[8] fb[8] fa[8] + pad
-constexpr uint32_t OFF_QS = OFF_EG + 2 * ROWS * 32;      // float [2][8][QS_STRIDE]
-constexpr uint32_t OFF_RAW = OFF_QS + 2 * 8 * QS_STRIDE * 4;  // per-stage inputs as loaded, 2 buffers:
-constexpr uint32_t RAW_BYTES = 32 + KQ * 16 + KQ * 4;    //   block {c_b, L_b}, points {d, F^B}, points F^A
-constexpr uint32_t OFF_BAR = OFF_RAW + 2 * RAW_BYTES;    // 4 mbarriers + TMEM address
-constexpr uint32_t SMEM_BYTES = OFF_BAR + 64 + 1024;     // + alignment slack
+constexpr uint32_t RAW_BYTES = 32 + KQ * 16 + KQ * 4;    // per-stage inputs as loaded: block {c_b, L_b},
+                                                         // points {d, F^B}, points F^A
 constexpr int TMEM_COLS = 2 * N;                          // two FP32 accumulators
 constexpr int SCR_PER_CTA = M * N;                        // FP64 drain scratch per CTA
 
@@ -214,7 +204,11 @@ __device__ __forceinline__ f2 mul2(f2 a, f2 b)
     return d;
 }
 
-// Shared-memory layout per CTA.  PAIR: the CTA is one of an SM pair that
+// Shared-memory layout per CTA: NS operand stage buffers (Ahi, Alo, Bhi, Blo;
+// 128B-swizzled, K-major), two buffers of per-row E/G (float [ROWS][8]:
+// E,E,Gx,Gx,Gy,Gy,Gz,Gz) and of per-K-chunk point data (float [8][QS_STRIDE]),
+// two raw input buffers, the mbarriers, 1 KB of alignment slack.
+// PAIR: the CTA is one of an SM pair that
 // runs M = 256 products together (tcgen05 cta_group::2): each CTA holds its
 // 128 A rows and half of the 256 B rows of a stage, and its TMEM holds its
 // 128 rows x 256 columns of the tile.
@@ -455,54 +449,53 @@ __global__ void __launch_bounds__(DG ? DG_THREADS : THREADS, 1) k_hessian_tc(con
     };
     auto raw_copy = [&](int buf, int st) {   // 2 + 64 + 16 copies of 16 bytes (FACT: 2 + 16 + 32)
         const uint32_t d = rawb_s + buf * RAW_BYTES;
-        const int tid = sid;
-        if (tid < 2) cp_async16(d + tid * 16, reinterpret_cast<const uint8_t *>(a.blk + st) + tid * 16);
+        if (sid < 2) cp_async16(d + sid * 16, reinterpret_cast<const uint8_t *>(a.blk + st) + sid * 16);
         else if constexpr (FACT) {
             // chunk data: 8 chunks x 2 float4; point factors: 64 float2 = 32 x 16 bytes
-            if (tid < 2 + 16) cp_async16(d + 32 + (tid - 2) * 16, a.cd + (int64_t)st * 16 + (tid - 2));
-            else if (tid < 2 + 16 + 32)
-                cp_async16(d + 32 + 256 + (tid - 18) * 16, a.qw + (int64_t)st * KQ + (tid - 18) * 2);
+            if (sid < 2 + 16) cp_async16(d + 32 + (sid - 2) * 16, a.cd + (int64_t)st * 16 + (sid - 2));
+            else if (sid < 2 + 16 + 32)
+                cp_async16(d + 32 + 256 + (sid - 18) * 16, a.qw + (int64_t)st * KQ + (sid - 18) * 2);
         } else {
-            if (tid < 2 + KQ) cp_async16(d + 32 + (tid - 2) * 16, a.qa + (int64_t)st * KQ + (tid - 2));
-            else if (tid < 2 + KQ + KQ / 4) cp_async16(d + 32 + KQ * 16 + (tid - 2 - KQ) * 16, a.qb + (int64_t)st * KQ + (tid - 2 - KQ) * 4);
+            if (sid < 2 + KQ) cp_async16(d + 32 + (sid - 2) * 16, a.qa + (int64_t)st * KQ + (sid - 2));
+            else if (sid < 2 + KQ + KQ / 4) cp_async16(d + 32 + KQ * 16 + (sid - 2 - KQ) * 16, a.qb + (int64_t)st * KQ + (sid - 2 - KQ) * 4);
         }
         cp_async_commit();
     };
-    // raw[buf] + pt -> Eg / qs [buf]: item tid (rows, then points); with DG a
+    // raw[buf] + pt -> Eg / qs [buf] for one staging item (rows, then points); with DG a
     // group's 256 threads take the rows and then, the first 128, the points
-    auto stage_store = [&](int buf, int tid) {
+    auto stage_store = [&](int buf, int item) {
         const uint8_t *rb = raw + buf * RAW_BYTES;
-        if (tid < L::ROWS) {
+        if (item < L::ROWS) {
             const double4 pb = *reinterpret_cast<const double4 *>(rb);
             const double dx = pt.x - pb.x, dy = pt.y - pb.y, dz = DIM == 3 ? pt.z - pb.z : 0.0;
             const float e = (float)(pt.w - 0.5 * a.l2e_eps * (dx * dx + dy * dy + dz * dz) - pb.w);
             const float gx = (float)(a.l2e_eps * dx), gy = (float)(a.l2e_eps * dy), gz = (float)(a.l2e_eps * dz);
-            float4 *dst = reinterpret_cast<float4 *>(Eg + (buf * L::ROWS + tid) * 8);
+            float4 *dst = reinterpret_cast<float4 *>(Eg + (buf * L::ROWS + item) * 8);
             dst[0] = make_float4(e, e, gx, gx);
             dst[1] = make_float4(gy, gy, gz, gz);
         } else if constexpr (FACT) {
             // chunk layout in qs: [0, 3) dc, 3 F_c^B, [4, 7) a, 7 F_c^A,
             // [8, 16) 2^(F^B - F_c^B), [16, 24) 2^(F^A - F_c^A)
-            if (tid < L::ROWS + KQ) {
-                const int p = tid - L::ROWS;
+            if (item < L::ROWS + KQ) {
+                const int p = item - L::ROWS;
                 const float2 wv = reinterpret_cast<const float2 *>(rb + 32 + 256)[p];
                 float *d = qs + (buf * 8 + (p >> 3)) * QS_STRIDE + (p & 7);
                 d[8] = wv.x;
                 d[16] = wv.y;
-            } else if (tid < L::ROWS + 2 * KQ) {
-                const int t = tid - L::ROWS - KQ;       // 64 threads: chunk t >> 3, float t & 7
+            } else if (item < L::ROWS + 2 * KQ) {
+                const int t = item - L::ROWS - KQ;       // 64 threads: chunk t >> 3, float t & 7
                 qs[(buf * 8 + (t >> 3)) * QS_STRIDE + (t & 7)] = reinterpret_cast<const float *>(rb + 32)[t];
             }
-        } else if (tid < L::ROWS + KQ) {
-            const int p = tid - L::ROWS;            // point p of the stage: K-chunk p >> 3, slot p & 7
+        } else if (item < L::ROWS + KQ) {
+            const int p = item - L::ROWS;            // point p of the stage: K-chunk p >> 3, slot p & 7
             const float4 pq = reinterpret_cast<const float4 *>(rb + 32)[p];
             float *d = qs + (buf * 8 + (p >> 3)) * QS_STRIDE + (p & 7);
             d[0] = pq.x;
             d[8] = pq.y;
             d[16] = pq.z;
             d[24] = pq.w;
-        } else if (tid < L::ROWS + 2 * KQ) {
-            const int p = tid - L::ROWS - KQ;
+        } else if (item < L::ROWS + 2 * KQ) {
+            const int p = item - L::ROWS - KQ;
             qs[(buf * 8 + (p >> 3)) * QS_STRIDE + 32 + (p & 7)] = reinterpret_cast<const float *>(rb + 32 + KQ * 16)[p];
         }
     };
