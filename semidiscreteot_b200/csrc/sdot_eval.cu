@@ -196,8 +196,15 @@ k_finalize_grad(int64_t nt, int nks, const double *__restrict__ gpart, const dou
 {
     double psinu = 0.0, l1 = 0.0, linf = 0.0, comp = -CUDART_INF, l2 = 0.0, gp = 0.0, bad = 0.0;
     for (int64_t j = blockIdx.x * (int64_t)FIN_THREADS + threadIdx.x; j < nt; j += (int64_t)gridDim.x * FIN_THREADS) {
-        double s = 0.0;
-        for (int k = 0; k < nks; ++k) s += gpart[(int64_t)k * nt + j];
+        // the q-slice partials in eight interleaved sums (eight loads in flight), added in a fixed tree
+        double acc[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        int k = 0;
+        for (; k + 8 <= nks; k += 8) {
+#pragma unroll
+            for (int u = 0; u < 8; ++u) acc[u] += gpart[(int64_t)(k + u) * nt + j];
+        }
+        for (; k < nks; ++k) acc[k & 7] += gpart[(int64_t)k * nt + j];
+        const double s = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
         const double g = s - nu[j];
         grad[j] = sub_nu ? g : s;
         psinu += psi[j] * nu[j];
@@ -623,8 +630,8 @@ sdot_status evaluate_enqueue(sdot_ctx *c, const double *p_dir, double comp_tol, 
         a.sstar = NAN;
     }
     // everything after the threshold, up to the copy of the scalars to the host
+    // (an untruncated evaluation needs no ψ range: k_minmax runs only for the threshold)
     auto body = [&]() -> sdot_status {
-        if (!may_truncate) launch_minmax();
         const sdot_status s = (c->dim == 2) ? run_eval<2>(c, a, dense_ok, p_dir, comp_tol, partial)
                                             : run_eval<3>(c, a, dense_ok, p_dir, comp_tol, partial);
         if (s != SDOT_OK) return s;
@@ -657,6 +664,7 @@ sdot_status evaluate_enqueue(sdot_ctx *c, const double *p_dir, double comp_tol, 
     cudaEventRecord(c->ev1, c->stream);
     pend.r = r;
     pend.dense = dense_ok;
+    pend.ranged = may_truncate;
     return SDOT_OK;
 }
 
@@ -671,8 +679,10 @@ sdot_status evaluate_complete(sdot_ctx *c, const EvalPending &pend, double *ms_o
     }
     if (c->profiling) {
         float t = 0.f;
-        cudaEventElapsedTime(&t, c->pev[5], c->pev[6]);
-        c->kms[0] += t;
+        if (pend.ranged) {
+            cudaEventElapsedTime(&t, c->pev[5], c->pev[6]);
+            c->kms[0] += t;
+        }
         cudaEventElapsedTime(&t, c->pev[0], c->pev[1]);
         c->kms[1] += t;
         if (dense_ok) {
@@ -690,6 +700,12 @@ sdot_status evaluate_complete(sdot_ctx *c, const EvalPending &pend, double *ms_o
         c->kms[4] += t;
     }
     c->scal_host[SC_R] = r;
+    if (!pend.ranged) {
+        // no ψ range was computed (untruncated): the slots say so
+        c->scal_host[SC_MAXPSI] = NAN;
+        c->scal_host[SC_MINPSI] = NAN;
+        c->scal_host[SC_PSIBAD] = 0.0;
+    }
     c->global_functional = c->scal_host[SC_VALUE];
     c->C_global = c->scal_host[SC_C];
     if (c->scal_host[SC_NONFINITE] != 0.0) return set_error(c, SDOT_ENONFINITE, "non-finite value or gradient");

@@ -241,6 +241,7 @@ sdot_status evaluate_internal(sdot_ctx *c, const double *p_dir, double comp_tol,
 struct EvalPending {
     double r = 0.0;
     bool dense = false;
+    bool ranged = false;   // the ψ range was computed (for the threshold)
 };
 sdot_status evaluate_enqueue(sdot_ctx *c, const double *p_dir, double comp_tol, bool partial, EvalPending &pend);
 sdot_status evaluate_complete(sdot_ctx *c, const EvalPending &pend, double *ms_out);
