@@ -171,6 +171,127 @@ k_value_dense_merge(const double *__restrict__ x, const double *__restrict__ rho
     dense_value_merge<DIM>(x, rho, jxw, ms, nslice, a, blockIdx.x, Lq, part + (int64_t)blockIdx.x * 4);
 }
 
+// Dense value sweep over cells whose points form a TM^DIM tensor grid
+// symmetric about the cell centre (point i = i_0 + TM i_1 (+ TM^2 i_2)):
+// thread <-> cell, one slice of the targets per blockIdx.y, with the same
+// output as k_value_dense_slice (per point: its largest scaled exponent mx
+// and the sum relative to it), merged by k_value_dense_merge.  The exponent
+// of point q and target j, b_qj = A_j + B_j.(c - o) + sum_d B_jd delta_qd,
+// factors per dimension: with G_d = B_jd a_d and the lowest point's
+// exponent b_0 = B0 - sum_d G_d, b_qj = b_0 + sum_d i_d h_d G_d (h = 2 for
+// TM = 2, 1 for TM = 3), so one exponential 2^((b_0 - M)/16) and one per
+// dimension serve the cell's TM^DIM points.  M is a common shift per cell,
+// an upper bound of every exponent so far (raised lazily, as in
+// lse_update).  The per-point maxima are exact: a target updates them only
+// when its upper bound B0 + sum |G_d| reaches the largest lower bound
+// B0 - sum |G_d| seen so far, below which it cannot be any point's maximum.
+template <int DIM, int TM>
+__global__ void __launch_bounds__(DENSE_A_THREADS)
+k_value_dense_tensor(const double *__restrict__ x, const double *__restrict__ tpack, EvalArgs a, int64_t ncells,
+                     int64_t tslice, double *__restrict__ ms)
+{
+    constexpr int NQ = DIM == 3 ? TM * TM * TM : TM * TM;
+    constexpr int TSZ = DIM + 2;  // A, B(DIM), nu
+    constexpr double H = TM == 2 ? 2.0 : 1.0;
+    __shared__ double tab[16];
+    __shared__ double stg[DA_CHUNK * TSZ];
+    if (threadIdx.x < 16) tab[threadIdx.x] = c_exp2_tab[threadIdx.x];
+    const int64_t cell = blockIdx.x * (int64_t)DENSE_A_THREADS + threadIdx.x;
+    const bool valid = cell < ncells;
+    const int64_t q0 = (valid ? cell : 0) * NQ;
+    // cell centre (relative to o) and half spacing per dimension, from the extreme points along d
+    double cp[DIM], ah[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+        const int stride = d == 0 ? 1 : (d == 1 ? TM : TM * TM);
+        const double lo = x[q0 * DIM + d], hi = x[(q0 + (int64_t)(TM - 1) * stride) * DIM + d];
+        const double cd = 0.5 * (lo + hi);
+        cp[d] = cd - a.o[d];
+        ah[d] = hi - cd;
+    }
+    const int64_t t0 = blockIdx.y * tslice;
+    const int64_t t1 = min(a.nt, t0 + tslice);
+    double S[NQ], mx[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+        S[q] = 0.0;
+        mx[q] = -CUDART_INF;
+    }
+    double M = -CUDART_INF, lbmax = -CUDART_INF;
+    for (int64_t c0 = t0; c0 < t1; c0 += DA_CHUNK) {
+        const int cn = (int)min((int64_t)DA_CHUNK, t1 - c0);
+        __syncthreads();
+        for (int i = threadIdx.x; i < cn * TSZ; i += DENSE_A_THREADS) {
+            const int t = i / TSZ, f = i - t * TSZ;
+            stg[i] = tpack[(c0 + t) * TPACK + f];
+        }
+        __syncthreads();
+        for (int t = 0; t < cn; ++t) {
+            const double *tp = stg + t * TSZ;
+            double B0 = tp[0], G[DIM], sg = 0.0, ag = 0.0;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                B0 = fma(tp[1 + d], cp[d], B0);
+                G[d] = tp[1 + d] * ah[d];
+                sg += G[d];
+                ag += fabs(G[d]);
+            }
+            const double ub = B0 + ag;
+            if (ub - M > LSE_THR) {   // raise the shift (the first target sets it)
+                if (M > -CUDART_INF) {
+                    const double sc = exp2_16(M - ub, tab);
+#pragma unroll
+                    for (int q = 0; q < NQ; ++q) S[q] *= sc;
+                }
+                M = ub;
+            }
+            const double P = tp[1 + DIM] * exp2_16(B0 - sg - M, tab);
+            double r[DIM];
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) r[d] = exp2_16(H * G[d], tab);
+#pragma unroll
+            for (int i0 = 0; i0 < TM; ++i0) {
+                const double f0 = i0 == 0 ? P : (i0 == 1 ? P * r[0] : P * r[0] * r[0]);
+#pragma unroll
+                for (int i1 = 0; i1 < TM; ++i1) {
+                    const double f1 = i1 == 0 ? f0 : (i1 == 1 ? f0 * r[1] : f0 * r[1] * r[1]);
+                    if constexpr (DIM == 2) {
+                        S[i0 + TM * i1] += f1;
+                    } else {
+#pragma unroll
+                        for (int i2 = 0; i2 < TM; ++i2) {
+                            const double f2 = i2 == 0 ? f1 : (i2 == 1 ? f1 * r[2] : f1 * r[2] * r[2]);
+                            S[i0 + TM * i1 + TM * TM * i2] += f2;
+                        }
+                    }
+                }
+            }
+            if (ub >= lbmax) {
+                lbmax = fmax(lbmax, B0 - ag);
+#pragma unroll
+                for (int q = 0; q < NQ; ++q) {
+                    double b = B0;
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) {
+                        const int id = (d == 0 ? q : (d == 1 ? q / TM : q / (TM * TM))) % TM;
+                        const double sd = TM == 2 ? (id == 0 ? -1.0 : 1.0) : (double)(id - 1);
+                        b = fma(sd, G[d], b);
+                    }
+                    mx[q] = fmax(mx[q], b);
+                }
+            }
+        }
+    }
+    if (valid) {
+        double *out = ms + (int64_t)blockIdx.y * 2 * a.nq + 2 * q0;
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            out[2 * q] = mx[q];
+            out[2 * q + 1] = (mx[q] == -CUDART_INF) ? 0.0 : S[q] * exp2_16(M - mx[q], tab);
+        }
+    }
+}
+
 template <int DIM, bool FP32>
 __global__ void __launch_bounds__(DENSE_B_THREADS)
 k_grad_dense(const double *__restrict__ x, const double *__restrict__ w, const double *__restrict__ Lq,
@@ -408,13 +529,31 @@ double host_threshold(sdot_ctx *c, double maxpsi, double minpsi)
 // all, at least 64 targets per slice, at most 16 slices) merged per point;
 // gradient target blocks, and q-slices of the gradient sweep (about eight
 // CTAs per SM in all, at least 256 points per slice, at most 64 slices).
+// With tm > 0 (cells whose points form a tm^dim tensor grid, at most 9
+// points) the value sweep runs over cells (k_value_dense_tensor): ncb cell
+// blocks x nvs target slices (about six CTAs per SM in all, at least 32
+// targets per slice, at most 64 slices), always merged per point.
 struct DenseShape {
     int64_t nval, tb;
     int nks;
     int nvs;          // target slices of the value sweep (1: unsliced)
     int64_t tslice;   // targets per value slice
+    int tm;           // > 0: the cell-based tensor value sweep with tm points per dimension
+    int64_t ncb;      // its cell blocks
 };
-static DenseShape dense_shape(int64_t nq, int64_t nt)
+// The tensor value sweep applies to the euclidean untruncated evaluation of
+// cells whose points form a symmetric tensor grid of at most 9 points, with
+// per-dimension factors that stay within 2^100 over the domain.
+static int dense_tensor_m(const sdot_ctx *c, double s_scale)
+{
+    if (c->distance != 0 || c->tensor_m <= 0) return 0;
+    const int tm = c->tensor_m;
+    const int np = c->dim == 3 ? tm * tm * tm : tm * tm;
+    if (np > 9 || c->qpc != np) return 0;
+    const double span = (tm == 2 ? 2.0 : 1.0) * s_scale * 0.5 * c->diam * c->tensor_amax * (tm - 1) * c->dim / 16.0;
+    return span <= 100.0 ? tm : 0;
+}
+static DenseShape dense_shape(int64_t nq, int64_t nt, int tm = 0, int64_t ncells = 0)
 {
     DenseShape d{};
     const int64_t per = (int64_t)DENSE_A_THREADS * DENSE_A_QT;
@@ -431,7 +570,28 @@ static DenseShape dense_shape(int64_t nq, int64_t nt)
     const int64_t maxks = (nq + 255) / 256;
     d.nks = (int)std::max<int64_t>(1, std::min<int64_t>(want, maxks));
     if (d.nks > 64) d.nks = 64;
+    d.tm = tm;
+    if (tm > 0) {
+        d.ncb = (ncells + DENSE_A_THREADS - 1) / DENSE_A_THREADS;
+        const int64_t want = (148 * 6 + d.ncb - 1) / d.ncb;
+        const int64_t maxs = std::max<int64_t>(1, nt / 32);
+        d.nvs = (int)std::max<int64_t>(1, std::min<int64_t>(64, std::min(want, maxs)));
+        d.tslice = (nt + d.nvs - 1) / d.nvs;
+    }
     return d;
+}
+
+template <int DIM>
+static void launch_value_dense_tensor(const DenseShape &ds, const double *x, const double *tpack, const EvalArgs &a,
+                                      int64_t ncells, double *ms, cudaStream_t st)
+{
+    const dim3 grid((unsigned)ds.ncb, (unsigned)ds.nvs);
+    if constexpr (DIM == 2) {
+        if (ds.tm == 3) k_value_dense_tensor<2, 3><<<grid, DENSE_A_THREADS, 0, st>>>(x, tpack, a, ncells, ds.tslice, ms);
+        else k_value_dense_tensor<2, 2><<<grid, DENSE_A_THREADS, 0, st>>>(x, tpack, a, ncells, ds.tslice, ms);
+    } else {
+        k_value_dense_tensor<3, 2><<<grid, DENSE_A_THREADS, 0, st>>>(x, tpack, a, ncells, ds.tslice, ms);
+    }
 }
 
 template <int DIM>
@@ -457,9 +617,16 @@ static sdot_status run_eval(sdot_ctx *c, const EvalArgs &a, bool dense, const do
         c->klaunch[2] += 1;
         c->klaunch[3] += 1;
     } else if (dense) {
-        const DenseShape ds = dense_shape(a.nq, a.nt);
+        const DenseShape ds = dense_shape(a.nq, a.nt, dense_tensor_m(c, a.s), c->ncells);
         nval = ds.nval;
-        if (ds.nvs > 1) {
+        if (ds.tm > 0) {
+            const cudaError_t e = c->vpart.alloc((size_t)2 * ds.nvs * a.nq);
+            if (e != cudaSuccess) return cuda_error(c, e, "dense value slices");
+            launch_value_dense_tensor<DIM>(ds, c->x.p, c->tpack.p, a, c->ncells, c->vpart.p, st);
+            k_value_dense_merge<DIM><<<(unsigned)nval, DENSE_A_THREADS, 0, st>>>(c->x.p, c->rho.p, c->jxw.p,
+                                                                                 c->vpart.p, ds.nvs, a, c->Lq.p,
+                                                                                 c->blkpart.p);
+        } else if (ds.nvs > 1) {
             const cudaError_t e = c->vpart.alloc((size_t)2 * ds.nvs * a.nq);
             if (e != cudaSuccess) return cuda_error(c, e, "dense value slices");
             k_value_dense_slice<DIM><<<dim3((unsigned)nval, (unsigned)ds.nvs), DENSE_A_THREADS, 0, st>>>(
@@ -748,13 +915,17 @@ struct NoallocLayout {
     int nks;
     int nvs;
     int64_t tslice;
+    DenseShape ds;
 };
 
-static NoallocLayout noalloc_layout(int64_t nq, int64_t nt)
+static NoallocLayout noalloc_layout(const sdot_ctx *c)
 {
+    const int64_t nq = c->nq, nt = c->nt;
     auto up = [](int64_t n) { return (n + 31) / 32 * 32; };
     NoallocLayout L{};
-    const DenseShape ds = dense_shape(nq, nt);  // the launch shape of the allocating dense path
+    // the launch shape of the allocating dense path
+    const DenseShape ds = dense_shape(nq, nt, dense_tensor_m(c, KAPPA / c->prm.epsilon), c->ncells);
+    L.ds = ds;
     L.nval = ds.nval;
     L.nks = ds.nks;
     L.nvs = ds.nvs;
@@ -768,7 +939,7 @@ static NoallocLayout noalloc_layout(int64_t nq, int64_t nt)
     L.blkpart = o; o += up(4 * L.nval);
     L.redpart = o; o += up((int64_t)FIN_BLOCKS * NRED);
     L.scal = o;    o += up(SC_COUNT);
-    L.vpart = o;   o += L.nvs > 1 ? up((int64_t)2 * L.nvs * nq) : 0;
+    L.vpart = o;   o += (L.nvs > 1 || ds.tm > 0) ? up((int64_t)2 * L.nvs * nq) : 0;
     L.total = o;
     return L;
 }
@@ -795,7 +966,12 @@ static void noalloc_launch(sdot_ctx *c, const EvalArgs &a, double *S, const Noal
     double *psi = S + L.psi, *grad = S + L.grad, *tpack = S + L.tpack, *Lq = S + L.Lq, *gpart = S + L.gpart;
     double *blkpart = S + L.blkpart, *redpart = S + L.redpart, *scal = S + L.scal;
     k_target_prep<DIM><<<grid_for(a.nt, 256), 256, 0, st>>>(a.nt, c->y.p, c->nu.p, psi, a, tpack);
-    if (L.nvs > 1) {
+    if (L.ds.tm > 0) {
+        double *vpart = S + L.vpart;
+        launch_value_dense_tensor<DIM>(L.ds, c->x.p, tpack, a, c->ncells, vpart, st);
+        k_value_dense_merge<DIM><<<(unsigned)L.nval, DENSE_A_THREADS, 0, st>>>(c->x.p, c->rho.p, c->jxw.p, vpart,
+                                                                               L.nvs, a, Lq, blkpart);
+    } else if (L.nvs > 1) {
         double *vpart = S + L.vpart;
         k_value_dense_slice<DIM><<<dim3((unsigned)L.nval, (unsigned)L.nvs), DENSE_A_THREADS, 0, st>>>(
             c->x.p, tpack, a, L.tslice, vpart);
@@ -831,7 +1007,7 @@ extern "C" sdot_status sdot_evaluate_device_noalloc(sdot_ctx *c, const double *p
         return set_error(c, SDOT_EINVAL,
                          "no-alloc evaluation covers untruncated problems only (pointwise threshold, tau <= 0)");
     if (c->distance != 0) return set_error(c, SDOT_EINVAL, "no-alloc evaluation covers the euclidean distance only");
-    const NoallocLayout L = noalloc_layout(c->nq, c->nt);
+    const NoallocLayout L = noalloc_layout(c);
     const size_t need = (size_t)L.total * sizeof(double);
     if (need > NOALLOC_BYTES)
         return set_error(c, SDOT_EINVAL,
