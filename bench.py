@@ -461,7 +461,8 @@ def roofline_of(m, wl, peaks, precision):
     if tv >= tg or truncated:
         ach = VALUE_FLOPS_PER_PAIR[dim] * pairs / (tv * 1e-3) / 1e12
         kname = ("k_fused (FP64 exp2 value sweep + FP32 ex2 gradient sweep, one kernel)" if truncated else
-                 "k_value_dense (FP64 exp2 value sweep)")
+                 "dense FP64 value sweep: k_value_dense_tensor (per tensor-grid cell and target slice) + "
+                 "k_value_dense_merge, or per point; flops counted for the unfactored form")
         return {"kernel": kname, "bound": "fp64", "achieved": ach, "peak": peaks["fp64_tflops"], "unit": "TFLOP/s",
                 "frac": ach / peaks["fp64_tflops"], "traffic": TRAFFIC_BYTES.get((wl["name"], precision)),
                 "flops_per_pair": VALUE_FLOPS_PER_PAIR[dim], "ms_per_launch": tv,
