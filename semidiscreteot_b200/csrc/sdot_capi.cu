@@ -224,14 +224,16 @@ sdot_status ensure_eval_buffers(sdot_ctx *c)
     const int64_t nt = c->nt, nq = c->nq;
     const int64_t dense_blocks = (nq + DENSE_A_THREADS * DENSE_A_QT - 1) / (DENSE_A_THREADS * DENSE_A_QT);
     const int64_t nval = std::max<int64_t>(dense_blocks, c->nsblk);
-    const size_t need = (size_t)(nt * (2 + TPACK + 64 + 2) + nq + 4 * nval + 148 * 8 + 64) * sizeof(double);
+    const size_t need =
+        (size_t)(nt * (2 + TPACK + dense_grad_slices(INT64_MAX / 2, nt) + 2) + nq + 4 * nval + 148 * 8 + 64) *
+        sizeof(double);
     if (c->budget && device_bytes(c) + need > c->budget && c->tpack.n < (size_t)(nt * TPACK))
         return set_error(c, SDOT_EBUDGET, "evaluation buffers exceed the context memory budget");
     CK(c->psi.alloc(nt), "alloc psi");
     CK(c->grad.alloc(nt), "alloc grad");
     CK(c->tpack.alloc(nt * TPACK), "alloc tpack");
     CK(c->Lq.alloc(nq), "alloc Lq");
-    CK(c->gpart.alloc(nt * 64), "alloc gpart");
+    CK(c->gpart.alloc(nt * dense_grad_slices(INT64_MAX / 2, nt)), "alloc gpart");
     CK(c->blkpart.alloc(4 * nval), "alloc blkpart");
     CK(c->redpart.alloc(148 * 8), "alloc redpart");
     CK(c->scal.alloc(SC_COUNT), "alloc scal");

@@ -183,8 +183,12 @@ constexpr int DB_CHUNK = 256;
 
 // One CTA's work of the dense gradient sweep: targets of block tblk against
 // quadrature slice ks; writes gpart[ks * nt + j].  Shared by the
-// single-problem kernel and the batched one.
-template <int DIM, bool FP32>
+// single-problem kernel (QG = DENSE_B_QG) and the batched one (QG = 1).
+// The CTA is QG groups of DENSE_B_THREADS threads: thread lt of every group
+// holds the same TT targets, group g takes the staged points g, g + QG, ...,
+// and the groups' sums are added in group order at the end, so a slice's
+// partial does not depend on the scheduling.
+template <int DIM, bool FP32, int QG = 1>
 __device__ __forceinline__ void dense_grad_block(const double *__restrict__ x, const double *__restrict__ w,
                                                  const double *__restrict__ Lq, const double *__restrict__ tpack,
                                                  const double *__restrict__ psi, const EvalArgs &a, int64_t qslice,
@@ -192,13 +196,17 @@ __device__ __forceinline__ void dense_grad_block(const double *__restrict__ x, c
 {
     constexpr int TT = DENSE_B_TT;
     constexpr int TB = DENSE_B_THREADS * TT;
+    constexpr int NTH = DENSE_B_THREADS * QG;          // threads of the CTA
+    constexpr int CH = DB_CHUNK * (QG > 1 ? 2 : 1);    // points staged at a time
     __shared__ double tab[16];
-    __shared__ double red[2][32];
-    __shared__ __align__(16) double stgd[FP32 ? 1 : DB_CHUNK * (DIM + 2)];
-    __shared__ __align__(16) float stgf[FP32 ? DB_CHUNK * 4 : 1];
-    __shared__ float stgw[FP32 ? DB_CHUNK : 1];
+    __shared__ __align__(16) double stgd[FP32 ? 1 : CH * (DIM + 2)];
+    __shared__ __align__(16) float stgf[FP32 ? CH * 4 : 1];
+    __shared__ float stgw[FP32 ? CH : 1];
+    __shared__ double gsum[QG > 1 ? (QG - 1) * TT * DENSE_B_THREADS : 1];
     if (threadIdx.x < 16) tab[threadIdx.x] = c_exp2_tab[threadIdx.x];
     const int tid = threadIdx.x;
+    const int lt = tid % DENSE_B_THREADS;  // target lane
+    const int grp = tid / DENSE_B_THREADS; // point group
     const int64_t j0 = tblk * TB;
     const int64_t qa = ks * qslice;
     const int64_t qb = min(a.nq, qa + qslice);
@@ -214,7 +222,7 @@ __device__ __forceinline__ void dense_grad_block(const double *__restrict__ x, c
         double amax = -DBL_MAX;
 #pragma unroll
         for (int k = 0; k < TT; ++k) {
-            const int64_t j = j0 + tid + k * DENSE_B_THREADS;
+            const int64_t j = j0 + lt + k * DENSE_B_THREADS;
             if (j < a.nt) {
                 const double *tp = tpack + j * TPACK;
 #pragma unroll
@@ -227,7 +235,7 @@ __device__ __forceinline__ void dense_grad_block(const double *__restrict__ x, c
             }
         }
         // block reductions (lo/hi/amax) through shared memory
-        __shared__ double sred[7][DENSE_B_THREADS / 32];
+        __shared__ double sred[7][NTH / 32];
         for (int o = 16; o > 0; o >>= 1) {
 #pragma unroll
             for (int d = 0; d < DIM; ++d) {
@@ -242,7 +250,7 @@ __device__ __forceinline__ void dense_grad_block(const double *__restrict__ x, c
             sred[6][tid >> 5] = amax;
         }
         __syncthreads();
-        for (int i = 0; i < DENSE_B_THREADS / 32; ++i) {
+        for (int i = 0; i < NTH / 32; ++i) {
 #pragma unroll
             for (int d = 0; d < DIM; ++d) { lo[d] = fmin(lo[d], sred[d][i]); hi[d] = fmax(hi[d], sred[3 + d][i]); }
             amax = fmax(amax, sred[6][i]);
@@ -253,7 +261,7 @@ __device__ __forceinline__ void dense_grad_block(const double *__restrict__ x, c
     }
 #pragma unroll
     for (int k = 0; k < TT; ++k) {
-        const int64_t j = j0 + tid + k * DENSE_B_THREADS;
+        const int64_t j = j0 + lt + k * DENSE_B_THREADS;
         has[k] = j < a.nt;
         acc64[k] = 0.0;
         const double *tp = tpack + (has[k] ? j : 0) * TPACK;
@@ -268,10 +276,10 @@ __device__ __forceinline__ void dense_grad_block(const double *__restrict__ x, c
         }
     }
     const float c32 = (float)a.c32;
-    for (int64_t c0 = qa; c0 < qb; c0 += DB_CHUNK) {
-        const int cn = (int)min((int64_t)DB_CHUNK, qb - c0);
+    for (int64_t c0 = qa; c0 < qb; c0 += CH) {
+        const int cn = (int)min((int64_t)CH, qb - c0);
         __syncthreads();
-        for (int i = tid; i < cn; i += DENSE_B_THREADS) {
+        for (int i = tid; i < cn; i += NTH) {
             const int64_t q = c0 + i;
             double xt[3];
             double xsq = 0.0;
@@ -302,8 +310,8 @@ __device__ __forceinline__ void dense_grad_block(const double *__restrict__ x, c
             float acc[TT];
 #pragma unroll
             for (int k = 0; k < TT; ++k) acc[k] = 0.f;
-            int t = 0;
-            for (; t < cn; ++t) {
+            int i = 0;
+            for (int t = grp; t < cn; t += QG, ++i) {
                 const float4 v = reinterpret_cast<const float4 *>(stgf)[t];
                 const float beta = DIM == 3 ? v.w : v.z;
                 const float wq = stgw[t];
@@ -319,7 +327,7 @@ __device__ __forceinline__ void dense_grad_block(const double *__restrict__ x, c
                     const float e = fmaf(-c32, d2, alpha[k] + beta);
                     acc[k] = fmaf(wq, ex2_approx(e), acc[k]);
                 }
-                if ((t & 7) == 7) {
+                if ((i & 7) == 7) {
 #pragma unroll
                     for (int k = 0; k < TT; ++k) { acc64[k] += (double)acc[k]; acc[k] = 0.f; }
                 }
@@ -327,7 +335,7 @@ __device__ __forceinline__ void dense_grad_block(const double *__restrict__ x, c
 #pragma unroll
             for (int k = 0; k < TT; ++k) acc64[k] += (double)acc[k];
         } else {
-            for (int t = 0; t < cn; ++t) {
+            for (int t = grp; t < cn; t += QG) {
                 const double *v = stgd + t * (DIM + 2);
                 const double D = v[DIM], wq = v[DIM + 1];
 #pragma unroll
@@ -340,16 +348,26 @@ __device__ __forceinline__ void dense_grad_block(const double *__restrict__ x, c
             }
         }
     }
+    if (QG > 1) {
+        // the groups' sums, added in group order by group 0
+        if (grp > 0) {
+#pragma unroll
+            for (int k = 0; k < TT; ++k) gsum[((grp - 1) * TT + k) * DENSE_B_THREADS + lt] = acc64[k];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < TT; ++k)
+            for (int g = 1; g < QG; ++g) acc64[k] += gsum[((g - 1) * TT + k) * DENSE_B_THREADS + lt];
+    }
 #pragma unroll
     for (int k = 0; k < TT; ++k) {
-        const int64_t j = j0 + tid + k * DENSE_B_THREADS;
-        if (j < a.nt) {
+        const int64_t j = j0 + lt + k * DENSE_B_THREADS;
+        if (grp == 0 && j < a.nt) {
             double g = acc64[k];
             if (!FP32) g *= tpack[j * TPACK + 1 + DIM];  // nu_j (FP32 path folds it into alpha)
             gpart[ks * a.nt + j] = g;
         }
     }
-    (void)red;
 }
 
 }  // namespace sdot

@@ -293,12 +293,12 @@ k_value_dense_tensor(const double *__restrict__ x, const double *__restrict__ tp
 }
 
 template <int DIM, bool FP32>
-__global__ void __launch_bounds__(DENSE_B_THREADS)
+__global__ void __launch_bounds__(DENSE_B_CTA, DENSE_B_PER_SM)
 k_grad_dense(const double *__restrict__ x, const double *__restrict__ w, const double *__restrict__ Lq,
              const double *__restrict__ tpack, const double *__restrict__ psi, EvalArgs a, int64_t qslice,
              double *__restrict__ gpart)
 {
-    dense_grad_block<DIM, FP32>(x, w, Lq, tpack, psi, a, qslice, blockIdx.x, blockIdx.y, gpart);
+    dense_grad_block<DIM, FP32, DENSE_B_QG>(x, w, Lq, tpack, psi, a, qslice, blockIdx.x, blockIdx.y, gpart);
 }
 
 // ---------------------------------------------------------------------------
@@ -566,10 +566,7 @@ static DenseShape dense_shape(int64_t nq, int64_t nt, int tm = 0, int64_t ncells
     }
     d.tslice = (nt + d.nvs - 1) / d.nvs;
     d.tb = (nt + DENSE_B_THREADS * DENSE_B_TT - 1) / (DENSE_B_THREADS * DENSE_B_TT);
-    const int64_t want = (148 * 8 + d.tb - 1) / d.tb;
-    const int64_t maxks = (nq + 255) / 256;
-    d.nks = (int)std::max<int64_t>(1, std::min<int64_t>(want, maxks));
-    if (d.nks > 64) d.nks = 64;
+    d.nks = dense_grad_slices(nq, nt);
     d.tm = tm;
     if (tm > 0) {
         d.ncb = (ncells + DENSE_A_THREADS - 1) / DENSE_A_THREADS;
@@ -645,10 +642,10 @@ static sdot_status run_eval(sdot_ctx *c, const EvalArgs &a, bool dense, const do
         const int64_t qslice = (a.nq + nks - 1) / nks;
         dim3 g((unsigned)tb, (unsigned)nks);
         if (prec == SDOT_PREC_FP64)
-            k_grad_dense<DIM, false><<<g, DENSE_B_THREADS, 0, st>>>(c->x.p, c->w.p, c->Lq.p, c->tpack.p, c->psi.p, a,
+            k_grad_dense<DIM, false><<<g, DENSE_B_CTA, 0, st>>>(c->x.p, c->w.p, c->Lq.p, c->tpack.p, c->psi.p, a,
                                                                     qslice, c->gpart.p);
         else
-            k_grad_dense<DIM, true><<<g, DENSE_B_THREADS, 0, st>>>(c->x.p, c->w.p, c->Lq.p, c->tpack.p, c->psi.p, a,
+            k_grad_dense<DIM, true><<<g, DENSE_B_CTA, 0, st>>>(c->x.p, c->w.p, c->Lq.p, c->tpack.p, c->psi.p, a,
                                                                    qslice, c->gpart.p);
     } else {
         nval = c->nsblk;
@@ -985,9 +982,9 @@ static void noalloc_launch(sdot_ctx *c, const EvalArgs &a, double *S, const Noal
     const int64_t qslice = (a.nq + L.nks - 1) / L.nks;
     dim3 g((unsigned)tb, (unsigned)L.nks);
     if (c->precision == SDOT_PREC_FP64)
-        k_grad_dense<DIM, false><<<g, DENSE_B_THREADS, 0, st>>>(c->x.p, c->w.p, Lq, tpack, psi, a, qslice, gpart);
+        k_grad_dense<DIM, false><<<g, DENSE_B_CTA, 0, st>>>(c->x.p, c->w.p, Lq, tpack, psi, a, qslice, gpart);
     else
-        k_grad_dense<DIM, true><<<g, DENSE_B_THREADS, 0, st>>>(c->x.p, c->w.p, Lq, tpack, psi, a, qslice, gpart);
+        k_grad_dense<DIM, true><<<g, DENSE_B_CTA, 0, st>>>(c->x.p, c->w.p, Lq, tpack, psi, a, qslice, gpart);
     k_finalize_grad<<<FIN_BLOCKS, FIN_THREADS, 0, st>>>(a.nt, L.nks, gpart, c->nu.p, psi, nullptr,
                                                        c->prm.tolerance, 1, grad, redpart);
     k_finalize_scalars<<<1, FIN_SCALAR_THREADS, 0, st>>>(FIN_BLOCKS, redpart, L.nval, blkpart, scal);

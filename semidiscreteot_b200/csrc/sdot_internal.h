@@ -34,6 +34,26 @@ constexpr int DENSE_A_THREADS = 128; // dense value sweep: threads per CTA
 constexpr int DENSE_A_QT = 1;        // dense value sweep: quadrature points per thread (1: the most CTAs for small sources)
 constexpr int DENSE_B_THREADS = 128; // dense gradient sweep: threads per CTA
 constexpr int DENSE_B_TT = 2;        // dense gradient sweep: targets per thread
+constexpr int DENSE_B_QG = 4;        // dense gradient sweep: point groups per CTA (single-problem path)
+constexpr int DENSE_B_CTA = DENSE_B_THREADS * DENSE_B_QG;  // its threads per CTA
+
+// Quadrature slices of the single-problem dense gradient sweep for nq points
+// and nt targets: the (target block, slice) CTAs fill two CTAs per SM of a
+// 148-SM part (rounded down, so that they run as one wave), slices of at
+// least 256 points, at most DENSE_B_MAXKS.  Two CTAs of DENSE_B_CTA threads
+// per SM (32 warps) measured faster than three with registers capped at 40
+// (spills) and than 256-thread CTAs.
+constexpr int DENSE_B_MAXKS = 128;
+constexpr int DENSE_B_PER_SM = 2;
+inline int dense_grad_slices(int64_t nq, int64_t nt)
+{
+    const int64_t tb = (nt + DENSE_B_THREADS * DENSE_B_TT - 1) / (DENSE_B_THREADS * DENSE_B_TT);
+    int64_t k = (int64_t)148 * DENSE_B_PER_SM / (tb > 0 ? tb : 1);
+    const int64_t maxks = (nq + 255) / 256;
+    if (k > maxks) k = maxks;
+    if (k > DENSE_B_MAXKS) k = DENSE_B_MAXKS;
+    return (int)(k < 1 ? 1 : k);
+}
 constexpr int TPACK = 8;             // doubles per packed target
 constexpr int MAX_QPC = 64;          // quadrature points per cell supported
 constexpr double KAPPA = 23.083120654223414;  // 16 / ln 2
