@@ -181,42 +181,26 @@ __device__ __forceinline__ void dense_value_merge(const double *__restrict__ x, 
 
 constexpr int DB_CHUNK = 256;
 
-// One CTA's work of the dense gradient sweep: targets of block tblk against
-// quadrature slice ks; writes gpart[ks * nt + j].  Shared by the
-// single-problem kernel (QG = DENSE_B_QG) and the batched one (QG = 1).
-// The CTA is QG groups of DENSE_B_THREADS threads: thread lt of every group
-// holds the same TT targets, group g takes the staged points g, g + QG, ...,
-// and the groups' sums are added in group order at the end, so a slice's
-// partial does not depend on the scheduling.
-template <int DIM, bool FP32, int QG = 1>
-__device__ __forceinline__ void dense_grad_block(const double *__restrict__ x, const double *__restrict__ w,
-                                                 const double *__restrict__ Lq, const double *__restrict__ tpack,
-                                                 const double *__restrict__ psi, const EvalArgs &a, int64_t qslice,
-                                                 int64_t tblk, int64_t ks, double *__restrict__ gpart)
-{
-    constexpr int TT = DENSE_B_TT;
-    constexpr int TB = DENSE_B_THREADS * TT;
-    constexpr int NTH = DENSE_B_THREADS * QG;          // threads of the CTA
-    constexpr int CH = DB_CHUNK * (QG > 1 ? 2 : 1);    // points staged at a time
-    __shared__ double tab[16];
-    __shared__ __align__(16) double stgd[FP32 ? 1 : CH * (DIM + 2)];
-    __shared__ __align__(16) float stgf[FP32 ? CH * 4 : 1];
-    __shared__ float stgw[FP32 ? CH : 1];
-    __shared__ double gsum[QG > 1 ? (QG - 1) * TT * DENSE_B_THREADS : 1];
-    if (threadIdx.x < 16) tab[threadIdx.x] = c_exp2_tab[threadIdx.x];
-    const int tid = threadIdx.x;
-    const int lt = tid % DENSE_B_THREADS;  // target lane
-    const int grp = tid / DENSE_B_THREADS; // point group
-    const int64_t j0 = tblk * TB;
-    const int64_t qa = ks * qslice;
-    const int64_t qb = min(a.nq, qa + qslice);
-
-    // per-target data and the block centring (FP32 path)
+// Per-target data of one CTA of the gradient sweep: the TT targets j0 + lt +
+// k * DENSE_B_THREADS of thread lane lt.  FP32: the CTA's target box centre
+// ob and the reference aref = max_j (log2 nu_j + psi_j log2(e) / eps) (block
+// reductions over the CTA's NTH threads), each target relative to ob (yt) and
+// its exponent offset alpha = log2 nu_j + psi_j log2(e) / eps - aref; FP64:
+// A_j and B_j of the packed target.
+template <int TT>
+struct GradTargets {
     double ob[3] = {0.0, 0.0, 0.0};
     double aref = 0.0;
     float yt[TT][3], alpha[TT];
-    double A[TT], B[TT][3], acc64[TT];
+    double A[TT], B[TT][3];
     bool has[TT];
+};
+
+template <int DIM, bool FP32, int NTH, int TT>
+__device__ __forceinline__ void grad_targets(const double *__restrict__ tpack, const double *__restrict__ psi,
+                                             const EvalArgs &a, int64_t j0, int lt, GradTargets<TT> &T)
+{
+    const int tid = threadIdx.x;
     if (FP32) {
         double lo[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, hi[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
         double amax = -DBL_MAX;
@@ -256,25 +240,67 @@ __device__ __forceinline__ void dense_grad_block(const double *__restrict__ x, c
             amax = fmax(amax, sred[6][i]);
         }
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) ob[d] = 0.5 * (lo[d] + hi[d]);
-        aref = (amax > -DBL_MAX && isfinite(amax)) ? amax : 0.0;
+        for (int d = 0; d < DIM; ++d) T.ob[d] = 0.5 * (lo[d] + hi[d]);
+        T.aref = (amax > -DBL_MAX && isfinite(amax)) ? amax : 0.0;
     }
 #pragma unroll
     for (int k = 0; k < TT; ++k) {
         const int64_t j = j0 + lt + k * DENSE_B_THREADS;
-        has[k] = j < a.nt;
-        acc64[k] = 0.0;
-        const double *tp = tpack + (has[k] ? j : 0) * TPACK;
+        T.has[k] = j < a.nt;
+        const double *tp = tpack + (T.has[k] ? j : 0) * TPACK;
         if (FP32) {
 #pragma unroll
-            for (int d = 0; d < 3; ++d) yt[k][d] = (d < DIM && has[k]) ? (float)(tp[2 + DIM + d] - ob[d]) : 0.f;
-            alpha[k] = has[k] ? (float)(log2(tp[1 + DIM]) + a.l2e_eps * psi[j] - aref) : -INFINITY;
+            for (int d = 0; d < 3; ++d) T.yt[k][d] = (d < DIM && T.has[k]) ? (float)(tp[2 + DIM + d] - T.ob[d]) : 0.f;
+            T.alpha[k] = T.has[k] ? (float)(log2(tp[1 + DIM]) + a.l2e_eps * psi[j] - T.aref) : -INFINITY;
         } else {
-            A[k] = tp[0];
+            T.A[k] = tp[0];
 #pragma unroll
-            for (int d = 0; d < DIM; ++d) B[k][d] = tp[1 + d];
+            for (int d = 0; d < DIM; ++d) T.B[k][d] = tp[1 + d];
         }
     }
+}
+
+// One CTA's work of the dense gradient sweep: targets of block tblk against
+// quadrature slice ks; writes gpart[ks * nt + j].  Shared by the
+// single-problem kernel (QG = DENSE_B_QG) and the batched one (QG = 1).
+// The CTA is QG groups of DENSE_B_THREADS threads: thread lt of every group
+// holds the same TT targets, group g takes the staged points g, g + QG, ...,
+// and the groups' sums are added in group order at the end, so a slice's
+// partial does not depend on the scheduling.
+template <int DIM, bool FP32, int QG = 1>
+__device__ __forceinline__ void dense_grad_block(const double *__restrict__ x, const double *__restrict__ w,
+                                                 const double *__restrict__ Lq, const double *__restrict__ tpack,
+                                                 const double *__restrict__ psi, const EvalArgs &a, int64_t qslice,
+                                                 int64_t tblk, int64_t ks, double *__restrict__ gpart)
+{
+    constexpr int TT = DENSE_B_TT;
+    constexpr int TB = DENSE_B_THREADS * TT;
+    constexpr int NTH = DENSE_B_THREADS * QG;          // threads of the CTA
+    constexpr int CH = DB_CHUNK * (QG > 1 ? 2 : 1);    // points staged at a time
+    __shared__ double tab[16];
+    __shared__ __align__(16) double stgd[FP32 ? 1 : CH * (DIM + 2)];
+    __shared__ __align__(16) float stgf[FP32 ? CH * 4 : 1];
+    __shared__ float stgw[FP32 ? CH : 1];
+    __shared__ double gsum[QG > 1 ? (QG - 1) * TT * DENSE_B_THREADS : 1];
+    if (threadIdx.x < 16) tab[threadIdx.x] = c_exp2_tab[threadIdx.x];
+    const int tid = threadIdx.x;
+    const int lt = tid % DENSE_B_THREADS;  // target lane
+    const int grp = tid / DENSE_B_THREADS; // point group
+    const int64_t j0 = tblk * TB;
+    const int64_t qa = ks * qslice;
+    const int64_t qb = min(a.nq, qa + qslice);
+
+    GradTargets<TT> T;
+    grad_targets<DIM, FP32, NTH>(tpack, psi, a, j0, lt, T);
+    const double *ob = T.ob;
+    const double aref = T.aref;
+    const auto &yt = T.yt;
+    const auto &alpha = T.alpha;
+    const auto &A = T.A;
+    const auto &B = T.B;
+    double acc64[TT];
+#pragma unroll
+    for (int k = 0; k < TT; ++k) acc64[k] = 0.0;
     const float c32 = (float)a.c32;
     for (int64_t c0 = qa; c0 < qb; c0 += CH) {
         const int cn = (int)min((int64_t)CH, qb - c0);

@@ -27,6 +27,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <type_traits>
 
 #include "sdot_dense.cuh"
 #include "sdot_device.cuh"
@@ -288,6 +289,228 @@ k_value_dense_tensor(const double *__restrict__ x, const double *__restrict__ tp
         for (int q = 0; q < NQ; ++q) {
             out[2 * q] = mx[q];
             out[2 * q + 1] = (mx[q] == -CUDART_INF) ? 0.0 : S[q] * exp2_16(M - mx[q], tab);
+        }
+    }
+}
+
+// Sum over a tensor-grid cell's points of W_q prod_d r_d^(i_d) (point
+// q = i_0 + TM i_1 (+ TM^2 i_2)), by Horner's scheme along each dimension.
+template <typename R>
+__device__ __forceinline__ R fma_r(R x, R y, R z)
+{
+    if constexpr (sizeof(R) == 4) return fmaf(x, y, z);
+    else return fma(x, y, z);
+}
+
+template <int DIM, int TM, typename R>
+__device__ __forceinline__ R cell_sum(const R *W, const R *r)
+{
+    R t2 = R(0);
+#pragma unroll
+    for (int i2 = (DIM == 3 ? TM - 1 : 0); i2 >= 0; --i2) {
+        R t1 = R(0);
+#pragma unroll
+        for (int i1 = TM - 1; i1 >= 0; --i1) {
+            const R *Wr = W + TM * i1 + TM * TM * i2;
+            R t0 = Wr[TM - 1];
+#pragma unroll
+            for (int i0 = TM - 2; i0 >= 0; --i0) t0 = fma_r(t0, r[0], Wr[i0]);
+            t1 = (i1 == TM - 1) ? t0 : fma_r(t1, r[1], t0);
+        }
+        t2 = (DIM == 2 || i2 == TM - 1) ? t1 : fma_r(t2, r[DIM == 3 ? 2 : 0], t1);
+    }
+    return t2;
+}
+
+// Dense gradient sweep over the tensor-grid cells of k_value_dense_tensor:
+// thread lane <-> DENSE_B_TT targets, the CTA's slice of cells staged in
+// shared memory, DENSE_B_QG groups taking every QG-th staged cell, the
+// groups' sums added in group order.  With the cell centre C, the half
+// spacing a_d and point offsets delta_qd = (H i_d - 1) a_d,
+// |x_q - y|^2 = |C - y|^2 + sum_d (2 delta_qd (C_d - y_d) + delta_qd^2), so a
+// (point, target) term is a cell factor times one factor per dimension
+// raised to i_d times a per-point weight that does not depend on the target:
+//   FP32: 2^(alpha_j + beta_q - c |x_q - y_j|^2)
+//       = 2^(alpha_j + bref - c |C - y_j|^2 - sum_d v_d) prod_d 2^(H v_d i_d) W_q,
+//         v_d = -2 c a_d (C_d - y_d),  W_q = w_q 2^(beta_q - c |delta_q|^2 - bref);
+//   FP64: 2^(u_qj / 16), u_qj = A_j + B_j . (x_q - o) + D_q
+//       = 2^((A_j + B_j . (C - o) - sum_d G_d + Dref) / 16) prod_d 2^(H G_d i_d / 16) W_q,
+//         G_d = B_jd a_d,  W_q = w_q 2^((D_q - Dref) / 16),
+// where bref / Dref is the largest per-point part in the cell (W_q <= w_q).
+// One exponential per cell and one per dimension replace TM^DIM.  The
+// caller admits the FP32 form only when the factors of a cell span less
+// than 2^60 (dense_grad_tensor), so no factor or Horner sum leaves the FP32
+// range; the FP64 form inherits the tensor value sweep's bound.
+// Non-finite L_q: a cell whose parts are all -inf contributes 0 (as every
+// one of its terms does); a +inf part gives a NaN term where the per-point
+// form gives +inf (both non-finite, flagged by the finalize).
+template <int DIM, int TM, bool FP32>
+__global__ void __launch_bounds__(DENSE_B_CTA, DENSE_B_PER_SM)
+k_grad_dense_tensor(const double *__restrict__ x, const double *__restrict__ w, const double *__restrict__ Lq,
+                    const double *__restrict__ tpack, const double *__restrict__ psi, EvalArgs a, int64_t ncells,
+                    int64_t cslice, double *__restrict__ gpart)
+{
+    constexpr int NQ = DIM == 3 ? TM * TM * TM : TM * TM;
+    constexpr int TT = DENSE_B_TT;
+    constexpr int QG = DENSE_B_QG;
+    constexpr int NTH = DENSE_B_CTA;
+    constexpr int GC = NTH / NQ < 64 ? NTH / NQ : 64;  // cells staged at a time: one point per thread
+    constexpr int CR = 16;                             // cell record: W (NQ), C (DIM), k (DIM), reference
+    static_assert(NQ + 2 * DIM + 1 <= CR, "cell record");
+    constexpr double H = TM == 2 ? 2.0 : 1.0;
+    using R = typename std::conditional<FP32, float, double>::type;
+    __shared__ double tab[16];
+    __shared__ __align__(16) R crec[GC * CR];
+    __shared__ double pb[GC * NQ];
+    if (threadIdx.x < 16) tab[threadIdx.x] = c_exp2_tab[threadIdx.x];
+    const int tid = threadIdx.x;
+    const int lt = tid % DENSE_B_THREADS;
+    const int grp = tid / DENSE_B_THREADS;
+    const int64_t j0 = blockIdx.x * (int64_t)(DENSE_B_THREADS * TT);
+    GradTargets<TT> T;
+    grad_targets<DIM, FP32, NTH>(tpack, psi, a, j0, lt, T);
+    double acc64[TT];
+#pragma unroll
+    for (int k = 0; k < TT; ++k) acc64[k] = 0.0;
+    const int64_t ca = blockIdx.y * cslice;
+    const int64_t cb = min(ncells, ca + cslice);
+    const float c32 = (float)a.c32;
+    for (int64_t c0 = ca; c0 < cb; c0 += GC) {
+        const int cn = (int)min((int64_t)GC, cb - c0);
+        const int cl = tid / NQ, qi = tid - cl * NQ;
+        const bool act = cl < cn;
+        const int64_t cq0 = (c0 + (act ? cl : 0)) * NQ;
+        // the cell's centre and half spacing from its extreme points along each dimension
+        double cen[DIM], ah[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            const int stride = d == 0 ? 1 : (d == 1 ? TM : TM * TM);
+            const double lo = x[cq0 * DIM + d], hi = x[(cq0 + (int64_t)(TM - 1) * stride) * DIM + d];
+            cen[d] = 0.5 * (lo + hi);
+            ah[d] = hi - cen[d];
+        }
+        __syncthreads();  // the previous cells' records are consumed
+        double wq = 0.0;
+        if (act) {
+            // the part of point q's exponent that does not depend on the target
+            const int64_t q = cq0 + qi;
+            double part;
+            if (FP32) {
+                double dsq = 0.0;
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) {
+                    const double dl = x[q * DIM + d] - cen[d];
+                    dsq += dl * dl;
+                }
+                part = -LOG2E * Lq[q] + T.aref - a.c32 * dsq;
+            } else {
+                double xsq = 0.0;
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) {
+                    const double xt = x[q * DIM + d] - a.o[d];
+                    xsq += xt * xt;
+                }
+                part = -a.halfs * xsq - KAPPA * Lq[q];
+            }
+            pb[tid] = part;
+            wq = w[q];
+        }
+        __syncthreads();
+        if (act) {
+            double ref = -CUDART_INF;
+#pragma unroll
+            for (int u = 0; u < NQ; ++u) ref = fmax(ref, pb[cl * NQ + u]);
+            const bool none = ref == -CUDART_INF;  // every term of the cell is 0
+            const double own = pb[tid];
+            const double Wq = none ? 0.0 : (FP32 ? wq * exp2(own - ref) : wq * exp2_16(own - ref, tab));
+            R *rec = crec + cl * CR;
+            rec[qi] = (R)Wq;
+            if (qi == 0) {
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) {
+                    rec[NQ + d] = FP32 ? (R)(cen[d] - T.ob[d]) : (R)(cen[d] - a.o[d]);
+                    rec[NQ + DIM + d] = FP32 ? (R)(-2.0 * a.c32 * ah[d]) : (R)ah[d];
+                }
+                rec[NQ + 2 * DIM] = (R)(none ? 0.0 : ref);
+            }
+        }
+        __syncthreads();
+        if constexpr (FP32) {
+            float acc[TT];
+#pragma unroll
+            for (int k = 0; k < TT; ++k) acc[k] = 0.f;
+            int n = 0;
+            for (int cc = grp; cc < cn; cc += QG, ++n) {
+                const float *rec = crec + cc * CR;
+                float Wc[NQ], Cc[DIM], kd[DIM];
+#pragma unroll
+                for (int u = 0; u < NQ; ++u) Wc[u] = rec[u];
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) { Cc[d] = rec[NQ + d]; kd[d] = rec[NQ + DIM + d]; }
+                const float bref = rec[NQ + 2 * DIM];
+#pragma unroll
+                for (int k = 0; k < TT; ++k) {
+                    float D2 = 0.f, sv = 0.f, r[DIM];
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) {
+                        const float dc = Cc[d] - T.yt[k][d];
+                        D2 = fmaf(dc, dc, D2);
+                        const float v = kd[d] * dc;
+                        sv += v;
+                        r[d] = ex2_approx((float)H * v);
+                    }
+                    const float P = ex2_approx(fmaf(-c32, D2, T.alpha[k] + bref) - sv);
+                    acc[k] = fmaf(P, cell_sum<DIM, TM, float>(Wc, r), acc[k]);
+                }
+                if ((n & 7) == 7) {
+#pragma unroll
+                    for (int k = 0; k < TT; ++k) { acc64[k] += (double)acc[k]; acc[k] = 0.f; }
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < TT; ++k) acc64[k] += (double)acc[k];
+        } else {
+            for (int cc = grp; cc < cn; cc += QG) {
+                const double *rec = crec + cc * CR;
+                double Wc[NQ], Cm[DIM], ad[DIM];
+#pragma unroll
+                for (int u = 0; u < NQ; ++u) Wc[u] = rec[u];
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) { Cm[d] = rec[NQ + d]; ad[d] = rec[NQ + DIM + d]; }
+                const double Dref = rec[NQ + 2 * DIM];
+#pragma unroll
+                for (int k = 0; k < TT; ++k) {
+                    double B0 = T.A[k], sg = 0.0, r[DIM];
+#pragma unroll
+                    for (int d = 0; d < DIM; ++d) {
+                        B0 = fma(T.B[k][d], Cm[d], B0);
+                        const double G = T.B[k][d] * ad[d];
+                        sg += G;
+                        r[d] = exp2_16(H * G, tab);
+                    }
+                    const double P = exp2_16(B0 - sg + Dref, tab);
+                    acc64[k] = fma(P, cell_sum<DIM, TM, double>(Wc, r), acc64[k]);
+                }
+            }
+        }
+    }
+    // the groups' sums, added in group order by group 0
+    __shared__ double gsum[(QG - 1) * TT * DENSE_B_THREADS];
+    if (grp > 0) {
+#pragma unroll
+        for (int k = 0; k < TT; ++k) gsum[((grp - 1) * TT + k) * DENSE_B_THREADS + lt] = acc64[k];
+    }
+    __syncthreads();
+    if (grp == 0) {
+#pragma unroll
+        for (int k = 0; k < TT; ++k) {
+            for (int g = 1; g < QG; ++g) acc64[k] += gsum[((g - 1) * TT + k) * DENSE_B_THREADS + lt];
+            const int64_t j = j0 + lt + k * DENSE_B_THREADS;
+            if (j < a.nt) {
+                double gv = acc64[k];
+                if (!FP32) gv *= tpack[j * TPACK + 1 + DIM];  // nu_j (FP32 folds it into alpha)
+                gpart[blockIdx.y * a.nt + j] = gv;
+            }
         }
     }
 }
@@ -591,6 +814,41 @@ static void launch_value_dense_tensor(const DenseShape &ds, const double *x, con
     }
 }
 
+// The tensor-cell gradient sweep runs on the tensor value sweep's cells; its
+// FP32 form only where a cell's factors span at most 2^60 (their exponents
+// vary by H log2(e) / eps |C - y| a_d (TM - 1) per dimension, |C - y| <= diam).
+static bool dense_grad_tensor(const sdot_ctx *c, int tm, bool fp32, const EvalArgs &a)
+{
+    if (tm <= 0) return false;
+    if (!fp32) return true;
+    const double spread = (tm == 2 ? 2.0 : 1.0) * a.l2e_eps * c->diam * c->tensor_amax * (tm - 1) * c->dim;
+    return spread <= 60.0;
+}
+
+template <int DIM>
+static void launch_grad_dense(const sdot_ctx *c, const DenseShape &ds, bool fp32, const double *Lq,
+                              const double *tpack, const double *psi, const EvalArgs &a, double *gpart,
+                              cudaStream_t st)
+{
+    const dim3 g((unsigned)ds.tb, (unsigned)ds.nks);
+    if (dense_grad_tensor(c, ds.tm, fp32, a)) {
+        const int64_t cs = (c->ncells + ds.nks - 1) / ds.nks;
+        auto go = [&](auto kern) {
+            kern<<<g, DENSE_B_CTA, 0, st>>>(c->x.p, c->w.p, Lq, tpack, psi, a, c->ncells, cs, gpart);
+        };
+        if constexpr (DIM == 2) {
+            if (ds.tm == 3) fp32 ? go(k_grad_dense_tensor<2, 3, true>) : go(k_grad_dense_tensor<2, 3, false>);
+            else fp32 ? go(k_grad_dense_tensor<2, 2, true>) : go(k_grad_dense_tensor<2, 2, false>);
+        } else {
+            fp32 ? go(k_grad_dense_tensor<3, 2, true>) : go(k_grad_dense_tensor<3, 2, false>);
+        }
+        return;
+    }
+    const int64_t qslice = (a.nq + ds.nks - 1) / ds.nks;
+    if (fp32) k_grad_dense<DIM, true><<<g, DENSE_B_CTA, 0, st>>>(c->x.p, c->w.p, Lq, tpack, psi, a, qslice, gpart);
+    else k_grad_dense<DIM, false><<<g, DENSE_B_CTA, 0, st>>>(c->x.p, c->w.p, Lq, tpack, psi, a, qslice, gpart);
+}
+
 template <int DIM>
 static sdot_status run_eval(sdot_ctx *c, const EvalArgs &a, bool dense, const double *pdir, double tol, bool partial)
 {
@@ -636,17 +894,9 @@ static sdot_status run_eval(sdot_ctx *c, const EvalArgs &a, bool dense, const do
                                                                            c->Lq.p, c->blkpart.p);
         }
         mark(2);
-        // gradient: target blocks x q-slices
-        const int64_t tb = ds.tb;
+        // gradient: target blocks x point (or cell) slices
         nks = ds.nks;
-        const int64_t qslice = (a.nq + nks - 1) / nks;
-        dim3 g((unsigned)tb, (unsigned)nks);
-        if (prec == SDOT_PREC_FP64)
-            k_grad_dense<DIM, false><<<g, DENSE_B_CTA, 0, st>>>(c->x.p, c->w.p, c->Lq.p, c->tpack.p, c->psi.p, a,
-                                                                    qslice, c->gpart.p);
-        else
-            k_grad_dense<DIM, true><<<g, DENSE_B_CTA, 0, st>>>(c->x.p, c->w.p, c->Lq.p, c->tpack.p, c->psi.p, a,
-                                                                   qslice, c->gpart.p);
+        launch_grad_dense<DIM>(c, ds, prec != SDOT_PREC_FP64, c->Lq.p, c->tpack.p, c->psi.p, a, c->gpart.p, st);
     } else {
         nval = c->nsblk;
         k_target_prep_kd<DIM><<<grid_for(a.nt, 256), 256, 0, st>>>(a.nt, c->y.p, c->nu.p, c->psi.p, a, c->tpack.p);
@@ -978,13 +1228,7 @@ static void noalloc_launch(sdot_ctx *c, const EvalArgs &a, double *S, const Noal
         k_value_dense<DIM><<<(unsigned)L.nval, DENSE_A_THREADS, 0, st>>>(c->x.p, c->rho.p, c->jxw.p, tpack, a, Lq,
                                                                           blkpart);
     }
-    const int64_t tb = dense_shape(a.nq, a.nt).tb;
-    const int64_t qslice = (a.nq + L.nks - 1) / L.nks;
-    dim3 g((unsigned)tb, (unsigned)L.nks);
-    if (c->precision == SDOT_PREC_FP64)
-        k_grad_dense<DIM, false><<<g, DENSE_B_CTA, 0, st>>>(c->x.p, c->w.p, Lq, tpack, psi, a, qslice, gpart);
-    else
-        k_grad_dense<DIM, true><<<g, DENSE_B_CTA, 0, st>>>(c->x.p, c->w.p, Lq, tpack, psi, a, qslice, gpart);
+    launch_grad_dense<DIM>(c, L.ds, c->precision != SDOT_PREC_FP64, Lq, tpack, psi, a, gpart, st);
     k_finalize_grad<<<FIN_BLOCKS, FIN_THREADS, 0, st>>>(a.nt, L.nks, gpart, c->nu.p, psi, nullptr,
                                                        c->prm.tolerance, 1, grad, redpart);
     k_finalize_scalars<<<1, FIN_SCALAR_THREADS, 0, st>>>(FIN_BLOCKS, redpart, L.nval, blkpart, scal);
