@@ -133,29 +133,44 @@ __device__ __forceinline__ void dense_value_slice(const double *__restrict__ x, 
 }
 
 // Merge of the target slices of point block blk (slice s of point q at
-// ms[s * 2 nq + 2 q ..]): the largest exponent over the slices, the sums
-// rescaled to it and added in slice order, then the epilogue of
-// dense_value_block (L_q, value, C, skipped) and the block's partials.
+// ms[s * 2 nq + 2 q ..]) by DENSE_MERGE_SPLIT lanes per point: lane u takes
+// the slices s = u, u + SPLIT, ... (their loads in flight together); the
+// largest exponent over the slices, each lane's sums rescaled to it and
+// added in order of s, the lanes' sums added by xor exchanges in a fixed
+// tree; then the epilogue of dense_value_block (L_q, value, C, skipped) and
+// the block's partials.  The CTA has DENSE_A_THREADS * SPLIT threads.
+constexpr int DENSE_MERGE_SPLIT = 4;
+
 template <int DIM>
 __device__ __forceinline__ void dense_value_merge(const double *__restrict__ x, const double *__restrict__ rho,
                                                   const double *__restrict__ jxw, const double *__restrict__ ms,
                                                   int nslice, const EvalArgs &a, int64_t blk,
                                                   double *__restrict__ Lq, double *__restrict__ out4)
 {
+    constexpr int SP = DENSE_MERGE_SPLIT;
     __shared__ double tab[16];
     if (threadIdx.x < 16) tab[threadIdx.x] = c_exp2_tab[threadIdx.x];
     __syncthreads();
-    const int64_t q = blk * DENSE_A_THREADS + threadIdx.x;
+    const int u = threadIdx.x % SP;
+    const int64_t q = blk * DENSE_A_THREADS + threadIdx.x / SP;
+    const bool ok = q < a.nq;
+    const double *mq = ms + 2 * (ok ? q : 0);
+    const int64_t st = 2 * a.nq;
+    double mx = -CUDART_INF;
+    if (ok)
+        for (int s = u; s < nslice; s += SP) mx = fmax(mx, mq[s * st]);
+#pragma unroll
+    for (int o = 1; o < SP; o <<= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    double S = 0.0;
+    if (ok && mx > -CUDART_INF)
+        for (int s = u; s < nslice; s += SP) {
+            const double2 v = *reinterpret_cast<const double2 *>(mq + s * st);
+            if (v.x > -CUDART_INF) S += v.y * exp2_16(v.x - mx, tab);
+        }
+#pragma unroll
+    for (int o = 1; o < SP; o <<= 1) S += __shfl_xor_sync(0xffffffffu, S, o);
     double tv = 0.0, tc = 0.0, ts = 0.0;
-    if (q < a.nq) {
-        double mx = -CUDART_INF;
-        for (int s = 0; s < nslice; ++s) mx = fmax(mx, ms[(int64_t)s * 2 * a.nq + 2 * q]);
-        double S = 0.0;
-        if (mx > -CUDART_INF)
-            for (int s = 0; s < nslice; ++s) {
-                const double m = ms[(int64_t)s * 2 * a.nq + 2 * q];
-                if (m > -CUDART_INF) S += ms[(int64_t)s * 2 * a.nq + 2 * q + 1] * exp2_16(m - mx, tab);
-            }
+    if (ok && u == 0) {
         double xsq = 0.0;
 #pragma unroll
         for (int d = 0; d < DIM; ++d) {

@@ -163,8 +163,10 @@ k_value_dense_slice(const double *__restrict__ x, const double *__restrict__ tpa
     dense_value_slice<DIM>(x, tpack, a, blockIdx.x, t0, t1, ms + (int64_t)blockIdx.y * 2 * a.nq);
 }
 
+constexpr int MERGE_THREADS = DENSE_A_THREADS * DENSE_MERGE_SPLIT;
+
 template <int DIM>
-__global__ void __launch_bounds__(DENSE_A_THREADS)
+__global__ void __launch_bounds__(MERGE_THREADS)
 k_value_dense_merge(const double *__restrict__ x, const double *__restrict__ rho, const double *__restrict__ jxw,
                     const double *__restrict__ ms, int nslice, EvalArgs a, double *__restrict__ Lq,
                     double *__restrict__ part)
@@ -530,35 +532,63 @@ k_grad_dense(const double *__restrict__ x, const double *__restrict__ w, const d
 // ---------------------------------------------------------------------------
 
 constexpr int FIN_THREADS = 256;
-constexpr int FIN_BLOCKS = 148;
+constexpr int FIN_BLOCKS = 148;  // largest grid of k_finalize_grad
+constexpr int FIN_PARTS = 8;     // lanes per target in k_finalize_grad
 constexpr int NRED = 8;  // psinu, l1, linf, comp, l2sq, gp, nonfinite, unused
 
+// Grid of k_finalize_grad for nt targets (FIN_THREADS / FIN_PARTS targets per CTA and pass).
+static int fin_blocks(int64_t nt)
+{
+    const int64_t per = FIN_THREADS / FIN_PARTS;
+    const int64_t g = (nt + per - 1) / per;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(FIN_BLOCKS, g));
+}
+
+// Lanes 8t .. 8t+7 of a warp own target j: lane u sums the slice partials
+// k = u, u + 8, ... in order of k (the eight interleaved sums, each with its
+// loads in flight together), and three xor exchanges add them in the fixed
+// tree ((s0 + s1) + (s2 + s3)) + ((s4 + s5) + (s6 + s7)).
 __global__ void __launch_bounds__(FIN_THREADS)
 k_finalize_grad(int64_t nt, int nks, const double *__restrict__ gpart, const double *__restrict__ nu,
                 const double *__restrict__ psi, const double *__restrict__ pdir, double tol, int sub_nu,
                 double *__restrict__ grad, double *__restrict__ redpart)
 {
+    constexpr int TPB = FIN_THREADS / FIN_PARTS;  // targets per CTA and pass
+    const int u = threadIdx.x % FIN_PARTS;
     double psinu = 0.0, l1 = 0.0, linf = 0.0, comp = -CUDART_INF, l2 = 0.0, gp = 0.0, bad = 0.0;
-    for (int64_t j = blockIdx.x * (int64_t)FIN_THREADS + threadIdx.x; j < nt; j += (int64_t)gridDim.x * FIN_THREADS) {
-        // the q-slice partials in eight interleaved sums (eight loads in flight), added in a fixed tree
-        double acc[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-        int k = 0;
-        for (; k + 8 <= nks; k += 8) {
-#pragma unroll
-            for (int u = 0; u < 8; ++u) acc[u] += gpart[(int64_t)(k + u) * nt + j];
+    for (int64_t base = blockIdx.x * (int64_t)TPB; base < nt; base += (int64_t)gridDim.x * TPB) {
+        const int64_t j = base + threadIdx.x / FIN_PARTS;
+        const bool ok = j < nt;
+        double acc = 0.0;
+        if (ok) {
+            int k = u;
+            for (; k + 3 * FIN_PARTS < nks; k += 4 * FIN_PARTS) {
+                const double v0 = gpart[(int64_t)k * nt + j];
+                const double v1 = gpart[(int64_t)(k + FIN_PARTS) * nt + j];
+                const double v2 = gpart[(int64_t)(k + 2 * FIN_PARTS) * nt + j];
+                const double v3 = gpart[(int64_t)(k + 3 * FIN_PARTS) * nt + j];
+                acc += v0;
+                acc += v1;
+                acc += v2;
+                acc += v3;
+            }
+            for (; k < nks; k += FIN_PARTS) acc += gpart[(int64_t)k * nt + j];
         }
-        for (; k < nks; ++k) acc[k & 7] += gpart[(int64_t)k * nt + j];
-        const double s = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
-        const double g = s - nu[j];
-        grad[j] = sub_nu ? g : s;
-        psinu += psi[j] * nu[j];
-        const double ag = fabs(g);
-        l1 += ag;
-        linf = fmax(linf, ag);
-        comp = fmax(comp, ag - nu[j] * tol);
-        l2 += g * g;
-        if (pdir) gp += g * pdir[j];
-        if (!isfinite(g) || !isfinite(psi[j])) bad = 1.0;
+#pragma unroll
+        for (int o = 1; o < FIN_PARTS; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (ok && u == 0) {
+            const double s = acc;
+            const double g = s - nu[j];
+            grad[j] = sub_nu ? g : s;
+            psinu += psi[j] * nu[j];
+            const double ag = fabs(g);
+            l1 += ag;
+            linf = fmax(linf, ag);
+            comp = fmax(comp, ag - nu[j] * tol);
+            l2 += g * g;
+            if (pdir) gp += g * pdir[j];
+            if (!isfinite(g) || !isfinite(psi[j])) bad = 1.0;
+        }
     }
     __shared__ double sh[NRED][FIN_THREADS / 32];
     psinu = warp_sum(psinu);
@@ -584,22 +614,24 @@ k_finalize_grad(int64_t nt, int nks, const double *__restrict__ gpart, const dou
     }
 }
 
-// one CTA of FIN_SCALAR_THREADS: thread i sums blocks i, i + FIN_SCALAR_THREADS, ... (a fixed tree)
-constexpr int FIN_SCALAR_THREADS = 1024;
+// One CTA of FIN_SCALAR_THREADS: thread i sums value partials i, i + T, i +
+// 2T, ... into four accumulators (partial i + kT into accumulator k mod 4,
+// four loads in flight), added in a fixed order, and the gradient blocks'
+// reductions i, i + T, ...; then warp and CTA reductions in a fixed tree.
+constexpr int FIN_SCALAR_THREADS = 256;
 __global__ void __launch_bounds__(FIN_SCALAR_THREADS)
 k_finalize_scalars(int nred, const double *__restrict__ redpart, int64_t nval, const double *__restrict__ valpart,
                    double *__restrict__ scal)
 {
-    __shared__ double sh[11][FIN_SCALAR_THREADS / 32];
-    // four block partials per thread and pass, each into its own accumulator
-    // (loads in flight), the accumulators added in a fixed order
+    constexpr int T = FIN_SCALAR_THREADS;
+    __shared__ double sh[11][T / 32];
     double va[4] = {0, 0, 0, 0}, ca[4] = {0, 0, 0, 0}, ska[4] = {0, 0, 0, 0}, npa[4] = {0, 0, 0, 0};
-    const int64_t bs = blockDim.x;
+    const double4 *vp = reinterpret_cast<const double4 *>(valpart);
     int64_t b0 = threadIdx.x;
-    for (; b0 + 3 * bs < nval; b0 += 4 * bs) {
+    for (; b0 + 3 * T < nval; b0 += 4 * T) {
         double4 t[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) t[u] = reinterpret_cast<const double4 *>(valpart)[b0 + u * bs];
+        for (int u = 0; u < 4; ++u) t[u] = vp[b0 + u * T];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             va[u] += t[u].x;
@@ -608,12 +640,15 @@ k_finalize_scalars(int nred, const double *__restrict__ redpart, int64_t nval, c
             npa[u] += t[u].w;
         }
     }
-    for (int u = 0; b0 < nval; b0 += bs, ++u) {
-        const double4 t = reinterpret_cast<const double4 *>(valpart)[b0];
-        va[u] += t.x;
-        ca[u] += t.y;
-        ska[u] += t.z;
-        npa[u] += t.w;
+#pragma unroll
+    for (int u = 0; u < 3; ++u) {
+        if (b0 + u * T < nval) {
+            const double4 t = vp[b0 + u * T];
+            va[u] += t.x;
+            ca[u] += t.y;
+            ska[u] += t.z;
+            npa[u] += t.w;
+        }
     }
     double v = (va[0] + va[1]) + (va[2] + va[3]), c = (ca[0] + ca[1]) + (ca[2] + ca[3]);
     double sk = (ska[0] + ska[1]) + (ska[2] + ska[3]), np = (npa[0] + npa[1]) + (npa[2] + npa[3]);
@@ -642,7 +677,8 @@ k_finalize_scalars(int nred, const double *__restrict__ redpart, int64_t nval, c
             t[7] += sh[7][i]; t[8] += sh[8][i]; t[9] = fmax(t[9], sh[9][i]);
         }
         const double psinu = t[3];
-        scal[SC_VALUE] = t[0] - psinu;
+        const double value = t[0] - psinu;
+        scal[SC_VALUE] = value;
         scal[SC_VALSRC] = t[0];
         scal[SC_C] = t[1];
         scal[SC_SKIPPED] = t[2];
@@ -652,7 +688,7 @@ k_finalize_scalars(int nred, const double *__restrict__ redpart, int64_t nval, c
         scal[SC_COMP] = t[6];
         scal[SC_L2SQ] = t[7];
         scal[SC_DOT_GP] = t[8];
-        scal[SC_NONFINITE] = (t[9] != 0.0 || !isfinite(scal[SC_VALUE])) ? 1.0 : 0.0;
+        scal[SC_NONFINITE] = (t[9] != 0.0 || !isfinite(value)) ? 1.0 : 0.0;
         scal[SC_PAIRS] = tnp;
     }
 }
@@ -878,17 +914,15 @@ static sdot_status run_eval(sdot_ctx *c, const EvalArgs &a, bool dense, const do
             const cudaError_t e = c->vpart.alloc((size_t)2 * ds.nvs * a.nq);
             if (e != cudaSuccess) return cuda_error(c, e, "dense value slices");
             launch_value_dense_tensor<DIM>(ds, c->x.p, c->tpack.p, a, c->ncells, c->vpart.p, st);
-            k_value_dense_merge<DIM><<<(unsigned)nval, DENSE_A_THREADS, 0, st>>>(c->x.p, c->rho.p, c->jxw.p,
-                                                                                 c->vpart.p, ds.nvs, a, c->Lq.p,
-                                                                                 c->blkpart.p);
+            k_value_dense_merge<DIM><<<(unsigned)nval, MERGE_THREADS, 0, st>>>(c->x.p, c->rho.p, c->jxw.p, c->vpart.p,
+                                                                               ds.nvs, a, c->Lq.p, c->blkpart.p);
         } else if (ds.nvs > 1) {
             const cudaError_t e = c->vpart.alloc((size_t)2 * ds.nvs * a.nq);
             if (e != cudaSuccess) return cuda_error(c, e, "dense value slices");
             k_value_dense_slice<DIM><<<dim3((unsigned)nval, (unsigned)ds.nvs), DENSE_A_THREADS, 0, st>>>(
                 c->x.p, c->tpack.p, a, ds.tslice, c->vpart.p);
-            k_value_dense_merge<DIM><<<(unsigned)nval, DENSE_A_THREADS, 0, st>>>(c->x.p, c->rho.p, c->jxw.p,
-                                                                                 c->vpart.p, ds.nvs, a, c->Lq.p,
-                                                                                 c->blkpart.p);
+            k_value_dense_merge<DIM><<<(unsigned)nval, MERGE_THREADS, 0, st>>>(c->x.p, c->rho.p, c->jxw.p, c->vpart.p,
+                                                                               ds.nvs, a, c->Lq.p, c->blkpart.p);
         } else {
             k_value_dense<DIM><<<(unsigned)nval, DENSE_A_THREADS, 0, st>>>(c->x.p, c->rho.p, c->jxw.p, c->tpack.p, a,
                                                                            c->Lq.p, c->blkpart.p);
@@ -904,9 +938,10 @@ static sdot_status run_eval(sdot_ctx *c, const EvalArgs &a, bool dense, const do
         if (s != SDOT_OK) return s;
     }
     if (dense) mark(3);
-    k_finalize_grad<<<FIN_BLOCKS, FIN_THREADS, 0, st>>>(a.nt, nks, c->gpart.p, c->nu.p, c->psi.p, pdir, tol,
-                                                       partial ? 0 : 1, c->grad.p, c->redpart.p);
-    k_finalize_scalars<<<1, FIN_SCALAR_THREADS, 0, st>>>(FIN_BLOCKS, c->redpart.p, nval, c->blkpart.p, c->scal.p);
+    const int fb = fin_blocks(a.nt);
+    k_finalize_grad<<<fb, FIN_THREADS, 0, st>>>(a.nt, nks, c->gpart.p, c->nu.p, c->psi.p, pdir, tol, partial ? 0 : 1,
+                                                c->grad.p, c->redpart.p);
+    k_finalize_scalars<<<1, FIN_SCALAR_THREADS, 0, st>>>(fb, c->redpart.p, nval, c->blkpart.p, c->scal.p);
     mark(4);
     c->klaunch[1] += 1;
     if (dense && c->distance == 0) {
@@ -1216,22 +1251,23 @@ static void noalloc_launch(sdot_ctx *c, const EvalArgs &a, double *S, const Noal
     if (L.ds.tm > 0) {
         double *vpart = S + L.vpart;
         launch_value_dense_tensor<DIM>(L.ds, c->x.p, tpack, a, c->ncells, vpart, st);
-        k_value_dense_merge<DIM><<<(unsigned)L.nval, DENSE_A_THREADS, 0, st>>>(c->x.p, c->rho.p, c->jxw.p, vpart,
-                                                                               L.nvs, a, Lq, blkpart);
+        k_value_dense_merge<DIM><<<(unsigned)L.nval, MERGE_THREADS, 0, st>>>(c->x.p, c->rho.p, c->jxw.p, vpart, L.nvs,
+                                                                             a, Lq, blkpart);
     } else if (L.nvs > 1) {
         double *vpart = S + L.vpart;
         k_value_dense_slice<DIM><<<dim3((unsigned)L.nval, (unsigned)L.nvs), DENSE_A_THREADS, 0, st>>>(
             c->x.p, tpack, a, L.tslice, vpart);
-        k_value_dense_merge<DIM><<<(unsigned)L.nval, DENSE_A_THREADS, 0, st>>>(c->x.p, c->rho.p, c->jxw.p, vpart,
-                                                                               L.nvs, a, Lq, blkpart);
+        k_value_dense_merge<DIM><<<(unsigned)L.nval, MERGE_THREADS, 0, st>>>(c->x.p, c->rho.p, c->jxw.p, vpart, L.nvs,
+                                                                             a, Lq, blkpart);
     } else {
         k_value_dense<DIM><<<(unsigned)L.nval, DENSE_A_THREADS, 0, st>>>(c->x.p, c->rho.p, c->jxw.p, tpack, a, Lq,
                                                                           blkpart);
     }
     launch_grad_dense<DIM>(c, L.ds, c->precision != SDOT_PREC_FP64, Lq, tpack, psi, a, gpart, st);
-    k_finalize_grad<<<FIN_BLOCKS, FIN_THREADS, 0, st>>>(a.nt, L.nks, gpart, c->nu.p, psi, nullptr,
-                                                       c->prm.tolerance, 1, grad, redpart);
-    k_finalize_scalars<<<1, FIN_SCALAR_THREADS, 0, st>>>(FIN_BLOCKS, redpart, L.nval, blkpart, scal);
+    const int fb = fin_blocks(a.nt);
+    k_finalize_grad<<<fb, FIN_THREADS, 0, st>>>(a.nt, L.nks, gpart, c->nu.p, psi, nullptr, c->prm.tolerance, 1, grad,
+                                                redpart);
+    k_finalize_scalars<<<1, FIN_SCALAR_THREADS, 0, st>>>(fb, redpart, L.nval, blkpart, scal);
 }
 
 }  // namespace sdot
