@@ -525,6 +525,7 @@ sdot_status sdot_set_source(sdot_ctx *c, int dim, int64_t n_q, const double *x, 
     // truncated sweeps then factor 2^(G.delta) per dimension.
     int tm = 0;
     double amax = 0.0;
+    double alo[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, ahi[3] = {0.0, 0.0, 0.0};  // per-dimension offset range
     for (int m = 2; m <= 3 && tm == 0; ++m) {
         int64_t p = 1;
         for (int d = 0; d < dim; ++d) p *= m;
@@ -545,6 +546,8 @@ sdot_status sdot_set_source(sdot_ctx *c, int dim, int64_t n_q, const double *x, 
                     if (X[q * dim + d] != X[(dig * stride) * dim + d]) ok = false;
                 }
                 amax = std::max(amax, std::fabs(o[m - 1]));
+                alo[d] = std::min(alo[d], std::fabs(o[m - 1]));
+                ahi[d] = std::max(ahi[d], std::fabs(o[m - 1]));
             }
         }
         if (ok) tm = m;
@@ -552,6 +555,12 @@ sdot_status sdot_set_source(sdot_ctx *c, int dim, int64_t n_q, const double *x, 
     }
     c->tensor_m = tm;
     c->tensor_amax = amax;
+    // one spacing per dimension for every cell (a uniform grid): the dense
+    // value sweep then takes the per-dimension factors per target
+    bool uni = tm > 0;
+    for (int d = 0; d < dim && uni; ++d) uni = ahi[d] - alo[d] <= 1e-13 * ahi[d];
+    c->tensor_uniform = uni;
+    for (int d = 0; d < 3; ++d) c->tensor_a[d] = (uni && d < dim) ? ahi[d] : 0.0;
     const int64_t nsblk = (int64_t)bounds.size() - 1;
     std::vector<double> ssph(nsblk * 4);
     for (int64_t b = 0; b < nsblk; ++b) {

@@ -188,13 +188,22 @@ k_value_dense_merge(const double *__restrict__ x, const double *__restrict__ rho
 // lse_update).  The per-point maxima are exact: a target updates them only
 // when its upper bound B0 + sum |G_d| reaches the largest lower bound
 // B0 - sum |G_d| seen so far, below which it cannot be any point's maximum.
-template <int DIM, int TM>
+// UNI (every cell has the offsets ua_d): G_d, its factor 2^(H G_d / 16) and
+// the sums of G_d and |G_d| depend on the target alone, so they are computed
+// once per staged target instead of once per (cell, target), leaving one
+// exponential per (cell, target).
+struct Spacing {
+    double a[3];
+};
+
+template <int DIM, int TM, bool UNI>
 __global__ void __launch_bounds__(DENSE_A_THREADS)
 k_value_dense_tensor(const double *__restrict__ x, const double *__restrict__ tpack, EvalArgs a, int64_t ncells,
-                     int64_t tslice, double *__restrict__ ms)
+                     int64_t tslice, Spacing ua, double *__restrict__ ms)
 {
     constexpr int NQ = DIM == 3 ? TM * TM * TM : TM * TM;
-    constexpr int TSZ = DIM + 2;  // A, B(DIM), nu
+    // staged per target: A, B(DIM), nu; UNI adds G(DIM), 2^(H G / 16) (DIM), sum G, sum |G|
+    constexpr int TSZ = UNI ? 3 * DIM + 4 : DIM + 2;
     constexpr double H = TM == 2 ? 2.0 : 1.0;
     __shared__ double tab[16];
     __shared__ double stg[DA_CHUNK * TSZ];
@@ -224,9 +233,29 @@ k_value_dense_tensor(const double *__restrict__ x, const double *__restrict__ tp
     for (int64_t c0 = t0; c0 < t1; c0 += DA_CHUNK) {
         const int cn = (int)min((int64_t)DA_CHUNK, t1 - c0);
         __syncthreads();
-        for (int i = threadIdx.x; i < cn * TSZ; i += DENSE_A_THREADS) {
-            const int t = i / TSZ, f = i - t * TSZ;
-            stg[i] = tpack[(c0 + t) * TPACK + f];
+        if constexpr (UNI) {
+            for (int t = threadIdx.x; t < cn; t += DENSE_A_THREADS) {
+                const double *src = tpack + (c0 + t) * TPACK;
+                double *dst = stg + t * TSZ;
+                double sg = 0.0, ag = 0.0;
+#pragma unroll
+                for (int f = 0; f < DIM + 2; ++f) dst[f] = src[f];
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) {
+                    const double G = src[1 + d] * ua.a[d];
+                    dst[DIM + 2 + d] = G;
+                    dst[2 * DIM + 2 + d] = exp2_16(H * G, tab);
+                    sg += G;
+                    ag += fabs(G);
+                }
+                dst[3 * DIM + 2] = sg;
+                dst[3 * DIM + 3] = ag;
+            }
+        } else {
+            for (int i = threadIdx.x; i < cn * TSZ; i += DENSE_A_THREADS) {
+                const int t = i / TSZ, f = i - t * TSZ;
+                stg[i] = tpack[(c0 + t) * TPACK + f];
+            }
         }
         __syncthreads();
         for (int t = 0; t < cn; ++t) {
@@ -235,9 +264,17 @@ k_value_dense_tensor(const double *__restrict__ x, const double *__restrict__ tp
 #pragma unroll
             for (int d = 0; d < DIM; ++d) {
                 B0 = fma(tp[1 + d], cp[d], B0);
-                G[d] = tp[1 + d] * ah[d];
-                sg += G[d];
-                ag += fabs(G[d]);
+                if constexpr (UNI) {
+                    G[d] = tp[DIM + 2 + d];
+                } else {
+                    G[d] = tp[1 + d] * ah[d];
+                    sg += G[d];
+                    ag += fabs(G[d]);
+                }
+            }
+            if constexpr (UNI) {
+                sg = tp[3 * DIM + 2];
+                ag = tp[3 * DIM + 3];
             }
             const double ub = B0 + ag;
             if (ub - M > LSE_THR) {   // raise the shift (the first target sets it)
@@ -251,7 +288,7 @@ k_value_dense_tensor(const double *__restrict__ x, const double *__restrict__ tp
             const double P = tp[1 + DIM] * exp2_16(B0 - sg - M, tab);
             double r[DIM];
 #pragma unroll
-            for (int d = 0; d < DIM; ++d) r[d] = exp2_16(H * G[d], tab);
+            for (int d = 0; d < DIM; ++d) r[d] = UNI ? tp[2 * DIM + 2 + d] : exp2_16(H * G[d], tab);
 #pragma unroll
             for (int i0 = 0; i0 < TM; ++i0) {
                 const double f0 = i0 == 0 ? P : (i0 == 1 ? P * r[0] : P * r[0] * r[0]);
@@ -838,15 +875,21 @@ static DenseShape dense_shape(int64_t nq, int64_t nt, int tm = 0, int64_t ncells
 }
 
 template <int DIM>
-static void launch_value_dense_tensor(const DenseShape &ds, const double *x, const double *tpack, const EvalArgs &a,
-                                      int64_t ncells, double *ms, cudaStream_t st)
+static void launch_value_dense_tensor(const sdot_ctx *c, const DenseShape &ds, const double *tpack,
+                                      const EvalArgs &a, double *ms, cudaStream_t st)
 {
     const dim3 grid((unsigned)ds.ncb, (unsigned)ds.nvs);
+    Spacing ua;
+    for (int d = 0; d < 3; ++d) ua.a[d] = c->tensor_a[d];
+    auto go = [&](auto kern) {
+        kern<<<grid, DENSE_A_THREADS, 0, st>>>(c->x.p, tpack, a, c->ncells, ds.tslice, ua, ms);
+    };
+    const bool uni = c->tensor_uniform;
     if constexpr (DIM == 2) {
-        if (ds.tm == 3) k_value_dense_tensor<2, 3><<<grid, DENSE_A_THREADS, 0, st>>>(x, tpack, a, ncells, ds.tslice, ms);
-        else k_value_dense_tensor<2, 2><<<grid, DENSE_A_THREADS, 0, st>>>(x, tpack, a, ncells, ds.tslice, ms);
+        if (ds.tm == 3) uni ? go(k_value_dense_tensor<2, 3, true>) : go(k_value_dense_tensor<2, 3, false>);
+        else uni ? go(k_value_dense_tensor<2, 2, true>) : go(k_value_dense_tensor<2, 2, false>);
     } else {
-        k_value_dense_tensor<3, 2><<<grid, DENSE_A_THREADS, 0, st>>>(x, tpack, a, ncells, ds.tslice, ms);
+        uni ? go(k_value_dense_tensor<3, 2, true>) : go(k_value_dense_tensor<3, 2, false>);
     }
 }
 
@@ -913,7 +956,7 @@ static sdot_status run_eval(sdot_ctx *c, const EvalArgs &a, bool dense, const do
         if (ds.tm > 0) {
             const cudaError_t e = c->vpart.alloc((size_t)2 * ds.nvs * a.nq);
             if (e != cudaSuccess) return cuda_error(c, e, "dense value slices");
-            launch_value_dense_tensor<DIM>(ds, c->x.p, c->tpack.p, a, c->ncells, c->vpart.p, st);
+            launch_value_dense_tensor<DIM>(c, ds, c->tpack.p, a, c->vpart.p, st);
             k_value_dense_merge<DIM><<<(unsigned)nval, MERGE_THREADS, 0, st>>>(c->x.p, c->rho.p, c->jxw.p, c->vpart.p,
                                                                                ds.nvs, a, c->Lq.p, c->blkpart.p);
         } else if (ds.nvs > 1) {
@@ -1250,7 +1293,7 @@ static void noalloc_launch(sdot_ctx *c, const EvalArgs &a, double *S, const Noal
     k_target_prep<DIM><<<grid_for(a.nt, 256), 256, 0, st>>>(a.nt, c->y.p, c->nu.p, psi, a, tpack);
     if (L.ds.tm > 0) {
         double *vpart = S + L.vpart;
-        launch_value_dense_tensor<DIM>(L.ds, c->x.p, tpack, a, c->ncells, vpart, st);
+        launch_value_dense_tensor<DIM>(c, L.ds, tpack, a, vpart, st);
         k_value_dense_merge<DIM><<<(unsigned)L.nval, MERGE_THREADS, 0, st>>>(c->x.p, c->rho.p, c->jxw.p, vpart, L.nvs,
                                                                              a, Lq, blkpart);
     } else if (L.nvs > 1) {

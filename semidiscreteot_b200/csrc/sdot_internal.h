@@ -171,6 +171,8 @@ struct sdot_ctx {
     double delta_max = 0.0;            // max distance of a quadrature point to its cell centre
     int tensor_m = 0;                  // > 0: points form an m^dim tensor grid symmetric about the cell centre
     double tensor_amax = 0.0;          // largest per-dimension offset of that grid
+    bool tensor_uniform = false;       // the same offset per dimension in every cell (within 1e-13)
+    double tensor_a[3] = {0, 0, 0};    // that offset
 
     // ---- truncated path: block-pair lists and gradient partials ----
     sdot::DevBuf<int64_t> fwd_cnt, fwd_off, inv_cnt, inv_off, fwd2inv;
