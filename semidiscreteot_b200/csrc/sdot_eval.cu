@@ -383,11 +383,15 @@ __device__ __forceinline__ R cell_sum(const R *W, const R *r)
 // Non-finite L_q: a cell whose parts are all -inf contributes 0 (as every
 // one of its terms does); a +inf part gives a NaN term where the per-point
 // form gives +inf (both non-finite, flagged by the finalize).
-template <int DIM, int TM, bool FP32>
+// UNI (FP64 form, every cell has the offsets ua_d): G_d and its factor
+// depend on the target alone and are computed once per target, so one
+// exponential per (cell, target) remains.  (The FP32 form measured slower
+// with its factors split into cell and target parts: registers.)
+template <int DIM, int TM, bool FP32, bool UNI>
 __global__ void __launch_bounds__(DENSE_B_CTA, DENSE_B_PER_SM)
 k_grad_dense_tensor(const double *__restrict__ x, const double *__restrict__ w, const double *__restrict__ Lq,
                     const double *__restrict__ tpack, const double *__restrict__ psi, EvalArgs a, int64_t ncells,
-                    int64_t cslice, double *__restrict__ gpart)
+                    int64_t cslice, Spacing ua, double *__restrict__ gpart)
 {
     constexpr int NQ = DIM == 3 ? TM * TM * TM : TM * TM;
     constexpr int TT = DENSE_B_TT;
@@ -396,6 +400,7 @@ k_grad_dense_tensor(const double *__restrict__ x, const double *__restrict__ w, 
     constexpr int GC = NTH / NQ < 64 ? NTH / NQ : 64;  // cells staged at a time: one point per thread
     constexpr int CR = 16;                             // cell record: W (NQ), C (DIM), k (DIM), reference
     static_assert(NQ + 2 * DIM + 1 <= CR, "cell record");
+    static_assert(!(UNI && FP32), "per-target factors: FP64 form only");
     constexpr double H = TM == 2 ? 2.0 : 1.0;
     using R = typename std::conditional<FP32, float, double>::type;
     __shared__ double tab[16];
@@ -411,6 +416,21 @@ k_grad_dense_tensor(const double *__restrict__ x, const double *__restrict__ w, 
     double acc64[TT];
 #pragma unroll
     for (int k = 0; k < TT; ++k) acc64[k] = 0.0;
+    // UNI: the per-dimension factors and their exponents' sum, per target
+    double rt[TT][DIM], st[TT];
+    if constexpr (UNI) {
+        __syncthreads();  // tab
+#pragma unroll
+        for (int k = 0; k < TT; ++k) {
+            st[k] = 0.0;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                const double G = T.B[k][d] * ua.a[d];
+                rt[k][d] = exp2_16(H * G, tab);
+                st[k] += G;
+            }
+        }
+    }
     const int64_t ca = blockIdx.y * cslice;
     const int64_t cb = min(ncells, ca + cslice);
     const float c32 = (float)a.c32;
@@ -523,10 +543,15 @@ k_grad_dense_tensor(const double *__restrict__ x, const double *__restrict__ w, 
 #pragma unroll
                     for (int d = 0; d < DIM; ++d) {
                         B0 = fma(T.B[k][d], Cm[d], B0);
-                        const double G = T.B[k][d] * ad[d];
-                        sg += G;
-                        r[d] = exp2_16(H * G, tab);
+                        if constexpr (UNI) {
+                            r[d] = rt[k][d];
+                        } else {
+                            const double G = T.B[k][d] * ad[d];
+                            sg += G;
+                            r[d] = exp2_16(H * G, tab);
+                        }
                     }
+                    if constexpr (UNI) sg = st[k];
                     const double P = exp2_16(B0 - sg + Dref, tab);
                     acc64[k] = fma(P, cell_sum<DIM, TM, double>(Wc, r), acc64[k]);
                 }
@@ -912,14 +937,23 @@ static void launch_grad_dense(const sdot_ctx *c, const DenseShape &ds, bool fp32
     const dim3 g((unsigned)ds.tb, (unsigned)ds.nks);
     if (dense_grad_tensor(c, ds.tm, fp32, a)) {
         const int64_t cs = (c->ncells + ds.nks - 1) / ds.nks;
+        Spacing ua;
+        for (int d = 0; d < 3; ++d) ua.a[d] = c->tensor_a[d];
         auto go = [&](auto kern) {
-            kern<<<g, DENSE_B_CTA, 0, st>>>(c->x.p, c->w.p, Lq, tpack, psi, a, c->ncells, cs, gpart);
+            kern<<<g, DENSE_B_CTA, 0, st>>>(c->x.p, c->w.p, Lq, tpack, psi, a, c->ncells, cs, ua, gpart);
         };
+        const bool uni = c->tensor_uniform;
         if constexpr (DIM == 2) {
-            if (ds.tm == 3) fp32 ? go(k_grad_dense_tensor<2, 3, true>) : go(k_grad_dense_tensor<2, 3, false>);
-            else fp32 ? go(k_grad_dense_tensor<2, 2, true>) : go(k_grad_dense_tensor<2, 2, false>);
+            if (ds.tm == 3) {
+                if (fp32) go(k_grad_dense_tensor<2, 3, true, false>);
+                else uni ? go(k_grad_dense_tensor<2, 3, false, true>) : go(k_grad_dense_tensor<2, 3, false, false>);
+            } else {
+                if (fp32) go(k_grad_dense_tensor<2, 2, true, false>);
+                else uni ? go(k_grad_dense_tensor<2, 2, false, true>) : go(k_grad_dense_tensor<2, 2, false, false>);
+            }
         } else {
-            fp32 ? go(k_grad_dense_tensor<3, 2, true>) : go(k_grad_dense_tensor<3, 2, false>);
+            if (fp32) go(k_grad_dense_tensor<3, 2, true, false>);
+            else uni ? go(k_grad_dense_tensor<3, 2, false, true>) : go(k_grad_dense_tensor<3, 2, false, false>);
         }
         return;
     }
