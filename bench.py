@@ -283,7 +283,7 @@ class ClockSampler:
 #     ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum
 #         --clock-control none -k regex:k_fused -s 3 -c 1 --csv
 #         python bench.py --steps 1 --warmup 3 --no-cpu-baseline --no-extra
-#   k_value_dense / k_grad_dense, dense_2d: the inputs (0.9 MB) stay in L2, so
+#   dense sweeps (k_value_dense_tensor, k_grad_dense_tensor, ...), dense_2d: the inputs (0.9 MB) stay in L2, so
 #     DRAM traffic is not a meaningful bound there (null).
 TRAFFIC_BYTES = {
     ("trunc_3d", "hybrid"): 298063360.0,
@@ -461,16 +461,17 @@ def roofline_of(m, wl, peaks, precision):
     if tv >= tg or truncated:
         ach = VALUE_FLOPS_PER_PAIR[dim] * pairs / (tv * 1e-3) / 1e12
         kname = ("k_fused (FP64 exp2 value sweep + FP32 ex2 gradient sweep, one kernel)" if truncated else
-                 "dense FP64 value sweep: k_value_dense_tensor (per tensor-grid cell and target slice) + "
-                 "k_value_dense_merge, or per point; flops counted for the unfactored form")
+                 "dense FP64 value sweep: k_value_dense_tensor (per tensor-grid cell and target slice; one "
+                 "exponential per cell and target on uniform grids) + k_value_dense_merge, or per point; flops "
+                 "counted for the unfactored form")
         return {"kernel": kname, "bound": "fp64", "achieved": ach, "peak": peaks["fp64_tflops"], "unit": "TFLOP/s",
                 "frac": ach / peaks["fp64_tflops"], "traffic": TRAFFIC_BYTES.get((wl["name"], precision)),
                 "flops_per_pair": VALUE_FLOPS_PER_PAIR[dim], "ms_per_launch": tv,
                 "peak_source": "measured on this GPU by sdot_measure_peaks (FP64 FMA chains); "
                                "MEASURED_PEAKS.json has no FP64 figure"}
     ach = pairs / (tg * 1e-3) / 1e9
-    return {"kernel": "k_grad_dense (FP32 ex2 gradient sweep)" if precision != "fp64" else
-            "k_grad_dense (FP64 exp2 gradient sweep)", "bound": "mufu", "achieved": ach,
+    return {"kernel": "k_grad_dense_tensor / k_grad_dense (FP32 ex2 gradient sweep)" if precision != "fp64" else
+            "k_grad_dense_tensor / k_grad_dense (FP64 exp2 gradient sweep)", "bound": "mufu", "achieved": ach,
             "peak": peaks["ex2_gops"], "unit": "Gex2/s", "frac": ach / peaks["ex2_gops"],
             "traffic": TRAFFIC_BYTES.get((wl["name"], precision)), "ms_per_launch": tg,
             "peak_source": "measured on this GPU by sdot_measure_peaks (ex2.approx chains)"}

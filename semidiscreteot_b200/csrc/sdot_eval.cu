@@ -595,26 +595,35 @@ k_grad_dense(const double *__restrict__ x, const double *__restrict__ w, const d
 
 constexpr int FIN_THREADS = 256;
 constexpr int FIN_BLOCKS = 148;  // largest grid of k_finalize_grad
-constexpr int FIN_PARTS = 8;     // lanes per target in k_finalize_grad
 constexpr int NRED = 8;  // psinu, l1, linf, comp, l2sq, gp, nonfinite, unused
 
-// Grid of k_finalize_grad for nt targets (FIN_THREADS / FIN_PARTS targets per CTA and pass).
-static int fin_blocks(int64_t nt)
+// Lanes per target of k_finalize_grad for nks slice partials: the smallest
+// power of two >= nks, at most 8.
+static int fin_parts(int nks)
 {
-    const int64_t per = FIN_THREADS / FIN_PARTS;
+    return nks <= 1 ? 1 : (nks <= 2 ? 2 : (nks <= 4 ? 4 : 8));
+}
+
+// Grid of k_finalize_grad for nt targets (FIN_THREADS / parts targets per CTA and pass).
+static int fin_blocks(int64_t nt, int parts)
+{
+    const int64_t per = FIN_THREADS / parts;
     const int64_t g = (nt + per - 1) / per;
     return (int)std::max<int64_t>(1, std::min<int64_t>(FIN_BLOCKS, g));
 }
 
-// Lanes 8t .. 8t+7 of a warp own target j: lane u sums the slice partials
-// k = u, u + 8, ... in order of k (the eight interleaved sums, each with its
-// loads in flight together), and three xor exchanges add them in the fixed
-// tree ((s0 + s1) + (s2 + s3)) + ((s4 + s5) + (s6 + s7)).
+// PARTS consecutive lanes own target j: lane u sums the slice partials
+// k = u, u + PARTS, ... in order of k (each lane's loads in flight together),
+// and xor exchanges add the lanes' sums in the fixed tree (s0 + s1) + (s2 +
+// s3), ...  Any PARTS >= nks gives the same sums as eight interleaved sums
+// k mod 8 added in the tree ((s0 + s1) + (s2 + s3)) + ((s4 + s5) + (s6 + s7)).
+template <int PARTS>
 __global__ void __launch_bounds__(FIN_THREADS)
 k_finalize_grad(int64_t nt, int nks, const double *__restrict__ gpart, const double *__restrict__ nu,
                 const double *__restrict__ psi, const double *__restrict__ pdir, double tol, int sub_nu,
                 double *__restrict__ grad, double *__restrict__ redpart)
 {
+    constexpr int FIN_PARTS = PARTS;
     constexpr int TPB = FIN_THREADS / FIN_PARTS;  // targets per CTA and pass
     const int u = threadIdx.x % FIN_PARTS;
     double psinu = 0.0, l1 = 0.0, linf = 0.0, comp = -CUDART_INF, l2 = 0.0, gp = 0.0, bad = 0.0;
@@ -676,83 +685,112 @@ k_finalize_grad(int64_t nt, int nks, const double *__restrict__ gpart, const dou
     }
 }
 
-// One CTA of FIN_SCALAR_THREADS: thread i sums value partials i, i + T, i +
-// 2T, ... into four accumulators (partial i + kT into accumulator k mod 4,
-// four loads in flight), added in a fixed order, and the gradient blocks'
-// reductions i, i + T, ...; then warp and CTA reductions in a fixed tree.
-constexpr int FIN_SCALAR_THREADS = 256;
-__global__ void __launch_bounds__(FIN_SCALAR_THREADS)
+// k_finalize_grad with fin_parts(nks) lanes per target; returns its grid size.
+static int launch_finalize_grad(int64_t nt, int nks, const double *gpart, const double *nu, const double *psi,
+                                const double *pdir, double tol, int sub_nu, double *grad, double *redpart,
+                                cudaStream_t st)
+{
+    const int parts = fin_parts(nks);
+    const int fb = fin_blocks(nt, parts);
+    auto go = [&](auto kern) {
+        kern<<<fb, FIN_THREADS, 0, st>>>(nt, nks, gpart, nu, psi, pdir, tol, sub_nu, grad, redpart);
+    };
+    if (parts == 1) go(k_finalize_grad<1>);
+    else if (parts == 2) go(k_finalize_grad<2>);
+    else if (parts == 4) go(k_finalize_grad<4>);
+    else go(k_finalize_grad<8>);
+    return fb;
+}
+
+// One CTA of T threads: thread i sums value partials i, i + T, i + 2T, ...
+// into four accumulators (partial i + kT into accumulator k mod 4, eight
+// loads in flight), added in a fixed order, and the gradient blocks'
+// reductions i, i + T, ...; then warp reductions, and warp 0 reduces the
+// warps' results (a fixed tree throughout).  T = 256 for up to 2,048 value
+// partials (the dense path), 1,024 above (one per source block).
+template <int T>
+__global__ void __launch_bounds__(T)
 k_finalize_scalars(int nred, const double *__restrict__ redpart, int64_t nval, const double *__restrict__ valpart,
                    double *__restrict__ scal)
 {
-    constexpr int T = FIN_SCALAR_THREADS;
-    __shared__ double sh[11][T / 32];
+    constexpr int NW = T / 32;
+    __shared__ double sh[11][NW];
     double va[4] = {0, 0, 0, 0}, ca[4] = {0, 0, 0, 0}, ska[4] = {0, 0, 0, 0}, npa[4] = {0, 0, 0, 0};
     const double4 *vp = reinterpret_cast<const double4 *>(valpart);
     int64_t b0 = threadIdx.x;
-    for (; b0 + 3 * T < nval; b0 += 4 * T) {
-        double4 t[4];
+    for (; b0 + 7 * T < nval; b0 += 8 * T) {
+        double4 t[8];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) t[u] = vp[b0 + u * T];
+        for (int u = 0; u < 8; ++u) t[u] = vp[b0 + u * T];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            va[u] += t[u].x;
-            ca[u] += t[u].y;
-            ska[u] += t[u].z;
-            npa[u] += t[u].w;
+        for (int u = 0; u < 8; ++u) {
+            va[u & 3] += t[u].x;
+            ca[u & 3] += t[u].y;
+            ska[u & 3] += t[u].z;
+            npa[u & 3] += t[u].w;
         }
     }
 #pragma unroll
-    for (int u = 0; u < 3; ++u) {
+    for (int u = 0; u < 7; ++u) {
         if (b0 + u * T < nval) {
             const double4 t = vp[b0 + u * T];
-            va[u] += t.x;
-            ca[u] += t.y;
-            ska[u] += t.z;
-            npa[u] += t.w;
+            va[u & 3] += t.x;
+            ca[u & 3] += t.y;
+            ska[u & 3] += t.z;
+            npa[u & 3] += t.w;
         }
     }
     double v = (va[0] + va[1]) + (va[2] + va[3]), c = (ca[0] + ca[1]) + (ca[2] + ca[3]);
     double sk = (ska[0] + ska[1]) + (ska[2] + ska[3]), np = (npa[0] + npa[1]) + (npa[2] + npa[3]);
     double r[7] = {0, 0, 0, -CUDART_INF, 0, 0, 0};
-    for (int b = threadIdx.x; b < nred; b += blockDim.x) {
-        const double *p = redpart + b * NRED;
+    for (int b = threadIdx.x; b < nred; b += T) {
+        const double *p = redpart + (int64_t)b * NRED;
         r[0] += p[0]; r[1] += p[1]; r[2] = fmax(r[2], p[2]); r[3] = fmax(r[3], p[3]);
         r[4] += p[4]; r[5] += p[5]; r[6] = fmax(r[6], p[6]);
     }
     v = warp_sum(v); c = warp_sum(c); sk = warp_sum(sk); np = warp_sum(np);
     r[0] = warp_sum(r[0]); r[1] = warp_sum(r[1]); r[2] = warp_max(r[2]); r[3] = warp_max(r[3]);
     r[4] = warp_sum(r[4]); r[5] = warp_sum(r[5]); r[6] = warp_max(r[6]);
-    const int wi = threadIdx.x >> 5;
-    if ((threadIdx.x & 31) == 0) {
+    const int wi = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
         sh[0][wi] = v; sh[1][wi] = c; sh[2][wi] = sk; sh[10][wi] = np;
+#pragma unroll
         for (int k = 0; k < 7; ++k) sh[3 + k][wi] = r[k];
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        double t[10] = {0, 0, 0, 0, 0, 0, -CUDART_INF, 0, 0, 0};
-        double tnp = 0.0;
-        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) {
-            tnp += sh[10][i];
-            t[0] += sh[0][i]; t[1] += sh[1][i]; t[2] += sh[2][i];
-            t[3] += sh[3][i]; t[4] += sh[4][i]; t[5] = fmax(t[5], sh[5][i]); t[6] = fmax(t[6], sh[6][i]);
-            t[7] += sh[7][i]; t[8] += sh[8][i]; t[9] = fmax(t[9], sh[9][i]);
+    if (wi == 0) {
+        double t[11];
+        // sums: 0 value, 1 C, 2 skipped, 3 psinu, 4 l1, 7 l2sq, 8 dot_gp, 10 pairs; maxima: 5 linf, 6 comp, 9 bad
+#pragma unroll
+        for (int k = 0; k < 11; ++k)
+            t[k] = lane < NW ? sh[k][lane] : ((k == 5 || k == 6 || k == 9) ? -CUDART_INF : 0.0);
+#pragma unroll
+        for (int k = 0; k < 11; ++k) t[k] = (k == 5 || k == 6 || k == 9) ? warp_max(t[k]) : warp_sum(t[k]);
+        if (lane == 0) {
+            const double psinu = t[3];
+            const double value = t[0] - psinu;
+            scal[SC_VALUE] = value;
+            scal[SC_VALSRC] = t[0];
+            scal[SC_C] = t[1];
+            scal[SC_SKIPPED] = t[2];
+            scal[SC_PSINU] = psinu;
+            scal[SC_L1] = t[4];
+            scal[SC_LINF] = t[5];
+            scal[SC_COMP] = t[6];
+            scal[SC_L2SQ] = t[7];
+            scal[SC_DOT_GP] = t[8];
+            scal[SC_NONFINITE] = (t[9] != 0.0 || !isfinite(value)) ? 1.0 : 0.0;
+            scal[SC_PAIRS] = t[10];
         }
-        const double psinu = t[3];
-        const double value = t[0] - psinu;
-        scal[SC_VALUE] = value;
-        scal[SC_VALSRC] = t[0];
-        scal[SC_C] = t[1];
-        scal[SC_SKIPPED] = t[2];
-        scal[SC_PSINU] = psinu;
-        scal[SC_L1] = t[4];
-        scal[SC_LINF] = t[5];
-        scal[SC_COMP] = t[6];
-        scal[SC_L2SQ] = t[7];
-        scal[SC_DOT_GP] = t[8];
-        scal[SC_NONFINITE] = (t[9] != 0.0 || !isfinite(value)) ? 1.0 : 0.0;
-        scal[SC_PAIRS] = tnp;
     }
+}
+
+// k_finalize_scalars with its CTA size for nval value partials.
+static void launch_finalize_scalars(cudaStream_t st, int nred, const double *redpart, int64_t nval,
+                                    const double *valpart, double *scal)
+{
+    if (nval <= 2048) k_finalize_scalars<256><<<1, 256, 0, st>>>(nred, redpart, nval, valpart, scal);
+    else k_finalize_scalars<1024><<<1, 1024, 0, st>>>(nred, redpart, nval, valpart, scal);
 }
 
 // ---------------------------------------------------------------------------
@@ -1015,10 +1053,9 @@ static sdot_status run_eval(sdot_ctx *c, const EvalArgs &a, bool dense, const do
         if (s != SDOT_OK) return s;
     }
     if (dense) mark(3);
-    const int fb = fin_blocks(a.nt);
-    k_finalize_grad<<<fb, FIN_THREADS, 0, st>>>(a.nt, nks, c->gpart.p, c->nu.p, c->psi.p, pdir, tol, partial ? 0 : 1,
-                                                c->grad.p, c->redpart.p);
-    k_finalize_scalars<<<1, FIN_SCALAR_THREADS, 0, st>>>(fb, c->redpart.p, nval, c->blkpart.p, c->scal.p);
+    const int fb = launch_finalize_grad(a.nt, nks, c->gpart.p, c->nu.p, c->psi.p, pdir, tol, partial ? 0 : 1, c->grad.p,
+                                        c->redpart.p, st);
+    launch_finalize_scalars(st, fb, c->redpart.p, nval, c->blkpart.p, c->scal.p);
     mark(4);
     c->klaunch[1] += 1;
     if (dense && c->distance == 0) {
@@ -1341,10 +1378,9 @@ static void noalloc_launch(sdot_ctx *c, const EvalArgs &a, double *S, const Noal
                                                                           blkpart);
     }
     launch_grad_dense<DIM>(c, L.ds, c->precision != SDOT_PREC_FP64, Lq, tpack, psi, a, gpart, st);
-    const int fb = fin_blocks(a.nt);
-    k_finalize_grad<<<fb, FIN_THREADS, 0, st>>>(a.nt, L.nks, gpart, c->nu.p, psi, nullptr, c->prm.tolerance, 1, grad,
-                                                redpart);
-    k_finalize_scalars<<<1, FIN_SCALAR_THREADS, 0, st>>>(fb, redpart, L.nval, blkpart, scal);
+    const int fb = launch_finalize_grad(a.nt, L.nks, gpart, c->nu.p, psi, nullptr, c->prm.tolerance, 1, grad, redpart,
+                                        st);
+    launch_finalize_scalars(st, fb, redpart, L.nval, blkpart, scal);
 }
 
 }  // namespace sdot
