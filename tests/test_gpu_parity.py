@@ -43,6 +43,20 @@ def make_problem(kind, seed=0):
         y = rng.random((N, 3))
         nu = np.full(N, 1.0 / N)
         prm = dict(epsilon=1e-2, tau=0.0)
+    elif kind == "dense2d_o2":
+        # 2 x 2 Gauss points per cell: the TM = 2 tensor sweeps in 2D
+        src = structured_source(2, 20, 2, nodal_density=lambda p: 1.0 + 0.5 * p[:, 1])
+        N = 500
+        y = rng.random((N, 2))
+        nu = rng.dirichlet(np.ones(N) * 20)
+        prm = dict(epsilon=2e-2, tau=0.0)
+    elif kind == "graded2d":
+        # cells of different widths along x: tensor grids whose spacing varies from cell to cell
+        src = graded_source(rng, 2, 18, 3)
+        N = 600
+        y = rng.random((N, 2))
+        nu = np.full(N, 1.0 / N)
+        prm = dict(epsilon=2e-2, tau=0.0)
     elif kind == "order3_3d":
         src = structured_source(3, 6, 3)
         N = 600
@@ -52,6 +66,27 @@ def make_problem(kind, seed=0):
     else:
         raise KeyError(kind)
     return src, y, nu, prm
+
+
+def graded_source(rng, dim, n, order):
+    """structured_source with the cell columns along x given random widths (each cell mapped affinely, so
+    its points stay a tensor grid symmetric about its centre, with a spacing of its own)."""
+    src = structured_source(dim, n, order)
+    h = 1.0 / n
+    wid = rng.uniform(0.5, 1.5, n)
+    wid /= wid.sum()
+    left = np.concatenate([[0.0], np.cumsum(wid)[:-1]])
+    qpc = order ** dim
+    ncell = src["cell_centers"].shape[0]
+    col = np.arange(ncell) % n                    # cells are x fastest
+    x = src["x"].copy().reshape(ncell, qpc, dim)
+    x0 = col * h
+    x[:, :, 0] = left[col][:, None] + (x[:, :, 0] - x0[:, None]) * (wid[col] / h)[:, None]
+    c = src["cell_centers"].copy()
+    c[:, 0] = left[col] + 0.5 * wid[col]
+    jxw = (src["jxw"].reshape(ncell, qpc) * (wid[col] / h)[:, None]).ravel()
+    return dict(x=x.reshape(-1, dim), jxw=jxw, density=src["density"], cell_offsets=src["cell_offsets"],
+                cell_centers=c)
 
 
 def product(src, y, nu, dim, precision):
@@ -70,7 +105,7 @@ def grad_tol(nu, precision):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "hybrid"])
-@pytest.mark.parametrize("kind", ["dense2d", "trunc2d", "trunc3d", "dense3d", "order3_3d"])
+@pytest.mark.parametrize("kind", ["dense2d", "trunc2d", "trunc3d", "dense3d", "order3_3d", "dense2d_o2", "graded2d"])
 @pytest.mark.parametrize("lse", [True, False])
 def test_evaluate_matches_oracle(oracle_mod, kind, precision, lse):
     src, y, nu, kw = make_problem(kind)
