@@ -658,10 +658,13 @@ __global__ void __launch_bounds__(DG ? DG_THREADS : THREADS, 1) k_hessian_tc(con
                 const int col = cq * 64 + c16 * 16 + i;
                 const size_t idx = (size_t)col * M + row;
                 double s = (double)v[i];
-                if (!first) s += scr[idx];
                 if (!last) {
-                    scr[idx] = s;
+                    // one thread owns each scratch entry, so a posted add (its result unused) keeps the chunk
+                    // order and the rounding of a load + add + store without waiting for the load
+                    if (first) scr[idx] = s;
+                    else atomicAdd(&scr[idx], s);
                 } else {
+                    if (!first) s += scr[idx];
                     const int64_t gb = (int64_t)tl.y * N + col;
                     if (ga < a.n && gb < a.n && gb >= ga) {
                         const double h = ((gb == ga ? a.diag[ga] : 0.0) - s) * a.inv_eps;
