@@ -10,6 +10,7 @@ sets are bit-exact: the number of (q, target) pairs must equal the oracle's.
 import numpy as np
 import pytest
 
+from cell_sources import graded_source
 from semidiscreteot_b200 import SolverParameters, SotSolver, structured_source
 
 pytestmark = pytest.mark.gpu
@@ -66,27 +67,6 @@ def make_problem(kind, seed=0):
     else:
         raise KeyError(kind)
     return src, y, nu, prm
-
-
-def graded_source(rng, dim, n, order):
-    """structured_source with the cell columns along x given random widths (each cell mapped affinely, so
-    its points stay a tensor grid symmetric about its centre, with a spacing of its own)."""
-    src = structured_source(dim, n, order)
-    h = 1.0 / n
-    wid = rng.uniform(0.5, 1.5, n)
-    wid /= wid.sum()
-    left = np.concatenate([[0.0], np.cumsum(wid)[:-1]])
-    qpc = order ** dim
-    ncell = src["cell_centers"].shape[0]
-    col = np.arange(ncell) % n                    # cells are x fastest
-    x = src["x"].copy().reshape(ncell, qpc, dim)
-    x0 = col * h
-    x[:, :, 0] = left[col][:, None] + (x[:, :, 0] - x0[:, None]) * (wid[col] / h)[:, None]
-    c = src["cell_centers"].copy()
-    c[:, 0] = left[col] + 0.5 * wid[col]
-    jxw = (src["jxw"].reshape(ncell, qpc) * (wid[col] / h)[:, None]).ravel()
-    return dict(x=x.reshape(-1, dim), jxw=jxw, density=src["density"], cell_offsets=src["cell_offsets"],
-                cell_centers=c)
 
 
 def product(src, y, nu, dim, precision):
