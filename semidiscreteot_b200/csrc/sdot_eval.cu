@@ -615,8 +615,9 @@ static int fin_blocks(int64_t nt, int parts)
 // PARTS consecutive lanes own target j: lane u sums the slice partials
 // k = u, u + PARTS, ... in order of k (each lane's loads in flight together),
 // and xor exchanges add the lanes' sums in the fixed tree (s0 + s1) + (s2 +
-// s3), ...  Any PARTS >= nks gives the same sums as eight interleaved sums
-// k mod 8 added in the tree ((s0 + s1) + (s2 + s3)) + ((s4 + s5) + (s6 + s7)).
+// s3), ...  PARTS = 8, or any power of two PARTS >= nks, gives the sums of
+// eight interleaved sums k mod 8 added in the tree ((s0 + s1) + (s2 + s3)) +
+// ((s4 + s5) + (s6 + s7)) (the lanes past nks hold zeros).
 template <int PARTS>
 __global__ void __launch_bounds__(FIN_THREADS)
 k_finalize_grad(int64_t nt, int nks, const double *__restrict__ gpart, const double *__restrict__ nu,
